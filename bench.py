@@ -1,0 +1,302 @@
+"""Benchmark: RK2 steps/s of the split RK2 step at 720x720x75, bt_nsteps=50.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: the seeded beta-plane state (CFG init,
+Philox4x32-10 normals, dt = 600 s, Kh = 1e3, halo fill on), ni = nj = 720,
+nk = 75, bt_nsteps = 50, plain FP64.  One "step" is one split RK2 iteration
+of rk2_serial_driver.F90:218-399 on the whole domain.  The state (~6 GB)
+stays resident in HBM and is far larger than L2, so no L2 flush is needed
+between steps.  Under torchrun each rank advances its own replica of the
+domain (the path does not shard across GPUs: replicas only, weak scaling);
+the timed region is bracketed by a barrier and device synchronisation and
+the time is the maximum over ranks.
+
+--impl reference times the reference's CPU implementation of the path on the
+host cores: the C restatement of the serial Fortran driver (the Fortran
+itself cannot be compiled here), on rank 0 only.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NI, NJ, NK, BT = 720, 720, 75, 50
+N3 = (NI + 2) * (NJ + 2) * NK * 8
+N2 = (NI + 2) * (NJ + 2) * 8
+# algorithmic bytes of one RK2 step: 78 3-D + 30 2-D array touches of the
+# reference's 16 phases (compulsory reads + writes per phase)
+STEP_BYTES = 78 * N3 + 30 * N2
+METRIC = "RK2 steps/s @720x720x75 bt50: plain FP64 vs mixed/learned at stated error"
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as td
+        torch.cuda.set_device(local)
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist = td
+    return world, rank, local, dist
+
+
+def max_over_ranks(x, dist, local):
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x, dist, local):
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def cpu_reference_rate(nthreads, seconds_budget=20.0):
+    """Time the oracle restatement of the serial driver on a bounded sample of
+    the workload: strips of the 720x720x75 bt50 domain, scaled by cell count."""
+    from oracle.pyoracle import INIT_CFG, Oracle, lib
+    # sample: the full 720-point i extent and nj_s rows in j
+    nj_s = 40
+    o = Oracle(NI, nj_s, NK, BT, INIT_CFG, seed=0, dt=600.0)
+    t0 = time.perf_counter()
+    o.step(1)
+    dt = time.perf_counter() - t0
+    o.close()
+    scale = ((NI - 4) * (NJ - 4)) / ((NI - 4) * (nj_s - 4))
+    per_full_step = dt * scale
+    return 1.0 / per_full_step, f"1 RK2 step of a 720x{nj_s}x75 bt50 strip " \
+        f"({dt:.2f} s), scaled by compute cells to 720x720", 1
+
+
+def run_reference(args, world, rank, local, dist):
+    if rank != 0:
+        return
+    rates = []
+    sample = ""
+    for _ in range(args.warmup if args.warmup < 1 else 1):
+        pass
+    for _ in range(max(1, min(args.steps, 3))):
+        r, sample, cores = cpu_reference_rate(1)
+        rates.append(r)
+    value = sorted(rates)[len(rates) // 2]
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "split RK2 step 720x720x75 bt50 (seeded beta plane)",
+                       "ni": NI, "nj": NJ, "nk": NK, "bt_nsteps": BT},
+            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 1,
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local, dist):
+    import numpy as np
+    import torch
+    from hackathon_mom6_miniapp_b200 import INIT_CFG, Model
+    torch.cuda.set_device(local)
+    m = Model(NI, NJ, NK, BT, INIT_CFG, seed=rank, dt=600.0, device=local)
+    stream = torch.cuda.ExternalStream(m.stream(), device=f"cuda:{local}")
+    # warm-up
+    m.step(args.warmup)
+    m.synchronize()
+    barrier(dist)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    m.reset_launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    m.step(args.steps)
+    e1.record(stream)
+    m.synchronize()
+    torch.cuda.synchronize()
+    launches = m.launch_count()
+    ck = clocks.stop()
+    ms_local = e0.elapsed_time(e1)
+    barrier(dist)
+    ms = max_over_ranks(ms_local, dist, local)
+    value = world * args.steps / (ms / 1000.0)
+
+    # per-kernel timing pass (events around every launch) for the roofline
+    m.kernel_timing(True)
+    m.step(max(2, min(args.steps, 5)))
+    m.synchronize()
+    kt = {}
+    for name in ("tendency", "vertvisc", "continuity", "btstep", "halo_fill"):
+        avg, n = m.kernel_time_ms(name)
+        kt[name] = (avg, n)
+    m.kernel_timing(False)
+    steps_t = max(2, min(args.steps, 5))
+    per_step_ms = {k: v[0] * v[1] / steps_t for k, v in kt.items()}
+    dom = max(per_step_ms, key=per_step_ms.get)
+    # compulsory bytes per launch of each fused kernel (3-D arrays)
+    kbytes = {"tendency": 5 * N3 + 10 * N2, "vertvisc": 5 * N3 + 4 * N2,
+              "continuity": 10 * N3 + 7 * N2, "btstep": 6 * N2,
+              "halo_fill": 0}
+    peak, peak_kind = _peaks()
+    dom_avg_ms = kt[dom][0]
+    achieved = kbytes[dom] / (dom_avg_ms / 1000.0) / 1e9 if dom_avg_ms > 0 else 0.0
+
+    # end to end through the public API with pinned host buffers
+    shape3 = (NI + 2, NJ + 2, NK)
+    u = torch.empty(shape3[::-1], dtype=torch.float64, pin_memory=True).numpy().T
+    v = torch.empty(shape3[::-1], dtype=torch.float64, pin_memory=True).numpy().T
+    h = torch.empty(shape3[::-1], dtype=torch.float64, pin_memory=True).numpy().T
+    eta = torch.empty((NJ + 2, NI + 2), dtype=torch.float64, pin_memory=True).numpy().T
+    for name, a in (("u", u), ("v", v), ("h", h), ("eta", eta)):
+        a[...] = m.get(name)
+    barrier(dist)
+    t0 = time.perf_counter()
+    m.step_host(args.steps, u, v, h, eta)
+    t1 = time.perf_counter()
+    e2e_s = max_over_ranks(t1 - t0, dist, local)
+    e2e = world * args.steps / e2e_s
+    bytes_h2d = (3 * N3 + N2) / args.steps
+    bytes_d2h = (3 * N3 + N2) / args.steps
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        r, sample, cores = cpu_reference_rate(1)
+        cpu = {"value": r, "unit": "steps/s", "cores": cores, "kind": "port",
+               "sample": sample}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic",
+                "config": {"workload": "split RK2 step 720x720x75 bt50, plain FP64, "
+                                       "seeded beta plane (Philox), replicas per GPU",
+                           "ni": NI, "nj": NJ, "nk": NK, "bt_nsteps": BT, "dt": 600.0,
+                           "l2": "state 6 GB >> 126 MB L2, no flush needed",
+                           "parallelism": f"replicas x{world}"},
+                "step_bytes_algorithmic": STEP_BYTES,
+                "step_roofline": {"achieved_GBs": STEP_BYTES / (ms / args.steps / 1000.0) / 1e9,
+                                  "peak_GBs": peak, "frac": STEP_BYTES / (ms / args.steps / 1000.0) / 1e9 / peak},
+                "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved,
+                             "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                             "peak_kind": peak_kind, "traffic": None,
+                             "bytes_per_launch": kbytes[dom], "avg_launch_ms": dom_avg_ms},
+                "kernel_ms_per_step": per_step_ms,
+                "cpu_baseline": cpu,
+                "e2e": {"value": e2e, "unit": "steps/s", "h2d_bytes_per_step": bytes_h2d,
+                        "d2h_bytes_per_step": bytes_d2h},
+                "gpu_launches": launches,
+                "clocks": ck}
+        print(json.dumps(line), flush=True)
+    m.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world, rank, local, dist = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank, local, dist)
+        else:
+            run_ours(args, world, rank, local, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

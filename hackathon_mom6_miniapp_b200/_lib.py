@@ -1,0 +1,198 @@
+"""ctypes binding of libmom6b.so (the product library)."""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+INIT_REF, INIT_CFG = 0, 1
+FP64, MIXED = 0, 1
+
+FIELDS = ["u", "v", "h", "h0", "uh", "vh", "up", "vp", "eta", "ubt", "vbt",
+          "ubt_av", "vbt_av", "eta_av", "hu_bt", "FA_u_W0", "FA_u_WW",
+          "FA_u_E0", "FA_u_EE", "uBT_WW", "uBT_EE", "du_cor", "taux_bot",
+          "tauy_bot", "taux", "tauy", "Ray_u", "Ray_v"]
+FID = {n: i for i, n in enumerate(FIELDS)}
+FIELDS_3D = {"u", "v", "h", "h0", "uh", "vh", "up", "vp", "hu_bt", "Ray_u", "Ray_v"}
+
+STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of memory",
+          4: "grid barrier timeout", 5: "invalid state"}
+
+
+class Mom6bError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"mom6b error {code} ({STATUS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+class MixedNotBuilt(Mom6bError):
+    pass
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("ni", ctypes.c_int), ("nj", ctypes.c_int), ("nk", ctypes.c_int),
+                ("bt_nsteps", ctypes.c_int), ("init_mode", ctypes.c_int),
+                ("seed", ctypes.c_uint64), ("dt", ctypes.c_double),
+                ("dx_km", ctypes.c_double), ("lat_deg", ctypes.c_double),
+                ("Kh", ctypes.c_double), ("Kv", ctypes.c_double),
+                ("Kv_ml", ctypes.c_double), ("Kv_extra_bbl", ctypes.c_double),
+                ("Hmix", ctypes.c_double), ("Hbbl", ctypes.c_double),
+                ("bc_fill", ctypes.c_int), ("precision", ctypes.c_int),
+                ("device", ctypes.c_int), ("use_graph", ctypes.c_int)]
+
+
+def library_path():
+    return os.path.join(_HERE, "libmom6b.so")
+
+
+def library():
+    """Load libmom6b.so; raises OSError when it has not been built."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = library_path()
+    if not os.path.exists(path):
+        raise OSError(f"{path} is missing: run __graft_entry__.build() first")
+    L = ctypes.CDLL(path)
+    P, d, vp, i64 = ctypes.POINTER, ctypes.c_double, ctypes.c_void_p, ctypes.c_int64
+    L.mom6b_config_default.argtypes = [P(Config), ctypes.c_int]
+    L.mom6b_create.argtypes = [P(Config), P(vp)]
+    L.mom6b_destroy.argtypes = [vp]
+    L.mom6b_step.argtypes = [vp, ctypes.c_int]
+    L.mom6b_synchronize.argtypes = [vp]
+    L.mom6b_field_size.argtypes = [vp, ctypes.c_int]
+    L.mom6b_field_size.restype = ctypes.c_size_t
+    L.mom6b_get_field.argtypes = [vp, ctypes.c_int, P(d), ctypes.c_size_t]
+    L.mom6b_set_field.argtypes = [vp, ctypes.c_int, P(d), ctypes.c_size_t]
+    L.mom6b_field_device_ptr.argtypes = [vp, ctypes.c_int, P(vp)]
+    L.mom6b_dims.argtypes = [vp, P(ctypes.c_int)]
+    L.mom6b_stream.argtypes = [vp, P(vp)]
+    L.mom6b_step_host.argtypes = [vp, ctypes.c_int, P(d), P(d), P(d), P(d)]
+    L.mom6b_verify.argtypes = [vp, P(d)]
+    L.mom6b_launch_count.argtypes = [vp]
+    L.mom6b_launch_count.restype = i64
+    L.mom6b_reset_launch_count.argtypes = [vp]
+    L.mom6b_reset_launch_count.restype = None
+    L.mom6b_kernel_timing.argtypes = [vp, ctypes.c_int]
+    L.mom6b_kernel_time_ms.argtypes = [vp, ctypes.c_char_p, P(d), P(i64)]
+    L.mom6b_last_error.restype = ctypes.c_char_p
+    L.mom6b_version.restype = ctypes.c_char_p
+    _LIB = L
+    return L
+
+
+def _check(rc):
+    if rc != 0:
+        msg = library().mom6b_last_error().decode()
+        raise Mom6bError(rc, msg)
+
+
+def _dptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Model:
+    """A split RK2 model resident on one GPU (mirrors rk2_serial_driver's
+    state: u, v, h, h0, eta, ubt, vbt, ...)."""
+
+    def __init__(self, ni=180, nj=180, nk=75, bt_nsteps=30, init_mode=INIT_CFG,
+                 seed=0, dt=None, Kh=None, bc_fill=None, precision=FP64,
+                 device=0, use_graph=False):
+        L = library()
+        c = Config()
+        _check(L.mom6b_config_default(ctypes.byref(c), init_mode))
+        c.ni, c.nj, c.nk, c.bt_nsteps, c.seed = ni, nj, nk, bt_nsteps, seed
+        if dt is not None:
+            c.dt = dt
+        if Kh is not None:
+            c.Kh = Kh
+        if bc_fill is not None:
+            c.bc_fill = int(bc_fill)
+        c.precision, c.device, c.use_graph = precision, device, int(use_graph)
+        self.cfg = c
+        h = ctypes.c_void_p()
+        rc = L.mom6b_create(ctypes.byref(c), ctypes.byref(h))
+        if rc != 0:
+            msg = L.mom6b_last_error().decode()
+            if precision == MIXED and "not built" in msg:
+                raise MixedNotBuilt(rc, msg)
+            raise Mom6bError(rc, msg)
+        self._m = h
+        dims = (ctypes.c_int * 8)()
+        _check(L.mom6b_dims(self._m, dims))
+        self.n1, self.n2, self.nk, self.is_, self.ie, self.js, self.je, _ = list(dims)
+
+    def close(self):
+        if getattr(self, "_m", None):
+            library().mom6b_destroy(self._m)
+            self._m = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def shape(self, name):
+        return (self.n1, self.n2, self.nk) if name in FIELDS_3D else (self.n1, self.n2)
+
+    def get(self, name):
+        a = np.zeros(self.shape(name), dtype=np.float64, order="F")
+        _check(library().mom6b_get_field(self._m, FID[name], _dptr(a), a.size))
+        return a
+
+    def set(self, name, a):
+        a = np.asfortranarray(a, dtype=np.float64)
+        if a.shape != self.shape(name):
+            raise ValueError(f"{name}: expected shape {self.shape(name)}, got {a.shape}")
+        _check(library().mom6b_set_field(self._m, FID[name], _dptr(a), a.size))
+
+    def step(self, n=1):
+        _check(library().mom6b_step(self._m, int(n)))
+
+    def synchronize(self):
+        _check(library().mom6b_synchronize(self._m))
+
+    def step_host(self, n, u=None, v=None, h=None, eta=None):
+        """End-to-end: upload the given host arrays, run n steps, download them."""
+        def p(a):
+            if a is None:
+                return None
+            assert a.dtype == np.float64 and a.flags["F_CONTIGUOUS"]
+            return _dptr(a)
+        _check(library().mom6b_step_host(self._m, int(n), p(u), p(v), p(h), p(eta)))
+
+    def verify(self):
+        out = (ctypes.c_double * 7)()
+        _check(library().mom6b_verify(self._m, out))
+        keys = ["mass_init", "mass_final", "rel_error", "max_u", "max_v",
+                "max_eta", "ke_total"]
+        return dict(zip(keys, list(out)))
+
+    def device_ptr(self, name):
+        p = ctypes.c_void_p()
+        _check(library().mom6b_field_device_ptr(self._m, FID[name], ctypes.byref(p)))
+        return p.value
+
+    def stream(self):
+        p = ctypes.c_void_p()
+        _check(library().mom6b_stream(self._m, ctypes.byref(p)))
+        return p.value
+
+    def launch_count(self):
+        return int(library().mom6b_launch_count(self._m))
+
+    def reset_launch_count(self):
+        library().mom6b_reset_launch_count(self._m)
+
+    def kernel_timing(self, enable=True):
+        _check(library().mom6b_kernel_timing(self._m, int(enable)))
+
+    def kernel_time_ms(self, name):
+        ms = ctypes.c_double()
+        n = ctypes.c_int64()
+        _check(library().mom6b_kernel_time_ms(self._m, name.encode(), ctypes.byref(ms),
+                                              ctypes.byref(n)))
+        return ms.value, n.value

@@ -1,0 +1,73 @@
+"""Build libmom6b.so in-tree with nvcc for sm_100a.
+
+Every CUDA source is compiled with
+    -gencode arch=compute_100a,code=sm_100a -O3 -lineinfo --fmad=false
+(no FMA contraction: the FP64 kernels reproduce the serial reference's
+roundings exactly) and linked into hackathon_mom6_miniapp_b200/libmom6b.so.
+Host C++ is compiled with -ffp-contract=off for the same reason.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libmom6b.so")
+NVCC = os.environ.get("NVCC", "nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+CU_FLAGS = ARCH + ["-O3", "-lineinfo", "--fmad=false", "-std=c++17",
+                   "-Xcompiler", "-fPIC,-ffp-contract=off", "-Xptxas", "-O3"]
+CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", "-Wall"]
+
+CU_SOURCES = ["k_tendency.cu", "k_vertvisc.cu", "k_continuity.cu", "k_btstep.cu",
+              "mom6b_api.cu"]
+CXX_SOURCES = ["host_init.cpp"]
+HEADERS = ["common.cuh", "kernels.h", "host_init.h"]
+
+
+def _newer(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
+        raise RuntimeError("compile failed: " + os.path.basename(cmd[-1]))
+    return r
+
+
+def build(verbose=False, force=False):
+    os.makedirs(BUILD, exist_ok=True)
+    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [
+        os.path.join(HERE, "..", "include", "mom6b.h"),
+        os.path.join(HERE, "..", "include", "mom6_cuda_c.h")]
+    objs = []
+    for src in CU_SOURCES + CXX_SOURCES:
+        path = os.path.join(CSRC, src)
+        obj = os.path.join(BUILD, src + ".o")
+        objs.append(obj)
+        if force or _newer(obj, [path] + hdrs):
+            if src.endswith(".cu"):
+                cmd = [NVCC] + CU_FLAGS + ["-I", CSRC, "-c", "-o", obj, path]
+            else:
+                cmd = ["g++"] + CXX_FLAGS + ["-I", CSRC, "-I", "/usr/local/cuda/include",
+                                             "-c", "-o", obj, path]
+            if verbose:
+                print(" ".join(cmd))
+            _run(cmd)
+    if force or _newer(LIB, objs):
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        if verbose:
+            print(" ".join(cmd))
+        _run(cmd)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(verbose=True, force="--force" in sys.argv)
+    print(LIB)

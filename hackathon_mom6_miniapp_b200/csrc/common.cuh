@@ -1,0 +1,56 @@
+// common.cuh -- shared definitions of the B200 split RK2 kernels.
+//
+// Layout: every field is the reference's Fortran array (n1, n2[, nk]),
+// column-major, 1-based (mom6_types.F90:145-148).  Kernels index with the
+// reference's 1-based (i, j, k) so that loop ranges can be compared with the
+// Fortran line for line; A2/A3 subtract the 1.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace mom6b {
+
+// Grid metrics and static fields on the device.  Every pointer addresses an
+// (n1, n2) array of doubles, except f_4_u / f_4_v which are (4, n1, n2)
+// (mom6_barotropic_serial.F90:97-98).
+struct Metrics {
+    const double *IareaT, *areaT, *dxT, *IdxT, *dxCu, *dyCu, *dy_Cu, *IdxCu,
+        *IdyCu, *dxCv, *dyCv, *IdxCv, *IdyCv, *IareaBu, *CoriolisBu, *IareaCu,
+        *IareaCv, *mask2dT, *mask2dBu, *mask2dCu, *mask2dCv;
+    // derived at initialisation exactly as hor_visc_init / coriolis_init do
+    const double *Area_q, *DX_dyT, *DY_dxT, *DX_dyBu, *DY_dxBu, *dx2h, *dy2h,
+        *dx2q, *dy2q, *red_xx, *red_xy, *Kh_xx, *Kh_xy;
+    // barotropic_init (mom6_barotropic_serial.F90:106-133)
+    const double *Datu, *Datv, *gtot_E, *gtot_W, *gtot_N, *gtot_S, *f_4_u,
+        *f_4_v, *bt_rem_u, *bt_rem_v;
+    // forcing (rk2_serial_driver.F90:508-542)
+    const double *taux, *tauy, *Ray_u, *Ray_v;
+    const unsigned char *ray_layer_u, *ray_layer_v; // 1 where the layer is nonzero
+};
+
+struct Dims {
+    int n1, n2, nk;
+    int is, ie, js, je;   // compute domain, 1-based
+    int isd, ied, jsd, jed;
+    long long plane;      // n1 * n2
+};
+
+#define MOM6B_A2(a, i, j, D) (a)[(size_t)((j)-1) * (size_t)(D).n1 + (size_t)((i)-1)]
+#define MOM6B_A3(a, i, j, k, D)                                                 \
+    (a)[(size_t)((k)-1) * (size_t)(D).plane + (size_t)((j)-1) * (size_t)(D).n1 + \
+        (size_t)((i)-1)]
+#define MOM6B_F4(a, c, i, j, D)                                                 \
+    (a)[(((size_t)((j)-1) * (size_t)(D).n1 + (size_t)((i)-1)) * 4) + (size_t)((c)-1)]
+
+// Physical constants, mom6_types.F90:80-85.
+constexpr double kGEarth = 9.80;
+constexpr double kRho0 = 1035.0;
+
+// Status flags written by kernels that can give up (grid barrier timeouts).
+enum : int { kDevOk = 0, kDevTimeout = 1 };
+
+__device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }
+__device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }
+
+} // namespace mom6b

@@ -1,0 +1,189 @@
+// k_vertvisc.cu -- vertical viscosity, one thread per water column (FP64).
+//
+// Restates vert_visc_coef + vert_visc_apply of the serial module
+// (mom6_vert_visc_serial.F90:138-287 and :394-506) as the driver calls them
+// (rk2_serial_driver.F90:276-277, :356-357): harmonic/upwind-blended face
+// thickness, mixed-layer and bottom-boundary-layer viscosity profile, wind
+// stress at the surface, Rayleigh drag, Schopf & Loughe forward elimination
+// and back substitution, and the bottom stress output.
+//
+// Three sweeps per column, all in the reference's order:
+//   1. bottom-up: h_harm and the running z_i; botfn(z_i(m)) is stored per
+//      interface in shared memory (the value the reference recomputes);
+//   2. top-down: hvel, a(K) and the forward elimination; the eliminated
+//      velocity is written back in place, and c1(k) overwrites the botfn slot
+//      k, which is dead by then;
+//   3. bottom-up: back substitution.
+// The coefficient arrays a_u/h_u of the serial control structure are never
+// materialised.  Layers in which the Rayleigh array is identically zero (a
+// per-layer flag computed when the model is built) skip the Rayleigh loads;
+// adding RHO_0*0*u is exact, so this changes no result.
+#include "kernels.h"
+
+namespace mom6b {
+
+__device__ __forceinline__ double vv_botfn(double z2) {
+    return 1.0 / (1.0 + 0.09 * z2 * z2 * z2 * z2 * z2 * z2);
+}
+
+// blockDim.x columns along i; blockIdx.y enumerates u rows then v rows.
+__global__ void __launch_bounds__(128)
+k_vertvisc(Dims D, Metrics M, double* __restrict__ u, double* __restrict__ v,
+           const double* __restrict__ h, double dt, VVParams P,
+           double* __restrict__ taux_bot, double* __restrict__ tauy_bot)
+{
+    extern __shared__ double s_slot[];  // [(nk + 2) * blockDim.x]
+    const int nz = D.nk;
+    const int nb = (int)blockDim.x;
+    const int nrow_u = D.je - D.js + 1;
+    bool is_u = (int)blockIdx.y < nrow_u;
+    int i, j, di, dj;
+    double* vel;
+    const double *mask, *tau, *Ray;
+    const unsigned char* ray_on;
+    double* tbot;
+    if (is_u) {  // u columns: I in [is-1, ie], j in [js, je]
+        j = D.js + (int)blockIdx.y;
+        i = D.is - 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+        if (i > D.ie) return;
+        di = 1; dj = 0;
+        vel = u; mask = M.mask2dCu; tau = M.taux; Ray = M.Ray_u;
+        ray_on = M.ray_layer_u; tbot = taux_bot;
+    } else {     // v columns: i in [is, ie], J in [js-1, je]
+        j = D.js - 1 + ((int)blockIdx.y - nrow_u);
+        i = D.is + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+        if (i > D.ie) return;
+        di = 0; dj = 1;
+        vel = v; mask = M.mask2dCv; tau = M.tauy; Ray = M.Ray_v;
+        ray_on = M.ray_layer_v; tbot = tauy_bot;
+    }
+    const double msk = MOM6B_A2(mask, i, j, D);
+    if (!(msk > 0.0)) return;  // vert_visc_apply leaves masked columns alone
+
+#define SL(m) s_slot[(size_t)(m) * nb + threadIdx.x]
+    const size_t col = (size_t)(j - 1) * D.n1 + (i - 1);
+    const size_t nbr = (size_t)(j - 1 + dj) * D.n1 + (i - 1 + di);
+    const double hn = P.h_neglect;
+
+    // ---- sweep 1: z_i bottom-up (vert_visc_coef :160-179) ----------------
+    double z = 0.0;
+    SL(nz + 1) = vv_botfn(0.0);
+    for (int k = nz; k >= 2; --k) {
+        size_t o = (size_t)(k - 1) * D.plane;
+        double h0 = h[o + col], h1 = h[o + nbr];
+        double h_harm = 2.0 * h0 * h1 / (h0 + h1 + hn);
+        z = z + h_harm * P.I_Hbbl;
+        SL(k) = vv_botfn(z);
+    }
+
+    // hvel(k): harmonic mean, blended toward the arithmetic mean where the
+    // flow opposes the thickness gradient (:162-177)
+    auto hvel_of = [&](int k) -> double {
+        size_t o = (size_t)(k - 1) * D.plane;
+        double h0 = h[o + col], h1 = h[o + nbr];
+        double h_harm = 2.0 * h0 * h1 / (h0 + h1 + hn);
+        double hv = h_harm;
+        if (vel[o + col] * (h1 - h0) < 0.0) {
+            double bf = SL(k + 1);
+            double h_arith = 0.5 * (h1 + h0);
+            hv = (1.0 - bf) * h_harm + bf * h_arith;
+        }
+        return hv;
+    };
+    // a(K2) for K2 in [2, nz] given the running z_top (:185-202)
+    auto a_of = [&](int K2, double z_top, double hv_lo, double hv_up) -> double {
+        double Kv_tot = P.Kv;
+        if (z_top < P.Hmix) {
+            double topfn = 1.0 - z_top / P.Hmix;
+            Kv_tot = Kv_tot + (P.Kv_ml - P.Kv) * topfn;
+        }
+        Kv_tot = Kv_tot + P.Kv_extra_bbl * SL(K2);
+        double h_shear = 0.5 * (hv_lo + hv_up + hn);
+        return Kv_tot / h_shear;
+    };
+    const double a_bot_num = P.Kv + P.Kv_extra_bbl;
+
+    // ---- sweep 2: coefficients + forward elimination, top-down -----------
+    const double dt_Rho0 = dt / kRho0;
+    const double sfc_stress = dt_Rho0 * MOM6B_A2(tau, i, j, D) * msk;
+    double hv_k = hvel_of(1);
+    double z_top = 0.0;
+    double hv_next, a_next;
+    if (nz >= 2) {
+        hv_next = hvel_of(2);
+        z_top = z_top + hv_k;
+        a_next = a_of(2, z_top, hv_next, hv_k);
+    } else {
+        hv_next = 0.0;
+        a_next = a_bot_num / (0.5 * hv_k + hn);
+    }
+    double a_k = 0.0;  // a(1) = 0, surface
+    double Rayk = ray_on[0] ? Ray[col] : 0.0;
+    double h_u = hv_k + hn;
+    double b_denom_1 = h_u + dt * (Rayk + a_k);
+    double b1 = 1.0 / (b_denom_1 + dt * a_next);
+    double d1 = b_denom_1 * b1;
+    double u_prev = b1 * (h_u * vel[col] + sfc_stress);
+    vel[col] = u_prev;
+    for (int k = 2; k <= nz; ++k) {
+        a_k = a_next;
+        hv_k = hv_next;
+        if (k < nz) {
+            hv_next = hvel_of(k + 1);
+            z_top = z_top + hv_k;
+            a_next = a_of(k + 1, z_top, hv_next, hv_k);
+        } else {
+            a_next = a_bot_num / (0.5 * hv_k + hn);
+        }
+        size_t o = (size_t)(k - 1) * D.plane + col;
+        Rayk = ray_on[k - 1] ? Ray[o] : 0.0;
+        double c1 = dt * a_k * b1;
+        SL(k) = c1;
+        h_u = hv_k + hn;
+        b_denom_1 = h_u + dt * (Rayk + a_k * d1);
+        b1 = 1.0 / (b_denom_1 + dt * a_next);
+        d1 = b_denom_1 * b1;
+        u_prev = (h_u * vel[o] + dt * a_k * u_prev) * b1;
+        vel[o] = u_prev;
+    }
+    const double a_bottom = a_next;
+
+    // ---- sweep 3: back substitution (:447-449) ----------------------------
+    double u_below = u_prev;
+    for (int k = nz - 1; k >= 1; --k) {
+        size_t o = (size_t)(k - 1) * D.plane + col;
+        double uk = vel[o] + SL(k + 1) * u_below;
+        vel[o] = uk;
+        u_below = uk;
+    }
+    // bottom stress (:452-458)
+    double tb = kRho0 * u_prev * a_bottom;
+    for (int k = 1; k <= nz; ++k)
+        if (ray_on[k - 1]) {
+            size_t o = (size_t)(k - 1) * D.plane + col;
+            tb = tb + kRho0 * Ray[o] * vel[o];
+        }
+    tbot[col] = tb;
+#undef SL
+}
+
+cudaError_t launch_vertvisc(const Dims& D, const Metrics& M, double* u, double* v,
+                            const double* h, double dt, const VVParams& P,
+                            double* taux_bot, double* tauy_bot, cudaStream_t s)
+{
+    const int nb = 128;
+    int ncol = D.ie - D.is + 2;  // u rows have one more column than v rows
+    int nrows = (D.je - D.js + 1) + (D.je - D.js + 2);
+    dim3 grid((ncol + nb - 1) / nb, nrows, 1);
+    size_t smem = (size_t)(D.nk + 2) * nb * sizeof(double);
+    static bool attr_set = false;
+    if (!attr_set || smem > 48 * 1024) {
+        cudaFuncSetAttribute(k_vertvisc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        attr_set = true;
+    }
+    k_vertvisc<<<grid, nb, smem, s>>>(D, M, u, v, h, dt, P, taux_bot, tauy_bot);
+    return cudaGetLastError();
+}
+
+} // namespace mom6b

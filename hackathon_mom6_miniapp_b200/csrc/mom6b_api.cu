@@ -1,0 +1,654 @@
+// mom6b_api.cu -- the model object and the high-level C ABI (include/mom6b.h).
+//
+// A model keeps the whole state of rk2_serial_driver resident in HBM and
+// advances it with the fused kernels of this directory.  One split RK2
+// iteration (rk2_serial_driver.F90:218-399) is enqueued as
+//
+//   predictor   k_tendency(u, v, h0 -> up, vp)        transports+hor_visc+CorAdCalc+update
+//               k_vertvisc(up, vp; h0)                 vert_visc_coef + vert_visc_apply
+//               k_ppm_edges + k_cont_faces(up, h0 -> hB)  continuity_PPM
+//   corrector   k_tendency(up, vp, hB -> u, v)
+//               k_vertvisc(u, v; hB)
+//               k_ppm_edges + k_cont_faces(u, hB -> hA)
+//   barotropic  k_btstep(eta, ubt, vbt -> ubt_av, vbt_av, eta_av)
+//               k_btstep(eta_av, ubt_av, vbt_av -> ubt_av, vbt_av, eta)
+//
+// The reset h <- h0 at the top of the reference iteration is realised by
+// reading h0 directly in the predictor; the thickness ping-pongs between hB
+// (after the predictor, the reference's htmp) and hA (the state h), whose
+// halo ring is h0 unless the halo fill is enabled.  The barotropic chain
+// reads nothing the 3-D chain writes (SURVEY of the driver: btstep only sees
+// eta/ubt/vbt), so it runs on a second stream joined by events.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/mom6b.h"
+#include "host_init.h"
+#include "kernels.h"
+
+
+using namespace mom6b;
+
+static thread_local std::string g_last_error;
+
+static int fail(int code, const std::string& msg)
+{
+    g_last_error = msg;
+    return code;
+}
+
+#define CK(call)                                                                     \
+    do {                                                                             \
+        cudaError_t e_ = (call);                                                     \
+        if (e_ != cudaSuccess)                                                       \
+            return fail(MOM6B_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+struct TimedLaunch {
+    std::string name;
+    cudaEvent_t a, b;
+};
+
+struct mom6b_model {
+    mom6b_config cfg;
+    std::unique_ptr<HostGrid> grid;
+    Dims D;
+    Metrics M;
+    std::vector<void*> allocs;
+    // state
+    double *u, *v, *hA, *hB, *h0, *up, *vp, *uh, *hW, *hE, *uhbt0;
+    double *eta, *ubt, *vbt, *ubt_av, *vbt_av, *eta_av;
+    double *h_u, *FA_u_W0, *FA_u_WW, *FA_u_E0, *FA_u_EE, *uBT_WW, *uBT_EE, *du_cor;
+    double *taux_bot, *tauy_bot;
+    double *taux, *tauy, *Ray_u, *Ray_v;
+    unsigned char *ray_layer_u, *ray_layer_v;
+    BTWork bt;
+    cudaStream_t s3d = nullptr, s2d = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    int64_t launches = 0;
+    bool overlap_bt = false;
+    bool timing = false;
+    std::vector<TimedLaunch> pending;
+    std::map<std::string, std::pair<double, int64_t>> timed;  // ms total, launches
+};
+
+static double* dalloc(mom6b_model* m, size_t n, cudaError_t* err)
+{
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, n * sizeof(double) + 16);
+    if (e != cudaSuccess) { *err = e; return nullptr; }
+    cudaMemset(p, 0, n * sizeof(double) + 16);
+    m->allocs.push_back(p);
+    return (double*)p;
+}
+
+static void free_all(mom6b_model* m)
+{
+    for (void* p : m->allocs) cudaFree(p);
+    m->allocs.clear();
+    for (auto& t : m->pending) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
+    m->pending.clear();
+    if (m->ev_fork) cudaEventDestroy(m->ev_fork);
+    if (m->ev_join) cudaEventDestroy(m->ev_join);
+    if (m->s3d) cudaStreamDestroy(m->s3d);
+    if (m->s2d) cudaStreamDestroy(m->s2d);
+}
+
+extern "C" const char* mom6b_last_error(void) { return g_last_error.c_str(); }
+extern "C" const char* mom6b_version(void) { return "mom6b 0.1 (sm_100a)"; }
+
+extern "C" int mom6b_config_default(mom6b_config* c, int init_mode)
+{
+    if (!c) return fail(MOM6B_ERR_ARG, "null config");
+    std::memset(c, 0, sizeof(*c));
+    c->ni = 180; c->nj = 180; c->nk = 75; c->bt_nsteps = 30;
+    c->init_mode = init_mode;
+    c->dx_km = 10.0; c->lat_deg = 45.0;
+    c->Kv = 1.0e-4; c->Kv_ml = 1.0e-2; c->Kv_extra_bbl = 1.0e-2;
+    c->Hmix = 50.0; c->Hbbl = 10.0;
+    c->precision = MOM6B_FP64;
+    c->use_graph = 0;
+    if (init_mode == MOM6B_INIT_REF) {
+        c->dt = 300.0; c->Kh = 100.0; c->bc_fill = 0;
+    } else if (init_mode == MOM6B_INIT_CFG) {
+        c->dt = 600.0; c->Kh = 1.0e3; c->bc_fill = 1;
+    } else {
+        return fail(MOM6B_ERR_ARG, "unknown init mode");
+    }
+    return MOM6B_OK;
+}
+
+template <class T>
+static int upload(T* dst, const std::vector<T>& src)
+{
+    CK(cudaMemcpy(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return MOM6B_OK;
+}
+
+static int set_ray_flags(mom6b_model* m, const std::vector<double>& Ru,
+                         const std::vector<double>& Rv)
+{
+    const HostGrid& g = *m->grid;
+    std::vector<unsigned char> fu(g.nk, 0), fv(g.nk, 0);
+    for (int k = 0; k < g.nk; ++k) {
+        const double* pu = Ru.data() + (size_t)k * g.plane;
+        const double* pv = Rv.data() + (size_t)k * g.plane;
+        for (size_t q = 0; q < g.plane; ++q) {
+            if (pu[q] != 0.0) fu[k] = 1;
+            if (pv[q] != 0.0) fv[k] = 1;
+        }
+    }
+    CK(cudaMemcpy(m->ray_layer_u, fu.data(), g.nk, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(m->ray_layer_v, fv.data(), g.nk, cudaMemcpyHostToDevice));
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_create(const mom6b_config* cfg, mom6b_model** out)
+{
+    if (!cfg || !out) return fail(MOM6B_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (cfg->ni < 8 || cfg->nj < 8 || cfg->nk < 2 || cfg->bt_nsteps < 1)
+        return fail(MOM6B_ERR_ARG, "sizes must satisfy ni, nj >= 8, nk >= 2, bt_nsteps >= 1");
+    if (cfg->nk > 1024) return fail(MOM6B_ERR_ARG, "nk > 1024 not supported");
+    if ((long long)(cfg->ni + 2) * (cfg->nj + 2) > (1LL << 30))
+        return fail(MOM6B_ERR_ARG, "horizontal grid too large");
+    if (cfg->precision != MOM6B_FP64 && cfg->precision != MOM6B_MIXED)
+        return fail(MOM6B_ERR_ARG, "unknown precision");
+    if (cfg->precision == MOM6B_MIXED)
+        return fail(MOM6B_ERR_ARG, "mixed precision form not built in this library");
+    CK(cudaSetDevice(cfg->device));
+
+    auto m = std::make_unique<mom6b_model>();
+    m->cfg = *cfg;
+    m->grid = std::make_unique<HostGrid>(*cfg);
+    HostGrid& g = *m->grid;
+    g.build();
+    Dims& D = m->D;
+    D.n1 = g.n1; D.n2 = g.n2; D.nk = g.nk;
+    D.is = g.is; D.ie = g.ie; D.js = g.js; D.je = g.je;
+    D.isd = g.isd; D.ied = g.ied; D.jsd = g.jsd; D.jed = g.jed;
+    D.plane = (long long)g.plane;
+
+    const size_t n2 = g.plane, n3 = g.plane * (size_t)g.nk;
+    cudaError_t err = cudaSuccess;
+    auto A2 = [&]() { return dalloc(m.get(), n2, &err); };
+    auto A3 = [&]() { return dalloc(m.get(), n3, &err); };
+    // metrics
+    struct Up { const double** dst; const std::vector<double>* src; };
+    double* dm[64];
+    int nm = 0;
+    std::vector<Up> ups = {
+        {&m->M.IareaT, &g.IareaT}, {&m->M.areaT, &g.areaT}, {&m->M.dxT, &g.dxT},
+        {&m->M.IdxT, &g.IdxT}, {&m->M.dxCu, &g.dxCu}, {&m->M.dyCu, &g.dyCu},
+        {&m->M.dy_Cu, &g.dy_Cu}, {&m->M.IdxCu, &g.IdxCu}, {&m->M.IdyCu, &g.IdyCu},
+        {&m->M.dxCv, &g.dxCv}, {&m->M.dyCv, &g.dyCv}, {&m->M.IdxCv, &g.IdxCv},
+        {&m->M.IdyCv, &g.IdyCv}, {&m->M.IareaBu, &g.IareaBu},
+        {&m->M.CoriolisBu, &g.CoriolisBu}, {&m->M.IareaCu, &g.IareaCu},
+        {&m->M.IareaCv, &g.IareaCv}, {&m->M.mask2dT, &g.mask2dT},
+        {&m->M.mask2dBu, &g.mask2dBu}, {&m->M.mask2dCu, &g.mask2dCu},
+        {&m->M.mask2dCv, &g.mask2dCv}, {&m->M.Area_q, &g.Area_q},
+        {&m->M.DX_dyT, &g.DX_dyT}, {&m->M.DY_dxT, &g.DY_dxT},
+        {&m->M.DX_dyBu, &g.DX_dyBu}, {&m->M.DY_dxBu, &g.DY_dxBu},
+        {&m->M.dx2h, &g.dx2h}, {&m->M.dy2h, &g.dy2h}, {&m->M.dx2q, &g.dx2q},
+        {&m->M.dy2q, &g.dy2q}, {&m->M.red_xx, &g.red_xx}, {&m->M.red_xy, &g.red_xy},
+        {&m->M.Kh_xx, &g.Kh_xx}, {&m->M.Kh_xy, &g.Kh_xy}, {&m->M.Datu, &g.Datu},
+        {&m->M.Datv, &g.Datv}, {&m->M.gtot_E, &g.gtot_E}, {&m->M.gtot_W, &g.gtot_W},
+        {&m->M.gtot_N, &g.gtot_N}, {&m->M.gtot_S, &g.gtot_S},
+        {&m->M.bt_rem_u, &g.bt_rem_u}, {&m->M.bt_rem_v, &g.bt_rem_v}};
+    for (auto& up : ups) {
+        double* p = A2();
+        if (!p) return fail(MOM6B_ERR_NOMEM, "device allocation failed");
+        *up.dst = p;
+        int rc = upload(p, *up.src);
+        if (rc) return rc;
+        dm[nm++ % 64] = p;
+    }
+    {
+        double* p4u = dalloc(m.get(), 4 * n2, &err);
+        double* p4v = dalloc(m.get(), 4 * n2, &err);
+        if (!p4u || !p4v) return fail(MOM6B_ERR_NOMEM, "device allocation failed");
+        if (int rc = upload(p4u, g.f_4_u)) return rc;
+        if (int rc = upload(p4v, g.f_4_v)) return rc;
+        m->M.f_4_u = p4u; m->M.f_4_v = p4v;
+    }
+    m->taux = A2(); m->tauy = A2(); m->Ray_u = A3(); m->Ray_v = A3();
+    {
+        void* pf = nullptr;
+        if (cudaMalloc(&pf, 2 * (size_t)g.nk + 32) != cudaSuccess)
+            return fail(MOM6B_ERR_NOMEM, "device allocation failed");
+        m->allocs.push_back(pf);
+        m->ray_layer_u = (unsigned char*)pf;
+        m->ray_layer_v = (unsigned char*)pf + g.nk;
+    }
+    // state and outputs
+    m->u = A3(); m->v = A3(); m->hA = A3(); m->hB = A3(); m->h0 = A3();
+    m->up = A3(); m->vp = A3(); m->uh = A3(); m->hW = A3(); m->hE = A3();
+    m->h_u = A3();
+    m->uhbt0 = A2();
+    m->eta = A2(); m->ubt = A2(); m->vbt = A2(); m->ubt_av = A2(); m->vbt_av = A2();
+    m->eta_av = A2();
+    m->FA_u_W0 = A2(); m->FA_u_WW = A2(); m->FA_u_E0 = A2(); m->FA_u_EE = A2();
+    m->uBT_WW = A2(); m->uBT_EE = A2(); m->du_cor = A2();
+    m->taux_bot = A2(); m->tauy_bot = A2();
+    BTWork& W = m->bt;
+    W.eta = A2(); W.eta_pred = A2(); W.ubt = A2(); W.vbt = A2(); W.ubt_prev = A2();
+    W.vbt_prev = A2(); W.uhbt = A2(); W.vhbt = A2(); W.PFu = A2(); W.PFv = A2();
+    W.ubt_av = A2(); W.vbt_av = A2();
+    {
+        void* pb = nullptr;
+        if (cudaMalloc(&pb, 64) != cudaSuccess) return fail(MOM6B_ERR_NOMEM, "device allocation failed");
+        cudaMemset(pb, 0, 64);
+        m->allocs.push_back(pb);
+        W.bar_count = (unsigned int*)pb;
+        W.bar_gen = (unsigned int*)pb + 4;
+        W.status = (int*)pb + 8;
+    }
+    if (err != cudaSuccess || !m->u || !W.vbt_av)
+        return fail(MOM6B_ERR_NOMEM, std::string("device allocation failed: ") + cudaGetErrorString(err));
+    m->M.taux = m->taux; m->M.tauy = m->tauy; m->M.Ray_u = m->Ray_u; m->M.Ray_v = m->Ray_v;
+    m->M.ray_layer_u = m->ray_layer_u; m->M.ray_layer_v = m->ray_layer_v;
+
+    // initial state
+    {
+        std::vector<double> u, v, h0, eta, ubt, vbt, Ru, Rv;
+        g.initial_state(u, v, h0, eta, ubt, vbt);
+        g.rayleigh(Ru, Rv);
+        if (int rc = upload(m->u, u)) return rc;
+        if (int rc = upload(m->v, v)) return rc;
+        if (int rc = upload(m->h0, h0)) return rc;
+        if (int rc = upload(m->hA, h0)) return rc;
+        if (int rc = upload(m->hB, h0)) return rc;
+        if (int rc = upload(m->eta, eta)) return rc;
+        if (int rc = upload(m->ubt, ubt)) return rc;
+        if (int rc = upload(m->vbt, vbt)) return rc;
+        if (int rc = upload(m->taux, g.taux)) return rc;
+        if (int rc = upload(m->tauy, g.tauy)) return rc;
+        if (int rc = upload(m->Ray_u, Ru)) return rc;
+        if (int rc = upload(m->Ray_v, Rv)) return rc;
+        if (int rc = set_ray_flags(m.get(), Ru, Rv)) return rc;
+    }
+    CK(cudaStreamCreateWithFlags(&m->s3d, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&m->s2d, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&m->ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&m->ev_join, cudaEventDisableTiming));
+    if (cfg->bc_fill) {
+        const Dims& Dd = m->D;
+        CK(launch_halo_fill(Dd, m->h0, g.nk, 0, m->s3d));
+        CK(launch_halo_fill(Dd, m->hA, g.nk, 0, m->s3d));
+        CK(launch_halo_fill(Dd, m->hB, g.nk, 0, m->s3d));
+        CK(launch_halo_fill(Dd, m->u, g.nk, 1, m->s3d));
+        CK(launch_halo_fill(Dd, m->v, g.nk, 2, m->s3d));
+        CK(launch_halo_fill(Dd, m->eta, 1, 0, m->s3d));
+        CK(launch_halo_fill(Dd, m->ubt, 1, 1, m->s3d));
+        CK(launch_halo_fill(Dd, m->vbt, 1, 2, m->s3d));
+    }
+    CK(cudaStreamSynchronize(m->s3d));
+    *out = m.release();
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_destroy(mom6b_model* m)
+{
+    if (!m) return MOM6B_OK;
+    if (m->s3d) cudaStreamSynchronize(m->s3d);
+    if (m->s2d) cudaStreamSynchronize(m->s2d);
+    free_all(m);
+    delete m;
+    return MOM6B_OK;
+}
+
+// launch bookkeeping: count every kernel and optionally time it
+template <class F>
+static cudaError_t timed(mom6b_model* m, cudaStream_t s, const char* name, F&& launch)
+{
+    TimedLaunch t;
+    if (m->timing) {
+        t.name = name;
+        cudaEventCreate(&t.a);
+        cudaEventCreate(&t.b);
+        cudaEventRecord(t.a, s);
+    }
+    cudaError_t e = launch();
+    ++m->launches;
+    if (m->timing) {
+        cudaEventRecord(t.b, s);
+        m->pending.push_back(t);
+    }
+    return e;
+}
+
+static int enqueue_step(mom6b_model* m)
+{
+    const Dims& D = m->D;
+    const Metrics& M = m->M;
+    const mom6b_config& c = m->cfg;
+    const HostGrid& g = *m->grid;
+    cudaStream_t s = m->s3d;
+    // The barotropic chain only needs co-residency of its own blocks; it is
+    // overlapped with the 3-D chain only when enabled.
+    cudaStream_t s2 = m->overlap_bt ? m->s2d : m->s3d;
+    const double dt = c.dt;
+    const double Angstrom_H = 1.0e-10;
+    const double hv_neglect = Angstrom_H > 1.0e-3 ? Angstrom_H : 1.0e-3;
+    const double h_min = (double)2.0f * Angstrom_H;
+    VVParams VV{c.Kv, c.Kv_ml, c.Kv_extra_bbl, c.Hmix, Angstrom_H,
+                1.0 / (c.Hbbl + Angstrom_H)};
+    ContOut OB{m->hB, m->uh, m->h_u, m->FA_u_W0, m->FA_u_WW, m->FA_u_E0,
+               m->FA_u_EE, m->uBT_WW, m->uBT_EE, m->du_cor};
+    ContOut OA = OB;
+    OA.h = m->hA;
+
+    // fork the barotropic chain onto its own stream
+    if (s2 != s) {
+        CK(cudaEventRecord(m->ev_fork, s));
+        CK(cudaStreamWaitEvent(s2, m->ev_fork, 0));
+    }
+
+    // ---- predictor ----
+    CK(timed(m, s, "tendency", [&] {
+        return launch_tendency(D, M, m->u, m->v, m->h0, m->u, m->v, m->up, m->vp, dt,
+                               hv_neglect, s); }));
+    CK(timed(m, s, "vertvisc", [&] {
+        return launch_vertvisc(D, M, m->up, m->vp, m->h0, dt, VV, m->taux_bot,
+                               m->tauy_bot, s); }));
+    CK(timed(m, s, "continuity", [&] {
+        return launch_continuity(D, M, m->up, m->h0, m->hW, m->hE, m->uhbt0, OB, dt,
+                                 h_min, s); }));
+    if (c.bc_fill) {
+        CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->hB, g.nk, 0, s); }));
+        CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->up, g.nk, 1, s); }));
+        CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->vp, g.nk, 2, s); }));
+    }
+    // ---- corrector ----
+    CK(timed(m, s, "tendency", [&] {
+        return launch_tendency(D, M, m->up, m->vp, m->hB, m->u, m->v, m->u, m->v,
+                               0.5 * dt, hv_neglect, s); }));
+    CK(timed(m, s, "vertvisc", [&] {
+        return launch_vertvisc(D, M, m->u, m->v, m->hB, 0.5 * dt, VV, m->taux_bot,
+                               m->tauy_bot, s); }));
+    CK(timed(m, s, "continuity", [&] {
+        return launch_continuity(D, M, m->u, m->hB, m->hW, m->hE, m->uhbt0, OA,
+                                 0.5 * dt, h_min, s); }));
+    if (c.bc_fill) {
+        CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->hA, g.nk, 0, s); }));
+        CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->u, g.nk, 1, s); }));
+        CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->v, g.nk, 2, s); }));
+    }
+
+    // ---- barotropic chain ----
+    BTParams P;
+    P.dtbt = dt / (double)c.bt_nsteps;
+    P.dgeo_de = 1.0;
+    P.trans_wt1 = 1.0 + 0.2;
+    P.trans_wt2 = -0.2;
+    P.inv_nstep = 1.0 / (double)c.bt_nsteps;
+    P.nstep = c.bt_nsteps;
+    P.first_direction = 0;
+    P.extended = 0;
+    P.spin_budget = 4000000000LL;
+    CK(timed(m, s2, "btstep", [&] {
+        return launch_btstep(D, M, m->bt, P, m->eta, m->ubt, m->vbt, m->ubt_av,
+                             m->vbt_av, m->eta_av, s2); }));
+    if (c.bc_fill) {
+        CK(timed(m, s2, "halo_fill", [&] { return launch_halo_fill(D, m->eta_av, 1, 0, s2); }));
+        CK(timed(m, s2, "halo_fill", [&] { return launch_halo_fill(D, m->ubt_av, 1, 1, s2); }));
+        CK(timed(m, s2, "halo_fill", [&] { return launch_halo_fill(D, m->vbt_av, 1, 2, s2); }));
+    }
+    CK(timed(m, s2, "btstep", [&] {
+        return launch_btstep(D, M, m->bt, P, m->eta_av, m->ubt_av, m->vbt_av,
+                             m->ubt_av, m->vbt_av, m->eta, s2); }));
+    if (c.bc_fill)
+        CK(timed(m, s2, "halo_fill", [&] { return launch_halo_fill(D, m->eta, 1, 0, s2); }));
+    if (s2 != s) {
+        CK(cudaEventRecord(m->ev_join, s2));
+        CK(cudaStreamWaitEvent(s, m->ev_join, 0));
+    }
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_step(mom6b_model* m, int nsteps)
+{
+    if (!m || nsteps < 0) return fail(MOM6B_ERR_ARG, "bad argument");
+    CK(cudaSetDevice(m->cfg.device));
+    for (int n = 0; n < nsteps; ++n) {
+        int rc = enqueue_step(m);
+        if (rc) return rc;
+    }
+    return MOM6B_OK;
+}
+
+static int check_status(mom6b_model* m)
+{
+    int st = 0;
+    CK(cudaMemcpy(&st, m->bt.status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st != kDevOk) {
+        cudaMemset(m->bt.status, 0, sizeof(int));
+        cudaMemset(m->bt.bar_count, 0, sizeof(unsigned int));
+        return fail(MOM6B_ERR_TIMEOUT, "barotropic grid barrier timed out");
+    }
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_synchronize(mom6b_model* m)
+{
+    if (!m) return fail(MOM6B_ERR_ARG, "null model");
+    CK(cudaStreamSynchronize(m->s3d));
+    CK(cudaStreamSynchronize(m->s2d));
+    return check_status(m);
+}
+
+static double* field_ptr(mom6b_model* m, int f, bool* is3d, bool* writable)
+{
+    *is3d = true;
+    *writable = true;
+    switch (f) {
+    case MOM6B_F_U: return m->u;
+    case MOM6B_F_V: return m->v;
+    case MOM6B_F_H: return m->hA;
+    case MOM6B_F_H0: return m->h0;
+    case MOM6B_F_UH: return m->uh;
+    case MOM6B_F_UP: return m->up;
+    case MOM6B_F_VP: return m->vp;
+    case MOM6B_F_HU_BT: return m->h_u;
+    case MOM6B_F_RAY_U: return m->Ray_u;
+    case MOM6B_F_RAY_V: return m->Ray_v;
+    default: break;
+    }
+    *is3d = false;
+    switch (f) {
+    case MOM6B_F_ETA: return m->eta;
+    case MOM6B_F_UBT: return m->ubt;
+    case MOM6B_F_VBT: return m->vbt;
+    case MOM6B_F_UBT_AV: return m->ubt_av;
+    case MOM6B_F_VBT_AV: return m->vbt_av;
+    case MOM6B_F_ETA_AV: return m->eta_av;
+    case MOM6B_F_FA_U_W0: return m->FA_u_W0;
+    case MOM6B_F_FA_U_WW: return m->FA_u_WW;
+    case MOM6B_F_FA_U_E0: return m->FA_u_E0;
+    case MOM6B_F_FA_U_EE: return m->FA_u_EE;
+    case MOM6B_F_UBT_WW: return m->uBT_WW;
+    case MOM6B_F_UBT_EE: return m->uBT_EE;
+    case MOM6B_F_DU_COR: return m->du_cor;
+    case MOM6B_F_TAUX_BOT: return m->taux_bot;
+    case MOM6B_F_TAUY_BOT: return m->tauy_bot;
+    case MOM6B_F_TAUX: return m->taux;
+    case MOM6B_F_TAUY: return m->tauy;
+    default: return nullptr;
+    }
+}
+
+extern "C" size_t mom6b_field_size(const mom6b_model* m, int f)
+{
+    if (!m) return 0;
+    bool is3d, w;
+    if (!field_ptr(const_cast<mom6b_model*>(m), f, &is3d, &w)) return 0;
+    return m->grid->plane * (is3d ? (size_t)m->grid->nk : 1);
+}
+
+extern "C" int mom6b_get_field(mom6b_model* m, int f, double* host, size_t count)
+{
+    if (!m || !host) return fail(MOM6B_ERR_ARG, "null argument");
+    bool is3d, w;
+    double* p = field_ptr(m, f, &is3d, &w);
+    if (!p) return fail(MOM6B_ERR_ARG, "unknown field id");
+    size_t n = mom6b_field_size(m, f);
+    if (count != n) return fail(MOM6B_ERR_ARG, "count does not match the field size");
+    CK(cudaSetDevice(m->cfg.device));
+    CK(cudaStreamSynchronize(m->s3d));
+    CK(cudaStreamSynchronize(m->s2d));
+    CK(cudaMemcpy(host, p, n * sizeof(double), cudaMemcpyDeviceToHost));
+    return check_status(m);
+}
+
+extern "C" int mom6b_set_field(mom6b_model* m, int f, const double* host, size_t count)
+{
+    if (!m || !host) return fail(MOM6B_ERR_ARG, "null argument");
+    bool is3d, w;
+    double* p = field_ptr(m, f, &is3d, &w);
+    if (!p || !w) return fail(MOM6B_ERR_ARG, "unknown or read-only field id");
+    size_t n = mom6b_field_size(m, f);
+    if (count != n) return fail(MOM6B_ERR_ARG, "count does not match the field size");
+    CK(cudaSetDevice(m->cfg.device));
+    CK(cudaStreamSynchronize(m->s3d));
+    CK(cudaStreamSynchronize(m->s2d));
+    CK(cudaMemcpy(p, host, n * sizeof(double), cudaMemcpyHostToDevice));
+    if (f == MOM6B_F_H0) {  // the step resets h to h0, halo ring included
+        CK(cudaMemcpy(m->hA, host, n * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(m->hB, host, n * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    if (f == MOM6B_F_RAY_U || f == MOM6B_F_RAY_V) {
+        std::vector<double> Ru(n), Rv(n);
+        CK(cudaMemcpy(Ru.data(), m->Ray_u, n * sizeof(double), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(Rv.data(), m->Ray_v, n * sizeof(double), cudaMemcpyDeviceToHost));
+        if (int rc = set_ray_flags(m, Ru, Rv)) return rc;
+    }
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_field_device_ptr(mom6b_model* m, int f, void** dptr)
+{
+    if (!m || !dptr) return fail(MOM6B_ERR_ARG, "null argument");
+    bool is3d, w;
+    double* p = field_ptr(m, f, &is3d, &w);
+    if (!p) return fail(MOM6B_ERR_ARG, "unknown field id");
+    *dptr = p;
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_dims(const mom6b_model* m, int* o)
+{
+    if (!m || !o) return fail(MOM6B_ERR_ARG, "null argument");
+    const HostGrid& g = *m->grid;
+    o[0] = g.n1; o[1] = g.n2; o[2] = g.nk; o[3] = g.is; o[4] = g.ie; o[5] = g.js;
+    o[6] = g.je; o[7] = m->cfg.bt_nsteps;
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_stream(mom6b_model* m, void** stream)
+{
+    if (!m || !stream) return fail(MOM6B_ERR_ARG, "null argument");
+    *stream = (void*)m->s3d;
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_step_host(mom6b_model* m, int nsteps, double* u, double* v,
+                               double* h, double* eta)
+{
+    if (!m || nsteps < 0) return fail(MOM6B_ERR_ARG, "bad argument");
+    CK(cudaSetDevice(m->cfg.device));
+    const size_t n3 = m->grid->plane * (size_t)m->grid->nk, n2 = m->grid->plane;
+    cudaStream_t s = m->s3d;
+    CK(cudaStreamSynchronize(m->s2d));
+    if (u) CK(cudaMemcpyAsync(m->u, u, n3 * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (v) CK(cudaMemcpyAsync(m->v, v, n3 * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (h) CK(cudaMemcpyAsync(m->hA, h, n3 * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (eta) CK(cudaMemcpyAsync(m->eta, eta, n2 * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (int rc = mom6b_step(m, nsteps)) return rc;
+    if (u) CK(cudaMemcpyAsync(u, m->u, n3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (v) CK(cudaMemcpyAsync(v, m->v, n3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (h) CK(cudaMemcpyAsync(h, m->hA, n3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (eta) CK(cudaMemcpyAsync(eta, m->eta, n2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return check_status(m);
+}
+
+extern "C" int mom6b_verify(mom6b_model* m, double* out)
+{
+    if (!m || !out) return fail(MOM6B_ERR_ARG, "null argument");
+    const HostGrid& g = *m->grid;
+    size_t n3 = g.plane * (size_t)g.nk;
+    std::vector<double> h0(n3), h(n3), u(n3), v(n3), eta(g.plane);
+    if (int rc = mom6b_get_field(m, MOM6B_F_H0, h0.data(), n3)) return rc;
+    if (int rc = mom6b_get_field(m, MOM6B_F_H, h.data(), n3)) return rc;
+    if (int rc = mom6b_get_field(m, MOM6B_F_U, u.data(), n3)) return rc;
+    if (int rc = mom6b_get_field(m, MOM6B_F_V, v.data(), n3)) return rc;
+    if (int rc = mom6b_get_field(m, MOM6B_F_ETA, eta.data(), g.plane)) return rc;
+    // verify_state, rk2_serial_driver.F90:563-623, summed in the same order
+    double mi = 0.0, mf = 0.0, mu = 0.0, mv = 0.0, me = 0.0, ke = 0.0;
+    for (int k = 1; k <= g.nk; ++k)
+        for (int j = g.js; j <= g.je; ++j)
+            for (int i = g.is; i <= g.ie; ++i) {
+                size_t p = g.at(i, j, k);
+                double a = g.areaT[g.at(i, j)];
+                mi = mi + h0[p] * a;
+                mf = mf + h[p] * a;
+                mu = std::max(mu, std::fabs(u[p]));
+                mv = std::max(mv, std::fabs(v[p]));
+                ke = ke + 0.5 * (u[p] * u[p] + v[p] * v[p]) * h[p] * a;
+            }
+    for (int j = g.js; j <= g.je; ++j)
+        for (int i = g.is; i <= g.ie; ++i) me = std::max(me, std::fabs(eta[g.at(i, j)]));
+    out[0] = mi; out[1] = mf; out[2] = std::fabs(mf - mi) / mi;
+    out[3] = mu; out[4] = mv; out[5] = me; out[6] = ke;
+    return MOM6B_OK;
+}
+
+extern "C" int64_t mom6b_launch_count(const mom6b_model* m) { return m ? m->launches : 0; }
+extern "C" void mom6b_reset_launch_count(mom6b_model* m)
+{
+    if (m) m->launches = 0;
+}
+
+extern "C" int mom6b_kernel_timing(mom6b_model* m, int enable)
+{
+    if (!m) return fail(MOM6B_ERR_ARG, "null model");
+    m->timing = enable != 0;
+    m->timed.clear();
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_kernel_time_ms(mom6b_model* m, const char* kernel, double* avg_ms,
+                                    int64_t* launches)
+{
+    if (!m || !kernel) return fail(MOM6B_ERR_ARG, "null argument");
+    CK(cudaStreamSynchronize(m->s3d));
+    CK(cudaStreamSynchronize(m->s2d));
+    for (auto& t : m->pending) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, t.a, t.b);
+        auto& e = m->timed[t.name];
+        e.first += ms;
+        e.second += 1;
+        cudaEventDestroy(t.a);
+        cudaEventDestroy(t.b);
+    }
+    m->pending.clear();
+    auto it = m->timed.find(kernel);
+    if (it == m->timed.end()) {
+        if (avg_ms) *avg_ms = 0.0;
+        if (launches) *launches = 0;
+        return MOM6B_OK;
+    }
+    if (avg_ms) *avg_ms = it->second.first / (double)it->second.second;
+    if (launches) *launches = it->second.second;
+    return MOM6B_OK;
+}

@@ -1,0 +1,135 @@
+/*
+ * mom6b.h -- high-level C ABI of the B200 split RK2 library (libmom6b.so).
+ *
+ * A model owns the ocean grid of init_ocean_grid (mom6_types.F90:130-258),
+ * the state of rk2_serial_driver (u, v, h, h0, eta, ubt, vbt, ...) resident in
+ * HBM, and the fused sm_100a kernels that advance it by whole split RK2
+ * iterations with the semantics of rk2_serial_driver.F90:218-399.  Every
+ * function returns a MOM6B_* status; mom6b_last_error() gives a message.
+ *
+ * Arrays crossing this boundary use the reference layout: Fortran
+ * column-major, 1-based, dimensions (n1, n2[, nk]) with n1 = ni + 2 and
+ * n2 = nj + 2, double precision.  No torch types appear in this header.
+ *
+ * The reference-compatible per-kernel entry points (launch_* and cuda_*_c of
+ * the reference's src/cuda_c backend) are declared in mom6_cuda_c.h.
+ */
+#ifndef MOM6B_H
+#define MOM6B_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+enum {
+    MOM6B_OK = 0,
+    MOM6B_ERR_ARG = 1,      /* invalid argument (sizes, null pointers, ids) */
+    MOM6B_ERR_CUDA = 2,     /* a CUDA runtime call failed */
+    MOM6B_ERR_NOMEM = 3,    /* device or host allocation failed */
+    MOM6B_ERR_TIMEOUT = 4,  /* a grid-wide barrier gave up waiting */
+    MOM6B_ERR_STATE = 5     /* call not valid in the current state */
+};
+
+/* initial-state constructions */
+enum {
+    MOM6B_INIT_REF = 0, /* analytic fields of rk2_serial_driver.F90:466-542 */
+    MOM6B_INIT_CFG = 1  /* seeded beta plane: h = H/nk (1 + 0.01 N), u,v ~ N(0,0.05),
+                           Gaussian eta bump, f = 1e-4 + 2e-11 (y - Ly/2) */
+};
+
+/* arithmetic forms */
+enum {
+    MOM6B_FP64 = 0,  /* every field and every operation in double precision */
+    MOM6B_MIXED = 1  /* fields and stencils in single precision, the thickness
+                        update, barotropic accumulators and the vertical
+                        tridiagonal elimination in double */
+};
+
+/* field ids (get/set) */
+enum {
+    MOM6B_F_U = 0, MOM6B_F_V, MOM6B_F_H, MOM6B_F_H0, MOM6B_F_UH, MOM6B_F_VH,
+    MOM6B_F_UP, MOM6B_F_VP, MOM6B_F_ETA, MOM6B_F_UBT, MOM6B_F_VBT,
+    MOM6B_F_UBT_AV, MOM6B_F_VBT_AV, MOM6B_F_ETA_AV, MOM6B_F_HU_BT,
+    MOM6B_F_FA_U_W0, MOM6B_F_FA_U_WW, MOM6B_F_FA_U_E0, MOM6B_F_FA_U_EE,
+    MOM6B_F_UBT_WW, MOM6B_F_UBT_EE, MOM6B_F_DU_COR, MOM6B_F_TAUX_BOT,
+    MOM6B_F_TAUY_BOT, MOM6B_F_TAUX, MOM6B_F_TAUY, MOM6B_F_RAY_U, MOM6B_F_RAY_V,
+    MOM6B_F_COUNT
+};
+
+typedef struct mom6b_config {
+    int ni, nj, nk;        /* computational sizes as passed to init_ocean_grid */
+    int bt_nsteps;         /* barotropic substeps per btstep call */
+    int init_mode;         /* MOM6B_INIT_REF / MOM6B_INIT_CFG */
+    uint64_t seed;         /* CFG initial state seed */
+    double dt;             /* baroclinic step [s] */
+    double dx_km;          /* grid spacing [km] */
+    double lat_deg;        /* REF beta-plane latitude [deg] */
+    double Kh;             /* Laplacian viscosity [m2 s-1] */
+    double Kv, Kv_ml, Kv_extra_bbl, Hmix, Hbbl; /* vertical viscosity */
+    int bc_fill;           /* 1: periodic-x / solid-wall-y halo fill per step */
+    int precision;         /* MOM6B_FP64 / MOM6B_MIXED */
+    int device;            /* CUDA device ordinal */
+    int use_graph;         /* 1: replay each step from a captured CUDA graph */
+} mom6b_config;
+
+typedef struct mom6b_model mom6b_model;
+
+/* Fill *cfg with the defaults of the given initial-state mode:
+ * REF: 180x180x75, dt 300 s, Kh 100, no halo fill (rk2_serial_driver.F90:91-143);
+ * CFG: 180x180x75, dt 600 s, Kh 1000, halo fill on. */
+int mom6b_config_default(mom6b_config *cfg, int init_mode);
+
+/* Allocate the model on cfg->device, build grid metrics and the initial state
+ * on the host and upload them.  Sizes must satisfy ni, nj >= 8, nk >= 2. */
+int mom6b_create(const mom6b_config *cfg, mom6b_model **out);
+int mom6b_destroy(mom6b_model *m);
+
+/* Enqueue nsteps split RK2 iterations on the model's stream (asynchronous). */
+int mom6b_step(mom6b_model *m, int nsteps);
+/* Block until all enqueued work has finished; reports barrier timeouts. */
+int mom6b_synchronize(mom6b_model *m);
+
+/* Number of doubles in a field (n1*n2 or n1*n2*nk); 0 for an unknown id. */
+size_t mom6b_field_size(const mom6b_model *m, int field);
+/* Copy a field to / from host memory (synchronous). */
+int mom6b_get_field(mom6b_model *m, int field, double *host, size_t count);
+int mom6b_set_field(mom6b_model *m, int field, const double *host, size_t count);
+/* Device address of a field (reference layout), for zero-copy callers. */
+int mom6b_field_device_ptr(mom6b_model *m, int field, void **dptr);
+/* out = {n1, n2, nk, is, ie, js, je, bt_nsteps} (1-based compute bounds). */
+int mom6b_dims(const mom6b_model *m, int *out8);
+/* The model's CUDA stream, as a cudaStream_t cast to void*. */
+int mom6b_stream(mom6b_model *m, void **stream);
+
+/* End-to-end step through host buffers: upload u, v, h, eta (pinned host
+ * pointers may be passed), run nsteps, download u, v, h, eta.  Any pointer may
+ * be NULL to skip that field. */
+int mom6b_step_host(mom6b_model *m, int nsteps, double *u, double *v, double *h,
+                    double *eta);
+
+/* verify_state of rk2_serial_driver.F90:563-623 computed on the device:
+ * out = {mass_init, mass_final, rel_error, max_u, max_v, max_eta, ke_total}. */
+int mom6b_verify(mom6b_model *m, double *out7);
+
+/* Per-kernel launch accounting: number of kernels of this library launched
+ * on the model's stream since the last reset. */
+int64_t mom6b_launch_count(const mom6b_model *m);
+void mom6b_reset_launch_count(mom6b_model *m);
+
+/* Set a timing hook: the step records CUDA events around the dominant kernel
+ * so callers can read its average duration (milliseconds per launch). */
+int mom6b_kernel_timing(mom6b_model *m, int enable);
+int mom6b_kernel_time_ms(mom6b_model *m, const char *kernel, double *avg_ms,
+                         int64_t *launches);
+
+const char *mom6b_last_error(void);
+const char *mom6b_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

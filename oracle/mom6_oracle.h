@@ -1,0 +1,105 @@
+/*
+ * mom6_oracle.h -- CPU restatement of the MOM6 mini-app's split RK2 step.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is the parity oracle for the B200 library:
+ * it restates, in plain C, the serial Fortran path of the reference
+ * (app/rk2_serial_driver.F90 + src/serial/*.F90 + src/common/mom6_types.F90)
+ * and, in a second family of functions prefixed occ_, the reference CUDA C
+ * kernels of src/cuda_c/*.cu.  Only tests/, the smoke check and the
+ * cpu_baseline leg of bench.py may link or call it; the product library never
+ * does.
+ *
+ * Array convention: every field is stored exactly as the reference stores it,
+ * Fortran column-major with 1-based indices, dimensions (n1, n2[, nk]) with
+ * n1 = ni + 2, n2 = nj + 2 (mom6_types.F90:145-148).
+ *
+ * Floating point: built with -ffp-contract=off, so every a*b+c is two
+ * roundings, as the reference's x86-64 -O3 gfortran build computes it.  The
+ * single-precision quirks of the serial Fortran (default-real literals such as
+ * 1e-6, 1e-15, 1e-12, 0.1 and the real(4) locals of PPM_limit_pos) are kept.
+ */
+#ifndef MOM6_ORACLE_H
+#define MOM6_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Initial-state constructions. */
+enum {
+    OR_INIT_REF = 0, /* analytic fields of rk2_serial_driver.F90:466-542 */
+    OR_INIT_CFG = 1  /* seeded beta-plane construction (Philox4x32-10) */
+};
+
+/* Field identifiers shared with the product's mom6b.h (same numbering). */
+enum {
+    OR_F_U = 0, OR_F_V, OR_F_H, OR_F_H0, OR_F_UH, OR_F_VH, OR_F_UP, OR_F_VP,
+    OR_F_ETA, OR_F_UBT, OR_F_VBT, OR_F_UBT_AV, OR_F_VBT_AV, OR_F_ETA_AV,
+    OR_F_HU_BT, OR_F_FA_U_W0, OR_F_FA_U_WW, OR_F_FA_U_E0, OR_F_FA_U_EE,
+    OR_F_UBT_WW, OR_F_UBT_EE, OR_F_DU_COR, OR_F_TAUX_BOT, OR_F_TAUY_BOT,
+    OR_F_TAUX, OR_F_TAUY, OR_F_RAY_U, OR_F_RAY_V, OR_F_CAU, OR_F_CAV,
+    OR_F_DIFFU, OR_F_DIFFV, OR_F_COUNT
+};
+
+typedef struct oracle_model oracle_model;
+
+typedef struct {
+    int ni, nj, nk;
+    int bt_nsteps;
+    int init_mode;      /* OR_INIT_REF / OR_INIT_CFG */
+    uint64_t seed;      /* CFG mode only */
+    double dt;          /* baroclinic step [s] */
+    double dx_km;       /* grid spacing [km] */
+    double lat_deg;     /* REF-mode central latitude for the beta plane */
+    double Kh;          /* Laplacian viscosity [m2 s-1] */
+    double Kv, Kv_ml, Kv_extra_bbl, Hmix, Hbbl;
+    int bc_fill;        /* 1: apply the periodic-x / wall-y halo fill */
+} oracle_config;
+
+void oracle_config_default(oracle_config *c, int init_mode);
+
+oracle_model *oracle_create(const oracle_config *c);
+void oracle_destroy(oracle_model *m);
+
+/* One split RK2 iteration of rk2_serial_driver.F90:218-399 per call. */
+void oracle_step(oracle_model *m, int nsteps);
+
+/* Field access: element count = n1*n2 (2-D) or n1*n2*nk (3-D). */
+size_t oracle_field_size(const oracle_model *m, int field);
+int oracle_get(const oracle_model *m, int field, double *out);
+int oracle_set(oracle_model *m, int field, const double *in);
+void oracle_dims(const oracle_model *m, int *out8); /* n1 n2 nk is ie js je ... */
+
+/* verify_state of rk2_serial_driver.F90:563-623: out = {mass_init,
+ * mass_final, rel_error, max_u, max_v, max_eta, ke_total}. */
+void oracle_verify(const oracle_model *m, double *out7);
+
+/* Single physics phases on the model's grid, for per-kernel tests.  Each
+ * operates on caller arrays laid out (n1, n2[, nk]) and on the model's
+ * persistent work arrays exactly as the serial module does. */
+void oracle_compute_transports(oracle_model *m, const double *u, const double *v,
+                               const double *h, double *uh, double *vh);
+void oracle_hor_visc(oracle_model *m, const double *u, const double *v,
+                     const double *h, double *diffu, double *diffv);
+void oracle_coriolis(oracle_model *m, const double *u, const double *v,
+                     const double *h, const double *uh, const double *vh,
+                     double *CAu, double *CAv);
+void oracle_vert_visc(oracle_model *m, double *u, double *v, const double *h,
+                      double dt);
+void oracle_btstep(oracle_model *m, const double *eta_in, const double *ubt_in,
+                   const double *vbt_in, double *u_av, double *v_av,
+                   double *eta_av);
+void oracle_continuity(oracle_model *m, const double *u, const double *hin,
+                       double *h, double *uh, double dt);
+void oracle_halo_fill(const oracle_model *m, double *f, int nz, int kind);
+
+/* Philox4x32-10 normal deviate used by the CFG initial state. */
+double oracle_normal(uint64_t seed, uint32_t stream, uint64_t index);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

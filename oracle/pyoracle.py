@@ -1,0 +1,186 @@
+"""ctypes binding of oracle/liboracle.so (test infrastructure only).
+
+The oracle restates app/rk2_serial_driver.F90 and src/serial/*.F90 of the
+reference in C; this module exposes it to numpy for the parity tests.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+INIT_REF, INIT_CFG = 0, 1
+
+# field ids (same numbering as mom6b.h / mom6_oracle.h)
+FIELDS = ["u", "v", "h", "h0", "uh", "vh", "up", "vp", "eta", "ubt", "vbt",
+          "ubt_av", "vbt_av", "eta_av", "hu_bt", "FA_u_W0", "FA_u_WW",
+          "FA_u_E0", "FA_u_EE", "uBT_WW", "uBT_EE", "du_cor", "taux_bot",
+          "tauy_bot", "taux", "tauy", "Ray_u", "Ray_v", "CAu", "CAv",
+          "diffu", "diffv"]
+FID = {n: i for i, n in enumerate(FIELDS)}
+FIELDS_3D = {"u", "v", "h", "h0", "uh", "vh", "up", "vp", "hu_bt", "Ray_u",
+             "Ray_v", "CAu", "CAv", "diffu", "diffv"}
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("ni", ctypes.c_int), ("nj", ctypes.c_int), ("nk", ctypes.c_int),
+                ("bt_nsteps", ctypes.c_int), ("init_mode", ctypes.c_int),
+                ("seed", ctypes.c_uint64), ("dt", ctypes.c_double),
+                ("dx_km", ctypes.c_double), ("lat_deg", ctypes.c_double),
+                ("Kh", ctypes.c_double), ("Kv", ctypes.c_double),
+                ("Kv_ml", ctypes.c_double), ("Kv_extra_bbl", ctypes.c_double),
+                ("Hmix", ctypes.c_double), ("Hbbl", ctypes.c_double),
+                ("bc_fill", ctypes.c_int)]
+
+
+def build():
+    """Compile liboracle.so with its Makefile (idempotent)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        P = ctypes.POINTER
+        d = ctypes.c_double
+        vp = ctypes.c_void_p
+        L.oracle_config_default.argtypes = [P(Config), ctypes.c_int]
+        L.oracle_create.argtypes = [P(Config)]
+        L.oracle_create.restype = vp
+        L.oracle_destroy.argtypes = [vp]
+        L.oracle_step.argtypes = [vp, ctypes.c_int]
+        L.oracle_field_size.argtypes = [vp, ctypes.c_int]
+        L.oracle_field_size.restype = ctypes.c_size_t
+        L.oracle_get.argtypes = [vp, ctypes.c_int, P(d)]
+        L.oracle_set.argtypes = [vp, ctypes.c_int, P(d)]
+        L.oracle_dims.argtypes = [vp, P(ctypes.c_int)]
+        L.oracle_verify.argtypes = [vp, P(d)]
+        for name in ("oracle_compute_transports",):
+            getattr(L, name).argtypes = [vp] + [P(d)] * 5
+        L.oracle_hor_visc.argtypes = [vp] + [P(d)] * 5
+        L.oracle_coriolis.argtypes = [vp] + [P(d)] * 7
+        L.oracle_vert_visc.argtypes = [vp, P(d), P(d), P(d), d]
+        L.oracle_btstep.argtypes = [vp] + [P(d)] * 6
+        L.oracle_continuity.argtypes = [vp, P(d), P(d), P(d), P(d), d]
+        L.oracle_halo_fill.argtypes = [vp, P(d), ctypes.c_int, ctypes.c_int]
+        L.oracle_normal.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64]
+        L.oracle_normal.restype = d
+        _LIB = L
+    return _LIB
+
+
+def _ptr(a):
+    assert a.dtype == np.float64 and a.flags["F_CONTIGUOUS"]
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Oracle:
+    """One oracle model (grid + state + persistent module work arrays)."""
+
+    def __init__(self, ni, nj, nk, bt_nsteps, init_mode=INIT_CFG, seed=0,
+                 dt=None, Kh=None, bc_fill=None):
+        L = lib()
+        c = Config()
+        L.oracle_config_default(ctypes.byref(c), init_mode)
+        c.ni, c.nj, c.nk, c.bt_nsteps, c.seed = ni, nj, nk, bt_nsteps, seed
+        if dt is not None:
+            c.dt = dt
+        if Kh is not None:
+            c.Kh = Kh
+        if bc_fill is not None:
+            c.bc_fill = int(bc_fill)
+        self.cfg = c
+        self._m = L.oracle_create(ctypes.byref(c))
+        if not self._m:
+            raise ValueError("oracle_create rejected the configuration")
+        dims = (ctypes.c_int * 8)()
+        L.oracle_dims(self._m, dims)
+        self.n1, self.n2, self.nk, self.is_, self.ie, self.js, self.je, _ = list(dims)
+
+    def close(self):
+        if self._m:
+            lib().oracle_destroy(self._m)
+            self._m = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def shape(self, name):
+        return (self.n1, self.n2, self.nk) if name in FIELDS_3D else (self.n1, self.n2)
+
+    def empty(self, name):
+        return np.zeros(self.shape(name), dtype=np.float64, order="F")
+
+    def get(self, name):
+        a = self.empty(name)
+        if lib().oracle_get(self._m, FID[name], _ptr(a)) != 0:
+            raise KeyError(name)
+        return a
+
+    def set(self, name, a):
+        a = np.asfortranarray(a, dtype=np.float64)
+        assert a.shape == self.shape(name)
+        if lib().oracle_set(self._m, FID[name], _ptr(a)) != 0:
+            raise KeyError(name)
+
+    def step(self, n=1):
+        lib().oracle_step(self._m, int(n))
+
+    def verify(self):
+        out = (ctypes.c_double * 7)()
+        lib().oracle_verify(self._m, out)
+        keys = ["mass_init", "mass_final", "rel_error", "max_u", "max_v",
+                "max_eta", "ke_total"]
+        return dict(zip(keys, list(out)))
+
+    # single phases -------------------------------------------------------
+    def continuity(self, u, hin, dt):
+        h = self.get("h")
+        uh = self.get("uh")
+        lib().oracle_continuity(self._m, _ptr(u), _ptr(hin), _ptr(h), _ptr(uh), dt)
+        return h, uh
+
+    def vert_visc(self, u, v, h, dt):
+        u = u.copy(order="F")
+        v = v.copy(order="F")
+        lib().oracle_vert_visc(self._m, _ptr(u), _ptr(v), _ptr(h), dt)
+        return u, v
+
+    def btstep(self, eta, ubt, vbt):
+        ua, va, ea = self.empty("ubt"), self.empty("vbt"), self.empty("eta")
+        lib().oracle_btstep(self._m, _ptr(eta), _ptr(ubt), _ptr(vbt), _ptr(ua),
+                            _ptr(va), _ptr(ea))
+        return ua, va, ea
+
+    def hor_visc(self, u, v, h):
+        du, dv = self.empty("u"), self.empty("v")
+        lib().oracle_hor_visc(self._m, _ptr(u), _ptr(v), _ptr(h), _ptr(du), _ptr(dv))
+        return du, dv
+
+    def coriolis(self, u, v, h, uh, vh):
+        cu, cv = self.empty("u"), self.empty("v")
+        lib().oracle_coriolis(self._m, _ptr(u), _ptr(v), _ptr(h), _ptr(uh),
+                              _ptr(vh), _ptr(cu), _ptr(cv))
+        return cu, cv
+
+    def transports(self, u, v, h):
+        uh, vh = self.empty("u"), self.empty("v")
+        lib().oracle_compute_transports(self._m, _ptr(u), _ptr(v), _ptr(h),
+                                        _ptr(uh), _ptr(vh))
+        return uh, vh
+
+    def halo_fill(self, f, kind):
+        f = np.asfortranarray(f.copy())
+        nz = f.shape[2] if f.ndim == 3 else 1
+        lib().oracle_halo_fill(self._m, _ptr(f), nz, kind)
+        return f
