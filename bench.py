@@ -279,6 +279,19 @@ def run_ours(args, world, rank, local, dist):
     m.close()
 
 
+def run_profile_case(args):
+    """A small case of the same kernels for ncu: ni = nj = args.profile_case,
+    nk = 75, bt 50, args.warmup + args.steps steps, nothing else."""
+    from hackathon_mom6_miniapp_b200 import INIT_CFG, Model
+    n = args.profile_case
+    m = Model(n, n, NK, BT, INIT_CFG, seed=0, dt=600.0)
+    m.step(args.warmup + args.steps)
+    m.synchronize()
+    print(json.dumps({"profile_case": n, "steps": args.warmup + args.steps,
+                      "launches": m.launch_count()}))
+    m.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -286,10 +299,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile-case", type=int, default=0,
+                    help="run N steps of a ni=nj=N domain only (for ncu captures)")
     args = ap.parse_args()
     world, rank, local, dist = dist_setup(args)
     try:
-        if args.impl == "reference":
+        if args.profile_case:
+            run_profile_case(args)
+        elif args.impl == "reference":
             run_reference(args, world, rank, local, dist)
         else:
             run_ours(args, world, rank, local, dist)

@@ -176,12 +176,11 @@ cudaError_t launch_vertvisc(const Dims& D, const Metrics& M, double* u, double* 
     int nrows = (D.je - D.js + 1) + (D.je - D.js + 2);
     dim3 grid((ncol + nb - 1) / nb, nrows, 1);
     size_t smem = (size_t)(D.nk + 2) * nb * sizeof(double);
-    static bool attr_set = false;
-    if (!attr_set || smem > 48 * 1024) {
-        cudaFuncSetAttribute(k_vertvisc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
-        attr_set = true;
-    }
+    // the attribute caps the dynamic shared memory of every later launch, so
+    // it is set for each launch's own size
+    cudaError_t e = cudaFuncSetAttribute(k_vertvisc,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
     k_vertvisc<<<grid, nb, smem, s>>>(D, M, u, v, h, dt, P, taux_bot, tauy_bot);
     return cudaGetLastError();
 }
