@@ -185,7 +185,8 @@ def run_ours(args, world, rank, local, dist):
     import torch
     from hackathon_mom6_miniapp_b200 import INIT_CFG, Model
     torch.cuda.set_device(local)
-    m = Model(NI, NJ, NK, BT, INIT_CFG, seed=rank, dt=600.0, device=local)
+    m = Model(NI, NJ, NK, BT, INIT_CFG, seed=rank, dt=600.0, device=local,
+              use_graph=not args.no_graph)
     stream = torch.cuda.ExternalStream(m.stream(), device=f"cuda:{local}")
     # warm-up
     m.step(args.warmup)
@@ -299,6 +300,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--profile-case", type=int, default=0,
                     help="run N steps of a ni=nj=N domain only (for ncu captures)")
     args = ap.parse_args()

@@ -21,9 +21,25 @@
 // of btstep_do_step and the CUDA C kernels ([is-1, ie] / [js-1, je],
 // :443-452).  The barrier spins with a clock64 budget; when it expires the
 // kernel records kDevTimeout and every block returns.
+#include <cstdlib>
+
 #include "kernels.h"
 
 namespace mom6b {
+
+// Global home of the per-point private quantities when they do not fit in
+// shared memory.
+__device__ __forceinline__ double* priv_global(const BTWork& W, int q, int p)
+{
+    switch (q) {
+    case 0: return W.ubt_prev + p;
+    case 1: return W.vbt_prev + p;
+    case 2: return W.PFu + p;
+    case 3: return W.PFv + p;
+    case 4: return W.ubt_av + p;
+    default: return W.vbt_av + p;
+    }
+}
 
 // Sense-counting grid barrier.  Returns false when the wait budget ran out
 // (or another block reported a timeout); callers then return.
@@ -45,14 +61,17 @@ __device__ __forceinline__ bool grid_barrier(const BTWork& W, unsigned int nbloc
             atomicAdd(W.bar_gen, 1u);
         } else {
             long long t0 = clock64();
+            unsigned int spins = 0;
             while (*gen == g) {
-                if (*st != kDevOk) { ok = 0; break; }
-                if (clock64() - t0 > budget) {
-                    atomicExch(W.status, kDevTimeout);
-                    ok = 0;
-                    break;
+                if ((++spins & 63u) == 0) {
+                    if (*st != kDevOk) { ok = 0; break; }
+                    if (clock64() - t0 > budget) {
+                        atomicExch(W.status, kDevTimeout);
+                        ok = 0;
+                        break;
+                    }
+                    if (spins > 4096u) __nanosleep(64);
                 }
-                __nanosleep(32);
             }
         }
         __threadfence();
@@ -62,11 +81,22 @@ __device__ __forceinline__ bool grid_barrier(const BTWork& W, unsigned int nbloc
     return s_ok != 0;
 }
 
-__global__ void __launch_bounds__(512)
+// Points are owned per thread inside the active box [is-1, ie+1] x
+// [js-1, je+1] (nothing outside it changes during the loop).  With FAST, a
+// thread owns at most kBtMaxR points, caches their (i, j) in registers and
+// keeps the quantities only it reads (ubt_prev, vbt_prev, PFu, PFv, ubt_av,
+// vbt_av) in shared memory; otherwise indices are recomputed per phase and
+// those quantities live in the global work arrays (any grid size).
+constexpr int kBtThreads = 1024, kBtMaxR = 4;
+enum { PV_PREVU = 0, PV_PREVV, PV_PFU, PV_PFV, PV_AVU, PV_AVV, PV_N };
+
+template <bool FAST>
+__global__ void __launch_bounds__(kBtThreads, 1)
 k_btstep(Dims D, Metrics M, BTWork W, BTParams P, const double* eta_in,
          const double* ubt_in, const double* vbt_in, double* u_av, double* v_av,
          double* eta_av)
 {
+    extern __shared__ double s_priv[];  // [PV_N][kBtMaxR][blockDim.x] when FAST
     const unsigned int nblocks = gridDim.x;
     const int npts = D.n1 * D.n2;
     const int gtid = (int)(blockIdx.x * blockDim.x + threadIdx.x);
@@ -75,25 +105,55 @@ k_btstep(Dims D, Metrics M, BTWork W, BTParams P, const double* eta_in,
     // serial ranges vs. extended ranges for uhbt/vhbt and the averages
     const int iu0 = P.extended ? is - 1 : is, iu1 = P.extended ? ie : ie - 1;
     const int jv0 = P.extended ? js - 1 : js, jv1 = P.extended ? je : je - 1;
-#define PT_LOOP for (int p = gtid; p < npts; p += gsz)
-#define PT_IJ const int i = p % D.n1 + 1, j = p / D.n1 + 1
+    const int bw = ie - is + 3;                 // active box width
+    const int nbox = bw * (je - js + 3);
+    const int nr = FAST ? (nbox - gtid + gsz - 1) / gsz : 0;
 #define A(a, ii, jj) MOM6B_A2(a, ii, jj, D)
+#define PV(q, r, p) (*(FAST ? &s_priv[((q) * kBtMaxR + (r)) * blockDim.x + threadIdx.x] \
+                            : priv_global(W, q, p)))
 
-    // init (:199-207)
-    PT_LOOP {
+    int pi[kBtMaxR], pj[kBtMaxR], pp[kBtMaxR];
+    if (FAST) {
+#pragma unroll
+        for (int r = 0; r < kBtMaxR; ++r) {
+            int q = gtid + r * gsz;
+            pi[r] = is - 1 + q % bw;
+            pj[r] = js - 1 + q / bw;
+            pp[r] = (pj[r] - 1) * D.n1 + (pi[r] - 1);
+#pragma unroll
+            for (int v = 0; v < PV_N; ++v)
+                s_priv[(v * kBtMaxR + r) * blockDim.x + threadIdx.x] = 0.0;
+        }
+    }
+    // visit every owned point: f(r, i, j, p)
+    auto for_points = [&](auto&& f) {
+        if (FAST) {
+#pragma unroll
+            for (int r = 0; r < kBtMaxR; ++r) {
+                if (r >= nr) break;
+                f(r, pi[r], pj[r], pp[r]);
+            }
+        } else {
+            for (int q = gtid; q < nbox; q += gsz) {
+                int i = is - 1 + q % bw, j = js - 1 + q / bw;
+                f(0, i, j, (j - 1) * D.n1 + (i - 1));
+            }
+        }
+    };
+
+    // init (:199-207): state copies over the whole data domain
+    for (int p = gtid; p < npts; p += gsz) {
         W.eta[p] = eta_in[p];
         W.ubt[p] = ubt_in[p];
         W.vbt[p] = vbt_in[p];
-        W.ubt_av[p] = 0.0;
-        W.vbt_av[p] = 0.0;
+        if (!FAST) { W.ubt_av[p] = 0.0; W.vbt_av[p] = 0.0; }
     }
     if (!grid_barrier(W, nblocks, P.spin_budget)) return;
 
     auto phase_A = [&]() {
-        PT_LOOP {
-            PT_IJ;
-            if (j >= js && j <= je && i >= is - 1 && i <= ie + 1) W.ubt_prev[p] = W.ubt[p];
-            if (j >= js - 1 && j <= je + 1 && i >= is && i <= ie) W.vbt_prev[p] = W.vbt[p];
+        for_points([&](int r, int i, int j, int p) {
+            if (j >= js && j <= je) PV(PV_PREVU, r, p) = W.ubt[p];  // i in [is-1, ie+1]
+            if (i >= is && i <= ie) PV(PV_PREVV, r, p) = W.vbt[p];  // j in [js-1, je+1]
             if (i >= is && i <= ie && j >= js && j <= je)
                 W.eta_pred[p] =
                     W.eta[p] + (P.dtbt * A(M.IareaT, i, j)) *
@@ -101,7 +161,7 @@ k_btstep(Dims D, Metrics M, BTWork W, BTParams P, const double* eta_in,
                                      (A(M.Datu, i, j) * W.ubt[p])) +
                                     ((A(M.Datv, i, j - 1) * A(W.vbt, i, j - 1)) -
                                      (A(M.Datv, i, j) * W.vbt[p])));
-        }
+        });
     };
     auto update_u = [&](int p, int i, int j, double PFu) {
         double Cor_u = (((MOM6B_F4(M.f_4_u, 4, i, j, D) * A(W.vbt, i + 1, j)) +
@@ -124,102 +184,354 @@ k_btstep(Dims D, Metrics M, BTWork W, BTParams P, const double* eta_in,
     for (int n = 1; n <= P.nstep; ++n) {
         const bool v_first = ((n + P.first_direction) % 2) == 1;
         // phase B: pressure force (:234-247) and the first update
-        PT_LOOP {
-            PT_IJ;
+        for_points([&](int r, int i, int j, int p) {
             if (j >= js && j <= je && i >= is && i <= ie - 1)
-                W.PFu[p] = ((W.eta_pred[p] * A(M.gtot_E, i, j)) -
-                            (A(W.eta_pred, i + 1, j) * A(M.gtot_W, i + 1, j))) *
-                           P.dgeo_de * A(M.IdxCu, i, j);
+                PV(PV_PFU, r, p) = ((W.eta_pred[p] * A(M.gtot_E, i, j)) -
+                                    (A(W.eta_pred, i + 1, j) * A(M.gtot_W, i + 1, j))) *
+                                   P.dgeo_de * A(M.IdxCu, i, j);
             if (j >= js && j <= je - 1 && i >= is && i <= ie)
-                W.PFv[p] = ((W.eta_pred[p] * A(M.gtot_N, i, j)) -
-                            (A(W.eta_pred, i, j + 1) * A(M.gtot_S, i, j + 1))) *
-                           P.dgeo_de * A(M.IdyCv, i, j);
+                PV(PV_PFV, r, p) = ((W.eta_pred[p] * A(M.gtot_N, i, j)) -
+                                    (A(W.eta_pred, i, j + 1) * A(M.gtot_S, i, j + 1))) *
+                                   P.dgeo_de * A(M.IdyCv, i, j);
             if (v_first) {
-                if (i >= is && i <= ie && j >= js && j <= je - 1) update_v(p, i, j, W.PFv[p]);
+                if (i >= is && i <= ie && j >= js && j <= je - 1)
+                    update_v(p, i, j, PV(PV_PFV, r, p));
             } else {
-                if (i >= is && i <= ie - 1 && j >= js && j <= je) update_u(p, i, j, W.PFu[p]);
+                if (i >= is && i <= ie - 1 && j >= js && j <= je)
+                    update_u(p, i, j, PV(PV_PFU, r, p));
             }
-        }
+        });
         if (!grid_barrier(W, nblocks, P.spin_budget)) return;
         // phase C: second update, transports (:263-272), averages (:282-291)
-        PT_LOOP {
-            PT_IJ;
+        for_points([&](int r, int i, int j, int p) {
             if (v_first) {
-                if (i >= is && i <= ie - 1 && j >= js && j <= je) update_u(p, i, j, W.PFu[p]);
+                if (i >= is && i <= ie - 1 && j >= js && j <= je)
+                    update_u(p, i, j, PV(PV_PFU, r, p));
             } else {
-                if (i >= is && i <= ie && j >= js && j <= je - 1) update_v(p, i, j, W.PFv[p]);
+                if (i >= is && i <= ie && j >= js && j <= je - 1)
+                    update_v(p, i, j, PV(PV_PFV, r, p));
             }
             if (j >= js && j <= je && i >= iu0 && i <= iu1) {
-                W.uhbt[p] = A(M.Datu, i, j) * (P.trans_wt1 * W.ubt[p] + P.trans_wt2 * W.ubt_prev[p]);
-                W.ubt_av[p] = W.ubt_av[p] + W.ubt[p] * P.inv_nstep;
+                double ub = W.ubt[p];
+                W.uhbt[p] = A(M.Datu, i, j) * (P.trans_wt1 * ub + P.trans_wt2 * PV(PV_PREVU, r, p));
+                PV(PV_AVU, r, p) = PV(PV_AVU, r, p) + ub * P.inv_nstep;
             }
             if (j >= jv0 && j <= jv1 && i >= is && i <= ie) {
-                W.vhbt[p] = A(M.Datv, i, j) * (P.trans_wt1 * W.vbt[p] + P.trans_wt2 * W.vbt_prev[p]);
-                W.vbt_av[p] = W.vbt_av[p] + W.vbt[p] * P.inv_nstep;
+                double vb = W.vbt[p];
+                W.vhbt[p] = A(M.Datv, i, j) * (P.trans_wt1 * vb + P.trans_wt2 * PV(PV_PREVV, r, p));
+                PV(PV_AVV, r, p) = PV(PV_AVV, r, p) + vb * P.inv_nstep;
             }
-        }
+        });
         if (!grid_barrier(W, nblocks, P.spin_budget)) return;
         // phase D: eta update (:274-279), then phase A of the next substep
-        PT_LOOP {
-            PT_IJ;
+        for_points([&](int r, int i, int j, int p) {
             if (i >= is && i <= ie && j >= js && j <= je)
                 W.eta[p] = W.eta[p] - P.dtbt * A(M.IareaT, i, j) *
                                           ((W.uhbt[p] - A(W.uhbt, i - 1, j)) +
                                            (W.vhbt[p] - A(W.vhbt, i, j - 1)));
+        });
+        // eta_pred(i,j) needs only this thread's new eta(i,j); the velocity
+        // neighbours were final before the last barrier
+        if (n < P.nstep) phase_A();
+        if (!grid_barrier(W, nblocks, P.spin_budget)) return;
+    }
+    // copy output (:296-302); outputs may alias the inputs.  The averages are
+    // zero outside their ranges (the init of :204-205).
+    if (FAST) {
+        for (int p = gtid; p < npts; p += gsz) {
+            u_av[p] = 0.0;
+            v_av[p] = 0.0;
+            eta_av[p] = W.eta[p];
         }
-        if (n < P.nstep) {
-            // eta_pred(i,j) needs only this thread's new eta(i,j); the velocity
-            // neighbours were final before the last barrier
-            phase_A();
+        if (!grid_barrier(W, nblocks, P.spin_budget)) return;
+        for_points([&](int r, int i, int j, int p) {
+            u_av[p] = PV(PV_AVU, r, p);
+            v_av[p] = PV(PV_AVV, r, p);
+        });
+    } else {
+        for (int p = gtid; p < npts; p += gsz) {
+            u_av[p] = W.ubt_av[p];
+            v_av[p] = W.vbt_av[p];
+            eta_av[p] = W.eta[p];
+        }
+    }
+#undef A
+#undef PV
+}
+
+// ---------------------------------------------------------------------------
+// Tiled variant: one grid barrier per substep.
+// ---------------------------------------------------------------------------
+// The updated box [is-1, ie] x [js-1, je] is split into nbx x nby tiles, one
+// per CTA.  Each substep a CTA loads the previous eta/ubt/vbt on its tile
+// widened by two points below and one above, recomputes eta_pred, the two
+// velocity updates and the transports on the halo it needs, and writes its
+// own tile's new state to the other buffer; a single grid barrier then ends
+// the substep.  The evaluation order of every point is the serial one.  The
+// averages of the owned points stay in registers (at most kBtTileR per
+// thread).
+constexpr int kBtTileR = 4;
+
+struct BTTiles {
+    int nbx, nby, tw, th;  // tiles and tile size
+};
+
+template <int NT, bool UNI>
+__global__ void __launch_bounds__(NT, 1)
+k_btstep_tiled(Dims D, Metrics M, UniMetrics U, BTWork W, BTParams P, BTTiles T,
+               const double* eta_in, const double* ubt_in, const double* vbt_in,
+               double* u_av, double* v_av, double* eta_av)
+{
+    extern __shared__ double smem[];
+    const unsigned int nblocks = gridDim.x;
+    const int tid = (int)threadIdx.x;
+    const int npts = D.n1 * D.n2;
+    const int gtid = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int gsz = (int)(gridDim.x * blockDim.x);
+    const int is = D.is, ie = D.ie, js = D.js, je = D.je;
+    const int iu0 = P.extended ? is - 1 : is, iu1 = P.extended ? ie : ie - 1;
+    const int jv0 = P.extended ? js - 1 : js, jv1 = P.extended ? je : je - 1;
+    const int tx = (int)blockIdx.x % T.nbx, ty = (int)blockIdx.x / T.nbx;
+    const int x0 = is - 1 + tx * T.tw, y0 = js - 1 + ty * T.th;
+    const int x1 = min(x0 + T.tw - 1, ie), y1 = min(y0 + T.th - 1, je);
+    const int lx0 = x0 - 2, ly0 = y0 - 2;              // local origin
+    const int LW = T.tw + 3, LH = T.th + 3;
+    const int LN = LW * LH;
+    double* Se = smem;            // eta, previous substep
+    double* Su = Se + LN;         // ubt, previous substep (= ubt_prev)
+    double* Sv = Su + LN;         // vbt, previous substep (= vbt_prev)
+    double* Sp = Sv + LN;         // eta_pred
+    double* Sun = Sp + LN;        // ubt after this substep
+    double* Svn = Sun + LN;       // vbt after this substep
+#define L(a, i, j) a[((j) - ly0) * LW + ((i) - lx0)]
+#define G(a, i, j) MOM6B_A2(a, i, j, D)
+#define GM(f, i, j) (UNI ? U.f : MOM6B_A2(M.f, i, j, D))
+#define F4U(c, i, j) (UNI ? U.f4u_row[((j) - 1) * 4 + (c) - 1] : MOM6B_F4(M.f_4_u, c, i, j, D))
+#define F4V(c, i, j) (UNI ? U.f4v_row[((j) - 1) * 4 + (c) - 1] : MOM6B_F4(M.f_4_v, c, i, j, D))
+
+    // owned points and their averages
+    // empty when the tile lies beyond the box (both extents clamp to zero)
+    const int ow = max(x1 - x0 + 1, 0), oh = max(y1 - y0 + 1, 0);
+    double avu[kBtTileR], avv[kBtTileR];
+#pragma unroll
+    for (int r = 0; r < kBtTileR; ++r) avu[r] = avv[r] = 0.0;
+
+    // init (:199-207): both buffers hold the whole input state
+    for (int p = gtid; p < npts; p += gsz) {
+        double e = eta_in[p], ub = ubt_in[p], vb = vbt_in[p];
+        W.eta[p] = e; W.ubt[p] = ub; W.vbt[p] = vb;
+        W.eta_pred[p] = e; W.ubt_prev[p] = ub; W.vbt_prev[p] = vb;
+    }
+    if (!grid_barrier(W, nblocks, P.spin_budget)) return;
+
+    for (int n = 1; n <= P.nstep; ++n) {
+        const bool v_first = ((n + P.first_direction) % 2) == 1;
+        const double* ce = (n & 1) ? W.eta : W.eta_pred;
+        const double* cu = (n & 1) ? W.ubt : W.ubt_prev;
+        const double* cv = (n & 1) ? W.vbt : W.vbt_prev;
+        double* ne = (n & 1) ? W.eta_pred : W.eta;
+        double* nu = (n & 1) ? W.ubt_prev : W.ubt;
+        double* nv = (n & 1) ? W.vbt_prev : W.vbt;
+        // S1: previous state on the local window
+        for (int q = tid; q < LN; q += NT) {
+            int i = lx0 + q % LW, j = ly0 + q / LW;
+            double e = 0.0, ub = 0.0, vb = 0.0;
+            if (i >= 1 && i <= D.n1 && j >= 1 && j <= D.n2) {
+                int p = (j - 1) * D.n1 + (i - 1);
+                e = ce[p]; ub = cu[p]; vb = cv[p];
+            }
+            Se[q] = e; Su[q] = ub; Sv[q] = vb; Sun[q] = ub; Svn[q] = vb;
+        }
+        __syncthreads();
+        // S2: eta_pred on [x0-1, x1+1] x [y0-1, y1+1] within [is, ie] x [js, je]
+        {
+            int a0 = max(x0 - 1, is), a1 = min(x1 + 1, ie);
+            int b0 = max(y0 - 1, js), b1 = min(y1 + 1, je);
+            int w = a1 - a0 + 1, hgt = b1 - b0 + 1;
+            for (int q = tid; q < w * hgt; q += NT) {
+                int i = a0 + q % w, j = b0 + q / w;
+                L(Sp, i, j) = L(Se, i, j) + (P.dtbt * GM(IareaT, i, j)) *
+                                                (((GM(Datu, i - 1, j) * L(Su, i - 1, j)) -
+                                                  (GM(Datu, i, j) * L(Su, i, j))) +
+                                                 ((GM(Datv, i, j - 1) * L(Sv, i, j - 1)) -
+                                                  (GM(Datv, i, j) * L(Sv, i, j))));
+            }
+        }
+        __syncthreads();
+        auto upd_u = [&](int i, int j, const double* Vsrc) {
+            double PFu = ((L(Sp, i, j) * GM(gtot_E, i, j)) -
+                          (L(Sp, i + 1, j) * GM(gtot_W, i + 1, j))) *
+                         P.dgeo_de * GM(IdxCu, i, j);
+            double Cor_u = (((F4U(4, i, j) * L(Vsrc, i + 1, j)) +
+                             (F4U(1, i, j) * L(Vsrc, i, j - 1))) +
+                            ((F4U(3, i, j) * L(Vsrc, i, j)) +
+                             (F4U(2, i, j) * L(Vsrc, i + 1, j - 1))));
+            L(Sun, i, j) = GM(bt_rem_u, i, j) * (L(Su, i, j) + P.dtbt * (Cor_u + PFu));
+        };
+        auto upd_v = [&](int i, int j, const double* Usrc) {
+            double PFv = ((L(Sp, i, j) * GM(gtot_N, i, j)) -
+                          (L(Sp, i, j + 1) * GM(gtot_S, i, j + 1))) *
+                         P.dgeo_de * GM(IdyCv, i, j);
+            double Cor_v = -1.0 * (((F4V(1, i, j) * L(Usrc, i - 1, j)) +
+                                    (F4V(4, i, j) * L(Usrc, i, j + 1))) +
+                                   ((F4V(2, i, j) * L(Usrc, i, j)) +
+                                    (F4V(3, i, j) * L(Usrc, i - 1, j + 1))));
+            L(Svn, i, j) = GM(bt_rem_v, i, j) * (L(Sv, i, j) + P.dtbt * (Cor_v + PFv));
+        };
+        // S3 / S4: the two velocity updates on the regions the tile needs
+        if (v_first) {
+            int a0 = max(x0 - 1, is), a1 = min(x1 + 1, ie);
+            int b0 = max(y0 - 1, js), b1 = min(y1, je - 1);
+            int w = a1 - a0 + 1, hgt = b1 - b0 + 1;
+            for (int q = tid; q < w * hgt; q += NT) upd_v(a0 + q % w, b0 + q / w, Su);
+            __syncthreads();
+            a0 = max(x0 - 1, is); a1 = min(x1, ie - 1);
+            b0 = max(y0, js); b1 = min(y1, je);
+            w = a1 - a0 + 1; hgt = b1 - b0 + 1;
+            for (int q = tid; q < w * hgt; q += NT) upd_u(a0 + q % w, b0 + q / w, Svn);
+        } else {
+            int a0 = max(x0 - 1, is), a1 = min(x1, ie - 1);
+            int b0 = max(y0 - 1, js), b1 = min(y1 + 1, je);
+            int w = a1 - a0 + 1, hgt = b1 - b0 + 1;
+            for (int q = tid; q < w * hgt; q += NT) upd_u(a0 + q % w, b0 + q / w, Sv);
+            __syncthreads();
+            a0 = max(x0, is); a1 = min(x1, ie);
+            b0 = max(y0 - 1, js); b1 = min(y1, je - 1);
+            w = a1 - a0 + 1; hgt = b1 - b0 + 1;
+            for (int q = tid; q < w * hgt; q += NT) upd_v(a0 + q % w, b0 + q / w, Sun);
+        }
+        __syncthreads();
+        // S5: transports, eta update and averages on the owned points
+        auto uhbt_at = [&](int i, int j) -> double {
+            if (i < iu0 || i > iu1 || j < js || j > je) return 0.0;
+            return GM(Datu, i, j) * (P.trans_wt1 * L(Sun, i, j) + P.trans_wt2 * L(Su, i, j));
+        };
+        auto vhbt_at = [&](int i, int j) -> double {
+            if (j < jv0 || j > jv1 || i < is || i > ie) return 0.0;
+            return GM(Datv, i, j) * (P.trans_wt1 * L(Svn, i, j) + P.trans_wt2 * L(Sv, i, j));
+        };
+#pragma unroll
+        for (int r = 0; r < kBtTileR; ++r) {
+            int q = tid + r * NT;
+            if (q >= ow * oh) break;
+            int i = x0 + q % ow, j = y0 + q / ow;
+            int p = (j - 1) * D.n1 + (i - 1);
+            if (i >= is && i <= ie && j >= js && j <= je) {
+                double e = L(Se, i, j) - P.dtbt * GM(IareaT, i, j) *
+                                             ((uhbt_at(i, j) - uhbt_at(i - 1, j)) +
+                                              (vhbt_at(i, j) - vhbt_at(i, j - 1)));
+                ne[p] = e;
+            }
+            if (i >= is && i <= ie - 1 && j >= js && j <= je) nu[p] = L(Sun, i, j);
+            if (i >= is && i <= ie && j >= js && j <= je - 1) nv[p] = L(Svn, i, j);
+            if (j >= js && j <= je && i >= iu0 && i <= iu1)
+                avu[r] = avu[r] + L(Sun, i, j) * P.inv_nstep;
+            if (j >= jv0 && j <= jv1 && i >= is && i <= ie)
+                avv[r] = avv[r] + L(Svn, i, j) * P.inv_nstep;
         }
         if (!grid_barrier(W, nblocks, P.spin_budget)) return;
     }
-    // copy output (:296-302); outputs may alias the inputs
-    PT_LOOP {
-        u_av[p] = W.ubt_av[p];
-        v_av[p] = W.vbt_av[p];
-        eta_av[p] = W.eta[p];
+    // outputs (:296-302); they may alias the inputs
+    const double* fe = (P.nstep & 1) ? W.eta_pred : W.eta;
+    for (int p = gtid; p < npts; p += gsz) {
+        eta_av[p] = fe[p];
+        int i = p % D.n1 + 1, j = p / D.n1 + 1;
+        if (i < is - 1 || i > ie || j < js - 1 || j > je) {  // not owned by a tile
+            u_av[p] = 0.0;
+            v_av[p] = 0.0;
+        }
     }
-#undef PT_LOOP
-#undef PT_IJ
-#undef A
+#pragma unroll
+    for (int r = 0; r < kBtTileR; ++r) {
+        int q = tid + r * NT;
+        if (q >= ow * oh) break;
+        int i = x0 + q % ow, j = y0 + q / ow;
+        int p = (j - 1) * D.n1 + (i - 1);
+        u_av[p] = avu[r];
+        v_av[p] = avv[r];
+    }
+#undef L
+#undef G
+#undef GM
+#undef F4U
+#undef F4V
 }
 
 static int g_bt_blocks = 0;
 
-cudaError_t launch_btstep(const Dims& D, const Metrics& M, const BTWork& W,
+cudaError_t launch_btstep(const Dims& D, const Metrics& M, const UniMetrics& U,
+                          const BTWork& W,
                           const BTParams& P, const double* eta_in,
                           const double* ubt_in, const double* vbt_in,
                           double* u_av, double* v_av, double* eta_av,
                           cudaStream_t s)
 {
-    const int nb = 512;
+    const size_t smem_fast = (size_t)PV_N * kBtMaxR * kBtThreads * sizeof(double);
     if (g_bt_blocks == 0) {
-        int dev = 0, nsm = 0, per_sm = 0;
+        int dev = 0, nsm = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_btstep, nb, 0);
-        if (per_sm < 1) return cudaErrorLaunchOutOfResources;
-        g_bt_blocks = nsm * (per_sm < 2 ? per_sm : 2);
+        cudaError_t e = cudaFuncSetAttribute(k_btstep<true>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem_fast);
+        if (e != cudaSuccess) return e;
+        g_bt_blocks = nsm;
     }
-    int npts = D.n1 * D.n2;
+    // tiled variant: the updated box split into at most one tile per SM
+    {
+        const int NT = 1024;
+        int bw = D.ie - D.is + 2, bh = D.je - D.js + 2;
+        int nbx = 1, nby = 1;
+        while ((long long)(nbx + 1) * (nby + 1) <= g_bt_blocks) { ++nbx; ++nby; }
+        while ((long long)(nbx + 1) * nby <= g_bt_blocks && (bw + nbx) / (nbx + 1) >= 8) ++nbx;
+        BTTiles T;
+        T.nbx = nbx; T.nby = nby;
+        T.tw = (bw + nbx - 1) / nbx; T.th = (bh + nby - 1) / nby;
+        size_t smem = (size_t)6 * (T.tw + 3) * (T.th + 3) * sizeof(double);
+        if ((long long)T.tw * T.th <= (long long)NT * kBtTileR && smem <= 227 * 1024 &&
+            !getenv("MOM6B_BT_UNTILED")) {
+            const void* fn = U.valid_bt ? (const void*)k_btstep_tiled<NT, true>
+                                        : (const void*)k_btstep_tiled<NT, false>;
+            cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem);
+            if (e != cudaSuccess) return e;
+            Dims Dc = D; Metrics Mc = M; UniMetrics Uc = U; BTWork Wc = W; BTParams Pc = P;
+            BTTiles Tc = T;
+            void* args[] = {&Dc, &Mc, &Uc, &Wc, &Pc, &Tc, (void*)&eta_in, (void*)&ubt_in,
+                            (void*)&vbt_in, (void*)&u_av, (void*)&v_av, (void*)&eta_av};
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(nbx * nby, 1, 1);
+            cfg.blockDim = dim3(NT, 1, 1);
+            cfg.dynamicSmemBytes = smem;
+            cfg.stream = s;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeCooperative;
+            attr[0].val.cooperative = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            return cudaLaunchKernelExC(&cfg, fn, args);
+        }
+    }
+    const long long nbox = (long long)(D.ie - D.is + 3) * (D.je - D.js + 3);
     int blocks = g_bt_blocks;
-    int need = (npts + nb - 1) / nb;
+    int need = (int)((nbox + kBtThreads - 1) / kBtThreads);
     if (blocks > need) blocks = need;
+    const bool fast = (long long)blocks * kBtThreads * kBtMaxR >= nbox;
     Dims Dc = D; Metrics Mc = M; BTWork Wc = W; BTParams Pc = P;
     void* args[] = {&Dc, &Mc, &Wc, &Pc, (void*)&eta_in, (void*)&ubt_in, (void*)&vbt_in,
                     (void*)&u_av, (void*)&v_av, (void*)&eta_av};
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(blocks, 1, 1);
-    cfg.blockDim = dim3(nb, 1, 1);
-    cfg.dynamicSmemBytes = 0;
+    cfg.blockDim = dim3(kBtThreads, 1, 1);
+    cfg.dynamicSmemBytes = fast ? smem_fast : 0;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelExC(&cfg, (const void*)k_btstep, args);
+    return cudaLaunchKernelExC(&cfg, fast ? (const void*)k_btstep<true>
+                                          : (const void*)k_btstep<false>, args);
 }
 
 // ---------------------------------------------------------------------------

@@ -26,6 +26,8 @@
 // The FP32 quirks of the serial source are kept: the real(4) locals of
 // PPM_limit_pos and the default-real literals 1e-6, 1e-4, 1e-2, 1e-15, 1e-12
 // and 0.1.
+#include <cstdlib>
+
 #include "kernels.h"
 
 namespace mom6b {
@@ -105,28 +107,28 @@ struct FaceCol {
 };
 
 // zonal_flux_layer (:554-583) for one layer; returns uh and sets h_marg.
+// The two upwind cases are one operation sequence on (base, other, h) =
+// (h_E(i), h_W(i), h(i)) for u > 0 or (h_W(i+1), h_E(i+1), h(i+1)) for u < 0,
+// and CFL = (|u| dt) Idx equals the reference's -(u dt Idx) for u < 0 exactly,
+// so the evaluation is written without a divergent branch.
 __device__ __forceinline__ double flux_eval(const FaceCol& F, int k, double uI,
                                             double dt, double& h_marg)
 {
     const size_t o = (size_t)(k - 1) * F.plane;
-    double uh;
-    if (uI > 0.0) {
-        double CFL = uI * dt * F.IdxT_i;
-        double hWi = F.hWc[o], hEi = F.hEc[o];
-        double curv_3 = (hWi + hEi) - 2.0 * F.hc[o];
-        uh = F.dy * uI * (hEi + CFL * (0.5 * (hWi - hEi) + curv_3 * (CFL - 1.5)));
-        h_marg = hEi + CFL * ((hWi - hEi) + 3.0 * curv_3 * (CFL - 1.0));
-    } else if (uI < 0.0) {
-        double CFL = -(uI * dt * F.IdxT_ip1);
-        double hWp = F.hWc[o + 1], hEp = F.hEc[o + 1];
-        double curv_3 = (hWp + hEp) - 2.0 * F.hc[o + 1];
-        uh = F.dy * uI * (hWp + CFL * (0.5 * (hEp - hWp) + curv_3 * (CFL - 1.5)));
-        h_marg = hWp + CFL * ((hEp - hWp) + 3.0 * curv_3 * (CFL - 1.0));
-    } else {
-        uh = 0.0;
-        h_marg = 0.5 * (F.hWc[o + 1] + F.hEc[o]);
-    }
-    return uh;
+    const double hWi = F.hWc[o], hEi = F.hEc[o], hi = F.hc[o];
+    const double hWp = F.hWc[o + 1], hEp = F.hEc[o + 1], hp = F.hc[o + 1];
+    const bool pos = uI > 0.0;
+    const double base = pos ? hEi : hWp;
+    const double oth = pos ? hWi : hEp;
+    const double hc = pos ? hi : hp;
+    const double Idx = pos ? F.IdxT_i : F.IdxT_ip1;
+    const double CFL = fabs(uI) * dt * Idx;
+    const double curv_3 = (oth + base) - 2.0 * hc;
+    const double uh = F.dy * uI * (base + CFL * (0.5 * (oth - base) + curv_3 * (CFL - 1.5)));
+    const double hm = base + CFL * ((oth - base) + 3.0 * curv_3 * (CFL - 1.0));
+    const bool zero = !(uI > 0.0) && !(uI < 0.0);
+    h_marg = zero ? 0.5 * (hWp + hEi) : hm;
+    return zero ? 0.0 : uh;
 }
 
 // zonal_flux_adjust for one face (:813-903).  When uh_out is given the flux of
@@ -335,6 +337,9 @@ k_cont_faces(Dims D, Metrics M, const double* __restrict__ u,
     }
 }
 
+// CTAs per SM for k_cont_faces; 0 lets the hardware fill the SM.
+constexpr int kContCtasPerSM = 0;
+
 cudaError_t launch_continuity(const Dims& D, const Metrics& M, const double* u,
                               const double* hin, double* hW, double* hE,
                               const double* uhbt, const ContOut& O, double dt,
@@ -346,11 +351,27 @@ cudaError_t launch_continuity(const Dims& D, const Metrics& M, const double* u,
         k_ppm_edges<<<grid, 128, 0, s>>>(D, M, hin, hW, hE, h_min);
     }
     {
+        // Residency: each face re-reads its column on every Newton pass, so
+        // the resident CTAs' columns should stay in L2.  The dynamic shared
+        // memory request is padded to cap the CTAs per SM (kContCtasPerSM).
         const int nb = 128, step = nb - 1;
         int nfaces = D.ie - (D.is - 1) + 1;
         dim3 grid((nfaces - 1 + step - 1) / step, D.je - D.js + 1, 1);
-        k_cont_faces<<<grid, nb, (size_t)D.nk * sizeof(double), s>>>(D, M, u, hin, hW, hE,
-                                                                     uhbt, O, dt);
+        size_t smem = (size_t)D.nk * sizeof(double);
+        static int ctas = -1;
+        if (ctas < 0) {
+            const char* e = getenv("MOM6B_CONT_CTAS_PER_SM");
+            ctas = e ? atoi(e) : kContCtasPerSM;
+        }
+        if (ctas > 0) {
+            size_t pad = (size_t)(227 * 1024) / (size_t)ctas - 1024;
+            if (pad > smem) smem = pad;
+        }
+        cudaError_t e = cudaFuncSetAttribute(k_cont_faces,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+        k_cont_faces<<<grid, nb, smem, s>>>(D, M, u, hin, hW, hE, uhbt, O, dt);
     }
     return cudaGetLastError();
 }

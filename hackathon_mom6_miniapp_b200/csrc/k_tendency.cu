@@ -21,12 +21,15 @@
 
 namespace mom6b {
 
-template <int TX, int TY>
+// UNI selects the uniform-metric instantiation (metrics as scalars, Coriolis
+// per row); otherwise every metric is read from its 2-D array.  Each CTA
+// walks KC consecutive layers of its tile.
+template <int TX, int TY, bool UNI>
 __global__ void __launch_bounds__(TX * TY)
-k_tendency(Dims D, Metrics M, const double* __restrict__ uin,
+k_tendency(Dims D, Metrics M, UniMetrics U, const double* __restrict__ uin,
            const double* __restrict__ vin, const double* __restrict__ h,
            const double* ubase, const double* vbase, double* uout, double* vout,
-           double coef, double h_neglect, int k0)
+           double coef, double h_neglect, int k0, int KC)
 {
     constexpr int SX = TX + 2, SY = TY + 2;  // staged inputs: [i0-1, i0+TX] x [j0-1, j0+TY]
     constexpr int CX = TX + 1, CY = TY + 1;  // intermediates
@@ -36,11 +39,14 @@ k_tendency(Dims D, Metrics M, const double* __restrict__ uin,
     __shared__ double s_uh[CY][CX];                 // u-faces  [i0-1, i0+TX-1] x [j0, j0+TY]
     __shared__ double s_vh[CY][CX];                 // v-faces  [i0, i0+TX] x [j0-1, j0+TY-1]
 
-    const int k = k0 + (int)blockIdx.z;
     const int i0 = D.is + (int)blockIdx.x * TX;
     const int j0 = D.js + (int)blockIdx.y * TY;
     const int tid = (int)threadIdx.y * TX + (int)threadIdx.x;
+    const int kb = k0 + (int)blockIdx.z * KC;
+    const int ke = (kb + KC - 1 < D.nk) ? kb + KC - 1 : D.nk;
+  for (int k = kb; k <= ke; ++k) {
     const size_t koff = (size_t)(k - 1) * (size_t)D.plane;
+    if (k > kb) __syncthreads();  // the previous layer's tiles are consumed
 
     // ---- stage u, v, h --------------------------------------------------
     for (int p = tid; p < SX * SY; p += TX * TY) {
@@ -58,7 +64,8 @@ k_tendency(Dims D, Metrics M, const double* __restrict__ uin,
 #define SU(i, j) s_u[(j) - (j0 - 1)][(i) - (i0 - 1)]
 #define SV(i, j) s_v[(j) - (j0 - 1)][(i) - (i0 - 1)]
 #define SH(i, j) s_h[(j) - (j0 - 1)][(i) - (i0 - 1)]
-#define G2(a, i, j) MOM6B_A2(M.a, i, j, D)
+#define G2(a, i, j) (UNI ? U.a : MOM6B_A2(M.a, i, j, D))
+#define COR(i, j) (UNI ? U.cor_row[(j) - 1] : MOM6B_A2(M.CoriolisBu, i, j, D))
 
     // ---- intermediates ----------------------------------------------------
     for (int p = tid; p < CX * CY; p += TX * TY) {
@@ -76,7 +83,7 @@ k_tendency(Dims D, Metrics M, const double* __restrict__ uin,
                 double dvdx = (v1 * G2(dyCv, I + 1, J)) - (v0 * G2(dyCv, I, J));
                 double dudy = (u1 * G2(dxCu, I, J + 1)) - (u0 * G2(dxCu, I, J));
                 double rel = G2(mask2dBu, I, J) * (dvdx - dudy) * G2(IareaBu, I, J);
-                double absv = G2(CoriolisBu, I, J) + rel;
+                double absv = COR(I, J) + rel;
                 double aT00 = G2(areaT, I, J), aT10 = G2(areaT, I + 1, J),
                        aT01 = G2(areaT, I, J + 1), aT11 = G2(areaT, I + 1, J + 1);
                 double hAu0 = (J >= D.js) ? 0.5 * ((aT00 * h00) + (aT10 * h10)) : 0.0;
@@ -191,10 +198,12 @@ k_tendency(Dims D, Metrics M, const double* __restrict__ uin,
         size_t o = koff + (size_t)(J - 1) * D.n1 + (i - 1);
         vout[o] = vbase[o] + coef * (CAv + diffv);
     }
+  }  // layer loop
 #undef SU
 #undef SV
 #undef SH
 #undef G2
+#undef COR
 #undef Q
 #undef SXY
 #undef KE
@@ -203,24 +212,25 @@ k_tendency(Dims D, Metrics M, const double* __restrict__ uin,
 #undef VH
 }
 
-constexpr int kTendTX = 32, kTendTY = 8;
+constexpr int kTendTX = 32, kTendTY = 8, kTendKC = 5;
 
-// Host launcher: one CTA per (TX x TY) tile of the compute domain per layer.
-cudaError_t launch_tendency(const Dims& D, const Metrics& M, const double* uin,
-                            const double* vin, const double* h,
-                            const double* ubase, const double* vbase,
-                            double* uout, double* vout, double coef,
-                            double h_neglect, cudaStream_t s)
+// Host launcher: one CTA per (TX x TY) tile of the compute domain and chunk of
+// kTendKC layers.
+cudaError_t launch_tendency(const Dims& D, const Metrics& M, const UniMetrics& U,
+                            const double* uin, const double* vin, const double* h,
+                            const double* ubase, const double* vbase, double* uout,
+                            double* vout, double coef, double h_neglect, cudaStream_t s)
 {
     int nx = D.ie - D.is + 1, ny = D.je - D.js + 1;
     dim3 block(kTendTX, kTendTY, 1);
-    // gridDim.z is limited to 65535 layers per launch
-    for (int k0 = 1; k0 <= D.nk; k0 += 65535) {
-        int nz = D.nk - k0 + 1 < 65535 ? D.nk - k0 + 1 : 65535;
-        dim3 grid((nx + kTendTX - 1) / kTendTX, (ny + kTendTY - 1) / kTendTY, nz);
-        k_tendency<kTendTX, kTendTY><<<grid, block, 0, s>>>(
-            D, M, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, k0);
-    }
+    int nchunks = (D.nk + kTendKC - 1) / kTendKC;
+    dim3 grid((nx + kTendTX - 1) / kTendTX, (ny + kTendTY - 1) / kTendTY, nchunks);
+    if (U.valid)
+        k_tendency<kTendTX, kTendTY, true><<<grid, block, 0, s>>>(
+            D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, kTendKC);
+    else
+        k_tendency<kTendTX, kTendTY, false><<<grid, block, 0, s>>>(
+            D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, kTendKC);
     return cudaGetLastError();
 }
 

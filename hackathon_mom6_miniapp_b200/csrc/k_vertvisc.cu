@@ -8,8 +8,8 @@
 // and back substitution, and the bottom stress output.
 //
 // Three sweeps per column, all in the reference's order:
-//   1. bottom-up: h_harm and the running z_i; botfn(z_i(m)) is stored per
-//      interface in shared memory (the value the reference recomputes);
+//   1. bottom-up: h_harm and the running z_i; h_harm(k) and botfn(z_i(m))
+//      are kept per layer/interface (the values the reference recomputes);
 //   2. top-down: hvel, a(K) and the forward elimination; the eliminated
 //      velocity is written back in place, and c1(k) overwrites the botfn slot
 //      k, which is dead by then;
@@ -26,15 +26,21 @@ __device__ __forceinline__ double vv_botfn(double z2) {
     return 1.0 / (1.0 + 0.09 * z2 * z2 * z2 * z2 * z2 * z2);
 }
 
-// blockDim.x columns along i; blockIdx.y enumerates u rows then v rows.
-__global__ void __launch_bounds__(128)
+// One thread per column.  KMAX bounds nk at compile time so that the two
+// per-column scratch arrays live in local memory: the hardware interleaves
+// local memory across the threads of a warp, so slot m of 32 consecutive
+// columns is one contiguous 256-byte segment, cached in L1/L2.  The grid is
+// blockDim.x columns along i by one row: blockIdx.y enumerates u rows then
+// v rows.
+template <int KMAX>
+__global__ void __launch_bounds__(256)
 k_vertvisc(Dims D, Metrics M, double* __restrict__ u, double* __restrict__ v,
            const double* __restrict__ h, double dt, VVParams P,
            double* __restrict__ taux_bot, double* __restrict__ tauy_bot)
 {
-    extern __shared__ double s_slot[];  // [(nk + 2) * blockDim.x]
+    double slot[KMAX + 2];   // botfn(z_i(m)), then c1(m)
+    double hh[KMAX + 2];     // h_harm(k) from sweep 1, reused in sweep 2
     const int nz = D.nk;
-    const int nb = (int)blockDim.x;
     const int nrow_u = D.je - D.js + 1;
     bool is_u = (int)blockIdx.y < nrow_u;
     int i, j, di, dj;
@@ -60,31 +66,34 @@ k_vertvisc(Dims D, Metrics M, double* __restrict__ u, double* __restrict__ v,
     const double msk = MOM6B_A2(mask, i, j, D);
     if (!(msk > 0.0)) return;  // vert_visc_apply leaves masked columns alone
 
-#define SL(m) s_slot[(size_t)(m) * nb + threadIdx.x]
     const size_t col = (size_t)(j - 1) * D.n1 + (i - 1);
     const size_t nbr = (size_t)(j - 1 + dj) * D.n1 + (i - 1 + di);
+    const size_t plane = (size_t)D.plane;
     const double hn = P.h_neglect;
 
-    // ---- sweep 1: z_i bottom-up (vert_visc_coef :160-179) ----------------
+    // ---- sweep 1: h_harm and z_i bottom-up (vert_visc_coef :160-179) -----
     double z = 0.0;
-    SL(nz + 1) = vv_botfn(0.0);
-    for (int k = nz; k >= 2; --k) {
-        size_t o = (size_t)(k - 1) * D.plane;
+    slot[nz + 1] = vv_botfn(0.0);
+    for (int k = nz; k >= 1; --k) {
+        size_t o = (size_t)(k - 1) * plane;
         double h0 = h[o + col], h1 = h[o + nbr];
         double h_harm = 2.0 * h0 * h1 / (h0 + h1 + hn);
-        z = z + h_harm * P.I_Hbbl;
-        SL(k) = vv_botfn(z);
+        hh[k] = h_harm;
+        if (k >= 2) {
+            z = z + h_harm * P.I_Hbbl;
+            slot[k] = vv_botfn(z);
+        }
     }
 
     // hvel(k): harmonic mean, blended toward the arithmetic mean where the
     // flow opposes the thickness gradient (:162-177)
     auto hvel_of = [&](int k) -> double {
-        size_t o = (size_t)(k - 1) * D.plane;
+        size_t o = (size_t)(k - 1) * plane;
         double h0 = h[o + col], h1 = h[o + nbr];
-        double h_harm = 2.0 * h0 * h1 / (h0 + h1 + hn);
+        double h_harm = hh[k];
         double hv = h_harm;
         if (vel[o + col] * (h1 - h0) < 0.0) {
-            double bf = SL(k + 1);
+            double bf = slot[k + 1];
             double h_arith = 0.5 * (h1 + h0);
             hv = (1.0 - bf) * h_harm + bf * h_arith;
         }
@@ -97,7 +106,7 @@ k_vertvisc(Dims D, Metrics M, double* __restrict__ u, double* __restrict__ v,
             double topfn = 1.0 - z_top / P.Hmix;
             Kv_tot = Kv_tot + (P.Kv_ml - P.Kv) * topfn;
         }
-        Kv_tot = Kv_tot + P.Kv_extra_bbl * SL(K2);
+        Kv_tot = Kv_tot + P.Kv_extra_bbl * slot[K2];
         double h_shear = 0.5 * (hv_lo + hv_up + hn);
         return Kv_tot / h_shear;
     };
@@ -135,10 +144,10 @@ k_vertvisc(Dims D, Metrics M, double* __restrict__ u, double* __restrict__ v,
         } else {
             a_next = a_bot_num / (0.5 * hv_k + hn);
         }
-        size_t o = (size_t)(k - 1) * D.plane + col;
+        size_t o = (size_t)(k - 1) * plane + col;
         Rayk = ray_on[k - 1] ? Ray[o] : 0.0;
         double c1 = dt * a_k * b1;
-        SL(k) = c1;
+        slot[k] = c1;
         h_u = hv_k + hn;
         b_denom_1 = h_u + dt * (Rayk + a_k * d1);
         b1 = 1.0 / (b_denom_1 + dt * a_next);
@@ -151,8 +160,8 @@ k_vertvisc(Dims D, Metrics M, double* __restrict__ u, double* __restrict__ v,
     // ---- sweep 3: back substitution (:447-449) ----------------------------
     double u_below = u_prev;
     for (int k = nz - 1; k >= 1; --k) {
-        size_t o = (size_t)(k - 1) * D.plane + col;
-        double uk = vel[o] + SL(k + 1) * u_below;
+        size_t o = (size_t)(k - 1) * plane + col;
+        double uk = vel[o] + slot[k + 1] * u_below;
         vel[o] = uk;
         u_below = uk;
     }
@@ -160,29 +169,33 @@ k_vertvisc(Dims D, Metrics M, double* __restrict__ u, double* __restrict__ v,
     double tb = kRho0 * u_prev * a_bottom;
     for (int k = 1; k <= nz; ++k)
         if (ray_on[k - 1]) {
-            size_t o = (size_t)(k - 1) * D.plane + col;
+            size_t o = (size_t)(k - 1) * plane + col;
             tb = tb + kRho0 * Ray[o] * vel[o];
         }
     tbot[col] = tb;
-#undef SL
+}
+
+template <int KMAX>
+static cudaError_t launch_vv(const Dims& D, const Metrics& M, double* u, double* v,
+                             const double* h, double dt, const VVParams& P,
+                             double* taux_bot, double* tauy_bot, cudaStream_t s)
+{
+    const int nb = 128;
+    int ncol = D.ie - D.is + 2;  // u rows have one more column than v rows
+    int nrows = (D.je - D.js + 1) + (D.je - D.js + 2);
+    dim3 grid((ncol + nb - 1) / nb, nrows, 1);
+    k_vertvisc<KMAX><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P, taux_bot, tauy_bot);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_vertvisc(const Dims& D, const Metrics& M, double* u, double* v,
                             const double* h, double dt, const VVParams& P,
                             double* taux_bot, double* tauy_bot, cudaStream_t s)
 {
-    const int nb = 128;
-    int ncol = D.ie - D.is + 2;  // u rows have one more column than v rows
-    int nrows = (D.je - D.js + 1) + (D.je - D.js + 2);
-    dim3 grid((ncol + nb - 1) / nb, nrows, 1);
-    size_t smem = (size_t)(D.nk + 2) * nb * sizeof(double);
-    // the attribute caps the dynamic shared memory of every later launch, so
-    // it is set for each launch's own size
-    cudaError_t e = cudaFuncSetAttribute(k_vertvisc,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    k_vertvisc<<<grid, nb, smem, s>>>(D, M, u, v, h, dt, P, taux_bot, tauy_bot);
-    return cudaGetLastError();
+    if (D.nk <= 80) return launch_vv<80>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s);
+    if (D.nk <= 128) return launch_vv<128>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s);
+    if (D.nk <= 256) return launch_vv<256>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s);
+    return launch_vv<1024>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s);
 }
 
 } // namespace mom6b

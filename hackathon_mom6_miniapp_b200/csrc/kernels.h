@@ -5,6 +5,25 @@
 
 namespace mom6b {
 
+// Spatially uniform metrics as scalars.  init_ocean_grid builds every metric
+// array uniform (mom6_types.F90:193-228) except CoriolisBu, which varies with
+// j only; when the model detects this it passes the values here and the
+// kernels read them from the parameter bank instead of 2-D arrays.  The
+// arithmetic is unchanged: the same values enter the same operations.
+struct UniMetrics {
+    double IareaT, areaT, dxT, IdxT, dxCu, dyCu, dy_Cu, IdxCu, IdyCu, dxCv, dyCv,
+        IdxCv, IdyCv, IareaBu, IareaCu, IareaCv, mask2dT, mask2dBu, mask2dCu,
+        mask2dCv, Area_q, DX_dyT, DY_dxT, DX_dyBu, DY_dxBu, dx2h, dy2h, dx2q, dy2q,
+        red_xx, red_xy, Kh_xx, Kh_xy;
+    const double* cor_row;  // CoriolisBu(:, J) for J = 1..n2 (constant in i)
+    int valid;              // 1 when the grid qualifies
+    // barotropic metrics (barotropic_init): scalars, and f_4_u/f_4_v per row
+    double Datu, Datv, gtot_E, gtot_W, gtot_N, gtot_S, bt_rem_u, bt_rem_v;
+    const double* f4u_row;  // f_4_u(c, :, J) at [(J-1)*4 + c-1]
+    const double* f4v_row;
+    int valid_bt;
+};
+
 // vertical viscosity constants (vert_visc_init, mom6_vert_visc_serial.F90:60-112)
 struct VVParams {
     double Kv, Kv_ml, Kv_extra_bbl, Hmix, h_neglect, I_Hbbl;
@@ -33,10 +52,10 @@ struct BTParams {
     long long spin_budget;     // clock64 cycles a block may wait at one barrier
 };
 
-cudaError_t launch_tendency(const Dims& D, const Metrics& M, const double* uin,
-                            const double* vin, const double* h, const double* ubase,
-                            const double* vbase, double* uout, double* vout,
-                            double coef, double h_neglect, cudaStream_t s);
+cudaError_t launch_tendency(const Dims& D, const Metrics& M, const UniMetrics& U,
+                            const double* uin, const double* vin, const double* h,
+                            const double* ubase, const double* vbase, double* uout,
+                            double* vout, double coef, double h_neglect, cudaStream_t s);
 cudaError_t launch_vertvisc(const Dims& D, const Metrics& M, double* u, double* v,
                             const double* h, double dt, const VVParams& P,
                             double* taux_bot, double* tauy_bot, cudaStream_t s);
@@ -44,7 +63,8 @@ cudaError_t launch_continuity(const Dims& D, const Metrics& M, const double* u,
                               const double* hin, double* hW, double* hE,
                               const double* uhbt, const ContOut& O, double dt,
                               double h_min, cudaStream_t s);
-cudaError_t launch_btstep(const Dims& D, const Metrics& M, const BTWork& W,
+cudaError_t launch_btstep(const Dims& D, const Metrics& M, const UniMetrics& U,
+                          const BTWork& W,
                           const BTParams& P, const double* eta_in,
                           const double* ubt_in, const double* vbt_in, double* u_av,
                           double* v_av, double* eta_av, cudaStream_t s);

@@ -25,6 +25,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -63,6 +64,7 @@ struct mom6b_model {
     std::unique_ptr<HostGrid> grid;
     Dims D;
     Metrics M;
+    UniMetrics U{};
     std::vector<void*> allocs;
     // state
     double *u, *v, *hA, *hB, *h0, *up, *vp, *uh, *hW, *hE, *uhbt0;
@@ -75,6 +77,9 @@ struct mom6b_model {
     cudaStream_t s3d = nullptr, s2d = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int64_t launches = 0;
+    int64_t launches_per_step = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
     bool overlap_bt = false;
     bool timing = false;
     std::vector<TimedLaunch> pending;
@@ -97,6 +102,8 @@ static void free_all(mom6b_model* m)
     m->allocs.clear();
     for (auto& t : m->pending) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
     m->pending.clear();
+    if (m->graph_exec) cudaGraphExecDestroy(m->graph_exec);
+    if (m->graph) cudaGraphDestroy(m->graph);
     if (m->ev_fork) cudaEventDestroy(m->ev_fork);
     if (m->ev_join) cudaEventDestroy(m->ev_join);
     if (m->s3d) cudaStreamDestroy(m->s3d);
@@ -149,6 +156,97 @@ static int set_ray_flags(mom6b_model* m, const std::vector<double>& Ru,
     }
     CK(cudaMemcpy(m->ray_layer_u, fu.data(), g.nk, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(m->ray_layer_v, fv.data(), g.nk, cudaMemcpyHostToDevice));
+    return MOM6B_OK;
+}
+
+static bool IareaT_uniform(const HostGrid& g)
+{
+    for (const std::vector<double>* a : {&g.IareaT, &g.IdxCu, &g.IdyCv}) {
+        double v0 = (*a)[g.at(1, 1)];
+        for (int j = 1; j <= g.n2 - 1; ++j)
+            for (int i = 1; i <= g.n1 - 1; ++i)
+                if ((*a)[g.at(i, j)] != v0) return false;
+    }
+    return true;
+}
+
+// The uniform-metric kernels apply when every metric the step reads is one
+// value over the points the kernels touch ([1, n1-1] x [1, n2-1]) and
+// CoriolisBu depends on j only.
+static int detect_uniform(mom6b_model* m)
+{
+    const HostGrid& g = *m->grid;
+    UniMetrics& U = m->U;
+    U.valid = 0;
+    U.valid_bt = 0;
+    if (getenv("MOM6B_GENERAL_METRICS")) return MOM6B_OK;
+    bool ok = true;
+    auto uni = [&](const std::vector<double>& a, double* out) {
+        double v0 = a[g.at(1, 1)];
+        for (int j = 1; j <= g.n2 - 1 && ok; ++j)
+            for (int i = 1; i <= g.n1 - 1; ++i)
+                if (a[g.at(i, j)] != v0) { ok = false; break; }
+        *out = v0;
+    };
+    uni(g.IareaT, &U.IareaT); uni(g.areaT, &U.areaT); uni(g.dxT, &U.dxT);
+    uni(g.IdxT, &U.IdxT); uni(g.dxCu, &U.dxCu); uni(g.dyCu, &U.dyCu);
+    uni(g.dy_Cu, &U.dy_Cu); uni(g.IdxCu, &U.IdxCu); uni(g.IdyCu, &U.IdyCu);
+    uni(g.dxCv, &U.dxCv); uni(g.dyCv, &U.dyCv); uni(g.IdxCv, &U.IdxCv);
+    uni(g.IdyCv, &U.IdyCv); uni(g.IareaBu, &U.IareaBu); uni(g.IareaCu, &U.IareaCu);
+    uni(g.IareaCv, &U.IareaCv); uni(g.mask2dT, &U.mask2dT); uni(g.mask2dBu, &U.mask2dBu);
+    uni(g.mask2dCu, &U.mask2dCu); uni(g.mask2dCv, &U.mask2dCv); uni(g.Area_q, &U.Area_q);
+    uni(g.DX_dyT, &U.DX_dyT); uni(g.DY_dxT, &U.DY_dxT); uni(g.DX_dyBu, &U.DX_dyBu);
+    uni(g.DY_dxBu, &U.DY_dxBu); uni(g.dx2h, &U.dx2h); uni(g.dy2h, &U.dy2h);
+    uni(g.dx2q, &U.dx2q); uni(g.dy2q, &U.dy2q); uni(g.red_xx, &U.red_xx);
+    uni(g.red_xy, &U.red_xy); uni(g.Kh_xx, &U.Kh_xx); uni(g.Kh_xy, &U.Kh_xy);
+    std::vector<double> cor(g.n2);
+    for (int j = 1; j <= g.n2 && ok; ++j) {
+        cor[j - 1] = g.CoriolisBu[g.at(1, j)];
+        for (int i = 1; i <= g.n1; ++i)
+            if (g.CoriolisBu[g.at(i, j)] != cor[j - 1]) { ok = false; break; }
+    }
+    // barotropic metrics, checked separately
+    bool okb = true;
+    auto unib = [&](const std::vector<double>& a, double* out) {
+        double v0 = a[g.at(1, 1)];
+        for (int j = 1; j <= g.n2 - 1 && okb; ++j)
+            for (int i = 1; i <= g.n1 - 1; ++i)
+                if (a[g.at(i, j)] != v0) { okb = false; break; }
+        *out = v0;
+    };
+    unib(g.Datu, &U.Datu); unib(g.Datv, &U.Datv); unib(g.gtot_E, &U.gtot_E);
+    unib(g.gtot_W, &U.gtot_W); unib(g.gtot_N, &U.gtot_N); unib(g.gtot_S, &U.gtot_S);
+    unib(g.bt_rem_u, &U.bt_rem_u); unib(g.bt_rem_v, &U.bt_rem_v);
+    std::vector<double> f4u(4 * (size_t)g.n2), f4v(4 * (size_t)g.n2);
+    for (int j = 1; j <= g.n2 && okb; ++j)
+        for (int c = 0; c < 4 && okb; ++c) {
+            f4u[(j - 1) * 4 + c] = g.f_4_u[4 * g.at(1, j) + c];
+            f4v[(j - 1) * 4 + c] = g.f_4_v[4 * g.at(1, j) + c];
+            for (int i = 1; i <= g.n1; ++i)
+                if (g.f_4_u[4 * g.at(i, j) + c] != f4u[(j - 1) * 4 + c] ||
+                    g.f_4_v[4 * g.at(i, j) + c] != f4v[(j - 1) * 4 + c]) { okb = false; break; }
+        }
+    cudaError_t err = cudaSuccess;
+    if (ok) {
+        double* d = dalloc(m, g.n2, &err);
+        if (!d) return fail(MOM6B_ERR_NOMEM, "device allocation failed");
+        CK(cudaMemcpy(d, cor.data(), g.n2 * sizeof(double), cudaMemcpyHostToDevice));
+        U.cor_row = d;
+        U.valid = 1;
+    }
+    if (okb && IareaT_uniform(g)) {
+        double* du = dalloc(m, 4 * (size_t)g.n2, &err);
+        double* dv = dalloc(m, 4 * (size_t)g.n2, &err);
+        if (!du || !dv) return fail(MOM6B_ERR_NOMEM, "device allocation failed");
+        CK(cudaMemcpy(du, f4u.data(), f4u.size() * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(dv, f4v.data(), f4v.size() * sizeof(double), cudaMemcpyHostToDevice));
+        U.f4u_row = du;
+        U.f4v_row = dv;
+        U.IareaT = g.IareaT[g.at(1, 1)];
+        U.IdxCu = g.IdxCu[g.at(1, 1)];
+        U.IdyCv = g.IdyCv[g.at(1, 1)];
+        U.valid_bt = 1;
+    }
     return MOM6B_OK;
 }
 
@@ -255,6 +353,7 @@ extern "C" int mom6b_create(const mom6b_config* cfg, mom6b_model** out)
     if (err != cudaSuccess || !m->u || !W.vbt_av)
         return fail(MOM6B_ERR_NOMEM, std::string("device allocation failed: ") + cudaGetErrorString(err));
     m->M.taux = m->taux; m->M.tauy = m->tauy; m->M.Ray_u = m->Ray_u; m->M.Ray_v = m->Ray_v;
+    if (int rc = detect_uniform(m.get())) return rc;
     m->M.ray_layer_u = m->ray_layer_u; m->M.ray_layer_v = m->ray_layer_v;
 
     // initial state
@@ -355,7 +454,7 @@ static int enqueue_step(mom6b_model* m)
 
     // ---- predictor ----
     CK(timed(m, s, "tendency", [&] {
-        return launch_tendency(D, M, m->u, m->v, m->h0, m->u, m->v, m->up, m->vp, dt,
+        return launch_tendency(D, M, m->U, m->u, m->v, m->h0, m->u, m->v, m->up, m->vp, dt,
                                hv_neglect, s); }));
     CK(timed(m, s, "vertvisc", [&] {
         return launch_vertvisc(D, M, m->up, m->vp, m->h0, dt, VV, m->taux_bot,
@@ -370,7 +469,7 @@ static int enqueue_step(mom6b_model* m)
     }
     // ---- corrector ----
     CK(timed(m, s, "tendency", [&] {
-        return launch_tendency(D, M, m->up, m->vp, m->hB, m->u, m->v, m->u, m->v,
+        return launch_tendency(D, M, m->U, m->up, m->vp, m->hB, m->u, m->v, m->u, m->v,
                                0.5 * dt, hv_neglect, s); }));
     CK(timed(m, s, "vertvisc", [&] {
         return launch_vertvisc(D, M, m->u, m->v, m->hB, 0.5 * dt, VV, m->taux_bot,
@@ -396,7 +495,7 @@ static int enqueue_step(mom6b_model* m)
     P.extended = 0;
     P.spin_budget = 4000000000LL;
     CK(timed(m, s2, "btstep", [&] {
-        return launch_btstep(D, M, m->bt, P, m->eta, m->ubt, m->vbt, m->ubt_av,
+        return launch_btstep(D, M, m->U, m->bt, P, m->eta, m->ubt, m->vbt, m->ubt_av,
                              m->vbt_av, m->eta_av, s2); }));
     if (c.bc_fill) {
         CK(timed(m, s2, "halo_fill", [&] { return launch_halo_fill(D, m->eta_av, 1, 0, s2); }));
@@ -404,7 +503,7 @@ static int enqueue_step(mom6b_model* m)
         CK(timed(m, s2, "halo_fill", [&] { return launch_halo_fill(D, m->vbt_av, 1, 2, s2); }));
     }
     CK(timed(m, s2, "btstep", [&] {
-        return launch_btstep(D, M, m->bt, P, m->eta_av, m->ubt_av, m->vbt_av,
+        return launch_btstep(D, M, m->U, m->bt, P, m->eta_av, m->ubt_av, m->vbt_av,
                              m->ubt_av, m->vbt_av, m->eta, s2); }));
     if (c.bc_fill)
         CK(timed(m, s2, "halo_fill", [&] { return launch_halo_fill(D, m->eta, 1, 0, s2); }));
@@ -415,10 +514,44 @@ static int enqueue_step(mom6b_model* m)
     return MOM6B_OK;
 }
 
+// Capture one whole step (every kernel of both chains) into a CUDA graph.
+static int capture_step(mom6b_model* m)
+{
+    cudaStream_t s = m->s3d;
+    int64_t before = m->launches;
+    bool timing = m->timing;
+    m->timing = false;  // no event records inside the graph
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_step(m);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s, &g);
+    m->timing = timing;
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return fail(MOM6B_ERR_CUDA, std::string("stream capture: ") + cudaGetErrorString(e));
+    m->graph = g;
+    CK(cudaGraphInstantiate(&m->graph_exec, g, 0));
+    m->launches_per_step = m->launches - before;
+    m->launches = before;
+    return MOM6B_OK;
+}
+
 extern "C" int mom6b_step(mom6b_model* m, int nsteps)
 {
     if (!m || nsteps < 0) return fail(MOM6B_ERR_ARG, "bad argument");
     CK(cudaSetDevice(m->cfg.device));
+    if (m->cfg.use_graph && !m->timing) {
+        if (!m->graph_exec) {
+            if (int rc = capture_step(m)) return rc;
+        }
+        for (int n = 0; n < nsteps; ++n) {
+            CK(cudaGraphLaunch(m->graph_exec, m->s3d));
+            m->launches += m->launches_per_step;
+        }
+        return MOM6B_OK;
+    }
     for (int n = 0; n < nsteps; ++n) {
         int rc = enqueue_step(m);
         if (rc) return rc;

@@ -120,3 +120,30 @@ def test_step_host_roundtrip():
     o.step(3)
     for n, a in zip(("u", "v", "h", "eta"), (u, v, h, eta)):
         assert np.array_equal(a, o.get(n)), n
+
+
+@pytest.mark.gpu
+def test_graph_replay_matches_eager():
+    from hackathon_mom6_miniapp_b200 import Model
+    a = Model(36, 30, 8, 40, INIT_CFG, seed=3, use_graph=False)
+    b = Model(36, 30, 8, 40, INIT_CFG, seed=3, use_graph=True)
+    a.step(4)
+    b.step(4)
+    for n in STATE + EXTRA:
+        assert np.array_equal(a.get(n), b.get(n)), n
+    assert b.launch_count() == a.launch_count()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("untiled", [False, True])
+def test_barotropic_variants_bitwise(untiled, monkeypatch):
+    # the tiled (one barrier per substep) and the point-parallel persistent
+    # kernels give the oracle's btstep bit for bit
+    if untiled:
+        monkeypatch.setenv("MOM6B_BT_UNTILED", "1")
+    o, g = _pair(70, 50, 6, 40, INIT_CFG, seed=6)
+    o.step(2)
+    g.step(2)
+    for n in ["eta", "eta_av", "ubt_av", "vbt_av"]:
+        a, b = g.get(n), o.get(n)
+        assert np.array_equal(a, b), f"{n}: {describe(a, b)}"
