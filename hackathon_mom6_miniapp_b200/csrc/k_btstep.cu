@@ -23,6 +23,7 @@
 // kernel records kDevTimeout and every block returns.
 #include <cstdlib>
 
+#include "../../include/mom6b.h"
 #include "kernels.h"
 
 namespace mom6b {
@@ -459,59 +460,85 @@ k_btstep_tiled(Dims D, Metrics M, UniMetrics U, BTWork W, BTParams P, BTTiles T,
 
 static int g_bt_blocks = 0;
 
+static cudaError_t init_bt_blocks()
+{
+    if (g_bt_blocks != 0) return cudaSuccess;
+    int dev = 0, nsm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    g_bt_blocks = nsm;
+    return cudaSuccess;
+}
+
+static bool tiles_for(const Dims& D, BTTiles& T)
+{
+    int bw = D.ie - D.is + 2, bh = D.je - D.js + 2;
+    int nbx = 1, nby = 1;
+    while ((long long)(nbx + 1) * (nby + 1) <= g_bt_blocks) { ++nbx; ++nby; }
+    while ((long long)(nbx + 1) * nby <= g_bt_blocks && (bw + nbx) / (nbx + 1) >= 8) ++nbx;
+    T.nbx = nbx; T.nby = nby;
+    T.tw = (bw + nbx - 1) / nbx; T.th = (bh + nby - 1) / nby;
+    size_t smem = (size_t)6 * (T.tw + 3) * (T.th + 3) * sizeof(double);
+    return (long long)T.tw * T.th <= 1024LL * kBtTileR && smem <= 227 * 1024;
+}
+
+
+static cudaError_t launch_btstep_tiled(const Dims& D, const Metrics& M, const UniMetrics& U,
+                                       const BTWork& W, const BTParams& P, const BTTiles& T,
+                                       const double* eta_in, const double* ubt_in,
+                                       const double* vbt_in, double* u_av, double* v_av,
+                                       double* eta_av, cudaStream_t s)
+{
+    const int NT = 1024;
+    size_t smem = (size_t)6 * (T.tw + 3) * (T.th + 3) * sizeof(double);
+    const void* fn = U.valid_bt ? (const void*)k_btstep_tiled<NT, true>
+                                : (const void*)k_btstep_tiled<NT, false>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    Dims Dc = D; Metrics Mc = M; UniMetrics Uc = U; BTWork Wc = W; BTParams Pc = P;
+    BTTiles Tc = T;
+    void* args[] = {&Dc, &Mc, &Uc, &Wc, &Pc, &Tc, (void*)&eta_in, (void*)&ubt_in,
+                    (void*)&vbt_in, (void*)&u_av, (void*)&v_av, (void*)&eta_av};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(T.nbx * T.nby, 1, 1);
+    cfg.blockDim = dim3(NT, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelExC(&cfg, fn, args);
+}
+
 cudaError_t launch_btstep(const Dims& D, const Metrics& M, const UniMetrics& U,
-                          const BTWork& W,
-                          const BTParams& P, const double* eta_in,
+                          const BTWork& W, const BTParams& P, const double* eta_in,
                           const double* ubt_in, const double* vbt_in,
                           double* u_av, double* v_av, double* eta_av,
                           cudaStream_t s)
 {
     const size_t smem_fast = (size_t)PV_N * kBtMaxR * kBtThreads * sizeof(double);
-    if (g_bt_blocks == 0) {
-        int dev = 0, nsm = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        cudaError_t e = cudaFuncSetAttribute(k_btstep<true>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem_fast);
-        if (e != cudaSuccess) return e;
-        g_bt_blocks = nsm;
-    }
-    // tiled variant: the updated box split into at most one tile per SM
+    cudaError_t e0 = init_bt_blocks();
+    if (e0 != cudaSuccess) return e0;
     {
-        const int NT = 1024;
-        int bw = D.ie - D.is + 2, bh = D.je - D.js + 2;
-        int nbx = 1, nby = 1;
-        while ((long long)(nbx + 1) * (nby + 1) <= g_bt_blocks) { ++nbx; ++nby; }
-        while ((long long)(nbx + 1) * nby <= g_bt_blocks && (bw + nbx) / (nbx + 1) >= 8) ++nbx;
-        BTTiles T;
-        T.nbx = nbx; T.nby = nby;
-        T.tw = (bw + nbx - 1) / nbx; T.th = (bh + nby - 1) / nby;
-        size_t smem = (size_t)6 * (T.tw + 3) * (T.th + 3) * sizeof(double);
-        if ((long long)T.tw * T.th <= (long long)NT * kBtTileR && smem <= 227 * 1024 &&
-            !getenv("MOM6B_BT_UNTILED")) {
-            const void* fn = U.valid_bt ? (const void*)k_btstep_tiled<NT, true>
-                                        : (const void*)k_btstep_tiled<NT, false>;
-            cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)smem);
+        static bool fast_attr = false;
+        if (!fast_attr) {
+            cudaError_t e = cudaFuncSetAttribute(k_btstep<true>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem_fast);
             if (e != cudaSuccess) return e;
-            Dims Dc = D; Metrics Mc = M; UniMetrics Uc = U; BTWork Wc = W; BTParams Pc = P;
-            BTTiles Tc = T;
-            void* args[] = {&Dc, &Mc, &Uc, &Wc, &Pc, &Tc, (void*)&eta_in, (void*)&ubt_in,
-                            (void*)&vbt_in, (void*)&u_av, (void*)&v_av, (void*)&eta_av};
-            cudaLaunchConfig_t cfg = {};
-            cfg.gridDim = dim3(nbx * nby, 1, 1);
-            cfg.blockDim = dim3(NT, 1, 1);
-            cfg.dynamicSmemBytes = smem;
-            cfg.stream = s;
-            cudaLaunchAttribute attr[1];
-            attr[0].id = cudaLaunchAttributeCooperative;
-            attr[0].val.cooperative = 1;
-            cfg.attrs = attr;
-            cfg.numAttrs = 1;
-            return cudaLaunchKernelExC(&cfg, fn, args);
+            fast_attr = true;
         }
     }
+    // tiled variant: the updated box split into at most one tile per SM
+    BTTiles T;
+    if (tiles_for(D, T) && !getenv("MOM6B_BT_UNTILED"))
+        return launch_btstep_tiled(D, M, U, W, P, T, eta_in, ubt_in, vbt_in, u_av, v_av,
+                                   eta_av, s);
     const long long nbox = (long long)(D.ie - D.is + 3) * (D.je - D.js + 3);
     int blocks = g_bt_blocks;
     int need = (int)((nbox + kBtThreads - 1) / kBtThreads);
@@ -532,6 +559,44 @@ cudaError_t launch_btstep(const Dims& D, const Metrics& M, const UniMetrics& U,
     cfg.numAttrs = 1;
     return cudaLaunchKernelExC(&cfg, fast ? (const void*)k_btstep<true>
                                           : (const void*)k_btstep<false>, args);
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free barotropic entry point
+// ---------------------------------------------------------------------------
+// Some callers cannot allocate device memory at the point where they need
+// the barotropic loop: a Fortran host whose device arrays are owned by an
+// OpenMP-target or OpenACC runtime (map clauses; cudaMalloc from inside its
+// data regions would fragment or bypass that runtime's pool), and code that
+// must not allocate while a stream is being captured into a CUDA graph.
+// mom6b_btstep_noalloc therefore keeps every work array of the loop in the
+// file-scope array below, sized for grids of at most kNoAllocMaxPoints
+// points (n1 * n2), i.e. 6 x 589,824 doubles plus a 256-byte header, about
+// 28.3 MB per GPU that loads this library, held until the process exits.
+constexpr long long kNoAllocMaxPoints = 768LL * 768LL;
+constexpr long long kNoAllocHeader = 32;  // doubles: barrier words and status
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocHeader +
+                                                          6 * kNoAllocMaxPoints];
+
+// Device address of g_noalloc_scratch, looked up once per device with that
+// device current.  In host code the symbol is only a host-side stand-in;
+// kernels must be given the address returned by cudaGetSymbolAddress.
+static double* g_noalloc_ptr[64];
+
+static cudaError_t noalloc_scratch(double** out)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!g_noalloc_ptr[dev]) {
+        double* p = nullptr;
+        e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return cudaSuccess;
 }
 
 // ---------------------------------------------------------------------------
@@ -596,3 +661,71 @@ cudaError_t launch_halo_fill(const Dims& D, double* f, int nz, int kind, cudaStr
 }
 
 } // namespace mom6b
+
+// See mom6b.h.  Every call shares g_noalloc_scratch: calls that overlap on
+// the GPU (two streams, or two host threads) race on it.  The first call on a
+// device looks up the array's device address; make that first call before
+// any stream capture begins.
+extern "C" int mom6b_btstep_noalloc(
+    const double* eta_in, const double* ubt_in, const double* vbt_in, double* u_av,
+    double* v_av, double* eta_av, const double* Datu, const double* Datv,
+    const double* gtot_E, const double* gtot_W, const double* gtot_N,
+    const double* gtot_S, const double* f_4_u, const double* f_4_v,
+    const double* bt_rem_u, const double* bt_rem_v, const double* IareaT,
+    const double* IdxCu, const double* IdyCv, int n1, int n2, int is, int ie, int js,
+    int je, int nstep, double dtbt, double bebt, double dgeo_de, int first_direction,
+    int extended_ranges, void* stream)
+{
+    using namespace mom6b;
+    if (!eta_in || !ubt_in || !vbt_in || !u_av || !v_av || !eta_av || !Datu || !Datv ||
+        !gtot_E || !gtot_W || !gtot_N || !gtot_S || !f_4_u || !f_4_v || !bt_rem_u ||
+        !bt_rem_v || !IareaT || !IdxCu || !IdyCv)
+        return MOM6B_NOALLOC_ERR_ARG;
+    if (n1 < 4 || n2 < 4 || nstep < 1 || is < 2 || js < 2 || ie > n1 - 1 || je > n2 - 1 ||
+        ie - is < 2 || je - js < 2)
+        return MOM6B_NOALLOC_ERR_ARG;
+    if ((long long)n1 * (long long)n2 > kNoAllocMaxPoints)
+        return MOM6B_NOALLOC_ERR_TOO_LARGE;
+    double* base = nullptr;
+    if (noalloc_scratch(&base) != cudaSuccess) return MOM6B_NOALLOC_ERR_CUDA;
+    cudaStream_t s = (cudaStream_t)stream;
+    // barrier words and status must start at zero; the field buffers are
+    // fully written by the kernel's initial copy
+    if (cudaMemsetAsync(base, 0, kNoAllocHeader * sizeof(double), s) != cudaSuccess)
+        return MOM6B_NOALLOC_ERR_CUDA;
+    const size_t np = (size_t)n1 * (size_t)n2;
+    double* f = base + kNoAllocHeader;
+    BTWork W{};
+    W.eta = f; W.ubt = f + np; W.vbt = f + 2 * np;
+    W.eta_pred = f + 3 * np; W.ubt_prev = f + 4 * np; W.vbt_prev = f + 5 * np;
+    W.uhbt = nullptr; W.vhbt = nullptr; W.PFu = nullptr; W.PFv = nullptr;
+    W.ubt_av = nullptr; W.vbt_av = nullptr;
+    W.bar_count = (unsigned int*)base;
+    W.bar_gen = (unsigned int*)base + 4;
+    W.status = (int*)base + 8;
+    Dims D{};
+    D.n1 = n1; D.n2 = n2; D.nk = 1;
+    D.is = is; D.ie = ie; D.js = js; D.je = je;
+    D.isd = 1; D.ied = n1; D.jsd = 1; D.jed = n2;
+    D.plane = (long long)np;
+    Metrics M{};
+    M.Datu = Datu; M.Datv = Datv; M.gtot_E = gtot_E; M.gtot_W = gtot_W;
+    M.gtot_N = gtot_N; M.gtot_S = gtot_S; M.f_4_u = f_4_u; M.f_4_v = f_4_v;
+    M.bt_rem_u = bt_rem_u; M.bt_rem_v = bt_rem_v; M.IareaT = IareaT;
+    M.IdxCu = IdxCu; M.IdyCv = IdyCv;
+    UniMetrics U{};
+    BTParams P{};
+    P.dtbt = dtbt; P.dgeo_de = dgeo_de;
+    P.trans_wt1 = 1.0 + bebt; P.trans_wt2 = -bebt;
+    P.inv_nstep = 1.0 / (double)nstep;
+    P.nstep = nstep; P.first_direction = first_direction;
+    P.extended = extended_ranges ? 1 : 0;
+    P.spin_budget = 4000000000LL;
+    if (init_bt_blocks() != cudaSuccess) return MOM6B_NOALLOC_ERR_CUDA;
+    BTTiles T;
+    if (!tiles_for(D, T)) return MOM6B_NOALLOC_ERR_TOO_LARGE;
+    if (launch_btstep_tiled(D, M, U, W, P, T, eta_in, ubt_in, vbt_in, u_av, v_av, eta_av,
+                            s) != cudaSuccess)
+        return MOM6B_NOALLOC_ERR_CUDA;
+    return MOM6B_NOALLOC_OK;
+}

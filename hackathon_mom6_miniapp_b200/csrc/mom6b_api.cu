@@ -677,6 +677,21 @@ extern "C" int mom6b_field_device_ptr(mom6b_model* m, int f, void** dptr)
     return MOM6B_OK;
 }
 
+extern "C" int mom6b_metric_device_ptr(mom6b_model* m, const char* name, void** dptr)
+{
+    if (!m || !name || !dptr) return fail(MOM6B_ERR_ARG, "null argument");
+    const Metrics& M = m->M;
+    const std::map<std::string, const double*> t = {
+        {"IareaT", M.IareaT}, {"IdxCu", M.IdxCu}, {"IdyCv", M.IdyCv}, {"Datu", M.Datu},
+        {"Datv", M.Datv}, {"gtot_E", M.gtot_E}, {"gtot_W", M.gtot_W},
+        {"gtot_N", M.gtot_N}, {"gtot_S", M.gtot_S}, {"f_4_u", M.f_4_u},
+        {"f_4_v", M.f_4_v}, {"bt_rem_u", M.bt_rem_u}, {"bt_rem_v", M.bt_rem_v}};
+    auto it = t.find(name);
+    if (it == t.end()) return fail(MOM6B_ERR_ARG, std::string("unknown metric ") + name);
+    *dptr = (void*)it->second;
+    return MOM6B_OK;
+}
+
 extern "C" int mom6b_dims(const mom6b_model* m, int* o)
 {
     if (!m || !o) return fail(MOM6B_ERR_ARG, "null argument");

@@ -126,6 +126,47 @@ int mom6b_kernel_timing(mom6b_model *m, int enable);
 int mom6b_kernel_time_ms(mom6b_model *m, const char *kernel, double *avg_ms,
                          int64_t *launches);
 
+/* ---- allocation-free barotropic loop ------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory where they run the barotropic solver -- a Fortran host whose device
+ * arrays belong to an OpenMP-target or OpenACC runtime, or code that must not
+ * allocate while a stream is being captured -- this entry point runs all
+ * nstep substeps of btstep (mom6_barotropic_serial.F90:178-304; extended
+ * uhbt/vhbt ranges when extended_ranges != 0, as btstep_do_step and the CUDA C
+ * kernels use) and allocates nothing.  The caller passes every input, metric
+ * and output as device arrays in the reference layout (n1, n2; f_4_u and
+ * f_4_v are (4, n1, n2)); the outputs may alias the inputs.  The loop's work
+ * arrays live in one static device array of the library sized for
+ * n1 * n2 <= 589,824 points (768 x 768, about 28.3 MB per GPU, held until the
+ * process exits); larger grids return MOM6B_NOALLOC_ERR_TOO_LARGE.  All calls
+ * share that array, so calls that overlap on the GPU race.  The first call on
+ * each device looks up the array's device address: make it before any stream
+ * capture.  The work is enqueued on `stream` (a cudaStream_t); the call does
+ * not synchronize. */
+enum {
+    MOM6B_NOALLOC_OK = 0,
+    MOM6B_NOALLOC_ERR_ARG = 1,       /* null pointer or inconsistent bounds */
+    MOM6B_NOALLOC_ERR_TOO_LARGE = 2, /* n1 * n2 above the static capacity */
+    MOM6B_NOALLOC_ERR_CUDA = 3       /* a CUDA runtime call failed */
+};
+int mom6b_btstep_noalloc(const double *eta_in, const double *ubt_in,
+                         const double *vbt_in, double *u_av, double *v_av,
+                         double *eta_av, const double *Datu, const double *Datv,
+                         const double *gtot_E, const double *gtot_W,
+                         const double *gtot_N, const double *gtot_S,
+                         const double *f_4_u, const double *f_4_v,
+                         const double *bt_rem_u, const double *bt_rem_v,
+                         const double *IareaT, const double *IdxCu,
+                         const double *IdyCv, int n1, int n2, int is, int ie,
+                         int js, int je, int nstep, double dtbt, double bebt,
+                         double dgeo_de, int first_direction,
+                         int extended_ranges, void *stream);
+
+/* Device address of one of the model's 2-D metric arrays by name ("IareaT",
+ * "IdxCu", "IdyCv", "Datu", "Datv", "gtot_E", "gtot_W", "gtot_N", "gtot_S",
+ * "f_4_u", "f_4_v", "bt_rem_u", "bt_rem_v"). */
+int mom6b_metric_device_ptr(mom6b_model *m, const char *name, void **dptr);
+
 const char *mom6b_last_error(void);
 const char *mom6b_version(void);
 
