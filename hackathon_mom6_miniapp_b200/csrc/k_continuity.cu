@@ -49,17 +49,12 @@ __device__ __forceinline__ double ppm_slope(const double* __restrict__ hrow,
     return copysign(1.0, s) * dmin(fabs(s), 2.0 * dmin(dMx, dMn));
 }
 
-__global__ void __launch_bounds__(128)
-k_ppm_edges(Dims D, Metrics M, const double* __restrict__ hin,
-            double* __restrict__ hW, double* __restrict__ hE, double h_min)
+// PPM_reconstruction_x + PPM_limit_pos for cell i of one row (hrow/mrow point
+// at element i = 1 of the row).
+__device__ __forceinline__ void ppm_cell(const double* __restrict__ hrow,
+                                         const double* __restrict__ mrow, int i,
+                                         double h_min, double& hL, double& hR)
 {
-    const int i = D.is - 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
-    const int j = D.js + (int)blockIdx.y;
-    const int k = 1 + (int)blockIdx.z;
-    if (i > D.ie + 1) return;
-    const size_t rowoff = (size_t)(k - 1) * D.plane + (size_t)(j - 1) * D.n1;
-    const double* hrow = hin + rowoff;                    // hrow[i-1] = h(i)
-    const double* mrow = M.mask2dT + (size_t)(j - 1) * D.n1;
     const double oneSixth = 1.0 / 6.0;
     double slm = ppm_slope(hrow, mrow, i - 1);
     double slc = ppm_slope(hrow, mrow, i);
@@ -67,8 +62,8 @@ k_ppm_edges(Dims D, Metrics M, const double* __restrict__ hin,
     double hc = hrow[i - 1];
     double h_im1 = mrow[i - 2] * hrow[i - 2] + (1.0 - mrow[i - 2]) * hc;
     double h_ip1 = mrow[i] * hrow[i] + (1.0 - mrow[i]) * hc;
-    double hL = 0.5 * (h_im1 + hc) + oneSixth * (slm - slc);
-    double hR = 0.5 * (h_ip1 + hc) + oneSixth * (slc - slp);
+    hL = 0.5 * (h_im1 + hc) + oneSixth * (slm - slc);
+    hR = 0.5 * (h_ip1 + hc) + oneSixth * (slc - slp);
     // PPM_limit_pos with real(4) curv, dh, scale (:1266-1268)
     float curv = (float)(3.0 * ((hL + hR) - 2.0 * hc));
     if ((double)curv > 0.0) {
@@ -89,6 +84,19 @@ k_ppm_edges(Dims D, Metrics M, const double* __restrict__ hin,
             }
         }
     }
+}
+
+__global__ void __launch_bounds__(128)
+k_ppm_edges(Dims D, Metrics M, const double* __restrict__ hin,
+            double* __restrict__ hW, double* __restrict__ hE, double h_min)
+{
+    const int i = D.is - 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int j = D.js + (int)blockIdx.y;
+    const int k = 1 + (int)blockIdx.z;
+    if (i > D.ie + 1) return;
+    const size_t rowoff = (size_t)(k - 1) * D.plane + (size_t)(j - 1) * D.n1;
+    double hL, hR;
+    ppm_cell(hin + rowoff, M.mask2dT + (size_t)(j - 1) * D.n1, i, h_min, hL, hR);
     hW[rowoff + (i - 1)] = hL;
     hE[rowoff + (i - 1)] = hR;
 }
@@ -96,44 +104,102 @@ k_ppm_edges(Dims D, Metrics M, const double* __restrict__ hin,
 // ---------------------------------------------------------------------------
 // face column work
 // ---------------------------------------------------------------------------
+// EI is the index type of the edge arrays: size_t for the global scratch
+// pair, int for the shared-memory copies (shared memory is always indexed
+// with 32-bit offsets here).
+template <typename EI>
 struct FaceCol {
     const double* u;     // u(I, j, 1), layer stride = plane
     const double* hc;    // h(I, j, 1)   (cell i = I)
-    const double* hWc;   // h_W(I, j, 1)
-    const double* hEc;   // h_E(I, j, 1)
+    const double* hWc;   // h_W of cell I at layer 1, layer stride = estride
+    const double* hEc;   // h_E of cell I at layer 1
     size_t plane;
+    EI estride;          // layer stride of hWc/hEc (plane, or the smem row length)
     double dy;           // dy_Cu(I, j) (times por_face_areaU = 1)
     double IdxT_i, IdxT_ip1;
 };
+
+// The inputs of one layer of one face: u(I) and the cell values of the two
+// cells either side (h_W, h_E, h of i = I and of i + 1).
+struct LayerVals {
+    double u, hWi, hEi, hi, hWp, hEp, hp;
+};
+
+// Layers whose inputs one prefetch brings into registers (CH).  Each pass
+// over a face column is a chain of dependent sums, so the loads of CH layers
+// are issued together and their latency is paid once per chunk.
+constexpr int kContChunk = 4;
+
+template <typename EI>
+__device__ __forceinline__ LayerVals load_layer(const FaceCol<EI>& F, int k)
+{
+    const size_t o = (size_t)(k - 1) * F.plane;
+    const EI oe = (EI)(k - 1) * F.estride;
+    LayerVals L;
+    L.u = F.u[o];
+    L.hWi = F.hWc[oe]; L.hEi = F.hEc[oe]; L.hi = F.hc[o];
+    L.hWp = F.hWc[oe + 1]; L.hEp = F.hEc[oe + 1]; L.hp = F.hc[o + 1];
+    return L;
+}
+
+// Visit layers 1..nz in order, fn(k, LayerVals).
+template <int CH, typename EI, typename Fn>
+__device__ __forceinline__ void for_layers(const FaceCol<EI>& F, int nz, Fn&& fn)
+{
+    for (int kt = 1; kt <= nz; kt += CH) {
+        LayerVals L[CH];
+#pragma unroll
+        for (int c = 0; c < CH; ++c)
+            if (kt + c <= nz) L[c] = load_layer(F, kt + c);
+#pragma unroll
+        for (int c = 0; c < CH; ++c)
+            if (kt + c <= nz) fn(kt + c, L[c]);
+    }
+}
+
+// Visit u(I, k) for k = 1..nz in order, fn(k, u).
+template <int CH, typename EI, typename Fn>
+__device__ __forceinline__ void for_u(const FaceCol<EI>& F, int nz, Fn&& fn)
+{
+    constexpr int CU = 2 * CH;
+    for (int kt = 1; kt <= nz; kt += CU) {
+        double uk[CU];
+#pragma unroll
+        for (int c = 0; c < CU; ++c)
+            if (kt + c <= nz) uk[c] = F.u[(size_t)(kt + c - 1) * F.plane];
+#pragma unroll
+        for (int c = 0; c < CU; ++c)
+            if (kt + c <= nz) fn(kt + c, uk[c]);
+    }
+}
 
 // zonal_flux_layer (:554-583) for one layer; returns uh and sets h_marg.
 // The two upwind cases are one operation sequence on (base, other, h) =
 // (h_E(i), h_W(i), h(i)) for u > 0 or (h_W(i+1), h_E(i+1), h(i+1)) for u < 0,
 // and CFL = (|u| dt) Idx equals the reference's -(u dt Idx) for u < 0 exactly,
 // so the evaluation is written without a divergent branch.
-__device__ __forceinline__ double flux_eval(const FaceCol& F, int k, double uI,
-                                            double dt, double& h_marg)
+template <typename EI>
+__device__ __forceinline__ double flux_eval(const FaceCol<EI>& F, const LayerVals& L,
+                                            double uI, double dt, double& h_marg)
 {
-    const size_t o = (size_t)(k - 1) * F.plane;
-    const double hWi = F.hWc[o], hEi = F.hEc[o], hi = F.hc[o];
-    const double hWp = F.hWc[o + 1], hEp = F.hEc[o + 1], hp = F.hc[o + 1];
     const bool pos = uI > 0.0;
-    const double base = pos ? hEi : hWp;
-    const double oth = pos ? hWi : hEp;
-    const double hc = pos ? hi : hp;
+    const double base = pos ? L.hEi : L.hWp;
+    const double oth = pos ? L.hWi : L.hEp;
+    const double hc = pos ? L.hi : L.hp;
     const double Idx = pos ? F.IdxT_i : F.IdxT_ip1;
     const double CFL = fabs(uI) * dt * Idx;
     const double curv_3 = (oth + base) - 2.0 * hc;
     const double uh = F.dy * uI * (base + CFL * (0.5 * (oth - base) + curv_3 * (CFL - 1.5)));
     const double hm = base + CFL * ((oth - base) + 3.0 * curv_3 * (CFL - 1.0));
     const bool zero = !(uI > 0.0) && !(uI < 0.0);
-    h_marg = zero ? 0.5 * (hWp + hEi) : hm;
+    h_marg = zero ? 0.5 * (L.hWp + L.hEi) : hm;
     return zero ? 0.0 : uh;
 }
 
 // zonal_flux_adjust for one face (:813-903).  When uh_out is given the flux of
 // every evaluated iteration is stored (the present(uh_3d) call).
-__device__ double flux_adjust_face(const FaceCol& F, int nz, double dt,
+template <int CH, typename EI>
+__device__ double flux_adjust_face(const FaceCol<EI>& F, int nz, double dt,
                                    double uhbt, double uh_tot_0,
                                    double duhdu_tot_0, double du_max_CFL,
                                    double du_min_CFL, double tol_eta_dt_fac,
@@ -184,16 +250,14 @@ __device__ double flux_adjust_face(const FaceCol& F, int nz, double dt,
         const bool update = itt < max_itts;
         if (update || uh_out) {
             double e = -uhbt, dt_sum = 0.0;
-            for (int k = 1; k <= nz; ++k) {
-                const size_t o = (size_t)(k - 1) * F.plane;
-                double u_new = F.u[o] + du;
+            for_layers<CH>(F, nz, [&](int k, const LayerVals& L) {
                 double hm;
-                double uhk = flux_eval(F, k, u_new, dt, hm);
+                double uhk = flux_eval(F, L, L.u + du, dt, hm);
                 double duhdu = F.dy * hm;
                 if (uh_out) uh_out[(size_t)(k - 1) * uh_stride] = uhk;
                 e = e + uhk;
                 dt_sum = dt_sum + duhdu;
-            }
+            });
             if (update) {
                 uh_err = e;
                 duhdu_tot = dt_sum;
@@ -205,146 +269,250 @@ __device__ double flux_adjust_face(const FaceCol& F, int nz, double dt,
 }
 
 
+// The work of one face (I, j) after its column views are set up: initial
+// fluxes, CFL limits, zonal_flux_adjust, du_cor and, for the owner,
+// set_zonal_BT_cont and zonal_flux_thickness.  uh/ust receive the face's
+// transports (the output array, or the CTA's overlap column).
+template <int CH, typename EI>
+__device__ __forceinline__ void face_work(const Dims& D, const Metrics& M, FaceCol<EI>& F,
+                                          int I, int j, size_t f0, double* uh, size_t ust,
+                                          bool owner, const double* uhbt2d, const ContOut& O,
+                                          double dt)
+{
+    const int nz = D.nk;
+    // initial fluxes and their column sums (:305-355)
+    double uh_tot_0 = 0.0, duhdu_tot_0 = 0.0;
+    for_layers<CH>(F, nz, [&](int k, const LayerVals& L) {
+        double hm;
+        double uhk = flux_eval(F, L, L.u, dt, hm);
+        uh[(size_t)(k - 1) * ust] = uhk;
+        duhdu_tot_0 = duhdu_tot_0 + F.dy * hm;
+        uh_tot_0 = uh_tot_0 + uhk;
+    });
+    // CFL limits (:335-433), vol_CFL = aggress_adjust = .false.
+    const double CFL_dt = 0.5 / dt;
+    const double dx_W = MOM6B_A2(M.dxT, I, j, D), dx_E = MOM6B_A2(M.dxT, I + 1, j, D);
+    const double mCu = MOM6B_A2(M.mask2dCu, I, j, D);
+    double du_max_CFL = 2.0 * (CFL_dt * dx_W);
+    double du_min_CFL = -(2.0 * (CFL_dt * dx_E));
+    for_u<CH>(F, nz, [&](int, double uk) {
+        if (du_max_CFL > dx_W * CFL_dt - uk * mCu) du_max_CFL = dx_W * CFL_dt - uk;
+        if (du_min_CFL < -(dx_E * CFL_dt) - uk * mCu) du_min_CFL = -(dx_E * CFL_dt + uk);
+    });
+    du_max_CFL = dmax(du_max_CFL, 0.0);
+    du_min_CFL = dmin(du_min_CFL, 0.0);
+
+    const double fac = dt * dmin(MOM6B_A2(M.IareaT, I, j, D), MOM6B_A2(M.IareaT, I + 1, j, D));
+    const double uhbt = MOM6B_A2(uhbt2d, I, j, D);
+    double du = flux_adjust_face<CH>(F, nz, dt, uhbt, uh_tot_0, duhdu_tot_0,
+                                 du_max_CFL, du_min_CFL, fac, uh, ust);
+    if (!owner) return;
+    O.du_cor[f0] = du;
+
+    // set_zonal_BT_cont (:991-1121)
+    double du0 = (uhbt == 0.0)
+                     ? du
+                     : flux_adjust_face<CH>(F, nz, dt, 0.0, uh_tot_0, duhdu_tot_0,
+                                        du_max_CFL, du_min_CFL, fac, (double*)nullptr, 0);
+    const double Idt = 1.0 / dt;
+    const double du_CFL = (F32(1e-6) * Idt) * MOM6B_A2(M.dxCu, I, j, D);
+    double duR = dmin(0.0, du0 - du_CFL);
+    double duL = dmax(0.0, du0 + du_CFL);
+    // visc_rem_lim = max(1, 0.1 * 1) = 1 > 0 on every layer
+    for_u<CH>(F, nz, [&](int, double uk) {
+        if (uk + duR > -du_CFL) duR = -(uk + du_CFL);
+        if (uk + duL < du_CFL) duL = -(uk - du_CFL);
+    });
+    double FAmt_0 = 0.0, FAmt_L = 0.0, FAmt_R = 0.0, uhtot_L = 0.0, uhtot_R = 0.0;
+    double* h_u = O.h_u + f0;
+    const bool same = (du0 == du);
+    for_layers<CH>(F, nz, [&](int k, const LayerVals& L) {
+        const double uk = L.u;
+        double hm0, hmL, hmR;
+        flux_eval(F, L, uk + du0, dt, hm0);
+        double uhL = flux_eval(F, L, uk + duL, dt, hmL);
+        double uhR = flux_eval(F, L, uk + duR, dt, hmR);
+        FAmt_0 = FAmt_0 + F.dy * hm0;
+        FAmt_L = FAmt_L + F.dy * hmL;
+        FAmt_R = FAmt_R + F.dy * hmR;
+        uhtot_L = uhtot_L + uhL;
+        uhtot_R = uhtot_R + uhR;
+        // zonal_flux_thickness with u_cor = u + du (marginal faces)
+        double hmc = hm0;
+        if (!same) flux_eval(F, L, uk + du, dt, hmc);
+        h_u[(size_t)(k - 1) * F.plane] = hmc;
+    });
+    double FA_0 = FAmt_0, FA_avg = FAmt_0;
+    if ((duL - du0) != 0.0) FA_avg = uhtot_L / (duL - du0);
+    if (FA_avg > dmax(FA_0, FAmt_L)) FA_avg = dmax(FA_0, FAmt_L);
+    else if (FA_avg < dmin(FA_0, FAmt_L)) FA_0 = FA_avg;
+    O.FA_u_W0[f0] = FA_0;
+    O.FA_u_WW[f0] = FAmt_L;
+    O.uBT_WW[f0] = (fabs(FA_0 - FAmt_L) <= F32(1e-12) * FA_0)
+                       ? 0.0
+                       : (1.5 * (duL - du0)) * ((FAmt_L - FA_avg) / (FAmt_L - FA_0));
+    FA_0 = FAmt_0; FA_avg = FAmt_0;
+    if ((duR - du0) != 0.0) FA_avg = uhtot_R / (duR - du0);
+    if (FA_avg > dmax(FA_0, FAmt_R)) FA_avg = dmax(FA_0, FAmt_R);
+    else if (FA_avg < dmin(FA_0, FAmt_R)) FA_0 = FA_avg;
+    O.FA_u_E0[f0] = FA_0;
+    O.FA_u_EE[f0] = FAmt_R;
+    O.uBT_EE[f0] = (fabs(FAmt_R - FA_0) <= F32(1e-12) * FA_0)
+                       ? 0.0
+                       : (1.5 * (duR - du0)) * ((FAmt_R - FA_avg) / (FAmt_R - FA_0));
+}
+
 // blockDim.x faces per CTA along I; consecutive CTAs overlap by one face.
 // Face ownership: thread 0 recomputes the last face of the CTA to its left
 // (it owns face is-1 only in the first CTA) and keeps that face's transport
-// column in shared memory, so no CTA ever reads a global transport another
-// CTA may still be iterating on.
+// column in the CTA's own slot of uh_ovl ([CTA][nk]), so no CTA ever reads a
+// global transport another CTA may still be iterating on.
+__device__ __forceinline__ double* overlap_column(double* uh_ovl, int nz)
+{
+    return uh_ovl + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * (size_t)nz;
+}
+
+// continuity_zonal_convergence (:148-176) for cell i = I, whose faces I-1 and
+// I both belong to this CTA.
+__device__ __forceinline__ void cell_convergence(const Dims& D, const Metrics& M, int i, int j,
+                                                 const double* __restrict__ hin,
+                                                 const double* uh_left_col, const ContOut& O,
+                                                 double dt)
+{
+    if (threadIdx.x >= 1 && i >= D.is && i <= D.ie) {
+        const size_t c0 = (size_t)(j - 1) * D.n1 + (i - 1);
+        const double fac = dt * MOM6B_A2(M.IareaT, i, j, D);
+        const bool from_ovl = threadIdx.x == 1 && blockIdx.x > 0;
+        for (int k = 1; k <= D.nk; ++k) {
+            const size_t o = (size_t)(k - 1) * D.plane + c0;
+            double uh_left = from_ovl ? uh_left_col[k - 1] : O.uh[o - 1];
+            O.h[o] = dmax(hin[o] - fac * (O.uh[o] - uh_left), 0.0);
+        }
+    }
+}
+
+template <int CH>
 __global__ void __launch_bounds__(128)
 k_cont_faces(Dims D, Metrics M, const double* __restrict__ u,
              const double* __restrict__ hin, const double* __restrict__ hW,
              const double* __restrict__ hE, const double* __restrict__ uhbt2d,
-             ContOut O, double dt)
+             ContOut O, double* uh_ovl, double dt)
 {
-    extern __shared__ double s_uh_left[];  // [nk], transports of thread 0's face
     const int nz = D.nk;
     const int step = (int)blockDim.x - 1;
     const int I = D.is - 1 + (int)blockIdx.x * step + (int)threadIdx.x;
     const int j = D.js + (int)blockIdx.y;
     const bool face_ok = I <= D.ie;
     const bool owner = threadIdx.x >= 1 || blockIdx.x == 0;
+    double* ovl = overlap_column(uh_ovl, nz);
     if (face_ok) {
         const size_t f0 = (size_t)(j - 1) * D.n1 + (I - 1);
-        FaceCol F;
+        FaceCol<size_t> F;
         F.u = u + f0; F.hc = hin + f0; F.hWc = hW + f0; F.hEc = hE + f0;
         F.plane = (size_t)D.plane;
+        F.estride = (size_t)D.plane;
         F.dy = MOM6B_A2(M.dy_Cu, I, j, D);
         F.IdxT_i = MOM6B_A2(M.IdxT, I, j, D);
         F.IdxT_ip1 = MOM6B_A2(M.IdxT, I + 1, j, D);
-        double* uh = (threadIdx.x == 0) ? s_uh_left : O.uh + f0;
-        const size_t ust = (threadIdx.x == 0) ? 1 : F.plane;
-
-        // initial fluxes and their column sums (:305-355)
-        double uh_tot_0 = 0.0, duhdu_tot_0 = 0.0;
-        for (int k = 1; k <= nz; ++k) {
-            const size_t o = (size_t)(k - 1) * F.plane;
-            double hm;
-            double uhk = flux_eval(F, k, F.u[o], dt, hm);
-            uh[(size_t)(k - 1) * ust] = uhk;
-            duhdu_tot_0 = duhdu_tot_0 + F.dy * hm;
-            uh_tot_0 = uh_tot_0 + uhk;
-        }
-        // CFL limits (:335-433), vol_CFL = aggress_adjust = .false.
-        const double CFL_dt = 0.5 / dt;
-        const double dx_W = MOM6B_A2(M.dxT, I, j, D), dx_E = MOM6B_A2(M.dxT, I + 1, j, D);
-        const double mCu = MOM6B_A2(M.mask2dCu, I, j, D);
-        double du_max_CFL = 2.0 * (CFL_dt * dx_W);
-        double du_min_CFL = -(2.0 * (CFL_dt * dx_E));
-        for (int k = 1; k <= nz; ++k) {
-            double uk = F.u[(size_t)(k - 1) * F.plane];
-            if (du_max_CFL > dx_W * CFL_dt - uk * mCu) du_max_CFL = dx_W * CFL_dt - uk;
-            if (du_min_CFL < -(dx_E * CFL_dt) - uk * mCu) du_min_CFL = -(dx_E * CFL_dt + uk);
-        }
-        du_max_CFL = dmax(du_max_CFL, 0.0);
-        du_min_CFL = dmin(du_min_CFL, 0.0);
-
-        const double fac = dt * dmin(MOM6B_A2(M.IareaT, I, j, D), MOM6B_A2(M.IareaT, I + 1, j, D));
-        const double uhbt = MOM6B_A2(uhbt2d, I, j, D);
-        double du = flux_adjust_face(F, nz, dt, uhbt, uh_tot_0, duhdu_tot_0,
-                                     du_max_CFL, du_min_CFL, fac, uh, ust);
-        if (owner) {
-            if (threadIdx.x == 0)  // face is-1 of the first CTA: publish its column
-                for (int k = 1; k <= nz; ++k)
-                    O.uh[f0 + (size_t)(k - 1) * F.plane] = s_uh_left[k - 1];
-            O.du_cor[f0] = du;
-
-            // set_zonal_BT_cont (:991-1121)
-            double du0 = (uhbt == 0.0)
-                             ? du
-                             : flux_adjust_face(F, nz, dt, 0.0, uh_tot_0, duhdu_tot_0,
-                                                du_max_CFL, du_min_CFL, fac, nullptr, 0);
-            const double Idt = 1.0 / dt;
-            const double du_CFL = (F32(1e-6) * Idt) * MOM6B_A2(M.dxCu, I, j, D);
-            double duR = dmin(0.0, du0 - du_CFL);
-            double duL = dmax(0.0, du0 + du_CFL);
-            // visc_rem_lim = max(1, 0.1 * 1) = 1 > 0 on every layer
-            for (int k = 1; k <= nz; ++k) {
-                double uk = F.u[(size_t)(k - 1) * F.plane];
-                if (uk + duR > -du_CFL) duR = -(uk + du_CFL);
-                if (uk + duL < du_CFL) duL = -(uk - du_CFL);
-            }
-            double FAmt_0 = 0.0, FAmt_L = 0.0, FAmt_R = 0.0, uhtot_L = 0.0, uhtot_R = 0.0;
-            double* h_u = O.h_u + f0;
-            const bool same = (du0 == du);
-            for (int k = 1; k <= nz; ++k) {
-                const size_t o = (size_t)(k - 1) * F.plane;
-                double uk = F.u[o];
-                double hm0, hmL, hmR;
-                flux_eval(F, k, uk + du0, dt, hm0);
-                double uhL = flux_eval(F, k, uk + duL, dt, hmL);
-                double uhR = flux_eval(F, k, uk + duR, dt, hmR);
-                FAmt_0 = FAmt_0 + F.dy * hm0;
-                FAmt_L = FAmt_L + F.dy * hmL;
-                FAmt_R = FAmt_R + F.dy * hmR;
-                uhtot_L = uhtot_L + uhL;
-                uhtot_R = uhtot_R + uhR;
-                // zonal_flux_thickness with u_cor = u + du (marginal faces)
-                double hmc = hm0;
-                if (!same) flux_eval(F, k, uk + du, dt, hmc);
-                h_u[o] = hmc;
-            }
-            double FA_0 = FAmt_0, FA_avg = FAmt_0;
-            if ((duL - du0) != 0.0) FA_avg = uhtot_L / (duL - du0);
-            if (FA_avg > dmax(FA_0, FAmt_L)) FA_avg = dmax(FA_0, FAmt_L);
-            else if (FA_avg < dmin(FA_0, FAmt_L)) FA_0 = FA_avg;
-            O.FA_u_W0[f0] = FA_0;
-            O.FA_u_WW[f0] = FAmt_L;
-            O.uBT_WW[f0] = (fabs(FA_0 - FAmt_L) <= F32(1e-12) * FA_0)
-                               ? 0.0
-                               : (1.5 * (duL - du0)) * ((FAmt_L - FA_avg) / (FAmt_L - FA_0));
-            FA_0 = FAmt_0; FA_avg = FAmt_0;
-            if ((duR - du0) != 0.0) FA_avg = uhtot_R / (duR - du0);
-            if (FA_avg > dmax(FA_0, FAmt_R)) FA_avg = dmax(FA_0, FAmt_R);
-            else if (FA_avg < dmin(FA_0, FAmt_R)) FA_0 = FA_avg;
-            O.FA_u_E0[f0] = FA_0;
-            O.FA_u_EE[f0] = FAmt_R;
-            O.uBT_EE[f0] = (fabs(FAmt_R - FA_0) <= F32(1e-12) * FA_0)
-                               ? 0.0
-                               : (1.5 * (duR - du0)) * ((FAmt_R - FA_avg) / (FAmt_R - FA_0));
-        }
+        const bool to_ovl = !owner;
+        double* uh = to_ovl ? ovl : O.uh + f0;
+        const size_t ust = to_ovl ? 1 : F.plane;
+        face_work<CH>(D, M, F, I, j, f0, uh, ust, owner, uhbt2d, O, dt);
     }
     __syncthreads();  // the CTA's transport columns are complete and visible
-    // continuity_zonal_convergence for cell i = I (faces I-1 and I in this CTA)
-    const int i = I;
-    if (threadIdx.x >= 1 && i >= D.is && i <= D.ie) {
-        const size_t c0 = (size_t)(j - 1) * D.n1 + (i - 1);
-        const double fac = dt * MOM6B_A2(M.IareaT, i, j, D);
-        for (int k = 1; k <= nz; ++k) {
-            const size_t o = (size_t)(k - 1) * D.plane + c0;
-            double uh_left = (threadIdx.x == 1) ? s_uh_left[k - 1] : O.uh[o - 1];
-            O.h[o] = dmax(hin[o] - fac * (O.uh[o] - uh_left), 0.0);
+    cell_convergence(D, M, I, j, hin, ovl, O, dt);
+}
+
+// Fused variant: the PPM edges of the CTA's cells are computed straight into
+// shared memory (no h_W/h_E scratch in HBM) and the Newton passes read them
+// there; u and h come from L1/L2.  Warp w of the CTA owns faces
+// F0 + 32w .. F0 + 32w + 31 and the 33 cells F0 + 32w .. F0 + 32w + 32.
+constexpr int kFusedWarps = 4;
+constexpr int kFusedCells = 33;   // cells per warp
+
+template <int CH>
+__global__ void __launch_bounds__(32 * kFusedWarps)
+k_cont_fused(Dims D, Metrics M, const double* __restrict__ u,
+             const double* __restrict__ hin, const double* __restrict__ uhbt2d,
+             ContOut O, double* uh_ovl, double dt, double h_min)
+{
+    extern __shared__ double s_edges[];                   // [warps][2][nz][CW]
+    const int nz = D.nk;
+    const int CW = kFusedCells;
+    const int lane = (int)threadIdx.x & 31, warp = (int)threadIdx.x >> 5;
+    const int wbase = warp * 2 * nz * CW;                 // this warp's h_W block
+    const int ebase = wbase + nz * CW;                    // this warp's h_E block
+    const int step = (int)blockDim.x - 1;
+    const int F0 = D.is - 1 + (int)blockIdx.x * step;
+    const int I = F0 + (int)threadIdx.x;
+    const int j = D.js + (int)blockIdx.y;
+    const int c0 = F0 + 32 * warp;                        // first cell of the warp
+    const double* mrow = M.mask2dT + (size_t)(j - 1) * D.n1;
+
+    // PPM edges of cells c0 .. c0+32 (within [is-1, ie+1]) for every layer
+    for (int k = 1; k <= nz; ++k) {
+        const double* hrow = hin + (size_t)(k - 1) * D.plane + (size_t)(j - 1) * D.n1;
+        for (int c = lane; c < CW; c += 32) {
+            int i = c0 + c;
+            double hL = 0.0, hR = 0.0;
+            if (i >= D.is - 1 && i <= D.ie + 1) ppm_cell(hrow, mrow, i, h_min, hL, hR);
+            s_edges[wbase + (k - 1) * CW + c] = hL;
+            s_edges[ebase + (k - 1) * CW + c] = hR;
         }
     }
+    __syncwarp();
+
+    const bool face_ok = I <= D.ie;
+    const bool owner = threadIdx.x >= 1 || blockIdx.x == 0;
+    double* ovl = overlap_column(uh_ovl, nz);
+    if (face_ok) {
+        const size_t f0 = (size_t)(j - 1) * D.n1 + (I - 1);
+        FaceCol<int> F;
+        F.u = u + f0; F.hc = hin + f0;
+        F.hWc = s_edges + wbase + lane; F.hEc = s_edges + ebase + lane;
+        F.plane = (size_t)D.plane;
+        F.estride = CW;
+        F.dy = MOM6B_A2(M.dy_Cu, I, j, D);
+        F.IdxT_i = MOM6B_A2(M.IdxT, I, j, D);
+        F.IdxT_ip1 = MOM6B_A2(M.IdxT, I + 1, j, D);
+        const bool to_ovl = !owner;
+        double* uh = to_ovl ? ovl : O.uh + f0;
+        const size_t ust = to_ovl ? 1 : F.plane;
+        face_work<CH>(D, M, F, I, j, f0, uh, ust, owner, uhbt2d, O, dt);
+    }
+    __syncthreads();  // the CTA's transport columns are complete and visible
+    cell_convergence(D, M, I, j, hin, ovl, O, dt);
 }
 
 // CTAs per SM for k_cont_faces; 0 lets the hardware fill the SM.
 constexpr int kContCtasPerSM = 0;
 
+size_t continuity_overlap_doubles(const Dims& D)
+{
+    // at most one CTA per 127 faces along each row (both kernels use 128 threads)
+    int nfaces = D.ie - (D.is - 1) + 1;
+    size_t nbx = (size_t)(nfaces - 1 + 126) / 127;
+    return nbx * (size_t)(D.je - D.js + 1) * (size_t)D.nk;
+}
+
 cudaError_t launch_continuity(const Dims& D, const Metrics& M, const double* u,
                               const double* hin, double* hW, double* hE,
-                              const double* uhbt, const ContOut& O, double dt,
-                              double h_min, cudaStream_t s)
+                              const double* uhbt, const ContOut& O, double* uh_ovl,
+                              double dt, double h_min, cudaStream_t s)
 {
+    {
+        const int nb = 32 * kFusedWarps, step = nb - 1;
+        size_t smem = (size_t)kFusedWarps * 2 * D.nk * kFusedCells * sizeof(double);
+        if (smem <= 227 * 1024 && getenv("MOM6B_CONT_FUSED")) {
+            cudaError_t e = cudaFuncSetAttribute(
+                k_cont_fused<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            int nfaces = D.ie - (D.is - 1) + 1;
+            dim3 grid((nfaces - 1 + step - 1) / step, D.je - D.js + 1, 1);
+            k_cont_fused<1><<<grid, nb, smem, s>>>(D, M, u, hin, uhbt, O, uh_ovl, dt, h_min);
+            return cudaGetLastError();
+        }
+    }
     {
         int n = (D.ie + 1) - (D.is - 1) + 1;
         dim3 grid((n + 127) / 128, D.je - D.js + 1, D.nk);
@@ -357,21 +525,23 @@ cudaError_t launch_continuity(const Dims& D, const Metrics& M, const double* u,
         const int nb = 128, step = nb - 1;
         int nfaces = D.ie - (D.is - 1) + 1;
         dim3 grid((nfaces - 1 + step - 1) / step, D.je - D.js + 1, 1);
-        size_t smem = (size_t)D.nk * sizeof(double);
+        size_t smem = 0;
         static int ctas = -1;
         if (ctas < 0) {
             const char* e = getenv("MOM6B_CONT_CTAS_PER_SM");
             ctas = e ? atoi(e) : kContCtasPerSM;
         }
-        if (ctas > 0) {
-            size_t pad = (size_t)(227 * 1024) / (size_t)ctas - 1024;
-            if (pad > smem) smem = pad;
+        if (ctas > 0) smem = (size_t)(227 * 1024) / (size_t)ctas - 1024;
+        static int chunk = -1;
+        if (chunk < 0) {
+            const char* e = getenv("MOM6B_CONT_CHUNK");
+            chunk = e ? atoi(e) : kContChunk;
         }
-        cudaError_t e = cudaFuncSetAttribute(k_cont_faces,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+        auto kern = chunk == 1 ? k_cont_faces<1> : chunk == 4 ? k_cont_faces<4> : k_cont_faces<2>;
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e != cudaSuccess) return e;
-        k_cont_faces<<<grid, nb, smem, s>>>(D, M, u, hin, hW, hE, uhbt, O, dt);
+        kern<<<grid, nb, smem, s>>>(D, M, u, hin, hW, hE, uhbt, O, uh_ovl, dt);
     }
     return cudaGetLastError();
 }

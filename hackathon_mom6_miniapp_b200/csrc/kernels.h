@@ -59,10 +59,13 @@ cudaError_t launch_tendency(const Dims& D, const Metrics& M, const UniMetrics& U
 cudaError_t launch_vertvisc(const Dims& D, const Metrics& M, double* u, double* v,
                             const double* h, double dt, const VVParams& P,
                             double* taux_bot, double* tauy_bot, cudaStream_t s);
+// uh_ovl: scratch of continuity_overlap_doubles(D) doubles holding the
+// recomputed overlap face column of every CTA.
+size_t continuity_overlap_doubles(const Dims& D);
 cudaError_t launch_continuity(const Dims& D, const Metrics& M, const double* u,
                               const double* hin, double* hW, double* hE,
-                              const double* uhbt, const ContOut& O, double dt,
-                              double h_min, cudaStream_t s);
+                              const double* uhbt, const ContOut& O, double* uh_ovl,
+                              double dt, double h_min, cudaStream_t s);
 cudaError_t launch_btstep(const Dims& D, const Metrics& M, const UniMetrics& U,
                           const BTWork& W,
                           const BTParams& P, const double* eta_in,

@@ -67,7 +67,7 @@ struct mom6b_model {
     UniMetrics U{};
     std::vector<void*> allocs;
     // state
-    double *u, *v, *hA, *hB, *h0, *up, *vp, *uh, *hW, *hE, *uhbt0;
+    double *u, *v, *hA, *hB, *h0, *up, *vp, *uh, *hW, *hE, *uhbt0, *uh_ovl;
     double *eta, *ubt, *vbt, *ubt_av, *vbt_av, *eta_av;
     double *h_u, *FA_u_W0, *FA_u_WW, *FA_u_E0, *FA_u_EE, *uBT_WW, *uBT_EE, *du_cor;
     double *taux_bot, *tauy_bot;
@@ -331,6 +331,7 @@ extern "C" int mom6b_create(const mom6b_config* cfg, mom6b_model** out)
     m->u = A3(); m->v = A3(); m->hA = A3(); m->hB = A3(); m->h0 = A3();
     m->up = A3(); m->vp = A3(); m->uh = A3(); m->hW = A3(); m->hE = A3();
     m->h_u = A3();
+    m->uh_ovl = dalloc(m.get(), continuity_overlap_doubles(m->D), &err);
     m->uhbt0 = A2();
     m->eta = A2(); m->ubt = A2(); m->vbt = A2(); m->ubt_av = A2(); m->vbt_av = A2();
     m->eta_av = A2();
@@ -460,8 +461,8 @@ static int enqueue_step(mom6b_model* m)
         return launch_vertvisc(D, M, m->up, m->vp, m->h0, dt, VV, m->taux_bot,
                                m->tauy_bot, s); }));
     CK(timed(m, s, "continuity", [&] {
-        return launch_continuity(D, M, m->up, m->h0, m->hW, m->hE, m->uhbt0, OB, dt,
-                                 h_min, s); }));
+        return launch_continuity(D, M, m->up, m->h0, m->hW, m->hE, m->uhbt0, OB,
+                                 m->uh_ovl, dt, h_min, s); }));
     if (c.bc_fill) {
         CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->hB, g.nk, 0, s); }));
         CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->up, g.nk, 1, s); }));
@@ -476,7 +477,7 @@ static int enqueue_step(mom6b_model* m)
                                m->tauy_bot, s); }));
     CK(timed(m, s, "continuity", [&] {
         return launch_continuity(D, M, m->u, m->hB, m->hW, m->hE, m->uhbt0, OA,
-                                 0.5 * dt, h_min, s); }));
+                                 m->uh_ovl, 0.5 * dt, h_min, s); }));
     if (c.bc_fill) {
         CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->hA, g.nk, 0, s); }));
         CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->u, g.nk, 1, s); }));
