@@ -16,14 +16,15 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmom6b.so")
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_FLAGS = ARCH + ["-O3", "-lineinfo", "--fmad=false", "-std=c++17",
+CU_FLAGS = ARCH + ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "--extended-lambda",
                    "-Xcompiler", "-fPIC,-ffp-contract=off", "-Xptxas", "-O3"]
 CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", "-Wall"]
 
 CU_SOURCES = ["k_tendency.cu", "k_vertvisc.cu", "k_continuity.cu", "k_btstep.cu",
-              "mom6b_api.cu"]
+              "mom6b_api.cu", "abi_helpers.cu", "abi_barotropic.cu", "abi_hor_visc.cu",
+              "abi_vert_visc.cu", "abi_coriolis.cu", "abi_continuity.cu"]
 CXX_SOURCES = ["host_init.cpp"]
-HEADERS = ["common.cuh", "kernels.h", "host_init.h"]
+HEADERS = ["common.cuh", "kernels.h", "host_init.h", "abi_common.cuh"]
 
 
 def _newer(target, deps):
