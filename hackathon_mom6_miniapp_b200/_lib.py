@@ -77,6 +77,13 @@ def library():
     L.mom6b_reset_launch_count.restype = None
     L.mom6b_kernel_timing.argtypes = [vp, ctypes.c_int]
     L.mom6b_kernel_time_ms.argtypes = [vp, ctypes.c_char_p, P(d), P(i64)]
+    L.mom6b_cudac_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_double, ctypes.c_char_p, P(vp)]
+    L.mom6b_cudac_step.argtypes = [vp, ctypes.c_int]
+    L.mom6b_cudac_field_size.argtypes = [vp, ctypes.c_int]
+    L.mom6b_cudac_field_size.restype = ctypes.c_size_t
+    L.mom6b_cudac_get_field.argtypes = [vp, ctypes.c_int, P(d), ctypes.c_size_t]
+    L.mom6b_cudac_destroy.argtypes = [vp]
     L.mom6b_last_error.restype = ctypes.c_char_p
     L.mom6b_version.restype = ctypes.c_char_p
     _LIB = L
@@ -196,3 +203,44 @@ class Model:
         _check(library().mom6b_kernel_time_ms(self._m, name.encode(), ctypes.byref(ms),
                                               ctypes.byref(n)))
         return ms.value, n.value
+
+
+class CudaCDriver:
+    """The reference's CUDA C host side (rk2_cuda_c_driver + the src/cuda_c
+    Fortran wrappers) restated in C++ and driven through the launch_* ABI.
+
+    kernel_lib=None runs this library's own entry points; a path runs the
+    entry points of another shared object with the same symbols."""
+
+    def __init__(self, ni=180, nj=180, nk=75, bt_nsteps=30, dt=300.0, kernel_lib=None):
+        L = library()
+        h = ctypes.c_void_p()
+        lib = kernel_lib.encode() if kernel_lib else None
+        _check(L.mom6b_cudac_create(ni, nj, nk, bt_nsteps, dt, lib, ctypes.byref(h)))
+        self._h = h
+        self.n1, self.n2, self.nk = ni + 2, nj + 2, nk
+
+    def close(self):
+        if getattr(self, "_h", None):
+            library().mom6b_cudac_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, n=1):
+        _check(library().mom6b_cudac_step(self._h, n))
+
+    def get(self, name):
+        L = library()
+        fid = FID[name]
+        n = L.mom6b_cudac_field_size(self._h, fid)
+        if n == 0:
+            raise KeyError(name)
+        a = np.empty(n, dtype=np.float64)
+        _check(L.mom6b_cudac_get_field(self._h, fid, _dptr(a), n))
+        shp = (self.n1, self.n2, self.nk) if n == self.n1 * self.n2 * self.nk else (self.n1, self.n2)
+        return a.reshape(shp, order="F")

@@ -22,7 +22,8 @@ CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", "-Wall"]
 
 CU_SOURCES = ["k_tendency.cu", "k_vertvisc.cu", "k_continuity.cu", "k_btstep.cu",
               "mom6b_api.cu", "abi_helpers.cu", "abi_barotropic.cu", "abi_hor_visc.cu",
-              "abi_vert_visc.cu", "abi_coriolis.cu", "abi_continuity.cu"]
+              "abi_vert_visc.cu", "abi_coriolis.cu", "abi_continuity.cu",
+              "cudac_driver.cu"]
 CXX_SOURCES = ["host_init.cpp"]
 HEADERS = ["common.cuh", "kernels.h", "host_init.h", "abi_common.cuh"]
 
@@ -62,7 +63,7 @@ def build(verbose=False, force=False):
                 print(" ".join(cmd))
             _run(cmd)
     if force or _newer(LIB, objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-ldl"]
         if verbose:
             print(" ".join(cmd))
         _run(cmd)

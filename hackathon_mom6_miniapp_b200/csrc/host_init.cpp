@@ -143,7 +143,7 @@ void HostGrid::build()
     // forcing: wind stress and bottom-layer Rayleigh drag
     for (int j = jsd; j <= jed; ++j)
         for (int i = isd; i <= ied; ++i) {
-            taux[at(i, j)] = 0.1 * std::sin((double)(j - 1) / (double)nj * 3.14159);
+            taux[at(i, j)] = 0.1 * std::sin((double)(j - 1) / (double)nj * pi_init);
             tauy[at(i, j)] = 0.0;
         }
 }
@@ -162,21 +162,21 @@ void HostGrid::initial_state(std::vector<double>& u, std::vector<double>& v,
                 for (int i = isd; i <= ied; ++i) {
                     size_t p = at(i, j, k);
                     h0[p] = total_depth / (double)nk +
-                            10.0 * std::sin((double)(i - 1) / (double)ni * 3.14159) *
-                                std::cos((double)(j - 1) / (double)nj * 3.14159) *
+                            10.0 * std::sin((double)(i - 1) / (double)ni * pi_init) *
+                                std::cos((double)(j - 1) / (double)nj * pi_init) *
                                 std::exp(-(double)k / 20.0);
-                    u[p] = 0.1 * std::sin((double)(j - 1) / (double)nj * 3.14159 * 2.0) *
+                    u[p] = 0.1 * std::sin((double)(j - 1) / (double)nj * pi_init * 2.0) *
                            std::exp(-(double)k / 30.0);
-                    v[p] = 0.1 * std::cos((double)(i - 1) / (double)ni * 3.14159 * 2.0) *
+                    v[p] = 0.1 * std::cos((double)(i - 1) / (double)ni * pi_init * 2.0) *
                            std::exp(-(double)k / 30.0);
                 }
         for (int j = jsd; j <= jed; ++j)
             for (int i = isd; i <= ied; ++i) {
                 size_t p = at(i, j);
-                eta[p] = 0.5 * std::sin((double)(i - 1) / (double)ni * 3.14159 * 2.0) *
-                         std::cos((double)(j - 1) / (double)nj * 3.14159 * 2.0);
-                ubt[p] = 0.05 * std::sin((double)(j - 1) / (double)nj * 3.14159);
-                vbt[p] = 0.05 * std::cos((double)(i - 1) / (double)ni * 3.14159);
+                eta[p] = 0.5 * std::sin((double)(i - 1) / (double)ni * pi_init * 2.0) *
+                         std::cos((double)(j - 1) / (double)nj * pi_init * 2.0);
+                ubt[p] = 0.05 * std::sin((double)(j - 1) / (double)nj * pi_init);
+                vbt[p] = 0.05 * std::cos((double)(i - 1) / (double)ni * pi_init);
             }
     } else {
         const double hbar = 4000.0 / (double)nk;

@@ -19,6 +19,9 @@ struct HostGrid {
     int isd, ied, jsd, jed, is, ie, js, je;
     size_t plane;
     double dx = 0.0;
+    // pi in the analytic initial state and wind stress: 3.14159 in
+    // rk2_serial_driver.F90:477-530, PI (mom6_types.F90:83) in rk2_cuda_c_driver
+    double pi_init = 3.14159;
 
     std::vector<double> IareaT, areaT, dxT, dyT, IdxT, IdyT, dxCu, dyCu, dy_Cu,
         IdxCu, IdyCu, dxCv, dyCv, IdxCv, IdyCv, IareaBu, areaBu, CoriolisBu,

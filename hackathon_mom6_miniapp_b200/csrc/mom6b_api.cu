@@ -47,6 +47,8 @@ static int fail(int code, const std::string& msg)
     return code;
 }
 
+int mom6b_internal_fail(int code, const std::string& msg) { return fail(code, msg); }
+
 #define CK(call)                                                                     \
     do {                                                                             \
         cudaError_t e_ = (call);                                                     \

@@ -167,6 +167,28 @@ int mom6b_btstep_noalloc(const double *eta_in, const double *ubt_in,
  * "f_4_u", "f_4_v", "bt_rem_u", "bt_rem_v"). */
 int mom6b_metric_device_ptr(mom6b_model *m, const char *name, void **dptr);
 
+/* ---- the reference's CUDA C host side, mirrored ---------------------------
+ * No counterpart as a C function in the reference: rk2_cuda_c_driver.F90 and
+ * the Fortran wrappers of src/cuda_c (*_cuda_c.F90) are restated in C++ so
+ * that a whole split RK2 iteration can be driven through the launch_* ABI of
+ * mom6_cuda_c.h.  The state is the driver's analytic initial state
+ * (rk2_cuda_c_driver.F90:663-700) on init_ocean_grid's grid; each call of
+ * mom6b_cudac_step runs rk2_cuda_c_driver.F90:263-481 once per step, with the
+ * wrappers' launch order, arguments and per-phase device synchronisation.
+ * kernel_lib NULL drives this library's own launch_* entry points (the
+ * drop-in path); otherwise the path of a shared object exporting the same
+ * symbols is opened and its entry points are driven instead.  Fields are read
+ * with the MOM6B_F_* ids (u, v, h, h0, uh, vh, up, vp, eta, ubt, vbt, ubt_av,
+ * vbt_av, eta_av, the BT_cont arrays, taux_bot = the last bottom stress,
+ * taux, tauy). */
+typedef struct mom6b_cudac mom6b_cudac;
+int mom6b_cudac_create(int ni, int nj, int nk, int bt_nsteps, double dt,
+                       const char *kernel_lib, mom6b_cudac **out);
+int mom6b_cudac_step(mom6b_cudac *m, int nsteps);
+size_t mom6b_cudac_field_size(const mom6b_cudac *m, int field);
+int mom6b_cudac_get_field(mom6b_cudac *m, int field, double *host, size_t count);
+int mom6b_cudac_destroy(mom6b_cudac *m);
+
 const char *mom6b_last_error(void);
 const char *mom6b_version(void);
 
