@@ -180,6 +180,20 @@ def run_reference(args, world, rank, local, dist):
     print(json.dumps(line), flush=True)
 
 
+def measured_traffic():
+    """DRAM bytes per launch of each phase at the bench size, from the committed
+    ncu summary (profiles/traffic_720x720x75.txt); {} when absent."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles",
+                        "traffic_720x720x75.txt")
+    out = {}
+    if os.path.exists(path):
+        for line in open(path):
+            parts = line.split()
+            if len(parts) == 2 and not line.startswith("#"):
+                out[parts[0]] = float(parts[1])
+    return out
+
+
 def run_ours(args, world, rank, local, dist):
     import numpy as np
     import torch
@@ -222,10 +236,17 @@ def run_ours(args, world, rank, local, dist):
     steps_t = max(2, min(args.steps, 5))
     per_step_ms = {k: v[0] * v[1] / steps_t for k, v in kt.items()}
     dom = max(per_step_ms, key=per_step_ms.get)
-    # compulsory bytes per launch of each fused kernel (3-D arrays)
-    kbytes = {"tendency": 5 * N3 + 10 * N2, "vertvisc": 5 * N3 + 4 * N2,
-              "continuity": 10 * N3 + 7 * N2, "btstep": 6 * N2,
-              "halo_fill": 0}
+    # algorithmic bytes per launch: the reference phases each fused kernel
+    # covers (per step 78 N3 + 30 N2 = STEP_BYTES, split evenly over the
+    # predictor and corrector launches):
+    #   tendency   = h reset (2, predictor only) + transports 5 + hor_visc 5
+    #                + CorAdCalc 7 + velocity update 8 -> 26 N3 on average
+    #   vertvisc   = 7 N3 + 2 N2
+    #   continuity = 5 N3 + 7 N2 (+ the corrector's htmp copy 2 N3) -> 6 N3 + 7 N2
+    #   btstep     = 6 N2
+    kbytes = {"tendency": 26 * N3, "vertvisc": 7 * N3 + 2 * N2,
+              "continuity": 6 * N3 + 7 * N2, "btstep": 6 * N2, "halo_fill": 0}
+    assert 2 * sum(kbytes.values()) == STEP_BYTES
     peak, peak_kind = _peaks()
     dom_avg_ms = kt[dom][0]
     achieved = kbytes[dom] / (dom_avg_ms / 1000.0) / 1e9 if dom_avg_ms > 0 else 0.0
@@ -238,14 +259,23 @@ def run_ours(args, world, rank, local, dist):
     eta = torch.empty((NJ + 2, NI + 2), dtype=torch.float64, pin_memory=True).numpy().T
     for name, a in (("u", u), ("v", v), ("h", h), ("eta", eta)):
         a[...] = m.get(name)
+    # every step: upload u, v, h, eta from pinned host memory, one RK2 step,
+    # read u, v, h, eta back (the host-buffer C-ABI call mom6b_step_host)
+    barrier(dist)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        m.step_host(1, u, v, h, eta)
+    t1 = time.perf_counter()
+    e2e_s = max_over_ranks(t1 - t0, dist, local)
+    e2e = world * args.steps / e2e_s
+    bytes_h2d = 3 * N3 + N2
+    bytes_d2h = 3 * N3 + N2
+    # state resident on the device: one upload, K steps, one read-back
     barrier(dist)
     t0 = time.perf_counter()
     m.step_host(args.steps, u, v, h, eta)
     t1 = time.perf_counter()
-    e2e_s = max_over_ranks(t1 - t0, dist, local)
-    e2e = world * args.steps / e2e_s
-    bytes_h2d = (3 * N3 + N2) / args.steps
-    bytes_d2h = (3 * N3 + N2) / args.steps
+    e2e_res = world * args.steps / max_over_ranks(t1 - t0, dist, local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -268,12 +298,20 @@ def run_ours(args, world, rank, local, dist):
                                   "peak_GBs": peak, "frac": STEP_BYTES / (ms / args.steps / 1000.0) / 1e9 / peak},
                 "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved,
                              "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                             "peak_kind": peak_kind, "traffic": None,
+                             "peak_kind": peak_kind,
+                             "traffic": measured_traffic().get(dom),
+                             "traffic_source": "ncu 360x360x75 capture scaled by units "
+                                               "processed (profiles/traffic_720x720x75.txt)",
                              "bytes_per_launch": kbytes[dom], "avg_launch_ms": dom_avg_ms},
                 "kernel_ms_per_step": per_step_ms,
                 "cpu_baseline": cpu,
                 "e2e": {"value": e2e, "unit": "steps/s", "h2d_bytes_per_step": bytes_h2d,
-                        "d2h_bytes_per_step": bytes_d2h},
+                        "d2h_bytes_per_step": bytes_d2h,
+                        "what": "mom6b_step_host(1, u, v, h, eta) per step: pinned host "
+                                "state uploaded, one step, state read back"},
+                "e2e_resident": {"value": e2e_res, "unit": "steps/s",
+                                 "h2d_bytes_per_step": bytes_h2d / args.steps,
+                                 "d2h_bytes_per_step": bytes_d2h / args.steps},
                 "gpu_launches": launches,
                 "clocks": ck}
         print(json.dumps(line), flush=True)
