@@ -484,6 +484,388 @@ k_cont_fused(Dims D, Metrics M, const double* __restrict__ u,
     cell_convergence(D, M, I, j, hin, ovl, O, dt);
 }
 
+// ---------------------------------------------------------------------------
+// Tile kernel (selected with MOM6B_CONT_TILE=1): one CTA owns 32 consecutive u faces of one row
+// (lane = face) and kTileWarps warps, warp g owning a contiguous chunk of
+// layers.  The h of cells F0-2 .. F0+34 and the PPM edges of cells
+// F0 .. F0+32 are computed once into shared memory; each thread keeps u and
+// the latest transport of its layers in registers.  Every pass over a face
+// column (initial fluxes, each Newton iterate, the BT_cont test velocities)
+// evaluates the layers of all warps in parallel and then hands the running
+// column sums from warp to warp through named barriers, so each sum is formed
+// in layer order 1..nz exactly as the serial loop forms it.  The Newton and
+// BT_cont scalar logic of a face runs in the last warp.  Consecutive CTAs
+// overlap by one face; lane 0 of every CTA but the first recomputes the last
+// face of its left neighbour and keeps it private.
+// ---------------------------------------------------------------------------
+constexpr int kTileWarps = 8;
+constexpr int kTileFaces = 32;
+constexpr int kTileCells = kTileFaces + 1;          // cells with edges
+constexpr int kTileHalo = kTileFaces + 5;           // cells with h (PPM stencil)
+
+__device__ __forceinline__ void named_bar_sync(int id, int count)
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+__device__ __forceinline__ void named_bar_arrive(int id, int count)
+{
+    asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+// PPM_reconstruction_x + PPM_limit_pos for one cell from its 5-cell stencil
+// (h[0..4] = cells i-2..i+2, m[0..4] their masks); same operations as ppm_cell.
+__device__ __forceinline__ void ppm_stencil(const double* h, const double* m, double h_min,
+                                            double& hL, double& hR)
+{
+    auto slope = [&](int c) -> double {   // slope of cell c (1..3 here)
+        if ((m[c - 1] * m[c] * m[c + 1]) == 0.0) return 0.0;
+        const double hp = h[c + 1], hm = h[c - 1], hc = h[c];
+        const double s = 0.5 * (hp - hm);
+        const double dMx = dmax(dmax(hp, hm), hc) - hc;
+        const double dMn = hc - dmin(dmin(hp, hm), hc);
+        return copysign(1.0, s) * dmin(fabs(s), 2.0 * dmin(dMx, dMn));
+    };
+    const double oneSixth = 1.0 / 6.0;
+    const double slm = slope(1), slc = slope(2), slp = slope(3);
+    const double hc = h[2];
+    const double h_im1 = m[1] * h[1] + (1.0 - m[1]) * hc;
+    const double h_ip1 = m[3] * h[3] + (1.0 - m[3]) * hc;
+    hL = 0.5 * (h_im1 + hc) + oneSixth * (slm - slc);
+    hR = 0.5 * (h_ip1 + hc) + oneSixth * (slc - slp);
+    float curv = (float)(3.0 * ((hL + hR) - 2.0 * hc));
+    if ((double)curv > 0.0) {
+        float dh = (float)(hR - hL);
+        if (fabsf(dh) < curv) {
+            if (hc <= h_min) {
+                hL = hc; hR = hc;
+            } else {
+                float c12 = __fmul_rn(12.0f, curv);
+                float den = __fadd_rn(__fmul_rn(curv, curv), __fmul_rn(3.0f, __fmul_rn(dh, dh)));
+                double lhs = (double)c12 * (hc - h_min);
+                if (lhs < (double)den) {
+                    float scale = (float)(lhs / (double)den);
+                    hL = hc + (double)scale * (hL - hc);
+                    hR = hc + (double)scale * (hR - hc);
+                }
+            }
+        }
+    }
+}
+
+template <int LMAX>
+__global__ void __launch_bounds__(32 * kTileWarps, 2)
+k_cont_tile(Dims D, Metrics M, const double* __restrict__ u, const double* __restrict__ hin,
+            const double* __restrict__ uhbt2d, ContOut O, double dt, double h_min)
+{
+    extern __shared__ double sm[];
+    const int nz = D.nk;
+    const int HW = kTileHalo, CW = kTileCells;
+    // shared layout (double offsets)
+    const int oH = 0;                        // h      [nz][HW]
+    const int oW = oH + nz * HW;             // h_W    [nz][CW]
+    const int oE = oW + nz * CW;             // h_E    [nz][CW]
+    const int oMask = oE + nz * CW;          // mask2dT of the HW cells
+    const int oCh = oMask + HW;              // chain  [4][32]
+    const int oDu = oCh + 4 * 32;            // broadcast du per face
+    const int oAct = oDu + 32;               // broadcast flags per face (as double)
+    const int tid = (int)threadIdx.x, f = tid & 31, g = tid >> 5;
+    const int F0 = D.is - 1 + (int)blockIdx.x * (kTileFaces - 1);
+    const int I = F0 + f;
+    const int j = D.js + (int)blockIdx.y;
+    const size_t plane = (size_t)D.plane;
+    const size_t row = (size_t)(j - 1) * D.n1;
+    const bool face_ok = I <= D.ie;
+    const bool owner = face_ok && (f >= 1 || blockIdx.x == 0);
+    const int Ic = face_ok ? I : D.ie;       // clamped face for metric reads
+
+    // ---- load h and masks, then the PPM edges of the tile's cells ----------
+    for (int t = tid; t < nz * HW; t += blockDim.x) {
+        const int k = t / HW, c = t - k * HW, i = F0 - 2 + c;
+        sm[oH + t] = (i >= 1 && i <= D.n1) ? hin[(size_t)k * plane + row + (i - 1)] : 0.0;
+    }
+    for (int c = tid; c < HW; c += blockDim.x) {
+        const int i = F0 - 2 + c;
+        sm[oMask + c] = (i >= 1 && i <= D.n1) ? M.mask2dT[row + (i - 1)] : 0.0;
+    }
+    __syncthreads();
+    for (int t = tid; t < nz * CW; t += blockDim.x) {
+        const int k = t / CW, c = t - k * CW, i = F0 + c;
+        double hL = 0.0, hR = 0.0;
+        if (i >= D.is - 1 && i <= D.ie + 1)
+            ppm_stencil(&sm[oH + k * HW + c], &sm[oMask + c], h_min, hL, hR);
+        sm[oW + t] = hL;
+        sm[oE + t] = hR;
+    }
+
+    // ---- per-thread layer chunk and face constants --------------------------
+    const int L = (nz + kTileWarps - 1) / kTileWarps;
+    const int k0 = g * L + 1;
+    const int nmine = max(0, min(L, nz - k0 + 1));
+    const double dy = MOM6B_A2(M.dy_Cu, Ic, j, D);
+    const double Idx_i = MOM6B_A2(M.IdxT, Ic, j, D), Idx_p = MOM6B_A2(M.IdxT, Ic + 1, j, D);
+    double uk[LMAX], uhk[LMAX], tA[LMAX], tB[LMAX];
+#pragma unroll
+    for (int c = 0; c < LMAX; ++c) {
+        uk[c] = (c < nmine) ? u[(size_t)(k0 + c - 1) * plane + row + (Ic - 1)] : 0.0;
+        uhk[c] = 0.0; tA[c] = 0.0; tB[c] = 0.0;
+    }
+    __syncthreads();
+
+    // zonal_flux_layer at face velocity uI for layer k (flux_eval on the tile)
+    auto eval = [&](int k, double uI, double& hm) -> double {
+        const bool pos = uI > 0.0;
+        const int cc = pos ? f : f + 1;
+        const int e = (k - 1) * CW + cc;
+        const double hWc = sm[oW + e], hEc = sm[oE + e], hc = sm[oH + (k - 1) * HW + cc + 2];
+        const double base = pos ? hEc : hWc;
+        const double oth = pos ? hWc : hEc;
+        const double Idx = pos ? Idx_i : Idx_p;
+        const double CFL = fabs(uI) * dt * Idx;
+        const double curv_3 = (oth + base) - 2.0 * hc;
+        const double uh = dy * uI * (base + CFL * (0.5 * (oth - base) + curv_3 * (CFL - 1.5)));
+        const double hmm = base + CFL * ((oth - base) + 3.0 * curv_3 * (CFL - 1.0));
+        if (!(uI > 0.0) && !(uI < 0.0)) {
+            hm = 0.5 * (sm[oW + (k - 1) * CW + f + 1] + sm[oE + (k - 1) * CW + f]);
+            return 0.0;
+        }
+        hm = hmm;
+        return uh;
+    };
+    // hand the running values v[0..nv) from warp g-1 to warp g, add this
+    // warp's layers with add(c, v), pass them on; the last warp keeps them
+    auto chain = [&](int nv, double* v, auto&& add) {
+        if (g > 0) {
+            named_bar_sync(g, 64);
+            for (int q = 0; q < nv; ++q) v[q] = sm[oCh + q * 32 + f];
+        }
+#pragma unroll
+        for (int c = 0; c < LMAX; ++c)
+            if (c < nmine) add(c, v);
+        if (g < kTileWarps - 1) {
+            for (int q = 0; q < nv; ++q) sm[oCh + q * 32 + f] = v[q];
+            named_bar_arrive(g + 1, 64);
+        }
+    };
+    const bool last = g == kTileWarps - 1;
+
+    // ---- initial fluxes and CFL limits (:305-433) ----------------------------
+    const double CFL_dt = 0.5 / dt;
+    const double dx_W = MOM6B_A2(M.dxT, Ic, j, D), dx_E = MOM6B_A2(M.dxT, Ic + 1, j, D);
+    const double mCu = MOM6B_A2(M.mask2dCu, Ic, j, D);
+#pragma unroll
+    for (int c = 0; c < LMAX; ++c)
+        if (c < nmine) {
+            double hm;
+            uhk[c] = eval(k0 + c, uk[c], hm);
+            tA[c] = dy * hm;
+        }
+    double v4[4] = {0.0, 0.0, 2.0 * (CFL_dt * dx_W), -(2.0 * (CFL_dt * dx_E))};
+    chain(4, v4, [&](int c, double* v) {
+        v[0] = v[0] + uhk[c];
+        v[1] = v[1] + tA[c];
+        if (v[2] > dx_W * CFL_dt - uk[c] * mCu) v[2] = dx_W * CFL_dt - uk[c];
+        if (v[3] < -(dx_E * CFL_dt) - uk[c] * mCu) v[3] = -(dx_E * CFL_dt + uk[c]);
+    });
+    // Newton state of the face (last warp only)
+    const double uhbt = MOM6B_A2(uhbt2d, Ic, j, D);
+    const double fac = dt * dmin(MOM6B_A2(M.IareaT, Ic, j, D), MOM6B_A2(M.IareaT, Ic + 1, j, D));
+    const double tol_eta_cs = 1.0e-12, tol_vel = 3.0e8;
+    const int max_itts = 20;
+    const double uh_tot_0 = v4[0], duhdu_tot_0 = v4[1];
+    const double du_max_CFL = dmax(v4[2], 0.0), du_min_CFL = dmin(v4[3], 0.0);
+    double du = 0.0, du_max = du_max_CFL, du_min = du_min_CFL;
+    double uh_err = uh_tot_0 - uhbt, duhdu_tot = duhdu_tot_0, uh_err_best = fabs(uh_err);
+    int itt = 1;
+    bool do_I = face_ok;
+    // one decision of zonal_flux_adjust's loop (:813-890) for iteration itt
+    auto decide = [&]() {
+        if (!do_I) return;
+        double tol_eta;
+        if (itt <= 1) tol_eta = F32(1e-6) * tol_eta_cs;
+        else if (itt == 2) tol_eta = F32(1e-4) * tol_eta_cs;
+        else if (itt == 3) tol_eta = F32(1e-2) * tol_eta_cs;
+        else tol_eta = tol_eta_cs;
+        if (uh_err > 0.0) du_max = du;
+        else if (uh_err < 0.0) du_min = du;
+        else do_I = false;
+        if (!do_I) return;
+        const double ae = fabs(uh_err);
+        if ((fac * ae > tol_eta) || ((ae > tol_vel * duhdu_tot) || (ae > uh_err_best))) {
+            const double ddu = -(uh_err / duhdu_tot);
+            const double du_prev = du;
+            du = du + ddu;
+            if (fabs(ddu) < F32(1.0e-15) * fabs(du)) {
+                do_I = false;
+            } else if (ddu > 0.0) {
+                if (du >= du_max) {
+                    du = 0.5 * (du_prev + du_max);
+                    if (du_max - du_prev < F32(1.0e-15) * fabs(du)) do_I = false;
+                }
+            } else if (du <= du_min) {
+                du = 0.5 * (du_prev + du_min);
+                if (du_prev - du_min < F32(1.0e-15) * fabs(du)) do_I = false;
+            }
+        } else {
+            do_I = false;
+        }
+    };
+    // Newton passes: keep_uh selects zonal_flux_adjust (transports kept) or
+    // the zero-transport solve of set_zonal_BT_cont (nothing kept)
+    auto newton = [&](double target, bool keep_uh) {
+        for (;;) {
+            if (last) {
+                decide();
+                sm[oDu + f] = du;
+                sm[oAct + f] = do_I ? 1.0 : 0.0;
+            }
+            if (!__syncthreads_or(last && do_I)) break;
+            const double du_b = sm[oDu + f];
+            const bool act = sm[oAct + f] != 0.0;
+#pragma unroll
+            for (int c = 0; c < LMAX; ++c)
+                if (c < nmine && act) {
+                    double hm;
+                    const double uh = eval(k0 + c, uk[c] + du_b, hm);
+                    if (keep_uh) uhk[c] = uh;
+                    tB[c] = uh;
+                    tA[c] = dy * hm;
+                }
+            double v2[2] = {target, 0.0};
+            chain(2, v2, [&](int c, double* v) {
+                v[0] = v[0] + tB[c];
+                v[1] = v[1] + tA[c];
+            });
+            if (last && do_I) {
+                if (itt < max_itts) {
+                    uh_err = v2[0];
+                    duhdu_tot = v2[1];
+                    uh_err_best = dmin(uh_err_best, fabs(uh_err));
+                }
+                ++itt;
+                if (itt > max_itts) do_I = false;
+            }
+            __syncthreads();
+        }
+    };
+    newton(-uhbt, true);
+    const double du_cor = du;
+
+    // ---- set_zonal_BT_cont (:991-1121) ---------------------------------------
+    if (last) {   // zero-transport solve only where uhbt != 0
+        du = 0.0; du_max = du_max_CFL; du_min = du_min_CFL;
+        uh_err = uh_tot_0; duhdu_tot = duhdu_tot_0; uh_err_best = fabs(uh_err);
+        itt = 1;
+        do_I = owner && uhbt != 0.0;
+    }
+    __syncthreads();
+    newton(-0.0, false);   // e = -uhbt with uhbt = 0
+    if (last) {
+        const double du0 = (owner && uhbt != 0.0) ? du : du_cor;
+        sm[oDu + f] = du0;
+        sm[oAct + f] = du_cor;   // reused: du_cor of the face
+    }
+    __syncthreads();
+    const double du0 = sm[oDu + f];
+    const double du_c = sm[oAct + f];
+    const double Idt = 1.0 / dt;
+    const double du_CFL = (F32(1e-6) * Idt) * MOM6B_A2(M.dxCu, Ic, j, D);
+    double vLR[2] = {dmin(0.0, du0 - du_CFL), dmax(0.0, du0 + du_CFL)};   // duR, duL
+    chain(2, vLR, [&](int c, double* v) {
+        if (uk[c] + v[0] > -du_CFL) v[0] = -(uk[c] + du_CFL);
+        if (uk[c] + v[1] < du_CFL) v[1] = -(uk[c] - du_CFL);
+    });
+    if (last) {
+        sm[oCh + 0 * 32 + f] = vLR[0];
+        sm[oCh + 1 * 32 + f] = vLR[1];
+    }
+    __syncthreads();
+    const double duR = sm[oCh + f], duL = sm[oCh + 32 + f];
+    __syncthreads();
+    const bool same = du0 == du_c;
+    // test velocity u + du0: FAmt_0, and h_u at u_cor = u + du (marginal faces)
+#pragma unroll
+    for (int c = 0; c < LMAX; ++c)
+        if (c < nmine) {
+            double hm0;
+            eval(k0 + c, uk[c] + du0, hm0);
+            tA[c] = dy * hm0;
+            double hmc = hm0;
+            if (!same) eval(k0 + c, uk[c] + du_c, hmc);
+            if (owner) O.h_u[(size_t)(k0 + c - 1) * plane + row + (I - 1)] = hmc;
+        }
+    double v0[1] = {0.0};
+    chain(1, v0, [&](int c, double* v) { v[0] = v[0] + tA[c]; });
+    __syncthreads();
+    // test velocity u + duL: FAmt_L, uhtot_L
+#pragma unroll
+    for (int c = 0; c < LMAX; ++c)
+        if (c < nmine) {
+            double hm;
+            tB[c] = eval(k0 + c, uk[c] + duL, hm);
+            tA[c] = dy * hm;
+        }
+    double vL[2] = {0.0, 0.0};
+    chain(2, vL, [&](int c, double* v) {
+        v[0] = v[0] + tA[c];
+        v[1] = v[1] + tB[c];
+    });
+    __syncthreads();
+    // test velocity u + duR: FAmt_R, uhtot_R
+#pragma unroll
+    for (int c = 0; c < LMAX; ++c)
+        if (c < nmine) {
+            double hm;
+            tB[c] = eval(k0 + c, uk[c] + duR, hm);
+            tA[c] = dy * hm;
+        }
+    double vR[2] = {0.0, 0.0};
+    chain(2, vR, [&](int c, double* v) {
+        v[0] = v[0] + tA[c];
+        v[1] = v[1] + tB[c];
+    });
+    if (last && owner) {
+        const size_t f0 = row + (I - 1);
+        O.du_cor[f0] = du_c;
+        const double FAmt_0 = v0[0], FAmt_L = vL[0], uhtot_L = vL[1];
+        const double FAmt_R = vR[0], uhtot_R = vR[1];
+        double FA_0 = FAmt_0, FA_avg = FAmt_0;
+        if ((duL - du0) != 0.0) FA_avg = uhtot_L / (duL - du0);
+        if (FA_avg > dmax(FA_0, FAmt_L)) FA_avg = dmax(FA_0, FAmt_L);
+        else if (FA_avg < dmin(FA_0, FAmt_L)) FA_0 = FA_avg;
+        O.FA_u_W0[f0] = FA_0;
+        O.FA_u_WW[f0] = FAmt_L;
+        O.uBT_WW[f0] = (fabs(FA_0 - FAmt_L) <= F32(1e-12) * FA_0)
+                           ? 0.0
+                           : (1.5 * (duL - du0)) * ((FAmt_L - FA_avg) / (FAmt_L - FA_0));
+        FA_0 = FAmt_0; FA_avg = FAmt_0;
+        if ((duR - du0) != 0.0) FA_avg = uhtot_R / (duR - du0);
+        if (FA_avg > dmax(FA_0, FAmt_R)) FA_avg = dmax(FA_0, FAmt_R);
+        else if (FA_avg < dmin(FA_0, FAmt_R)) FA_0 = FA_avg;
+        O.FA_u_E0[f0] = FA_0;
+        O.FA_u_EE[f0] = FAmt_R;
+        O.uBT_EE[f0] = (fabs(FAmt_R - FA_0) <= F32(1e-12) * FA_0)
+                           ? 0.0
+                           : (1.5 * (duR - du0)) * ((FAmt_R - FA_avg) / (FAmt_R - FA_0));
+    }
+
+    // ---- transports and continuity_zonal_convergence (:148-176) --------------
+    const int i = I;   // cell i = I uses faces I-1 (lane f-1) and I (lane f)
+    const bool cell_ok = f >= 1 && i >= D.is && i <= D.ie;
+    const double facc = cell_ok ? dt * MOM6B_A2(M.IareaT, i, j, D) : 0.0;
+#pragma unroll
+    for (int c = 0; c < LMAX; ++c) {
+        const double uh_left = __shfl_up_sync(0xffffffffu, uhk[c], 1);
+        if (c < nmine) {
+            const size_t o = (size_t)(k0 + c - 1) * plane + row;
+            if (owner) O.uh[o + (I - 1)] = uhk[c];
+            if (cell_ok) {
+                const double hc = sm[oH + (k0 + c - 1) * HW + f + 2];
+                O.h[o + (i - 1)] = dmax(hc - facc * (uhk[c] - uh_left), 0.0);
+            }
+        }
+    }
+}
+
 // CTAs per SM for k_cont_faces; 0 lets the hardware fill the SM.
 constexpr int kContCtasPerSM = 0;
 
@@ -500,6 +882,29 @@ cudaError_t launch_continuity(const Dims& D, const Metrics& M, const double* u,
                               const double* uhbt, const ContOut& O, double* uh_ovl,
                               double dt, double h_min, cudaStream_t s)
 {
+    // The tile kernel keeps every column on chip (a quarter of the face
+    // kernel's DRAM traffic) but is bounded by its serial column sums; the
+    // face kernel below is faster on B200 and stays the default.
+    if (D.nk <= 16 * kTileWarps && getenv("MOM6B_CONT_TILE")) {
+        const size_t smem = ((size_t)D.nk * (kTileHalo + 2 * kTileCells) + kTileHalo + 6 * 32) *
+                            sizeof(double);
+        const int nfaces = D.ie - (D.is - 1) + 1;
+        dim3 grid((nfaces - 1 + kTileFaces - 2) / (kTileFaces - 1), D.je - D.js + 1, 1);
+        if (D.nk <= 10 * kTileWarps) {
+            cudaError_t e = cudaFuncSetAttribute(k_cont_tile<10>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem);
+            if (e != cudaSuccess) return e;
+            k_cont_tile<10><<<grid, 32 * kTileWarps, smem, s>>>(D, M, u, hin, uhbt, O, dt, h_min);
+        } else {
+            cudaError_t e = cudaFuncSetAttribute(k_cont_tile<16>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem);
+            if (e != cudaSuccess) return e;
+            k_cont_tile<16><<<grid, 32 * kTileWarps, smem, s>>>(D, M, u, hin, uhbt, O, dt, h_min);
+        }
+        return cudaGetLastError();
+    }
     {
         const int nb = 32 * kFusedWarps, step = nb - 1;
         size_t smem = (size_t)kFusedWarps * 2 * D.nk * kFusedCells * sizeof(double);

@@ -147,3 +147,15 @@ def test_barotropic_variants_bitwise(untiled, monkeypatch):
     for n in ["eta", "eta_av", "ubt_av", "vbt_av"]:
         a, b = g.get(n), o.get(n)
         assert np.array_equal(a, b), f"{n}: {describe(a, b)}"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", [(36, 30, 8), (70, 50, 12), (13, 11, 5)])
+def test_continuity_tile_kernel_bitwise(shape, monkeypatch):
+    # the shared-memory tile variant of continuity gives the same step
+    monkeypatch.setenv("MOM6B_CONT_TILE", "1")
+    ni, nj, nk = shape
+    o, g = _pair(ni, nj, nk, 40, INIT_CFG, seed=9)
+    o.step(3)
+    g.step(3)
+    _cmp(o, g, STATE + EXTRA, 0.0, bitwise=True)
