@@ -564,7 +564,9 @@ k_cont_tile(Dims D, Metrics M, const double* __restrict__ u, const double* __res
     const int oH = 0;                        // h      [nz][HW]
     const int oW = oH + nz * HW;             // h_W    [nz][CW]
     const int oE = oW + nz * CW;             // h_E    [nz][CW]
-    const int oMask = oE + nz * CW;          // mask2dT of the HW cells
+    const int oDf = oE + nz * CW;            // h_W - h_E            [nz][CW]
+    const int oCv = oDf + nz * CW;           // (h_W + h_E) - 2 h    [nz][CW]
+    const int oMask = oCv + nz * CW;         // mask2dT of the HW cells
     const int oCh = oMask + HW;              // chain  [4][32]
     const int oDu = oCh + 4 * 32;            // broadcast du per face
     const int oAct = oDu + 32;               // broadcast flags per face (as double)
@@ -595,6 +597,10 @@ k_cont_tile(Dims D, Metrics M, const double* __restrict__ u, const double* __res
             ppm_stencil(&sm[oH + k * HW + c], &sm[oMask + c], h_min, hL, hR);
         sm[oW + t] = hL;
         sm[oE + t] = hR;
+        // (other - base) of either upwind case is +-(h_W - h_E) exactly, and
+        // curv_3 = (h_W + h_E) - 2 h in both (addition commutes)
+        sm[oDf + t] = hL - hR;
+        sm[oCv + t] = (hL + hR) - 2.0 * sm[oH + k * HW + c + 2];
     }
 
     // ---- per-thread layer chunk and face constants --------------------------
@@ -616,14 +622,14 @@ k_cont_tile(Dims D, Metrics M, const double* __restrict__ u, const double* __res
         const bool pos = uI > 0.0;
         const int cc = pos ? f : f + 1;
         const int e = (k - 1) * CW + cc;
-        const double hWc = sm[oW + e], hEc = sm[oE + e], hc = sm[oH + (k - 1) * HW + cc + 2];
-        const double base = pos ? hEc : hWc;
-        const double oth = pos ? hWc : hEc;
+        const double base = sm[(pos ? oE : oW) + e];
+        const double dfc = sm[oDf + e];
+        const double d = pos ? dfc : -dfc;               // other - base
+        const double curv_3 = sm[oCv + e];
         const double Idx = pos ? Idx_i : Idx_p;
         const double CFL = fabs(uI) * dt * Idx;
-        const double curv_3 = (oth + base) - 2.0 * hc;
-        const double uh = dy * uI * (base + CFL * (0.5 * (oth - base) + curv_3 * (CFL - 1.5)));
-        const double hmm = base + CFL * ((oth - base) + 3.0 * curv_3 * (CFL - 1.0));
+        const double uh = dy * uI * (base + CFL * (0.5 * d + curv_3 * (CFL - 1.5)));
+        const double hmm = base + CFL * (d + 3.0 * curv_3 * (CFL - 1.0));
         if (!(uI > 0.0) && !(uI < 0.0)) {
             hm = 0.5 * (sm[oW + (k - 1) * CW + f + 1] + sm[oE + (k - 1) * CW + f]);
             return 0.0;
@@ -782,7 +788,9 @@ k_cont_tile(Dims D, Metrics M, const double* __restrict__ u, const double* __res
     const double duR = sm[oCh + f], duL = sm[oCh + 32 + f];
     __syncthreads();
     const bool same = du0 == du_c;
-    // test velocity u + du0: FAmt_0, and h_u at u_cor = u + du (marginal faces)
+    // test velocities u + du0 (FAmt_0, and h_u at u_cor = u + du for the
+    // marginal faces) and u + duL (FAmt_L, uhtot_L) in one pass
+    double tC[LMAX];
 #pragma unroll
     for (int c = 0; c < LMAX; ++c)
         if (c < nmine) {
@@ -792,23 +800,20 @@ k_cont_tile(Dims D, Metrics M, const double* __restrict__ u, const double* __res
             double hmc = hm0;
             if (!same) eval(k0 + c, uk[c] + du_c, hmc);
             if (owner) O.h_u[(size_t)(k0 + c - 1) * plane + row + (I - 1)] = hmc;
+            double hmL;
+            tC[c] = eval(k0 + c, uk[c] + duL, hmL);
+            tB[c] = dy * hmL;
         }
-    double v0[1] = {0.0};
-    chain(1, v0, [&](int c, double* v) { v[0] = v[0] + tA[c]; });
-    __syncthreads();
-    // test velocity u + duL: FAmt_L, uhtot_L
-#pragma unroll
-    for (int c = 0; c < LMAX; ++c)
-        if (c < nmine) {
-            double hm;
-            tB[c] = eval(k0 + c, uk[c] + duL, hm);
-            tA[c] = dy * hm;
-        }
-    double vL[2] = {0.0, 0.0};
-    chain(2, vL, [&](int c, double* v) {
-        v[0] = v[0] + tA[c];
-        v[1] = v[1] + tB[c];
-    });
+    double v0[1], vL[2];
+    {
+        double v3[3] = {0.0, 0.0, 0.0};
+        chain(3, v3, [&](int c, double* v) {
+            v[0] = v[0] + tA[c];
+            v[1] = v[1] + tB[c];
+            v[2] = v[2] + tC[c];
+        });
+        v0[0] = v3[0]; vL[0] = v3[1]; vL[1] = v3[2];
+    }
     __syncthreads();
     // test velocity u + duR: FAmt_R, uhtot_R
 #pragma unroll
@@ -886,7 +891,7 @@ cudaError_t launch_continuity(const Dims& D, const Metrics& M, const double* u,
     // kernel's DRAM traffic) but is bounded by its serial column sums; the
     // face kernel below is faster on B200 and stays the default.
     if (D.nk <= 16 * kTileWarps && getenv("MOM6B_CONT_TILE")) {
-        const size_t smem = ((size_t)D.nk * (kTileHalo + 2 * kTileCells) + kTileHalo + 6 * 32) *
+        const size_t smem = ((size_t)D.nk * (kTileHalo + 4 * kTileCells) + kTileHalo + 6 * 32) *
                             sizeof(double);
         const int nfaces = D.ie - (D.is - 1) + 1;
         dim3 grid((nfaces - 1 + kTileFaces - 2) / (kTileFaces - 1), D.je - D.js + 1, 1);
