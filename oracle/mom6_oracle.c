@@ -72,6 +72,7 @@ struct oracle_model {
         *bt_Datv, *bt_gtot_E, *bt_gtot_W, *bt_gtot_N, *bt_gtot_S, *bt_f_4_u,
         *bt_f_4_v, *bt_rem_u, *bt_rem_v, *bt_ubt_av, *bt_vbt_av;
     int first_direction;
+    int bt_extended; /* 1: uhbt/vhbt and averages on the extended ranges */
 };
 
 /* ------------------------------------------------------------------------ */
@@ -887,12 +888,16 @@ void oracle_btstep(oracle_model *m, const double *eta_in, const double *ubt_in,
             bt_update_u(m, is, ie - 1, js, je);
             bt_update_v(m, is, ie, js, je - 1);
         }
+        /* transport ranges: serial (:263-291) or, with bt_extended, those
+         * of btstep_do_step and the CUDA C kernels (:443-452) */
+        const int iu0 = m->bt_extended ? is - 1 : is, iu1 = m->bt_extended ? ie : ie - 1;
+        const int jv0 = m->bt_extended ? js - 1 : js, jv1 = m->bt_extended ? je : je - 1;
         for (int j = js; j <= je; ++j)
-            for (int i = is; i <= ie - 1; ++i)
+            for (int i = iu0; i <= iu1; ++i)
                 A2(m->bt_uhbt, i, j) =
                     A2(m->bt_Datu, i, j) *
                     (trans_wt1 * A2(m->bt_ubt, i, j) + trans_wt2 * A2(m->bt_ubt_prev, i, j));
-        for (int j = js; j <= je - 1; ++j)
+        for (int j = jv0; j <= jv1; ++j)
             for (int i = is; i <= ie; ++i)
                 A2(m->bt_vhbt, i, j) =
                     A2(m->bt_Datv, i, j) *
@@ -905,9 +910,9 @@ void oracle_btstep(oracle_model *m, const double *eta_in, const double *ubt_in,
                         ((A2(m->bt_uhbt, i, j) - A2(m->bt_uhbt, i - 1, j)) +
                          (A2(m->bt_vhbt, i, j) - A2(m->bt_vhbt, i, j - 1)));
         for (int j = js; j <= je; ++j)
-            for (int i = is; i <= ie - 1; ++i)
+            for (int i = iu0; i <= iu1; ++i)
                 A2(m->bt_ubt_av, i, j) = A2(m->bt_ubt_av, i, j) + A2(m->bt_ubt, i, j) * inv_nstep;
-        for (int j = js; j <= je - 1; ++j)
+        for (int j = jv0; j <= jv1; ++j)
             for (int i = is; i <= ie; ++i)
                 A2(m->bt_vbt_av, i, j) = A2(m->bt_vbt_av, i, j) + A2(m->bt_vbt, i, j) * inv_nstep;
     }
@@ -1486,6 +1491,39 @@ int oracle_set(oracle_model *m, int field, const double *in) {
     if (!p) return -1;
     memcpy(p, in, oracle_field_size(m, field) * sizeof(double));
     return 0;
+}
+
+void oracle_set_bt_extended(oracle_model *m, int on) { m->bt_extended = on ? 1 : 0; }
+
+/* Copy one of the oracle's grid or control-structure arrays by name (count
+ * doubles: n1*n2, or 4*n1*n2 for f_4_u/f_4_v).  Returns 0, or -1 for an
+ * unknown name or a count mismatch. */
+int oracle_array(const oracle_model *m, const char *name, double *out, size_t count) {
+    struct { const char *n; const double *p; size_t k; } tab[] = {
+        {"IareaT", m->IareaT, 1}, {"areaT", m->areaT, 1}, {"dxT", m->dxT, 1},
+        {"IdxT", m->IdxT, 1}, {"dxCu", m->dxCu, 1}, {"dyCu", m->dyCu, 1},
+        {"dy_Cu", m->dy_Cu, 1}, {"IdxCu", m->IdxCu, 1}, {"IdyCu", m->IdyCu, 1},
+        {"dxCv", m->dxCv, 1}, {"dyCv", m->dyCv, 1}, {"IdxCv", m->IdxCv, 1},
+        {"IdyCv", m->IdyCv, 1}, {"IareaBu", m->IareaBu, 1}, {"CoriolisBu", m->CoriolisBu, 1},
+        {"IareaCu", m->IareaCu, 1}, {"IareaCv", m->IareaCv, 1}, {"mask2dT", m->mask2dT, 1},
+        {"mask2dBu", m->mask2dBu, 1}, {"mask2dCu", m->mask2dCu, 1},
+        {"mask2dCv", m->mask2dCv, 1}, {"Area_q", m->co_Area_q, 1},
+        {"dx2h", m->hv_dx2h, 1}, {"dy2h", m->hv_dy2h, 1}, {"dx2q", m->hv_dx2q, 1},
+        {"dy2q", m->hv_dy2q, 1}, {"DX_dyT", m->hv_DX_dyT, 1}, {"DY_dxT", m->hv_DY_dxT, 1},
+        {"DX_dyBu", m->hv_DX_dyBu, 1}, {"DY_dxBu", m->hv_DY_dxBu, 1},
+        {"reduction_xx", m->hv_red_xx, 1}, {"reduction_xy", m->hv_red_xy, 1},
+        {"Datu", m->bt_Datu, 1}, {"Datv", m->bt_Datv, 1}, {"gtot_E", m->bt_gtot_E, 1},
+        {"gtot_W", m->bt_gtot_W, 1}, {"gtot_N", m->bt_gtot_N, 1},
+        {"gtot_S", m->bt_gtot_S, 1}, {"f_4_u", m->bt_f_4_u, 4}, {"f_4_v", m->bt_f_4_v, 4},
+        {"bt_rem_u", m->bt_rem_u, 1}, {"bt_rem_v", m->bt_rem_v, 1}};
+    for (size_t t = 0; t < sizeof(tab) / sizeof(tab[0]); ++t)
+        if (strcmp(tab[t].n, name) == 0) {
+            size_t n = (size_t)N1 * N2 * tab[t].k;
+            if (count != n || !tab[t].p) return -1;
+            memcpy(out, tab[t].p, n * sizeof(double));
+            return 0;
+        }
+    return -1;
 }
 
 void oracle_dims(const oracle_model *m, int *o) {

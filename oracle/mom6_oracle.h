@@ -3,11 +3,17 @@
  *
  * TEST INFRASTRUCTURE ONLY.  This is the parity oracle for the B200 library:
  * it restates, in plain C, the serial Fortran path of the reference
- * (app/rk2_serial_driver.F90 + src/serial/*.F90 + src/common/mom6_types.F90)
- * and, in a second family of functions prefixed occ_, the reference CUDA C
- * kernels of src/cuda_c/*.cu.  Only tests/, the smoke check and the
- * cpu_baseline leg of bench.py may link or call it; the product library never
- * does.
+ * (app/rk2_serial_driver.F90 + src/serial/*.F90 + src/common/mom6_types.F90).
+ * Only tests/, the smoke check and the cpu_baseline leg of bench.py may link
+ * or call it; the product library never does.
+ *
+ * Pinning: the reference has no golden vectors and its Fortran does not
+ * compile here, but its CUDA C kernels (src/cuda_c/*.cu) build from their
+ * sources into oracle/_ref.  Where the serial semantics and those kernels
+ * coincide -- horizontal viscosity, the Sadourny Coriolis term, vertical
+ * viscosity without Rayleigh drag, and btstep with extended ranges -- the
+ * GPU tests (tests/test_gpu_oracle_pin.py) run this oracle's phase functions
+ * and the reference kernels on the same inputs and compare them.
  *
  * Array convention: every field is stored exactly as the reference stores it,
  * Fortran column-major with 1-based indices, dimensions (n1, n2[, nk]) with
@@ -71,7 +77,11 @@ void oracle_step(oracle_model *m, int nsteps);
 size_t oracle_field_size(const oracle_model *m, int field);
 int oracle_get(const oracle_model *m, int field, double *out);
 int oracle_set(oracle_model *m, int field, const double *in);
-void oracle_dims(const oracle_model *m, int *out8); /* n1 n2 nk is ie js je ... */
+void oracle_dims(const oracle_model *m, int *out8);
+/* btstep transport ranges: 0 serial (default), 1 extended (CUDA C kernels). */
+void oracle_set_bt_extended(oracle_model *m, int on);
+/* Copy a named grid / control-structure array (see mom6_oracle.c). */
+int oracle_array(const oracle_model *m, const char *name, double *out, size_t count); /* n1 n2 nk is ie js je ... */
 
 /* verify_state of rk2_serial_driver.F90:563-623: out = {mass_init,
  * mass_final, rel_error, max_u, max_v, max_eta, ke_total}. */

@@ -72,6 +72,9 @@ def lib():
         L.oracle_halo_fill.argtypes = [vp, P(d), ctypes.c_int, ctypes.c_int]
         L.oracle_normal.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64]
         L.oracle_normal.restype = d
+        L.oracle_set_bt_extended.argtypes = [vp, ctypes.c_int]
+        L.oracle_array.argtypes = [vp, ctypes.c_char_p, P(d), ctypes.c_size_t]
+        L.oracle_array.restype = ctypes.c_int
         _LIB = L
     return _LIB
 
@@ -178,6 +181,19 @@ class Oracle:
         lib().oracle_compute_transports(self._m, _ptr(u), _ptr(v), _ptr(h),
                                         _ptr(uh), _ptr(vh))
         return uh, vh
+
+    def array(self, name):
+        """A named grid / control-structure array, (n1, n2) or (4, n1, n2)."""
+        n1, n2 = self.shape("eta")
+        four = name in ("f_4_u", "f_4_v")
+        out = np.zeros((4, n1, n2) if four else (n1, n2), order="F")
+        rc = lib().oracle_array(self._m, name.encode(), _ptr(out), out.size)
+        if rc != 0:
+            raise KeyError(name)
+        return out
+
+    def set_bt_extended(self, on):
+        lib().oracle_set_bt_extended(self._m, 1 if on else 0)
 
     def halo_fill(self, f, kind):
         f = np.asfortranarray(f.copy())
