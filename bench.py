@@ -100,7 +100,14 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_setup(args):
+_DIST_DEVICE = "cpu"
+
+
+def dist_setup(args, backend="nccl"):
+    """One process per GPU (torchrun env vars).  The replicas share nothing:
+    the process group only carries the timing barrier and reductions, with a
+    short timeout so that ranks waiting for a failed peer end with an error."""
+    global _DIST_DEVICE
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -108,30 +115,33 @@ def dist_setup(args):
     if world > 1:
         import datetime
 
-        import torch
         import torch.distributed as td
-        torch.cuda.set_device(local)
-        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local)
+            _DIST_DEVICE = f"cuda:{local}"
+        else:
+            _DIST_DEVICE = "cpu"
+        td.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
         dist = td
     return world, rank, local, dist
 
 
-def max_over_ranks(x, dist, local):
+def _reduce(x, dist, op):
     if dist is None:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    t = torch.tensor([x], dtype=torch.float64, device=_DIST_DEVICE)
+    dist.all_reduce(t, op=op)
     return float(t.item())
+
+
+def max_over_ranks(x, dist, local):
+    return x if dist is None else _reduce(x, dist, dist.ReduceOp.MAX)
 
 
 def sum_over_ranks(x, dist, local):
-    if dist is None:
-        return x
-    import torch
-    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return x if dist is None else _reduce(x, dist, dist.ReduceOp.SUM)
 
 
 def barrier(dist):
