@@ -23,9 +23,12 @@ CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", "-Wall"]
 CU_SOURCES = ["k_tendency.cu", "k_vertvisc.cu", "k_continuity.cu", "k_btstep.cu",
               "mom6b_api.cu", "abi_helpers.cu", "abi_barotropic.cu", "abi_hor_visc.cu",
               "abi_vert_visc.cu", "abi_coriolis.cu", "abi_continuity.cu",
-              "cudac_driver.cu"]
+              "cudac_driver.cu", "k_mixed.cu"]
+# the mixed-precision form contracts FMAs; the FP64 files must not
+FMA_SOURCES = {"k_mixed.cu"}
 CXX_SOURCES = ["host_init.cpp"]
-HEADERS = ["common.cuh", "kernels.h", "host_init.h", "abi_common.cuh"]
+HEADERS = ["common.cuh", "kernels.h", "host_init.h", "abi_common.cuh", "tendency_impl.cuh",
+           "vertvisc_impl.cuh"]
 
 
 def _newer(target, deps):
@@ -55,7 +58,10 @@ def build(verbose=False, force=False):
         objs.append(obj)
         if force or _newer(obj, [path] + hdrs):
             if src.endswith(".cu"):
-                cmd = [NVCC] + CU_FLAGS + ["-I", CSRC, "-c", "-o", obj, path]
+                flags = CU_FLAGS
+                if src in FMA_SOURCES:
+                    flags = [f if f != "--fmad=false" else "--fmad=true" for f in CU_FLAGS]
+                cmd = [NVCC] + flags + ["-I", CSRC, "-c", "-o", obj, path]
             else:
                 cmd = ["g++"] + CXX_FLAGS + ["-I", CSRC, "-I", "/usr/local/cuda/include",
                                              "-c", "-o", obj, path]

@@ -277,6 +277,40 @@ struct BTTiles {
     int nbx, nby, tw, th;  // tiles and tile size
 };
 
+// Wait until every tile in nb[0..nnb) has published substep `target` (its
+// tile_flag reached it).  Lanes of warp 0 each watch one neighbour with the
+// clock64 budget; false when the budget ran out or another block failed.
+__device__ __forceinline__ bool wait_neighbours(const BTWork& W, const int* nb, int nnb,
+                                                unsigned int target, long long budget)
+{
+    __shared__ int s_wok;
+    if (threadIdx.x < 32) {
+        int ok = 1;
+        if ((int)threadIdx.x < nnb) {
+            volatile unsigned int* fl = W.tile_flag + nb[threadIdx.x];
+            volatile int* st = W.status;
+            long long t0 = clock64();
+            unsigned int spins = 0;
+            while (*fl < target) {
+                if ((++spins & 63u) == 0) {
+                    if (*st != kDevOk) { ok = 0; break; }
+                    if (clock64() - t0 > budget) {
+                        atomicExch(W.status, kDevTimeout);
+                        ok = 0;
+                        break;
+                    }
+                    if (spins > 4096u) __nanosleep(32);
+                }
+            }
+        }
+        ok = __all_sync(0xffffffffu, ok);
+        __threadfence();
+        if (threadIdx.x == 0) s_wok = ok;
+    }
+    __syncthreads();
+    return s_wok != 0;
+}
+
 template <int NT, bool UNI>
 __global__ void __launch_bounds__(NT, 1)
 k_btstep_tiled(Dims D, Metrics M, UniMetrics U, BTWork W, BTParams P, BTTiles T,
@@ -286,6 +320,8 @@ k_btstep_tiled(Dims D, Metrics M, UniMetrics U, BTWork W, BTParams P, BTTiles T,
     extern __shared__ double smem[];
     const unsigned int nblocks = gridDim.x;
     const int tid = (int)threadIdx.x;
+    const int txl = tid & 31, tyl = tid >> 5;        // 32 x (NT/32) layout over the tile
+    constexpr int TY = NT / 32;
     const int npts = D.n1 * D.n2;
     const int gtid = (int)(blockIdx.x * blockDim.x + threadIdx.x);
     const int gsz = (int)(gridDim.x * blockDim.x);
@@ -310,9 +346,8 @@ k_btstep_tiled(Dims D, Metrics M, UniMetrics U, BTWork W, BTParams P, BTTiles T,
 #define F4U(c, i, j) (UNI ? U.f4u_row[((j) - 1) * 4 + (c) - 1] : MOM6B_F4(M.f_4_u, c, i, j, D))
 #define F4V(c, i, j) (UNI ? U.f4v_row[((j) - 1) * 4 + (c) - 1] : MOM6B_F4(M.f_4_v, c, i, j, D))
 
-    // owned points and their averages
-    // empty when the tile lies beyond the box (both extents clamp to zero)
-    const int ow = max(x1 - x0 + 1, 0), oh = max(y1 - y0 + 1, 0);
+    // averages of the owned points (x0 + txl + 32a, y0 + tyl + TY b), a, b in
+    // {0, 1}, kept in registers; a tile beyond the box owns nothing
     double avu[kBtTileR], avv[kBtTileR];
 #pragma unroll
     for (int r = 0; r < kBtTileR; ++r) avu[r] = avv[r] = 0.0;
@@ -323,7 +358,18 @@ k_btstep_tiled(Dims D, Metrics M, UniMetrics U, BTWork W, BTParams P, BTTiles T,
         W.eta[p] = e; W.ubt[p] = ub; W.vbt[p] = vb;
         W.eta_pred[p] = e; W.ubt_prev[p] = ub; W.vbt_prev[p] = vb;
     }
+    if (tid == 0) W.tile_flag[blockIdx.x] = 0u;
     if (!grid_barrier(W, nblocks, P.spin_budget)) return;
+
+    // the (up to 8) tiles whose points lie in this tile's width-2 halo
+    int nbr[8];
+    int nnb = 0;
+    for (int dyt = -1; dyt <= 1; ++dyt)
+        for (int dxt = -1; dxt <= 1; ++dxt) {
+            const int ax = tx + dxt, ay = ty + dyt;
+            if ((dxt || dyt) && ax >= 0 && ax < T.nbx && ay >= 0 && ay < T.nby)
+                nbr[nnb++] = ay * T.nbx + ax;
+        }
 
     for (int n = 1; n <= P.nstep; ++n) {
         const bool v_first = ((n + P.first_direction) % 2) == 1;
@@ -333,13 +379,20 @@ k_btstep_tiled(Dims D, Metrics M, UniMetrics U, BTWork W, BTParams P, BTTiles T,
         double* ne = (n & 1) ? W.eta_pred : W.eta;
         double* nu = (n & 1) ? W.ubt_prev : W.ubt;
         double* nv = (n & 1) ? W.vbt_prev : W.vbt;
-        // S1: previous state on the local window
-        for (int q = tid; q < LN; q += NT) {
-            int i = lx0 + q % LW, j = ly0 + q / LW;
+        // S1: previous state on the local window.  Owned points carry over in
+        // shared memory (new eta in Sp, new ubt/vbt in Sun/Svn); the halo comes
+        // from the neighbours' published buffers once they finished substep n-1.
+        if (n > 1 && !wait_neighbours(W, nbr, nnb, (unsigned int)(n - 1), P.spin_budget)) return;
+        for (int jl = tyl; jl < LH; jl += TY)
+        for (int il = txl; il < LW; il += 32) {
+            const int q = jl * LW + il, i = lx0 + il, j = ly0 + jl;
             double e = 0.0, ub = 0.0, vb = 0.0;
-            if (i >= 1 && i <= D.n1 && j >= 1 && j <= D.n2) {
+            const bool mine = n > 1 && i >= x0 && i <= x1 && j >= y0 && j <= y1;
+            if (mine) {
+                e = Sp[q]; ub = Sun[q]; vb = Svn[q];
+            } else if (i >= 1 && i <= D.n1 && j >= 1 && j <= D.n2) {
                 int p = (j - 1) * D.n1 + (i - 1);
-                e = ce[p]; ub = cu[p]; vb = cv[p];
+                e = __ldcg(ce + p); ub = __ldcg(cu + p); vb = __ldcg(cv + p);
             }
             Se[q] = e; Su[q] = ub; Sv[q] = vb; Sun[q] = ub; Svn[q] = vb;
         }
@@ -348,9 +401,8 @@ k_btstep_tiled(Dims D, Metrics M, UniMetrics U, BTWork W, BTParams P, BTTiles T,
         {
             int a0 = max(x0 - 1, is), a1 = min(x1 + 1, ie);
             int b0 = max(y0 - 1, js), b1 = min(y1 + 1, je);
-            int w = a1 - a0 + 1, hgt = b1 - b0 + 1;
-            for (int q = tid; q < w * hgt; q += NT) {
-                int i = a0 + q % w, j = b0 + q / w;
+            for (int j = b0 + tyl; j <= b1; j += TY)
+            for (int i = a0 + txl; i <= a1; i += 32) {
                 L(Sp, i, j) = L(Se, i, j) + (P.dtbt * GM(IareaT, i, j)) *
                                                 (((GM(Datu, i - 1, j) * L(Su, i - 1, j)) -
                                                   (GM(Datu, i, j) * L(Su, i, j))) +
@@ -383,23 +435,23 @@ k_btstep_tiled(Dims D, Metrics M, UniMetrics U, BTWork W, BTParams P, BTTiles T,
         if (v_first) {
             int a0 = max(x0 - 1, is), a1 = min(x1 + 1, ie);
             int b0 = max(y0 - 1, js), b1 = min(y1, je - 1);
-            int w = a1 - a0 + 1, hgt = b1 - b0 + 1;
-            for (int q = tid; q < w * hgt; q += NT) upd_v(a0 + q % w, b0 + q / w, Su);
+            for (int j = b0 + tyl; j <= b1; j += TY)
+            for (int i = a0 + txl; i <= a1; i += 32) upd_v(i, j, Su);
             __syncthreads();
             a0 = max(x0 - 1, is); a1 = min(x1, ie - 1);
             b0 = max(y0, js); b1 = min(y1, je);
-            w = a1 - a0 + 1; hgt = b1 - b0 + 1;
-            for (int q = tid; q < w * hgt; q += NT) upd_u(a0 + q % w, b0 + q / w, Svn);
+            for (int j = b0 + tyl; j <= b1; j += TY)
+            for (int i = a0 + txl; i <= a1; i += 32) upd_u(i, j, Svn);
         } else {
             int a0 = max(x0 - 1, is), a1 = min(x1, ie - 1);
             int b0 = max(y0 - 1, js), b1 = min(y1 + 1, je);
-            int w = a1 - a0 + 1, hgt = b1 - b0 + 1;
-            for (int q = tid; q < w * hgt; q += NT) upd_u(a0 + q % w, b0 + q / w, Sv);
+            for (int j = b0 + tyl; j <= b1; j += TY)
+            for (int i = a0 + txl; i <= a1; i += 32) upd_u(i, j, Sv);
             __syncthreads();
             a0 = max(x0, is); a1 = min(x1, ie);
             b0 = max(y0 - 1, js); b1 = min(y1, je - 1);
-            w = a1 - a0 + 1; hgt = b1 - b0 + 1;
-            for (int q = tid; q < w * hgt; q += NT) upd_v(a0 + q % w, b0 + q / w, Sun);
+            for (int j = b0 + tyl; j <= b1; j += TY)
+            for (int i = a0 + txl; i <= a1; i += 32) upd_v(i, j, Sun);
         }
         __syncthreads();
         // S5: transports, eta update and averages on the owned points
@@ -413,16 +465,17 @@ k_btstep_tiled(Dims D, Metrics M, UniMetrics U, BTWork W, BTParams P, BTTiles T,
         };
 #pragma unroll
         for (int r = 0; r < kBtTileR; ++r) {
-            int q = tid + r * NT;
-            if (q >= ow * oh) break;
-            int i = x0 + q % ow, j = y0 + q / ow;
+            const int i = x0 + txl + 32 * (r & 1), j = y0 + tyl + TY * (r >> 1);
+            if (i > x1 || j > y1) continue;
             int p = (j - 1) * D.n1 + (i - 1);
+            double e = L(Se, i, j);
             if (i >= is && i <= ie && j >= js && j <= je) {
-                double e = L(Se, i, j) - P.dtbt * GM(IareaT, i, j) *
-                                             ((uhbt_at(i, j) - uhbt_at(i - 1, j)) +
-                                              (vhbt_at(i, j) - vhbt_at(i, j - 1)));
+                e = L(Se, i, j) - P.dtbt * GM(IareaT, i, j) *
+                                      ((uhbt_at(i, j) - uhbt_at(i - 1, j)) +
+                                       (vhbt_at(i, j) - vhbt_at(i, j - 1)));
                 ne[p] = e;
             }
+            L(Sp, i, j) = e;   // eta_pred is dead: it carries the new eta
             if (i >= is && i <= ie - 1 && j >= js && j <= je) nu[p] = L(Sun, i, j);
             if (i >= is && i <= ie && j >= js && j <= je - 1) nv[p] = L(Svn, i, j);
             if (j >= js && j <= je && i >= iu0 && i <= iu1)
@@ -430,8 +483,14 @@ k_btstep_tiled(Dims D, Metrics M, UniMetrics U, BTWork W, BTParams P, BTTiles T,
             if (j >= jv0 && j <= jv1 && i >= is && i <= ie)
                 avv[r] = avv[r] + L(Svn, i, j) * P.inv_nstep;
         }
-        if (!grid_barrier(W, nblocks, P.spin_budget)) return;
+        // publish substep n: every global write of this tile is done
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            atomicExch(W.tile_flag + blockIdx.x, (unsigned int)n);
+        }
     }
+    if (!grid_barrier(W, nblocks, P.spin_budget)) return;
     // outputs (:296-302); they may alias the inputs
     const double* fe = (P.nstep & 1) ? W.eta_pred : W.eta;
     for (int p = gtid; p < npts; p += gsz) {
@@ -444,9 +503,8 @@ k_btstep_tiled(Dims D, Metrics M, UniMetrics U, BTWork W, BTParams P, BTTiles T,
     }
 #pragma unroll
     for (int r = 0; r < kBtTileR; ++r) {
-        int q = tid + r * NT;
-        if (q >= ow * oh) break;
-        int i = x0 + q % ow, j = y0 + q / ow;
+        const int i = x0 + txl + 32 * (r & 1), j = y0 + tyl + TY * (r >> 1);
+        if (i > x1 || j > y1) continue;
         int p = (j - 1) * D.n1 + (i - 1);
         u_av[p] = avu[r];
         v_av[p] = avv[r];
@@ -481,7 +539,8 @@ static bool tiles_for(const Dims& D, BTTiles& T)
     T.nbx = nbx; T.nby = nby;
     T.tw = (bw + nbx - 1) / nbx; T.th = (bh + nby - 1) / nby;
     size_t smem = (size_t)6 * (T.tw + 3) * (T.th + 3) * sizeof(double);
-    return (long long)T.tw * T.th <= 1024LL * kBtTileR && smem <= 227 * 1024;
+    // each of the 32 x 32 threads owns the points (txl + 32a, tyl + 32b), a, b in {0, 1}
+    return T.tw <= 64 && T.th <= 64 && smem <= 227 * 1024;
 }
 
 
@@ -574,7 +633,7 @@ cudaError_t launch_btstep(const Dims& D, const Metrics& M, const UniMetrics& U,
 // points (n1 * n2), i.e. 6 x 589,824 doubles plus a 256-byte header, about
 // 28.3 MB per GPU that loads this library, held until the process exits.
 constexpr long long kNoAllocMaxPoints = 768LL * 768LL;
-constexpr long long kNoAllocHeader = 32;  // doubles: barrier words and status
+constexpr long long kNoAllocHeader = 160;  // doubles: barrier words, status, tile flags
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocHeader +
                                                           6 * kNoAllocMaxPoints];
 
@@ -605,7 +664,8 @@ static cudaError_t noalloc_scratch(double** out)
 // kind 0: h point, 1: u point (faces is-1 and ie are the basin walls and keep
 // their values), 2: v point (antisymmetric about the wall faces js-1, je).
 // Every halo value is read from non-halo points only, so one pass suffices.
-__global__ void k_halo_fill(Dims D, double* f, int nz, int kind)
+template <typename T>
+__global__ void k_halo_fill(Dims D, T* f, int nz, int kind)
 {
     const int is = D.is, ie = D.ie, js = D.js, je = D.je;
     const int P = ie - is + 1;
@@ -643,11 +703,12 @@ __global__ void k_halo_fill(Dims D, double* f, int nz, int kind)
             sj = (j < js) ? 2 * js - 1 - j : 2 * je + 1 - j;
         }
     }
-    double val = MOM6B_A3(f, si, sj, k, D);
+    T val = MOM6B_A3(f, si, sj, k, D);
     MOM6B_A3(f, i, j, k, D) = (sgn < 0.0) ? -val : val;
 }
 
-cudaError_t launch_halo_fill(const Dims& D, double* f, int nz, int kind, cudaStream_t s)
+template <typename T>
+static cudaError_t launch_halo_fill_t(const Dims& D, T* f, int nz, int kind, cudaStream_t s)
 {
     const int lo_x = (kind == 1) ? D.is - 2 : D.is - 1;
     const int lo_y = (kind == 2) ? D.js - 2 : D.js - 1;
@@ -656,8 +717,18 @@ cudaError_t launch_halo_fill(const Dims& D, double* f, int nz, int kind, cudaStr
     long long total = per_layer * nz;
     int nb = 256;
     long long blocks = (total + nb - 1) / nb;
-    k_halo_fill<<<(unsigned)blocks, nb, 0, s>>>(D, f, nz, kind);
+    k_halo_fill<T><<<(unsigned)blocks, nb, 0, s>>>(D, f, nz, kind);
     return cudaGetLastError();
+}
+
+cudaError_t launch_halo_fill(const Dims& D, double* f, int nz, int kind, cudaStream_t s)
+{
+    return launch_halo_fill_t<double>(D, f, nz, kind, s);
+}
+
+cudaError_t launch_halo_fill_f(const Dims& D, float* f, int nz, int kind, cudaStream_t s)
+{
+    return launch_halo_fill_t<float>(D, f, nz, kind, s);
 }
 
 } // namespace mom6b
@@ -703,6 +774,8 @@ extern "C" int mom6b_btstep_noalloc(
     W.bar_count = (unsigned int*)base;
     W.bar_gen = (unsigned int*)base + 4;
     W.status = (int*)base + 8;
+    W.tile_flag = (unsigned int*)base + 16;   // kBtMaxTiles words, inside the header
+    static_assert(64 + kBtMaxTiles * 4 <= kNoAllocHeader * 8, "noalloc header too small");
     Dims D{};
     D.n1 = n1; D.n2 = n2; D.nk = 1;
     D.is = is; D.ie = ie; D.js = js; D.je = je;

@@ -44,7 +44,11 @@ struct BTWork {
     unsigned int* bar_count;   // grid barrier state (zeroed at allocation)
     unsigned int* bar_gen;
     int* status;               // kDevOk / kDevTimeout
+    unsigned int* tile_flag;   // per-tile substep counters (kBtMaxTiles entries)
 };
+
+// Upper bound on the tiles of the tiled barotropic kernel (one per SM).
+constexpr int kBtMaxTiles = 256;
 
 struct BTParams {
     double dtbt, dgeo_de, trans_wt1, trans_wt2, inv_nstep;
@@ -72,5 +76,22 @@ cudaError_t launch_btstep(const Dims& D, const Metrics& M, const UniMetrics& U,
                           const double* ubt_in, const double* vbt_in, double* u_av,
                           double* v_av, double* eta_av, cudaStream_t s);
 cudaError_t launch_halo_fill(const Dims& D, double* f, int nz, int kind, cudaStream_t s);
+
+// Mixed-precision form (k_mixed.cu): FP32 state and stencils, FP64 column
+// sums, Newton scalars, thickness update and tridiagonal elimination.
+cudaError_t launch_halo_fill_f(const Dims& D, float* f, int nz, int kind, cudaStream_t s);
+cudaError_t launch_tendency_f(const Dims& D, const Metrics& M, const UniMetrics& U,
+                              const float* uin, const float* vin, const float* h,
+                              const float* ubase, const float* vbase, float* uout,
+                              float* vout, float coef, float h_neglect, cudaStream_t s);
+cudaError_t launch_vertvisc_f(const Dims& D, const Metrics& M, float* u, float* v,
+                              const float* h, double dt, const VVParams& P, double* taux_bot,
+                              double* tauy_bot, cudaStream_t s);
+// O2 supplies the FP64 2-D outputs (BT_cont face areas, du_cor); h, uh, h_u
+// are the FP32 3-D outputs.
+cudaError_t launch_continuity_f(const Dims& D, const Metrics& M, const float* u,
+                                const float* hin, float* hW, float* hE, const double* uhbt,
+                                float* h, float* uh, float* h_u, const ContOut& O2,
+                                double* uh_ovl, double dt, double h_min, cudaStream_t s);
 
 }  // namespace mom6b

@@ -263,8 +263,6 @@ extern "C" int mom6b_create(const mom6b_config* cfg, mom6b_model** out)
         return fail(MOM6B_ERR_ARG, "horizontal grid too large");
     if (cfg->precision != MOM6B_FP64 && cfg->precision != MOM6B_MIXED)
         return fail(MOM6B_ERR_ARG, "unknown precision");
-    if (cfg->precision == MOM6B_MIXED)
-        return fail(MOM6B_ERR_ARG, "mixed precision form not built in this library");
     CK(cudaSetDevice(cfg->device));
 
     auto m = std::make_unique<mom6b_model>();
@@ -346,12 +344,14 @@ extern "C" int mom6b_create(const mom6b_config* cfg, mom6b_model** out)
     W.ubt_av = A2(); W.vbt_av = A2();
     {
         void* pb = nullptr;
-        if (cudaMalloc(&pb, 64) != cudaSuccess) return fail(MOM6B_ERR_NOMEM, "device allocation failed");
-        cudaMemset(pb, 0, 64);
+        const size_t nb = 64 + kBtMaxTiles * sizeof(unsigned int);
+        if (cudaMalloc(&pb, nb) != cudaSuccess) return fail(MOM6B_ERR_NOMEM, "device allocation failed");
+        cudaMemset(pb, 0, nb);
         m->allocs.push_back(pb);
         W.bar_count = (unsigned int*)pb;
         W.bar_gen = (unsigned int*)pb + 4;
         W.status = (int*)pb + 8;
+        W.tile_flag = (unsigned int*)pb + 16;
     }
     if (err != cudaSuccess || !m->u || !W.vbt_av)
         return fail(MOM6B_ERR_NOMEM, std::string("device allocation failed: ") + cudaGetErrorString(err));
@@ -364,11 +364,25 @@ extern "C" int mom6b_create(const mom6b_config* cfg, mom6b_model** out)
         std::vector<double> u, v, h0, eta, ubt, vbt, Ru, Rv;
         g.initial_state(u, v, h0, eta, ubt, vbt);
         g.rayleigh(Ru, Rv);
-        if (int rc = upload(m->u, u)) return rc;
-        if (int rc = upload(m->v, v)) return rc;
-        if (int rc = upload(m->h0, h0)) return rc;
-        if (int rc = upload(m->hA, h0)) return rc;
-        if (int rc = upload(m->hB, h0)) return rc;
+        if (cfg->precision == MOM6B_MIXED) {
+            // 3-D state stored as FP32 in the same buffers
+            auto upf = [&](double* dst, const std::vector<double>& src) -> int {
+                std::vector<float> f(src.begin(), src.end());
+                CK(cudaMemcpy(dst, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice));
+                return MOM6B_OK;
+            };
+            if (int rc = upf(m->u, u)) return rc;
+            if (int rc = upf(m->v, v)) return rc;
+            if (int rc = upf(m->h0, h0)) return rc;
+            if (int rc = upf(m->hA, h0)) return rc;
+            if (int rc = upf(m->hB, h0)) return rc;
+        } else {
+            if (int rc = upload(m->u, u)) return rc;
+            if (int rc = upload(m->v, v)) return rc;
+            if (int rc = upload(m->h0, h0)) return rc;
+            if (int rc = upload(m->hA, h0)) return rc;
+            if (int rc = upload(m->hB, h0)) return rc;
+        }
         if (int rc = upload(m->eta, eta)) return rc;
         if (int rc = upload(m->ubt, ubt)) return rc;
         if (int rc = upload(m->vbt, vbt)) return rc;
@@ -384,11 +398,19 @@ extern "C" int mom6b_create(const mom6b_config* cfg, mom6b_model** out)
     CK(cudaEventCreateWithFlags(&m->ev_join, cudaEventDisableTiming));
     if (cfg->bc_fill) {
         const Dims& Dd = m->D;
-        CK(launch_halo_fill(Dd, m->h0, g.nk, 0, m->s3d));
-        CK(launch_halo_fill(Dd, m->hA, g.nk, 0, m->s3d));
-        CK(launch_halo_fill(Dd, m->hB, g.nk, 0, m->s3d));
-        CK(launch_halo_fill(Dd, m->u, g.nk, 1, m->s3d));
-        CK(launch_halo_fill(Dd, m->v, g.nk, 2, m->s3d));
+        if (cfg->precision == MOM6B_MIXED) {
+            CK(launch_halo_fill_f(Dd, (float*)m->h0, g.nk, 0, m->s3d));
+            CK(launch_halo_fill_f(Dd, (float*)m->hA, g.nk, 0, m->s3d));
+            CK(launch_halo_fill_f(Dd, (float*)m->hB, g.nk, 0, m->s3d));
+            CK(launch_halo_fill_f(Dd, (float*)m->u, g.nk, 1, m->s3d));
+            CK(launch_halo_fill_f(Dd, (float*)m->v, g.nk, 2, m->s3d));
+        } else {
+            CK(launch_halo_fill(Dd, m->h0, g.nk, 0, m->s3d));
+            CK(launch_halo_fill(Dd, m->hA, g.nk, 0, m->s3d));
+            CK(launch_halo_fill(Dd, m->hB, g.nk, 0, m->s3d));
+            CK(launch_halo_fill(Dd, m->u, g.nk, 1, m->s3d));
+            CK(launch_halo_fill(Dd, m->v, g.nk, 2, m->s3d));
+        }
         CK(launch_halo_fill(Dd, m->eta, 1, 0, m->s3d));
         CK(launch_halo_fill(Dd, m->ubt, 1, 1, m->s3d));
         CK(launch_halo_fill(Dd, m->vbt, 1, 2, m->s3d));
@@ -455,6 +477,42 @@ static int enqueue_step(mom6b_model* m)
         CK(cudaStreamWaitEvent(s2, m->ev_fork, 0));
     }
 
+    if (c.precision == MOM6B_MIXED) {
+        auto F = [](double* p) { return (float*)p; };
+        const float hvn = (float)hv_neglect;
+        // ---- predictor ----
+        CK(timed(m, s, "tendency", [&] {
+            return launch_tendency_f(D, M, m->U, F(m->u), F(m->v), F(m->h0), F(m->u), F(m->v),
+                                     F(m->up), F(m->vp), (float)dt, hvn, s); }));
+        CK(timed(m, s, "vertvisc", [&] {
+            return launch_vertvisc_f(D, M, F(m->up), F(m->vp), F(m->h0), dt, VV, m->taux_bot,
+                                     m->tauy_bot, s); }));
+        CK(timed(m, s, "continuity", [&] {
+            return launch_continuity_f(D, M, F(m->up), F(m->h0), F(m->hW), F(m->hE), m->uhbt0,
+                                       F(m->hB), F(m->uh), F(m->h_u), OB, m->uh_ovl, dt, h_min,
+                                       s); }));
+        if (c.bc_fill) {
+            CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill_f(D, F(m->hB), g.nk, 0, s); }));
+            CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill_f(D, F(m->up), g.nk, 1, s); }));
+            CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill_f(D, F(m->vp), g.nk, 2, s); }));
+        }
+        // ---- corrector ----
+        CK(timed(m, s, "tendency", [&] {
+            return launch_tendency_f(D, M, m->U, F(m->up), F(m->vp), F(m->hB), F(m->u), F(m->v),
+                                     F(m->u), F(m->v), (float)(0.5 * dt), hvn, s); }));
+        CK(timed(m, s, "vertvisc", [&] {
+            return launch_vertvisc_f(D, M, F(m->u), F(m->v), F(m->hB), 0.5 * dt, VV,
+                                     m->taux_bot, m->tauy_bot, s); }));
+        CK(timed(m, s, "continuity", [&] {
+            return launch_continuity_f(D, M, F(m->u), F(m->hB), F(m->hW), F(m->hE), m->uhbt0,
+                                       F(m->hA), F(m->uh), F(m->h_u), OA, m->uh_ovl, 0.5 * dt,
+                                       h_min, s); }));
+        if (c.bc_fill) {
+            CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill_f(D, F(m->hA), g.nk, 0, s); }));
+            CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill_f(D, F(m->u), g.nk, 1, s); }));
+            CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill_f(D, F(m->v), g.nk, 2, s); }));
+        }
+    } else {
     // ---- predictor ----
     CK(timed(m, s, "tendency", [&] {
         return launch_tendency(D, M, m->U, m->u, m->v, m->h0, m->u, m->v, m->up, m->vp, dt,
@@ -484,6 +542,8 @@ static int enqueue_step(mom6b_model* m)
         CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->hA, g.nk, 0, s); }));
         CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->u, g.nk, 1, s); }));
         CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->v, g.nk, 2, s); }));
+    }
+
     }
 
     // ---- barotropic chain ----
@@ -622,6 +682,17 @@ static double* field_ptr(mom6b_model* m, int f, bool* is3d, bool* writable)
     }
 }
 
+// In the mixed form these 3-D fields are stored as FP32 in their buffers.
+static bool is_f32(const mom6b_model* m, int f)
+{
+    if (m->cfg.precision != MOM6B_MIXED) return false;
+    switch (f) {
+    case MOM6B_F_U: case MOM6B_F_V: case MOM6B_F_H: case MOM6B_F_H0: case MOM6B_F_UH:
+    case MOM6B_F_UP: case MOM6B_F_VP: case MOM6B_F_HU_BT: return true;
+    default: return false;
+    }
+}
+
 extern "C" size_t mom6b_field_size(const mom6b_model* m, int f)
 {
     if (!m) return 0;
@@ -641,7 +712,13 @@ extern "C" int mom6b_get_field(mom6b_model* m, int f, double* host, size_t count
     CK(cudaSetDevice(m->cfg.device));
     CK(cudaStreamSynchronize(m->s3d));
     CK(cudaStreamSynchronize(m->s2d));
-    CK(cudaMemcpy(host, p, n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (is_f32(m, f)) {
+        std::vector<float> tmp(n);
+        CK(cudaMemcpy(tmp.data(), p, n * sizeof(float), cudaMemcpyDeviceToHost));
+        for (size_t q = 0; q < n; ++q) host[q] = (double)tmp[q];
+    } else {
+        CK(cudaMemcpy(host, p, n * sizeof(double), cudaMemcpyDeviceToHost));
+    }
     return check_status(m);
 }
 
@@ -656,10 +733,18 @@ extern "C" int mom6b_set_field(mom6b_model* m, int f, const double* host, size_t
     CK(cudaSetDevice(m->cfg.device));
     CK(cudaStreamSynchronize(m->s3d));
     CK(cudaStreamSynchronize(m->s2d));
-    CK(cudaMemcpy(p, host, n * sizeof(double), cudaMemcpyHostToDevice));
+    const void* src = host;
+    size_t bytes = n * sizeof(double);
+    std::vector<float> tmp;
+    if (is_f32(m, f)) {
+        tmp.assign(host, host + n);
+        src = tmp.data();
+        bytes = n * sizeof(float);
+    }
+    CK(cudaMemcpy(p, src, bytes, cudaMemcpyHostToDevice));
     if (f == MOM6B_F_H0) {  // the step resets h to h0, halo ring included
-        CK(cudaMemcpy(m->hA, host, n * sizeof(double), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(m->hB, host, n * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(m->hA, src, bytes, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(m->hB, src, bytes, cudaMemcpyHostToDevice));
     }
     if (f == MOM6B_F_RAY_U || f == MOM6B_F_RAY_V) {
         std::vector<double> Ru(n), Rv(n);
@@ -718,6 +803,18 @@ extern "C" int mom6b_step_host(mom6b_model* m, int nsteps, double* u, double* v,
     CK(cudaSetDevice(m->cfg.device));
     const size_t n3 = m->grid->plane * (size_t)m->grid->nk, n2 = m->grid->plane;
     cudaStream_t s = m->s3d;
+    if (m->cfg.precision == MOM6B_MIXED) {  // FP32 state: convert through set/get
+        if (u) if (int rc = mom6b_set_field(m, MOM6B_F_U, u, n3)) return rc;
+        if (v) if (int rc = mom6b_set_field(m, MOM6B_F_V, v, n3)) return rc;
+        if (h) if (int rc = mom6b_set_field(m, MOM6B_F_H, h, n3)) return rc;
+        if (eta) if (int rc = mom6b_set_field(m, MOM6B_F_ETA, eta, n2)) return rc;
+        if (int rc = mom6b_step(m, nsteps)) return rc;
+        if (u) if (int rc = mom6b_get_field(m, MOM6B_F_U, u, n3)) return rc;
+        if (v) if (int rc = mom6b_get_field(m, MOM6B_F_V, v, n3)) return rc;
+        if (h) if (int rc = mom6b_get_field(m, MOM6B_F_H, h, n3)) return rc;
+        if (eta) if (int rc = mom6b_get_field(m, MOM6B_F_ETA, eta, n2)) return rc;
+        return check_status(m);
+    }
     CK(cudaStreamSynchronize(m->s2d));
     if (u) CK(cudaMemcpyAsync(m->u, u, n3 * sizeof(double), cudaMemcpyHostToDevice, s));
     if (v) CK(cudaMemcpyAsync(m->v, v, n3 * sizeof(double), cudaMemcpyHostToDevice, s));

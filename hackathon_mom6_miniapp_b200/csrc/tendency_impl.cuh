@@ -1,0 +1,246 @@
+// tendency_impl.cuh -- the fused momentum tendency kernel, templated on the
+// state/arithmetic type R.  R = double is the bit-exact FP64 form (built
+// without FMA contraction in k_tendency.cu); R = float is the mixed form's
+// stencil arithmetic (k_mixed.cu).  Metrics are read as double and rounded
+// to R; literals are written R(...) so the float instantiation never
+// promotes to double.
+//
+// One kernel replaces four phases of the serial driver for one half of the
+// RK2 step:
+//   compute_transports   rk2_serial_driver.F90:544-561
+//   hor_visc             mom6_hor_visc_serial.F90:464-1109 (Laplacian path)
+//   CorAdCalc            mom6_coriolis_serial.F90:112-252 (Sadourny scheme)
+//   velocity update      rk2_serial_driver.F90:257-270 / :337-350
+// so uh, vh, diffu, diffv, CAu and CAv never reach HBM.  Per layer a CTA
+// stages u, v, h on a (TX+2) x (TY+2) tile in shared memory, evaluates the
+// q/str_xy (corner), KE/str_xx (centre) and uh/vh intermediates the tile
+// needs, and writes
+//   uout(I,j) = ubase(I,j) + coef * (CAu + diffu)   I in [is, ie-1], j in [js, je]
+//   vout(i,J) = vbase(i,J) + coef * (CAv + diffv)   i in [is, ie],   J in [js, je-1]
+// Each intermediate is evaluated with the reference's operation order, so
+// the FP64 result equals the serial Fortran bit for bit.  Two reference
+// quirks are reproduced: hArea_u(:, js-1) and hArea_v(is-1, :) are never
+// written by CorAdCalc and enter q as zero (mom6_coriolis_serial.F90:142-152
+// vs :162-168).
+#pragma once
+
+#include "kernels.h"
+
+namespace mom6b {
+
+// UNI selects the uniform-metric instantiation (metrics as scalars, Coriolis
+// per row); otherwise every metric is read from its 2-D array.  Each CTA
+// walks KC consecutive layers of its tile.
+template <int TX, int TY, bool UNI, typename R>
+__global__ void __launch_bounds__(TX * TY)
+k_tendency(Dims D, Metrics M, UniMetrics U, const R* __restrict__ uin,
+           const R* __restrict__ vin, const R* __restrict__ h,
+           const R* ubase, const R* vbase, R* uout, R* vout,
+           R coef, R h_neglect, int k0, int KC)
+{
+    constexpr int SX = TX + 2, SY = TY + 2;  // staged inputs: [i0-1, i0+TX] x [j0-1, j0+TY]
+    constexpr int CX = TX + 1, CY = TY + 1;  // intermediates
+    __shared__ R s_u[SY][SX], s_v[SY][SX], s_h[SY][SX];
+    __shared__ R s_q[CY][CX], s_sxy[CY][CX];   // corners  [i0-1, i0+TX-1] x [j0-1, j0+TY-1]
+    __shared__ R s_ke[CY][CX], s_sxx[CY][CX];  // centres  [i0, i0+TX] x [j0, j0+TY]
+    __shared__ R s_uh[CY][CX];                 // u-faces  [i0-1, i0+TX-1] x [j0, j0+TY]
+    __shared__ R s_vh[CY][CX];                 // v-faces  [i0, i0+TX] x [j0-1, j0+TY-1]
+
+    const int i0 = D.is + (int)blockIdx.x * TX;
+    const int j0 = D.js + (int)blockIdx.y * TY;
+    const int tid = (int)threadIdx.y * TX + (int)threadIdx.x;
+    const int kb = k0 + (int)blockIdx.z * KC;
+    const int ke = (kb + KC - 1 < D.nk) ? kb + KC - 1 : D.nk;
+  for (int k = kb; k <= ke; ++k) {
+    const size_t koff = (size_t)(k - 1) * (size_t)D.plane;
+    if (k > kb) __syncthreads();  // the previous layer's tiles are consumed
+
+    // ---- stage u, v, h --------------------------------------------------
+    for (int p = tid; p < SX * SY; p += TX * TY) {
+        int r = p / SX, c = p - r * SX;
+        int i = i0 - 1 + c, j = j0 - 1 + r;
+        R uu = R(0.0), vv = R(0.0), hh = R(0.0);
+        if (i <= D.n1 && j <= D.n2) {
+            size_t o = koff + (size_t)(j - 1) * D.n1 + (i - 1);
+            uu = uin[o]; vv = vin[o]; hh = h[o];
+        }
+        s_u[r][c] = uu; s_v[r][c] = vv; s_h[r][c] = hh;
+    }
+    __syncthreads();
+
+#define SU(i, j) s_u[(j) - (j0 - 1)][(i) - (i0 - 1)]
+#define SV(i, j) s_v[(j) - (j0 - 1)][(i) - (i0 - 1)]
+#define SH(i, j) s_h[(j) - (j0 - 1)][(i) - (i0 - 1)]
+#define G2(a, i, j) ((R)(UNI ? U.a : MOM6B_A2(M.a, i, j, D)))
+#define COR(i, j) ((R)(UNI ? U.cor_row[(j) - 1] : MOM6B_A2(M.CoriolisBu, i, j, D)))
+
+    // ---- intermediates ----------------------------------------------------
+    for (int p = tid; p < CX * CY; p += TX * TY) {
+        int r = p / CX, c = p - r * CX;
+        // corner point (I, J) = (i0-1+c, j0-1+r): q and str_xy
+        {
+            int I = i0 - 1 + c, J = j0 - 1 + r;
+            R qv = R(0.0), sxy = R(0.0);
+            if (I + 1 <= D.n1 && J + 1 <= D.n2) {
+                R v0 = SV(I, J), v1 = SV(I + 1, J);
+                R u0 = SU(I, J), u1 = SU(I, J + 1);
+                R h00 = SH(I, J), h10 = SH(I + 1, J), h01 = SH(I, J + 1),
+                       h11 = SH(I + 1, J + 1);
+                // CorAdCalc: circulation, areas, PV (mom6_coriolis_serial.F90:134-168)
+                R dvdx = (v1 * G2(dyCv, I + 1, J)) - (v0 * G2(dyCv, I, J));
+                R dudy = (u1 * G2(dxCu, I, J + 1)) - (u0 * G2(dxCu, I, J));
+                R rel = G2(mask2dBu, I, J) * (dvdx - dudy) * G2(IareaBu, I, J);
+                R absv = COR(I, J) + rel;
+                R aT00 = G2(areaT, I, J), aT10 = G2(areaT, I + 1, J),
+                       aT01 = G2(areaT, I, J + 1), aT11 = G2(areaT, I + 1, J + 1);
+                R hAu0 = (J >= D.js) ? R(0.5) * ((aT00 * h00) + (aT10 * h10)) : R(0.0);
+                R hAu1 = R(0.5) * ((aT01 * h01) + (aT11 * h11));
+                R hAv0 = (I >= D.is) ? R(0.5) * ((aT00 * h00) + (aT01 * h01)) : R(0.0);
+                R hAv1 = R(0.5) * ((aT10 * h10) + (aT11 * h11));
+                R hArea_q = (hAu0 + hAu1) + (hAv0 + hAv1);
+                R Ih_q = G2(Area_q, I, J) / (hArea_q + R(1.0e-20));
+                qv = absv * Ih_q;
+                // hor_visc: shearing strain and stress at q-points (:513-520, :544, :579, :964, :1050)
+                R dvdx_v = G2(DY_dxBu, I, J) *
+                                ((v1 * G2(IdyCv, I + 1, J)) - (v0 * G2(IdyCv, I, J)));
+                R dudy_v = G2(DX_dyBu, I, J) *
+                                ((u1 * G2(IdxCu, I, J + 1)) - (u0 * G2(IdxCu, I, J)));
+                R mBu = G2(mask2dBu, I, J);
+                R sh_xy = mBu * (dvdx_v + dudy_v);
+                R hq = R(0.25) * ((h00 + h11) + (h10 + h01));
+                sxy = -(G2(Kh_xy, I, J) * sh_xy);
+                sxy = sxy * (hq * mBu * G2(red_xy, I, J));
+            }
+            s_q[r][c] = qv;
+            s_sxy[r][c] = sxy;
+        }
+        // centre point (i, j) = (i0+c, j0+r): KE and str_xx
+        {
+            int i = i0 + c, j = j0 + r;
+            R ke = R(0.0), sxx = R(0.0);
+            if (i <= D.n1 && j <= D.n2) {
+                R uc = SU(i, j), um = SU(i - 1, j), vc = SV(i, j), vm = SV(i, j - 1);
+                ke = R(0.25) *
+                     ((G2(dyCu, i, j) * (uc * uc) + G2(dyCu, i - 1, j) * (um * um)) +
+                      (G2(dxCv, i, j) * (vc * vc) + G2(dxCv, i, j - 1) * (vm * vm))) /
+                     G2(areaT, i, j);
+                R dudx = G2(DY_dxT, i, j) *
+                              ((G2(IdyCu, i, j) * uc) - (G2(IdyCu, i - 1, j) * um));
+                R dvdy = G2(DX_dyT, i, j) *
+                              ((G2(IdxCv, i, j) * vc) - (G2(IdxCv, i, j - 1) * vm));
+                R sh_xx = dudx - dvdy;
+                sxx = -(G2(Kh_xx, i, j) * sh_xx);
+                sxx = sxx * (SH(i, j) * G2(red_xx, i, j));
+            }
+            s_ke[r][c] = ke;
+            s_sxx[r][c] = sxx;
+        }
+        // transports (compute_transports uses min(i+1, ied), min(j+1, jed))
+        {
+            int I = i0 - 1 + c, J = j0 + r;
+            R uhv = R(0.0);
+            if (I <= D.n1 && J <= D.n2) {
+                int Ip = I + 1 < D.ied ? I + 1 : D.ied;
+                R hp = (Ip - (i0 - 1) < SX) ? SH(Ip, J) : R(0.0);
+                uhv = SU(I, J) * R(0.5) * (SH(I, J) + hp) * G2(dyCu, I, J);
+            }
+            s_uh[r][c] = uhv;
+            int i = i0 + c, j = j0 - 1 + r;
+            R vhv = R(0.0);
+            if (i <= D.n1 && j <= D.n2) {
+                int Jp = j + 1 < D.jed ? j + 1 : D.jed;
+                R hp = (Jp - (j0 - 1) < SY) ? SH(i, Jp) : R(0.0);
+                vhv = SV(i, j) * R(0.5) * (SH(i, j) + hp) * G2(dxCv, i, j);
+            }
+            s_vh[r][c] = vhv;
+        }
+    }
+    __syncthreads();
+
+#define Q(I, J) s_q[(J) - (j0 - 1)][(I) - (i0 - 1)]
+#define SXY(I, J) s_sxy[(J) - (j0 - 1)][(I) - (i0 - 1)]
+#define KE(i, j) s_ke[(j) - j0][(i) - i0]
+#define SXX(i, j) s_sxx[(j) - j0][(i) - i0]
+#define UH(I, J) s_uh[(J) - j0][(I) - (i0 - 1)]
+#define VH(i, j) s_vh[(j) - (j0 - 1)][(i) - i0]
+
+    const int I = i0 + (int)threadIdx.x;
+    const int j = j0 + (int)threadIdx.y;
+    // ---- u point (I, j) ---------------------------------------------------
+    if (I <= D.ie - 1 && j <= D.je) {
+        R IdxCu = G2(IdxCu, I, j);
+        R KEx = (KE(I + 1, j) - KE(I, j)) * IdxCu;
+        R CAu = R(0.25) *
+                         ((Q(I, j) * (VH(I + 1, j) + VH(I, j))) +
+                          (Q(I, j - 1) * (VH(I, j - 1) + VH(I + 1, j - 1)))) *
+                         IdxCu -
+                     KEx;
+        R h_u = R(0.5) * (G2(mask2dT, I, j) * SH(I, j) + G2(mask2dT, I + 1, j) * SH(I + 1, j));
+        R diffu = ((IdxCu * ((G2(dx2q, I, j - 1) * SXY(I, j - 1)) -
+                                  (G2(dx2q, I, j) * SXY(I, j))) +
+                         G2(IdyCu, I, j) * ((G2(dy2h, I, j) * SXX(I, j)) -
+                                            (G2(dy2h, I + 1, j) * SXX(I + 1, j)))) *
+                        G2(IareaCu, I, j)) /
+                       (h_u + h_neglect);
+        size_t o = koff + (size_t)(j - 1) * D.n1 + (I - 1);
+        uout[o] = ubase[o] + coef * (CAu + diffu);
+    }
+    // ---- v point (i, J) = (I, j) -------------------------------------------
+    if (I <= D.ie && j <= D.je - 1) {
+        const int i = I, J = j;
+        R IdyCv = G2(IdyCv, i, J);
+        R KEy = (KE(i, J + 1) - KE(i, J)) * IdyCv;
+        R CAv = R(-0.25) *
+                         ((Q(i - 1, J) * (UH(i - 1, J) + UH(i - 1, J + 1))) +
+                          (Q(i, J) * (UH(i, J) + UH(i, J + 1)))) *
+                         IdyCv -
+                     KEy;
+        R h_v = R(0.5) * (G2(mask2dT, i, J) * SH(i, J) + G2(mask2dT, i, J + 1) * SH(i, J + 1));
+        R diffv = ((IdyCv * ((G2(dy2q, i - 1, J) * SXY(i - 1, J)) -
+                                  (G2(dy2q, i, J) * SXY(i, J))) -
+                         G2(IdxCv, i, J) * ((G2(dx2h, i, J) * SXX(i, J)) -
+                                            (G2(dx2h, i, J + 1) * SXX(i, J + 1)))) *
+                        G2(IareaCv, i, J)) /
+                       (h_v + h_neglect);
+        size_t o = koff + (size_t)(J - 1) * D.n1 + (i - 1);
+        vout[o] = vbase[o] + coef * (CAv + diffv);
+    }
+  }  // layer loop
+#undef SU
+#undef SV
+#undef SH
+#undef G2
+#undef COR
+#undef Q
+#undef SXY
+#undef KE
+#undef SXX
+#undef UH
+#undef VH
+}
+
+constexpr int kTendTX = 32, kTendTY = 8, kTendKC = 5;
+
+// Host launcher: one CTA per (TX x TY) tile of the compute domain and chunk of
+// kTendKC layers.
+template <typename R>
+cudaError_t launch_tendency_t(const Dims& D, const Metrics& M, const UniMetrics& U,
+                              const R* uin, const R* vin, const R* h, const R* ubase,
+                              const R* vbase, R* uout, R* vout, R coef, R h_neglect,
+                              cudaStream_t s)
+{
+    constexpr int TY = kTendTY;
+    int nx = D.ie - D.is + 1, ny = D.je - D.js + 1;
+    dim3 block(kTendTX, TY, 1);
+    int nchunks = (D.nk + kTendKC - 1) / kTendKC;
+    dim3 grid((nx + kTendTX - 1) / kTendTX, (ny + TY - 1) / TY, nchunks);
+    if (U.valid)
+        k_tendency<kTendTX, TY, true, R><<<grid, block, 0, s>>>(
+            D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, kTendKC);
+    else
+        k_tendency<kTendTX, TY, false, R><<<grid, block, 0, s>>>(
+            D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, kTendKC);
+    return cudaGetLastError();
+}
+
+} // namespace mom6b

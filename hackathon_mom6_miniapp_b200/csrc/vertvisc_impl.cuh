@@ -1,0 +1,268 @@
+// vertvisc_impl.cuh -- the prefetching vertical viscosity kernel, templated
+// on the storage type R of u, v and h.  Every coefficient and the whole
+// tridiagonal elimination are computed in double whatever R is: R = double
+// is the bit-exact FP64 form (k_vertvisc.cu); R = float is the mixed form
+// (k_mixed.cu), which loads and stores FP32 and eliminates in FP64.
+//
+// Restates vert_visc_coef + vert_visc_apply of the serial module
+// (mom6_vert_visc_serial.F90:138-287 and :394-506) as the driver calls them
+// (rk2_serial_driver.F90:276-277, :356-357).
+#pragma once
+
+#include <cstdlib>
+
+#include "kernels.h"
+
+namespace mom6b {
+
+template <typename C>
+__device__ __forceinline__ C vv_botfn(C z2) {
+    return C(1.0) / (C(1.0) + C(0.09) * z2 * z2 * z2 * z2 * z2 * z2);
+}
+
+// Prefetching variant (the default): one per-column local array (botfn(z_i(m)),
+// then c1(m)); h_harm is recomputed in sweep 2 from the same two thicknesses
+// and the same expression, so it is bit-identical to the sweep-1 value.  The
+// sweeps are latency-bound chains, so every sweep loads the inputs of CH
+// layers into registers before it computes them: one memory latency per CH
+// layers instead of one per layer.
+// Layers whose inputs one prefetch brings in.
+constexpr int kVvChunk = 4;
+
+template <int KMAX, int CH, typename R>
+__global__ void __launch_bounds__(128)
+k_vertvisc_pf(Dims D, Metrics M, R* __restrict__ u, R* __restrict__ v,
+              const R* __restrict__ h, double dt, VVParams P,
+              double* __restrict__ taux_bot, double* __restrict__ tauy_bot)
+{
+    // Coefficients (h_harm, z_i, botfn, hvel, a(K)) are computed in the
+    // storage type R; the tridiagonal elimination (b1, d1, c1, the eliminated
+    // velocity and the back substitution) always in double.
+    using C = R;
+    double slot[KMAX + 2];   // botfn(z_i(m)), then c1(m)
+    const int nz = D.nk;
+    const int nrow_u = D.je - D.js + 1;
+    bool is_u = (int)blockIdx.y < nrow_u;
+    int i, j, di, dj;
+    R* vel;
+    const double *mask, *tau, *Ray;
+    const unsigned char* ray_on;
+    double* tbot;
+    if (is_u) {  // u columns: I in [is-1, ie], j in [js, je]
+        j = D.js + (int)blockIdx.y;
+        i = D.is - 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+        if (i > D.ie) return;
+        di = 1; dj = 0;
+        vel = u; mask = M.mask2dCu; tau = M.taux; Ray = M.Ray_u;
+        ray_on = M.ray_layer_u; tbot = taux_bot;
+    } else {     // v columns: i in [is, ie], J in [js-1, je]
+        j = D.js - 1 + ((int)blockIdx.y - nrow_u);
+        i = D.is + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+        if (i > D.ie) return;
+        di = 0; dj = 1;
+        vel = v; mask = M.mask2dCv; tau = M.tauy; Ray = M.Ray_v;
+        ray_on = M.ray_layer_v; tbot = tauy_bot;
+    }
+    const double msk = MOM6B_A2(mask, i, j, D);
+    if (!(msk > 0.0)) return;  // vert_visc_apply leaves masked columns alone
+
+    const size_t plane = (size_t)D.plane;
+    const R* hc = h + (size_t)(j - 1) * D.n1 + (i - 1);               // h(i, j, 1)
+    const R* hn_ = h + (size_t)(j - 1 + dj) * D.n1 + (i - 1 + di);     // neighbour
+    R* vc = vel + (size_t)(j - 1) * D.n1 + (i - 1);
+    const double* rc = Ray + (size_t)(j - 1) * D.n1 + (i - 1);
+    const C hn = (C)P.h_neglect, I_Hbbl = (C)P.I_Hbbl, Kv = (C)P.Kv, Kv_ml = (C)P.Kv_ml;
+    const C Kv_extra_bbl = (C)P.Kv_extra_bbl, Hmix = (C)P.Hmix;
+
+    // ---- sweep 1: h_harm and z_i bottom-up (vert_visc_coef :160-179) -----
+    C z = C(0.0);
+    slot[nz + 1] = vv_botfn(C(0.0));
+    for (int kt = nz; kt >= 2; kt -= CH) {
+        C a0[CH], a1[CH];
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            int k = kt - c;
+            if (k >= 2) {
+                a0[c] = hc[(size_t)(k - 1) * plane];
+                a1[c] = hn_[(size_t)(k - 1) * plane];
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            int k = kt - c;
+            if (k >= 2) {
+                C h_harm = C(2.0) * a0[c] * a1[c] / (a0[c] + a1[c] + hn);
+                z = z + h_harm * I_Hbbl;
+                slot[k] = vv_botfn(z);
+            }
+        }
+    }
+
+    // hvel(k): harmonic mean, blended toward the arithmetic mean where the
+    // flow opposes the thickness gradient (:162-177)
+    // bf_up = botfn(z_i(k+1)) (slot k+1 of sweep 1)
+    auto hvel = [&](C bf_up, C h0, C h1, C vk) -> C {
+        C h_harm = C(2.0) * h0 * h1 / (h0 + h1 + hn);
+        C hv = h_harm;
+        if (vk * (h1 - h0) < C(0.0)) {
+            C bf = bf_up;
+            C h_arith = C(0.5) * (h1 + h0);
+            hv = (C(1.0) - bf) * h_harm + bf * h_arith;
+        }
+        return hv;
+    };
+    // a(K2) for K2 in [2, nz] given the running z_top (:185-202)
+    // bf_K2 = botfn(z_i(K2)) (slot K2 of sweep 1)
+    auto a_of = [&](C bf_K2, C z_top, C hv_lo, C hv_up) -> C {
+        C Kv_tot = Kv;
+        if (z_top < Hmix) {
+            C topfn = C(1.0) - z_top / Hmix;
+            Kv_tot = Kv_tot + (Kv_ml - Kv) * topfn;
+        }
+        Kv_tot = Kv_tot + Kv_extra_bbl * bf_K2;
+        C h_shear = C(0.5) * (hv_lo + hv_up + hn);
+        return Kv_tot / h_shear;
+    };
+    const C a_bot_num = Kv + Kv_extra_bbl;
+
+    // ---- sweep 2: coefficients + forward elimination, top-down -----------
+    const double dt_Rho0 = dt / kRho0;
+    const double sfc_stress = dt_Rho0 * MOM6B_A2(tau, i, j, D) * msk;
+    const double v1 = vc[0];
+    C hv_k = hvel((C)slot[2], hc[0], hn_[0], (C)v1);
+    C z_top = C(0.0);
+    C hv_next, a_next;
+    double vnext = 0.0;                      // vel(k + 1) before elimination
+    if (nz >= 2) {
+        vnext = vc[plane];
+        hv_next = hvel((C)slot[3], hc[plane], hn_[plane], (C)vnext);
+        z_top = z_top + hv_k;
+        a_next = a_of((C)slot[2], z_top, hv_next, hv_k);
+    } else {
+        hv_next = C(0.0);
+        a_next = a_bot_num / (C(0.5) * hv_k + hn);
+    }
+    double a_k = 0.0;  // a(1) = 0, surface
+    double Rayk = ray_on[0] ? rc[0] : 0.0;
+    double h_u = (double)(hv_k + hn);
+    double b_denom_1 = h_u + dt * (Rayk + a_k);
+    double b1 = 1.0 / (b_denom_1 + dt * (double)a_next);
+    double d1 = b_denom_1 * b1;
+    double u_prev = b1 * (h_u * v1 + sfc_stress);
+    vc[0] = (R)u_prev;
+    for (int kt = 2; kt <= nz; kt += CH) {
+        // layers kt .. kt+CH-1 are eliminated; they need h and vel of the
+        // layer below each (k + 1) and Ray of k
+        // and botfn of interfaces k+1, k+2 (slots kt+1 .. kt+CH+1, read
+        // before this chunk overwrites slots kt .. kt+CH-1 with c1)
+        C p0[CH], p1[CH], pb[CH + 1];
+        double pv[CH], pr[CH];
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            int k = kt + c;
+            if (k < nz) {
+                p0[c] = hc[(size_t)k * plane];
+                p1[c] = hn_[(size_t)k * plane];
+                pv[c] = vc[(size_t)k * plane];
+            }
+            if (k <= nz) pr[c] = ray_on[k - 1] ? rc[(size_t)(k - 1) * plane] : 0.0;
+        }
+#pragma unroll
+        for (int c = 0; c <= CH; ++c)
+            if (kt + 1 + c <= nz + 1) pb[c] = (C)slot[kt + 1 + c];
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            int k = kt + c;
+            if (k <= nz) {
+                const double vk = vnext;     // vel(k) before elimination
+                a_k = (double)a_next;
+                hv_k = hv_next;
+                if (k < nz) {
+                    vnext = pv[c];
+                    hv_next = hvel(pb[c + 1], p0[c], p1[c], (C)vnext);
+                    z_top = z_top + hv_k;
+                    a_next = a_of(pb[c], z_top, hv_next, hv_k);
+                } else {
+                    a_next = a_bot_num / (C(0.5) * hv_k + hn);
+                }
+                Rayk = pr[c];
+                double c1 = dt * a_k * b1;
+                slot[k] = c1;
+                h_u = (double)(hv_k + hn);
+                b_denom_1 = h_u + dt * (Rayk + a_k * d1);
+                b1 = 1.0 / (b_denom_1 + dt * (double)a_next);
+                d1 = b_denom_1 * b1;
+                u_prev = (h_u * vk + dt * a_k * u_prev) * b1;
+                vc[(size_t)(k - 1) * plane] = (R)u_prev;
+            }
+        }
+    }
+    const double a_bottom = (double)a_next;
+
+    // ---- sweep 3: back substitution (:447-449) ----------------------------
+    double u_below = u_prev;
+    for (int kt = nz - 1; kt >= 1; kt -= CH) {
+        double pv[CH], pc[CH];
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            int k = kt - c;
+            if (k >= 1) {
+                pv[c] = vc[(size_t)(k - 1) * plane];
+                pc[c] = slot[k + 1];
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            int k = kt - c;
+            if (k >= 1) {
+                double uk = pv[c] + pc[c] * u_below;
+                vc[(size_t)(k - 1) * plane] = (R)uk;
+                u_below = uk;
+            }
+        }
+    }
+    // bottom stress (:452-458)
+    double tb = kRho0 * u_prev * a_bottom;
+    for (int k = 1; k <= nz; ++k)
+        if (ray_on[k - 1]) {
+            size_t o = (size_t)(k - 1) * plane;
+            tb = tb + kRho0 * rc[o] * (double)vc[o];
+        }
+    tbot[(size_t)(j - 1) * D.n1 + (i - 1)] = tb;
+}
+
+template <int KMAX, typename R>
+static cudaError_t launch_vv_pf(const Dims& D, const Metrics& M, R* u, R* v, const R* h,
+                                double dt, const VVParams& P, double* taux_bot,
+                                double* tauy_bot, cudaStream_t s)
+{
+    const int nb = 128;
+    int ncol = D.ie - D.is + 2;
+    int nrows = (D.je - D.js + 1) + (D.je - D.js + 2);
+    dim3 grid((ncol + nb - 1) / nb, nrows, 1);
+    static int chunk = -1;
+    if (chunk < 0) {
+        const char* e = getenv("MOM6B_VV_CHUNK");
+        chunk = e ? atoi(e) : kVvChunk;
+    }
+    if (chunk == 2)
+        k_vertvisc_pf<KMAX, 2, R><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P, taux_bot, tauy_bot);
+    else if (chunk == 8)
+        k_vertvisc_pf<KMAX, 8, R><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P, taux_bot, tauy_bot);
+    else
+        k_vertvisc_pf<KMAX, 4, R><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P, taux_bot, tauy_bot);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_vertvisc_pf_t(const Dims& D, const Metrics& M, R* u, R* v, const R* h,
+                                 double dt, const VVParams& P, double* taux_bot,
+                                 double* tauy_bot, cudaStream_t s)
+{
+    if (D.nk <= 80) return launch_vv_pf<80>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s);
+    if (D.nk <= 128) return launch_vv_pf<128>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s);
+    if (D.nk <= 256) return launch_vv_pf<256>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s);
+    return launch_vv_pf<1024>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s);
+}
+
+} // namespace mom6b
