@@ -12,6 +12,18 @@ domain (the path does not shard across GPUs: replicas only, weak scaling);
 the timed region is bracketed by a barrier and device synchronisation and
 the time is the maximum over ranks.
 
+The line's "mixed" object measures the mixed-precision form (FP32 state,
+fluxes and stencils; FP64 column sums, thickness update, vertical elimination
+and barotropic loop) on the same workload and protocol, with its speed-up
+over the FP64 form and its per-field relative L2 error against the FP64 form
+of the same seed after 10 steps at 720x720x75 and after 100 steps at
+1440x1080x75 (the mixed-form configuration).
+
+The "ensemble" object advances 64 independent domains of uneven size
+(ni = nj in {90, ..., 360}, nk in {25, 50, 75}, bt_nsteps = 30, mixed form)
+together, one launch per phase for all of them with launch shapes from the
+autotuner, and reports aggregate cell-layer updates/s over 50 steps.
+
 --impl reference times the reference's CPU implementation of the path on the
 host cores: the C restatement of the serial Fortran driver (the Fortran
 itself cannot be compiled here), on rank 0 only.
@@ -204,6 +216,123 @@ def measured_traffic():
     return out
 
 
+MIXED_FIELDS = ("h", "u", "v", "eta", "ubt_av", "vbt_av")
+
+
+def _rel_l2(a, b):
+    import numpy as np
+    d = float(np.linalg.norm((a - b).ravel()))
+    n = float(np.linalg.norm(b.ravel()))
+    return d / n if n > 0 else d
+
+
+def mixed_errors(ni, nj, nsteps, seed, local):
+    """Per-field relative L2 error of the mixed form against the FP64 form
+    (bit-identical to the serial driver) after nsteps from the same seed."""
+    from hackathon_mom6_miniapp_b200 import FP64, INIT_CFG, MIXED, Model
+    ref = Model(ni, nj, NK, BT, INIT_CFG, seed=seed, dt=600.0, device=local,
+                precision=FP64, use_graph=True)
+    ref.step(nsteps)
+    want = {f: ref.get(f) for f in MIXED_FIELDS}
+    ref.close()
+    mx = Model(ni, nj, NK, BT, INIT_CFG, seed=seed, dt=600.0, device=local,
+               precision=MIXED, use_graph=True)
+    mx.step(nsteps)
+    errs = {f: _rel_l2(mx.get(f), want[f]) for f in MIXED_FIELDS}
+    mx.close()
+    return errs
+
+
+def run_mixed(args, world, rank, local, dist, fp64_ms_per_step):
+    """The mixed form (FP32 state, fluxes and stencils; FP64 column sums,
+    thickness update, vertical elimination and barotropic loop) on the same
+    workload and timing protocol, with its per-field error."""
+    import torch
+    from hackathon_mom6_miniapp_b200 import INIT_CFG, MIXED, Model
+    m = Model(NI, NJ, NK, BT, INIT_CFG, seed=rank, dt=600.0, device=local,
+              precision=MIXED, use_graph=not args.no_graph)
+    stream = torch.cuda.ExternalStream(m.stream(), device=f"cuda:{local}")
+    m.step(args.warmup)
+    m.synchronize()
+    barrier(dist)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    m.step(args.steps)
+    e1.record(stream)
+    m.synchronize()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), dist, local)
+    m.kernel_timing(True)
+    m.step(2)
+    m.synchronize()
+    kt = {k: m.kernel_time_ms(k) for k in ("tendency", "vertvisc", "continuity", "btstep",
+                                           "halo_fill")}
+    m.close()
+    out = {"value": world * args.steps / (ms / 1000.0), "unit": "steps/s",
+           "ms_per_step": ms / args.steps,
+           "speedup_vs_fp64": fp64_ms_per_step / (ms / args.steps),
+           "kernel_ms_per_step": {k: v[0] * v[1] / 2 for k, v in kt.items()},
+           "dtype": "f32 state/stencils, f64 sums/thickness update/elimination/btstep"}
+    if rank == 0:
+        out["rel_l2_720x720x75_10_steps"] = mixed_errors(NI, NJ, 10, 0, local)
+        if not args.no_cfg2:
+            out["rel_l2_1440x1080x75_100_steps"] = mixed_errors(1440, 1080, 100, 0, local)
+        out["error_reference"] = "FP64 form of the same seed (bit-identical to the oracle)"
+    return out
+
+
+def ensemble_domains(n=64, seed=0):
+    """The batched-ensemble configuration: n domains, square ni = nj drawn
+    uniformly from {90, 120, ..., 360} and nk from {25, 50, 75}, each built
+    like the 180x180 case (seeded beta plane, bt_nsteps = 30) with its own
+    seed."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    sizes = rng.choice(np.arange(90, 361, 30), size=n)
+    depths = rng.choice(np.array([25, 50, 75]), size=n)
+    return [dict(ni=int(a), nj=int(a), nk=int(k), bt_nsteps=30, seed=q)
+            for q, (a, k) in enumerate(zip(sizes, depths))]
+
+
+def run_ensemble(args, world, rank, local, dist):
+    """64 uneven domains advanced together (one launch per phase for all of
+    them, launch shapes from the autotuner): aggregate cell-layer updates/s
+    over 50 steps."""
+    import torch
+    from hackathon_mom6_miniapp_b200 import Ensemble
+    doms = ensemble_domains(64, seed=rank)
+    e = Ensemble(doms, device=local)
+    t_tune = time.perf_counter()
+    best = e.autotune(reps=2)
+    t_tune = time.perf_counter() - t_tune
+    stream = torch.cuda.ExternalStream(e.stream(), device=f"cuda:{local}")
+    e.step(3)
+    e.synchronize()
+    barrier(dist)
+    steps = 50
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    n0 = e.launch_count()
+    e0.record(stream)
+    e.step(steps)
+    e1.record(stream)
+    e.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), dist, local)
+    launches = e.launch_count() - n0
+    cells = e.cell_layers()
+    out = {"value": world * cells * steps / (ms / 1000.0), "unit": "cell-layer updates/s",
+           "domains": len(doms), "steps": steps, "bt_nsteps": 30, "ms_per_step": ms / steps,
+           "cell_layers": cells, "launches_per_step": launches / steps,
+           "tuning": e.tuning(), "autotune_best_ms": best, "autotune_s": t_tune,
+           "sizes": "ni=nj from {90..360 step 30}, nk from {25,50,75}, numpy "
+                    "default_rng(rank) draws, seeds 0..63",
+           "dtype": "mixed form (f32 state, f64 sums/thickness update/elimination/btstep)"}
+    e.close()
+    return out
+
+
 def run_ours(args, world, rank, local, dist):
     import numpy as np
     import torch
@@ -287,6 +416,10 @@ def run_ours(args, world, rank, local, dist):
     t1 = time.perf_counter()
     e2e_res = world * args.steps / max_over_ranks(t1 - t0, dist, local)
 
+    mixed = None if args.no_mixed else run_mixed(args, world, rank, local, dist,
+                                                   ms / args.steps)
+    ensemble = None if args.no_ensemble else run_ensemble(args, world, rank, local, dist)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         r, sample, cores = cpu_reference_rate(1)
@@ -322,6 +455,8 @@ def run_ours(args, world, rank, local, dist):
                 "e2e_resident": {"value": e2e_res, "unit": "steps/s",
                                  "h2d_bytes_per_step": bytes_h2d / args.steps,
                                  "d2h_bytes_per_step": bytes_d2h / args.steps},
+                "mixed": mixed,
+                "ensemble": ensemble,
                 "gpu_launches": launches,
                 "clocks": ck}
         print(json.dumps(line), flush=True)
@@ -348,6 +483,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true",
+                    help="skip the mixed-precision form's line items")
+    ap.add_argument("--no-ensemble", action="store_true",
+                    help="skip the 64-domain ensemble line item")
+    ap.add_argument("--no-cfg2", action="store_true",
+                    help="skip the mixed form's error at 1440x1080x75 after 100 steps")
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--profile-case", type=int, default=0,
                     help="run N steps of a ni=nj=N domain only (for ncu captures)")

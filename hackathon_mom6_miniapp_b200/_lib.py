@@ -84,6 +84,21 @@ def library():
     L.mom6b_cudac_field_size.restype = ctypes.c_size_t
     L.mom6b_cudac_get_field.argtypes = [vp, ctypes.c_int, P(d), ctypes.c_size_t]
     L.mom6b_cudac_destroy.argtypes = [vp]
+    L.mom6b_ensemble_create.argtypes = [ctypes.c_int, P(Config), P(vp)]
+    L.mom6b_ensemble_destroy.argtypes = [vp]
+    L.mom6b_ensemble_size.argtypes = [vp]
+    L.mom6b_ensemble_step.argtypes = [vp, ctypes.c_int]
+    L.mom6b_ensemble_synchronize.argtypes = [vp]
+    L.mom6b_ensemble_stream.argtypes = [vp, P(vp)]
+    L.mom6b_ensemble_launch_count.argtypes = [vp]
+    L.mom6b_ensemble_launch_count.restype = i64
+    L.mom6b_ensemble_member.argtypes = [vp, ctypes.c_int]
+    L.mom6b_ensemble_member.restype = vp
+    L.mom6b_ensemble_get_field.argtypes = [vp, ctypes.c_int, ctypes.c_int, P(d),
+                                           ctypes.c_size_t]
+    L.mom6b_ensemble_autotune.argtypes = [vp, ctypes.c_int, P(d)]
+    L.mom6b_ensemble_get_tuning.argtypes = [vp, P(ctypes.c_int)]
+    L.mom6b_ensemble_set_tuning.argtypes = [vp, P(ctypes.c_int)]
     L.mom6b_last_error.restype = ctypes.c_char_p
     L.mom6b_version.restype = ctypes.c_char_p
     _LIB = L
@@ -203,6 +218,113 @@ class Model:
         _check(library().mom6b_kernel_time_ms(self._m, name.encode(), ctypes.byref(ms),
                                               ctypes.byref(n)))
         return ms.value, n.value
+
+
+def make_config(ni=180, nj=180, nk=75, bt_nsteps=30, init_mode=INIT_CFG, seed=0, dt=None,
+                Kh=None, bc_fill=None, precision=FP64, device=0, use_graph=False):
+    """A mom6b_config with the defaults of init_mode and the given overrides."""
+    c = Config()
+    _check(library().mom6b_config_default(ctypes.byref(c), init_mode))
+    c.ni, c.nj, c.nk, c.bt_nsteps, c.seed = ni, nj, nk, bt_nsteps, seed
+    if dt is not None:
+        c.dt = dt
+    if Kh is not None:
+        c.Kh = Kh
+    if bc_fill is not None:
+        c.bc_fill = int(bc_fill)
+    c.precision, c.device, c.use_graph = precision, device, int(use_graph)
+    return c
+
+
+TUNING_KEYS = ["tend_tile", "tend_kc", "vv_nb", "vv_ch", "ppm_nb", "faces_nb", "bt_tile"]
+
+
+class Ensemble:
+    """Many independent domains of any sizes advanced together in the mixed
+    form, one launch per phase for all of them (mom6b_ensemble_*).
+
+    domains: list of dicts of make_config arguments (ni, nj, nk, bt_nsteps,
+    seed, init_mode, dt, ...); precision is MIXED for every domain."""
+
+    def __init__(self, domains, device=0, use_graph=True):
+        L = library()
+        n = len(domains)
+        arr = (Config * n)()
+        for q, kw in enumerate(domains):
+            kw = dict(kw)
+            kw["precision"] = MIXED
+            kw["device"] = device
+            arr[q] = make_config(**kw)
+        self.cfgs = [arr[q] for q in range(n)]
+        h = ctypes.c_void_p()
+        _check(L.mom6b_ensemble_create(n, arr, ctypes.byref(h)))
+        self._e = h
+        self.n = n
+        self.dims = []
+        for q in range(n):
+            dims = (ctypes.c_int * 8)()
+            _check(L.mom6b_dims(L.mom6b_ensemble_member(self._e, q), dims))
+            self.dims.append(tuple(dims))
+        if not use_graph:
+            raise ValueError("the ensemble always steps through its CUDA graph")
+
+    def close(self):
+        if getattr(self, "_e", None):
+            library().mom6b_ensemble_destroy(self._e)
+            self._e = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self):
+        return self.n
+
+    def step(self, n=1):
+        _check(library().mom6b_ensemble_step(self._e, int(n)))
+
+    def synchronize(self):
+        _check(library().mom6b_ensemble_synchronize(self._e))
+
+    def stream(self):
+        p = ctypes.c_void_p()
+        _check(library().mom6b_ensemble_stream(self._e, ctypes.byref(p)))
+        return p.value
+
+    def launch_count(self):
+        return int(library().mom6b_ensemble_launch_count(self._e))
+
+    def shape(self, d, name):
+        n1, n2, nk = self.dims[d][0], self.dims[d][1], self.dims[d][2]
+        return (n1, n2, nk) if name in FIELDS_3D else (n1, n2)
+
+    def get(self, d, name):
+        a = np.zeros(self.shape(d, name), dtype=np.float64, order="F")
+        _check(library().mom6b_ensemble_get_field(self._e, int(d), FID[name], _dptr(a), a.size))
+        return a
+
+    def cell_layers(self):
+        """Compute cells x layers of all domains (the unit of the ensemble rate)."""
+        tot = 0
+        for c in self.cfgs:
+            tot += c.ni * c.nj * c.nk
+        return tot
+
+    def autotune(self, reps=3):
+        out = (ctypes.c_double * 5)()
+        _check(library().mom6b_ensemble_autotune(self._e, int(reps), out))
+        return dict(zip(["tendency", "vertvisc", "ppm", "faces", "btstep"], list(out)))
+
+    def tuning(self):
+        out = (ctypes.c_int * 7)()
+        _check(library().mom6b_ensemble_get_tuning(self._e, out))
+        return dict(zip(TUNING_KEYS, list(out)))
+
+    def set_tuning(self, t):
+        vals = (ctypes.c_int * 7)(*[int(t[k]) for k in TUNING_KEYS])
+        _check(library().mom6b_ensemble_set_tuning(self._e, vals))
 
 
 class CudaCDriver:

@@ -24,6 +24,7 @@
 #include <cstdlib>
 
 #include "../../include/mom6b.h"
+#include "halo_impl.cuh"
 #include "kernels.h"
 
 namespace mom6b {
@@ -516,6 +517,247 @@ k_btstep_tiled(Dims D, Metrics M, UniMetrics U, BTWork W, BTParams P, BTTiles T,
 #undef F4V
 }
 
+// ---------------------------------------------------------------------------
+// Ensemble variant: the barotropic loops of many domains in one cooperative
+// launch.
+// ---------------------------------------------------------------------------
+// Every domain is split into tiles as above (EnsBtGeo, at most 64 x 64
+// points); the tiles of all domains form one list and CTA c processes tiles
+// c, c + gridDim.x, ... in that order at every substep.  A tile waits only for
+// the tiles of its own domain that border it (flag >= n - 1), so the domains
+// advance independently; a CTA that owns several tiles keeps nothing on chip
+// between substeps: the owned points are re-read from the published buffers
+// and the time averages accumulate in the domain's ubt_av / vbt_av work arrays.
+// Waiting on substep n - 1 only cannot deadlock: the CTA at the lowest
+// (substep, tile position) always finds every tile done with the previous
+// substep.  The evaluation order of every point is the serial one.
+// Largest d with tstart[d] <= t (the domain of global tile t).
+__device__ __forceinline__ int ens_tile_domain(const int* __restrict__ tstart, int n, int t)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(tstart + mid) <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <int NT, bool UNI>
+__global__ void __launch_bounds__(NT, 1)
+k_btstep_ens(const EnsDomain* __restrict__ doms, const EnsBtGeo* __restrict__ geo,
+             const int* __restrict__ tstart, int ndom, int ntiles, int max_tw, int max_th,
+             int call, int max_nstep, BTWork C)
+{
+    extern __shared__ double smem[];
+    __shared__ __align__(16) EnsDomain E;
+    const unsigned int nblocks = gridDim.x;
+    const int tid = (int)threadIdx.x;
+    const int txl = tid & 31, tyl = tid >> 5;
+    constexpr int TY = NT / 32;
+    const int gtid = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int gsz = (int)(gridDim.x * blockDim.x);
+    const int LWm = max_tw + 3, LHm = max_th + 3;
+    const int LNm = LWm * LHm;
+    double* Se = smem;
+    double* Su = Se + LNm;
+    double* Sv = Su + LNm;
+    double* Sp = Sv + LNm;
+    double* Sun = Sp + LNm;
+    double* Svn = Sun + LNm;
+
+    // init (:199-207) of every domain: both buffers hold the input state, the
+    // averages start at zero
+    for (int d = 0; d < ndom; ++d) {
+        const EnsDomain& Q = doms[d];
+        const double* ein = call ? Q.eta_av : Q.eta;
+        const double* uin = call ? Q.ubt_av : Q.ubt;
+        const double* vin = call ? Q.vbt_av : Q.vbt;
+        const BTWork W = Q.W;
+        const int npts = Q.D.n1 * Q.D.n2;
+        for (int p = gtid; p < npts; p += gsz) {
+            double e = ein[p], ub = uin[p], vb = vin[p];
+            W.eta[p] = e; W.ubt[p] = ub; W.vbt[p] = vb;
+            W.eta_pred[p] = e; W.ubt_prev[p] = ub; W.vbt_prev[p] = vb;
+            W.ubt_av[p] = 0.0; W.vbt_av[p] = 0.0;
+        }
+    }
+    for (int t = gtid; t < ntiles; t += gsz) C.tile_flag[t] = 0u;
+    if (!grid_barrier(C, nblocks, 4000000000LL)) return;
+
+    for (int n = 1; n <= max_nstep; ++n) {
+        for (int t = (int)blockIdx.x; t < ntiles; t += (int)nblocks) {
+            const int d = ens_tile_domain(tstart, ndom, t);
+            __syncthreads();   // the previous tile's reads of E are done
+            {
+                const unsigned long long* src = (const unsigned long long*)(doms + d);
+                unsigned long long* dst = (unsigned long long*)&E;
+                for (int w = tid; w < (int)(sizeof(EnsDomain) / 8); w += NT) dst[w] = __ldg(src + w);
+            }
+            __syncthreads();
+            const Dims& D = E.D;
+            const Metrics& M = E.M;
+            const UniMetrics& U = E.U;
+            const BTParams& P = E.P;
+            const BTWork& W = E.W;
+            if (n > P.nstep) continue;
+            const EnsBtGeo G = geo[d];
+            const int lt = t - G.t0;
+            const int tx = lt % G.nbx, ty = lt / G.nbx;
+            const int is = D.is, ie = D.ie, js = D.js, je = D.je;
+            const int iu0 = P.extended ? is - 1 : is, iu1 = P.extended ? ie : ie - 1;
+            const int jv0 = P.extended ? js - 1 : js, jv1 = P.extended ? je : je - 1;
+            const int x0 = is - 1 + tx * G.tw, y0 = js - 1 + ty * G.th;
+            const int x1 = min(x0 + G.tw - 1, ie), y1 = min(y0 + G.th - 1, je);
+            const int lx0 = x0 - 2, ly0 = y0 - 2;
+            const int LW = G.tw + 3, LH = G.th + 3;
+#define L(a, i, j) a[((j) - ly0) * LW + ((i) - lx0)]
+#define GM(f, i, j) (UNI ? U.f : MOM6B_A2(M.f, i, j, D))
+#define F4U(c, i, j) (UNI ? U.f4u_row[((j) - 1) * 4 + (c) - 1] : MOM6B_F4(M.f_4_u, c, i, j, D))
+#define F4V(c, i, j) (UNI ? U.f4v_row[((j) - 1) * 4 + (c) - 1] : MOM6B_F4(M.f_4_v, c, i, j, D))
+            const bool v_first = ((n + P.first_direction) % 2) == 1;
+            const double* ce = (n & 1) ? W.eta : W.eta_pred;
+            const double* cu = (n & 1) ? W.ubt : W.ubt_prev;
+            const double* cv = (n & 1) ? W.vbt : W.vbt_prev;
+            double* ne = (n & 1) ? W.eta_pred : W.eta;
+            double* nu = (n & 1) ? W.ubt_prev : W.ubt;
+            double* nv = (n & 1) ? W.vbt_prev : W.vbt;
+            // neighbours of this tile in its own domain
+            int nbr[8];
+            int nnb = 0;
+            for (int dyt = -1; dyt <= 1; ++dyt)
+                for (int dxt = -1; dxt <= 1; ++dxt) {
+                    const int ax = tx + dxt, ay = ty + dyt;
+                    if ((dxt || dyt) && ax >= 0 && ax < G.nbx && ay >= 0 && ay < G.nby)
+                        nbr[nnb++] = G.t0 + ay * G.nbx + ax;
+                }
+            if (n > 1 && !wait_neighbours(C, nbr, nnb, (unsigned int)(n - 1), P.spin_budget))
+                return;
+            // S1: the previous state on the window, owned points included
+            for (int jl = tyl; jl < LH; jl += TY)
+            for (int il = txl; il < LW; il += 32) {
+                const int q = jl * LW + il, i = lx0 + il, j = ly0 + jl;
+                double e = 0.0, ub = 0.0, vb = 0.0;
+                if (i >= 1 && i <= D.n1 && j >= 1 && j <= D.n2) {
+                    int p = (j - 1) * D.n1 + (i - 1);
+                    e = __ldcg(ce + p); ub = __ldcg(cu + p); vb = __ldcg(cv + p);
+                }
+                Se[q] = e; Su[q] = ub; Sv[q] = vb; Sun[q] = ub; Svn[q] = vb;
+            }
+            __syncthreads();
+            // S2: eta_pred on [x0-1, x1+1] x [y0-1, y1+1] within [is, ie] x [js, je]
+            {
+                int a0 = max(x0 - 1, is), a1 = min(x1 + 1, ie);
+                int b0 = max(y0 - 1, js), b1 = min(y1 + 1, je);
+                for (int j = b0 + tyl; j <= b1; j += TY)
+                for (int i = a0 + txl; i <= a1; i += 32) {
+                    L(Sp, i, j) = L(Se, i, j) + (P.dtbt * GM(IareaT, i, j)) *
+                                                    (((GM(Datu, i - 1, j) * L(Su, i - 1, j)) -
+                                                      (GM(Datu, i, j) * L(Su, i, j))) +
+                                                     ((GM(Datv, i, j - 1) * L(Sv, i, j - 1)) -
+                                                      (GM(Datv, i, j) * L(Sv, i, j))));
+                }
+            }
+            __syncthreads();
+            auto upd_u = [&](int i, int j, const double* Vsrc) {
+                double PFu = ((L(Sp, i, j) * GM(gtot_E, i, j)) -
+                              (L(Sp, i + 1, j) * GM(gtot_W, i + 1, j))) *
+                             P.dgeo_de * GM(IdxCu, i, j);
+                double Cor_u = (((F4U(4, i, j) * L(Vsrc, i + 1, j)) +
+                                 (F4U(1, i, j) * L(Vsrc, i, j - 1))) +
+                                ((F4U(3, i, j) * L(Vsrc, i, j)) +
+                                 (F4U(2, i, j) * L(Vsrc, i + 1, j - 1))));
+                L(Sun, i, j) = GM(bt_rem_u, i, j) * (L(Su, i, j) + P.dtbt * (Cor_u + PFu));
+            };
+            auto upd_v = [&](int i, int j, const double* Usrc) {
+                double PFv = ((L(Sp, i, j) * GM(gtot_N, i, j)) -
+                              (L(Sp, i, j + 1) * GM(gtot_S, i, j + 1))) *
+                             P.dgeo_de * GM(IdyCv, i, j);
+                double Cor_v = -1.0 * (((F4V(1, i, j) * L(Usrc, i - 1, j)) +
+                                        (F4V(4, i, j) * L(Usrc, i, j + 1))) +
+                                       ((F4V(2, i, j) * L(Usrc, i, j)) +
+                                        (F4V(3, i, j) * L(Usrc, i - 1, j + 1))));
+                L(Svn, i, j) = GM(bt_rem_v, i, j) * (L(Sv, i, j) + P.dtbt * (Cor_v + PFv));
+            };
+            // S3 / S4: the two velocity updates on the regions the tile needs
+            if (v_first) {
+                int a0 = max(x0 - 1, is), a1 = min(x1 + 1, ie);
+                int b0 = max(y0 - 1, js), b1 = min(y1, je - 1);
+                for (int j = b0 + tyl; j <= b1; j += TY)
+                for (int i = a0 + txl; i <= a1; i += 32) upd_v(i, j, Su);
+                __syncthreads();
+                a0 = max(x0 - 1, is); a1 = min(x1, ie - 1);
+                b0 = max(y0, js); b1 = min(y1, je);
+                for (int j = b0 + tyl; j <= b1; j += TY)
+                for (int i = a0 + txl; i <= a1; i += 32) upd_u(i, j, Svn);
+            } else {
+                int a0 = max(x0 - 1, is), a1 = min(x1, ie - 1);
+                int b0 = max(y0 - 1, js), b1 = min(y1 + 1, je);
+                for (int j = b0 + tyl; j <= b1; j += TY)
+                for (int i = a0 + txl; i <= a1; i += 32) upd_u(i, j, Sv);
+                __syncthreads();
+                a0 = max(x0, is); a1 = min(x1, ie);
+                b0 = max(y0 - 1, js); b1 = min(y1, je - 1);
+                for (int j = b0 + tyl; j <= b1; j += TY)
+                for (int i = a0 + txl; i <= a1; i += 32) upd_v(i, j, Sun);
+            }
+            __syncthreads();
+            // S5: transports, eta update and averages on the owned points
+            auto uhbt_at = [&](int i, int j) -> double {
+                if (i < iu0 || i > iu1 || j < js || j > je) return 0.0;
+                return GM(Datu, i, j) * (P.trans_wt1 * L(Sun, i, j) + P.trans_wt2 * L(Su, i, j));
+            };
+            auto vhbt_at = [&](int i, int j) -> double {
+                if (j < jv0 || j > jv1 || i < is || i > ie) return 0.0;
+                return GM(Datv, i, j) * (P.trans_wt1 * L(Svn, i, j) + P.trans_wt2 * L(Sv, i, j));
+            };
+#pragma unroll
+            for (int r = 0; r < kBtTileR; ++r) {
+                const int i = x0 + txl + 32 * (r & 1), j = y0 + tyl + TY * (r >> 1);
+                if (i > x1 || j > y1) continue;
+                int p = (j - 1) * D.n1 + (i - 1);
+                if (i >= is && i <= ie && j >= js && j <= je)
+                    ne[p] = L(Se, i, j) - P.dtbt * GM(IareaT, i, j) *
+                                              ((uhbt_at(i, j) - uhbt_at(i - 1, j)) +
+                                               (vhbt_at(i, j) - vhbt_at(i, j - 1)));
+                if (i >= is && i <= ie - 1 && j >= js && j <= je) nu[p] = L(Sun, i, j);
+                if (i >= is && i <= ie && j >= js && j <= je - 1) nv[p] = L(Svn, i, j);
+                if (j >= js && j <= je && i >= iu0 && i <= iu1)
+                    W.ubt_av[p] = W.ubt_av[p] + L(Sun, i, j) * P.inv_nstep;
+                if (j >= jv0 && j <= jv1 && i >= is && i <= ie)
+                    W.vbt_av[p] = W.vbt_av[p] + L(Svn, i, j) * P.inv_nstep;
+            }
+#undef L
+#undef GM
+#undef F4U
+#undef F4V
+            // publish substep n of tile t: every global write of it is done
+            __syncthreads();
+            if (tid == 0) {
+                __threadfence();
+                atomicExch(C.tile_flag + t, (unsigned int)n);
+            }
+        }
+    }
+    if (!grid_barrier(C, nblocks, 4000000000LL)) return;
+    // outputs (:296-302); they may alias the inputs.  The averages are zero
+    // outside their ranges (the init of :204-205).
+    for (int d = 0; d < ndom; ++d) {
+        const EnsDomain& Q = doms[d];
+        const BTWork W = Q.W;
+        double* u_av = Q.ubt_av;
+        double* v_av = Q.vbt_av;
+        double* e_out = call ? Q.eta : Q.eta_av;
+        const double* fe = (Q.P.nstep & 1) ? W.eta_pred : W.eta;
+        const int npts = Q.D.n1 * Q.D.n2;
+        for (int p = gtid; p < npts; p += gsz) {
+            e_out[p] = fe[p];
+            u_av[p] = W.ubt_av[p];
+            v_av[p] = W.vbt_av[p];
+        }
+    }
+}
+
 static int g_bt_blocks = 0;
 
 static cudaError_t init_bt_blocks()
@@ -620,6 +862,54 @@ cudaError_t launch_btstep(const Dims& D, const Metrics& M, const UniMetrics& U,
                                           : (const void*)k_btstep<false>, args);
 }
 
+EnsBtGeo ens_bt_geometry(const Dims& D, int max_edge)
+{
+    EnsBtGeo G;
+    const int bw = D.ie - D.is + 2, bh = D.je - D.js + 2;
+    G.nbx = (bw + max_edge - 1) / max_edge;
+    G.nby = (bh + max_edge - 1) / max_edge;
+    G.tw = (bw + G.nbx - 1) / G.nbx;
+    G.th = (bh + G.nby - 1) / G.nby;
+    G.t0 = 0;
+    return G;
+}
+
+cudaError_t launch_ens_btstep(const EnsDomain* doms, const EnsBtGeo* geo, const int* tstart,
+                              int n, int ntiles, int max_tw, int max_th, int call,
+                              int max_nstep, const BTWork& ctl, bool uni, cudaStream_t s)
+{
+    if (ntiles <= 0) return cudaSuccess;
+    if (max_tw > 64 || max_th > 64) return cudaErrorInvalidValue;
+    cudaError_t e0 = init_bt_blocks();
+    if (e0 != cudaSuccess) return e0;
+    const int NT = 1024;
+    const size_t smem = (size_t)6 * (max_tw + 3) * (max_th + 3) * sizeof(double);
+    const void* fn = uni ? (const void*)k_btstep_ens<NT, true> : (const void*)k_btstep_ens<NT, false>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, NT, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    int blocks = per_sm * g_bt_blocks;
+    if (blocks > ntiles) blocks = ntiles;
+    BTWork C = ctl;
+    void* args[] = {(void*)&doms, (void*)&geo, (void*)&tstart, (void*)&n, (void*)&ntiles,
+                    (void*)&max_tw, (void*)&max_th, (void*)&call, (void*)&max_nstep, (void*)&C};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks, 1, 1);
+    cfg.blockDim = dim3(NT, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelExC(&cfg, fn, args);
+}
+
 // ---------------------------------------------------------------------------
 // Allocation-free barotropic entry point
 // ---------------------------------------------------------------------------
@@ -659,52 +949,12 @@ static cudaError_t noalloc_scratch(double** out)
 }
 
 // ---------------------------------------------------------------------------
-// halo / boundary fill: periodic in i, solid walls in j
+// halo / boundary fill (halo_impl.cuh): one thread per halo point
 // ---------------------------------------------------------------------------
-// kind 0: h point, 1: u point (faces is-1 and ie are the basin walls and keep
-// their values), 2: v point (antisymmetric about the wall faces js-1, je).
-// Every halo value is read from non-halo points only, so one pass suffices.
 template <typename T>
 __global__ void k_halo_fill(Dims D, T* f, int nz, int kind)
 {
-    const int is = D.is, ie = D.ie, js = D.js, je = D.je;
-    const int P = ie - is + 1;
-    const int lo_x = (kind == 1) ? is - 2 : is - 1;   // x halo: i <= lo_x or i > ie
-    const int lo_y = (kind == 2) ? js - 2 : js - 1;   // y halo: j <= lo_y or j > je
-    const int nxh = lo_x + (D.n1 - ie);               // halo columns
-    const int nyh = lo_y + (D.n2 - je);               // halo rows
-    // enumerate: halo rows (all i) first, then halo columns of the other rows
-    const long long per_layer = (long long)nyh * D.n1 + (long long)nxh * (D.n2 - nyh);
-    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= per_layer * nz) return;
-    const int k = (int)(t / per_layer) + 1;
-    long long r = t % per_layer;
-    int i, j;
-    if (r < (long long)nyh * D.n1) {
-        int row = (int)(r / D.n1);
-        i = (int)(r % D.n1) + 1;
-        j = row < lo_y ? row + 1 : je + 1 + (row - lo_y);
-    } else {
-        r -= (long long)nyh * D.n1;
-        int col = (int)(r % nxh);
-        j = lo_y + 1 + (int)(r / nxh);
-        i = col < lo_x ? col + 1 : ie + 1 + (col - lo_x);
-    }
-    const bool xh = (i <= lo_x) || (i > ie);
-    const bool yh = (j <= lo_y) || (j > je);
-    int si = xh ? (i < is ? i + P : i - P) : i;
-    int sj = j;
-    double sgn = 1.0;
-    if (yh) {
-        if (kind == 2) {
-            sj = (j < js) ? 2 * (js - 1) - j : 2 * je - j;
-            sgn = -1.0;
-        } else {
-            sj = (j < js) ? 2 * js - 1 - j : 2 * je + 1 - j;
-        }
-    }
-    T val = MOM6B_A3(f, si, sj, k, D);
-    MOM6B_A3(f, i, j, k, D) = (sgn < 0.0) ? -val : val;
+    halo_fill_point<T>(D, f, nz, kind, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 template <typename T>

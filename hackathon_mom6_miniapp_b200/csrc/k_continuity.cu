@@ -196,78 +196,107 @@ __device__ __forceinline__ double flux_eval(const FaceCol<EI>& F, const LayerVal
     return zero ? 0.0 : uh;
 }
 
-// zonal_flux_adjust for one face (:813-903).  When uh_out is given the flux of
-// every evaluated iteration is stored (the present(uh_3d) call).
-template <int CH, typename EI>
-__device__ double flux_adjust_face(const FaceCol<EI>& F, int nz, double dt,
-                                   double uhbt, double uh_tot_0,
-                                   double duhdu_tot_0, double du_max_CFL,
-                                   double du_min_CFL, double tol_eta_dt_fac,
-                                   double* uh_out, size_t uh_stride)
+// State of one zonal_flux_adjust iteration (:813-903) for one face.
+struct Newton {
+    double du, du_max, du_min, uh_err, duhdu_tot, uh_err_best;
+    bool live;  // the iteration loop has not exited yet
+};
+
+__device__ __forceinline__ Newton newton_start(double uh_err, double duhdu_tot,
+                                               double du_max_CFL, double du_min_CFL, bool live)
 {
-    const int max_itts = 20;
-    const double tol_eta_cs = 1.0e-12, tol_vel = 3.0e8;
-    double du = 0.0;
-    bool do_I = true;
-    double du_max = du_max_CFL, du_min = du_min_CFL;
-    double uh_err = uh_tot_0 - uhbt;
-    double duhdu_tot = duhdu_tot_0;
-    double uh_err_best = fabs(uh_err);
-    for (int itt = 1; itt <= max_itts; ++itt) {
-        double tol_eta;
-        if (itt <= 1) tol_eta = F32(1e-6) * tol_eta_cs;
-        else if (itt == 2) tol_eta = F32(1e-4) * tol_eta_cs;
-        else if (itt == 3) tol_eta = F32(1e-2) * tol_eta_cs;
-        else tol_eta = tol_eta_cs;
-        if (uh_err > 0.0) du_max = du;
-        else if (uh_err < 0.0) du_min = du;
-        else do_I = false;
-        if (do_I) {
-            double ae = fabs(uh_err);
-            if ((tol_eta_dt_fac * ae > tol_eta) ||
-                ((ae > tol_vel * duhdu_tot) || (ae > uh_err_best))) {
-                double ddu = -(uh_err / duhdu_tot);
-                double du_prev = du;
-                du = du + ddu;
-                if (fabs(ddu) < F32(1.0e-15) * fabs(du)) {
-                    do_I = false;
-                } else if (ddu > 0.0) {
-                    if (du >= du_max) {
-                        du = 0.5 * (du_prev + du_max);
-                        if (du_max - du_prev < F32(1.0e-15) * fabs(du)) do_I = false;
-                    }
-                } else {
-                    if (du <= du_min) {
-                        du = 0.5 * (du_prev + du_min);
-                        if (du_prev - du_min < F32(1.0e-15) * fabs(du)) do_I = false;
-                    }
-                }
-            } else {
-                do_I = false;
-            }
-        }
-        if (!do_I) break;
-        const bool update = itt < max_itts;
-        if (update || uh_out) {
-            double e = -uhbt, dt_sum = 0.0;
-            for_layers<CH>(F, nz, [&](int k, const LayerVals& L) {
-                double hm;
-                double uhk = flux_eval(F, L, L.u + du, dt, hm);
-                double duhdu = F.dy * hm;
-                if (uh_out) uh_out[(size_t)(k - 1) * uh_stride] = uhk;
-                e = e + uhk;
-                dt_sum = dt_sum + duhdu;
-            });
-            if (update) {
-                uh_err = e;
-                duhdu_tot = dt_sum;
-                uh_err_best = dmin(uh_err_best, fabs(uh_err));
-            }
-        }
-    }
-    return du;
+    return Newton{0.0, du_max_CFL, du_min_CFL, uh_err, duhdu_tot, fabs(uh_err), live};
 }
 
+// Iteration itt of zonal_flux_adjust up to its exit test (:829-883): bounds
+// the root, takes the Newton (or bisection) step; returns do_I.
+__device__ __forceinline__ bool newton_iter(Newton& S, int itt, double tol_eta_dt_fac)
+{
+    const double tol_eta_cs = 1.0e-12, tol_vel = 3.0e8;
+    double tol_eta;
+    if (itt <= 1) tol_eta = F32(1e-6) * tol_eta_cs;
+    else if (itt == 2) tol_eta = F32(1e-4) * tol_eta_cs;
+    else if (itt == 3) tol_eta = F32(1e-2) * tol_eta_cs;
+    else tol_eta = tol_eta_cs;
+    bool do_I = true;
+    if (S.uh_err > 0.0) S.du_max = S.du;
+    else if (S.uh_err < 0.0) S.du_min = S.du;
+    else do_I = false;
+    if (do_I) {
+        double ae = fabs(S.uh_err);
+        if ((tol_eta_dt_fac * ae > tol_eta) ||
+            ((ae > tol_vel * S.duhdu_tot) || (ae > S.uh_err_best))) {
+            double ddu = -(S.uh_err / S.duhdu_tot);
+            double du_prev = S.du;
+            S.du = S.du + ddu;
+            if (fabs(ddu) < F32(1.0e-15) * fabs(S.du)) {
+                do_I = false;
+            } else if (ddu > 0.0) {
+                if (S.du >= S.du_max) {
+                    S.du = 0.5 * (du_prev + S.du_max);
+                    if (S.du_max - du_prev < F32(1.0e-15) * fabs(S.du)) do_I = false;
+                }
+            } else {
+                if (S.du <= S.du_min) {
+                    S.du = 0.5 * (du_prev + S.du_min);
+                    if (du_prev - S.du_min < F32(1.0e-15) * fabs(S.du)) do_I = false;
+                }
+            }
+        } else {
+            do_I = false;
+        }
+    }
+    return do_I;
+}
+
+// The two zonal_flux_adjust solves of one face run in lockstep: A drives the
+// face transport toward uhbt and stores the transports of every evaluated
+// iteration in uh (the present(uh_3d) call, :307); B is set_zonal_BT_cont's
+// zero-transport solve (:1002), live only when it is needed.  The two are
+// independent iterations, each with its own operation sequence; sharing the
+// column passes only halves how often the column is read.
+template <int CH, typename EI>
+__device__ void flux_adjust_pair(const FaceCol<EI>& F, int nz, double dt, double uhbt,
+                                 double tol_eta_dt_fac, Newton& A, Newton& B,
+                                 double* uh_out, size_t uh_stride)
+{
+    const int max_itts = 20;
+    for (int itt = 1; itt <= max_itts; ++itt) {
+        if (A.live) A.live = newton_iter(A, itt, tol_eta_dt_fac);
+        if (B.live) B.live = newton_iter(B, itt, tol_eta_dt_fac);
+        const bool update = itt < max_itts;
+        const bool pa = A.live;            // A always stores, so it evaluates
+        const bool pb = B.live && update;  // B evaluates only to update
+        if (!pa && !pb) break;
+        const double duA = A.du, duB = B.du;
+        double eA = -uhbt, sA = 0.0, eB = -0.0, sB = 0.0;
+        for_layers<CH>(F, nz, [&](int k, const LayerVals& L) {
+            if (pa) {
+                double hm;
+                double uhk = flux_eval(F, L, L.u + duA, dt, hm);
+                uh_out[(size_t)(k - 1) * uh_stride] = uhk;
+                eA = eA + uhk;
+                sA = sA + F.dy * hm;
+            }
+            if (pb) {
+                double hm;
+                double uhk = flux_eval(F, L, L.u + duB, dt, hm);
+                eB = eB + uhk;
+                sB = sB + F.dy * hm;
+            }
+        });
+        if (pa && update) {
+            A.uh_err = eA;
+            A.duhdu_tot = sA;
+            A.uh_err_best = dmin(A.uh_err_best, fabs(A.uh_err));
+        }
+        if (pb) {
+            B.uh_err = eB;
+            B.duhdu_tot = sB;
+            B.uh_err_best = dmin(B.uh_err_best, fabs(B.uh_err));
+        }
+    }
+}
 
 // The work of one face (I, j) after its column views are set up: initial
 // fluxes, CFL limits, zonal_flux_adjust, du_cor and, for the owner,
@@ -280,7 +309,13 @@ __device__ __forceinline__ void face_work(const Dims& D, const Metrics& M, FaceC
                                           double dt)
 {
     const int nz = D.nk;
-    // initial fluxes and their column sums (:305-355)
+    // initial fluxes and their column sums (:305-355), and the CFL limits
+    // (:335-433, vol_CFL = aggress_adjust = .false.) from the same u values
+    const double CFL_dt = 0.5 / dt;
+    const double dx_W = MOM6B_A2(M.dxT, I, j, D), dx_E = MOM6B_A2(M.dxT, I + 1, j, D);
+    const double mCu = MOM6B_A2(M.mask2dCu, I, j, D);
+    double du_max_CFL = 2.0 * (CFL_dt * dx_W);
+    double du_min_CFL = -(2.0 * (CFL_dt * dx_E));
     double uh_tot_0 = 0.0, duhdu_tot_0 = 0.0;
     for_layers<CH>(F, nz, [&](int k, const LayerVals& L) {
         double hm;
@@ -288,14 +323,7 @@ __device__ __forceinline__ void face_work(const Dims& D, const Metrics& M, FaceC
         uh[(size_t)(k - 1) * ust] = uhk;
         duhdu_tot_0 = duhdu_tot_0 + F.dy * hm;
         uh_tot_0 = uh_tot_0 + uhk;
-    });
-    // CFL limits (:335-433), vol_CFL = aggress_adjust = .false.
-    const double CFL_dt = 0.5 / dt;
-    const double dx_W = MOM6B_A2(M.dxT, I, j, D), dx_E = MOM6B_A2(M.dxT, I + 1, j, D);
-    const double mCu = MOM6B_A2(M.mask2dCu, I, j, D);
-    double du_max_CFL = 2.0 * (CFL_dt * dx_W);
-    double du_min_CFL = -(2.0 * (CFL_dt * dx_E));
-    for_u<CH>(F, nz, [&](int, double uk) {
+        const double uk = L.u;
         if (du_max_CFL > dx_W * CFL_dt - uk * mCu) du_max_CFL = dx_W * CFL_dt - uk;
         if (du_min_CFL < -(dx_E * CFL_dt) - uk * mCu) du_min_CFL = -(dx_E * CFL_dt + uk);
     });
@@ -304,16 +332,19 @@ __device__ __forceinline__ void face_work(const Dims& D, const Metrics& M, FaceC
 
     const double fac = dt * dmin(MOM6B_A2(M.IareaT, I, j, D), MOM6B_A2(M.IareaT, I + 1, j, D));
     const double uhbt = MOM6B_A2(uhbt2d, I, j, D);
-    double du = flux_adjust_face<CH>(F, nz, dt, uhbt, uh_tot_0, duhdu_tot_0,
-                                 du_max_CFL, du_min_CFL, fac, uh, ust);
+    // zonal_flux_adjust (A) and, for the owner with uhbt /= 0, the
+    // zero-transport solve of set_zonal_BT_cont (B, :991-1002); with uhbt = 0
+    // B would repeat A exactly, so du0 = du.
+    const bool solve0 = owner && uhbt != 0.0;
+    Newton A = newton_start(uh_tot_0 - uhbt, duhdu_tot_0, du_max_CFL, du_min_CFL, true);
+    Newton B = newton_start(uh_tot_0 - 0.0, duhdu_tot_0, du_max_CFL, du_min_CFL, solve0);
+    flux_adjust_pair<CH>(F, nz, dt, uhbt, fac, A, B, uh, ust);
+    const double du = A.du;
     if (!owner) return;
     O.du_cor[f0] = du;
 
     // set_zonal_BT_cont (:991-1121)
-    double du0 = (uhbt == 0.0)
-                     ? du
-                     : flux_adjust_face<CH>(F, nz, dt, 0.0, uh_tot_0, duhdu_tot_0,
-                                        du_max_CFL, du_min_CFL, fac, (double*)nullptr, 0);
+    const double du0 = solve0 ? B.du : du;
     const double Idt = 1.0 / dt;
     const double du_CFL = (F32(1e-6) * Idt) * MOM6B_A2(M.dxCu, I, j, D);
     double duR = dmin(0.0, du0 - du_CFL);

@@ -12,6 +12,7 @@
 //               latency of the substep loop, not bytes).
 // This file is built with FMA contraction (the FP64 files are not), and the
 // FP32 Newton iteration uses a tolerance suited to FP32 fluxes (below).
+#include "mixed_impl.cuh"
 #include "tendency_impl.cuh"
 #include "vertvisc_impl.cuh"
 
@@ -33,272 +34,21 @@ cudaError_t launch_vertvisc_f(const Dims& D, const Metrics& M, float* u, float* 
     return launch_vertvisc_pf_t<float>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s);
 }
 
-// ---------------------------------------------------------------------------
-// FP32 continuity
-// ---------------------------------------------------------------------------
-// Newton tolerance of the FP32 form: the adjustment stops when the implied
-// sea-surface change dt * IareaT * |uh_err| is below kMixedTolEta metres (the
-// FP64 form follows the serial schedule 1e-18 .. 1e-12 m, below what FP32
-// fluxes resolve), or when the step is below kMixedRelStep of |du|.
-constexpr double kMixedTolEta = 1.0e-6;
-constexpr double kMixedRelStep = 1.0e-6;
-
-__device__ __forceinline__ float ppm_slope_f(const float* h, const float* m, int c)
-{
-    if ((m[c - 1] * m[c] * m[c + 1]) == 0.0f) return 0.0f;
-    const float hp = h[c + 1], hm = h[c - 1], hc = h[c];
-    const float s = 0.5f * (hp - hm);
-    const float dMx = fmaxf(fmaxf(hp, hm), hc) - hc;
-    const float dMn = hc - fminf(fminf(hp, hm), hc);
-    return copysignf(1.0f, s) * fminf(fabsf(s), 2.0f * fminf(dMx, dMn));
-}
-
-// PPM_reconstruction_x + PPM_limit_pos in FP32 for one cell of a row.
+// PPM edges of every cell of the face rows, then the faces.
 __global__ void __launch_bounds__(128)
 k_ppm_edges_f(Dims D, Metrics M, const float* __restrict__ hin, float* __restrict__ hW,
               float* __restrict__ hE, float h_min)
 {
-    const int i = D.is - 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
-    const int j = D.js + (int)blockIdx.y;
-    const int k = 1 + (int)blockIdx.z;
-    if (i > D.ie + 1) return;
-    const size_t row = (size_t)(k - 1) * D.plane + (size_t)(j - 1) * D.n1;
-    float h[5], m[5];
-#pragma unroll
-    for (int c = 0; c < 5; ++c) {
-        h[c] = hin[row + (i - 3 + c)];
-        m[c] = (float)M.mask2dT[(size_t)(j - 1) * D.n1 + (i - 3 + c)];
-    }
-    const float oneSixth = 1.0f / 6.0f;
-    const float slm = ppm_slope_f(h, m, 1), slc = ppm_slope_f(h, m, 2), slp = ppm_slope_f(h, m, 3);
-    const float hc = h[2];
-    const float h_im1 = m[1] * h[1] + (1.0f - m[1]) * hc;
-    const float h_ip1 = m[3] * h[3] + (1.0f - m[3]) * hc;
-    float hL = 0.5f * (h_im1 + hc) + oneSixth * (slm - slc);
-    float hR = 0.5f * (h_ip1 + hc) + oneSixth * (slc - slp);
-    const float curv = 3.0f * ((hL + hR) - 2.0f * hc);
-    if (curv > 0.0f) {
-        const float dh = hR - hL;
-        if (fabsf(dh) < curv) {
-            if (hc <= h_min) {
-                hL = hc; hR = hc;
-            } else if (12.0f * curv * (hc - h_min) < curv * curv + 3.0f * dh * dh) {
-                const float scale = 12.0f * curv * (hc - h_min) / (curv * curv + 3.0f * dh * dh);
-                hL = hc + scale * (hL - hc);
-                hR = hc + scale * (hR - hc);
-            }
-        }
-    }
-    hW[row + (i - 1)] = hL;
-    hE[row + (i - 1)] = hR;
+    ppm_cell_f(D, M, hin, hW, hE, h_min, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z);
 }
 
-struct LayerF {
-    float u, hWi, hEi, hi, hWp, hEp, hp;
-};
-
-struct FaceF {
-    const float *u, *hc, *hW, *hE;
-    size_t plane;
-    float dy, Idx_i, Idx_p, dt;
-    __device__ LayerF load(int k) const
-    {
-        const size_t o = (size_t)(k - 1) * plane;
-        return LayerF{u[o], hW[o], hE[o], hc[o], hW[o + 1], hE[o + 1], hc[o + 1]};
-    }
-    // upwind PPM transport and marginal thickness at face velocity uI
-    __device__ float eval(const LayerF& L, float uI, float& hm) const
-    {
-        const bool pos = uI > 0.0f;
-        const float base = pos ? L.hEi : L.hWp, oth = pos ? L.hWi : L.hEp;
-        const float hcl = pos ? L.hi : L.hp, Idx = pos ? Idx_i : Idx_p;
-        const float CFL = fabsf(uI) * dt * Idx;
-        const float curv_3 = (oth + base) - 2.0f * hcl;
-        const float uh = dy * uI * (base + CFL * (0.5f * (oth - base) + curv_3 * (CFL - 1.5f)));
-        const float hmm = base + CFL * ((oth - base) + 3.0f * curv_3 * (CFL - 1.0f));
-        const bool zero = !(uI > 0.0f) && !(uI < 0.0f);
-        hm = zero ? 0.5f * (L.hWp + L.hEi) : hmm;
-        return zero ? 0.0f : uh;
-    }
-};
-
-constexpr int kMixCH = 4;
-
-template <typename Fn>
-__device__ __forceinline__ void mix_layers(const FaceF& F, int nz, Fn&& fn)
-{
-    for (int kt = 1; kt <= nz; kt += kMixCH) {
-        LayerF L[kMixCH];
-#pragma unroll
-        for (int c = 0; c < kMixCH; ++c)
-            if (kt + c <= nz) L[c] = F.load(kt + c);
-#pragma unroll
-        for (int c = 0; c < kMixCH; ++c)
-            if (kt + c <= nz) fn(kt + c, L[c]);
-    }
-}
-
-// zonal_flux_adjust on FP32 fluxes with FP64 sums; keeps the last evaluated
-// transports in uh (stride ust) when uh != nullptr.
-__device__ double mix_adjust(const FaceF& F, int nz, double target, double uh_err,
-                             double duhdu_tot, double du_max, double du_min, double fac,
-                             float* uh, size_t ust)
-{
-    double du = 0.0, best = fabs(uh_err);
-    for (int itt = 1; itt <= 20; ++itt) {
-        bool more = true;
-        if (uh_err > 0.0) du_max = du;
-        else if (uh_err < 0.0) du_min = du;
-        else more = false;
-        if (more) {
-            const double ae = fabs(uh_err);
-            if (fac * ae > kMixedTolEta || ae > best) {
-                const double ddu = -(uh_err / duhdu_tot);
-                const double du_prev = du;
-                du = du + ddu;
-                if (fabs(ddu) < kMixedRelStep * fabs(du)) {
-                    more = false;
-                } else if (ddu > 0.0) {
-                    if (du >= du_max) {
-                        du = 0.5 * (du_prev + du_max);
-                        if (du_max - du_prev < kMixedRelStep * fabs(du)) more = false;
-                    }
-                } else if (du <= du_min) {
-                    du = 0.5 * (du_prev + du_min);
-                    if (du_prev - du_min < kMixedRelStep * fabs(du)) more = false;
-                }
-            } else {
-                more = false;
-            }
-        }
-        if (!more) break;
-        double e = target, ds = 0.0;
-        const float duf = (float)du;
-        mix_layers(F, nz, [&](int k, const LayerF& L) {
-            float hm;
-            const float t = F.eval(L, L.u + duf, hm);
-            if (uh) uh[(size_t)(k - 1) * ust] = t;
-            e += (double)t;
-            ds += (double)(F.dy * hm);
-        });
-        uh_err = e;
-        duhdu_tot = ds;
-        best = fmin(best, fabs(uh_err));
-    }
-    return du;
-}
-
-struct ContOutF {
-    float *h, *uh, *h_u;
-    double *FA_u_W0, *FA_u_WW, *FA_u_E0, *FA_u_EE, *uBT_WW, *uBT_EE, *du_cor;
-};
-
-// One thread per u face, 127 faces per CTA, consecutive CTAs overlapping by
-// one face whose transports thread 0 keeps in its CTA's slot of ovl.
 __global__ void __launch_bounds__(128)
 k_cont_faces_f(Dims D, Metrics M, const float* __restrict__ u, const float* __restrict__ hin,
                const float* __restrict__ hW, const float* __restrict__ hE,
                const double* __restrict__ uhbt2d, ContOutF O, float* ovl_all, double dt)
 {
-    const int nz = D.nk;
-    const int I = D.is - 1 + (int)blockIdx.x * ((int)blockDim.x - 1) + (int)threadIdx.x;
-    const int j = D.js + (int)blockIdx.y;
-    const bool face_ok = I <= D.ie;
-    const bool owner = threadIdx.x >= 1 || blockIdx.x == 0;
-    float* ovl = ovl_all + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * (size_t)nz;
-    const size_t plane = (size_t)D.plane;
-    if (face_ok) {
-        const size_t f0 = (size_t)(j - 1) * D.n1 + (I - 1);
-        FaceF F{u + f0, hin + f0, hW + f0, hE + f0, plane,
-                (float)MOM6B_A2(M.dy_Cu, I, j, D), (float)MOM6B_A2(M.IdxT, I, j, D),
-                (float)MOM6B_A2(M.IdxT, I + 1, j, D), (float)dt};
-        float* uh = owner ? O.uh + f0 : ovl;
-        const size_t ust = owner ? plane : 1;
-        // initial fluxes, column sums, CFL limits
-        double uh_tot_0 = 0.0, duhdu_tot_0 = 0.0;
-        const double CFL_dt = 0.5 / dt;
-        const double dx_W = MOM6B_A2(M.dxT, I, j, D), dx_E = MOM6B_A2(M.dxT, I + 1, j, D);
-        const double mCu = MOM6B_A2(M.mask2dCu, I, j, D);
-        double du_max_CFL = 2.0 * (CFL_dt * dx_W), du_min_CFL = -(2.0 * (CFL_dt * dx_E));
-        mix_layers(F, nz, [&](int k, const LayerF& L) {
-            float hm;
-            const float t = F.eval(L, L.u, hm);
-            uh[(size_t)(k - 1) * ust] = t;
-            uh_tot_0 += (double)t;
-            duhdu_tot_0 += (double)(F.dy * hm);
-            const double uk = (double)L.u;
-            if (du_max_CFL > dx_W * CFL_dt - uk * mCu) du_max_CFL = dx_W * CFL_dt - uk;
-            if (du_min_CFL < -(dx_E * CFL_dt) - uk * mCu) du_min_CFL = -(dx_E * CFL_dt + uk);
-        });
-        du_max_CFL = fmax(du_max_CFL, 0.0);
-        du_min_CFL = fmin(du_min_CFL, 0.0);
-        const double fac = dt * fmin(MOM6B_A2(M.IareaT, I, j, D), MOM6B_A2(M.IareaT, I + 1, j, D));
-        const double uhbt = MOM6B_A2(uhbt2d, I, j, D);
-        const double du = mix_adjust(F, nz, -uhbt, uh_tot_0 - uhbt, duhdu_tot_0, du_max_CFL,
-                                     du_min_CFL, fac, uh, ust);
-        if (owner) {
-            O.du_cor[f0] = du;
-            const double du0 = (uhbt == 0.0)
-                                   ? du
-                                   : mix_adjust(F, nz, 0.0, uh_tot_0, duhdu_tot_0, du_max_CFL,
-                                                du_min_CFL, fac, nullptr, 0);
-            const double du_CFL = (1.0e-6 / dt) * MOM6B_A2(M.dxCu, I, j, D);
-            double duR = fmin(0.0, du0 - du_CFL), duL = fmax(0.0, du0 + du_CFL);
-            for (int k = 1; k <= nz; ++k) {
-                const double uk = (double)u[f0 + (size_t)(k - 1) * plane];
-                if (uk + duR > -du_CFL) duR = -(uk + du_CFL);
-                if (uk + duL < du_CFL) duL = -(uk - du_CFL);
-            }
-            double FAmt_0 = 0.0, FAmt_L = 0.0, FAmt_R = 0.0, uhtot_L = 0.0, uhtot_R = 0.0;
-            const float d0 = (float)du0, dL = (float)duL, dR = (float)duR, dc = (float)du;
-            const bool same = du0 == du;
-            mix_layers(F, nz, [&](int k, const LayerF& L) {
-                float hm0, hmL, hmR;
-                F.eval(L, L.u + d0, hm0);
-                const float uL = F.eval(L, L.u + dL, hmL);
-                const float uR = F.eval(L, L.u + dR, hmR);
-                FAmt_0 += (double)(F.dy * hm0);
-                FAmt_L += (double)(F.dy * hmL);
-                FAmt_R += (double)(F.dy * hmR);
-                uhtot_L += (double)uL;
-                uhtot_R += (double)uR;
-                float hmc = hm0;
-                if (!same) F.eval(L, L.u + dc, hmc);
-                O.h_u[f0 + (size_t)(k - 1) * plane] = hmc;
-            });
-            double FA_0 = FAmt_0, FA_avg = FAmt_0;
-            if ((duL - du0) != 0.0) FA_avg = uhtot_L / (duL - du0);
-            if (FA_avg > fmax(FA_0, FAmt_L)) FA_avg = fmax(FA_0, FAmt_L);
-            else if (FA_avg < fmin(FA_0, FAmt_L)) FA_0 = FA_avg;
-            O.FA_u_W0[f0] = FA_0;
-            O.FA_u_WW[f0] = FAmt_L;
-            O.uBT_WW[f0] = (fabs(FA_0 - FAmt_L) <= 1e-12 * FA_0)
-                               ? 0.0
-                               : (1.5 * (duL - du0)) * ((FAmt_L - FA_avg) / (FAmt_L - FA_0));
-            FA_0 = FAmt_0; FA_avg = FAmt_0;
-            if ((duR - du0) != 0.0) FA_avg = uhtot_R / (duR - du0);
-            if (FA_avg > fmax(FA_0, FAmt_R)) FA_avg = fmax(FA_0, FAmt_R);
-            else if (FA_avg < fmin(FA_0, FAmt_R)) FA_0 = FA_avg;
-            O.FA_u_E0[f0] = FA_0;
-            O.FA_u_EE[f0] = FAmt_R;
-            O.uBT_EE[f0] = (fabs(FAmt_R - FA_0) <= 1e-12 * FA_0)
-                               ? 0.0
-                               : (1.5 * (duR - du0)) * ((FAmt_R - FA_avg) / (FAmt_R - FA_0));
-        }
-    }
-    __syncthreads();  // the CTA's transports are complete and visible
-    // thickness update in FP64 for cell i = I (faces I-1 and I in this CTA)
-    const int i = I;
-    if (threadIdx.x >= 1 && i >= D.is && i <= D.ie) {
-        const size_t c0 = (size_t)(j - 1) * D.n1 + (i - 1);
-        const double fac = dt * MOM6B_A2(M.IareaT, i, j, D);
-        const bool from_ovl = threadIdx.x == 1 && blockIdx.x > 0;
-        for (int k = 1; k <= nz; ++k) {
-            const size_t o = (size_t)(k - 1) * plane + c0;
-            const double left = from_ovl ? (double)ovl[k - 1] : (double)O.uh[o - 1];
-            O.h[o] = (float)fmax((double)hin[o] - fac * ((double)O.uh[o] - left), 0.0);
-        }
-    }
+    cont_faces_f(D, M, u, hin, hW, hE, uhbt2d, O, ovl_all, dt, (int)blockIdx.x,
+                 (int)blockIdx.y, (int)gridDim.x);
 }
 
 cudaError_t launch_continuity_f(const Dims& D, const Metrics& M, const float* u,

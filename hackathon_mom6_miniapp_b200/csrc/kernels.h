@@ -94,4 +94,80 @@ cudaError_t launch_continuity_f(const Dims& D, const Metrics& M, const float* u,
                                 float* h, float* uh, float* h_u, const ContOut& O2,
                                 double* uh_ovl, double dt, double h_min, cudaStream_t s);
 
+// ---------------------------------------------------------------------------
+// Ensemble: many independent domains advanced in the mixed form with one
+// launch per phase for all of them (k_ensemble.cu, and k_btstep.cu for the
+// FP64 barotropic loop).
+// ---------------------------------------------------------------------------
+// One domain: dimensions, metrics, parameters and device arrays (3-D state in
+// FP32).  An array of these lives in device memory; each CTA of a batched
+// kernel copies its domain's entry to shared memory first.
+struct EnsDomain {
+    Dims D;
+    Metrics M;
+    UniMetrics U;
+    float *u, *v, *hA, *hB, *h0, *up, *vp, *uh, *hW, *hE, *h_u, *ovl;
+    double *uhbt0, *taux_bot, *tauy_bot;
+    ContOut O2;                 // FP64 2-D outputs of continuity (h, uh, h_u unused)
+    double *eta, *ubt, *vbt, *ubt_av, *vbt_av, *eta_av;
+    BTWork W;                   // barotropic work arrays (control words unused)
+    VVParams VV;
+    BTParams P;
+    double dt, h_min;
+    float hv_neglect;
+    int bc_fill;
+};
+
+// Launch shapes of the batched kernels, chosen by the ensemble's autotuner.
+struct EnsTuning {
+    int tend;      // tendency tile: index into kEnsTendTiles
+    int tend_kc;   // layers per tendency CTA
+    int vv_nb;     // vertvisc threads per CTA (64, 128, 256)
+    int vv_ch;     // vertvisc layers per prefetch (2, 4)
+    int ppm_nb;    // PPM edge threads per CTA (128, 256)
+    int faces_nb;  // continuity faces per CTA + 1 (64, 128, 256)
+    int bt_tile;   // largest barotropic tile edge (32, 48, 64)
+};
+
+constexpr int kEnsTendTiles[4][2] = {{32, 8}, {32, 4}, {64, 4}, {32, 16}};
+
+// Barotropic tiles of one domain: nbx x nby tiles of tw x th points covering
+// [is-1, ie] x [js-1, je]; t0 is the domain's first tile in the global list.
+struct EnsBtGeo {
+    int nbx, nby, tw, th, t0;
+};
+
+// Blocks each batched kernel gives one domain under a tuning (host side).
+long long ens_blocks_tendency(const Dims& D, const EnsTuning& T);
+long long ens_blocks_vertvisc(const Dims& D, const EnsTuning& T);
+long long ens_blocks_ppm(const Dims& D, const EnsTuning& T);
+long long ens_blocks_faces(const Dims& D, const EnsTuning& T);
+long long ens_blocks_halo(const Dims& D, int which);
+// FP32 overlap slots continuity needs for one domain at the smallest face block.
+size_t ens_ovl_floats(const Dims& D);
+EnsBtGeo ens_bt_geometry(const Dims& D, int max_edge);
+
+// half: 0 = predictor, 1 = corrector.  start[d] is domain d's first block
+// (start[n] = total).  uni: every domain has uniform metrics.
+cudaError_t launch_ens_tendency(const EnsDomain* doms, const int* start, int n, int total,
+                                int half, const EnsTuning& T, bool uni, cudaStream_t s);
+cudaError_t launch_ens_vertvisc(const EnsDomain* doms, const int* start, int n, int total,
+                                int half, int kmax, const EnsTuning& T, cudaStream_t s);
+cudaError_t launch_ens_ppm(const EnsDomain* doms, const int* start, int n, int total, int half,
+                           const EnsTuning& T, cudaStream_t s);
+cudaError_t launch_ens_faces(const EnsDomain* doms, const int* start, int n, int total,
+                             int half, const EnsTuning& T, cudaStream_t s);
+// which: 0 = after the predictor (hB, up, vp), 1 = after the corrector (hA, u,
+// v), 2 = between the barotropic calls (eta_av, ubt_av, vbt_av), 3 = after
+// them (eta).  Jobs are (domain, field) pairs, start over n * fields(which).
+cudaError_t launch_ens_halo(const EnsDomain* doms, const int* start, int njobs, int total,
+                            int which, cudaStream_t s);
+// The barotropic loop of every domain in one cooperative persistent launch.
+// call 0: eta, ubt, vbt -> ubt_av, vbt_av, eta_av; call 1: eta_av, ubt_av,
+// vbt_av -> ubt_av, vbt_av, eta.  ctl supplies the barrier words, status and
+// one flag per tile.
+cudaError_t launch_ens_btstep(const EnsDomain* doms, const EnsBtGeo* geo, const int* tstart,
+                              int n, int ntiles, int max_tw, int max_th, int call,
+                              int max_nstep, const BTWork& ctl, bool uni, cudaStream_t s);
+
 }  // namespace mom6b

@@ -450,6 +450,39 @@ static cudaError_t timed(mom6b_model* m, cudaStream_t s, const char* name, F&& l
     return e;
 }
 
+// Constants of the serial step: Angstrom_H = 1e-10 (mom6_types.F90:323), the
+// hor_visc h_neglect = max(Angstrom_H, 1e-3) (mom6_hor_visc_serial.F90:203)
+// and continuity's h_min = 2.0 * Angstrom_H with a default-real 2.0
+// (mom6_continuity_serial.F90:211).
+constexpr double kAngstromH = 1.0e-10;
+static double step_hv_neglect() { return kAngstromH > 1.0e-3 ? kAngstromH : 1.0e-3; }
+static double step_h_min() { return (double)2.0f * kAngstromH; }
+
+// vert_visc_init as the driver calls it (rk2_serial_driver.F90:141-142,
+// mom6_vert_visc_serial.F90:60-112), h_neglect = Angstrom_H (:151-152)
+static VVParams step_vv_params(const mom6b_config& c)
+{
+    return VVParams{c.Kv, c.Kv_ml, c.Kv_extra_bbl, c.Hmix, kAngstromH,
+                    1.0 / (c.Hbbl + kAngstromH)};
+}
+
+// barotropic_init / btstep: dtbt = dt / nstep, bebt = 0.2
+// (mom6_barotropic_serial.F90:73-74, :194-195)
+static BTParams step_bt_params(const mom6b_config& c)
+{
+    BTParams P;
+    P.dtbt = c.dt / (double)c.bt_nsteps;
+    P.dgeo_de = 1.0;
+    P.trans_wt1 = 1.0 + 0.2;
+    P.trans_wt2 = -0.2;
+    P.inv_nstep = 1.0 / (double)c.bt_nsteps;
+    P.nstep = c.bt_nsteps;
+    P.first_direction = 0;
+    P.extended = 0;
+    P.spin_budget = 4000000000LL;
+    return P;
+}
+
 static int enqueue_step(mom6b_model* m)
 {
     const Dims& D = m->D;
@@ -461,11 +494,9 @@ static int enqueue_step(mom6b_model* m)
     // overlapped with the 3-D chain only when enabled.
     cudaStream_t s2 = m->overlap_bt ? m->s2d : m->s3d;
     const double dt = c.dt;
-    const double Angstrom_H = 1.0e-10;
-    const double hv_neglect = Angstrom_H > 1.0e-3 ? Angstrom_H : 1.0e-3;
-    const double h_min = (double)2.0f * Angstrom_H;
-    VVParams VV{c.Kv, c.Kv_ml, c.Kv_extra_bbl, c.Hmix, Angstrom_H,
-                1.0 / (c.Hbbl + Angstrom_H)};
+    const double hv_neglect = step_hv_neglect();
+    const double h_min = step_h_min();
+    VVParams VV = step_vv_params(c);
     ContOut OB{m->hB, m->uh, m->h_u, m->FA_u_W0, m->FA_u_WW, m->FA_u_E0,
                m->FA_u_EE, m->uBT_WW, m->uBT_EE, m->du_cor};
     ContOut OA = OB;
@@ -547,16 +578,7 @@ static int enqueue_step(mom6b_model* m)
     }
 
     // ---- barotropic chain ----
-    BTParams P;
-    P.dtbt = dt / (double)c.bt_nsteps;
-    P.dgeo_de = 1.0;
-    P.trans_wt1 = 1.0 + 0.2;
-    P.trans_wt2 = -0.2;
-    P.inv_nstep = 1.0 / (double)c.bt_nsteps;
-    P.nstep = c.bt_nsteps;
-    P.first_direction = 0;
-    P.extended = 0;
-    P.spin_budget = 4000000000LL;
+    BTParams P = step_bt_params(c);
     CK(timed(m, s2, "btstep", [&] {
         return launch_btstep(D, M, m->U, m->bt, P, m->eta, m->ubt, m->vbt, m->ubt_av,
                              m->vbt_av, m->eta_av, s2); }));
@@ -898,5 +920,529 @@ extern "C" int mom6b_kernel_time_ms(mom6b_model* m, const char* kernel, double* 
     }
     if (avg_ms) *avg_ms = it->second.first / (double)it->second.second;
     if (launches) *launches = it->second.second;
+    return MOM6B_OK;
+}
+
+// ===========================================================================
+// Ensemble: many independent domains of uneven size in the mixed form, one
+// launch per phase for all of them (k_ensemble.cu, k_btstep.cu).
+// ===========================================================================
+// Each domain is a full mixed-form model (its own allocations, initial state
+// and halo fill, exactly as mom6b_create builds it); the ensemble adds the
+// device table of domain descriptors, the per-phase block tables of the
+// current tuning, the barotropic tile list and its flags, and a stream and
+// CUDA graph of its own.  One step is fourteen launches whatever the number
+// of domains (ten when no domain fills halos): tendency, vertvisc, PPM edges,
+// faces and halo fill for the predictor and the corrector, then the two
+// barotropic calls with their halo fills.
+struct mom6b_ensemble {
+    std::vector<mom6b_model*> doms;
+    std::vector<EnsDomain> host;
+    EnsDomain* d_doms = nullptr;
+    EnsTuning T{0, 5, 128, 4, 128, 128, 64};
+    bool uni = true, uni_bt = true;
+    int kmax = 0, max_nstep = 0, device = 0;
+    // block tables of the current tuning (device) and their totals
+    int *st_tend = nullptr, *st_vv = nullptr, *st_ppm = nullptr, *st_faces = nullptr;
+    int *st_halo[4] = {nullptr, nullptr, nullptr, nullptr};
+    int tot_tend = 0, tot_vv = 0, tot_ppm = 0, tot_faces = 0, tot_halo[4] = {0, 0, 0, 0};
+    EnsBtGeo* d_geo = nullptr;
+    int* d_tstart = nullptr;
+    int ntiles = 0, max_tw = 0, max_th = 0;
+    BTWork ctl{};
+    int max_tiles_alloc = 0;
+    std::vector<void*> allocs;
+    std::vector<void*> plan_allocs;
+    cudaStream_t s = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int use_graph = 1;
+    int64_t launches = 0, launches_per_step = 0;
+};
+
+static void ens_free_plan(mom6b_ensemble* e)
+{
+    for (void* p : e->plan_allocs) cudaFree(p);
+    e->plan_allocs.clear();
+    if (e->exec) { cudaGraphExecDestroy(e->exec); e->exec = nullptr; }
+    if (e->graph) { cudaGraphDestroy(e->graph); e->graph = nullptr; }
+}
+
+static void ens_free(mom6b_ensemble* e)
+{
+    if (e->s) cudaStreamSynchronize(e->s);
+    ens_free_plan(e);
+    for (void* p : e->allocs) cudaFree(p);
+    e->allocs.clear();
+    for (mom6b_model* m : e->doms) mom6b_destroy(m);
+    e->doms.clear();
+    if (e->s) cudaStreamDestroy(e->s);
+    e->s = nullptr;
+}
+
+// Upload a block table built from per-job block counts; returns the total.
+static int ens_table(mom6b_ensemble* e, const std::vector<long long>& counts, int** dst,
+                     int* total)
+{
+    std::vector<int> st(counts.size() + 1, 0);
+    long long acc = 0;
+    for (size_t q = 0; q < counts.size(); ++q) {
+        st[q] = (int)acc;
+        acc += counts[q];
+        if (acc > 2147483647LL) return fail(MOM6B_ERR_ARG, "ensemble grid too large");
+    }
+    st[counts.size()] = (int)acc;
+    void* p = nullptr;
+    CK(cudaMalloc(&p, st.size() * sizeof(int)));
+    e->plan_allocs.push_back(p);
+    CK(cudaMemcpy(p, st.data(), st.size() * sizeof(int), cudaMemcpyHostToDevice));
+    *dst = (int*)p;
+    *total = (int)acc;
+    return MOM6B_OK;
+}
+
+// Block tables and barotropic tiles for the current tuning.
+static int ens_plan(mom6b_ensemble* e)
+{
+    ens_free_plan(e);
+    const int n = (int)e->doms.size();
+    const EnsTuning& T = e->T;
+    std::vector<long long> ct(n), cv(n), cp(n), cf(n);
+    for (int d = 0; d < n; ++d) {
+        const Dims& D = e->host[d].D;
+        ct[d] = ens_blocks_tendency(D, T);
+        cv[d] = ens_blocks_vertvisc(D, T);
+        cp[d] = ens_blocks_ppm(D, T);
+        cf[d] = ens_blocks_faces(D, T);
+    }
+    if (int rc = ens_table(e, ct, &e->st_tend, &e->tot_tend)) return rc;
+    if (int rc = ens_table(e, cv, &e->st_vv, &e->tot_vv)) return rc;
+    if (int rc = ens_table(e, cp, &e->st_ppm, &e->tot_ppm)) return rc;
+    if (int rc = ens_table(e, cf, &e->st_faces, &e->tot_faces)) return rc;
+    for (int w = 0; w < 4; ++w) {
+        const int F = w == 3 ? 1 : 3;
+        std::vector<long long> ch((size_t)n * F);
+        for (int d = 0; d < n; ++d)
+            for (int f = 0; f < F; ++f)
+                ch[(size_t)d * F + f] = e->host[d].bc_fill ? ens_blocks_halo(e->host[d].D, w) : 0;
+        if (int rc = ens_table(e, ch, &e->st_halo[w], &e->tot_halo[w])) return rc;
+    }
+    std::vector<EnsBtGeo> geo(n);
+    std::vector<int> tst(n + 1);
+    int nt = 0, mtw = 0, mth = 0;
+    for (int d = 0; d < n; ++d) {
+        geo[d] = ens_bt_geometry(e->host[d].D, T.bt_tile);
+        geo[d].t0 = nt;
+        tst[d] = nt;
+        nt += geo[d].nbx * geo[d].nby;
+        mtw = std::max(mtw, geo[d].tw);
+        mth = std::max(mth, geo[d].th);
+    }
+    tst[n] = nt;
+    if (nt > e->max_tiles_alloc) return fail(MOM6B_ERR_ARG, "too many barotropic tiles");
+    void* pg = nullptr;
+    void* pt = nullptr;
+    CK(cudaMalloc(&pg, n * sizeof(EnsBtGeo)));
+    e->plan_allocs.push_back(pg);
+    CK(cudaMalloc(&pt, (n + 1) * sizeof(int)));
+    e->plan_allocs.push_back(pt);
+    CK(cudaMemcpy(pg, geo.data(), n * sizeof(EnsBtGeo), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(pt, tst.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice));
+    e->d_geo = (EnsBtGeo*)pg;
+    e->d_tstart = (int*)pt;
+    e->ntiles = nt;
+    e->max_tw = mtw;
+    e->max_th = mth;
+    return MOM6B_OK;
+}
+
+// One launch of phase `ph` (0..13 in step order); counts the launch.
+static int ens_launch(mom6b_ensemble* e, int ph)
+{
+    const int n = (int)e->doms.size();
+    cudaStream_t s = e->s;
+    cudaError_t r = cudaSuccess;
+    switch (ph) {
+    case 0: case 5:
+        r = launch_ens_tendency(e->d_doms, e->st_tend, n, e->tot_tend, ph == 5, e->T, e->uni, s);
+        break;
+    case 1: case 6:
+        r = launch_ens_vertvisc(e->d_doms, e->st_vv, n, e->tot_vv, ph == 6, e->kmax, e->T, s);
+        break;
+    case 2: case 7:
+        r = launch_ens_ppm(e->d_doms, e->st_ppm, n, e->tot_ppm, ph == 7, e->T, s);
+        break;
+    case 3: case 8:
+        r = launch_ens_faces(e->d_doms, e->st_faces, n, e->tot_faces, ph == 8, e->T, s);
+        break;
+    case 4: case 9:
+        r = launch_ens_halo(e->d_doms, e->st_halo[ph == 9], 3 * n, e->tot_halo[ph == 9],
+                            ph == 9, s);
+        break;
+    case 10: case 12:
+        r = launch_ens_btstep(e->d_doms, e->d_geo, e->d_tstart, n, e->ntiles, e->max_tw,
+                              e->max_th, ph == 12, e->max_nstep, e->ctl, e->uni_bt, s);
+        break;
+    case 11:
+        r = launch_ens_halo(e->d_doms, e->st_halo[2], 3 * n, e->tot_halo[2], 2, s);
+        break;
+    case 13:
+        r = launch_ens_halo(e->d_doms, e->st_halo[3], n, e->tot_halo[3], 3, s);
+        break;
+    default: return fail(MOM6B_ERR_ARG, "unknown ensemble phase");
+    }
+    if (r != cudaSuccess) return fail(MOM6B_ERR_CUDA, std::string("ensemble launch: ") + cudaGetErrorString(r));
+    ++e->launches;
+    return MOM6B_OK;
+}
+
+static bool ens_phase_active(const mom6b_ensemble* e, int ph)
+{
+    if (ph == 4 || ph == 9) return e->tot_halo[ph == 9] > 0;
+    if (ph == 11) return e->tot_halo[2] > 0;
+    if (ph == 13) return e->tot_halo[3] > 0;
+    return true;
+}
+
+static int ens_enqueue(mom6b_ensemble* e)
+{
+    for (int ph = 0; ph < 14; ++ph)
+        if (ens_phase_active(e, ph))
+            if (int rc = ens_launch(e, ph)) return rc;
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_ensemble_create(int n, const mom6b_config* cfgs, mom6b_ensemble** out)
+{
+    if (!out || !cfgs || n < 1) return fail(MOM6B_ERR_ARG, "bad argument");
+    *out = nullptr;
+    auto e = std::make_unique<mom6b_ensemble>();
+    e->device = cfgs[0].device;
+    for (int d = 0; d < n; ++d) {
+        if (cfgs[d].precision != MOM6B_MIXED)
+            return fail(MOM6B_ERR_ARG, "ensemble domains run the mixed form (precision MOM6B_MIXED)");
+        if (cfgs[d].device != e->device)
+            return fail(MOM6B_ERR_ARG, "ensemble domains share one device");
+        if (cfgs[d].nk > 256) return fail(MOM6B_ERR_ARG, "ensemble domains need nk <= 256");
+    }
+    CK(cudaSetDevice(e->device));
+    for (int d = 0; d < n; ++d) {
+        mom6b_config c = cfgs[d];
+        c.use_graph = 0;
+        mom6b_model* m = nullptr;
+        int rc = mom6b_create(&c, &m);
+        if (rc) { ens_free(e.get()); return rc; }
+        e->doms.push_back(m);
+    }
+    // descriptors
+    size_t max_tiles = 0;
+    for (int d = 0; d < n; ++d) {
+        mom6b_model* m = e->doms[d];
+        const mom6b_config& c = m->cfg;
+        EnsDomain E{};
+        E.D = m->D; E.M = m->M; E.U = m->U;
+        auto F = [](double* p) { return (float*)p; };
+        E.u = F(m->u); E.v = F(m->v); E.hA = F(m->hA); E.hB = F(m->hB); E.h0 = F(m->h0);
+        E.up = F(m->up); E.vp = F(m->vp); E.uh = F(m->uh); E.hW = F(m->hW); E.hE = F(m->hE);
+        E.h_u = F(m->h_u);
+        void* po = nullptr;
+        if (cudaMalloc(&po, ens_ovl_floats(m->D) * sizeof(float) + 16) != cudaSuccess) {
+            ens_free(e.get());
+            return fail(MOM6B_ERR_NOMEM, "device allocation failed");
+        }
+        e->allocs.push_back(po);
+        E.ovl = (float*)po;
+        E.uhbt0 = m->uhbt0; E.taux_bot = m->taux_bot; E.tauy_bot = m->tauy_bot;
+        E.O2 = ContOut{nullptr, nullptr, nullptr, m->FA_u_W0, m->FA_u_WW, m->FA_u_E0,
+                       m->FA_u_EE, m->uBT_WW, m->uBT_EE, m->du_cor};
+        E.eta = m->eta; E.ubt = m->ubt; E.vbt = m->vbt;
+        E.ubt_av = m->ubt_av; E.vbt_av = m->vbt_av; E.eta_av = m->eta_av;
+        E.W = m->bt;
+        E.VV = step_vv_params(c);
+        E.P = step_bt_params(c);
+        E.dt = c.dt;
+        E.h_min = step_h_min();
+        E.hv_neglect = (float)step_hv_neglect();
+        E.bc_fill = c.bc_fill;
+        e->host.push_back(E);
+        e->uni = e->uni && m->U.valid;
+        e->uni_bt = e->uni_bt && m->U.valid_bt;
+        e->kmax = std::max(e->kmax, m->D.nk);
+        e->max_nstep = std::max(e->max_nstep, c.bt_nsteps);
+        EnsBtGeo g = ens_bt_geometry(m->D, 32);
+        max_tiles += (size_t)g.nbx * g.nby;
+    }
+    {
+        void* p = nullptr;
+        CK(cudaMalloc(&p, n * sizeof(EnsDomain)));
+        e->allocs.push_back(p);
+        CK(cudaMemcpy(p, e->host.data(), n * sizeof(EnsDomain), cudaMemcpyHostToDevice));
+        e->d_doms = (EnsDomain*)p;
+        // barrier words, status and one flag per tile (the smallest tile edge)
+        void* pc = nullptr;
+        const size_t bytes = 64 + max_tiles * sizeof(unsigned int);
+        CK(cudaMalloc(&pc, bytes));
+        e->allocs.push_back(pc);
+        CK(cudaMemset(pc, 0, bytes));
+        e->ctl.bar_count = (unsigned int*)pc;
+        e->ctl.bar_gen = (unsigned int*)pc + 4;
+        e->ctl.status = (int*)pc + 8;
+        e->ctl.tile_flag = (unsigned int*)pc + 16;
+        e->max_tiles_alloc = (int)max_tiles;
+    }
+    CK(cudaStreamCreateWithFlags(&e->s, cudaStreamNonBlocking));
+    if (int rc = ens_plan(e.get())) { ens_free(e.get()); return rc; }
+    *out = e.release();
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_ensemble_destroy(mom6b_ensemble* e)
+{
+    if (!e) return MOM6B_OK;
+    cudaSetDevice(e->device);
+    ens_free(e);
+    delete e;
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_ensemble_size(const mom6b_ensemble* e)
+{
+    return e ? (int)e->doms.size() : 0;
+}
+
+extern "C" int mom6b_ensemble_step(mom6b_ensemble* e, int nsteps)
+{
+    if (!e || nsteps < 0) return fail(MOM6B_ERR_ARG, "bad argument");
+    CK(cudaSetDevice(e->device));
+    if (e->use_graph) {
+        if (!e->exec) {
+            int64_t before = e->launches;
+            CK(cudaStreamBeginCapture(e->s, cudaStreamCaptureModeThreadLocal));
+            int rc = ens_enqueue(e);
+            cudaGraph_t g = nullptr;
+            cudaError_t r = cudaStreamEndCapture(e->s, &g);
+            if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+            if (r != cudaSuccess) return fail(MOM6B_ERR_CUDA, std::string("stream capture: ") + cudaGetErrorString(r));
+            e->graph = g;
+            CK(cudaGraphInstantiate(&e->exec, g, 0));
+            e->launches_per_step = e->launches - before;
+            e->launches = before;
+        }
+        for (int k = 0; k < nsteps; ++k) {
+            CK(cudaGraphLaunch(e->exec, e->s));
+            e->launches += e->launches_per_step;
+        }
+        return MOM6B_OK;
+    }
+    for (int k = 0; k < nsteps; ++k)
+        if (int rc = ens_enqueue(e)) return rc;
+    return MOM6B_OK;
+}
+
+static int ens_check_status(mom6b_ensemble* e)
+{
+    int st = 0;
+    CK(cudaMemcpy(&st, e->ctl.status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st != kDevOk) {
+        cudaMemset(e->ctl.status, 0, sizeof(int));
+        cudaMemset(e->ctl.bar_count, 0, sizeof(unsigned int));
+        return fail(MOM6B_ERR_TIMEOUT, "ensemble barotropic wait timed out");
+    }
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_ensemble_synchronize(mom6b_ensemble* e)
+{
+    if (!e) return fail(MOM6B_ERR_ARG, "null ensemble");
+    CK(cudaSetDevice(e->device));
+    CK(cudaStreamSynchronize(e->s));
+    return ens_check_status(e);
+}
+
+extern "C" int mom6b_ensemble_stream(mom6b_ensemble* e, void** stream)
+{
+    if (!e || !stream) return fail(MOM6B_ERR_ARG, "null argument");
+    *stream = (void*)e->s;
+    return MOM6B_OK;
+}
+
+extern "C" int64_t mom6b_ensemble_launch_count(const mom6b_ensemble* e)
+{
+    return e ? e->launches : 0;
+}
+
+extern "C" mom6b_model* mom6b_ensemble_member(mom6b_ensemble* e, int d)
+{
+    if (!e || d < 0 || d >= (int)e->doms.size()) return nullptr;
+    return e->doms[d];
+}
+
+extern "C" int mom6b_ensemble_get_field(mom6b_ensemble* e, int d, int field, double* host,
+                                        size_t count)
+{
+    if (!e || d < 0 || d >= (int)e->doms.size()) return fail(MOM6B_ERR_ARG, "bad domain index");
+    if (int rc = mom6b_ensemble_synchronize(e)) return rc;
+    return mom6b_get_field(e->doms[d], field, host, count);
+}
+
+// Tuning as 7 ints: tendency tile index, tendency layers per CTA, vertvisc
+// threads per CTA, vertvisc prefetch depth, PPM threads per CTA, faces per
+// CTA + 1, barotropic tile edge.
+static bool ens_tuning_valid(const EnsTuning& T)
+{
+    auto in = [](int v, std::initializer_list<int> set) {
+        for (int x : set) if (v == x) return true;
+        return false;
+    };
+    return T.tend >= 0 && T.tend < 4 && T.tend_kc >= 1 && T.tend_kc <= 16 &&
+           in(T.vv_nb, {64, 128, 256}) && in(T.vv_ch, {2, 4}) && in(T.ppm_nb, {128, 256}) &&
+           in(T.faces_nb, {64, 128, 256}) && in(T.bt_tile, {32, 48, 64});
+}
+
+extern "C" int mom6b_ensemble_get_tuning(const mom6b_ensemble* e, int* out7)
+{
+    if (!e || !out7) return fail(MOM6B_ERR_ARG, "null argument");
+    const EnsTuning& T = e->T;
+    int v[7] = {T.tend, T.tend_kc, T.vv_nb, T.vv_ch, T.ppm_nb, T.faces_nb, T.bt_tile};
+    std::memcpy(out7, v, sizeof(v));
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_ensemble_set_tuning(mom6b_ensemble* e, const int* in7)
+{
+    if (!e || !in7) return fail(MOM6B_ERR_ARG, "null argument");
+    EnsTuning T{in7[0], in7[1], in7[2], in7[3], in7[4], in7[5], in7[6]};
+    if (!ens_tuning_valid(T)) return fail(MOM6B_ERR_ARG, "tuning value outside the supported set");
+    CK(cudaSetDevice(e->device));
+    CK(cudaStreamSynchronize(e->s));
+    e->T = T;
+    return ens_plan(e);
+}
+
+// Device copies of every array a step rewrites, to undo the tuning trials.
+struct EnsSnapshot {
+    std::vector<std::pair<void*, void*>> saved;  // (live, copy)
+    std::vector<size_t> bytes;
+};
+
+static int ens_snapshot(mom6b_ensemble* e, EnsSnapshot& S)
+{
+    for (mom6b_model* m : e->doms) {
+        const size_t n3 = m->grid->plane * (size_t)m->grid->nk, n2 = m->grid->plane;
+        const size_t b3 = n3 * sizeof(float), b2 = n2 * sizeof(double);
+        void* live[] = {m->u, m->v, m->hA, m->hB, m->up, m->vp, m->uh, m->h_u, m->hW, m->hE,
+                        m->eta, m->ubt, m->vbt, m->ubt_av, m->vbt_av, m->eta_av,
+                        m->taux_bot, m->tauy_bot, m->FA_u_W0, m->FA_u_WW, m->FA_u_E0,
+                        m->FA_u_EE, m->uBT_WW, m->uBT_EE, m->du_cor};
+        for (int q = 0; q < 25; ++q) {
+            const size_t b = q < 10 ? b3 : b2;
+            void* c = nullptr;
+            CK(cudaMalloc(&c, b));
+            S.saved.push_back({live[q], c});
+            S.bytes.push_back(b);
+            CK(cudaMemcpyAsync(c, live[q], b, cudaMemcpyDeviceToDevice, e->s));
+        }
+    }
+    CK(cudaStreamSynchronize(e->s));
+    return MOM6B_OK;
+}
+
+static int ens_restore(mom6b_ensemble* e, EnsSnapshot& S)
+{
+    for (size_t q = 0; q < S.saved.size(); ++q)
+        CK(cudaMemcpyAsync(S.saved[q].first, S.saved[q].second, S.bytes[q],
+                           cudaMemcpyDeviceToDevice, e->s));
+    CK(cudaStreamSynchronize(e->s));
+    for (auto& p : S.saved) cudaFree(p.second);
+    S.saved.clear();
+    return MOM6B_OK;
+}
+
+// Time `reps` launches of phase ph under the current plan; the best average
+// of three rounds, in ms.
+static int ens_time_phase(mom6b_ensemble* e, int ph, int reps, double* ms)
+{
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    double best = 1e30;
+    if (int rc = ens_launch(e, ph)) return rc;   // warm-up
+    for (int round = 0; round < 3; ++round) {
+        CK(cudaEventRecord(a, e->s));
+        for (int r = 0; r < reps; ++r)
+            if (int rc = ens_launch(e, ph)) return rc;
+        CK(cudaEventRecord(b, e->s));
+        CK(cudaEventSynchronize(b));
+        float t = 0.f;
+        CK(cudaEventElapsedTime(&t, a, b));
+        best = std::min(best, (double)t / reps);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (int rc = ens_check_status(e)) return rc;
+    *ms = best;
+    return MOM6B_OK;
+}
+
+// The autotuner: for each phase group, time every candidate launch shape on
+// the ensemble's own domains (state saved before and restored after) and keep
+// the fastest.  out_ms (optional, 5 entries) receives the best time of the
+// tendency, vertvisc, PPM, faces and barotropic launches.
+extern "C" int mom6b_ensemble_autotune(mom6b_ensemble* e, int reps, double* out_ms)
+{
+    if (!e) return fail(MOM6B_ERR_ARG, "null ensemble");
+    if (reps < 1) reps = 1;
+    CK(cudaSetDevice(e->device));
+    CK(cudaStreamSynchronize(e->s));
+    EnsSnapshot S;
+    if (int rc = ens_snapshot(e, S)) return rc;
+    EnsTuning best = e->T;
+    double tbest[5] = {0, 0, 0, 0, 0};
+    auto sweep = [&](int slot, int ph, const std::vector<EnsTuning>& cands) -> int {
+        double bt = 1e30;
+        EnsTuning bc = best;
+        for (const EnsTuning& c : cands) {
+            e->T = c;
+            if (int rc = ens_plan(e)) return rc;
+            double ms = 0.0;
+            if (int rc = ens_time_phase(e, ph, reps, &ms)) return rc;
+            if (ms < bt) { bt = ms; bc = c; }
+        }
+        best = bc;
+        tbest[slot] = bt;
+        return MOM6B_OK;
+    };
+    std::vector<EnsTuning> c;
+    for (int t = 0; t < 4; ++t)
+        for (int kc : {3, 5, 8}) { EnsTuning x = best; x.tend = t; x.tend_kc = kc; c.push_back(x); }
+    int rc = sweep(0, 0, c);
+    if (!rc) {
+        c.clear();
+        for (int nb : {64, 128, 256})
+            for (int ch : {2, 4}) { EnsTuning x = best; x.vv_nb = nb; x.vv_ch = ch; c.push_back(x); }
+        rc = sweep(1, 1, c);
+    }
+    if (!rc) {
+        c.clear();
+        for (int nb : {128, 256}) { EnsTuning x = best; x.ppm_nb = nb; c.push_back(x); }
+        rc = sweep(2, 2, c);
+    }
+    if (!rc) {
+        c.clear();
+        for (int nb : {64, 128, 256}) { EnsTuning x = best; x.faces_nb = nb; c.push_back(x); }
+        rc = sweep(3, 3, c);
+    }
+    if (!rc) {
+        c.clear();
+        for (int t : {32, 48, 64}) { EnsTuning x = best; x.bt_tile = t; c.push_back(x); }
+        rc = sweep(4, 10, c);
+    }
+    int rr = ens_restore(e, S);
+    e->T = best;
+    int rp = ens_plan(e);
+    if (rc) return rc;
+    if (rr) return rr;
+    if (rp) return rp;
+    if (out_ms) std::memcpy(out_ms, tbest, sizeof(tbest));
     return MOM6B_OK;
 }

@@ -29,14 +29,15 @@
 namespace mom6b {
 
 // UNI selects the uniform-metric instantiation (metrics as scalars, Coriolis
-// per row); otherwise every metric is read from its 2-D array.  Each CTA
-// walks KC consecutive layers of its tile.
+// per row); otherwise every metric is read from its 2-D array.  The CTA with
+// block coordinates (bx, by, bz) owns the tile i0 = is + bx TX, j0 = js + by TY
+// and walks the KC consecutive layers from k0 + bz KC.
 template <int TX, int TY, bool UNI, typename R>
-__global__ void __launch_bounds__(TX * TY)
-k_tendency(Dims D, Metrics M, UniMetrics U, const R* __restrict__ uin,
-           const R* __restrict__ vin, const R* __restrict__ h,
-           const R* ubase, const R* vbase, R* uout, R* vout,
-           R coef, R h_neglect, int k0, int KC)
+__device__ __forceinline__ void
+tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __restrict__ uin,
+              const R* __restrict__ vin, const R* __restrict__ h,
+              const R* ubase, const R* vbase, R* uout, R* vout,
+              R coef, R h_neglect, int k0, int KC, int bx, int by, int bz)
 {
     constexpr int SX = TX + 2, SY = TY + 2;  // staged inputs: [i0-1, i0+TX] x [j0-1, j0+TY]
     constexpr int CX = TX + 1, CY = TY + 1;  // intermediates
@@ -46,10 +47,10 @@ k_tendency(Dims D, Metrics M, UniMetrics U, const R* __restrict__ uin,
     __shared__ R s_uh[CY][CX];                 // u-faces  [i0-1, i0+TX-1] x [j0, j0+TY]
     __shared__ R s_vh[CY][CX];                 // v-faces  [i0, i0+TX] x [j0-1, j0+TY-1]
 
-    const int i0 = D.is + (int)blockIdx.x * TX;
-    const int j0 = D.js + (int)blockIdx.y * TY;
+    const int i0 = D.is + bx * TX;
+    const int j0 = D.js + by * TY;
     const int tid = (int)threadIdx.y * TX + (int)threadIdx.x;
-    const int kb = k0 + (int)blockIdx.z * KC;
+    const int kb = k0 + bz * KC;
     const int ke = (kb + KC - 1 < D.nk) ? kb + KC - 1 : D.nk;
   for (int k = kb; k <= ke; ++k) {
     const size_t koff = (size_t)(k - 1) * (size_t)D.plane;
@@ -217,6 +218,18 @@ k_tendency(Dims D, Metrics M, UniMetrics U, const R* __restrict__ uin,
 #undef SXX
 #undef UH
 #undef VH
+}
+
+template <int TX, int TY, bool UNI, typename R>
+__global__ void __launch_bounds__(TX * TY)
+k_tendency(Dims D, Metrics M, UniMetrics U, const R* __restrict__ uin,
+           const R* __restrict__ vin, const R* __restrict__ h,
+           const R* ubase, const R* vbase, R* uout, R* vout,
+           R coef, R h_neglect, int k0, int KC)
+{
+    tendency_tile<TX, TY, UNI, R>(D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef,
+                                  h_neglect, k0, KC, (int)blockIdx.x, (int)blockIdx.y,
+                                  (int)blockIdx.z);
 }
 
 constexpr int kTendTX = 32, kTendTY = 8, kTendKC = 5;

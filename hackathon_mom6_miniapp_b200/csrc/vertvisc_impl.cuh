@@ -29,11 +29,13 @@ __device__ __forceinline__ C vv_botfn(C z2) {
 // Layers whose inputs one prefetch brings in.
 constexpr int kVvChunk = 4;
 
+// The column of thread tx of the CTA with block coordinates (bx, by): row
+// by of the interleaved u/v row list, column bx * blockDim.x + tx.
 template <int KMAX, int CH, typename R>
-__global__ void __launch_bounds__(128)
-k_vertvisc_pf(Dims D, Metrics M, R* __restrict__ u, R* __restrict__ v,
-              const R* __restrict__ h, double dt, VVParams P,
-              double* __restrict__ taux_bot, double* __restrict__ tauy_bot)
+__device__ __forceinline__ void
+vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restrict__ v,
+                const R* __restrict__ h, double dt, const VVParams& P,
+                double* __restrict__ taux_bot, double* __restrict__ tauy_bot, int bx, int by)
 {
     // Coefficients (h_harm, z_i, botfn, hvel, a(K)) are computed in the
     // storage type R; the tridiagonal elimination (b1, d1, c1, the eliminated
@@ -41,23 +43,27 @@ k_vertvisc_pf(Dims D, Metrics M, R* __restrict__ u, R* __restrict__ v,
     using C = R;
     double slot[KMAX + 2];   // botfn(z_i(m)), then c1(m)
     const int nz = D.nk;
-    const int nrow_u = D.je - D.js + 1;
-    bool is_u = (int)blockIdx.y < nrow_u;
+    // Rows are interleaved so that the u row j and the v rows j-1, j, which
+    // read the same rows of h, run close together: by = 0 is the v
+    // row js-1, then u row js+q at 1+2q and v row js+q at 2+2q.
+    const int yb = by;
+    const bool is_u = yb >= 1 && ((yb - 1) & 1) == 0;
+    const int q = yb >= 1 ? (yb - 1) >> 1 : -1;
     int i, j, di, dj;
     R* vel;
     const double *mask, *tau, *Ray;
     const unsigned char* ray_on;
     double* tbot;
     if (is_u) {  // u columns: I in [is-1, ie], j in [js, je]
-        j = D.js + (int)blockIdx.y;
-        i = D.is - 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+        j = D.js + q;
+        i = D.is - 1 + bx * (int)blockDim.x + (int)threadIdx.x;
         if (i > D.ie) return;
         di = 1; dj = 0;
         vel = u; mask = M.mask2dCu; tau = M.taux; Ray = M.Ray_u;
         ray_on = M.ray_layer_u; tbot = taux_bot;
     } else {     // v columns: i in [is, ie], J in [js-1, je]
-        j = D.js - 1 + ((int)blockIdx.y - nrow_u);
-        i = D.is + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+        j = D.js + q;
+        i = D.is + bx * (int)blockDim.x + (int)threadIdx.x;
         if (i > D.ie) return;
         di = 0; dj = 1;
         vel = v; mask = M.mask2dCv; tau = M.tauy; Ray = M.Ray_v;
@@ -229,6 +235,16 @@ k_vertvisc_pf(Dims D, Metrics M, R* __restrict__ u, R* __restrict__ v,
             tb = tb + kRho0 * rc[o] * (double)vc[o];
         }
     tbot[(size_t)(j - 1) * D.n1 + (i - 1)] = tb;
+}
+
+template <int KMAX, int CH, typename R>
+__global__ void __launch_bounds__(128)
+k_vertvisc_pf(Dims D, Metrics M, R* __restrict__ u, R* __restrict__ v,
+              const R* __restrict__ h, double dt, VVParams P,
+              double* __restrict__ taux_bot, double* __restrict__ tauy_bot)
+{
+    vertvisc_column<KMAX, CH, R>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, (int)blockIdx.x,
+                                 (int)blockIdx.y);
 }
 
 template <int KMAX, typename R>

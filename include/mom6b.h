@@ -189,6 +189,40 @@ size_t mom6b_cudac_field_size(const mom6b_cudac *m, int field);
 int mom6b_cudac_get_field(mom6b_cudac *m, int field, double *host, size_t count);
 int mom6b_cudac_destroy(mom6b_cudac *m);
 
+/* ---- ensemble: many domains in one launch per phase -----------------------
+ * No counterpart in the reference (its drivers advance one domain).  n
+ * independent domains of any sizes (cfgs[d], each with precision
+ * MOM6B_MIXED, all on one device, nk <= 256) are built exactly as
+ * mom6b_create builds them and advanced together: one RK2 step is fourteen
+ * launches whatever n is (ten without halo fills), each covering all domains
+ * (the barotropic loops of all domains share one cooperative persistent
+ * launch per call).  Each domain gets the same arithmetic as a mixed-form
+ * model of its own.  The launch shapes come from mom6b_ensemble_autotune,
+ * which times the candidate shapes of every phase on the ensemble's domains
+ * (their state is saved before and restored after) and keeps the fastest;
+ * out_ms (5 doubles, optional) receives the best tendency, vertvisc, PPM,
+ * faces and barotropic launch times.  Tuning as 7 ints: tendency tile (0: 32x8,
+ * 1: 32x4, 2: 64x4, 3: 32x16), tendency layers per CTA (1..16), vertvisc
+ * threads per CTA (64, 128, 256), vertvisc prefetch depth (2, 4), PPM threads
+ * per CTA (128, 256), threads per continuity face CTA (64, 128, 256),
+ * barotropic tile edge (32, 48, 64).  mom6b_ensemble_member returns domain d
+ * as a model (owned by the ensemble; read it after
+ * mom6b_ensemble_synchronize, or with mom6b_ensemble_get_field). */
+typedef struct mom6b_ensemble mom6b_ensemble;
+int mom6b_ensemble_create(int n, const mom6b_config *cfgs, mom6b_ensemble **out);
+int mom6b_ensemble_destroy(mom6b_ensemble *e);
+int mom6b_ensemble_size(const mom6b_ensemble *e);
+int mom6b_ensemble_step(mom6b_ensemble *e, int nsteps);
+int mom6b_ensemble_synchronize(mom6b_ensemble *e);
+int mom6b_ensemble_stream(mom6b_ensemble *e, void **stream);
+int64_t mom6b_ensemble_launch_count(const mom6b_ensemble *e);
+mom6b_model *mom6b_ensemble_member(mom6b_ensemble *e, int d);
+int mom6b_ensemble_get_field(mom6b_ensemble *e, int d, int field, double *host,
+                             size_t count);
+int mom6b_ensemble_autotune(mom6b_ensemble *e, int reps, double *out_ms);
+int mom6b_ensemble_get_tuning(const mom6b_ensemble *e, int *out7);
+int mom6b_ensemble_set_tuning(mom6b_ensemble *e, const int *in7);
+
 const char *mom6b_last_error(void);
 const char *mom6b_version(void);
 
