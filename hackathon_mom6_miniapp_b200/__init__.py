@@ -6,10 +6,10 @@ thin Python host mirror used by tests and benchmarks: it loads the library
 with ctypes and moves numpy arrays across the boundary.  There is no CPU
 fallback: every entry point raises if the CUDA library cannot be loaded.
 """
-from ._lib import (Model, Ensemble, CudaCDriver, MixedNotBuilt, Mom6bError, FIELDS,
+from ._lib import (Model, Ensemble, Mlp, CudaCDriver, MixedNotBuilt, Mom6bError, FIELDS,
                    FIELDS_3D, INIT_CFG, INIT_REF, FP64, MIXED, TUNING_KEYS, library,
                    library_path, make_config)
 
-__all__ = ["Model", "Ensemble", "CudaCDriver", "Mom6bError", "MixedNotBuilt", "FIELDS",
+__all__ = ["Model", "Ensemble", "Mlp", "CudaCDriver", "Mom6bError", "MixedNotBuilt", "FIELDS",
            "FIELDS_3D", "INIT_CFG", "INIT_REF", "FP64", "MIXED", "TUNING_KEYS", "library",
            "library_path", "make_config"]

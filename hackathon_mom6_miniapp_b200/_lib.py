@@ -99,6 +99,24 @@ def library():
     L.mom6b_ensemble_autotune.argtypes = [vp, ctypes.c_int, P(d)]
     L.mom6b_ensemble_get_tuning.argtypes = [vp, P(ctypes.c_int)]
     L.mom6b_ensemble_set_tuning.argtypes = [vp, P(ctypes.c_int)]
+    f32p, u64 = P(ctypes.c_float), ctypes.c_uint64
+    L.mom6b_surrogate_train.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, d, u64,
+                                        P(d)]
+    L.mom6b_surrogate_enable.argtypes = [vp, ctypes.c_int, ctypes.c_int, d]
+    L.mom6b_surrogate_eval.argtypes = [vp, u64, ctypes.c_int, ctypes.c_int, P(d)]
+    L.mom6b_surrogate_status.argtypes = [vp, P(d)]
+    L.mom6b_surrogate_param_count.restype = ctypes.c_size_t
+    L.mom6b_surrogate_get_params.argtypes = [vp, f32p, ctypes.c_size_t]
+    L.mom6b_surrogate_set_params.argtypes = [vp, f32p, ctypes.c_size_t]
+    L.mom6b_mlp_param_count.restype = ctypes.c_int
+    L.mom6b_mlp_create.argtypes = [ctypes.c_int, u64, P(vp)]
+    L.mom6b_mlp_destroy.argtypes = [vp]
+    L.mom6b_mlp_get_params.argtypes = [vp, f32p, ctypes.c_size_t]
+    L.mom6b_mlp_set_params.argtypes = [vp, f32p, ctypes.c_size_t]
+    L.mom6b_mlp_gradients.argtypes = [vp, f32p, f32p, ctypes.c_int, f32p, f32p, f32p]
+    L.mom6b_mlp_train.argtypes = [vp, f32p, f32p, ctypes.c_int, ctypes.c_float, ctypes.c_int,
+                                  f32p]
+    L.mom6b_mlp_predict.argtypes = [vp, f32p, ctypes.c_int, f32p]
     L.mom6b_last_error.restype = ctypes.c_char_p
     L.mom6b_version.restype = ctypes.c_char_p
     _LIB = L
@@ -219,6 +237,44 @@ class Model:
                                               ctypes.byref(n)))
         return ms.value, n.value
 
+    # ---- learned barotropic surrogate ----
+    def surrogate_train(self, nstates=8, nsteps=2000, batch=65536, lr=1e-3, seed=1):
+        out = (ctypes.c_double * 4)()
+        _check(library().mom6b_surrogate_train(self._m, int(nstates), int(nsteps), int(batch),
+                                               float(lr), int(seed), out))
+        return dict(zip(["loss_first", "loss_last", "batches", "seconds"], list(out)))
+
+    def surrogate_eval(self, seed=1, state=100, nsteps=10):
+        """Transport error of the network on a held-out state of the seeded
+        family (see mom6b_surrogate_eval)."""
+        out = (ctypes.c_double * 3)()
+        _check(library().mom6b_surrogate_eval(self._m, int(seed), int(state), int(nsteps), out))
+        return dict(zip(["rel_error", "zero_prediction_error", "calls"], list(out)))
+
+    def surrogate_enable(self, on=True, shadow_every=10, threshold=1e-3):
+        _check(library().mom6b_surrogate_enable(self._m, int(on), int(shadow_every),
+                                                float(threshold)))
+
+    def surrogate_status(self):
+        out = (ctypes.c_double * 10)()
+        _check(library().mom6b_surrogate_status(self._m, out))
+        keys = ["enabled", "fallen_back", "steps", "shadow_checks", "fallbacks",
+                "last_shadow_error", "max_shadow_error", "loss_first", "loss_last",
+                "train_batches"]
+        return dict(zip(keys, list(out)))
+
+    def surrogate_params(self):
+        n = int(library().mom6b_surrogate_param_count())
+        a = np.zeros(n, dtype=np.float32)
+        _check(library().mom6b_surrogate_get_params(
+            self._m, a.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), n))
+        return a
+
+    def set_surrogate_params(self, a):
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        _check(library().mom6b_surrogate_set_params(
+            self._m, a.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), a.size))
+
 
 def make_config(ni=180, nj=180, nk=75, bt_nsteps=30, init_mode=INIT_CFG, seed=0, dt=None,
                 Kh=None, bc_fill=None, precision=FP64, device=0, use_graph=False):
@@ -325,6 +381,66 @@ class Ensemble:
     def set_tuning(self, t):
         vals = (ctypes.c_int * 7)(*[int(t[k]) for k in TUNING_KEYS])
         _check(library().mom6b_ensemble_set_tuning(self._e, vals))
+
+
+def _fptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+class Mlp:
+    """The surrogate network alone (mom6b_mlp_*): gradients, Adam steps and
+    predictions of batches of 175 fp32 features."""
+
+    def __init__(self, batch=1024, seed=0):
+        h = ctypes.c_void_p()
+        _check(library().mom6b_mlp_create(int(batch), int(seed), ctypes.byref(h)))
+        self._p = h
+        self.nparams = int(library().mom6b_mlp_param_count())
+
+    def close(self):
+        if getattr(self, "_p", None):
+            library().mom6b_mlp_destroy(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self):
+        a = np.zeros(self.nparams, dtype=np.float32)
+        _check(library().mom6b_mlp_get_params(self._p, _fptr(a), a.size))
+        return a
+
+    def set_params(self, a):
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        _check(library().mom6b_mlp_set_params(self._p, _fptr(a), a.size))
+
+    def gradients(self, X, Y):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.ascontiguousarray(Y, dtype=np.float32)
+        B = X.shape[0]
+        g = np.zeros(self.nparams, dtype=np.float32)
+        loss = np.zeros(1, dtype=np.float32)
+        out = np.zeros((B, 2), dtype=np.float32)
+        _check(library().mom6b_mlp_gradients(self._p, _fptr(X), _fptr(Y), B, _fptr(g),
+                                             _fptr(loss), _fptr(out)))
+        return g, float(loss[0]), out
+
+    def train(self, X, Y, lr=1e-3, nsteps=1):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.ascontiguousarray(Y, dtype=np.float32)
+        losses = np.zeros(max(nsteps, 1), dtype=np.float32)
+        _check(library().mom6b_mlp_train(self._p, _fptr(X), _fptr(Y), X.shape[0], float(lr),
+                                         int(nsteps), _fptr(losses)))
+        return losses[:nsteps]
+
+    def predict(self, X):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        out = np.zeros((X.shape[0], 2), dtype=np.float32)
+        _check(library().mom6b_mlp_predict(self._p, _fptr(X), X.shape[0], _fptr(out)))
+        return out
 
 
 class CudaCDriver:

@@ -312,7 +312,10 @@ __device__ __forceinline__ bool wait_neighbours(const BTWork& W, const int* nb, 
     return s_wok != 0;
 }
 
-template <int NT, bool UNI>
+// TAVG: also accumulate the substep-averaged transports (1/nstep) sum_n
+// uhbt_n, vhbt_n of the owned points into W.uhbt / W.vhbt (the surrogate's
+// training targets; zero outside their ranges).
+template <int NT, bool UNI, bool TAVG>
 __global__ void __launch_bounds__(NT, 1)
 k_btstep_tiled(Dims D, Metrics M, UniMetrics U, BTWork W, BTParams P, BTTiles T,
                const double* eta_in, const double* ubt_in, const double* vbt_in,
@@ -358,6 +361,7 @@ k_btstep_tiled(Dims D, Metrics M, UniMetrics U, BTWork W, BTParams P, BTTiles T,
         double e = eta_in[p], ub = ubt_in[p], vb = vbt_in[p];
         W.eta[p] = e; W.ubt[p] = ub; W.vbt[p] = vb;
         W.eta_pred[p] = e; W.ubt_prev[p] = ub; W.vbt_prev[p] = vb;
+        if (TAVG) { W.uhbt[p] = 0.0; W.vhbt[p] = 0.0; }
     }
     if (tid == 0) W.tile_flag[blockIdx.x] = 0u;
     if (!grid_barrier(W, nblocks, P.spin_budget)) return;
@@ -483,6 +487,12 @@ k_btstep_tiled(Dims D, Metrics M, UniMetrics U, BTWork W, BTParams P, BTTiles T,
                 avu[r] = avu[r] + L(Sun, i, j) * P.inv_nstep;
             if (j >= jv0 && j <= jv1 && i >= is && i <= ie)
                 avv[r] = avv[r] + L(Svn, i, j) * P.inv_nstep;
+            if (TAVG) {
+                if (j >= js && j <= je && i >= iu0 && i <= iu1)
+                    W.uhbt[p] = W.uhbt[p] + uhbt_at(i, j) * P.inv_nstep;
+                if (j >= jv0 && j <= jv1 && i >= is && i <= ie)
+                    W.vhbt[p] = W.vhbt[p] + vhbt_at(i, j) * P.inv_nstep;
+            }
         }
         // publish substep n: every global write of this tile is done
         __syncthreads();
@@ -790,12 +800,14 @@ static cudaError_t launch_btstep_tiled(const Dims& D, const Metrics& M, const Un
                                        const BTWork& W, const BTParams& P, const BTTiles& T,
                                        const double* eta_in, const double* ubt_in,
                                        const double* vbt_in, double* u_av, double* v_av,
-                                       double* eta_av, cudaStream_t s)
+                                       double* eta_av, cudaStream_t s, bool tavg = false)
 {
     const int NT = 1024;
     size_t smem = (size_t)6 * (T.tw + 3) * (T.th + 3) * sizeof(double);
-    const void* fn = U.valid_bt ? (const void*)k_btstep_tiled<NT, true>
-                                : (const void*)k_btstep_tiled<NT, false>;
+    const void* fn = tavg ? (U.valid_bt ? (const void*)k_btstep_tiled<NT, true, true>
+                                        : (const void*)k_btstep_tiled<NT, false, true>)
+                          : (U.valid_bt ? (const void*)k_btstep_tiled<NT, true, false>
+                                        : (const void*)k_btstep_tiled<NT, false, false>);
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
@@ -908,6 +920,19 @@ cudaError_t launch_ens_btstep(const EnsDomain* doms, const EnsBtGeo* geo, const 
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     return cudaLaunchKernelExC(&cfg, fn, args);
+}
+
+cudaError_t launch_btstep_tavg(const Dims& D, const Metrics& M, const UniMetrics& U,
+                               const BTWork& W, const BTParams& P, const double* eta_in,
+                               const double* ubt_in, const double* vbt_in, double* u_av,
+                               double* v_av, double* eta_av, cudaStream_t s)
+{
+    cudaError_t e0 = init_bt_blocks();
+    if (e0 != cudaSuccess) return e0;
+    BTTiles T;
+    if (!tiles_for(D, T)) return cudaErrorNotSupported;
+    return launch_btstep_tiled(D, M, U, W, P, T, eta_in, ubt_in, vbt_in, u_av, v_av, eta_av, s,
+                               true);
 }
 
 // ---------------------------------------------------------------------------

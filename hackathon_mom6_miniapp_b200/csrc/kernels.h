@@ -75,6 +75,12 @@ cudaError_t launch_btstep(const Dims& D, const Metrics& M, const UniMetrics& U,
                           const BTParams& P, const double* eta_in,
                           const double* ubt_in, const double* vbt_in, double* u_av,
                           double* v_av, double* eta_av, cudaStream_t s);
+// The same loop, also leaving the substep-averaged transports in W.uhbt /
+// W.vhbt (tiled grids only; cudaErrorNotSupported otherwise).
+cudaError_t launch_btstep_tavg(const Dims& D, const Metrics& M, const UniMetrics& U,
+                               const BTWork& W, const BTParams& P, const double* eta_in,
+                               const double* ubt_in, const double* vbt_in, double* u_av,
+                               double* v_av, double* eta_av, cudaStream_t s);
 cudaError_t launch_halo_fill(const Dims& D, double* f, int nz, int kind, cudaStream_t s);
 
 // Mixed-precision form (k_mixed.cu): FP32 state and stencils, FP64 column

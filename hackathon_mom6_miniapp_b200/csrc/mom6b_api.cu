@@ -35,6 +35,7 @@
 #include "../../include/mom6b.h"
 #include "host_init.h"
 #include "kernels.h"
+#include "mlp.h"
 
 
 using namespace mom6b;
@@ -86,6 +87,22 @@ struct mom6b_model {
     bool timing = false;
     std::vector<TimedLaunch> pending;
     std::map<std::string, std::pair<double, int64_t>> timed;  // ms total, launches
+    // learned barotropic surrogate (k_mlp.cu): the network, whether it
+    // replaces btstep, the shadow check (every sur_every steps the plain loop
+    // runs from the same state and judges the surrogate's eta) and its record
+    std::unique_ptr<Mlp> sur;
+    bool sur_on = false, sur_fallen = false;
+    int sur_every = 10;
+    double sur_thresh = 1.0e-3;
+    int64_t sur_steps = 0, sur_checks = 0, sur_fallbacks = 0;
+    double sur_last_err = 0.0, sur_max_err = 0.0;
+    double sur_loss_first = 0.0, sur_loss_last = 0.0, sur_train_s = 0.0;
+    int64_t sur_train_steps = 0;
+    double *sh_eta = nullptr, *sh_ubt_av = nullptr, *sh_vbt_av = nullptr, *sh_eta_av = nullptr;
+    double* sur_acc = nullptr;
+    // barotropic state of the training and evaluation runs
+    double *tr_e = nullptr, *tr_u = nullptr, *tr_v = nullptr;
+    double *tr_ea = nullptr, *tr_ua = nullptr, *tr_va = nullptr;
 };
 
 static double* dalloc(mom6b_model* m, size_t n, cudaError_t* err)
@@ -483,6 +500,83 @@ static BTParams step_bt_params(const mom6b_config& c)
     return P;
 }
 
+// Grid quantities of the surrogate kernels.
+static SurGrid sur_grid(const mom6b_model* m)
+{
+    SurGrid g;
+    g.D = m->D;
+    g.IareaT = m->M.IareaT;
+    g.Datu = m->M.Datu;
+    g.Datv = m->M.Datv;
+    g.cor = m->M.CoriolisBu;
+    g.depth = 4000.0;   // the flat bottom of init_ocean_grid (barotropic_init's Datu, Datv)
+    const BTParams P = step_bt_params(m->cfg);
+    g.dt_total = P.dtbt * (double)P.nstep;
+    g.iu0 = P.extended ? m->D.is - 1 : m->D.is;
+    g.iu1 = P.extended ? m->D.ie : m->D.ie - 1;
+    g.jv0 = P.extended ? m->D.js - 1 : m->D.js;
+    g.jv1 = P.extended ? m->D.je : m->D.je - 1;
+    return g;
+}
+
+// One surrogate barotropic call: features of every compute cell from
+// (eta, ubt, vbt), the network, and the FP64 eta advance from the divergence
+// of the predicted substep-averaged transports.
+static int surrogate_call(mom6b_model* m, const double* eta, const double* ubt,
+                          const double* vbt, double* u_av, double* v_av, double* eta_out,
+                          cudaStream_t s)
+{
+    const SurGrid g = sur_grid(m);
+    const int nc = (m->D.ie - m->D.is + 1) * (m->D.je - m->D.js + 1);
+    Mlp& N = *m->sur;
+    CK(N.prepare_inference(nc));
+    CK(timed(m, s, "surrogate", [&] {
+        return launch_sur_features_all(g, BtInputs{eta, ubt, vbt}, N.d_norm, N.Xi, s); }));
+    CK(timed(m, s, "surrogate", [&] { return N.predict(nc, s); }));
+    m->launches += 1;   // predict is two launches
+    CK(timed(m, s, "surrogate", [&] {
+        return launch_sur_advance(g, N.outi, N.d_norm, eta, eta_out, u_av, v_av, s); }));
+    return MOM6B_OK;
+}
+
+static int enqueue_surrogate_chain(mom6b_model* m, cudaStream_t s)
+{
+    const Dims& D = m->D;
+    const bool fill = m->cfg.bc_fill != 0;
+    if (int rc = surrogate_call(m, m->eta, m->ubt, m->vbt, m->ubt_av, m->vbt_av, m->eta_av, s))
+        return rc;
+    if (fill) {
+        CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->eta_av, 1, 0, s); }));
+        CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->ubt_av, 1, 1, s); }));
+        CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->vbt_av, 1, 2, s); }));
+    }
+    if (int rc = surrogate_call(m, m->eta_av, m->ubt_av, m->vbt_av, m->ubt_av, m->vbt_av,
+                                m->eta, s))
+        return rc;
+    if (fill)
+        CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->eta, 1, 0, s); }));
+    return MOM6B_OK;
+}
+
+// The plain barotropic chain from the model's (eta, ubt, vbt) into the
+// shadow buffers (the judge of the surrogate).
+static int enqueue_shadow_chain(mom6b_model* m, cudaStream_t s)
+{
+    const Dims& D = m->D;
+    const BTParams P = step_bt_params(m->cfg);
+    CK(launch_btstep(D, m->M, m->U, m->bt, P, m->eta, m->ubt, m->vbt, m->sh_ubt_av,
+                     m->sh_vbt_av, m->sh_eta_av, s));
+    if (m->cfg.bc_fill) {
+        CK(launch_halo_fill(D, m->sh_eta_av, 1, 0, s));
+        CK(launch_halo_fill(D, m->sh_ubt_av, 1, 1, s));
+        CK(launch_halo_fill(D, m->sh_vbt_av, 1, 2, s));
+    }
+    CK(launch_btstep(D, m->M, m->U, m->bt, P, m->sh_eta_av, m->sh_ubt_av, m->sh_vbt_av,
+                     m->sh_ubt_av, m->sh_vbt_av, m->sh_eta, s));
+    if (m->cfg.bc_fill) CK(launch_halo_fill(D, m->sh_eta, 1, 0, s));
+    return MOM6B_OK;
+}
+
 static int enqueue_step(mom6b_model* m)
 {
     const Dims& D = m->D;
@@ -578,6 +672,15 @@ static int enqueue_step(mom6b_model* m)
     }
 
     // ---- barotropic chain ----
+    if (m->sur && m->sur_on && !m->sur_fallen) {
+        int rc = enqueue_surrogate_chain(m, s2);
+        if (rc) return rc;
+        if (s2 != s) {
+            CK(cudaEventRecord(m->ev_join, s2));
+            CK(cudaStreamWaitEvent(s, m->ev_join, 0));
+        }
+        return MOM6B_OK;
+    }
     BTParams P = step_bt_params(c);
     CK(timed(m, s2, "btstep", [&] {
         return launch_btstep(D, M, m->U, m->bt, P, m->eta, m->ubt, m->vbt, m->ubt_av,
@@ -623,10 +726,69 @@ static int capture_step(mom6b_model* m)
     return MOM6B_OK;
 }
 
+static void invalidate_graph(mom6b_model* m)
+{
+    if (m->graph_exec) { cudaGraphExecDestroy(m->graph_exec); m->graph_exec = nullptr; }
+    if (m->graph) { cudaGraphDestroy(m->graph); m->graph = nullptr; }
+}
+
+static int check_status(mom6b_model* m);
+static int step_plain_or_graph(mom6b_model* m, int nsteps);
+
+// One step with the shadow check: the plain barotropic chain runs into the
+// shadow buffers from the same (eta, ubt, vbt), the step runs with the
+// surrogate, and the relative L2 difference of the two etas over the compute
+// domain decides: above the threshold the plain results replace the
+// surrogate's and the model keeps the plain btstep from then on.
+static int shadow_step(mom6b_model* m)
+{
+    cudaStream_t s = m->s3d;
+    if (int rc = enqueue_shadow_chain(m, s)) return rc;
+    if (int rc = enqueue_step(m)) return rc;
+    CK(launch_sur_diff(m->D, m->eta, m->sh_eta, m->sur_acc, s));
+    double acc[2] = {0.0, 0.0};
+    CK(cudaMemcpyAsync(acc, m->sur_acc, sizeof(acc), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (int rc = check_status(m)) return rc;
+    const double err = acc[1] > 0.0 ? std::sqrt(acc[0] / acc[1]) : std::sqrt(acc[0]);
+    m->sur_last_err = err;
+    m->sur_max_err = std::max(m->sur_max_err, err);
+    ++m->sur_checks;
+    if (!(err <= m->sur_thresh)) {
+        const size_t b = m->grid->plane * sizeof(double);
+        CK(cudaMemcpyAsync(m->eta, m->sh_eta, b, cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemcpyAsync(m->eta_av, m->sh_eta_av, b, cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemcpyAsync(m->ubt_av, m->sh_ubt_av, b, cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemcpyAsync(m->vbt_av, m->sh_vbt_av, b, cudaMemcpyDeviceToDevice, s));
+        m->sur_fallen = true;
+        ++m->sur_fallbacks;
+        invalidate_graph(m);
+    }
+    return MOM6B_OK;
+}
+
 extern "C" int mom6b_step(mom6b_model* m, int nsteps)
 {
     if (!m || nsteps < 0) return fail(MOM6B_ERR_ARG, "bad argument");
     CK(cudaSetDevice(m->cfg.device));
+    if (m->sur && m->sur_on && !m->sur_fallen) {
+        for (int n = 0; n < nsteps; ++n) {
+            const bool shadow = m->sur_every > 0 && (m->sur_steps % m->sur_every) == 0 &&
+                                !m->sur_fallen;
+            ++m->sur_steps;
+            if (shadow) {
+                if (int rc = shadow_step(m)) return rc;
+                continue;
+            }
+            if (int rc = step_plain_or_graph(m, 1)) return rc;
+        }
+        return MOM6B_OK;
+    }
+    return step_plain_or_graph(m, nsteps);
+}
+
+static int step_plain_or_graph(mom6b_model* m, int nsteps)
+{
     if (m->cfg.use_graph && !m->timing) {
         if (!m->graph_exec) {
             if (int rc = capture_step(m)) return rc;
@@ -1444,5 +1606,481 @@ extern "C" int mom6b_ensemble_autotune(mom6b_ensemble* e, int reps, double* out_
     if (rr) return rr;
     if (rp) return rp;
     if (out_ms) std::memcpy(out_ms, tbest, sizeof(tbest));
+    return MOM6B_OK;
+}
+
+// ===========================================================================
+// Learned barotropic surrogate: training, control and the network's own ABI
+// ===========================================================================
+static uint64_t sur_hash(uint64_t z)
+{
+    z += 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+// Barotropic initial state k of the training set: a Gaussian eta bump whose
+// amplitude (0.05 .. 0.15 m), centre (the middle half of the basin in each
+// direction) and radius (120 .. 280 km) are drawn from (seed, k); ubt = vbt = 0
+// as in the configured beta-plane state.
+static void sur_initial_eta(const mom6b_model* m, uint64_t seed, int k, std::vector<double>& eta)
+{
+    const HostGrid& g = *m->grid;
+    uint64_t st = sur_hash(seed * 1000003ULL + (uint64_t)k);
+    auto uni = [&]() {
+        st = sur_hash(st);
+        return (double)(st >> 11) * (1.0 / 9007199254740992.0);
+    };
+    const double amp = 0.1 * (0.5 + uni());
+    const double cxf = 0.25 + 0.5 * uni(), cyf = 0.25 + 0.5 * uni();
+    const double R = 200.0e3 * (0.6 + 0.8 * uni());
+    const double Lx = (double)(g.ie - g.is + 1) * g.dx, Ly = (double)(g.je - g.js + 1) * g.dx;
+    eta.assign(g.plane, 0.0);
+    for (int j = g.jsd; j <= g.jed; ++j)
+        for (int i = g.isd; i <= g.ied; ++i) {
+            const double x = ((double)(i - g.is) + 0.5) * g.dx - cxf * Lx;
+            const double y = ((double)(j - g.js) + 0.5) * g.dx - cyf * Ly;
+            eta[g.at(i, j)] = amp * std::exp(-(x * x + y * y) / (R * R));
+        }
+}
+
+// Shadow and training buffers (allocated once, before any capture).
+static int sur_buffers(mom6b_model* m)
+{
+    if (m->sh_eta) return MOM6B_OK;
+    cudaError_t err = cudaSuccess;
+    const size_t n2 = m->grid->plane;
+    m->sh_eta = dalloc(m, n2, &err);
+    m->sh_ubt_av = dalloc(m, n2, &err);
+    m->sh_vbt_av = dalloc(m, n2, &err);
+    m->sh_eta_av = dalloc(m, n2, &err);
+    m->sur_acc = dalloc(m, 4, &err);
+    if (err != cudaSuccess || !m->sur_acc) return fail(MOM6B_ERR_NOMEM, "device allocation failed");
+    return MOM6B_OK;
+}
+
+// channel sums over the compute domain for the normalisation
+struct ChanStats {
+    double n = 0, s = 0, s2 = 0;
+    void add(double v) { n += 1; s += v; s2 += v * v; }
+    // std, or |mean| (or 1) when the channel is constant
+    float scale() const
+    {
+        if (n <= 0) return 1.0f;
+        const double mu = s / n;
+        const double var = std::max(0.0, s2 / n - mu * mu);
+        const double sd = std::sqrt(var);
+        if (sd > 1e-12 * std::max(std::fabs(mu), 1e-300)) return (float)sd;
+        return std::fabs(mu) > 0 ? (float)std::fabs(mu) : 1.0f;
+    }
+};
+
+static int sur_train_buffers(mom6b_model* m)
+{
+    if (m->tr_e) return MOM6B_OK;
+    cudaError_t err = cudaSuccess;
+    const size_t n2 = m->grid->plane;
+    m->tr_e = dalloc(m, n2, &err);
+    m->tr_u = dalloc(m, n2, &err);
+    m->tr_v = dalloc(m, n2, &err);
+    m->tr_ea = dalloc(m, n2, &err);
+    m->tr_ua = dalloc(m, n2, &err);
+    m->tr_va = dalloc(m, n2, &err);
+    if (err != cudaSuccess || !m->tr_va) return fail(MOM6B_ERR_NOMEM, "device allocation failed");
+    return MOM6B_OK;
+}
+
+// training / evaluation state k of the seeded family (synchronous)
+static int sur_reset_state(mom6b_model* m, uint64_t seed, int k, cudaStream_t s)
+{
+    const size_t n2 = m->grid->plane;
+    std::vector<double> eta;
+    sur_initial_eta(m, seed, k, eta);
+    CK(cudaMemcpyAsync(m->tr_e, eta.data(), n2 * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(m->tr_u, 0, n2 * sizeof(double), s));
+    CK(cudaMemsetAsync(m->tr_v, 0, n2 * sizeof(double), s));
+    if (m->cfg.bc_fill) CK(launch_halo_fill(m->D, m->tr_e, 1, 0, s));
+    CK(cudaStreamSynchronize(s));
+    return MOM6B_OK;
+}
+
+// one plain barotropic call that also leaves the averaged transports in
+// bt.uhbt / bt.vhbt
+static int sur_plain_call(mom6b_model* m, const double* e, const double* u, const double* v,
+                          double* uo, double* vo, double* eo, cudaStream_t s)
+{
+    CK(launch_btstep_tavg(m->D, m->M, m->U, m->bt, step_bt_params(m->cfg), e, u, v, uo, vo, eo,
+                          s));
+    return MOM6B_OK;
+}
+
+static int sur_fill3(mom6b_model* m, double* e, double* u, double* v, cudaStream_t s)
+{
+    if (!m->cfg.bc_fill) return MOM6B_OK;
+    CK(launch_halo_fill(m->D, e, 1, 0, s));
+    CK(launch_halo_fill(m->D, u, 1, 1, s));
+    CK(launch_halo_fill(m->D, v, 1, 2, s));
+    return MOM6B_OK;
+}
+
+// Run nsteps RK2 barotropic chains of state k with the plain btstep; visit
+// is called with the inputs of every call before it and after it (phase 0
+// and 1, with the call's index).
+template <class Visit>
+static int sur_run_state(mom6b_model* m, uint64_t seed, int k, int nsteps, cudaStream_t s,
+                         Visit&& visit)
+{
+    if (int rc = sur_reset_state(m, seed, k, s)) return rc;
+    double *te = m->tr_e, *tu = m->tr_u, *tv = m->tr_v;
+    double *tea = m->tr_ea, *tua = m->tr_ua, *tva = m->tr_va;
+    for (int n = 0; n < nsteps; ++n) {
+        if (int rc = visit(0, 2 * n, te, tu, tv)) return rc;
+        if (int rc = sur_plain_call(m, te, tu, tv, tua, tva, tea, s)) return rc;
+        if (int rc = visit(1, 2 * n, te, tu, tv)) return rc;
+        if (int rc = sur_fill3(m, tea, tua, tva, s)) return rc;
+        if (int rc = visit(0, 2 * n + 1, tea, tua, tva)) return rc;
+        if (int rc = sur_plain_call(m, tea, tua, tva, tua, tva, te, s)) return rc;
+        if (int rc = visit(1, 2 * n + 1, tea, tua, tva)) return rc;
+        if (m->cfg.bc_fill) CK(launch_halo_fill(m->D, te, 1, 0, s));
+    }
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_surrogate_train(mom6b_model* m, int nstates, int nsteps, int batch,
+                                     double lr, uint64_t seed, double* stats4)
+{
+    if (!m || nstates < 1 || nsteps < 1 || batch < 128 || batch % 8)
+        return fail(MOM6B_ERR_ARG, "bad argument (batch: a multiple of 8, at least 128)");
+    CK(cudaSetDevice(m->cfg.device));
+    cudaStream_t s = m->s3d;
+    CK(cudaStreamSynchronize(s));
+    CK(cudaStreamSynchronize(m->s2d));
+    const auto t0 = std::chrono::steady_clock::now();
+    if (!m->sur || m->sur->B_cap < batch) {
+        auto N = std::make_unique<Mlp>();
+        CK(N->init(batch, seed, s));
+        m->sur = std::move(N);
+    }
+    if (int rc = sur_buffers(m)) return rc;
+    if (int rc = sur_train_buffers(m)) return rc;
+    Mlp& N = *m->sur;
+    const HostGrid& hg = *m->grid;
+    const size_t n2 = hg.plane;
+    const SurGrid g = sur_grid(m);
+
+    // 1. normalisation from the first state's first steps: channel stds of the
+    //    call inputs and of the targets over the compute domain
+    {
+        ChanStats cs[kMlpChannels], ts[2];
+        std::vector<double> a(n2), b(n2), c(n2), tu_h(n2), tv_h(n2);
+        auto visit = [&](int phase, int, const double* e, const double* u, const double* v) -> int {
+            if (phase == 0) {
+                CK(cudaStreamSynchronize(s));
+                CK(cudaMemcpy(a.data(), e, n2 * sizeof(double), cudaMemcpyDeviceToHost));
+                CK(cudaMemcpy(b.data(), u, n2 * sizeof(double), cudaMemcpyDeviceToHost));
+                CK(cudaMemcpy(c.data(), v, n2 * sizeof(double), cudaMemcpyDeviceToHost));
+                return MOM6B_OK;
+            }
+            CK(cudaStreamSynchronize(s));
+            CK(cudaMemcpy(tu_h.data(), m->bt.uhbt, n2 * sizeof(double), cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(tv_h.data(), m->bt.vhbt, n2 * sizeof(double), cudaMemcpyDeviceToHost));
+            for (int j = hg.js; j <= hg.je; ++j)
+                for (int i = hg.is; i <= hg.ie; ++i) {
+                    const size_t p = hg.at(i, j);
+                    cs[0].add(a[p]); cs[1].add(b[p]); cs[2].add(c[p]);
+                    ts[0].add(tu_h[p]); ts[1].add(tv_h[p]);
+                }
+            return MOM6B_OK;
+        };
+        if (int rc = sur_run_state(m, seed, 0, std::min(nsteps, 10), s, visit)) return rc;
+        std::vector<double> cor(n2);
+        CK(cudaMemcpy(cor.data(), m->M.CoriolisBu, n2 * sizeof(double), cudaMemcpyDeviceToHost));
+        for (int j = hg.js; j <= hg.je; ++j)
+            for (int i = hg.is; i <= hg.ie; ++i) cs[6].add(cor[hg.at(i, j)]);
+        cs[5].add(g.depth);
+        for (int q = 0; q < kMlpChannels; ++q) N.feat_std[q] = cs[q].scale();
+        N.targ_std[0] = ts[0].scale();
+        N.targ_std[1] = ts[1].scale();
+        float nrm[16] = {0};
+        for (int q = 0; q < kMlpChannels; ++q) nrm[q] = 1.0f / N.feat_std[q];
+        nrm[7] = N.targ_std[0];
+        nrm[8] = N.targ_std[1];
+        CK(cudaMemcpy(N.d_norm, nrm, sizeof(nrm), cudaMemcpyHostToDevice));
+    }
+
+    // 2. training: every barotropic call of every step of every state gives one
+    //    batch of sampled columns and one Adam step
+    const int64_t total = (int64_t)nstates * nsteps * 2;
+    float* dloss = nullptr;
+    CK(cudaMalloc(&dloss, (size_t)total * sizeof(float)));
+    std::unique_ptr<float, decltype(&cudaFree)> dloss_guard(dloss, cudaFree);
+    int64_t q = 0;
+    uint64_t cseed = 0;
+    auto train_visit = [&](int phase, int, const double* e, const double* u,
+                           const double* v) -> int {
+        if (phase == 0) {   // features of the inputs, before the call overwrites them
+            cseed = sur_hash(seed ^ (0x5DEECE66DULL * (uint64_t)(q + 1)));
+            CK(launch_sur_features_train(g, BtInputs{e, u, v}, N.d_norm, batch, cseed, N.X, N.XT,
+                                         s));
+            return MOM6B_OK;
+        }
+        CK(launch_sur_targets(g, m->bt.uhbt, m->bt.vhbt, N.d_norm, batch, cseed, N.Y, s));
+        CK(N.train_step(batch, (float)lr, s));
+        CK(cudaMemcpyAsync(dloss + q, N.loss, sizeof(float), cudaMemcpyDeviceToDevice, s));
+        ++q;
+        return MOM6B_OK;
+    };
+    for (int k = 0; k < nstates; ++k)
+        if (int rc = sur_run_state(m, seed, k, nsteps, s, train_visit)) return rc;
+    CK(cudaStreamSynchronize(s));
+    int gerr = 0;
+    CK(cudaMemcpy(&gerr, N.err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (gerr) return fail(MOM6B_ERR_TIMEOUT, "tensor-core pipeline wait timed out");
+    if (int rc = check_status(m)) return rc;
+    std::vector<float> L((size_t)total);
+    CK(cudaMemcpy(L.data(), dloss, (size_t)total * sizeof(float), cudaMemcpyDeviceToHost));
+    auto mean = [&](int64_t lo, int64_t hi) {
+        double acc = 0.0;
+        for (int64_t t = lo; t < hi; ++t) acc += L[(size_t)t];
+        return hi > lo ? acc / (double)(hi - lo) : 0.0;
+    };
+    const int64_t w = std::min<int64_t>(total, 100);
+    m->sur_loss_first = mean(0, std::min<int64_t>(total, 10));
+    m->sur_loss_last = mean(total - w, total);
+    m->sur_train_steps += total;
+    m->sur_train_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (stats4) {
+        stats4[0] = m->sur_loss_first;
+        stats4[1] = m->sur_loss_last;
+        stats4[2] = (double)total;
+        stats4[3] = m->sur_train_s;
+    }
+    invalidate_graph(m);
+    return MOM6B_OK;
+}
+
+// Transport error of the network on state k of the seeded family (use a k the
+// training did not see): over nsteps RK2 barotropic chains of the plain
+// btstep, the network predicts the averaged transports of every compute cell
+// from each call's inputs.  out3: relative L2 error of the predictions over
+// all calls, the same for predicting zero transport (1 when the transports
+// are not all zero), calls.
+extern "C" int mom6b_surrogate_eval(mom6b_model* m, uint64_t seed, int k, int nsteps,
+                                    double* out3)
+{
+    if (!m || !out3 || nsteps < 1) return fail(MOM6B_ERR_ARG, "bad argument");
+    if (!m->sur) return fail(MOM6B_ERR_STATE, "no surrogate network");
+    CK(cudaSetDevice(m->cfg.device));
+    cudaStream_t s = m->s3d;
+    CK(cudaStreamSynchronize(s));
+    if (int rc = sur_buffers(m)) return rc;
+    if (int rc = sur_train_buffers(m)) return rc;
+    Mlp& N = *m->sur;
+    const SurGrid g = sur_grid(m);
+    const int nc = (m->D.ie - m->D.is + 1) * (m->D.je - m->D.js + 1);
+    CK(N.prepare_inference(nc));
+    CK(cudaMemsetAsync(m->sur_acc, 0, 2 * sizeof(double), s));
+    int calls = 0;
+    auto visit = [&](int phase, int, const double* e, const double* u, const double* v) -> int {
+        if (phase == 0) {
+            CK(launch_sur_features_all(g, BtInputs{e, u, v}, N.d_norm, N.Xi, s));
+            CK(N.predict(nc, s));
+            return MOM6B_OK;
+        }
+        CK(launch_sur_transport_err(g, N.outi, N.d_norm, m->bt.uhbt, m->bt.vhbt, m->sur_acc, s));
+        ++calls;
+        return MOM6B_OK;
+    };
+    if (int rc = sur_run_state(m, seed, k, nsteps, s, visit)) return rc;
+    double acc[2] = {0.0, 0.0};
+    CK(cudaMemcpyAsync(acc, m->sur_acc, sizeof(acc), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    int gerr = 0;
+    CK(cudaMemcpy(&gerr, N.err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (gerr) return fail(MOM6B_ERR_TIMEOUT, "tensor-core pipeline wait timed out");
+    if (int rc = check_status(m)) return rc;
+    out3[0] = acc[1] > 0.0 ? std::sqrt(acc[0] / acc[1]) : std::sqrt(acc[0]);
+    out3[1] = acc[1] > 0.0 ? 1.0 : 0.0;
+    out3[2] = (double)calls;
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_surrogate_enable(mom6b_model* m, int on, int shadow_every, double threshold)
+{
+    if (!m) return fail(MOM6B_ERR_ARG, "null model");
+    if (on && !m->sur) return fail(MOM6B_ERR_STATE, "no surrogate network: train or load one first");
+    CK(cudaSetDevice(m->cfg.device));
+    CK(cudaStreamSynchronize(m->s3d));
+    if (on) {
+        if (int rc = sur_buffers(m)) return rc;
+        const int nc = (m->D.ie - m->D.is + 1) * (m->D.je - m->D.js + 1);
+        CK(m->sur->prepare_inference(nc));   // allocations before any capture
+    }
+    m->sur_on = on != 0;
+    m->sur_fallen = false;
+    m->sur_every = shadow_every;
+    m->sur_thresh = threshold;
+    m->sur_steps = 0;
+    invalidate_graph(m);
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_surrogate_status(const mom6b_model* m, double* out10)
+{
+    if (!m || !out10) return fail(MOM6B_ERR_ARG, "null argument");
+    const double v[10] = {m->sur_on ? 1.0 : 0.0, m->sur_fallen ? 1.0 : 0.0,
+                          (double)m->sur_steps, (double)m->sur_checks,
+                          (double)m->sur_fallbacks, m->sur_last_err, m->sur_max_err,
+                          m->sur_loss_first, m->sur_loss_last, (double)m->sur_train_steps};
+    std::memcpy(out10, v, sizeof(v));
+    return MOM6B_OK;
+}
+
+// Parameters as kMlpParams floats followed by the 7 feature stds and the 2
+// target stds.
+extern "C" size_t mom6b_surrogate_param_count(void) { return (size_t)kMlpParams + 9; }
+
+extern "C" int mom6b_surrogate_get_params(const mom6b_model* m, float* host, size_t n)
+{
+    if (!m || !host || n != mom6b_surrogate_param_count()) return fail(MOM6B_ERR_ARG, "bad argument");
+    if (!m->sur) return fail(MOM6B_ERR_STATE, "no surrogate network");
+    CK(cudaSetDevice(m->cfg.device));
+    CK(m->sur->get_params(host));
+    for (int q = 0; q < kMlpChannels; ++q) host[kMlpParams + q] = m->sur->feat_std[q];
+    host[kMlpParams + 7] = m->sur->targ_std[0];
+    host[kMlpParams + 8] = m->sur->targ_std[1];
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_surrogate_set_params(mom6b_model* m, const float* host, size_t n)
+{
+    if (!m || !host || n != mom6b_surrogate_param_count()) return fail(MOM6B_ERR_ARG, "bad argument");
+    CK(cudaSetDevice(m->cfg.device));
+    if (!m->sur) {
+        auto N = std::make_unique<Mlp>();
+        CK(N->init(1024, 0, m->s3d));
+        m->sur = std::move(N);
+    }
+    Mlp& N = *m->sur;
+    for (int q = 0; q < kMlpChannels; ++q) N.feat_std[q] = host[kMlpParams + q];
+    N.targ_std[0] = host[kMlpParams + 7];
+    N.targ_std[1] = host[kMlpParams + 8];
+    float nrm[16] = {0};
+    for (int q = 0; q < kMlpChannels; ++q) nrm[q] = 1.0f / N.feat_std[q];
+    nrm[7] = N.targ_std[0];
+    nrm[8] = N.targ_std[1];
+    CK(cudaMemcpy(N.d_norm, nrm, sizeof(nrm), cudaMemcpyHostToDevice));
+    CK(N.set_params(host));
+    invalidate_graph(m);
+    return MOM6B_OK;
+}
+
+// ---- the network alone (tests against the CPU oracle) ------------------------
+struct mom6b_mlp {
+    Mlp net;
+};
+
+extern "C" int mom6b_mlp_param_count(void) { return kMlpParams; }
+
+extern "C" int mom6b_mlp_create(int batch, uint64_t seed, mom6b_mlp** out)
+{
+    if (!out || batch < 128 || batch % 8) return fail(MOM6B_ERR_ARG, "bad argument");
+    *out = nullptr;
+    auto p = std::make_unique<mom6b_mlp>();
+    CK(p->net.init(batch, seed, 0));
+    *out = p.release();
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_mlp_destroy(mom6b_mlp* p)
+{
+    delete p;
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_mlp_get_params(mom6b_mlp* p, float* host, size_t n)
+{
+    if (!p || !host || n != (size_t)kMlpParams) return fail(MOM6B_ERR_ARG, "bad argument");
+    CK(p->net.get_params(host));
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_mlp_set_params(mom6b_mlp* p, const float* host, size_t n)
+{
+    if (!p || !host || n != (size_t)kMlpParams) return fail(MOM6B_ERR_ARG, "bad argument");
+    CK(p->net.set_params(host));
+    return MOM6B_OK;
+}
+
+// bf16 features [rows][176] (and optionally [176][rows]) from fp32 [rows][175].
+static void mlp_pack(const float* X, int rows, std::vector<__nv_bfloat16>& row_major,
+                     std::vector<__nv_bfloat16>* col_major)
+{
+    row_major.assign((size_t)rows * kMlpInPad, __float2bfloat16_rn(0.0f));
+    if (col_major) col_major->assign((size_t)rows * kMlpInPad, __float2bfloat16_rn(0.0f));
+    for (int r = 0; r < rows; ++r)
+        for (int f = 0; f < kMlpIn; ++f) {
+            const __nv_bfloat16 v = __float2bfloat16_rn(X[(size_t)r * kMlpIn + f]);
+            row_major[(size_t)r * kMlpInPad + f] = v;
+            if (col_major) (*col_major)[(size_t)f * rows + r] = v;
+        }
+}
+
+static int mlp_upload(mom6b_mlp* p, const float* X, const float* Y, int B)
+{
+    if (B > p->net.B_cap || B < 128 || B % 8) return fail(MOM6B_ERR_ARG, "batch outside 128..capacity or not a multiple of 8");
+    std::vector<__nv_bfloat16> xr, xc;
+    mlp_pack(X, B, xr, &xc);
+    CK(cudaMemcpy(p->net.X, xr.data(), xr.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(p->net.XT, xc.data(), xc.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(p->net.Y, Y, (size_t)B * kMlpOut * sizeof(float), cudaMemcpyHostToDevice));
+    return MOM6B_OK;
+}
+
+static int mlp_check(mom6b_mlp* p)
+{
+    CK(cudaDeviceSynchronize());
+    int e = 0;
+    CK(cudaMemcpy(&e, p->net.err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) return fail(MOM6B_ERR_TIMEOUT, "tensor-core pipeline wait timed out");
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_mlp_gradients(mom6b_mlp* p, const float* X, const float* Y, int B,
+                                   float* grads, float* loss, float* out)
+{
+    if (!p || !X || !Y) return fail(MOM6B_ERR_ARG, "null argument");
+    if (int rc = mlp_upload(p, X, Y, B)) return rc;
+    CK(p->net.gradients(B, 0));
+    if (int rc = mlp_check(p)) return rc;
+    if (grads) CK(p->net.grads_to_host(grads, 0));
+    if (loss) CK(cudaMemcpy(loss, p->net.loss, sizeof(float), cudaMemcpyDeviceToHost));
+    if (out) CK(cudaMemcpy(out, p->net.out, (size_t)B * kMlpOut * sizeof(float), cudaMemcpyDeviceToHost));
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_mlp_train(mom6b_mlp* p, const float* X, const float* Y, int B, float lr,
+                               int nsteps, float* losses)
+{
+    if (!p || !X || !Y || nsteps < 0) return fail(MOM6B_ERR_ARG, "bad argument");
+    if (int rc = mlp_upload(p, X, Y, B)) return rc;
+    for (int t = 0; t < nsteps; ++t) {
+        CK(p->net.train_step(B, lr, 0));
+        if (losses) CK(cudaMemcpy(losses + t, p->net.loss, sizeof(float), cudaMemcpyDeviceToHost));
+    }
+    return mlp_check(p);
+}
+
+extern "C" int mom6b_mlp_predict(mom6b_mlp* p, const float* X, int n, float* out)
+{
+    if (!p || !X || !out || n < 1) return fail(MOM6B_ERR_ARG, "bad argument");
+    CK(p->net.prepare_inference(n));
+    std::vector<__nv_bfloat16> xr;
+    mlp_pack(X, n, xr, nullptr);
+    CK(cudaMemcpy(p->net.Xi, xr.data(), xr.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice));
+    CK(p->net.predict(n, 0));
+    if (int rc = mlp_check(p)) return rc;
+    CK(cudaMemcpy(out, p->net.outi, (size_t)n * kMlpOut * sizeof(float), cudaMemcpyDeviceToHost));
     return MOM6B_OK;
 }

@@ -223,6 +223,66 @@ int mom6b_ensemble_autotune(mom6b_ensemble *e, int reps, double *out_ms);
 int mom6b_ensemble_get_tuning(const mom6b_ensemble *e, int *out7);
 int mom6b_ensemble_set_tuning(mom6b_ensemble *e, const int *in7);
 
+/* ---- learned barotropic surrogate -----------------------------------------
+ * No counterpart in the reference.  A 175-256-256-2 MLP (GELU, bf16 weights and
+ * activations on the tensor cores, fp32 accumulation) maps the 5 x 5 stencil
+ * of 7 channels (eta, ubt, vbt, barotropic forcing u and v (zero: btstep has
+ * no forcing), depth, f) of a cell, each divided by its channel std, to the
+ * substep-averaged transports of its east and north faces; eta is then
+ * advanced in FP64 from their divergence (volume conserved to rounding), and
+ * the averaged velocities are transport / Datu, / Datv.
+ *
+ * mom6b_surrogate_train trains the model's network on the GPU: nstates
+ * seeded barotropic initial states (Gaussian eta bumps of seeded amplitude,
+ * centre and radius, ubt = vbt = 0), nsteps RK2 steps of the plain btstep
+ * each; every barotropic call gives one batch of `batch` sampled columns and
+ * one Adam step (lr).  The channel and target stds come from the first 10
+ * steps of the first state.  stats4 (optional): mean loss of the first 10 and
+ * of the last 100 batches, batches, seconds.
+ *
+ * mom6b_surrogate_enable(on = 1) makes mom6b_step use the network instead of
+ * btstep; every shadow_every steps (0: never) the plain btstep runs from the
+ * same state and judges: when the relative L2 difference of the two etas over
+ * the compute domain exceeds threshold, the plain results are kept and the
+ * model uses the plain btstep from then on (mom6b_surrogate_enable again
+ * re-arms it).  status10: enabled, fallen back, steps, shadow checks,
+ * fallbacks, last and largest shadow error, first and last training loss,
+ * training batches.  The parameters (mom6b_surrogate_param_count floats: the
+ * network's, then the 7 feature stds and the 2 target stds) move a trained
+ * network between models. */
+int mom6b_surrogate_train(mom6b_model *m, int nstates, int nsteps, int batch,
+                          double lr, uint64_t seed, double *stats4);
+/* Transport error on state k of the seeded family (pick a k the training did
+ * not use): out3 = relative L2 error of the network's averaged transports
+ * against the plain btstep's over nsteps RK2 barotropic chains, the same for
+ * the zero-transport prediction, calls. */
+int mom6b_surrogate_eval(mom6b_model *m, uint64_t seed, int k, int nsteps, double *out3);
+int mom6b_surrogate_enable(mom6b_model *m, int on, int shadow_every, double threshold);
+int mom6b_surrogate_status(const mom6b_model *m, double *status10);
+size_t mom6b_surrogate_param_count(void);
+int mom6b_surrogate_get_params(const mom6b_model *m, float *host, size_t n);
+int mom6b_surrogate_set_params(mom6b_model *m, const float *host, size_t n);
+
+/* The network alone, for checks against a CPU restatement: batches of B rows
+ * (128 <= B <= the batch it was created with, B a multiple of 8) of 175 fp32
+ * features (rounded to bf16 on upload) and 2 fp32 targets.
+ * mom6b_mlp_gradients: forward, loss = sum (out - y)^2 / (2 B), backward; the
+ * gradient of every parameter (mom6b_mlp_param_count floats, layout W1
+ * [256][176] (column 175 is padding), b1, W2 [256][256], b2, W3 [2][256], b3).
+ * mom6b_mlp_train: nsteps Adam steps (0.9, 0.999, 1e-8) on one batch.
+ * mom6b_mlp_predict: outputs of n rows. */
+typedef struct mom6b_mlp mom6b_mlp;
+int mom6b_mlp_param_count(void);
+int mom6b_mlp_create(int batch, uint64_t seed, mom6b_mlp **out);
+int mom6b_mlp_destroy(mom6b_mlp *p);
+int mom6b_mlp_get_params(mom6b_mlp *p, float *host, size_t n);
+int mom6b_mlp_set_params(mom6b_mlp *p, const float *host, size_t n);
+int mom6b_mlp_gradients(mom6b_mlp *p, const float *X, const float *Y, int B,
+                        float *grads, float *loss, float *out);
+int mom6b_mlp_train(mom6b_mlp *p, const float *X, const float *Y, int B, float lr,
+                    int nsteps, float *losses);
+int mom6b_mlp_predict(mom6b_mlp *p, const float *X, int n, float *out);
+
 const char *mom6b_last_error(void);
 const char *mom6b_version(void);
 
