@@ -24,6 +24,13 @@ The "ensemble" object advances 64 independent domains of uneven size
 together, one launch per phase for all of them with launch shapes from the
 autotuner, and reports aggregate cell-layer updates/s over 50 steps.
 
+The "surrogate" object trains the learned barotropic surrogate on the GPU
+(8 seeded states x 2000 steps of the plain btstep, batch 65536), reports its
+transport error on a held-out state, and times the step with the network in
+place of btstep: with the plain btstep as shadow judge every 10 steps
+(threshold 1e-3 relative eta error, falling back when exceeded) and alone,
+with the network-alone eta error after 100 steps against the FP64 form.
+
 --impl reference times the reference's CPU implementation of the path on the
 host cores: the C restatement of the serial Fortran driver (the Fortran
 itself cannot be compiled here), on rank 0 only.
@@ -333,6 +340,80 @@ def run_ensemble(args, world, rank, local, dist):
     return out
 
 
+def _timed_steps(m, steps, local):
+    import torch
+    stream = torch.cuda.ExternalStream(m.stream(), device=f"cuda:{local}")
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    m.step(steps)
+    e1.record(stream)
+    m.synchronize()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def run_surrogate(args, world, rank, local, dist, fp64_ms_per_step):
+    """The learned barotropic surrogate at 720x720x75 bt50: the network is
+    trained on the GPU (8 seeded barotropic states x args.sur_steps RK2 steps
+    of the plain btstep, batch 65536, Adam lr 1e-3), checked on a held-out
+    state, then run in place of btstep with the plain btstep as shadow judge
+    (every 10 steps, relative eta error threshold 1e-3), and on its own."""
+    from hackathon_mom6_miniapp_b200 import FP64, INIT_CFG, Model
+    t = Model(NI, NJ, 2, BT, INIT_CFG, seed=rank, dt=600.0, device=local)
+    train = t.surrogate_train(nstates=8, nsteps=args.sur_steps, batch=65536, lr=1e-3, seed=1)
+    held = t.surrogate_eval(seed=1, state=100, nsteps=10)
+    params = t.surrogate_params()
+    t.close()
+    out = {"training": dict(train, states=8, steps_per_state=args.sur_steps, batch=65536,
+                            lr=1e-3),
+           "heldout_transport_rel_l2": held["rel_error"],
+           "heldout_zero_transport_rel_l2": held["zero_prediction_error"]}
+    # with the shadow judge
+    m = Model(NI, NJ, NK, BT, INIT_CFG, seed=rank, dt=600.0, device=local, use_graph=True)
+    m.set_surrogate_params(params)
+    m.surrogate_enable(True, shadow_every=10, threshold=1e-3)
+    m.step(args.warmup)
+    m.synchronize()
+    barrier(dist)
+    ms = max_over_ranks(_timed_steps(m, args.steps, local), dist, local)
+    st = m.surrogate_status()
+    m.close()
+    out.update({"value": world * args.steps / (ms / 1000.0), "unit": "steps/s",
+                "ms_per_step": ms / args.steps,
+                "speedup_vs_fp64": fp64_ms_per_step / (ms / args.steps),
+                "shadow_every": 10, "threshold": 1e-3,
+                "fallen_back": bool(st["fallen_back"]),
+                "shadow_checks": st["shadow_checks"],
+                "max_shadow_rel_error": st["max_shadow_error"]})
+    # the network alone: speed, and eta after 100 steps against the plain form
+    m = Model(NI, NJ, NK, BT, INIT_CFG, seed=rank, dt=600.0, device=local, use_graph=True)
+    m.set_surrogate_params(params)
+    m.surrogate_enable(True, shadow_every=0)
+    m.step(args.warmup)
+    m.synchronize()
+    barrier(dist)
+    ms_n = max_over_ranks(_timed_steps(m, args.steps, local), dist, local)
+    m.close()
+    pure = {"value": world * args.steps / (ms_n / 1000.0), "unit": "steps/s",
+            "ms_per_step": ms_n / args.steps,
+            "speedup_vs_fp64": fp64_ms_per_step / (ms_n / args.steps)}
+    if rank == 0:
+        a = Model(NI, NJ, NK, BT, INIT_CFG, seed=0, dt=600.0, device=local, use_graph=True,
+                  precision=FP64)
+        a.step(100)
+        want = a.get("eta")
+        a.close()
+        b = Model(NI, NJ, NK, BT, INIT_CFG, seed=0, dt=600.0, device=local, use_graph=True)
+        b.set_surrogate_params(params)
+        b.surrogate_enable(True, shadow_every=0)
+        b.step(100)
+        pure["eta_rel_l2_100_steps"] = _rel_l2(b.get("eta"), want)
+        b.close()
+    out["network_alone"] = pure
+    return out
+
+
 def run_ours(args, world, rank, local, dist):
     import numpy as np
     import torch
@@ -419,6 +500,8 @@ def run_ours(args, world, rank, local, dist):
     mixed = None if args.no_mixed else run_mixed(args, world, rank, local, dist,
                                                    ms / args.steps)
     ensemble = None if args.no_ensemble else run_ensemble(args, world, rank, local, dist)
+    surrogate = None if args.no_surrogate else run_surrogate(args, world, rank, local, dist,
+                                                             ms / args.steps)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -457,6 +540,7 @@ def run_ours(args, world, rank, local, dist):
                                  "d2h_bytes_per_step": bytes_d2h / args.steps},
                 "mixed": mixed,
                 "ensemble": ensemble,
+                "surrogate": surrogate,
                 "gpu_launches": launches,
                 "clocks": ck}
         print(json.dumps(line), flush=True)
@@ -485,6 +569,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mixed", action="store_true",
                     help="skip the mixed-precision form's line items")
+    ap.add_argument("--no-surrogate", action="store_true",
+                    help="skip the learned-surrogate line item")
+    ap.add_argument("--sur-steps", type=int, default=2000,
+                    help="RK2 steps per training state of the surrogate (8 states)")
     ap.add_argument("--no-ensemble", action="store_true",
                     help="skip the 64-domain ensemble line item")
     ap.add_argument("--no-cfg2", action="store_true",

@@ -307,8 +307,8 @@ static cudaError_t dev_alloc(T** p, size_t n)
 
 Mlp::~Mlp()
 {
-    void* ptrs[] = {X, XT, Y, out, loss, err, Xi, outi, d_norm, P, G, Mo, Vo, W1b, W2b, W2Tb,
-                    W3r, Z1, Z2, H1, H1T, H2, dZ2, dZ2T, dZ1T, part, bpart, H1i};
+    void* ptrs[] = {X, XT, Y, amp, gacc, out, loss, err, Xi, outi, ampi, d_norm, P, G, Mo, Vo, W1b,
+                    W2b, W2Tb, W3r, Z1, Z2, H1, H1T, H2, dZ2, dZ2T, dZ1T, part, bpart, H1i};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }
@@ -338,6 +338,8 @@ cudaError_t Mlp::init(int batch, uint64_t seed, cudaStream_t s)
     MLP_CK(dev_alloc(&X, B * kMlpInPad));
     MLP_CK(dev_alloc(&XT, B * kMlpInPad));
     MLP_CK(dev_alloc(&Y, B * kMlpOut));
+    MLP_CK(dev_alloc(&amp, B));
+    MLP_CK(dev_alloc(&gacc, 4));
     MLP_CK(dev_alloc(&out, B * kMlpOut));
     MLP_CK(dev_alloc(&loss, 4));
     MLP_CK(dev_alloc(&err, 4));
@@ -510,10 +512,12 @@ cudaError_t Mlp::prepare_inference(int n)
     if (Xi) cudaFree(Xi);
     if (outi) cudaFree(outi);
     if (H1i) cudaFree(H1i);
-    Xi = nullptr; outi = nullptr; H1i = nullptr;
+    if (ampi) cudaFree(ampi);
+    Xi = nullptr; outi = nullptr; H1i = nullptr; ampi = nullptr;
     const int cap = ((n + kGemmBM - 1) / kGemmBM) * kGemmBM;
     MLP_CK(dev_alloc(&Xi, (size_t)cap * kMlpInPad));
     MLP_CK(dev_alloc(&outi, (size_t)cap * kMlpOut));
+    MLP_CK(dev_alloc(&ampi, (size_t)cap));
     MLP_CK(dev_alloc(&H1i, (size_t)cap * kMlpHidden));
     MLP_CK(map_bf16(&mXi, Xi, cap, kMlpInPad, kGemmBM));
     MLP_CK(map_bf16(&mH1i, H1i, cap, kMlpHidden, kGemmBM));
@@ -556,9 +560,68 @@ __device__ __forceinline__ void sur_sample(const Dims& D, uint64_t seed, int s, 
     j = D.js + idx / nx;
 }
 
-// Feature f (channel f / 25, stencil offset f % 25 = (dj + 2) * 5 + (di + 2)) of cell (i, j).
+// Amplitude of the dynamic channels (eta, ubt, vbt, each divided by its
+// channel std) over the 5 x 5 stencil of cell (i, j): their RMS.  The
+// barotropic equations are linear in (eta, ubt, vbt), so the averaged
+// transports are homogeneous of degree one in them; the network sees the
+// stencil divided by this amplitude and its outputs are scaled back by it.
+// gacc holds the sum of squares and the count of the same quantities over the
+// whole compute domain (k_sur_amp_reduce); a tenth of their RMS floors the
+// amplitude, so that a cell whose stencil is quiet while transports arrive
+// from beyond it is not divided by (nearly) zero.
+__device__ __forceinline__ float sur_amp(const SurGrid& g, const BtInputs& in,
+                                         const float* norm, const double* gacc, int i, int j)
+{
+    double acc = 0.0;
+    for (int r = 0; r < 25; ++r) {
+        const int ii = i + r % 5 - 2, jj = j + r / 5 - 2;
+        const size_t p = (size_t)(jj - 1) * g.D.n1 + (ii - 1);
+        const double e = in.eta[p] * norm[0], u = in.ubt[p] * norm[1], v = in.vbt[p] * norm[2];
+        acc += e * e + u * u + v * v;
+    }
+    const double glob = gacc[1] > 0.0 ? gacc[0] / gacc[1] : 0.0;
+    return (float)(sqrt(acc / 75.0 + 0.01 * glob) + 1e-30);
+}
+
+__global__ void __launch_bounds__(256)
+k_sur_amp_reduce(SurGrid g, BtInputs in, const float* __restrict__ norm, double* gacc)
+{
+    __shared__ double r0[256];
+    const Dims& D = g.D;
+    const int nx = D.ie - D.is + 1, ny = D.je - D.js + 1;
+    double s0 = 0.0;
+    for (int q = (int)(blockIdx.x * blockDim.x + threadIdx.x); q < nx * ny;
+         q += (int)(gridDim.x * blockDim.x)) {
+        const int i = D.is + q % nx, j = D.js + q / nx;
+        const size_t p = (size_t)(j - 1) * D.n1 + (i - 1);
+        const double e = in.eta[p] * norm[0], u = in.ubt[p] * norm[1], v = in.vbt[p] * norm[2];
+        s0 += (e * e + u * u + v * v) / 3.0;
+    }
+    r0[threadIdx.x] = s0;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) r0[threadIdx.x] += r0[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        atomicAdd(gacc, r0[0]);
+        if (blockIdx.x == 0) atomicAdd(gacc + 1, (double)nx * ny);
+    }
+}
+
+static cudaError_t sur_amp_reduce(const SurGrid& g, const BtInputs& in, const float* norm,
+                                  double* gacc, cudaStream_t s)
+{
+    cudaError_t e = cudaMemsetAsync(gacc, 0, 2 * sizeof(double), s);
+    if (e != cudaSuccess) return e;
+    k_sur_amp_reduce<<<148, 256, 0, s>>>(g, in, norm, gacc);
+    return cudaGetLastError();
+}
+
+// Feature f (channel f / 25, stencil offset f % 25 = (dj + 2) * 5 + (di + 2)) of
+// cell (i, j); the dynamic channels are divided by the stencil amplitude amp.
 __device__ __forceinline__ float sur_feature(const SurGrid& g, const BtInputs& in,
-                                             const float* norm, int i, int j, int f)
+                                             const float* norm, float amp, int i, int j, int f)
 {
     if (f >= kMlpIn) return 0.0f;
     const int c = f / 25, r = f - c * 25;
@@ -573,86 +636,117 @@ __device__ __forceinline__ float sur_feature(const SurGrid& g, const BtInputs& i
     case 6: v = g.cor[p]; break;
     default: v = 0.0; break;   // barotropic forcing: none in the barotropic solver
     }
-    return (float)v * norm[c];
+    const double x = v * (double)norm[c];
+    return (float)(c <= 2 ? x / (double)amp : x);
+}
+
+// amplitude of every sample (one thread per sample)
+__global__ void k_sur_amp_train(SurGrid g, BtInputs in, const float* __restrict__ norm,
+                                const double* __restrict__ gacc, int B, uint64_t seed, float* amp)
+{
+    const int s = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    if (s >= B) return;
+    int i, j;
+    sur_sample(g.D, seed, s, i, j);
+    amp[s] = sur_amp(g, in, norm, gacc, i, j);
 }
 
 __global__ void k_sur_features_train(SurGrid g, BtInputs in, const float* __restrict__ norm,
-                                     int B, uint64_t seed, __nv_bfloat16* X)
+                                     const float* __restrict__ amp, int B, uint64_t seed,
+                                     __nv_bfloat16* X)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)B * kMlpInPad) return;
     const int s = (int)(t / kMlpInPad), f = (int)(t - (long long)s * kMlpInPad);
     int i, j;
     sur_sample(g.D, seed, s, i, j);
-    X[t] = __float2bfloat16_rn(sur_feature(g, in, norm, i, j, f));
+    X[t] = __float2bfloat16_rn(sur_feature(g, in, norm, amp[s], i, j, f));
 }
 
 __global__ void k_sur_features_train_t(SurGrid g, BtInputs in, const float* __restrict__ norm,
-                                       int B, uint64_t seed, __nv_bfloat16* XT)
+                                       const float* __restrict__ amp, int B, uint64_t seed,
+                                       __nv_bfloat16* XT)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)B * kMlpInPad) return;
     const int f = (int)(t / B), s = (int)(t - (long long)f * B);
     int i, j;
     sur_sample(g.D, seed, s, i, j);
-    XT[t] = __float2bfloat16_rn(sur_feature(g, in, norm, i, j, f));
+    XT[t] = __float2bfloat16_rn(sur_feature(g, in, norm, amp[s], i, j, f));
 }
 
 cudaError_t launch_sur_features_train(const SurGrid& g, const BtInputs& in, const float* norm,
-                                      int B, uint64_t seed, __nv_bfloat16* X,
-                                      __nv_bfloat16* XT, cudaStream_t s)
+                                      double* gacc, int B, uint64_t seed, __nv_bfloat16* X,
+                                      __nv_bfloat16* XT, float* amp, cudaStream_t s)
 {
     const long long n = (long long)B * kMlpInPad;
     const int nb = 256;
     const unsigned blocks = (unsigned)((n + nb - 1) / nb);
-    k_sur_features_train<<<blocks, nb, 0, s>>>(g, in, norm, B, seed, X);
-    k_sur_features_train_t<<<blocks, nb, 0, s>>>(g, in, norm, B, seed, XT);
+    cudaError_t e = sur_amp_reduce(g, in, norm, gacc, s);
+    if (e != cudaSuccess) return e;
+    k_sur_amp_train<<<(B + nb - 1) / nb, nb, 0, s>>>(g, in, norm, gacc, B, seed, amp);
+    k_sur_features_train<<<blocks, nb, 0, s>>>(g, in, norm, amp, B, seed, X);
+    k_sur_features_train_t<<<blocks, nb, 0, s>>>(g, in, norm, amp, B, seed, XT);
     return cudaGetLastError();
 }
 
 __global__ void k_sur_targets(SurGrid g, const double* __restrict__ uh_avg,
                               const double* __restrict__ vh_avg, const float* __restrict__ norm,
-                              int B, uint64_t seed, float* Y)
+                              const float* __restrict__ amp, int B, uint64_t seed, float* Y)
 {
     const int s = (int)(blockIdx.x * blockDim.x + threadIdx.x);
     if (s >= B) return;
     int i, j;
     sur_sample(g.D, seed, s, i, j);
     const size_t p = (size_t)(j - 1) * g.D.n1 + (i - 1);
-    Y[(size_t)s * 2] = (float)(uh_avg[p] / (double)norm[7]);
-    Y[(size_t)s * 2 + 1] = (float)(vh_avg[p] / (double)norm[8]);
+    const double a = (double)amp[s];
+    Y[(size_t)s * 2] = (float)(uh_avg[p] / ((double)norm[7] * a));
+    Y[(size_t)s * 2 + 1] = (float)(vh_avg[p] / ((double)norm[8] * a));
 }
 
 cudaError_t launch_sur_targets(const SurGrid& g, const double* uh_avg, const double* vh_avg,
-                               const float* norm, int B, uint64_t seed, float* Y,
-                               cudaStream_t s)
+                               const float* norm, const float* amp, int B, uint64_t seed,
+                               float* Y, cudaStream_t s)
 {
-    k_sur_targets<<<(B + 255) / 256, 256, 0, s>>>(g, uh_avg, vh_avg, norm, B, seed, Y);
+    k_sur_targets<<<(B + 255) / 256, 256, 0, s>>>(g, uh_avg, vh_avg, norm, amp, B, seed, Y);
     return cudaGetLastError();
 }
 
+__global__ void k_sur_amp_all(SurGrid g, BtInputs in, const float* __restrict__ norm,
+                              const double* __restrict__ gacc, float* amp)
+{
+    const int nx = g.D.ie - g.D.is + 1, ny = g.D.je - g.D.js + 1;
+    const int s = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    if (s >= nx * ny) return;
+    amp[s] = sur_amp(g, in, norm, gacc, g.D.is + s % nx, g.D.js + s / nx);
+}
+
 __global__ void k_sur_features_all(SurGrid g, BtInputs in, const float* __restrict__ norm,
-                                   __nv_bfloat16* X)
+                                   const float* __restrict__ amp, __nv_bfloat16* X)
 {
     const int nx = g.D.ie - g.D.is + 1, ny = g.D.je - g.D.js + 1;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)nx * ny * kMlpInPad) return;
     const int s = (int)(t / kMlpInPad), f = (int)(t - (long long)s * kMlpInPad);
     const int i = g.D.is + s % nx, j = g.D.js + s / nx;
-    X[t] = __float2bfloat16_rn(sur_feature(g, in, norm, i, j, f));
+    X[t] = __float2bfloat16_rn(sur_feature(g, in, norm, amp[s], i, j, f));
 }
 
 cudaError_t launch_sur_features_all(const SurGrid& g, const BtInputs& in, const float* norm,
-                                    __nv_bfloat16* X, cudaStream_t s)
+                                    double* gacc, __nv_bfloat16* X, float* amp, cudaStream_t s)
 {
     const long long n = (long long)(g.D.ie - g.D.is + 1) * (g.D.je - g.D.js + 1) * kMlpInPad;
-    k_sur_features_all<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(g, in, norm, X);
+    cudaError_t e = sur_amp_reduce(g, in, norm, gacc, s);
+    if (e != cudaSuccess) return e;
+    const int nc = (g.D.ie - g.D.is + 1) * (g.D.je - g.D.js + 1);
+    k_sur_amp_all<<<(nc + 255) / 256, 256, 0, s>>>(g, in, norm, gacc, amp);
+    k_sur_features_all<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(g, in, norm, amp, X);
     return cudaGetLastError();
 }
 
 __global__ void k_sur_advance(SurGrid g, const float* __restrict__ outi,
-                              const float* __restrict__ norm, const double* eta_in,
-                              double* eta_out, double* u_av, double* v_av)
+                              const float* __restrict__ norm, const float* __restrict__ amp,
+                              const double* eta_in, double* eta_out, double* u_av, double* v_av)
 {
     const Dims& D = g.D;
     const int p = (int)(blockIdx.x * blockDim.x + threadIdx.x);
@@ -663,11 +757,13 @@ __global__ void k_sur_advance(SurGrid g, const float* __restrict__ outi,
     // predicted substep-averaged transports on their ranges, zero elsewhere
     auto U = [&](int a, int b) -> double {
         if (a < g.iu0 || a > g.iu1 || b < D.js || b > D.je || a < D.is) return 0.0;
-        return (double)outi[(size_t)((b - D.js) * nx + (a - D.is)) * 2] * su;
+        const size_t q = (size_t)((b - D.js) * nx + (a - D.is));
+        return (double)outi[q * 2] * su * (double)amp[q];
     };
     auto V = [&](int a, int b) -> double {
         if (b < g.jv0 || b > g.jv1 || a < D.is || a > D.ie || b < D.js) return 0.0;
-        return (double)outi[(size_t)((b - D.js) * nx + (a - D.is)) * 2 + 1] * sv;
+        const size_t q = (size_t)((b - D.js) * nx + (a - D.is));
+        return (double)outi[q * 2 + 1] * sv * (double)amp[q];
     };
     double e = eta_in[p];
     if (i >= D.is && i <= D.ie && j >= D.js && j <= D.je)
@@ -679,11 +775,12 @@ __global__ void k_sur_advance(SurGrid g, const float* __restrict__ outi,
 }
 
 cudaError_t launch_sur_advance(const SurGrid& g, const float* outi, const float* norm,
-                               const double* eta_in, double* eta_out, double* u_av,
-                               double* v_av, cudaStream_t s)
+                               const float* amp, const double* eta_in, double* eta_out,
+                               double* u_av, double* v_av, cudaStream_t s)
 {
     const int n = g.D.n1 * g.D.n2;
-    k_sur_advance<<<(n + 255) / 256, 256, 0, s>>>(g, outi, norm, eta_in, eta_out, u_av, v_av);
+    k_sur_advance<<<(n + 255) / 256, 256, 0, s>>>(g, outi, norm, amp, eta_in, eta_out, u_av,
+                                                  v_av);
     return cudaGetLastError();
 }
 
@@ -719,7 +816,8 @@ k_sur_diff(Dims D, const double* __restrict__ a, const double* __restrict__ b, d
 
 __global__ void __launch_bounds__(256)
 k_sur_transport_err(SurGrid g, const float* __restrict__ outi, const float* __restrict__ norm,
-                    const double* __restrict__ uh, const double* __restrict__ vh, double* acc)
+                    const float* __restrict__ amp, const double* __restrict__ uh,
+                    const double* __restrict__ vh, double* acc)
 {
     __shared__ double r0[256], r1[256];
     const Dims& D = g.D;
@@ -730,8 +828,9 @@ k_sur_transport_err(SurGrid g, const float* __restrict__ outi, const float* __re
         const int i = D.is + q % nx, j = D.js + q / nx;
         const size_t p = (size_t)(j - 1) * D.n1 + (i - 1);
         const bool inu = i >= g.iu0 && i <= g.iu1, inv = j >= g.jv0 && j <= g.jv1;
-        const double pu = inu ? (double)outi[(size_t)q * 2] * (double)norm[7] : 0.0;
-        const double pv = inv ? (double)outi[(size_t)q * 2 + 1] * (double)norm[8] : 0.0;
+        const double a = (double)amp[q];
+        const double pu = inu ? (double)outi[(size_t)q * 2] * (double)norm[7] * a : 0.0;
+        const double pv = inv ? (double)outi[(size_t)q * 2 + 1] * (double)norm[8] * a : 0.0;
         s0 += (pu - uh[p]) * (pu - uh[p]) + (pv - vh[p]) * (pv - vh[p]);
         s1 += uh[p] * uh[p] + vh[p] * vh[p];
     }
@@ -752,10 +851,10 @@ k_sur_transport_err(SurGrid g, const float* __restrict__ outi, const float* __re
 }
 
 cudaError_t launch_sur_transport_err(const SurGrid& g, const float* outi, const float* norm,
-                                     const double* uh_avg, const double* vh_avg, double* acc,
-                                     cudaStream_t s)
+                                     const float* amp, const double* uh_avg,
+                                     const double* vh_avg, double* acc, cudaStream_t s)
 {
-    k_sur_transport_err<<<148, 256, 0, s>>>(g, outi, norm, uh_avg, vh_avg, acc);
+    k_sur_transport_err<<<148, 256, 0, s>>>(g, outi, norm, amp, uh_avg, vh_avg, acc);
     return cudaGetLastError();
 }
 

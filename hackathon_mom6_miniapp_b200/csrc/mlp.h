@@ -43,30 +43,33 @@ struct SurGrid {
 };
 
 // Features of B sampled columns (cells of the compute domain picked by a
-// hash of (seed, sample)) into X [B][176] and XT [176][B]; norm holds the 7
-// inverse channel stds.
+// hash of (seed, sample)) into X [B][176] and XT [176][B], and each sample's
+// stencil amplitude into amp [B]; norm holds the 7 inverse channel stds.  The
+// dynamic channels (eta, ubt, vbt) are divided by the amplitude, floored by a
+// tenth of their RMS over the domain (reduced into gacc, 2 doubles).
 cudaError_t launch_sur_features_train(const SurGrid& g, const BtInputs& in, const float* norm,
-                                      int B, uint64_t seed, __nv_bfloat16* X,
-                                      __nv_bfloat16* XT, cudaStream_t s);
+                                      double* gacc, int B, uint64_t seed, __nv_bfloat16* X,
+                                      __nv_bfloat16* XT, float* amp, cudaStream_t s);
 // Targets of the same samples: the substep-averaged transports divided by
-// their stds (norm[7], norm[8]).
+// their stds (norm[7], norm[8]) and by the sample's amplitude.
 cudaError_t launch_sur_targets(const SurGrid& g, const double* uh_avg, const double* vh_avg,
-                               const float* norm, int B, uint64_t seed, float* Y,
-                               cudaStream_t s);
-// Features of every compute cell, row (j - js) * nx + (i - is).
+                               const float* norm, const float* amp, int B, uint64_t seed,
+                               float* Y, cudaStream_t s);
+// Features (and amplitudes) of every compute cell, row (j - js) * nx + (i - is).
 cudaError_t launch_sur_features_all(const SurGrid& g, const BtInputs& in, const float* norm,
-                                    __nv_bfloat16* X, cudaStream_t s);
+                                    double* gacc, __nv_bfloat16* X, float* amp, cudaStream_t s);
 // eta_out = eta_in - dt_total IareaT div(U, V) in FP64 from the predicted
-// transports, and the averaged velocities U / Datu, V / Datv.
+// transports (outputs times target std times amplitude), and the averaged
+// velocities U / Datu, V / Datv.
 cudaError_t launch_sur_advance(const SurGrid& g, const float* outi, const float* norm,
-                               const double* eta_in, double* eta_out, double* u_av,
-                               double* v_av, cudaStream_t s);
+                               const float* amp, const double* eta_in, double* eta_out,
+                               double* u_av, double* v_av, cudaStream_t s);
 // Error of the predicted transports (outi, all compute cells) against the
 // substep-averaged transports of the plain btstep: adds sum (pred - true)^2
 // and sum true^2 over both components and the compute domain to acc[0], acc[1].
 cudaError_t launch_sur_transport_err(const SurGrid& g, const float* outi, const float* norm,
-                                     const double* uh_avg, const double* vh_avg, double* acc,
-                                     cudaStream_t s);
+                                     const float* amp, const double* uh_avg,
+                                     const double* vh_avg, double* acc, cudaStream_t s);
 // Relative L2 difference of two 2-D fields over the compute domain: writes
 // sum (a - b)^2 and sum b^2 to acc[0], acc[1] (acc zeroed first).
 cudaError_t launch_sur_diff(const Dims& D, const double* a, const double* b, double* acc,
@@ -98,12 +101,15 @@ public:
     // batch buffers (training)
     __nv_bfloat16 *X = nullptr, *XT = nullptr;  // [B][176], [176][B]
     float* Y = nullptr;                          // targets [B][2]
+    float* amp = nullptr;                        // stencil amplitudes of the batch [B]
+    double* gacc = nullptr;                      // domain sums of the amplitude floor [2]
     float* out = nullptr;                        // outputs [B][2]
     float* loss = nullptr;                       // [1]: loss of the last train step
     int* err = nullptr;                          // tensor-core wait failures
     // inference buffers
     __nv_bfloat16* Xi = nullptr;                 // [n][176]
     float* outi = nullptr;                       // [n][2]
+    float* ampi = nullptr;                       // stencil amplitudes [n]
     int ni_cap = 0;
     int B_cap = 0;
     int64_t steps = 0;                           // Adam steps taken

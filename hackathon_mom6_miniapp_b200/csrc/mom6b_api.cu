@@ -531,11 +531,11 @@ static int surrogate_call(mom6b_model* m, const double* eta, const double* ubt,
     Mlp& N = *m->sur;
     CK(N.prepare_inference(nc));
     CK(timed(m, s, "surrogate", [&] {
-        return launch_sur_features_all(g, BtInputs{eta, ubt, vbt}, N.d_norm, N.Xi, s); }));
+        return launch_sur_features_all(g, BtInputs{eta, ubt, vbt}, N.d_norm, N.gacc, N.Xi, N.ampi, s); }));
     CK(timed(m, s, "surrogate", [&] { return N.predict(nc, s); }));
     m->launches += 1;   // predict is two launches
     CK(timed(m, s, "surrogate", [&] {
-        return launch_sur_advance(g, N.outi, N.d_norm, eta, eta_out, u_av, v_av, s); }));
+        return launch_sur_advance(g, N.outi, N.d_norm, N.ampi, eta, eta_out, u_av, v_av, s); }));
     return MOM6B_OK;
 }
 
@@ -1821,11 +1821,11 @@ extern "C" int mom6b_surrogate_train(mom6b_model* m, int nstates, int nsteps, in
                            const double* v) -> int {
         if (phase == 0) {   // features of the inputs, before the call overwrites them
             cseed = sur_hash(seed ^ (0x5DEECE66DULL * (uint64_t)(q + 1)));
-            CK(launch_sur_features_train(g, BtInputs{e, u, v}, N.d_norm, batch, cseed, N.X, N.XT,
-                                         s));
+            CK(launch_sur_features_train(g, BtInputs{e, u, v}, N.d_norm, N.gacc, batch, cseed, N.X,
+                                         N.XT, N.amp, s));
             return MOM6B_OK;
         }
-        CK(launch_sur_targets(g, m->bt.uhbt, m->bt.vhbt, N.d_norm, batch, cseed, N.Y, s));
+        CK(launch_sur_targets(g, m->bt.uhbt, m->bt.vhbt, N.d_norm, N.amp, batch, cseed, N.Y, s));
         CK(N.train_step(batch, (float)lr, s));
         CK(cudaMemcpyAsync(dloss + q, N.loss, sizeof(float), cudaMemcpyDeviceToDevice, s));
         ++q;
@@ -1884,11 +1884,12 @@ extern "C" int mom6b_surrogate_eval(mom6b_model* m, uint64_t seed, int k, int ns
     int calls = 0;
     auto visit = [&](int phase, int, const double* e, const double* u, const double* v) -> int {
         if (phase == 0) {
-            CK(launch_sur_features_all(g, BtInputs{e, u, v}, N.d_norm, N.Xi, s));
+            CK(launch_sur_features_all(g, BtInputs{e, u, v}, N.d_norm, N.gacc, N.Xi, N.ampi, s));
             CK(N.predict(nc, s));
             return MOM6B_OK;
         }
-        CK(launch_sur_transport_err(g, N.outi, N.d_norm, m->bt.uhbt, m->bt.vhbt, m->sur_acc, s));
+        CK(launch_sur_transport_err(g, N.outi, N.d_norm, N.ampi, m->bt.uhbt, m->bt.vhbt,
+                                    m->sur_acc, s));
         ++calls;
         return MOM6B_OK;
     };
