@@ -49,23 +49,38 @@ __device__ __forceinline__ float gelu_grad_f(float z)
 // transposed); with out != nullptr also the output layer out = W3 H + b3 of
 // the CTA's rows (N = 256 in one CTA).
 template <int BN>
-__global__ void __launch_bounds__(kGemmThreads, 1)
+__global__ void __launch_bounds__(kGemmThreads, 2)
 k_mlp_hidden(const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUtensorMap mB,
              int M, int N, int K, const float* __restrict__ bias, float* Z,
              __nv_bfloat16* H, __nv_bfloat16* HT, int ldt, const float* __restrict__ W3r,
              const float* __restrict__ b3, float* out, int* err)
 {
     float o0 = 0.f, o1 = 0.f;
-    gemm_tile<BN>(&mA, &mB, M, N, K, K, err, [&](int m, int n, const float* v) {
+    gemm_tile<BN, kGemmStagesShort>(&mA, &mB, M, N, K, K, err, [&](int m, int n, const float* v) {
+        // the thread's 16 consecutive columns: 64 B of Z and 32 B of H, stored
+        // as 16-byte vectors (n is a multiple of 16)
+        __align__(16) float z[16];
+        __align__(16) __nv_bfloat16 hb[16];
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
-            const float z = v[q] + bias[n + q];
-            if (Z) Z[(size_t)m * N + n + q] = z;
-            const __nv_bfloat16 hb = __float2bfloat16_rn(gelu_f(z));
-            if (H) H[(size_t)m * N + n + q] = hb;
-            if (HT) HT[(size_t)(n + q) * ldt + m] = hb;
+            z[q] = v[q] + bias[n + q];
+            hb[q] = __float2bfloat16_rn(gelu_f(z[q]));
+        }
+        if (Z) {
+            float4* zd = (float4*)(Z + (size_t)m * N + n);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) zd[q] = ((const float4*)z)[q];
+        }
+        if (H) {
+            uint4* hd = (uint4*)(H + (size_t)m * N + n);
+            hd[0] = ((const uint4*)hb)[0];
+            hd[1] = ((const uint4*)hb)[1];
+        }
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            if (HT) HT[(size_t)(n + q) * ldt + m] = hb[q];
             if (out) {
-                const float hr = __bfloat162float(hb);
+                const float hr = __bfloat162float(hb[q]);
                 o0 += hr * W3r[n + q];
                 o1 += hr * W3r[N + n + q];
             }
@@ -80,12 +95,12 @@ k_mlp_hidden(const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUt
 
 // Backward through a hidden layer: dZ = acc * GELU'(Z), stored transposed.
 template <int BN>
-__global__ void __launch_bounds__(kGemmThreads, 1)
+__global__ void __launch_bounds__(kGemmThreads, 2)
 k_mlp_dgelu(const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUtensorMap mB,
             int M, int N, int K, const float* __restrict__ Z, __nv_bfloat16* dZT, int ldt,
             int* err)
 {
-    gemm_tile<BN>(&mA, &mB, M, N, K, K, err, [&](int m, int n, const float* v) {
+    gemm_tile<BN, kGemmStagesShort>(&mA, &mB, M, N, K, K, err, [&](int m, int n, const float* v) {
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
             const float dz = v[q] * gelu_grad_f(Z[(size_t)m * N + n + q]);
@@ -101,9 +116,10 @@ k_mlp_wgrad(const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUte
             int M, int N, int K, int kps, float* part, int* err)
 {
     float* P = part + (size_t)blockIdx.z * M * N;
-    gemm_tile<BN>(&mA, &mB, M, N, K, kps, err, [&](int m, int n, const float* v) {
+    gemm_tile<BN, kGemmStages>(&mA, &mB, M, N, K, kps, err, [&](int m, int n, const float* v) {
+        float4* pd = (float4*)(P + (size_t)m * N + n);
 #pragma unroll
-        for (int q = 0; q < 16; ++q) P[(size_t)m * N + n + q] = v[q];
+        for (int q = 0; q < 4; ++q) pd[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
     });
 }
 
@@ -423,24 +439,24 @@ cudaError_t Mlp::set_params(const float* host)
 }
 
 template <class Kern>
-static cudaError_t gemm_attr(Kern k, int bn)
+static cudaError_t gemm_attr(Kern k, int bn, int stages)
 {
     return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                gemm_smem_bytes(bn));
+                                gemm_smem_bytes(bn, stages));
 }
 
 cudaError_t Mlp::forward(int B, bool keep, cudaStream_t s)
 {
     static bool attr = false;
     if (!attr) {
-        MLP_CK(gemm_attr(k_mlp_hidden<kMlpHidden>, kMlpHidden));
-        MLP_CK(gemm_attr(k_mlp_dgelu<kMlpHidden>, kMlpHidden));
-        MLP_CK(gemm_attr(k_mlp_wgrad<kMlpHidden>, kMlpHidden));
-        MLP_CK(gemm_attr(k_mlp_wgrad<kMlpInPad>, kMlpInPad));
+        MLP_CK(gemm_attr(k_mlp_hidden<kMlpHidden>, kMlpHidden, kGemmStagesShort));
+        MLP_CK(gemm_attr(k_mlp_dgelu<kMlpHidden>, kMlpHidden, kGemmStagesShort));
+        MLP_CK(gemm_attr(k_mlp_wgrad<kMlpHidden>, kMlpHidden, kGemmStages));
+        MLP_CK(gemm_attr(k_mlp_wgrad<kMlpInPad>, kMlpInPad, kGemmStages));
         attr = true;
     }
     const dim3 grid((B + kGemmBM - 1) / kGemmBM, 1, 1);
-    const int sm = gemm_smem_bytes(kMlpHidden);
+    const int sm = gemm_smem_bytes(kMlpHidden, kGemmStagesShort);
     k_mlp_hidden<kMlpHidden><<<grid, kGemmThreads, sm, s>>>(
         mX, mW1, B, kMlpHidden, kMlpInPad, P + kOffB1, keep ? Z1 : nullptr, H1,
         keep ? H1T : nullptr, B, nullptr, nullptr, nullptr, err);
@@ -458,18 +474,18 @@ cudaError_t Mlp::backward(int B, cudaStream_t s)
     k_mlp_out_reduce<<<(kOutPart + 255) / 256, 256, 0, s>>>(nb, B, bpart, G, loss);
     // dH1 = dZ2 W2, dZ1 = dH1 * GELU'(Z1) (transposed)
     const dim3 grid((B + kGemmBM - 1) / kGemmBM, 1, 1);
-    k_mlp_dgelu<kMlpHidden><<<grid, kGemmThreads, gemm_smem_bytes(kMlpHidden), s>>>(
+    k_mlp_dgelu<kMlpHidden><<<grid, kGemmThreads, gemm_smem_bytes(kMlpHidden, kGemmStagesShort), s>>>(
         mdZ2, mW2T, B, kMlpHidden, kMlpHidden, Z1, dZ1T, B, err);
     // weight gradients, split over the batch
     const int kps = splitk_kps(B);
     const int S = (B + kps - 1) / kps;
     k_mlp_wgrad<kMlpHidden><<<dim3(kMlpHidden / kGemmBM, 1, S), kGemmThreads,
-                              gemm_smem_bytes(kMlpHidden), s>>>(mdZ2T, mH1T_B, kMlpHidden,
+                              gemm_smem_bytes(kMlpHidden, kGemmStages), s>>>(mdZ2T, mH1T_B, kMlpHidden,
                                                                 kMlpHidden, B, kps, part, err);
     k_mlp_splitk_reduce<<<(kMlpHidden * kMlpHidden + 255) / 256, 256, 0, s>>>(
         S, kMlpHidden * kMlpHidden, part, G, kOffW2);
     k_mlp_wgrad<kMlpInPad><<<dim3(kMlpHidden / kGemmBM, 1, S), kGemmThreads,
-                             gemm_smem_bytes(kMlpInPad), s>>>(mdZ1T, mXT_B, kMlpHidden,
+                             gemm_smem_bytes(kMlpInPad, kGemmStages), s>>>(mdZ1T, mXT_B, kMlpHidden,
                                                               kMlpInPad, B, kps, part, err);
     k_mlp_splitk_reduce<<<(kMlpHidden * kMlpInPad + 255) / 256, 256, 0, s>>>(
         S, kMlpHidden * kMlpInPad, part, G, kOffW1);
@@ -530,7 +546,7 @@ cudaError_t Mlp::predict(int n, cudaStream_t s)
 {
     if (n > ni_cap || !imaps_ok) return cudaErrorInvalidValue;
     const dim3 grid((n + kGemmBM - 1) / kGemmBM, 1, 1);
-    const int sm = gemm_smem_bytes(kMlpHidden);
+    const int sm = gemm_smem_bytes(kMlpHidden, kGemmStagesShort);
     k_mlp_hidden<kMlpHidden><<<grid, kGemmThreads, sm, s>>>(
         mXi, mW1, n, kMlpHidden, kMlpInPad, P + kOffB1, nullptr, H1i, nullptr, n, nullptr,
         nullptr, nullptr, err);
@@ -655,9 +671,9 @@ __global__ void k_sur_features_train(SurGrid g, BtInputs in, const float* __rest
                                      const float* __restrict__ amp, int B, uint64_t seed,
                                      __nv_bfloat16* X)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)B * kMlpInPad) return;
-    const int s = (int)(t / kMlpInPad), f = (int)(t - (long long)s * kMlpInPad);
+    const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);   // B * 176 < 2^31
+    if (t >= B * kMlpInPad) return;
+    const int s = t / kMlpInPad, f = t - s * kMlpInPad;
     int i, j;
     sur_sample(g.D, seed, s, i, j);
     X[t] = __float2bfloat16_rn(sur_feature(g, in, norm, amp[s], i, j, f));
@@ -667,9 +683,9 @@ __global__ void k_sur_features_train_t(SurGrid g, BtInputs in, const float* __re
                                        const float* __restrict__ amp, int B, uint64_t seed,
                                        __nv_bfloat16* XT)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)B * kMlpInPad) return;
-    const int f = (int)(t / B), s = (int)(t - (long long)f * B);
+    const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    if (t >= B * kMlpInPad) return;
+    const int f = t / B, s = t - f * B;
     int i, j;
     sur_sample(g.D, seed, s, i, j);
     XT[t] = __float2bfloat16_rn(sur_feature(g, in, norm, amp[s], i, j, f));
@@ -680,6 +696,7 @@ cudaError_t launch_sur_features_train(const SurGrid& g, const BtInputs& in, cons
                                       __nv_bfloat16* XT, float* amp, cudaStream_t s)
 {
     const long long n = (long long)B * kMlpInPad;
+    if (n >= (1LL << 31)) return cudaErrorInvalidValue;
     const int nb = 256;
     const unsigned blocks = (unsigned)((n + nb - 1) / nb);
     cudaError_t e = sur_amp_reduce(g, in, norm, gacc, s);
@@ -725,9 +742,9 @@ __global__ void k_sur_features_all(SurGrid g, BtInputs in, const float* __restri
                                    const float* __restrict__ amp, __nv_bfloat16* X)
 {
     const int nx = g.D.ie - g.D.is + 1, ny = g.D.je - g.D.js + 1;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)nx * ny * kMlpInPad) return;
-    const int s = (int)(t / kMlpInPad), f = (int)(t - (long long)s * kMlpInPad);
+    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;   // < 2^32 (host checks)
+    if (t >= (unsigned)nx * (unsigned)ny * (unsigned)kMlpInPad) return;
+    const int s = (int)(t / (unsigned)kMlpInPad), f = (int)(t - (unsigned)s * kMlpInPad);
     const int i = g.D.is + s % nx, j = g.D.js + s / nx;
     X[t] = __float2bfloat16_rn(sur_feature(g, in, norm, amp[s], i, j, f));
 }
@@ -736,6 +753,7 @@ cudaError_t launch_sur_features_all(const SurGrid& g, const BtInputs& in, const 
                                     double* gacc, __nv_bfloat16* X, float* amp, cudaStream_t s)
 {
     const long long n = (long long)(g.D.ie - g.D.is + 1) * (g.D.je - g.D.js + 1) * kMlpInPad;
+    if (n >= (1LL << 32)) return cudaErrorInvalidValue;
     cudaError_t e = sur_amp_reduce(g, in, norm, gacc, s);
     if (e != cudaSuccess) return e;
     const int nc = (g.D.ie - g.D.is + 1) * (g.D.je - g.D.js + 1);

@@ -24,6 +24,9 @@
 namespace mom6b {
 
 constexpr int kGemmBM = 128, kGemmBK = 64, kGemmStages = 4, kGemmThreads = 128;
+// Stages of the short-K layers (K <= 256): two fit twice per SM, so one
+// CTA's epilogue overlaps the other's MMAs (2 x 256 TMEM columns = all 512).
+constexpr int kGemmStagesShort = 2;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
 {
@@ -152,7 +155,7 @@ constexpr long long kGemmWaitBudget = 2000000000LL;
 // base address in *tmem (all threads), or false when a wait gave up.  Epi is
 // called by every thread with (row, first column, 16 values) for each of the
 // BN / 16 column chunks of its row, then the tensor memory is freed.
-template <int BN, class Epi>
+template <int BN, int STAGES, class Epi>
 __device__ __forceinline__ void gemm_tile(const CUtensorMap* mapA, const CUtensorMap* mapB,
                                           int M, int N, int K, int k_per_split, int* err,
                                           Epi&& epi)
@@ -164,7 +167,7 @@ __device__ __forceinline__ void gemm_tile(const CUtensorMap* mapA, const CUtenso
     extern __shared__ __align__(1024) unsigned char gsm_raw[];
     // 1024-byte alignment of every stage (the swizzle atom)
     unsigned char* gsm = (unsigned char*)(((uintptr_t)gsm_raw + 1023) & ~(uintptr_t)1023);
-    __shared__ __align__(8) uint64_t full[kGemmStages], empty[kGemmStages], done;
+    __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], done;
     __shared__ uint32_t s_tmem;
     __shared__ int s_fail;
 
@@ -175,7 +178,7 @@ __device__ __forceinline__ void gemm_tile(const CUtensorMap* mapA, const CUtenso
     const int nk = k1 > k0 ? (k1 - k0 + kGemmBK - 1) / kGemmBK : 0;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < kGemmStages; ++s) {
+        for (int s = 0; s < STAGES; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
@@ -197,7 +200,7 @@ __device__ __forceinline__ void gemm_tile(const CUtensorMap* mapA, const CUtenso
     if (warp == 0 && lane == 0) {
         // producer: TMA loads of A rows [m0, m0+128) and B rows [n0, n0+BN)
         for (int kt = 0; kt < nk; ++kt) {
-            const int s = kt % kGemmStages, u = kt / kGemmStages;
+            const int s = kt % STAGES, u = kt / STAGES;
             if (u > 0 && !mbar_wait(&empty[s], (uint32_t)((u - 1) & 1), kGemmWaitBudget)) {
                 s_fail = 1;
                 break;
@@ -213,7 +216,7 @@ __device__ __forceinline__ void gemm_tile(const CUtensorMap* mapA, const CUtenso
         const uint32_t idesc = umma_idesc_bf16(BN);
         int issued = 0;
         for (int kt = 0; kt < nk; ++kt) {
-            const int s = kt % kGemmStages, u = kt / kGemmStages;
+            const int s = kt % STAGES, u = kt / STAGES;
             if (!mbar_wait(&full[s], (uint32_t)(u & 1), kGemmWaitBudget)) {
                 s_fail = 1;
                 break;
@@ -254,11 +257,10 @@ __device__ __forceinline__ void gemm_tile(const CUtensorMap* mapA, const CUtenso
                      "r"(TCOLS));
 }
 
-// Dynamic shared memory a gemm_tile<BN> launch needs.
-__host__ __device__ constexpr int gemm_smem_bytes(int bn)
+// Dynamic shared memory a gemm_tile<BN, STAGES> launch needs.
+__host__ __device__ constexpr int gemm_smem_bytes(int bn, int stages)
 {
-    return kGemmStages * (kGemmBM * kGemmBK * 2 + ((bn * kGemmBK * 2 + 1023) / 1024) * 1024) +
-           1024;
+    return stages * (kGemmBM * kGemmBK * 2 + ((bn * kGemmBK * 2 + 1023) / 1024) * 1024) + 1024;
 }
 
 } // namespace mom6b
