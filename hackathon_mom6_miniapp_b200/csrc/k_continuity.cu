@@ -422,8 +422,9 @@ __device__ __forceinline__ void cell_convergence(const Dims& D, const Metrics& M
     }
 }
 
-template <int CH>
-__global__ void __launch_bounds__(128)
+// MINB: the CTAs per SM the register allocation is held to (launch bounds).
+template <int CH, int MINB = 1>
+__global__ void __launch_bounds__(128, MINB)
 k_cont_faces(Dims D, Metrics M, const double* __restrict__ u,
              const double* __restrict__ hin, const double* __restrict__ hW,
              const double* __restrict__ hE, const double* __restrict__ uhbt2d,
@@ -904,6 +905,9 @@ k_cont_tile(Dims D, Metrics M, const double* __restrict__ u, const double* __res
 
 // CTAs per SM for k_cont_faces; 0 lets the hardware fill the SM.
 constexpr int kContCtasPerSM = 0;
+// CTAs per SM the face kernel's registers are held to: 4 (128 registers) is
+// the fastest on B200 (the unconstrained build takes 204 registers, 2 CTAs).
+constexpr int kContMinBlocks = 4;
 
 size_t continuity_overlap_doubles(const Dims& D)
 {
@@ -978,7 +982,16 @@ cudaError_t launch_continuity(const Dims& D, const Metrics& M, const double* u,
             const char* e = getenv("MOM6B_CONT_CHUNK");
             chunk = e ? atoi(e) : kContChunk;
         }
-        auto kern = chunk == 1 ? k_cont_faces<1> : chunk == 4 ? k_cont_faces<4> : k_cont_faces<2>;
+        static int minb = -1;
+        if (minb < 0) {
+            const char* e = getenv("MOM6B_CONT_MINB");
+            minb = e ? atoi(e) : kContMinBlocks;
+        }
+        auto kern = chunk == 1   ? k_cont_faces<1>
+                    : chunk == 4 ? (minb == 4 ? k_cont_faces<4, 4>
+                                    : minb == 5 ? k_cont_faces<4, 5>
+                                                : k_cont_faces<4>)
+                                 : (minb == 4 ? k_cont_faces<2, 4> : k_cont_faces<2>);
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e != cudaSuccess) return e;

@@ -146,8 +146,10 @@ cudaError_t launch_ens_tendency(const EnsDomain* doms, const int* start, int n, 
 }
 
 // ---- vertical viscosity ----------------------------------------------------------
+// Register caps as threads per SM, the single-domain kernels' measured best:
+// vertical viscosity 1024 (8 CTAs of 128), continuity faces 640 (5 of 128).
 template <int KMAX, int CH, int NB>
-__global__ void __launch_bounds__(NB)
+__global__ void __launch_bounds__(NB, 1024 / NB)
 k_ens_vertvisc(const EnsDomain* __restrict__ doms, const int* __restrict__ start, int n,
                int half)
 {
@@ -217,7 +219,7 @@ cudaError_t launch_ens_ppm(const EnsDomain* doms, const int* start, int n, int t
 }
 
 template <int NB>
-__global__ void __launch_bounds__(NB)
+__global__ void __launch_bounds__(NB, 640 / NB)
 k_ens_faces(const EnsDomain* __restrict__ doms, const int* __restrict__ start, int n, int half)
 {
     __shared__ __align__(16) EnsDomain E;

@@ -42,7 +42,8 @@ k_ppm_edges_f(Dims D, Metrics M, const float* __restrict__ hin, float* __restric
     ppm_cell_f(D, M, hin, hW, hE, h_min, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z);
 }
 
-__global__ void __launch_bounds__(128)
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB)
 k_cont_faces_f(Dims D, Metrics M, const float* __restrict__ u, const float* __restrict__ hin,
                const float* __restrict__ hW, const float* __restrict__ hE,
                const double* __restrict__ uhbt2d, ContOutF O, float* ovl_all, double dt)
@@ -66,7 +67,17 @@ cudaError_t launch_continuity_f(const Dims& D, const Metrics& M, const float* u,
     const int nb = 128, step = nb - 1;
     const int nfaces = D.ie - (D.is - 1) + 1;
     dim3 grid((nfaces - 1 + step - 1) / step, D.je - D.js + 1, 1);
-    k_cont_faces_f<<<grid, nb, 0, s>>>(D, M, u, hin, hW, hE, uhbt, O, (float*)uh_ovl, dt);
+    static int minb = -1;
+    if (minb < 0) {
+        const char* e = getenv("MOM6B_CONTF_MINB");
+        minb = e ? atoi(e) : 5;   // 5 CTAs per SM: 2.44 ms per step (no cap: 3.19)
+    }
+    if (minb == 4)
+        k_cont_faces_f<4><<<grid, nb, 0, s>>>(D, M, u, hin, hW, hE, uhbt, O, (float*)uh_ovl, dt);
+    else if (minb == 5)
+        k_cont_faces_f<5><<<grid, nb, 0, s>>>(D, M, u, hin, hW, hE, uhbt, O, (float*)uh_ovl, dt);
+    else
+        k_cont_faces_f<1><<<grid, nb, 0, s>>>(D, M, u, hin, hW, hE, uhbt, O, (float*)uh_ovl, dt);
     return cudaGetLastError();
 }
 

@@ -28,6 +28,10 @@ __device__ __forceinline__ C vv_botfn(C z2) {
 // layers instead of one per layer.
 // Layers whose inputs one prefetch brings in.
 constexpr int kVvChunk = 4;
+// CTAs per SM the registers are held to, by storage type: measured fastest on
+// B200 (FP64 6: 2.28 ms per step, no cap 2.50; FP32 8: 1.85 ms, no cap 2.67).
+template <typename R>
+constexpr int vv_min_blocks() { return sizeof(R) == 4 ? 8 : 6; }
 
 // The column of thread tx of the CTA with block coordinates (bx, by): row
 // by of the interleaved u/v row list, column bx * blockDim.x + tx.
@@ -237,8 +241,9 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
     tbot[(size_t)(j - 1) * D.n1 + (i - 1)] = tb;
 }
 
-template <int KMAX, int CH, typename R>
-__global__ void __launch_bounds__(128)
+// MINB: the CTAs per SM the register allocation is held to.
+template <int KMAX, int CH, typename R, int MINB = 1>
+__global__ void __launch_bounds__(128, MINB)
 k_vertvisc_pf(Dims D, Metrics M, R* __restrict__ u, R* __restrict__ v,
               const R* __restrict__ h, double dt, VVParams P,
               double* __restrict__ taux_bot, double* __restrict__ tauy_bot)
@@ -256,15 +261,21 @@ static cudaError_t launch_vv_pf(const Dims& D, const Metrics& M, R* u, R* v, con
     int ncol = D.ie - D.is + 2;
     int nrows = (D.je - D.js + 1) + (D.je - D.js + 2);
     dim3 grid((ncol + nb - 1) / nb, nrows, 1);
-    static int chunk = -1;
+    static int chunk = -1, minb = -1;
     if (chunk < 0) {
         const char* e = getenv("MOM6B_VV_CHUNK");
         chunk = e ? atoi(e) : kVvChunk;
+        const char* b = getenv("MOM6B_VV_MINB");
+        minb = b ? atoi(b) : vv_min_blocks<R>();
     }
     if (chunk == 2)
         k_vertvisc_pf<KMAX, 2, R><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P, taux_bot, tauy_bot);
     else if (chunk == 8)
         k_vertvisc_pf<KMAX, 8, R><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P, taux_bot, tauy_bot);
+    else if (minb == 6)
+        k_vertvisc_pf<KMAX, 4, R, 6><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P, taux_bot, tauy_bot);
+    else if (minb == 8)
+        k_vertvisc_pf<KMAX, 4, R, 8><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P, taux_bot, tauy_bot);
     else
         k_vertvisc_pf<KMAX, 4, R><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P, taux_bot, tauy_bot);
     return cudaGetLastError();
