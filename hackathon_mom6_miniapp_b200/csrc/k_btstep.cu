@@ -276,6 +276,8 @@ constexpr int kBtTileR = 4;
 
 struct BTTiles {
     int nbx, nby, tw, th;  // tiles and tile size
+    int nt;                // threads per CTA: 1024 (tiles <= 64 x 64, one CTA per SM)
+                           // or 512 (tiles <= 64 x 32, two CTAs per SM)
 };
 
 // Wait until every tile in nb[0..nnb) has published substep `target` (its
@@ -316,7 +318,7 @@ __device__ __forceinline__ bool wait_neighbours(const BTWork& W, const int* nb, 
 // uhbt_n, vhbt_n of the owned points into W.uhbt / W.vhbt (the surrogate's
 // training targets; zero outside their ranges).
 template <int NT, bool UNI, bool TAVG>
-__global__ void __launch_bounds__(NT, 1)
+__global__ void __launch_bounds__(NT, 1024 / NT)
 k_btstep_tiled(Dims D, Metrics M, UniMetrics U, BTWork W, BTParams P, BTTiles T,
                const double* eta_in, const double* ubt_in, const double* vbt_in,
                double* u_av, double* v_av, double* eta_av)
@@ -388,18 +390,53 @@ k_btstep_tiled(Dims D, Metrics M, UniMetrics U, BTWork W, BTParams P, BTTiles T,
         // shared memory (new eta in Sp, new ubt/vbt in Sun/Svn); the halo comes
         // from the neighbours' published buffers once they finished substep n-1.
         if (n > 1 && !wait_neighbours(W, nbr, nnb, (unsigned int)(n - 1), P.spin_budget)) return;
-        for (int jl = tyl; jl < LH; jl += TY)
-        for (int il = txl; il < LW; il += 32) {
-            const int q = jl * LW + il, i = lx0 + il, j = ly0 + jl;
-            double e = 0.0, ub = 0.0, vb = 0.0;
-            const bool mine = n > 1 && i >= x0 && i <= x1 && j >= y0 && j <= y1;
-            if (mine) {
-                e = Sp[q]; ub = Sun[q]; vb = Svn[q];
-            } else if (i >= 1 && i <= D.n1 && j >= 1 && j <= D.n2) {
-                int p = (j - 1) * D.n1 + (i - 1);
-                e = __ldcg(ce + p); ub = __ldcg(cu + p); vb = __ldcg(cv + p);
+        if (n == 1) {
+            for (int jl = tyl; jl < LH; jl += TY)
+            for (int il = txl; il < LW; il += 32) {
+                const int q = jl * LW + il, i = lx0 + il, j = ly0 + jl;
+                double e = 0.0, ub = 0.0, vb = 0.0;
+                if (i >= 1 && i <= D.n1 && j >= 1 && j <= D.n2) {
+                    int p = (j - 1) * D.n1 + (i - 1);
+                    e = __ldcg(ce + p); ub = __ldcg(cu + p); vb = __ldcg(cv + p);
+                }
+                Se[q] = e; Su[q] = ub; Sv[q] = vb; Sun[q] = ub; Svn[q] = vb;
             }
-            Se[q] = e; Su[q] = ub; Sv[q] = vb; Sun[q] = ub; Svn[q] = vb;
+        } else {
+            // owned points: each thread's own, already in shared memory
+#pragma unroll
+            for (int r = 0; r < kBtTileR; ++r) {
+                const int i = x0 + txl + 32 * (r & 1), j = y0 + tyl + TY * (r >> 1);
+                if (i > x1 || j > y1) continue;
+                const int q = (j - ly0) * LW + (i - lx0);
+                Se[q] = Sp[q]; Su[q] = Sun[q]; Sv[q] = Svn[q];
+            }
+            // the ring of the window around the owned rectangle, one flat index
+            // per point, so a thread's loads are all in flight at once
+            const int nb = y0 - ly0, na = (ly0 + LH - 1) - y1;
+            const int nl = x0 - lx0, nr = (lx0 + LW - 1) - x1;
+            const int mid = y1 - y0 + 1, side = nl + nr;
+            const int nring = (nb + na) * LW + mid * side;
+            for (int t = tid; t < nring; t += NT) {
+                int i, j;
+                if (t < nb * LW) {
+                    j = ly0 + t / LW; i = lx0 + t % LW;
+                } else if (t < (nb + na) * LW) {
+                    const int t2 = t - nb * LW;
+                    j = y1 + 1 + t2 / LW; i = lx0 + t2 % LW;
+                } else {
+                    const int t3 = t - (nb + na) * LW;
+                    const int c = t3 % side;
+                    j = y0 + t3 / side;
+                    i = c < nl ? lx0 + c : x1 + 1 + (c - nl);
+                }
+                const int q = (j - ly0) * LW + (i - lx0);
+                double e = 0.0, ub = 0.0, vb = 0.0;
+                if (i >= 1 && i <= D.n1 && j >= 1 && j <= D.n2) {
+                    int p = (j - 1) * D.n1 + (i - 1);
+                    e = __ldcg(ce + p); ub = __ldcg(cu + p); vb = __ldcg(cv + p);
+                }
+                Se[q] = e; Su[q] = ub; Sv[q] = vb; Sun[q] = ub; Svn[q] = vb;
+            }
         }
         __syncthreads();
         // S2: eta_pred on [x0-1, x1+1] x [y0-1, y1+1] within [is, ie] x [js, je]
@@ -784,7 +821,26 @@ static cudaError_t init_bt_blocks()
 
 static bool tiles_for(const Dims& D, BTTiles& T)
 {
+    static int nt = -1;
+    if (nt < 0) {
+        const char* e = getenv("MOM6B_BT_NT");
+        nt = (e && atoi(e) == 512) ? 512 : 1024;
+    }
     int bw = D.ie - D.is + 2, bh = D.je - D.js + 2;
+    T.nt = nt;
+    if (nt == 512) {
+        // two CTAs per SM, each thread of the 32 x 16 layout owns 2 x 2 points
+        const int maxt = 2 * g_bt_blocks;
+        int nbx = (bw + 63) / 64, nby = (bh + 31) / 32;
+        if ((long long)nbx * nby > maxt) return false;
+        while ((long long)nbx * (nby + 1) <= maxt && (long long)(nbx + 1) * nby > maxt &&
+               (bh + nby) / (nby + 1) >= 8)
+            ++nby;
+        T.nbx = nbx; T.nby = nby;
+        T.tw = (bw + nbx - 1) / nbx; T.th = (bh + nby - 1) / nby;
+        const size_t smem = (size_t)6 * (T.tw + 3) * (T.th + 3) * sizeof(double);
+        return T.tw <= 64 && T.th <= 32 && smem <= 113 * 1024 && nbx * nby <= kBtMaxTiles;
+    }
     int nbx = 1, nby = 1;
     while ((long long)(nbx + 1) * (nby + 1) <= g_bt_blocks) { ++nbx; ++nby; }
     while ((long long)(nbx + 1) * nby <= g_bt_blocks && (bw + nbx) / (nbx + 1) >= 8) ++nbx;
@@ -792,7 +848,7 @@ static bool tiles_for(const Dims& D, BTTiles& T)
     T.tw = (bw + nbx - 1) / nbx; T.th = (bh + nby - 1) / nby;
     size_t smem = (size_t)6 * (T.tw + 3) * (T.th + 3) * sizeof(double);
     // each of the 32 x 32 threads owns the points (txl + 32a, tyl + 32b), a, b in {0, 1}
-    return T.tw <= 64 && T.th <= 64 && smem <= 227 * 1024;
+    return T.tw <= 64 && T.th <= 64 && smem <= 227 * 1024 && nbx * nby <= kBtMaxTiles;
 }
 
 
@@ -802,12 +858,19 @@ static cudaError_t launch_btstep_tiled(const Dims& D, const Metrics& M, const Un
                                        const double* vbt_in, double* u_av, double* v_av,
                                        double* eta_av, cudaStream_t s, bool tavg = false)
 {
-    const int NT = 1024;
+    const int NT = T.nt;
     size_t smem = (size_t)6 * (T.tw + 3) * (T.th + 3) * sizeof(double);
-    const void* fn = tavg ? (U.valid_bt ? (const void*)k_btstep_tiled<NT, true, true>
-                                        : (const void*)k_btstep_tiled<NT, false, true>)
-                          : (U.valid_bt ? (const void*)k_btstep_tiled<NT, true, false>
-                                        : (const void*)k_btstep_tiled<NT, false, false>);
+    const void* fn;
+    if (NT == 512)
+        fn = tavg ? (U.valid_bt ? (const void*)k_btstep_tiled<512, true, true>
+                                : (const void*)k_btstep_tiled<512, false, true>)
+                  : (U.valid_bt ? (const void*)k_btstep_tiled<512, true, false>
+                                : (const void*)k_btstep_tiled<512, false, false>);
+    else
+        fn = tavg ? (U.valid_bt ? (const void*)k_btstep_tiled<1024, true, true>
+                                : (const void*)k_btstep_tiled<1024, false, true>)
+                  : (U.valid_bt ? (const void*)k_btstep_tiled<1024, true, false>
+                                : (const void*)k_btstep_tiled<1024, false, false>);
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
@@ -945,10 +1008,10 @@ cudaError_t launch_btstep_tavg(const Dims& D, const Metrics& M, const UniMetrics
 // must not allocate while a stream is being captured into a CUDA graph.
 // mom6b_btstep_noalloc therefore keeps every work array of the loop in the
 // file-scope array below, sized for grids of at most kNoAllocMaxPoints
-// points (n1 * n2), i.e. 6 x 589,824 doubles plus a 256-byte header, about
+// points (n1 * n2), i.e. 6 x 589,824 doubles plus a 2.3 KB header, about
 // 28.3 MB per GPU that loads this library, held until the process exits.
 constexpr long long kNoAllocMaxPoints = 768LL * 768LL;
-constexpr long long kNoAllocHeader = 160;  // doubles: barrier words, status, tile flags
+constexpr long long kNoAllocHeader = 288;  // doubles: barrier words, status, tile flags
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocHeader +
                                                           6 * kNoAllocMaxPoints];
 

@@ -298,11 +298,43 @@ __device__ void flux_adjust_pair(const FaceCol<EI>& F, int nz, double dt, double
     }
 }
 
+// One zonal_flux_adjust solve on its own (:813-903): the transports of every
+// evaluated iterate go to uh_out when it is given (then the last iterate is
+// evaluated even at max_itts), otherwise passes run only to update.
+template <int CH, typename EI>
+__device__ void flux_adjust_one(const FaceCol<EI>& F, int nz, double dt, double target,
+                                double tol_eta_dt_fac, Newton& S, double* uh_out,
+                                size_t uh_stride)
+{
+    const int max_itts = 20;
+    for (int itt = 1; itt <= max_itts; ++itt) {
+        if (!newton_iter(S, itt, tol_eta_dt_fac)) break;
+        const bool update = itt < max_itts;
+        if (!update && !uh_out) break;
+        const double du = S.du;
+        double e = -target, sm = 0.0;
+        for_layers<CH>(F, nz, [&](int k, const LayerVals& L) {
+            double hm;
+            double uhk = flux_eval(F, L, L.u + du, dt, hm);
+            if (uh_out) uh_out[(size_t)(k - 1) * uh_stride] = uhk;
+            e = e + uhk;
+            sm = sm + F.dy * hm;
+        });
+        if (update) {
+            S.uh_err = e;
+            S.duhdu_tot = sm;
+            S.uh_err_best = dmin(S.uh_err_best, fabs(S.uh_err));
+        }
+    }
+}
+
 // The work of one face (I, j) after its column views are set up: initial
 // fluxes, CFL limits, zonal_flux_adjust, du_cor and, for the owner,
 // set_zonal_BT_cont and zonal_flux_thickness.  uh/ust receive the face's
 // transports (the output array, or the CTA's overlap column).
-template <int CH, typename EI>
+// LOCK: the two solves in lockstep (one column pass serves both) or one
+// after the other (fewer live registers; the second runs only for uhbt /= 0).
+template <int CH, typename EI, bool LOCK = true>
 __device__ __forceinline__ void face_work(const Dims& D, const Metrics& M, FaceCol<EI>& F,
                                           int I, int j, size_t f0, double* uh, size_t ust,
                                           bool owner, const double* uhbt2d, const ContOut& O,
@@ -336,15 +368,28 @@ __device__ __forceinline__ void face_work(const Dims& D, const Metrics& M, FaceC
     // zero-transport solve of set_zonal_BT_cont (B, :991-1002); with uhbt = 0
     // B would repeat A exactly, so du0 = du.
     const bool solve0 = owner && uhbt != 0.0;
-    Newton A = newton_start(uh_tot_0 - uhbt, duhdu_tot_0, du_max_CFL, du_min_CFL, true);
-    Newton B = newton_start(uh_tot_0 - 0.0, duhdu_tot_0, du_max_CFL, du_min_CFL, solve0);
-    flux_adjust_pair<CH>(F, nz, dt, uhbt, fac, A, B, uh, ust);
-    const double du = A.du;
+    double du, du0;
+    if (LOCK) {
+        Newton A = newton_start(uh_tot_0 - uhbt, duhdu_tot_0, du_max_CFL, du_min_CFL, true);
+        Newton B = newton_start(uh_tot_0 - 0.0, duhdu_tot_0, du_max_CFL, du_min_CFL, solve0);
+        flux_adjust_pair<CH>(F, nz, dt, uhbt, fac, A, B, uh, ust);
+        du = A.du;
+        du0 = solve0 ? B.du : du;
+    } else {
+        Newton A = newton_start(uh_tot_0 - uhbt, duhdu_tot_0, du_max_CFL, du_min_CFL, true);
+        flux_adjust_one<CH>(F, nz, dt, uhbt, fac, A, uh, ust);
+        du = A.du;
+        du0 = du;
+        if (solve0) {
+            Newton B = newton_start(uh_tot_0 - 0.0, duhdu_tot_0, du_max_CFL, du_min_CFL, true);
+            flux_adjust_one<CH>(F, nz, dt, 0.0, fac, B, (double*)nullptr, 0);
+            du0 = B.du;
+        }
+    }
     if (!owner) return;
     O.du_cor[f0] = du;
 
     // set_zonal_BT_cont (:991-1121)
-    const double du0 = solve0 ? B.du : du;
     const double Idt = 1.0 / dt;
     const double du_CFL = (F32(1e-6) * Idt) * MOM6B_A2(M.dxCu, I, j, D);
     double duR = dmin(0.0, du0 - du_CFL);
@@ -423,7 +468,7 @@ __device__ __forceinline__ void cell_convergence(const Dims& D, const Metrics& M
 }
 
 // MINB: the CTAs per SM the register allocation is held to (launch bounds).
-template <int CH, int MINB = 1>
+template <int CH, int MINB = 1, bool LOCK = true>
 __global__ void __launch_bounds__(128, MINB)
 k_cont_faces(Dims D, Metrics M, const double* __restrict__ u,
              const double* __restrict__ hin, const double* __restrict__ hW,
@@ -449,7 +494,7 @@ k_cont_faces(Dims D, Metrics M, const double* __restrict__ u,
         const bool to_ovl = !owner;
         double* uh = to_ovl ? ovl : O.uh + f0;
         const size_t ust = to_ovl ? 1 : F.plane;
-        face_work<CH>(D, M, F, I, j, f0, uh, ust, owner, uhbt2d, O, dt);
+        face_work<CH, size_t, LOCK>(D, M, F, I, j, f0, uh, ust, owner, uhbt2d, O, dt);
     }
     __syncthreads();  // the CTA's transport columns are complete and visible
     cell_convergence(D, M, I, j, hin, ovl, O, dt);
@@ -987,10 +1032,18 @@ cudaError_t launch_continuity(const Dims& D, const Metrics& M, const double* u,
             const char* e = getenv("MOM6B_CONT_MINB");
             minb = e ? atoi(e) : kContMinBlocks;
         }
+        static int lock = -1;
+        if (lock < 0) {
+            const char* e = getenv("MOM6B_CONT_LOCK");
+            lock = e ? atoi(e) : 0;   // one solve after the other: 3.87 ms per step (lockstep 3.92)
+        }
         auto kern = chunk == 1   ? k_cont_faces<1>
-                    : chunk == 4 ? (minb == 4 ? k_cont_faces<4, 4>
-                                    : minb == 5 ? k_cont_faces<4, 5>
-                                                : k_cont_faces<4>)
+                    : chunk == 4 ? (lock ? (minb == 4 ? k_cont_faces<4, 4>
+                                            : minb == 5 ? k_cont_faces<4, 5>
+                                                        : k_cont_faces<4>)
+                                         : (minb == 4 ? k_cont_faces<4, 4, false>
+                                            : minb == 5 ? k_cont_faces<4, 5, false>
+                                                        : k_cont_faces<4, 3, false>))
                                  : (minb == 4 ? k_cont_faces<2, 4> : k_cont_faces<2>);
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);

@@ -47,8 +47,8 @@ struct BTWork {
     unsigned int* tile_flag;   // per-tile substep counters (kBtMaxTiles entries)
 };
 
-// Upper bound on the tiles of the tiled barotropic kernel (one per SM).
-constexpr int kBtMaxTiles = 256;
+// Upper bound on the tiles of the tiled barotropic kernel (one or two per SM).
+constexpr int kBtMaxTiles = 512;
 
 struct BTParams {
     double dtbt, dgeo_de, trans_wt1, trans_wt2, inv_nstep;
