@@ -33,7 +33,8 @@ with the network-alone eta error after 100 steps against the FP64 form.
 
 --impl reference times the reference's CPU implementation of the path on the
 host cores: the C restatement of the serial Fortran driver (the Fortran
-itself cannot be compiled here), on rank 0 only.
+itself cannot be compiled here), built with OpenMP over rows and run on all
+host threads (its single-thread rate beside it), on rank 0 only.
 """
 import argparse
 import json
@@ -168,42 +169,56 @@ def barrier(dist):
         dist.barrier()
 
 
-def cpu_reference_rate(nthreads, seconds_budget=20.0):
+def cpu_reference_rate(threads=None):
     """Time the oracle restatement of the serial driver on a bounded sample of
-    the workload: strips of the 720x720x75 bt50 domain, scaled by cell count."""
-    from oracle.pyoracle import INIT_CFG, Oracle, lib
-    # sample: the full 720-point i extent and nj_s rows in j
+    the workload: a strip of the 720x720x75 bt50 domain (all 720 points in i,
+    40 rows in j), one RK2 step, scaled by compute cells.  threads=None is the
+    single-threaded build (the reference serial backend has no threading);
+    threads=0 the OpenMP build of the same source on all host threads (rows in
+    parallel, results identical)."""
+    from oracle.pyoracle import INIT_CFG, Oracle
     nj_s = 40
-    o = Oracle(NI, nj_s, NK, BT, INIT_CFG, seed=0, dt=600.0)
+    o = Oracle(NI, nj_s, NK, BT, INIT_CFG, seed=0, dt=600.0, threads=threads)
+    cores = o.threads
     t0 = time.perf_counter()
     o.step(1)
     dt = time.perf_counter() - t0
     o.close()
     scale = ((NI - 4) * (NJ - 4)) / ((NI - 4) * (nj_s - 4))
     per_full_step = dt * scale
-    return 1.0 / per_full_step, f"1 RK2 step of a 720x{nj_s}x75 bt50 strip " \
-        f"({dt:.2f} s), scaled by compute cells to 720x720", 1
+    what = "OpenMP over rows" if threads is not None else "single thread"
+    return 1.0 / per_full_step, f"1 RK2 step of a 720x{nj_s}x75 bt50 strip ({dt:.2f} s, " \
+        f"{what}, {cores} thread(s)), scaled by compute cells to 720x720", cores
+
+
+def cpu_baseline_line():
+    """cpu_baseline: the oracle on all host threads, with its single-thread rate."""
+    r1, s1, _ = cpu_reference_rate(None)
+    rn, sn, cores = cpu_reference_rate(0)
+    return {"value": rn, "unit": "steps/s", "cores": cores, "kind": "port", "sample": sn,
+            "single_thread": {"value": r1, "unit": "steps/s", "cores": 1, "sample": s1}}
 
 
 def run_reference(args, world, rank, local, dist):
     if rank != 0:
         return
     rates = []
-    sample = ""
-    for _ in range(args.warmup if args.warmup < 1 else 1):
-        pass
+    sample, cores = "", 1
     for _ in range(max(1, min(args.steps, 3))):
-        r, sample, cores = cpu_reference_rate(1)
+        r, sample, cores = cpu_reference_rate(0)
         rates.append(r)
     value = sorted(rates)[len(rates) // 2]
+    r1, s1, _ = cpu_reference_rate(None)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "split RK2 step 720x720x75 bt50 (seeded beta plane)",
                        "ni": NI, "nj": NJ, "nk": NK, "bt_nsteps": BT},
-            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 1,
-                             "kind": "port", "sample": sample},
+            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": cores,
+                             "kind": "port", "sample": sample,
+                             "single_thread": {"value": r1, "unit": "steps/s", "cores": 1,
+                                               "sample": s1}},
             "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -505,9 +520,7 @@ def run_ours(args, world, rank, local, dist):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        r, sample, cores = cpu_reference_rate(1)
-        cpu = {"value": r, "unit": "steps/s", "cores": cores, "kind": "port",
-               "sample": sample}
+        cpu = cpu_baseline_line()
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup,

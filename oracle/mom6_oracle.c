@@ -19,6 +19,19 @@
 
 #define F32(x) ((double)(x##f))
 
+/* Row-parallel loops.  Built with -fopenmp (liboracle_omp.so) the marked
+ * loops, whose iterations write disjoint rows (or layers) and read only
+ * arrays no iteration writes, run on all host threads; the results equal the
+ * single-threaded build's bit for bit.  Without OpenMP the marks vanish. */
+#ifdef _OPENMP
+#include <omp.h>
+#define OMP_FOR _Pragma("omp parallel for schedule(static)")
+#define OMP_COLS _Pragma("omp for schedule(static)")
+#else
+#define OMP_FOR
+#define OMP_COLS
+#endif
+
 /* Physical constants, mom6_types.F90:80-85. */
 static const double G_EARTH = 9.80;
 static const double RHO_0 = 1035.0;
@@ -118,6 +131,16 @@ static void philox4x32_10(uint32_t ctr[4], uint32_t key[2]) {
         k0 += 0x9E3779B9u;
         k1 += 0xBB67AE85u;
     }
+}
+
+int oracle_set_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+    return omp_get_max_threads();
+#else
+    (void)n;
+    return 1;
+#endif
 }
 
 double oracle_normal(uint64_t seed, uint32_t stream, uint64_t index) {
@@ -483,6 +506,7 @@ void oracle_halo_fill(const oracle_model *m, double *f, int nz, int kind) {
 /* ------------------------------------------------------------------------ */
 void oracle_compute_transports(oracle_model *m, const double *u, const double *v,
                                const double *h, double *uh, double *vh) {
+    OMP_FOR
     for (int k = 1; k <= m->nk; ++k)
         for (int j = m->jsd; j <= m->jed; ++j)
             for (int i = m->isd; i <= m->ied; ++i) {
@@ -510,6 +534,7 @@ static void hor_visc_rows(oracle_model *m, const double *u, const double *v,
            *str_xx = m->hv_str_xx, *str_xy = m->hv_str_xy, *h_u = m->hv_h_u,
            *h_v = m->hv_h_v, *hq = m->hv_hq, *Kh = m->hv_Kh;
     /* STEP 1 */
+    OMP_FOR
     for (int j = Jsq; j <= Jeq + 1; ++j)
         for (int i = Isq; i <= Ieq + 1; ++i) {
             A2(dudx, i, j) = A2(m->hv_DY_dxT, i, j) *
@@ -519,6 +544,7 @@ static void hor_visc_rows(oracle_model *m, const double *u, const double *v,
                              ((A2(m->IdxCv, i, j) * A3(v, i, j, k)) -
                               (A2(m->IdxCv, i, j - 1) * A3(v, i, j - 1, k)));
         }
+    OMP_FOR
     for (int J = Jsq; J <= Jeq; ++J)
         for (int I = Isq; I <= Ieq; ++I) {
             A2(dvdx, I, J) = A2(m->hv_DY_dxBu, I, J) *
@@ -529,51 +555,65 @@ static void hor_visc_rows(oracle_model *m, const double *u, const double *v,
                               (A3(u, I, J, k) * A2(m->IdxCu, I, J)));
         }
     /* STEP 2 */
+    OMP_FOR
     for (int j = Jsq; j <= Jeq + 1; ++j)
         for (int i = Isq; i <= Ieq + 1; ++i)
             A2(sh_xx, i, j) = A2(dudx, i, j) - A2(dvdy, i, j);
+    OMP_FOR
     for (int J = Jsq; J <= Jeq; ++J)
         for (int I = Isq; I <= Ieq; ++I)
             A2(sh_xy, I, J) = A2(m->mask2dBu, I, J) * (A2(dvdx, I, J) + A2(dudy, I, J));
     /* STEP 3 (use_land_mask) */
+    OMP_FOR
     for (int j = js - 1; j <= je + 1; ++j)
         for (int I = Isq; I <= Ieq; ++I)
             A2(h_u, I, j) = 0.5 * (A2(m->mask2dT, I, j) * A3(h, I, j, k) +
                                    A2(m->mask2dT, I + 1, j) * A3(h, I + 1, j, k));
+    OMP_FOR
     for (int J = Jsq; J <= Jeq; ++J)
         for (int i = is - 1; i <= ie + 1; ++i)
             A2(h_v, i, J) = 0.5 * (A2(m->mask2dT, i, J) * A3(h, i, J, k) +
                                    A2(m->mask2dT, i, J + 1) * A3(h, i, J + 1, k));
+    OMP_FOR
     for (int J = Jsq; J <= Jeq; ++J)
         for (int I = Isq; I <= Ieq; ++I)
             A2(hq, I, J) = 0.25 * ((A3(h, I, J, k) + A3(h, I + 1, J + 1, k)) +
                                    (A3(h, I + 1, J, k) + A3(h, I, J + 1, k)));
     /* STEP 8: Kh at h-points (interior only), floor, str_xx */
+    OMP_FOR
     for (int j = js; j <= je; ++j)
         for (int i = is; i <= ie; ++i) A2(Kh, i, j) = A2(m->hv_Kh_bg_xx, i, j);
+    OMP_FOR
     for (int j = js; j <= je; ++j)
         for (int i = is; i <= ie; ++i) A2(Kh, i, j) = MAX(A2(Kh, i, j), m->hv_Kh_bg_min);
+    OMP_FOR
     for (int j = Jsq; j <= Jeq + 1; ++j)
         for (int i = Isq; i <= Ieq + 1; ++i)
             A2(str_xx, i, j) = -(A2(Kh, i, j) * A2(sh_xx, i, j));
     /* STEP 10 */
+    OMP_FOR
     for (int j = Jsq; j <= Jeq + 1; ++j)
         for (int i = Isq; i <= Ieq + 1; ++i)
             A2(str_xx, i, j) = A2(str_xx, i, j) * (A3(h, i, j, k) * A2(m->hv_red_xx, i, j));
     /* STEP 11: Kh at q-points (overwrites the shared CS%Kh), str_xy */
+    OMP_FOR
     for (int J = Jsq; J <= Jeq; ++J)
         for (int I = Isq; I <= Ieq; ++I) A2(Kh, I, J) = A2(m->hv_Kh_bg_xy, I, J);
+    OMP_FOR
     for (int J = Jsq; J <= Jeq; ++J)
         for (int I = Isq; I <= Ieq; ++I) A2(Kh, I, J) = MAX(A2(Kh, I, J), m->hv_Kh_bg_min);
+    OMP_FOR
     for (int J = Jsq; J <= Jeq; ++J)
         for (int I = Isq; I <= Ieq; ++I)
             A2(str_xy, I, J) = -(A2(Kh, I, J) * A2(sh_xy, I, J));
     /* STEP 13 (free slip) */
+    OMP_FOR
     for (int J = Jsq; J <= Jeq; ++J)
         for (int I = Isq; I <= Ieq; ++I)
             A2(str_xy, I, J) = A2(str_xy, I, J) *
                                (A2(hq, I, J) * A2(m->mask2dBu, I, J) * A2(m->hv_red_xy, I, J));
     /* STEP 14 */
+    OMP_FOR
     for (int j = js; j <= je; ++j)
         for (int I = Isq; I <= Ieq; ++I)
             A3(diffu, I, j, k) =
@@ -583,6 +623,7 @@ static void hor_visc_rows(oracle_model *m, const double *u, const double *v,
                                         (A2(m->hv_dy2h, I + 1, j) * A2(str_xx, I + 1, j)))) *
                  A2(m->IareaCu, I, j)) /
                 (A2(h_u, I, j) + h_neglect);
+    OMP_FOR
     for (int J = Jsq; J <= Jeq; ++J)
         for (int i = is; i <= ie; ++i)
             A3(diffv, i, J, k) =
@@ -615,6 +656,7 @@ void oracle_coriolis(oracle_model *m, const double *u, const double *v,
            *absv = m->co_abs_vort, *q = m->co_q, *Ihq = m->co_Ih_q,
            *hAu = m->co_hArea_u, *hAv = m->co_hArea_v, *KE = m->co_KE;
     for (int k = 1; k <= m->nk; ++k) {
+        OMP_FOR
         for (int j = js - 1; j <= je; ++j)
             for (int i = is - 1; i <= ie; ++i) {
                 A2(dvdx, i, j) = (A3(v, i + 1, j, k) * A2(m->dyCv, i + 1, j)) -
@@ -622,20 +664,24 @@ void oracle_coriolis(oracle_model *m, const double *u, const double *v,
                 A2(dudy, i, j) = (A3(u, i, j + 1, k) * A2(m->dxCu, i, j + 1)) -
                                  (A3(u, i, j, k) * A2(m->dxCu, i, j));
             }
+        OMP_FOR
         for (int j = js - 1; j <= je; ++j)
             for (int i = is; i <= ie + 1; ++i)
                 A2(hAv, i, j) = 0.5 * ((A2(m->areaT, i, j) * A3(h, i, j, k)) +
                                        (A2(m->areaT, i, j + 1) * A3(h, i, j + 1, k)));
+        OMP_FOR
         for (int j = js; j <= je + 1; ++j)
             for (int i = is - 1; i <= ie; ++i)
                 A2(hAu, i, j) = 0.5 * ((A2(m->areaT, i, j) * A3(h, i, j, k)) +
                                        (A2(m->areaT, i + 1, j) * A3(h, i + 1, j, k)));
+        OMP_FOR
         for (int j = js - 1; j <= je; ++j)
             for (int i = is - 1; i <= ie; ++i) {
                 A2(rel, i, j) = A2(m->mask2dBu, i, j) * (A2(dvdx, i, j) - A2(dudy, i, j)) *
                                 A2(m->IareaBu, i, j);
                 A2(absv, i, j) = A2(m->CoriolisBu, i, j) + A2(rel, i, j);
             }
+        OMP_FOR
         for (int j = js - 1; j <= je; ++j)
             for (int i = is - 1; i <= ie; ++i) {
                 double hArea_q = (A2(hAu, i, j) + A2(hAu, i, j + 1)) +
@@ -643,6 +689,7 @@ void oracle_coriolis(oracle_model *m, const double *u, const double *v,
                 A2(Ihq, i, j) = A2(m->co_Area_q, i, j) / (hArea_q + vol_neglect);
                 A2(q, i, j) = A2(absv, i, j) * A2(Ihq, i, j);
             }
+        OMP_FOR
         for (int j = js; j <= je; ++j)
             for (int i = is; i <= ie; ++i) {
                 double u0 = A3(u, i, j, k), um = A3(u, i - 1, j, k);
@@ -652,6 +699,7 @@ void oracle_coriolis(oracle_model *m, const double *u, const double *v,
                                 (A2(m->dxCv, i, j) * (v0 * v0) + A2(m->dxCv, i, j - 1) * (vm * vm))) /
                                A2(m->areaT, i, j);
             }
+        OMP_FOR
         for (int j = js; j <= je; ++j)
             for (int i = is; i <= ie - 1; ++i) {
                 double KEx = (A2(KE, i + 1, j) - A2(KE, i, j)) * A2(m->IdxCu, i, j);
@@ -662,6 +710,7 @@ void oracle_coriolis(oracle_model *m, const double *u, const double *v,
                         A2(m->IdxCu, i, j) -
                     KEx;
             }
+        OMP_FOR
         for (int j = js; j <= je - 1; ++j)
             for (int i = is; i <= ie; ++i) {
                 double KEy = (A2(KE, i, j + 1) - A2(KE, i, j)) * A2(m->IdyCv, i, j);
@@ -753,13 +802,20 @@ static void vv_apply_column(oracle_model *m, double *vel, const double *Ray3,
 void oracle_vert_visc(oracle_model *m, double *u, double *v, const double *h,
                       double dt) {
     int is = m->is, ie = m->ie, js = m->js, je = m->je, nz = m->nk;
+    double h_neglect = m->Angstrom_H;
+    /* columns are independent: with OpenMP each thread has its own column
+     * scratch and takes whole rows */
+#ifdef _OPENMP
+#pragma omp parallel
+#endif
+    {
     double *a = (double *)malloc(sizeof(double) * (nz + 2));
     double *hc = (double *)malloc(sizeof(double) * (nz + 2));
     double *hvel = (double *)malloc(sizeof(double) * (nz + 2));
     double *z_i = (double *)malloc(sizeof(double) * (nz + 2));
     double *c1 = (double *)malloc(sizeof(double) * (nz + 2));
-    double h_neglect = m->Angstrom_H;
     /* vert_visc_coef, u-points then v-points */
+    OMP_COLS
     for (int j = js; j <= je; ++j)
         for (int i = is - 1; i <= ie; ++i) {
             if (A2(m->mask2dCu, i, j) > 0.0) {
@@ -771,6 +827,7 @@ void oracle_vert_visc(oracle_model *m, double *u, double *v, const double *h,
                 for (int K = 1; K <= nz + 1; ++K) A3(m->vv_a_u, i, j, K) = 0.0;
             }
         }
+    OMP_COLS
     for (int j = js - 1; j <= je; ++j)
         for (int i = is; i <= ie; ++i) {
             if (A2(m->mask2dCv, i, j) > 0.0) {
@@ -783,6 +840,7 @@ void oracle_vert_visc(oracle_model *m, double *u, double *v, const double *h,
             }
         }
     /* vert_visc_apply, u-points then v-points */
+    OMP_COLS
     for (int j = js; j <= je; ++j)
         for (int i = is - 1; i <= ie; ++i) {
             if (!(A2(m->mask2dCu, i, j) > 0.0)) continue;
@@ -791,6 +849,7 @@ void oracle_vert_visc(oracle_model *m, double *u, double *v, const double *h,
             vv_apply_column(m, u, m->Ray_u, i, j, dt, A2(m->taux, i, j),
                             A2(m->mask2dCu, i, j), a, hc, c1, &A2(m->vv_taux_bot, i, j));
         }
+    OMP_COLS
     for (int j = js - 1; j <= je; ++j)
         for (int i = is; i <= ie; ++i) {
             if (!(A2(m->mask2dCv, i, j) > 0.0)) continue;
@@ -800,6 +859,7 @@ void oracle_vert_visc(oracle_model *m, double *u, double *v, const double *h,
                             A2(m->mask2dCv, i, j), a, hc, c1, &A2(m->vv_tauy_bot, i, j));
         }
     free(a); free(hc); free(hvel); free(z_i); free(c1);
+    }
 }
 
 /* ------------------------------------------------------------------------ */
@@ -807,6 +867,7 @@ void oracle_vert_visc(oracle_model *m, double *u, double *v, const double *h,
 /* uhbt(is-1,:), uhbt(ie,:), vhbt(:,js-1), vhbt(:,je) are never written.   */
 /* ------------------------------------------------------------------------ */
 static void bt_update_u(oracle_model *m, int is, int ie, int js, int je) {
+    OMP_FOR
     for (int j = js; j <= je; ++j)
         for (int i = is; i <= ie; ++i)
             A2(m->bt_Cor_u, i, j) =
@@ -814,6 +875,7 @@ static void bt_update_u(oracle_model *m, int is, int ie, int js, int je) {
                   (F4(m->bt_f_4_u, 1, i, j) * A2(m->bt_vbt, i, j - 1))) +
                  ((F4(m->bt_f_4_u, 3, i, j) * A2(m->bt_vbt, i, j)) +
                   (F4(m->bt_f_4_u, 2, i, j) * A2(m->bt_vbt, i + 1, j - 1))));
+    OMP_FOR
     for (int j = js; j <= je; ++j)
         for (int i = is; i <= ie; ++i)
             A2(m->bt_ubt, i, j) =
@@ -822,6 +884,7 @@ static void bt_update_u(oracle_model *m, int is, int ie, int js, int je) {
 }
 
 static void bt_update_v(oracle_model *m, int is, int ie, int js, int je) {
+    OMP_FOR
     for (int j = js; j <= je; ++j)
         for (int i = is; i <= ie; ++i)
             A2(m->bt_Cor_v, i, j) =
@@ -829,6 +892,7 @@ static void bt_update_v(oracle_model *m, int is, int ie, int js, int je) {
                          (F4(m->bt_f_4_v, 4, i, j) * A2(m->bt_ubt, i, j + 1))) +
                         ((F4(m->bt_f_4_v, 2, i, j) * A2(m->bt_ubt, i, j)) +
                          (F4(m->bt_f_4_v, 3, i, j) * A2(m->bt_ubt, i - 1, j + 1))));
+    OMP_FOR
     for (int j = js; j <= je; ++j)
         for (int i = is; i <= ie; ++i)
             A2(m->bt_vbt, i, j) =
@@ -844,6 +908,7 @@ void oracle_btstep(oracle_model *m, const double *eta_in, const double *ubt_in,
     double trans_wt2 = -m->bt_bebt;
     double inv_nstep = 1.0 / (double)m->nstep;
     double dtbt = m->bt_dtbt;
+    OMP_FOR
     for (int j = m->jsd; j <= m->jed; ++j)
         for (int i = m->isd; i <= m->ied; ++i) {
             A2(m->bt_eta, i, j) = A2(eta_in, i, j);
@@ -853,12 +918,15 @@ void oracle_btstep(oracle_model *m, const double *eta_in, const double *ubt_in,
             A2(m->bt_vbt_av, i, j) = 0.0;
         }
     for (int n = 1; n <= m->nstep; ++n) {
+        OMP_FOR
         for (int j = js; j <= je; ++j)
             for (int i = is - 1; i <= ie + 1; ++i)
                 A2(m->bt_ubt_prev, i, j) = A2(m->bt_ubt, i, j);
+        OMP_FOR
         for (int j = js - 1; j <= je + 1; ++j)
             for (int i = is; i <= ie; ++i)
                 A2(m->bt_vbt_prev, i, j) = A2(m->bt_vbt, i, j);
+        OMP_FOR
         for (int j = js; j <= je; ++j)
             for (int i = is; i <= ie; ++i)
                 A2(m->bt_eta_pred, i, j) =
@@ -868,12 +936,14 @@ void oracle_btstep(oracle_model *m, const double *eta_in, const double *ubt_in,
                           (A2(m->bt_Datu, i, j) * A2(m->bt_ubt, i, j))) +
                          ((A2(m->bt_Datv, i, j - 1) * A2(m->bt_vbt, i, j - 1)) -
                           (A2(m->bt_Datv, i, j) * A2(m->bt_vbt, i, j))));
+        OMP_FOR
         for (int j = js; j <= je; ++j)
             for (int i = is; i <= ie - 1; ++i)
                 A2(m->bt_PFu, i, j) =
                     ((A2(m->bt_eta_pred, i, j) * A2(m->bt_gtot_E, i, j)) -
                      (A2(m->bt_eta_pred, i + 1, j) * A2(m->bt_gtot_W, i + 1, j))) *
                     m->bt_dgeo_de * A2(m->IdxCu, i, j);
+        OMP_FOR
         for (int j = js; j <= je - 1; ++j)
             for (int i = is; i <= ie; ++i)
                 A2(m->bt_PFv, i, j) =
@@ -892,16 +962,19 @@ void oracle_btstep(oracle_model *m, const double *eta_in, const double *ubt_in,
          * of btstep_do_step and the CUDA C kernels (:443-452) */
         const int iu0 = m->bt_extended ? is - 1 : is, iu1 = m->bt_extended ? ie : ie - 1;
         const int jv0 = m->bt_extended ? js - 1 : js, jv1 = m->bt_extended ? je : je - 1;
+        OMP_FOR
         for (int j = js; j <= je; ++j)
             for (int i = iu0; i <= iu1; ++i)
                 A2(m->bt_uhbt, i, j) =
                     A2(m->bt_Datu, i, j) *
                     (trans_wt1 * A2(m->bt_ubt, i, j) + trans_wt2 * A2(m->bt_ubt_prev, i, j));
+        OMP_FOR
         for (int j = jv0; j <= jv1; ++j)
             for (int i = is; i <= ie; ++i)
                 A2(m->bt_vhbt, i, j) =
                     A2(m->bt_Datv, i, j) *
                     (trans_wt1 * A2(m->bt_vbt, i, j) + trans_wt2 * A2(m->bt_vbt_prev, i, j));
+        OMP_FOR
         for (int j = js; j <= je; ++j)
             for (int i = is; i <= ie; ++i)
                 A2(m->bt_eta, i, j) =
@@ -909,13 +982,16 @@ void oracle_btstep(oracle_model *m, const double *eta_in, const double *ubt_in,
                     dtbt * A2(m->IareaT, i, j) *
                         ((A2(m->bt_uhbt, i, j) - A2(m->bt_uhbt, i - 1, j)) +
                          (A2(m->bt_vhbt, i, j) - A2(m->bt_vhbt, i, j - 1)));
+        OMP_FOR
         for (int j = js; j <= je; ++j)
             for (int i = iu0; i <= iu1; ++i)
                 A2(m->bt_ubt_av, i, j) = A2(m->bt_ubt_av, i, j) + A2(m->bt_ubt, i, j) * inv_nstep;
+        OMP_FOR
         for (int j = jv0; j <= jv1; ++j)
             for (int i = is; i <= ie; ++i)
                 A2(m->bt_vbt_av, i, j) = A2(m->bt_vbt_av, i, j) + A2(m->bt_vbt, i, j) * inv_nstep;
     }
+    OMP_FOR
     for (int j = m->jsd; j <= m->jed; ++j)
         for (int i = m->isd; i <= m->ied; ++i) {
             A2(u_av, i, j) = A2(m->bt_ubt_av, i, j);
@@ -1352,10 +1428,13 @@ static void flux_thickness(oracle_model *m, const double *u, const double *h,
 
 void oracle_continuity(oracle_model *m, const double *u, const double *hin,
                        double *h, double *uh, double dt) {
+    OMP_FOR
     for (int k = 1; k <= m->nk; ++k) ppm_layer(m, hin, m->hW, m->hE, k);
+    OMP_FOR
     for (int j = m->js; j <= m->je; ++j) mass_flux_row(m, u, hin, uh, dt, j);
     flux_thickness(m, m->u_cor, hin, dt);
     /* continuity_zonal_convergence with hin, h_min = 0, :148-176 */
+    OMP_FOR
     for (int k = 1; k <= m->nk; ++k)
         for (int j = m->js; j <= m->je; ++j)
             for (int i = m->is; i <= m->ie; ++i)
@@ -1370,10 +1449,12 @@ void oracle_continuity(oracle_model *m, const double *u, const double *hin,
 static void vel_update(oracle_model *m, const double *ubase, const double *vbase,
                        double *uout, double *vout, double coef) {
     for (int k = 1; k <= m->nk; ++k) {
+        OMP_FOR
         for (int j = m->js; j <= m->je; ++j)
             for (int i = m->is; i <= m->ie - 1; ++i)
                 A3(uout, i, j, k) = A3(ubase, i, j, k) +
                                     coef * (A3(m->CAu, i, j, k) + A3(m->diffu, i, j, k));
+        OMP_FOR
         for (int j = m->js; j <= m->je - 1; ++j)
             for (int i = m->is; i <= m->ie; ++i)
                 A3(vout, i, j, k) = A3(vbase, i, j, k) +

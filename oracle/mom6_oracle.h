@@ -107,6 +107,10 @@ void oracle_continuity(oracle_model *m, const double *u, const double *hin,
 void oracle_halo_fill(const oracle_model *m, double *f, int nz, int kind);
 
 /* Philox4x32-10 normal deviate used by the CFG initial state. */
+/* Threads of the row-parallel loops in the OpenMP build (liboracle_omp.so);
+ * n <= 0 keeps the runtime's choice.  Returns the threads in use (1 in the
+ * single-threaded build). */
+int oracle_set_threads(int n);
 double oracle_normal(uint64_t seed, uint32_t stream, uint64_t index);
 
 #ifdef __cplusplus

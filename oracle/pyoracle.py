@@ -10,7 +10,7 @@ import subprocess
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_LIB = None
+_LIBS = {}
 
 INIT_REF, INIT_CFG = 0, 1
 
@@ -41,10 +41,11 @@ def build():
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
 
 
-def lib():
-    global _LIB
-    if _LIB is None:
-        path = os.path.join(_HERE, "liboracle.so")
+def lib(parallel=False):
+    """The single-threaded oracle, or (parallel=True) the same source built with
+    its row-parallel loops on OpenMP threads; the two give identical results."""
+    if parallel not in _LIBS:
+        path = os.path.join(_HERE, "liboracle_omp.so" if parallel else "liboracle.so")
         if not os.path.exists(path):
             build()
         L = ctypes.CDLL(path)
@@ -75,8 +76,10 @@ def lib():
         L.oracle_set_bt_extended.argtypes = [vp, ctypes.c_int]
         L.oracle_array.argtypes = [vp, ctypes.c_char_p, P(d), ctypes.c_size_t]
         L.oracle_array.restype = ctypes.c_int
-        _LIB = L
-    return _LIB
+        L.oracle_set_threads.argtypes = [ctypes.c_int]
+        L.oracle_set_threads.restype = ctypes.c_int
+        _LIBS[parallel] = L
+    return _LIBS[parallel]
 
 
 def _ptr(a):
@@ -88,8 +91,12 @@ class Oracle:
     """One oracle model (grid + state + persistent module work arrays)."""
 
     def __init__(self, ni, nj, nk, bt_nsteps, init_mode=INIT_CFG, seed=0,
-                 dt=None, Kh=None, bc_fill=None):
-        L = lib()
+                 dt=None, Kh=None, bc_fill=None, threads=None):
+        """threads: None for the single-threaded build, else the OpenMP build
+        on that many threads (0: all the runtime offers)."""
+        L = lib(parallel=threads is not None)
+        self._L = L
+        self.threads = 1 if threads is None else L.oracle_set_threads(int(threads))
         c = Config()
         L.oracle_config_default(ctypes.byref(c), init_mode)
         c.ni, c.nj, c.nk, c.bt_nsteps, c.seed = ni, nj, nk, bt_nsteps, seed
@@ -109,7 +116,7 @@ class Oracle:
 
     def close(self):
         if self._m:
-            lib().oracle_destroy(self._m)
+            self._L.oracle_destroy(self._m)
             self._m = None
 
     def __del__(self):
@@ -126,22 +133,22 @@ class Oracle:
 
     def get(self, name):
         a = self.empty(name)
-        if lib().oracle_get(self._m, FID[name], _ptr(a)) != 0:
+        if self._L.oracle_get(self._m, FID[name], _ptr(a)) != 0:
             raise KeyError(name)
         return a
 
     def set(self, name, a):
         a = np.asfortranarray(a, dtype=np.float64)
         assert a.shape == self.shape(name)
-        if lib().oracle_set(self._m, FID[name], _ptr(a)) != 0:
+        if self._L.oracle_set(self._m, FID[name], _ptr(a)) != 0:
             raise KeyError(name)
 
     def step(self, n=1):
-        lib().oracle_step(self._m, int(n))
+        self._L.oracle_step(self._m, int(n))
 
     def verify(self):
         out = (ctypes.c_double * 7)()
-        lib().oracle_verify(self._m, out)
+        self._L.oracle_verify(self._m, out)
         keys = ["mass_init", "mass_final", "rel_error", "max_u", "max_v",
                 "max_eta", "ke_total"]
         return dict(zip(keys, list(out)))
@@ -150,35 +157,35 @@ class Oracle:
     def continuity(self, u, hin, dt):
         h = self.get("h")
         uh = self.get("uh")
-        lib().oracle_continuity(self._m, _ptr(u), _ptr(hin), _ptr(h), _ptr(uh), dt)
+        self._L.oracle_continuity(self._m, _ptr(u), _ptr(hin), _ptr(h), _ptr(uh), dt)
         return h, uh
 
     def vert_visc(self, u, v, h, dt):
         u = u.copy(order="F")
         v = v.copy(order="F")
-        lib().oracle_vert_visc(self._m, _ptr(u), _ptr(v), _ptr(h), dt)
+        self._L.oracle_vert_visc(self._m, _ptr(u), _ptr(v), _ptr(h), dt)
         return u, v
 
     def btstep(self, eta, ubt, vbt):
         ua, va, ea = self.empty("ubt"), self.empty("vbt"), self.empty("eta")
-        lib().oracle_btstep(self._m, _ptr(eta), _ptr(ubt), _ptr(vbt), _ptr(ua),
+        self._L.oracle_btstep(self._m, _ptr(eta), _ptr(ubt), _ptr(vbt), _ptr(ua),
                             _ptr(va), _ptr(ea))
         return ua, va, ea
 
     def hor_visc(self, u, v, h):
         du, dv = self.empty("u"), self.empty("v")
-        lib().oracle_hor_visc(self._m, _ptr(u), _ptr(v), _ptr(h), _ptr(du), _ptr(dv))
+        self._L.oracle_hor_visc(self._m, _ptr(u), _ptr(v), _ptr(h), _ptr(du), _ptr(dv))
         return du, dv
 
     def coriolis(self, u, v, h, uh, vh):
         cu, cv = self.empty("u"), self.empty("v")
-        lib().oracle_coriolis(self._m, _ptr(u), _ptr(v), _ptr(h), _ptr(uh),
+        self._L.oracle_coriolis(self._m, _ptr(u), _ptr(v), _ptr(h), _ptr(uh),
                               _ptr(vh), _ptr(cu), _ptr(cv))
         return cu, cv
 
     def transports(self, u, v, h):
         uh, vh = self.empty("u"), self.empty("v")
-        lib().oracle_compute_transports(self._m, _ptr(u), _ptr(v), _ptr(h),
+        self._L.oracle_compute_transports(self._m, _ptr(u), _ptr(v), _ptr(h),
                                         _ptr(uh), _ptr(vh))
         return uh, vh
 
@@ -187,16 +194,16 @@ class Oracle:
         n1, n2 = self.shape("eta")
         four = name in ("f_4_u", "f_4_v")
         out = np.zeros((4, n1, n2) if four else (n1, n2), order="F")
-        rc = lib().oracle_array(self._m, name.encode(), _ptr(out), out.size)
+        rc = self._L.oracle_array(self._m, name.encode(), _ptr(out), out.size)
         if rc != 0:
             raise KeyError(name)
         return out
 
     def set_bt_extended(self, on):
-        lib().oracle_set_bt_extended(self._m, 1 if on else 0)
+        self._L.oracle_set_bt_extended(self._m, 1 if on else 0)
 
     def halo_fill(self, f, kind):
         f = np.asfortranarray(f.copy())
         nz = f.shape[2] if f.ndim == 3 else 1
-        lib().oracle_halo_fill(self._m, _ptr(f), nz, kind)
+        self._L.oracle_halo_fill(self._m, _ptr(f), nz, kind)
         return f
