@@ -86,6 +86,62 @@ __device__ __forceinline__ void ppm_cell(const double* __restrict__ hrow,
     }
 }
 
+// The PPM slope of a cell from h of its two neighbours (ppm_slope's
+// operations; ok = the product of the three masks is nonzero).
+__device__ __forceinline__ double ppm_slope3(double hm, double hc, double hp, bool ok)
+{
+    if (!ok) return 0.0;
+    const double s = 0.5 * (hp - hm);
+    const double dMx = dmax(dmax(hp, hm), hc) - hc;
+    const double dMn = hc - dmin(dmin(hp, hm), hc);
+    return copysign(1.0, s) * dmin(fabs(s), 2.0 * dmin(dMx, dMn));
+}
+
+// Edge values of a cell from h of the cell and its neighbours, their masks
+// (ml, mr; oml = 1 - ml, omr = 1 - mr) and the slopes of cells i-1, i, i+1:
+// the rest of PPM_reconstruction_x and PPM_limit_pos (ppm_cell's operations).
+__device__ __forceinline__ void ppm_edges_limited(double hm1, double hc, double hp1, double ml,
+                                                  double oml, double mr, double omr, double slm,
+                                                  double slc, double slp, double h_min,
+                                                  double& hL, double& hR)
+{
+    const double oneSixth = 1.0 / 6.0;
+    const double h_im1 = ml * hm1 + oml * hc;
+    const double h_ip1 = mr * hp1 + omr * hc;
+    hL = 0.5 * (h_im1 + hc) + oneSixth * (slm - slc);
+    hR = 0.5 * (h_ip1 + hc) + oneSixth * (slc - slp);
+    float curv = (float)(3.0 * ((hL + hR) - 2.0 * hc));
+    if ((double)curv > 0.0) {
+        float dh = (float)(hR - hL);
+        if (fabsf(dh) < curv) {
+            if (hc <= h_min) {
+                hL = hc; hR = hc;
+            } else {
+                float c12 = __fmul_rn(12.0f, curv);
+                float den = __fadd_rn(__fmul_rn(curv, curv), __fmul_rn(3.0f, __fmul_rn(dh, dh)));
+                double lhs = (double)c12 * (hc - h_min);
+                if (lhs < (double)den) {
+                    float scale = (float)(lhs / (double)den);
+                    hL = hc + (double)scale * (hL - hc);
+                    hR = hc + (double)scale * (hR - hc);
+                }
+            }
+        }
+    }
+}
+
+// PPM_reconstruction_x + PPM_limit_pos for one cell from its 5-cell stencil
+// (h[0..4] = cells i-2..i+2, m[0..4] their masks); same operations as ppm_cell.
+__device__ __forceinline__ void ppm_stencil(const double* h, const double* m, double h_min,
+                                            double& hL, double& hR)
+{
+    const double slm = ppm_slope3(h[0], h[1], h[2], (m[0] * m[1] * m[2]) != 0.0);
+    const double slc = ppm_slope3(h[1], h[2], h[3], (m[1] * m[2] * m[3]) != 0.0);
+    const double slp = ppm_slope3(h[2], h[3], h[4], (m[2] * m[3] * m[4]) != 0.0);
+    ppm_edges_limited(h[1], h[2], h[3], m[1], 1.0 - m[1], m[3], 1.0 - m[3], slm, slc, slp,
+                      h_min, hL, hR);
+}
+
 __global__ void __launch_bounds__(128)
 k_ppm_edges(Dims D, Metrics M, const double* __restrict__ hin,
             double* __restrict__ hW, double* __restrict__ hE, double h_min)
@@ -99,6 +155,61 @@ k_ppm_edges(Dims D, Metrics M, const double* __restrict__ hin,
     ppm_cell(hin + rowoff, M.mask2dT + (size_t)(j - 1) * D.n1, i, h_min, hL, hR);
     hW[rowoff + (i - 1)] = hL;
     hE[rowoff + (i - 1)] = hR;
+}
+
+// The same edges with each cell's slope formed once: lane l of a warp takes
+// cell c = is - 2 + 30 w + l (w = the warp's index along the row), forms the
+// slope of c, takes the slopes of c - 1 and c + 1 from lanes l - 1 and l + 1,
+// and lanes 1..30 write the edges of their cells.  The masks are read once
+// and each thread walks kEdgeLayers layers.
+constexpr int kEdgeCellsPerWarp = 30;
+constexpr int kEdgeLayers = 5;
+
+__global__ void __launch_bounds__(128)
+k_ppm_edges_warp(Dims D, Metrics M, const double* __restrict__ hin,
+                 double* __restrict__ hW, double* __restrict__ hE, double h_min)
+{
+    const unsigned FULL = 0xffffffffu;
+    const int lane = (int)threadIdx.x & 31;
+    const int wrow = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int c = D.is - 2 + kEdgeCellsPerWarp * wrow + lane;
+    const int j = D.js + (int)blockIdx.y;
+    const int k0 = 1 + (int)blockIdx.z * kEdgeLayers;
+    const bool load_ok = c <= D.ie + 2;
+    const bool write_ok = lane >= 1 && lane <= kEdgeCellsPerWarp && c <= D.ie + 1;
+    const size_t r = (size_t)(j - 1) * D.n1 + (size_t)(c - 1);
+    const double* mrow = M.mask2dT + r;
+    const double m0 = load_ok ? mrow[-1] : 0.0;
+    const double m1 = load_ok ? mrow[0] : 0.0;
+    const double m2 = load_ok ? mrow[1] : 0.0;
+    const bool slope_ok = (m0 * m1 * m2) != 0.0;
+    const double om0 = 1.0 - m0, om2 = 1.0 - m2;
+    const int kn = min(kEdgeLayers, D.nk - k0 + 1);   // uniform over the CTA
+    const double* hp0 = hin + (size_t)(k0 - 1) * D.plane + r;
+    double hm[kEdgeLayers], hc[kEdgeLayers], hp[kEdgeLayers];
+#pragma unroll
+    for (int q = 0; q < kEdgeLayers; ++q) {
+        const double* p = hp0 + (size_t)q * D.plane;
+        const bool ok = load_ok && q < kn;
+        hm[q] = ok ? p[-1] : 0.0;
+        hc[q] = ok ? p[0] : 0.0;
+        hp[q] = ok ? p[1] : 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < kEdgeLayers; ++q) {
+        if (q < kn) {
+            const double slc = ppm_slope3(hm[q], hc[q], hp[q], slope_ok);
+            const double slm = __shfl_up_sync(FULL, slc, 1);
+            const double slp = __shfl_down_sync(FULL, slc, 1);
+            double hL, hR;
+            ppm_edges_limited(hm[q], hc[q], hp[q], m0, om0, m2, om2, slm, slc, slp, h_min, hL, hR);
+            if (write_ok) {
+                const size_t o = (size_t)(k0 - 1 + q) * D.plane + r;
+                hW[o] = hL;
+                hE[o] = hR;
+            }
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -589,46 +700,6 @@ __device__ __forceinline__ void named_bar_arrive(int id, int count)
     asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
 
-// PPM_reconstruction_x + PPM_limit_pos for one cell from its 5-cell stencil
-// (h[0..4] = cells i-2..i+2, m[0..4] their masks); same operations as ppm_cell.
-__device__ __forceinline__ void ppm_stencil(const double* h, const double* m, double h_min,
-                                            double& hL, double& hR)
-{
-    auto slope = [&](int c) -> double {   // slope of cell c (1..3 here)
-        if ((m[c - 1] * m[c] * m[c + 1]) == 0.0) return 0.0;
-        const double hp = h[c + 1], hm = h[c - 1], hc = h[c];
-        const double s = 0.5 * (hp - hm);
-        const double dMx = dmax(dmax(hp, hm), hc) - hc;
-        const double dMn = hc - dmin(dmin(hp, hm), hc);
-        return copysign(1.0, s) * dmin(fabs(s), 2.0 * dmin(dMx, dMn));
-    };
-    const double oneSixth = 1.0 / 6.0;
-    const double slm = slope(1), slc = slope(2), slp = slope(3);
-    const double hc = h[2];
-    const double h_im1 = m[1] * h[1] + (1.0 - m[1]) * hc;
-    const double h_ip1 = m[3] * h[3] + (1.0 - m[3]) * hc;
-    hL = 0.5 * (h_im1 + hc) + oneSixth * (slm - slc);
-    hR = 0.5 * (h_ip1 + hc) + oneSixth * (slc - slp);
-    float curv = (float)(3.0 * ((hL + hR) - 2.0 * hc));
-    if ((double)curv > 0.0) {
-        float dh = (float)(hR - hL);
-        if (fabsf(dh) < curv) {
-            if (hc <= h_min) {
-                hL = hc; hR = hc;
-            } else {
-                float c12 = __fmul_rn(12.0f, curv);
-                float den = __fadd_rn(__fmul_rn(curv, curv), __fmul_rn(3.0f, __fmul_rn(dh, dh)));
-                double lhs = (double)c12 * (hc - h_min);
-                if (lhs < (double)den) {
-                    float scale = (float)(lhs / (double)den);
-                    hL = hc + (double)scale * (hL - hc);
-                    hR = hc + (double)scale * (hR - hc);
-                }
-            }
-        }
-    }
-}
-
 template <int LMAX>
 __global__ void __launch_bounds__(32 * kTileWarps, 2)
 k_cont_tile(Dims D, Metrics M, const double* __restrict__ u, const double* __restrict__ hin,
@@ -1004,9 +1075,20 @@ cudaError_t launch_continuity(const Dims& D, const Metrics& M, const double* u,
         }
     }
     {
+        static int edges_warp = -1;
+        if (edges_warp < 0) {
+            const char* e = getenv("MOM6B_PPM_WARP");
+            edges_warp = e ? atoi(e) : 1;
+        }
         int n = (D.ie + 1) - (D.is - 1) + 1;
-        dim3 grid((n + 127) / 128, D.je - D.js + 1, D.nk);
-        k_ppm_edges<<<grid, 128, 0, s>>>(D, M, hin, hW, hE, h_min);
+        if (edges_warp) {
+            const int warps = (n + kEdgeCellsPerWarp - 1) / kEdgeCellsPerWarp;
+            dim3 grid((warps + 3) / 4, D.je - D.js + 1, (D.nk + kEdgeLayers - 1) / kEdgeLayers);
+            k_ppm_edges_warp<<<grid, 128, 0, s>>>(D, M, hin, hW, hE, h_min);
+        } else {
+            dim3 grid((n + 127) / 128, D.je - D.js + 1, D.nk);
+            k_ppm_edges<<<grid, 128, 0, s>>>(D, M, hin, hW, hE, h_min);
+        }
     }
     {
         // Residency: each face re-reads its column on every Newton pass, so
