@@ -42,6 +42,15 @@ k_ppm_edges_f(Dims D, Metrics M, const float* __restrict__ hin, float* __restric
     ppm_cell_f(D, M, hin, hW, hE, h_min, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z);
 }
 
+__global__ void __launch_bounds__(128)
+k_ppm_edges_warp_f(Dims D, Metrics M, const float* __restrict__ hin, float* __restrict__ hW,
+                   float* __restrict__ hE, float h_min)
+{
+    ppm_cells_warp_f(D, M, hin, hW, hE, h_min,
+                     (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5),
+                     D.js + (int)blockIdx.y, 1 + (int)blockIdx.z * kEdgeLayersF);
+}
+
 template <int MINB>
 __global__ void __launch_bounds__(128, MINB)
 k_cont_faces_f(Dims D, Metrics M, const float* __restrict__ u, const float* __restrict__ hin,
@@ -58,9 +67,20 @@ cudaError_t launch_continuity_f(const Dims& D, const Metrics& M, const float* u,
                                 double* uh_ovl, double dt, double h_min, cudaStream_t s)
 {
     {
+        static int edges_warp = -1;
+        if (edges_warp < 0) {
+            const char* e = getenv("MOM6B_PPM_WARP");
+            edges_warp = e ? atoi(e) : 1;
+        }
         int n = (D.ie + 1) - (D.is - 1) + 1;
-        dim3 grid((n + 127) / 128, D.je - D.js + 1, D.nk);
-        k_ppm_edges_f<<<grid, 128, 0, s>>>(D, M, hin, hW, hE, (float)h_min);
+        if (edges_warp) {
+            const int warps = (n + kEdgeCellsPerWarpF - 1) / kEdgeCellsPerWarpF;
+            dim3 grid((warps + 3) / 4, D.je - D.js + 1, (D.nk + kEdgeLayersF - 1) / kEdgeLayersF);
+            k_ppm_edges_warp_f<<<grid, 128, 0, s>>>(D, M, hin, hW, hE, (float)h_min);
+        } else {
+            dim3 grid((n + 127) / 128, D.je - D.js + 1, D.nk);
+            k_ppm_edges_f<<<grid, 128, 0, s>>>(D, M, hin, hW, hE, (float)h_min);
+        }
     }
     ContOutF O{h, uh, h_u, O2.FA_u_W0, O2.FA_u_WW, O2.FA_u_E0, O2.FA_u_EE, O2.uBT_WW,
                O2.uBT_EE, O2.du_cor};

@@ -24,14 +24,42 @@ namespace mom6b {
 constexpr double kMixedTolEta = 1.0e-6;
 constexpr double kMixedRelStep = 1.0e-6;
 
-__device__ __forceinline__ float ppm_slope_f(const float* h, const float* m, int c)
+// The FP32 PPM slope of a cell from h of its neighbours (ok = the product of
+// the three masks is nonzero).
+__device__ __forceinline__ float ppm_slope3_f(float hm, float hc, float hp, bool ok)
 {
-    if ((m[c - 1] * m[c] * m[c + 1]) == 0.0f) return 0.0f;
-    const float hp = h[c + 1], hm = h[c - 1], hc = h[c];
+    if (!ok) return 0.0f;
     const float s = 0.5f * (hp - hm);
     const float dMx = fmaxf(fmaxf(hp, hm), hc) - hc;
     const float dMn = hc - fminf(fminf(hp, hm), hc);
     return copysignf(1.0f, s) * fminf(fabsf(s), 2.0f * fminf(dMx, dMn));
+}
+
+// FP32 edge values of a cell from h of the cell and its neighbours, their
+// masks and the slopes of cells i-1, i, i+1 (PPM_reconstruction_x and
+// PPM_limit_pos).
+__device__ __forceinline__ void ppm_edges_f(float hm1, float hc, float hp1, float ml, float mr,
+                                            float slm, float slc, float slp, float h_min,
+                                            float& hL, float& hR)
+{
+    const float oneSixth = 1.0f / 6.0f;
+    const float h_im1 = ml * hm1 + (1.0f - ml) * hc;
+    const float h_ip1 = mr * hp1 + (1.0f - mr) * hc;
+    hL = 0.5f * (h_im1 + hc) + oneSixth * (slm - slc);
+    hR = 0.5f * (h_ip1 + hc) + oneSixth * (slc - slp);
+    const float curv = 3.0f * ((hL + hR) - 2.0f * hc);
+    if (curv > 0.0f) {
+        const float dh = hR - hL;
+        if (fabsf(dh) < curv) {
+            if (hc <= h_min) {
+                hL = hc; hR = hc;
+            } else if (12.0f * curv * (hc - h_min) < curv * curv + 3.0f * dh * dh) {
+                const float scale = 12.0f * curv * (hc - h_min) / (curv * curv + 3.0f * dh * dh);
+                hL = hc + scale * (hL - hc);
+                hR = hc + scale * (hR - hc);
+            }
+        }
+    }
 }
 
 // PPM_reconstruction_x + PPM_limit_pos in FP32 for one cell of a row: cell
@@ -52,28 +80,63 @@ __device__ __forceinline__ void ppm_cell_f(const Dims& D, const Metrics& M,
         h[c] = hin[row + (i - 3 + c)];
         m[c] = (float)M.mask2dT[(size_t)(j - 1) * D.n1 + (i - 3 + c)];
     }
-    const float oneSixth = 1.0f / 6.0f;
-    const float slm = ppm_slope_f(h, m, 1), slc = ppm_slope_f(h, m, 2), slp = ppm_slope_f(h, m, 3);
-    const float hc = h[2];
-    const float h_im1 = m[1] * h[1] + (1.0f - m[1]) * hc;
-    const float h_ip1 = m[3] * h[3] + (1.0f - m[3]) * hc;
-    float hL = 0.5f * (h_im1 + hc) + oneSixth * (slm - slc);
-    float hR = 0.5f * (h_ip1 + hc) + oneSixth * (slc - slp);
-    const float curv = 3.0f * ((hL + hR) - 2.0f * hc);
-    if (curv > 0.0f) {
-        const float dh = hR - hL;
-        if (fabsf(dh) < curv) {
-            if (hc <= h_min) {
-                hL = hc; hR = hc;
-            } else if (12.0f * curv * (hc - h_min) < curv * curv + 3.0f * dh * dh) {
-                const float scale = 12.0f * curv * (hc - h_min) / (curv * curv + 3.0f * dh * dh);
-                hL = hc + scale * (hL - hc);
-                hR = hc + scale * (hR - hc);
+    const float slm = ppm_slope3_f(h[0], h[1], h[2], (m[0] * m[1] * m[2]) != 0.0f);
+    const float slc = ppm_slope3_f(h[1], h[2], h[3], (m[1] * m[2] * m[3]) != 0.0f);
+    const float slp = ppm_slope3_f(h[2], h[3], h[4], (m[2] * m[3] * m[4]) != 0.0f);
+    float hL, hR;
+    ppm_edges_f(h[1], h[2], h[3], m[1], m[3], slm, slc, slp, h_min, hL, hR);
+    hW[row + (i - 1)] = hL;
+    hE[row + (i - 1)] = hR;
+}
+
+// The same edges with each cell's slope formed once (the warp layout of the
+// FP64 k_ppm_edges_warp): lane l takes cell c = is - 2 + 30 w + l, lanes
+// 1..30 write their cells' edges, kEdgeLayersF layers per thread.
+constexpr int kEdgeCellsPerWarpF = 30;
+constexpr int kEdgeLayersF = 5;
+
+__device__ __forceinline__ void ppm_cells_warp_f(const Dims& D, const Metrics& M,
+                                                 const float* __restrict__ hin,
+                                                 float* __restrict__ hW, float* __restrict__ hE,
+                                                 float h_min, int wrow, int j, int k0)
+{
+    const unsigned FULL = 0xffffffffu;
+    const int lane = (int)threadIdx.x & 31;
+    const int c = D.is - 2 + kEdgeCellsPerWarpF * wrow + lane;
+    const bool load_ok = c <= D.ie + 2;
+    const bool write_ok = lane >= 1 && lane <= kEdgeCellsPerWarpF && c <= D.ie + 1;
+    const size_t r = (size_t)(j - 1) * D.n1 + (size_t)(c - 1);
+    const double* mrow = M.mask2dT + r;
+    const float m0 = load_ok ? (float)mrow[-1] : 0.0f;
+    const float m1 = load_ok ? (float)mrow[0] : 0.0f;
+    const float m2 = load_ok ? (float)mrow[1] : 0.0f;
+    const bool slope_ok = (m0 * m1 * m2) != 0.0f;
+    const int kn = min(kEdgeLayersF, D.nk - k0 + 1);
+    const float* hp0 = hin + (size_t)(k0 - 1) * D.plane + r;
+    float hm[kEdgeLayersF], hc[kEdgeLayersF], hp[kEdgeLayersF];
+#pragma unroll
+    for (int q = 0; q < kEdgeLayersF; ++q) {
+        const float* p = hp0 + (size_t)q * D.plane;
+        const bool ok = load_ok && q < kn;
+        hm[q] = ok ? p[-1] : 0.0f;
+        hc[q] = ok ? p[0] : 0.0f;
+        hp[q] = ok ? p[1] : 0.0f;
+    }
+#pragma unroll
+    for (int q = 0; q < kEdgeLayersF; ++q) {
+        if (q < kn) {
+            const float slc = ppm_slope3_f(hm[q], hc[q], hp[q], slope_ok);
+            const float slm = __shfl_up_sync(FULL, slc, 1);
+            const float slp = __shfl_down_sync(FULL, slc, 1);
+            float hL, hR;
+            ppm_edges_f(hm[q], hc[q], hp[q], m0, m2, slm, slc, slp, h_min, hL, hR);
+            if (write_ok) {
+                const size_t o = (size_t)(k0 - 1 + q) * D.plane + r;
+                hW[o] = hL;
+                hE[o] = hR;
             }
         }
     }
-    hW[row + (i - 1)] = hL;
-    hE[row + (i - 1)] = hR;
 }
 
 struct LayerF {
