@@ -24,6 +24,8 @@
 // vs :162-168).
 #pragma once
 
+#include <cstdlib>
+
 #include "kernels.h"
 
 namespace mom6b {
@@ -32,6 +34,31 @@ namespace mom6b {
 // per row); otherwise every metric is read from its 2-D array.  The CTA with
 // block coordinates (bx, by, bz) owns the tile i0 = is + bx TX, j0 = js + by TY
 // and walks the KC consecutive layers from k0 + bz KC.
+// One element global -> shared with cp.async (bypasses registers); ok = false
+// writes zero (src-size 0) and reads nothing.
+template <typename R>
+__device__ __forceinline__ void cp_async_elem(R* sdst, const R* gsrc, bool ok)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    if constexpr (sizeof(R) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gsrc),
+                     "r"(ok ? 8 : 0)
+                     : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(gsrc),
+                     "r"(ok ? 4 : 0)
+                     : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// UNI selects the uniform-metric instantiation (metrics as scalars, Coriolis
+// per row); otherwise every metric is read from its 2-D array.  The CTA with
+// block coordinates (bx, by, bz) owns the tile i0 = is + bx TX, j0 = js + by TY
+// and walks the KC consecutive layers from k0 + bz KC.  The u, v, h tiles are
+// double-buffered: layer k+1 is copied into shared memory (cp.async) while
+// layer k is evaluated, so the loads' latency leaves the layer loop and each
+// layer takes two barriers.
 template <int TX, int TY, bool UNI, typename R>
 __device__ __forceinline__ void
 tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __restrict__ uin,
@@ -41,7 +68,9 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
 {
     constexpr int SX = TX + 2, SY = TY + 2;  // staged inputs: [i0-1, i0+TX] x [j0-1, j0+TY]
     constexpr int CX = TX + 1, CY = TY + 1;  // intermediates
-    __shared__ R s_u[SY][SX], s_v[SY][SX], s_h[SY][SX];
+    constexpr int NT = TX * TY;
+    constexpr int NS = (SX * SY + NT - 1) / NT;  // staged elements per thread
+    __shared__ R s_u[2][SY][SX], s_v[2][SY][SX], s_h[2][SY][SX];
     __shared__ R s_q[CY][CX], s_sxy[CY][CX];   // corners  [i0-1, i0+TX-1] x [j0-1, j0+TY-1]
     __shared__ R s_ke[CY][CX], s_sxx[CY][CX];  // centres  [i0, i0+TX] x [j0, j0+TY]
     __shared__ R s_uh[CY][CX];                 // u-faces  [i0-1, i0+TX-1] x [j0, j0+TY]
@@ -52,26 +81,55 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
     const int tid = (int)threadIdx.y * TX + (int)threadIdx.x;
     const int kb = k0 + bz * KC;
     const int ke = (kb + KC - 1 < D.nk) ? kb + KC - 1 : D.nk;
+
+    // this thread's staged elements: shared index, offset in a layer, in range
+    int sp[NS];
+    size_t go[NS];
+    bool gok[NS];
+#pragma unroll
+    for (int q = 0; q < NS; ++q) {
+        const int p = tid + q * NT;
+        const int r = p / SX, c = p - r * SX;
+        const int i = i0 - 1 + c, j = j0 - 1 + r;
+        sp[q] = p < SX * SY ? p : -1;
+        gok[q] = p < SX * SY && i <= D.n1 && j <= D.n2;
+        go[q] = gok[q] ? (size_t)(j - 1) * D.n1 + (size_t)(i - 1) : 0;
+    }
+    auto stage = [&](int k, int b) {
+        const size_t koff = (size_t)(k - 1) * (size_t)D.plane;
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+            if (sp[q] >= 0) {
+                const size_t o = gok[q] ? koff + go[q] : 0;
+                cp_async_elem(&s_u[b][0][0] + sp[q], uin + o, gok[q]);
+                cp_async_elem(&s_v[b][0][0] + sp[q], vin + o, gok[q]);
+                cp_async_elem(&s_h[b][0][0] + sp[q], h + o, gok[q]);
+            }
+        }
+        cp_async_commit();
+    };
+    if (kb <= ke) stage(kb, 0);
   for (int k = kb; k <= ke; ++k) {
     const size_t koff = (size_t)(k - 1) * (size_t)D.plane;
-    if (k > kb) __syncthreads();  // the previous layer's tiles are consumed
-
-    // ---- stage u, v, h --------------------------------------------------
-    for (int p = tid; p < SX * SY; p += TX * TY) {
-        int r = p / SX, c = p - r * SX;
-        int i = i0 - 1 + c, j = j0 - 1 + r;
-        R uu = R(0.0), vv = R(0.0), hh = R(0.0);
-        if (i <= D.n1 && j <= D.n2) {
-            size_t o = koff + (size_t)(j - 1) * D.n1 + (i - 1);
-            uu = uin[o]; vv = vin[o]; hh = h[o];
-        }
-        s_u[r][c] = uu; s_v[r][c] = vv; s_h[r][c] = hh;
-    }
+    const int b = (k - kb) & 1;
+    cp_async_wait_all();
+    // layer k's tiles are visible to all threads, and every thread is done
+    // with layer k-1 (its outputs read buffer b^1 and the intermediates)
     __syncthreads();
+    if (k < ke) stage(k + 1, b ^ 1);
 
-#define SU(i, j) s_u[(j) - (j0 - 1)][(i) - (i0 - 1)]
-#define SV(i, j) s_v[(j) - (j0 - 1)][(i) - (i0 - 1)]
-#define SH(i, j) s_h[(j) - (j0 - 1)][(i) - (i0 - 1)]
+    // this thread's bases, loaded before the intermediates are evaluated
+    const int Io = i0 + (int)threadIdx.x;
+    const int jo = j0 + (int)threadIdx.y;
+    const bool do_u = Io <= D.ie - 1 && jo <= D.je;
+    const bool do_v = Io <= D.ie && jo <= D.je - 1;
+    const size_t oo = koff + (size_t)(jo - 1) * D.n1 + (Io - 1);
+    const R ub = do_u ? ubase[oo] : R(0.0);
+    const R vb = do_v ? vbase[oo] : R(0.0);
+
+#define SU(i, j) s_u[b][(j) - (j0 - 1)][(i) - (i0 - 1)]
+#define SV(i, j) s_v[b][(j) - (j0 - 1)][(i) - (i0 - 1)]
+#define SH(i, j) s_h[b][(j) - (j0 - 1)][(i) - (i0 - 1)]
 #define G2(a, i, j) ((R)(UNI ? U.a : MOM6B_A2(M.a, i, j, D)))
 #define COR(i, j) ((R)(UNI ? U.cor_row[(j) - 1] : MOM6B_A2(M.CoriolisBu, i, j, D)))
 
@@ -183,8 +241,7 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
                                             (G2(dy2h, I + 1, j) * SXX(I + 1, j)))) *
                         G2(IareaCu, I, j)) /
                        (h_u + h_neglect);
-        size_t o = koff + (size_t)(j - 1) * D.n1 + (I - 1);
-        uout[o] = ubase[o] + coef * (CAu + diffu);
+        uout[oo] = ub + coef * (CAu + diffu);
     }
     // ---- v point (i, J) = (I, j) -------------------------------------------
     if (I <= D.ie && j <= D.je - 1) {
@@ -203,8 +260,7 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
                                             (G2(dx2h, i, J + 1) * SXX(i, J + 1)))) *
                         G2(IareaCv, i, J)) /
                        (h_v + h_neglect);
-        size_t o = koff + (size_t)(J - 1) * D.n1 + (i - 1);
-        vout[o] = vbase[o] + coef * (CAv + diffv);
+        vout[oo] = vb + coef * (CAv + diffv);
     }
   }  // layer loop
 #undef SU
@@ -220,8 +276,8 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
 #undef VH
 }
 
-template <int TX, int TY, bool UNI, typename R>
-__global__ void __launch_bounds__(TX * TY)
+template <int TX, int TY, bool UNI, typename R, int MINB = 1>
+__global__ void __launch_bounds__(TX * TY, MINB)
 k_tendency(Dims D, Metrics M, UniMetrics U, const R* __restrict__ uin,
            const R* __restrict__ vin, const R* __restrict__ h,
            const R* ubase, const R* vbase, R* uout, R* vout,
@@ -247,12 +303,28 @@ cudaError_t launch_tendency_t(const Dims& D, const Metrics& M, const UniMetrics&
     dim3 block(kTendTX, TY, 1);
     int nchunks = (D.nk + kTendKC - 1) / kTendKC;
     dim3 grid((nx + kTendTX - 1) / kTendTX, (ny + TY - 1) / TY, nchunks);
-    if (U.valid)
-        k_tendency<kTendTX, TY, true, R><<<grid, block, 0, s>>>(
+    // CTAs per SM the registers are held to: 4 (64 registers) is the fastest
+    // uniform-metric form on B200 (FP64 tendency 2.01 ms per step against 2.13
+    // at 3 and 2.62 uncapped); the 2-D metric form keeps 3 (80 registers).
+    static int minb = -1;
+    if (minb < 0) {
+        const char* e = getenv("MOM6B_TEND_MINB");
+        minb = e ? atoi(e) : 4;
+    }
+    if (U.valid) {
+        if (minb == 4)
+            k_tendency<kTendTX, TY, true, R, 4><<<grid, block, 0, s>>>(
+                D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, kTendKC);
+        else if (minb == 3)
+            k_tendency<kTendTX, TY, true, R, 3><<<grid, block, 0, s>>>(
+                D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, kTendKC);
+        else
+            k_tendency<kTendTX, TY, true, R><<<grid, block, 0, s>>>(
+                D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, kTendKC);
+    } else {
+        k_tendency<kTendTX, TY, false, R, 3><<<grid, block, 0, s>>>(
             D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, kTendKC);
-    else
-        k_tendency<kTendTX, TY, false, R><<<grid, block, 0, s>>>(
-            D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, kTendKC);
+    }
     return cudaGetLastError();
 }
 
