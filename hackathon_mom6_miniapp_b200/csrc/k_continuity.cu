@@ -240,28 +240,44 @@ struct LayerVals {
 // over a face column is a chain of dependent sums, so the loads of CH layers
 // are issued together and their latency is paid once per chunk.
 constexpr int kContChunk = 4;
+// Cache hints in the face kernel: evict-first loads in the last column pass,
+// streaming stores of h_u and h.
+#ifndef MOM6B_CONT_HINTS
+#define MOM6B_CONT_HINTS 1
+#endif
+constexpr bool kContHints = MOM6B_CONT_HINTS != 0;
 
-template <typename EI>
+// LAST: the face's last pass over its column; u and the global edge arrays
+// are then read with the evict-first hint (nothing reads them again), which
+// leaves L2 to the columns whose Newton passes are still to come.
+template <bool LAST = false, typename EI>
 __device__ __forceinline__ LayerVals load_layer(const FaceCol<EI>& F, int k)
 {
     const size_t o = (size_t)(k - 1) * F.plane;
     const EI oe = (EI)(k - 1) * F.estride;
     LayerVals L;
-    L.u = F.u[o];
-    L.hWi = F.hWc[oe]; L.hEi = F.hEc[oe]; L.hi = F.hc[o];
-    L.hWp = F.hWc[oe + 1]; L.hEp = F.hEc[oe + 1]; L.hp = F.hc[o + 1];
+    if constexpr (LAST && sizeof(EI) == sizeof(size_t)) {
+        L.u = __ldcs(F.u + o);
+        L.hWi = __ldcs(F.hWc + oe); L.hEi = __ldcs(F.hEc + oe);
+        L.hWp = __ldcs(F.hWc + oe + 1); L.hEp = __ldcs(F.hEc + oe + 1);
+    } else {
+        L.u = F.u[o];
+        L.hWi = F.hWc[oe]; L.hEi = F.hEc[oe];
+        L.hWp = F.hWc[oe + 1]; L.hEp = F.hEc[oe + 1];
+    }
+    L.hi = F.hc[o]; L.hp = F.hc[o + 1];
     return L;
 }
 
 // Visit layers 1..nz in order, fn(k, LayerVals).
-template <int CH, typename EI, typename Fn>
+template <int CH, bool LAST = false, typename EI, typename Fn>
 __device__ __forceinline__ void for_layers(const FaceCol<EI>& F, int nz, Fn&& fn)
 {
     for (int kt = 1; kt <= nz; kt += CH) {
         LayerVals L[CH];
 #pragma unroll
         for (int c = 0; c < CH; ++c)
-            if (kt + c <= nz) L[c] = load_layer(F, kt + c);
+            if (kt + c <= nz) L[c] = load_layer<LAST>(F, kt + c);
 #pragma unroll
         for (int c = 0; c < CH; ++c)
             if (kt + c <= nz) fn(kt + c, L[c]);
@@ -513,7 +529,7 @@ __device__ __forceinline__ void face_work(const Dims& D, const Metrics& M, FaceC
     double FAmt_0 = 0.0, FAmt_L = 0.0, FAmt_R = 0.0, uhtot_L = 0.0, uhtot_R = 0.0;
     double* h_u = O.h_u + f0;
     const bool same = (du0 == du);
-    for_layers<CH>(F, nz, [&](int k, const LayerVals& L) {
+    for_layers<CH, kContHints>(F, nz, [&](int k, const LayerVals& L) {
         const double uk = L.u;
         double hm0, hmL, hmR;
         flux_eval(F, L, uk + du0, dt, hm0);
@@ -527,7 +543,8 @@ __device__ __forceinline__ void face_work(const Dims& D, const Metrics& M, FaceC
         // zonal_flux_thickness with u_cor = u + du (marginal faces)
         double hmc = hm0;
         if (!same) flux_eval(F, L, uk + du, dt, hmc);
-        h_u[(size_t)(k - 1) * F.plane] = hmc;
+        if (kContHints) __stcs(h_u + (size_t)(k - 1) * F.plane, hmc);
+        else h_u[(size_t)(k - 1) * F.plane] = hmc;
     });
     double FA_0 = FAmt_0, FA_avg = FAmt_0;
     if ((duL - du0) != 0.0) FA_avg = uhtot_L / (duL - du0);
@@ -573,7 +590,9 @@ __device__ __forceinline__ void cell_convergence(const Dims& D, const Metrics& M
         for (int k = 1; k <= D.nk; ++k) {
             const size_t o = (size_t)(k - 1) * D.plane + c0;
             double uh_left = from_ovl ? uh_left_col[k - 1] : O.uh[o - 1];
-            O.h[o] = dmax(hin[o] - fac * (O.uh[o] - uh_left), 0.0);
+            const double hn = dmax(hin[o] - fac * (O.uh[o] - uh_left), 0.0);
+            if (kContHints) __stcs(O.h + o, hn);
+            else O.h[o] = hn;
         }
     }
 }
