@@ -565,6 +565,282 @@ k_btstep_tiled(Dims D, Metrics M, UniMetrics U, BTWork W, BTParams P, BTTiles T,
 }
 
 // ---------------------------------------------------------------------------
+// Slot variant of the tiled loop (1024 threads, tiles of at most 62 x 62):
+// thread (txl, tyl) owns the four points (x0 - 1 + txl + 32 a, y0 - 1 + tyl +
+// 32 b), a, b in {0, 1}, of the 64 x 64 window that covers the tile and its
+// one-point rim, in every phase.  Each point's shared-memory offset and its
+// membership of every phase's region are worked out once, so a phase is
+// straight-line code over four slots.  A point's x neighbours belong to the
+// same warp, so the barrier between eta_pred and a first update of u is a
+// warp barrier.  The arithmetic of every point is k_btstep_tiled's.
+// ---------------------------------------------------------------------------
+enum : unsigned {
+    SB_ETA = 1u << 0,   // eta_pred
+    SB_V1 = 1u << 1,    // v update, v first
+    SB_U2 = 1u << 2,    // u update, v first
+    SB_U1 = 1u << 3,    // u update, u first
+    SB_V2 = 1u << 4,    // v update, u first
+    SB_OWN = 1u << 5,   // owned point of the tile
+    SB_E = 1u << 6,     // eta update
+    SB_NU = 1u << 7,    // ubt published
+    SB_NV = 1u << 8,    // vbt published
+    SB_AU = 1u << 9,    // uhbt(i, j) / ubt average range
+    SB_AV = 1u << 10,   // vhbt(i, j) / vbt average range
+    SB_UL = 1u << 11,   // uhbt(i - 1, j) range
+    SB_VL = 1u << 12,   // vhbt(i, j - 1) range
+};
+
+template <bool UNI, bool TAVG>
+__global__ void __launch_bounds__(1024, 1)
+k_btstep_slots(Dims D, Metrics M, UniMetrics U, BTWork W, BTParams P, BTTiles T,
+               const double* eta_in, const double* ubt_in, const double* vbt_in,
+               double* u_av, double* v_av, double* eta_av)
+{
+    constexpr int NT = 1024, TY = 32;
+    extern __shared__ double smem[];
+    const unsigned int nblocks = gridDim.x;
+    const int tid = (int)threadIdx.x;
+    const int txl = tid & 31, tyl = tid >> 5;
+    const int npts = D.n1 * D.n2;
+    const int gtid = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int gsz = (int)(gridDim.x * blockDim.x);
+    const int is = D.is, ie = D.ie, js = D.js, je = D.je;
+    const int iu0 = P.extended ? is - 1 : is, iu1 = P.extended ? ie : ie - 1;
+    const int jv0 = P.extended ? js - 1 : js, jv1 = P.extended ? je : je - 1;
+    const int tx = (int)blockIdx.x % T.nbx, ty = (int)blockIdx.x / T.nbx;
+    const int x0 = is - 1 + tx * T.tw, y0 = js - 1 + ty * T.th;
+    const int x1 = min(x0 + T.tw - 1, ie), y1 = min(y0 + T.th - 1, je);
+    const int lx0 = x0 - 2, ly0 = y0 - 2;
+    const int LW = T.tw + 3, LH = T.th + 3;
+    const int LN = LW * LH;
+    double* Se = smem;
+    double* Su = Se + LN;
+    double* Sv = Su + LN;
+    double* Sp = Sv + LN;
+    double* Sun = Sp + LN;
+    double* Svn = Sun + LN;
+#define GM(f, i, j) (UNI ? U.f : MOM6B_A2(M.f, i, j, D))
+#define F4U(c, i, j) (UNI ? U.f4u_row[((j) - 1) * 4 + (c) - 1] : MOM6B_F4(M.f_4_u, c, i, j, D))
+#define F4V(c, i, j) (UNI ? U.f4v_row[((j) - 1) * 4 + (c) - 1] : MOM6B_F4(M.f_4_v, c, i, j, D))
+#define SI(r) (x0 - 1 + txl + 32 * ((r) & 1))
+#define SJ(r) (y0 - 1 + tyl + TY * ((r) >> 1))
+#define SQ(r) (q0 + 32 * ((r) & 1) + TY * LW * ((r) >> 1))
+
+    // shared offset of slot 0 and the phase regions of the four slots
+    const int q0 = (tyl + 1) * LW + (txl + 1);
+    unsigned mk[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int i = SI(r), j = SJ(r);
+        auto in = [&](int a0, int a1, int b0, int b1) {
+            return i >= a0 && i <= a1 && j >= b0 && j <= b1;
+        };
+        unsigned m = 0;
+        if (in(max(x0 - 1, is), min(x1 + 1, ie), max(y0 - 1, js), min(y1 + 1, je))) m |= SB_ETA;
+        if (in(max(x0 - 1, is), min(x1 + 1, ie), max(y0 - 1, js), min(y1, je - 1))) m |= SB_V1;
+        if (in(max(x0 - 1, is), min(x1, ie - 1), max(y0, js), min(y1, je))) m |= SB_U2;
+        if (in(max(x0 - 1, is), min(x1, ie - 1), max(y0 - 1, js), min(y1 + 1, je))) m |= SB_U1;
+        if (in(max(x0, is), min(x1, ie), max(y0 - 1, js), min(y1, je - 1))) m |= SB_V2;
+        if (in(x0, x1, y0, y1)) m |= SB_OWN;
+        if (in(is, ie, js, je)) m |= SB_E;
+        if (in(is, ie - 1, js, je)) m |= SB_NU;
+        if (in(is, ie, js, je - 1)) m |= SB_NV;
+        if (in(iu0, iu1, js, je)) m |= SB_AU;
+        if (in(is, ie, jv0, jv1)) m |= SB_AV;
+        if (i - 1 >= iu0 && i - 1 <= iu1 && j >= js && j <= je) m |= SB_UL;
+        if (j - 1 >= jv0 && j - 1 <= jv1 && i >= is && i <= ie) m |= SB_VL;
+        mk[r] = m;
+    }
+
+    double avu[4], avv[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) avu[r] = avv[r] = 0.0;
+
+    // init (:199-207): both buffers hold the whole input state
+    for (int p = gtid; p < npts; p += gsz) {
+        double e = eta_in[p], ub = ubt_in[p], vb = vbt_in[p];
+        W.eta[p] = e; W.ubt[p] = ub; W.vbt[p] = vb;
+        W.eta_pred[p] = e; W.ubt_prev[p] = ub; W.vbt_prev[p] = vb;
+        if (TAVG) { W.uhbt[p] = 0.0; W.vhbt[p] = 0.0; }
+    }
+    if (tid == 0) W.tile_flag[blockIdx.x] = 0u;
+    if (!grid_barrier(W, nblocks, P.spin_budget)) return;
+
+    int nbr[8];
+    int nnb = 0;
+    for (int dyt = -1; dyt <= 1; ++dyt)
+        for (int dxt = -1; dxt <= 1; ++dxt) {
+            const int ax = tx + dxt, ay = ty + dyt;
+            if ((dxt || dyt) && ax >= 0 && ax < T.nbx && ay >= 0 && ay < T.nby)
+                nbr[nnb++] = ay * T.nbx + ax;
+        }
+
+    for (int n = 1; n <= P.nstep; ++n) {
+        const bool v_first = ((n + P.first_direction) % 2) == 1;
+        const double* ce = (n & 1) ? W.eta : W.eta_pred;
+        const double* cu = (n & 1) ? W.ubt : W.ubt_prev;
+        const double* cv = (n & 1) ? W.vbt : W.vbt_prev;
+        double* ne = (n & 1) ? W.eta_pred : W.eta;
+        double* nu = (n & 1) ? W.ubt_prev : W.ubt;
+        double* nv = (n & 1) ? W.vbt_prev : W.vbt;
+        // S1: previous state on the window (as in k_btstep_tiled)
+        if (n > 1 && !wait_neighbours(W, nbr, nnb, (unsigned int)(n - 1), P.spin_budget)) return;
+        if (n == 1) {
+            for (int jl = tyl; jl < LH; jl += TY)
+            for (int il = txl; il < LW; il += 32) {
+                const int q = jl * LW + il, i = lx0 + il, j = ly0 + jl;
+                double e = 0.0, ub = 0.0, vb = 0.0;
+                if (i >= 1 && i <= D.n1 && j >= 1 && j <= D.n2) {
+                    int p = (j - 1) * D.n1 + (i - 1);
+                    e = __ldcg(ce + p); ub = __ldcg(cu + p); vb = __ldcg(cv + p);
+                }
+                Se[q] = e; Su[q] = ub; Sv[q] = vb; Sun[q] = ub; Svn[q] = vb;
+            }
+        } else {
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                if (!(mk[r] & SB_OWN)) continue;
+                const int q = SQ(r);
+                Se[q] = Sp[q]; Su[q] = Sun[q]; Sv[q] = Svn[q];
+            }
+            const int nb = y0 - ly0, na = (ly0 + LH - 1) - y1;
+            const int nl = x0 - lx0, nr = (lx0 + LW - 1) - x1;
+            const int mid = y1 - y0 + 1, side = nl + nr;
+            const int nring = (nb + na) * LW + mid * side;
+            for (int t = tid; t < nring; t += NT) {
+                int i, j;
+                if (t < nb * LW) {
+                    j = ly0 + t / LW; i = lx0 + t % LW;
+                } else if (t < (nb + na) * LW) {
+                    const int t2 = t - nb * LW;
+                    j = y1 + 1 + t2 / LW; i = lx0 + t2 % LW;
+                } else {
+                    const int t3 = t - (nb + na) * LW;
+                    const int c = t3 % side;
+                    j = y0 + t3 / side;
+                    i = c < nl ? lx0 + c : x1 + 1 + (c - nl);
+                }
+                const int q = (j - ly0) * LW + (i - lx0);
+                double e = 0.0, ub = 0.0, vb = 0.0;
+                if (i >= 1 && i <= D.n1 && j >= 1 && j <= D.n2) {
+                    int p = (j - 1) * D.n1 + (i - 1);
+                    e = __ldcg(ce + p); ub = __ldcg(cu + p); vb = __ldcg(cv + p);
+                }
+                Se[q] = e; Su[q] = ub; Sv[q] = vb; Sun[q] = ub; Svn[q] = vb;
+            }
+        }
+        __syncthreads();
+        // S2: eta_pred
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            if (!(mk[r] & SB_ETA)) continue;
+            const int i = SI(r), j = SJ(r), q = SQ(r);
+            Sp[q] = Se[q] + (P.dtbt * GM(IareaT, i, j)) *
+                                (((GM(Datu, i - 1, j) * Su[q - 1]) - (GM(Datu, i, j) * Su[q])) +
+                                 ((GM(Datv, i, j - 1) * Sv[q - LW]) - (GM(Datv, i, j) * Sv[q])));
+        }
+        auto upd_u = [&](int r, const double* V) {
+            const int i = SI(r), j = SJ(r), q = SQ(r);
+            double PFu = ((Sp[q] * GM(gtot_E, i, j)) - (Sp[q + 1] * GM(gtot_W, i + 1, j))) *
+                         P.dgeo_de * GM(IdxCu, i, j);
+            double Cor_u = (((F4U(4, i, j) * V[q + 1]) + (F4U(1, i, j) * V[q - LW])) +
+                            ((F4U(3, i, j) * V[q]) + (F4U(2, i, j) * V[q + 1 - LW])));
+            Sun[q] = GM(bt_rem_u, i, j) * (Su[q] + P.dtbt * (Cor_u + PFu));
+        };
+        auto upd_v = [&](int r, const double* Uv) {
+            const int i = SI(r), j = SJ(r), q = SQ(r);
+            double PFv = ((Sp[q] * GM(gtot_N, i, j)) - (Sp[q + LW] * GM(gtot_S, i, j + 1))) *
+                         P.dgeo_de * GM(IdyCv, i, j);
+            double Cor_v = -1.0 * (((F4V(1, i, j) * Uv[q - 1]) + (F4V(4, i, j) * Uv[q + LW])) +
+                                   ((F4V(2, i, j) * Uv[q]) + (F4V(3, i, j) * Uv[q - 1 + LW])));
+            Svn[q] = GM(bt_rem_v, i, j) * (Sv[q] + P.dtbt * (Cor_v + PFv));
+        };
+        // S3 / S4: the two velocity updates
+        if (v_first) {
+            __syncthreads();   // eta_pred of the row above
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+                if (mk[r] & SB_V1) upd_v(r, Su);
+            __syncthreads();
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+                if (mk[r] & SB_U2) upd_u(r, Svn);
+        } else {
+            __syncwarp();      // eta_pred of x + 1: same warp
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+                if (mk[r] & SB_U1) upd_u(r, Sv);
+            __syncthreads();
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+                if (mk[r] & SB_V2) upd_v(r, Sun);
+        }
+        __syncthreads();
+        // S5: transports, eta update and averages on the owned points
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const unsigned m = mk[r];
+            if (!(m & SB_OWN)) continue;
+            const int i = SI(r), j = SJ(r), q = SQ(r);
+            const int p = (j - 1) * D.n1 + (i - 1);
+            const double uh0 = (m & SB_AU)
+                ? GM(Datu, i, j) * (P.trans_wt1 * Sun[q] + P.trans_wt2 * Su[q]) : 0.0;
+            const double vh0 = (m & SB_AV)
+                ? GM(Datv, i, j) * (P.trans_wt1 * Svn[q] + P.trans_wt2 * Sv[q]) : 0.0;
+            double e = Se[q];
+            if (m & SB_E) {
+                const double uh1 = (m & SB_UL)
+                    ? GM(Datu, i - 1, j) * (P.trans_wt1 * Sun[q - 1] + P.trans_wt2 * Su[q - 1])
+                    : 0.0;
+                const double vh1 = (m & SB_VL)
+                    ? GM(Datv, i, j - 1) * (P.trans_wt1 * Svn[q - LW] + P.trans_wt2 * Sv[q - LW])
+                    : 0.0;
+                e = Se[q] - P.dtbt * GM(IareaT, i, j) * ((uh0 - uh1) + (vh0 - vh1));
+                ne[p] = e;
+            }
+            Sp[q] = e;
+            if (m & SB_NU) nu[p] = Sun[q];
+            if (m & SB_NV) nv[p] = Svn[q];
+            if (m & SB_AU) avu[r] = avu[r] + Sun[q] * P.inv_nstep;
+            if (m & SB_AV) avv[r] = avv[r] + Svn[q] * P.inv_nstep;
+            if (TAVG) {
+                if (m & SB_AU) W.uhbt[p] = W.uhbt[p] + uh0 * P.inv_nstep;
+                if (m & SB_AV) W.vhbt[p] = W.vhbt[p] + vh0 * P.inv_nstep;
+            }
+        }
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            atomicExch(W.tile_flag + blockIdx.x, (unsigned int)n);
+        }
+    }
+    if (!grid_barrier(W, nblocks, P.spin_budget)) return;
+    const double* fe = (P.nstep & 1) ? W.eta_pred : W.eta;
+    for (int p = gtid; p < npts; p += gsz) {
+        eta_av[p] = fe[p];
+        int i = p % D.n1 + 1, j = p / D.n1 + 1;
+        if (i < is - 1 || i > ie || j < js - 1 || j > je) {
+            u_av[p] = 0.0;
+            v_av[p] = 0.0;
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        if (!(mk[r] & SB_OWN)) continue;
+        const int i = SI(r), j = SJ(r);
+        const int p = (j - 1) * D.n1 + (i - 1);
+        u_av[p] = avu[r];
+        v_av[p] = avv[r];
+    }
+#undef GM
+#undef F4U
+#undef F4V
+#undef SI
+#undef SJ
+#undef SQ
+}
+
+// ---------------------------------------------------------------------------
 // Ensemble variant: the barotropic loops of many domains in one cooperative
 // launch.
 // ---------------------------------------------------------------------------
@@ -861,7 +1137,17 @@ static cudaError_t launch_btstep_tiled(const Dims& D, const Metrics& M, const Un
     const int NT = T.nt;
     size_t smem = (size_t)6 * (T.tw + 3) * (T.th + 3) * sizeof(double);
     const void* fn;
-    if (NT == 512)
+    static int slots = -1;
+    if (slots < 0) {
+        const char* e = getenv("MOM6B_BT_SLOTS");
+        slots = e ? atoi(e) : 1;
+    }
+    if (slots && NT == 1024 && T.tw <= 62 && T.th <= 62)
+        fn = tavg ? (U.valid_bt ? (const void*)k_btstep_slots<true, true>
+                                : (const void*)k_btstep_slots<false, true>)
+                  : (U.valid_bt ? (const void*)k_btstep_slots<true, false>
+                                : (const void*)k_btstep_slots<false, false>);
+    else if (NT == 512)
         fn = tavg ? (U.valid_bt ? (const void*)k_btstep_tiled<512, true, true>
                                 : (const void*)k_btstep_tiled<512, false, true>)
                   : (U.valid_bt ? (const void*)k_btstep_tiled<512, true, false>
