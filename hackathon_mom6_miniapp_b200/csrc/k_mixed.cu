@@ -7,7 +7,8 @@
 //   continuity  the per-face column sums (uh_tot, duhdu_tot, the BT_cont face
 //               areas), the Newton scalars and the thickness update
 //               h = max(hin - dt IareaT (uh(I) - uh(I-1)), 0);
-//   vertvisc    the coefficients and the whole tridiagonal elimination;
+//   vertvisc    the bottom stress (the coefficients and the elimination are
+//               FP32: the system is diagonally dominant);
 //   btstep      runs in FP64 (its 2-D state is a few MB and its cost is the
 //               latency of the substep loop, not bytes).
 // This file is built with FMA contraction (the FP64 files are not), and the

@@ -1,8 +1,10 @@
 // vertvisc_impl.cuh -- the prefetching vertical viscosity kernel, templated
-// on the storage type R of u, v and h.  Every coefficient and the whole
-// tridiagonal elimination are computed in double whatever R is: R = double
-// is the bit-exact FP64 form (k_vertvisc.cu); R = float is the mixed form
-// (k_mixed.cu), which loads and stores FP32 and eliminates in FP64.
+// on the storage type R of u, v and h, in which the coefficients and the
+// tridiagonal elimination are computed: R = double is the bit-exact FP64
+// form (k_vertvisc.cu); R = float is the mixed form (k_mixed.cu).  The
+// system is diagonally dominant (every pivot is h + dt (Ray + a d1 + a_next)
+// with nonnegative terms), so the FP32 elimination loses only a few units in
+// the last place per layer; the bottom stress accumulates in double.
 //
 // Restates vert_visc_coef + vert_visc_apply of the serial module
 // (mom6_vert_visc_serial.F90:138-287 and :394-506) as the driver calls them
@@ -29,9 +31,10 @@ __device__ __forceinline__ C vv_botfn(C z2) {
 // Layers whose inputs one prefetch brings in.
 constexpr int kVvChunk = 4;
 // CTAs per SM the registers are held to, by storage type: measured fastest on
-// B200 (FP64 6: 2.28 ms per step, no cap 2.50; FP32 8: 1.85 ms, no cap 2.67).
+// B200 (FP64 6: 2.28 ms per step, no cap 2.50; FP32 10: 1.13 ms, 8: 1.23,
+// 12: 1.36).
 template <typename R>
-constexpr int vv_min_blocks() { return sizeof(R) == 4 ? 8 : 6; }
+constexpr int vv_min_blocks() { return sizeof(R) == 4 ? 10 : 6; }
 
 // The column of thread tx of the CTA with block coordinates (bx, by): row
 // by of the interleaved u/v row list, column bx * blockDim.x + tx.
@@ -41,11 +44,13 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
                 const R* __restrict__ h, double dt, const VVParams& P,
                 double* __restrict__ taux_bot, double* __restrict__ tauy_bot, int bx, int by)
 {
-    // Coefficients (h_harm, z_i, botfn, hvel, a(K)) are computed in the
-    // storage type R; the tridiagonal elimination (b1, d1, c1, the eliminated
-    // velocity and the back substitution) always in double.
+    // Coefficients (h_harm, z_i, botfn, hvel, a(K)) and the tridiagonal
+    // elimination (b1, d1, c1, the eliminated velocity and the back
+    // substitution) are computed in the storage type R; the bottom stress
+    // accumulates in double.
     using C = R;
-    double slot[KMAX + 2];   // botfn(z_i(m)), then c1(m)
+    using E = R;
+    E slot[KMAX + 2];   // botfn(z_i(m)), then c1(m)
     const int nz = D.nk;
     // Rows are interleaved so that the u row j and the v rows j-1, j, which
     // read the same rows of h, run close together: by = 0 is the v
@@ -136,13 +141,13 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
     const C a_bot_num = Kv + Kv_extra_bbl;
 
     // ---- sweep 2: coefficients + forward elimination, top-down -----------
-    const double dt_Rho0 = dt / kRho0;
-    const double sfc_stress = dt_Rho0 * MOM6B_A2(tau, i, j, D) * msk;
-    const double v1 = vc[0];
+    const E dtE = (E)dt;
+    const E sfc_stress = (E)(dt / kRho0 * MOM6B_A2(tau, i, j, D) * msk);
+    const E v1 = vc[0];
     C hv_k = hvel((C)slot[2], hc[0], hn_[0], (C)v1);
     C z_top = C(0.0);
     C hv_next, a_next;
-    double vnext = 0.0;                      // vel(k + 1) before elimination
+    E vnext = E(0.0);                        // vel(k + 1) before elimination
     if (nz >= 2) {
         vnext = vc[plane];
         hv_next = hvel((C)slot[3], hc[plane], hn_[plane], (C)vnext);
@@ -152,13 +157,13 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
         hv_next = C(0.0);
         a_next = a_bot_num / (C(0.5) * hv_k + hn);
     }
-    double a_k = 0.0;  // a(1) = 0, surface
-    double Rayk = ray_on[0] ? rc[0] : 0.0;
-    double h_u = (double)(hv_k + hn);
-    double b_denom_1 = h_u + dt * (Rayk + a_k);
-    double b1 = 1.0 / (b_denom_1 + dt * (double)a_next);
-    double d1 = b_denom_1 * b1;
-    double u_prev = b1 * (h_u * v1 + sfc_stress);
+    E a_k = E(0.0);  // a(1) = 0, surface
+    E Rayk = ray_on[0] ? (E)rc[0] : E(0.0);
+    E h_u = (E)(hv_k + hn);
+    E b_denom_1 = h_u + dtE * (Rayk + a_k);
+    E b1 = E(1.0) / (b_denom_1 + dtE * (E)a_next);
+    E d1 = b_denom_1 * b1;
+    E u_prev = b1 * (h_u * v1 + sfc_stress);
     vc[0] = (R)u_prev;
     for (int kt = 2; kt <= nz; kt += CH) {
         // layers kt .. kt+CH-1 are eliminated; they need h and vel of the
@@ -166,7 +171,7 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
         // and botfn of interfaces k+1, k+2 (slots kt+1 .. kt+CH+1, read
         // before this chunk overwrites slots kt .. kt+CH-1 with c1)
         C p0[CH], p1[CH], pb[CH + 1];
-        double pv[CH], pr[CH];
+        E pv[CH], pr[CH];
 #pragma unroll
         for (int c = 0; c < CH; ++c) {
             int k = kt + c;
@@ -175,7 +180,7 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
                 p1[c] = hn_[(size_t)k * plane];
                 pv[c] = vc[(size_t)k * plane];
             }
-            if (k <= nz) pr[c] = ray_on[k - 1] ? rc[(size_t)(k - 1) * plane] : 0.0;
+            if (k <= nz) pr[c] = ray_on[k - 1] ? (E)rc[(size_t)(k - 1) * plane] : E(0.0);
         }
 #pragma unroll
         for (int c = 0; c <= CH; ++c)
@@ -184,8 +189,8 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
         for (int c = 0; c < CH; ++c) {
             int k = kt + c;
             if (k <= nz) {
-                const double vk = vnext;     // vel(k) before elimination
-                a_k = (double)a_next;
+                const E vk = vnext;          // vel(k) before elimination
+                a_k = (E)a_next;
                 hv_k = hv_next;
                 if (k < nz) {
                     vnext = pv[c];
@@ -196,13 +201,13 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
                     a_next = a_bot_num / (C(0.5) * hv_k + hn);
                 }
                 Rayk = pr[c];
-                double c1 = dt * a_k * b1;
+                E c1 = dtE * a_k * b1;
                 slot[k] = c1;
-                h_u = (double)(hv_k + hn);
-                b_denom_1 = h_u + dt * (Rayk + a_k * d1);
-                b1 = 1.0 / (b_denom_1 + dt * (double)a_next);
+                h_u = (E)(hv_k + hn);
+                b_denom_1 = h_u + dtE * (Rayk + a_k * d1);
+                b1 = E(1.0) / (b_denom_1 + dtE * (E)a_next);
                 d1 = b_denom_1 * b1;
-                u_prev = (h_u * vk + dt * a_k * u_prev) * b1;
+                u_prev = (h_u * vk + dtE * a_k * u_prev) * b1;
                 vc[(size_t)(k - 1) * plane] = (R)u_prev;
             }
         }
@@ -210,9 +215,9 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
     const double a_bottom = (double)a_next;
 
     // ---- sweep 3: back substitution (:447-449) ----------------------------
-    double u_below = u_prev;
+    E u_below = u_prev;
     for (int kt = nz - 1; kt >= 1; kt -= CH) {
-        double pv[CH], pc[CH];
+        E pv[CH], pc[CH];
 #pragma unroll
         for (int c = 0; c < CH; ++c) {
             int k = kt - c;
@@ -225,14 +230,14 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
         for (int c = 0; c < CH; ++c) {
             int k = kt - c;
             if (k >= 1) {
-                double uk = pv[c] + pc[c] * u_below;
+                E uk = pv[c] + pc[c] * u_below;
                 vc[(size_t)(k - 1) * plane] = (R)uk;
                 u_below = uk;
             }
         }
     }
     // bottom stress (:452-458)
-    double tb = kRho0 * u_prev * a_bottom;
+    double tb = kRho0 * (double)u_prev * a_bottom;
     for (int k = 1; k <= nz; ++k)
         if (ray_on[k - 1]) {
             size_t o = (size_t)(k - 1) * plane;
@@ -276,6 +281,10 @@ static cudaError_t launch_vv_pf(const Dims& D, const Metrics& M, R* u, R* v, con
         k_vertvisc_pf<KMAX, 4, R, 6><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P, taux_bot, tauy_bot);
     else if (minb == 8)
         k_vertvisc_pf<KMAX, 4, R, 8><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P, taux_bot, tauy_bot);
+    else if (minb == 10 && sizeof(R) == 4)
+        k_vertvisc_pf<KMAX, 4, R, 10><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P, taux_bot, tauy_bot);
+    else if (minb == 12 && sizeof(R) == 4)
+        k_vertvisc_pf<KMAX, 4, R, 12><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P, taux_bot, tauy_bot);
     else
         k_vertvisc_pf<KMAX, 4, R><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P, taux_bot, tauy_bot);
     return cudaGetLastError();
