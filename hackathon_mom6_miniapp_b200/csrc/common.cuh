@@ -53,4 +53,10 @@ enum : int { kDevOk = 0, kDevTimeout = 1 };
 __device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }
 __device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }
 
+// a / b in the arithmetic type of a templated kernel: the IEEE quotient in
+// double (the bit-exact forms), the fast reciprocal-based quotient (2 ulp) in
+// float (the mixed form).
+__device__ __forceinline__ double div_r(double a, double b) { return a / b; }
+__device__ __forceinline__ float div_r(float a, float b) { return __fdividef(a, b); }
+
 } // namespace mom6b

@@ -157,7 +157,7 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
                 R hAv0 = (I >= D.is) ? R(0.5) * ((aT00 * h00) + (aT01 * h01)) : R(0.0);
                 R hAv1 = R(0.5) * ((aT10 * h10) + (aT11 * h11));
                 R hArea_q = (hAu0 + hAu1) + (hAv0 + hAv1);
-                R Ih_q = G2(Area_q, I, J) / (hArea_q + R(1.0e-20));
+                R Ih_q = div_r(G2(Area_q, I, J), hArea_q + R(1.0e-20));
                 qv = absv * Ih_q;
                 // hor_visc: shearing strain and stress at q-points (:513-520, :544, :579, :964, :1050)
                 R dvdx_v = G2(DY_dxBu, I, J) *
@@ -179,10 +179,10 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
             R ke = R(0.0), sxx = R(0.0);
             if (i <= D.n1 && j <= D.n2) {
                 R uc = SU(i, j), um = SU(i - 1, j), vc = SV(i, j), vm = SV(i, j - 1);
-                ke = R(0.25) *
-                     ((G2(dyCu, i, j) * (uc * uc) + G2(dyCu, i - 1, j) * (um * um)) +
-                      (G2(dxCv, i, j) * (vc * vc) + G2(dxCv, i, j - 1) * (vm * vm))) /
-                     G2(areaT, i, j);
+                ke = div_r(R(0.25) *
+                               ((G2(dyCu, i, j) * (uc * uc) + G2(dyCu, i - 1, j) * (um * um)) +
+                                (G2(dxCv, i, j) * (vc * vc) + G2(dxCv, i, j - 1) * (vm * vm))),
+                           G2(areaT, i, j));
                 R dudx = G2(DY_dxT, i, j) *
                               ((G2(IdyCu, i, j) * uc) - (G2(IdyCu, i - 1, j) * um));
                 R dvdy = G2(DX_dyT, i, j) *
@@ -235,12 +235,12 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
                          IdxCu -
                      KEx;
         R h_u = R(0.5) * (G2(mask2dT, I, j) * SH(I, j) + G2(mask2dT, I + 1, j) * SH(I + 1, j));
-        R diffu = ((IdxCu * ((G2(dx2q, I, j - 1) * SXY(I, j - 1)) -
+        R diffu = div_r((IdxCu * ((G2(dx2q, I, j - 1) * SXY(I, j - 1)) -
                                   (G2(dx2q, I, j) * SXY(I, j))) +
                          G2(IdyCu, I, j) * ((G2(dy2h, I, j) * SXX(I, j)) -
                                             (G2(dy2h, I + 1, j) * SXX(I + 1, j)))) *
-                        G2(IareaCu, I, j)) /
-                       (h_u + h_neglect);
+                            G2(IareaCu, I, j),
+                        h_u + h_neglect);
         uout[oo] = ub + coef * (CAu + diffu);
     }
     // ---- v point (i, J) = (I, j) -------------------------------------------
@@ -254,12 +254,12 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
                          IdyCv -
                      KEy;
         R h_v = R(0.5) * (G2(mask2dT, i, J) * SH(i, J) + G2(mask2dT, i, J + 1) * SH(i, J + 1));
-        R diffv = ((IdyCv * ((G2(dy2q, i - 1, J) * SXY(i - 1, J)) -
+        R diffv = div_r((IdyCv * ((G2(dy2q, i - 1, J) * SXY(i - 1, J)) -
                                   (G2(dy2q, i, J) * SXY(i, J))) -
                          G2(IdxCv, i, J) * ((G2(dx2h, i, J) * SXX(i, J)) -
                                             (G2(dx2h, i, J + 1) * SXX(i, J + 1)))) *
-                        G2(IareaCv, i, J)) /
-                       (h_v + h_neglect);
+                            G2(IareaCv, i, J),
+                        h_v + h_neglect);
         vout[oo] = vb + coef * (CAv + diffv);
     }
   }  // layer loop

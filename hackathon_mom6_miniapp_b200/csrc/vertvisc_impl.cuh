@@ -19,7 +19,7 @@ namespace mom6b {
 
 template <typename C>
 __device__ __forceinline__ C vv_botfn(C z2) {
-    return C(1.0) / (C(1.0) + C(0.09) * z2 * z2 * z2 * z2 * z2 * z2);
+    return div_r(C(1.0), C(1.0) + C(0.09) * z2 * z2 * z2 * z2 * z2 * z2);
 }
 
 // Prefetching variant (the default): one per-column local array (botfn(z_i(m)),
@@ -106,7 +106,7 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
         for (int c = 0; c < CH; ++c) {
             int k = kt - c;
             if (k >= 2) {
-                C h_harm = C(2.0) * a0[c] * a1[c] / (a0[c] + a1[c] + hn);
+                C h_harm = div_r(C(2.0) * a0[c] * a1[c], a0[c] + a1[c] + hn);
                 z = z + h_harm * I_Hbbl;
                 slot[k] = vv_botfn(z);
             }
@@ -117,7 +117,7 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
     // flow opposes the thickness gradient (:162-177)
     // bf_up = botfn(z_i(k+1)) (slot k+1 of sweep 1)
     auto hvel = [&](C bf_up, C h0, C h1, C vk) -> C {
-        C h_harm = C(2.0) * h0 * h1 / (h0 + h1 + hn);
+        C h_harm = div_r(C(2.0) * h0 * h1, h0 + h1 + hn);
         C hv = h_harm;
         if (vk * (h1 - h0) < C(0.0)) {
             C bf = bf_up;
@@ -131,12 +131,12 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
     auto a_of = [&](C bf_K2, C z_top, C hv_lo, C hv_up) -> C {
         C Kv_tot = Kv;
         if (z_top < Hmix) {
-            C topfn = C(1.0) - z_top / Hmix;
+            C topfn = C(1.0) - div_r(z_top, Hmix);
             Kv_tot = Kv_tot + (Kv_ml - Kv) * topfn;
         }
         Kv_tot = Kv_tot + Kv_extra_bbl * bf_K2;
         C h_shear = C(0.5) * (hv_lo + hv_up + hn);
-        return Kv_tot / h_shear;
+        return div_r(Kv_tot, h_shear);
     };
     const C a_bot_num = Kv + Kv_extra_bbl;
 
@@ -155,13 +155,13 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
         a_next = a_of((C)slot[2], z_top, hv_next, hv_k);
     } else {
         hv_next = C(0.0);
-        a_next = a_bot_num / (C(0.5) * hv_k + hn);
+        a_next = div_r(a_bot_num, C(0.5) * hv_k + hn);
     }
     E a_k = E(0.0);  // a(1) = 0, surface
     E Rayk = ray_on[0] ? (E)rc[0] : E(0.0);
     E h_u = (E)(hv_k + hn);
     E b_denom_1 = h_u + dtE * (Rayk + a_k);
-    E b1 = E(1.0) / (b_denom_1 + dtE * (E)a_next);
+    E b1 = div_r(E(1.0), b_denom_1 + dtE * (E)a_next);
     E d1 = b_denom_1 * b1;
     E u_prev = b1 * (h_u * v1 + sfc_stress);
     vc[0] = (R)u_prev;
@@ -198,14 +198,14 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
                     z_top = z_top + hv_k;
                     a_next = a_of(pb[c], z_top, hv_next, hv_k);
                 } else {
-                    a_next = a_bot_num / (C(0.5) * hv_k + hn);
+                    a_next = div_r(a_bot_num, C(0.5) * hv_k + hn);
                 }
                 Rayk = pr[c];
                 E c1 = dtE * a_k * b1;
                 slot[k] = c1;
                 h_u = (E)(hv_k + hn);
                 b_denom_1 = h_u + dtE * (Rayk + a_k * d1);
-                b1 = E(1.0) / (b_denom_1 + dtE * (E)a_next);
+                b1 = div_r(E(1.0), b_denom_1 + dtE * (E)a_next);
                 d1 = b_denom_1 * b1;
                 u_prev = (h_u * vk + dtE * a_k * u_prev) * b1;
                 vc[(size_t)(k - 1) * plane] = (R)u_prev;
