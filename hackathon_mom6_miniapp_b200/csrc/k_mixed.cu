@@ -91,12 +91,14 @@ cudaError_t launch_continuity_f(const Dims& D, const Metrics& M, const float* u,
     static int minb = -1;
     if (minb < 0) {
         const char* e = getenv("MOM6B_CONTF_MINB");
-        minb = e ? atoi(e) : 5;   // 5 CTAs per SM: 2.44 ms per step (no cap: 3.19)
+        minb = e ? atoi(e) : 6;   // 6 CTAs per SM: 2.19 ms per step (5: 2.23, 4: 2.38)
     }
     if (minb == 4)
         k_cont_faces_f<4><<<grid, nb, 0, s>>>(D, M, u, hin, hW, hE, uhbt, O, (float*)uh_ovl, dt);
     else if (minb == 5)
         k_cont_faces_f<5><<<grid, nb, 0, s>>>(D, M, u, hin, hW, hE, uhbt, O, (float*)uh_ovl, dt);
+    else if (minb == 6)
+        k_cont_faces_f<6><<<grid, nb, 0, s>>>(D, M, u, hin, hW, hE, uhbt, O, (float*)uh_ovl, dt);
     else
         k_cont_faces_f<1><<<grid, nb, 0, s>>>(D, M, u, hin, hW, hE, uhbt, O, (float*)uh_ovl, dt);
     return cudaGetLastError();

@@ -152,6 +152,13 @@ struct FaceF {
         const size_t o = (size_t)(k - 1) * plane;
         return LayerF{u[o], hW[o], hE[o], hc[o], hW[o + 1], hE[o + 1], hc[o + 1]};
     }
+    // the face's last pass: u and the edges with the evict-first hint
+    __device__ LayerF load_last(int k) const
+    {
+        const size_t o = (size_t)(k - 1) * plane;
+        return LayerF{__ldcs(u + o), __ldcs(hW + o), __ldcs(hE + o), hc[o],
+                      __ldcs(hW + o + 1), __ldcs(hE + o + 1), hc[o + 1]};
+    }
     // upwind PPM transport and marginal thickness at face velocity uI
     __device__ float eval(const LayerF& L, float uI, float& hm) const
     {
@@ -170,14 +177,14 @@ struct FaceF {
 
 constexpr int kMixCH = 4;
 
-template <typename Fn>
+template <bool LAST = false, typename Fn>
 __device__ __forceinline__ void mix_layers(const FaceF& F, int nz, Fn&& fn)
 {
     for (int kt = 1; kt <= nz; kt += kMixCH) {
         LayerF L[kMixCH];
 #pragma unroll
         for (int c = 0; c < kMixCH; ++c)
-            if (kt + c <= nz) L[c] = F.load(kt + c);
+            if (kt + c <= nz) L[c] = LAST ? F.load_last(kt + c) : F.load(kt + c);
 #pragma unroll
         for (int c = 0; c < kMixCH; ++c)
             if (kt + c <= nz) fn(kt + c, L[c]);
@@ -327,7 +334,7 @@ __device__ __forceinline__ void cont_faces_f(const Dims& D, const Metrics& M,
             double FAmt_0 = 0.0, FAmt_L = 0.0, FAmt_R = 0.0, uhtot_L = 0.0, uhtot_R = 0.0;
             const float d0 = (float)du0, dL = (float)duL, dR = (float)duR, dc = (float)du;
             const bool same = du0 == du;
-            mix_layers(F, nz, [&](int k, const LayerF& L) {
+            mix_layers<true>(F, nz, [&](int k, const LayerF& L) {
                 float hm0, hmL, hmR;
                 F.eval(L, L.u + d0, hm0);
                 const float uL = F.eval(L, L.u + dL, hmL);
@@ -339,7 +346,7 @@ __device__ __forceinline__ void cont_faces_f(const Dims& D, const Metrics& M,
                 uhtot_R += (double)uR;
                 float hmc = hm0;
                 if (!same) F.eval(L, L.u + dc, hmc);
-                O.h_u[f0 + (size_t)(k - 1) * plane] = hmc;
+                __stcs(O.h_u + f0 + (size_t)(k - 1) * plane, hmc);
             });
             double FA_0 = FAmt_0, FA_avg = FAmt_0;
             if ((duL - du0) != 0.0) FA_avg = uhtot_L / (duL - du0);
@@ -371,7 +378,7 @@ __device__ __forceinline__ void cont_faces_f(const Dims& D, const Metrics& M,
         for (int k = 1; k <= nz; ++k) {
             const size_t o = (size_t)(k - 1) * plane + c0;
             const double left = from_ovl ? (double)ovl[k - 1] : (double)O.uh[o - 1];
-            O.h[o] = (float)fmax((double)hin[o] - fac * ((double)O.uh[o] - left), 0.0);
+            __stcs(O.h + o, (float)fmax((double)hin[o] - fac * ((double)O.uh[o] - left), 0.0));
         }
     }
 }
