@@ -13,7 +13,7 @@ the timed region is bracketed by a barrier and device synchronisation and
 the time is the maximum over ranks.
 
 The line's "mixed" object measures the mixed-precision form (FP32 state,
-fluxes and stencils; FP64 column sums, thickness update, vertical elimination
+fluxes, stencils and vertical elimination; FP64 column sums, thickness update
 and barotropic loop) on the same workload and protocol, with its speed-up
 over the FP64 form and its per-field relative L2 error against the FP64 form
 of the same seed after 10 steps at 720x720x75 and after 100 steps at
@@ -38,6 +38,7 @@ host threads (its single-thread rate beside it), on rank 0 only.
 """
 import argparse
 import json
+import math
 import os
 import subprocess
 import sys
@@ -265,9 +266,21 @@ def mixed_errors(ni, nj, nsteps, seed, local):
     return errs
 
 
+def _finite(x):
+    """x with every non-finite float replaced by None (null in the JSON line:
+    NaN and Infinity are not JSON)."""
+    if isinstance(x, float):
+        return x if math.isfinite(x) else None
+    if isinstance(x, dict):
+        return {k: _finite(v) for k, v in x.items()}
+    if isinstance(x, (list, tuple)):
+        return [_finite(v) for v in x]
+    return x
+
+
 def run_mixed(args, world, rank, local, dist, fp64_ms_per_step):
-    """The mixed form (FP32 state, fluxes and stencils; FP64 column sums,
-    thickness update, vertical elimination and barotropic loop) on the same
+    """The mixed form (FP32 state, fluxes, stencils and vertical elimination;
+    FP64 column sums, thickness update and barotropic loop) on the same
     workload and timing protocol, with its per-field error."""
     import torch
     from hackathon_mom6_miniapp_b200 import INIT_CFG, MIXED, Model
@@ -296,7 +309,7 @@ def run_mixed(args, world, rank, local, dist, fp64_ms_per_step):
            "ms_per_step": ms / args.steps,
            "speedup_vs_fp64": fp64_ms_per_step / (ms / args.steps),
            "kernel_ms_per_step": {k: v[0] * v[1] / 2 for k, v in kt.items()},
-           "dtype": "f32 state/stencils, f64 sums/thickness update/elimination/btstep"}
+           "dtype": "f32 state/stencils/vertical elimination, f64 column sums/thickness update/btstep"}
     if rank == 0:
         out["rel_l2_720x720x75_10_steps"] = mixed_errors(NI, NJ, 10, 0, local)
         if not args.no_cfg2:
@@ -350,7 +363,7 @@ def run_ensemble(args, world, rank, local, dist):
            "tuning": e.tuning(), "autotune_best_ms": best, "autotune_s": t_tune,
            "sizes": "ni=nj from {90..360 step 30}, nk from {25,50,75}, numpy "
                     "default_rng(rank) draws, seeds 0..63",
-           "dtype": "mixed form (f32 state, f64 sums/thickness update/elimination/btstep)"}
+           "dtype": "mixed form (f32 state/stencils/vertical elimination, f64 column sums/thickness update/btstep)"}
     e.close()
     return out
 
@@ -556,7 +569,7 @@ def run_ours(args, world, rank, local, dist):
                 "surrogate": surrogate,
                 "gpu_launches": launches,
                 "clocks": ck}
-        print(json.dumps(line), flush=True)
+        print(json.dumps(_finite(line)), flush=True)
     m.close()
 
 
