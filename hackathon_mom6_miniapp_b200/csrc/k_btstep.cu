@@ -1290,8 +1290,7 @@ cudaError_t launch_btstep_tavg(const Dims& D, const Metrics& M, const UniMetrics
 // Some callers cannot allocate device memory at the point where they need
 // the barotropic loop: a Fortran host whose device arrays are owned by an
 // OpenMP-target or OpenACC runtime (map clauses; cudaMalloc from inside its
-// data regions would fragment or bypass that runtime's pool), and code that
-// must not allocate while a stream is being captured into a CUDA graph.
+// data regions would fragment or bypass that runtime's pool).
 // mom6b_btstep_noalloc therefore keeps every work array of the loop in the
 // file-scope array below, sized for grids of at most kNoAllocMaxPoints
 // points (n1 * n2), i.e. 6 x 589,824 doubles plus a 2.3 KB header, about

@@ -129,8 +129,8 @@ int mom6b_kernel_time_ms(mom6b_model *m, const char *kernel, double *avg_ms,
 /* ---- allocation-free barotropic loop ------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory where they run the barotropic solver -- a Fortran host whose device
- * arrays belong to an OpenMP-target or OpenACC runtime, or code that must not
- * allocate while a stream is being captured -- this entry point runs all
+ * arrays belong to an OpenMP-target or OpenACC runtime, which owns the device
+ * pool and which a separate cudaMalloc would bypass -- this entry point runs all
  * nstep substeps of btstep (mom6_barotropic_serial.F90:178-304; extended
  * uhbt/vhbt ranges when extended_ranges != 0, as btstep_do_step and the CUDA C
  * kernels use) and allocates nothing.  The caller passes every input, metric

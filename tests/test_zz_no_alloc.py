@@ -2,7 +2,7 @@
 
 Callers that cannot allocate device memory where they run the barotropic
 solver (a Fortran host whose device arrays belong to an OpenMP-target or
-OpenACC runtime, or code in the middle of a stream capture) get the whole
+OpenACC runtime, which owns the device pool) get the whole
 btstep loop from this entry point, with its work arrays in a static device
 array of the library.  These tests call it through the C ABI twice in a row,
 as the split RK2 step does (predictor, then corrector with aliased in/out),
