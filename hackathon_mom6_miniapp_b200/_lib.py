@@ -117,6 +117,19 @@ def library():
     L.mom6b_mlp_train.argtypes = [vp, f32p, f32p, ctypes.c_int, ctypes.c_float, ctypes.c_int,
                                   f32p]
     L.mom6b_mlp_predict.argtypes = [vp, f32p, ctypes.c_int, f32p]
+    cp, ip = ctypes.c_char_p, P(ctypes.c_int)
+    L.mom6b_diag_init.argtypes = [vp, cp, ctypes.c_int]
+    L.mom6b_diag_end.argtypes = [vp]
+    L.mom6b_diag_register.argtypes = [vp, cp, cp, cp, ctypes.c_int, cp, ctypes.c_int, ip]
+    L.mom6b_diag_post_2d.argtypes = [vp, ctypes.c_int, vp]
+    L.mom6b_diag_post_3d.argtypes = [vp, ctypes.c_int, vp]
+    L.mom6b_diag_post_product_sum_u.argtypes = [vp, ctypes.c_int, vp, vp]
+    L.mom6b_diag_post_product_sum_v.argtypes = [vp, ctypes.c_int, vp, vp]
+    L.mom6b_diag_stats.argtypes = [vp, ctypes.c_int, P(d)]
+    L.mom6b_diag_report.argtypes = [vp, ip]
+    L.mom6b_diag_driver.argtypes = [vp, ctypes.c_int]
+    L.mom6b_write_field_bin.argtypes = [vp, ctypes.c_int, cp]
+    L.mom6b_read_field_bin.argtypes = [vp, ctypes.c_int, cp]
     L.mom6b_last_error.restype = ctypes.c_char_p
     L.mom6b_version.restype = ctypes.c_char_p
     _LIB = L
@@ -236,6 +249,70 @@ class Model:
         _check(library().mom6b_kernel_time_ms(self._m, name.encode(), ctypes.byref(ms),
                                               ctypes.byref(n)))
         return ms.value, n.value
+
+    # ---- diagnostics (mom6_diag.F90) and binary dumps ----
+    def diag_init(self, output_dir="./", output_freq=1):
+        _check(library().mom6b_diag_init(self._m, str(output_dir).encode(), int(output_freq)))
+
+    def diag_end(self):
+        _check(library().mom6b_diag_end(self._m))
+
+    def diag_register(self, name, long_name, units, ndims, position, output_mode):
+        """register_diag_field: the id, -1 when inactive."""
+        i = ctypes.c_int()
+        _check(library().mom6b_diag_register(self._m, name.encode(), long_name.encode(),
+                                             units.encode(), int(ndims), position.encode(),
+                                             int(output_mode), ctypes.byref(i)))
+        return i.value
+
+    def diag_post(self, diag_id, field):
+        """post_data_2d / post_data_3d of a device field: a model field name
+        or a CUDA tensor of the model's 2-D or 3-D shape (float64)."""
+        ptr, nd = self._device_field(field)
+        fn = library().mom6b_diag_post_3d if nd == 3 else library().mom6b_diag_post_2d
+        _check(fn(self._m, int(diag_id), ptr))
+
+    def diag_post_product_sum(self, diag_id, a, b, position="u"):
+        """post_product_sum_u / _v of two device 3-D fields."""
+        pa, _ = self._device_field(a)
+        pb, _ = self._device_field(b)
+        fn = (library().mom6b_diag_post_product_sum_u if position == "u"
+              else library().mom6b_diag_post_product_sum_v)
+        _check(fn(self._m, int(diag_id), pa, pb))
+
+    def _device_field(self, f):
+        """(device pointer, 2 or 3) of a model field name, or of a contiguous
+        float64 CUDA tensor of n1*n2 or n1*n2*nk elements whose memory holds
+        the field in the reference (column-major) layout."""
+        if isinstance(f, str):
+            return ctypes.c_void_p(self.device_ptr(f)), len(self.shape(f))
+        n2d = self.n1 * self.n2
+        if not (f.is_cuda and f.dtype.is_floating_point and f.element_size() == 8
+                and f.is_contiguous() and f.numel() in (n2d, n2d * self.nk)):
+            raise ValueError("a contiguous float64 CUDA tensor of the model's 2-D or 3-D size")
+        return ctypes.c_void_p(f.data_ptr()), 2 if f.numel() == n2d else 3
+
+    def diag_stats(self, diag_id):
+        """(min, max, mean, rms) of the last post of diag_id."""
+        out = (ctypes.c_double * 4)()
+        _check(library().mom6b_diag_stats(self._m, int(diag_id), out))
+        return tuple(out)
+
+    def diag_report(self):
+        out = (ctypes.c_int * 3)()
+        _check(library().mom6b_diag_report(self._m, out))
+        return dict(zip(["registered", "post_calls", "call_count"], list(out)))
+
+    def diag_driver(self, output_mode=1):
+        """The diagnostics of rk2_serial_driver with diag_mode = 1 (KE,
+        diffu_sum, diffv_sum, mass), posted by every later step call."""
+        _check(library().mom6b_diag_driver(self._m, int(output_mode)))
+
+    def write_field_bin(self, name, path):
+        _check(library().mom6b_write_field_bin(self._m, FID[name], str(path).encode()))
+
+    def read_field_bin(self, name, path):
+        _check(library().mom6b_read_field_bin(self._m, FID[name], str(path).encode()))
 
     # ---- learned barotropic surrogate ----
     def surrogate_train(self, nstates=8, nsteps=2000, batch=65536, lr=1e-3, seed=1):

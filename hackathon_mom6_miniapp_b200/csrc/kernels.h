@@ -56,10 +56,13 @@ struct BTParams {
     long long spin_budget;     // clock64 cycles a block may wait at one barrier
 };
 
+// diffu, diffv (both or neither): also store the horizontal-viscosity
+// accelerations of the updated points (diagnostics).
 cudaError_t launch_tendency(const Dims& D, const Metrics& M, const UniMetrics& U,
                             const double* uin, const double* vin, const double* h,
                             const double* ubase, const double* vbase, double* uout,
-                            double* vout, double coef, double h_neglect, cudaStream_t s);
+                            double* vout, double coef, double h_neglect, cudaStream_t s,
+                            double* diffu = nullptr, double* diffv = nullptr);
 cudaError_t launch_vertvisc(const Dims& D, const Metrics& M, double* u, double* v,
                             const double* h, double dt, const VVParams& P,
                             double* taux_bot, double* tauy_bot, cudaStream_t s);

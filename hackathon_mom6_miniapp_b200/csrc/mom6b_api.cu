@@ -33,6 +33,7 @@
 #include <vector>
 
 #include "../../include/mom6b.h"
+#include "diag.h"
 #include "host_init.h"
 #include "kernels.h"
 #include "mlp.h"
@@ -103,6 +104,11 @@ struct mom6b_model {
     // barotropic state of the training and evaluation runs
     double *tr_e = nullptr, *tr_u = nullptr, *tr_v = nullptr;
     double *tr_ea = nullptr, *tr_ua = nullptr, *tr_va = nullptr;
+    // diagnostics (mom6_diag.F90) and the driver's four fields
+    std::unique_ptr<DiagCtrl> diag;
+    bool diag_driver = false;
+    int id_KE = -1, id_diffu_sum = -1, id_diffv_sum = -1, id_mass = -1;
+    double *dg_du = nullptr, *dg_dv = nullptr, *dg_ke = nullptr, *dg_mass = nullptr;
 };
 
 static double* dalloc(mom6b_model* m, size_t n, cudaError_t* err)
@@ -638,10 +644,11 @@ static int enqueue_step(mom6b_model* m)
             CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill_f(D, F(m->v), g.nk, 2, s); }));
         }
     } else {
-    // ---- predictor ----
+    // ---- predictor ----  (with the driver's diagnostics, diffu and diffv are kept)
     CK(timed(m, s, "tendency", [&] {
         return launch_tendency(D, M, m->U, m->u, m->v, m->h0, m->u, m->v, m->up, m->vp, dt,
-                               hv_neglect, s); }));
+                               hv_neglect, s, m->diag_driver ? m->dg_du : nullptr,
+                               m->diag_driver ? m->dg_dv : nullptr); }));
     CK(timed(m, s, "vertvisc", [&] {
         return launch_vertvisc(D, M, m->up, m->vp, m->h0, dt, VV, m->taux_bot,
                                m->tauy_bot, s); }));
@@ -767,10 +774,40 @@ static int shadow_step(mom6b_model* m)
     return MOM6B_OK;
 }
 
+// Steps with the driver's diagnostics (rk2_serial_driver.F90:299-304 and
+// :385-391): after every iteration the product sums of the predictor's diffu,
+// diffv with the predicted thickness hB (neither changes in the corrector, so
+// posting them after the whole iteration posts what the driver posts after
+// the predictor's continuity), after the last iteration KE and mass.
+static int diag_driver_steps(mom6b_model* m, int nsteps)
+{
+    cudaStream_t s = m->s3d;
+    DiagCtrl& G = *m->diag;
+    for (int n = 0; n < nsteps; ++n) {
+        if (int rc = enqueue_step(m)) return rc;
+        if (G.post_product_sum(m->id_diffu_sum, m->dg_du, m->hB, true, s) ||
+            G.post_product_sum(m->id_diffv_sum, m->dg_dv, m->hB, false, s))
+            return fail(MOM6B_ERR_CUDA, "diagnostic post failed");
+        if (int rc = check_status(m)) return rc;
+    }
+    if (nsteps > 0 && (m->id_KE > 0 || m->id_mass > 0)) {
+        if (m->id_KE > 0) {
+            CK(launch_diag_KE(m->D, m->u, m->v, m->dg_ke, s));
+            if (G.post_3d(m->id_KE, m->dg_ke, s)) return fail(MOM6B_ERR_CUDA, "diagnostic post failed");
+        }
+        if (m->id_mass > 0) {
+            CK(launch_diag_mass(m->D, m->hA, m->dg_mass, s));
+            if (G.post_2d(m->id_mass, m->dg_mass, s)) return fail(MOM6B_ERR_CUDA, "diagnostic post failed");
+        }
+    }
+    return MOM6B_OK;
+}
+
 extern "C" int mom6b_step(mom6b_model* m, int nsteps)
 {
     if (!m || nsteps < 0) return fail(MOM6B_ERR_ARG, "bad argument");
     CK(cudaSetDevice(m->cfg.device));
+    if (m->diag_driver) return diag_driver_steps(m, nsteps);
     if (m->sur && m->sur_on && !m->sur_fallen) {
         for (int n = 0; n < nsteps; ++n) {
             const bool shadow = m->sur_every > 0 && (m->sur_steps % m->sur_every) == 0 &&
@@ -1097,6 +1134,198 @@ extern "C" int mom6b_kernel_time_ms(mom6b_model* m, const char* kernel, double* 
 // of domains (ten when no domain fills halos): tendency, vertvisc, PPM edges,
 // faces and halo fill for the predictor and the corrector, then the two
 // barotropic calls with their halo fills.
+// ---------------------------------------------------------------------------
+// diagnostics (mom6_diag.F90) and binary field dumps
+// ---------------------------------------------------------------------------
+static int diag_ready(mom6b_model* m)
+{
+    if (!m) return fail(MOM6B_ERR_ARG, "null model");
+    if (!m->diag || !m->diag->initialized()) return fail(MOM6B_ERR_STATE, "diagnostics not initialized");
+    CK(cudaSetDevice(m->cfg.device));
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_diag_init(mom6b_model* m, const char* output_dir, int output_freq)
+{
+    if (!m || !output_dir) return fail(MOM6B_ERR_ARG, "null argument");
+    if (output_freq < 1) return fail(MOM6B_ERR_ARG, "output_freq must be at least 1");
+    CK(cudaSetDevice(m->cfg.device));
+    if (m->diag && m->diag->initialized()) return MOM6B_OK;   // as diag_init: once
+    m->diag.reset(new DiagCtrl());
+    if (m->diag->init(m->D, output_dir, output_freq, m->s3d))
+        return fail(MOM6B_ERR_NOMEM, "diagnostic work array");
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_diag_end(mom6b_model* m)
+{
+    if (!m) return fail(MOM6B_ERR_ARG, "null model");
+    CK(cudaSetDevice(m->cfg.device));
+    CK(cudaStreamSynchronize(m->s3d));
+    m->diag.reset();
+    m->diag_driver = false;
+    m->id_KE = m->id_diffu_sum = m->id_diffv_sum = m->id_mass = -1;
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_diag_register(mom6b_model* m, const char* name, const char* long_name,
+                                   const char* units, int ndims, const char* position,
+                                   int output_mode, int* id)
+{
+    if (int rc = diag_ready(m)) return rc;
+    if (!name || !long_name || !units || !position || !id) return fail(MOM6B_ERR_ARG, "null argument");
+    if (ndims != 2 && ndims != 3) return fail(MOM6B_ERR_ARG, "ndims must be 2 or 3");
+    *id = m->diag->register_field(name, long_name, units, ndims, position, output_mode);
+    return MOM6B_OK;
+}
+
+static int diag_post(mom6b_model* m, int id, const double* a, const double* b, int kind)
+{
+    if (int rc = diag_ready(m)) return rc;
+    if (id <= 0) return MOM6B_OK;   // inactive diagnostic: nothing to do
+    if (!m->diag->field(id)) return fail(MOM6B_ERR_ARG, "unknown diagnostic id");
+    if (!a || (kind >= 2 && !b)) return fail(MOM6B_ERR_ARG, "null field");
+    int rc;
+    switch (kind) {
+    case 0: rc = m->diag->post_2d(id, a, m->s3d); break;
+    case 1: rc = m->diag->post_3d(id, a, m->s3d); break;
+    default: rc = m->diag->post_product_sum(id, a, b, kind == 2, m->s3d); break;
+    }
+    return rc ? fail(MOM6B_ERR_CUDA, "diagnostic post failed") : MOM6B_OK;
+}
+
+extern "C" int mom6b_diag_post_2d(mom6b_model* m, int id, const double* field)
+{
+    return diag_post(m, id, field, nullptr, 0);
+}
+
+extern "C" int mom6b_diag_post_3d(mom6b_model* m, int id, const double* field)
+{
+    return diag_post(m, id, field, nullptr, 1);
+}
+
+extern "C" int mom6b_diag_post_product_sum_u(mom6b_model* m, int id, const double* u_a,
+                                             const double* u_b)
+{
+    return diag_post(m, id, u_a, u_b, 2);
+}
+
+extern "C" int mom6b_diag_post_product_sum_v(mom6b_model* m, int id, const double* v_a,
+                                             const double* v_b)
+{
+    return diag_post(m, id, v_a, v_b, 3);
+}
+
+extern "C" int mom6b_diag_stats(const mom6b_model* m, int id, double* out4)
+{
+    if (!m || !out4) return fail(MOM6B_ERR_ARG, "null argument");
+    if (!m->diag) return fail(MOM6B_ERR_STATE, "diagnostics not initialized");
+    const DiagField* F = m->diag->field(id);
+    if (!F) return fail(MOM6B_ERR_ARG, "unknown diagnostic id");
+    if (!F->posted) return fail(MOM6B_ERR_STATE, "diagnostic not posted yet");
+    for (int q = 0; q < 4; ++q) out4[q] = F->stats[q];
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_diag_report(mom6b_model* m, int* out3)
+{
+    if (int rc = diag_ready(m)) return rc;
+    std::printf("\nDiagnostic Summary:\n--------------------------------------------------\n"
+                "  Registered diagnostics:  %8d\n  Total post_data calls:   %8d\n",
+                m->diag->num_diags(), m->diag->total_calls());
+    std::fflush(stdout);
+    if (out3) {
+        out3[0] = m->diag->num_diags();
+        out3[1] = m->diag->total_calls();
+        out3[2] = m->diag->call_count();
+    }
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_diag_driver(mom6b_model* m, int output_mode)
+{
+    if (int rc = diag_ready(m)) return rc;
+    if (m->cfg.precision != MOM6B_FP64)
+        return fail(MOM6B_ERR_STATE, "the driver's diagnostics need the FP64 form");
+    if (m->sur && m->sur_on) return fail(MOM6B_ERR_STATE, "disable the surrogate first");
+    DiagCtrl& G = *m->diag;
+    m->id_KE = G.register_field("KE", "Kinetic Energy", "m2/s2", 3, "h", output_mode);
+    m->id_diffu_sum = G.register_field("diffu_sum", "Vertically summed u-diffusion", "m/s2", 2,
+                                       "u", output_mode);
+    m->id_diffv_sum = G.register_field("diffv_sum", "Vertically summed v-diffusion", "m/s2", 2,
+                                       "v", output_mode);
+    m->id_mass = G.register_field("mass", "Vertically summed thickness", "m", 2, "h",
+                                  output_mode);
+    if (!m->dg_du) {
+        cudaError_t e = cudaSuccess;
+        const size_t n3 = (size_t)m->D.plane * m->D.nk, n2 = (size_t)m->D.plane;
+        m->dg_du = dalloc(m, n3, &e);
+        m->dg_dv = dalloc(m, n3, &e);
+        m->dg_ke = dalloc(m, n3, &e);
+        m->dg_mass = dalloc(m, n2, &e);
+        if (e != cudaSuccess || !m->dg_du || !m->dg_dv || !m->dg_ke || !m->dg_mass)
+            return fail(MOM6B_ERR_NOMEM, "diagnostic fields");
+    }
+    m->diag_driver = true;
+    invalidate_graph(m);   // the predictor's tendency launch changes
+    return MOM6B_OK;
+}
+
+// the computational domain of field f <-> a column-major host block
+static int comp_domain(mom6b_model* m, int f, std::vector<double>& full, int* ni, int* nj,
+                       int* nk)
+{
+    bool is3d, w;
+    if (!field_ptr(m, f, &is3d, &w)) return fail(MOM6B_ERR_ARG, "unknown field id");
+    const HostGrid& g = *m->grid;
+    *ni = g.ie - g.is + 1;
+    *nj = g.je - g.js + 1;
+    *nk = is3d ? g.nk : 0;
+    full.resize(mom6b_field_size(m, f));
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_write_field_bin(mom6b_model* m, int f, const char* path)
+{
+    if (!m || !path) return fail(MOM6B_ERR_ARG, "null argument");
+    std::vector<double> full;
+    int ni, nj, nk;
+    if (int rc = comp_domain(m, f, full, &ni, &nj, &nk)) return rc;
+    if (int rc = mom6b_get_field(m, f, full.data(), full.size())) return rc;
+    const HostGrid& g = *m->grid;
+    const int nl = nk > 0 ? nk : 1;
+    std::vector<double> comp((size_t)ni * nj * nl);
+    for (int k = 0; k < nl; ++k)
+        for (int j = 0; j < nj; ++j)
+            for (int i = 0; i < ni; ++i)
+                comp[((size_t)k * nj + j) * ni + i] =
+                    full[(size_t)k * g.plane + (size_t)(g.js - 1 + j) * g.n1 + (g.is - 1 + i)];
+    if (diag_write_bin(path, comp.data(), ni, nj, nk) != 0)
+        return fail(MOM6B_ERR_ARG, std::string("cannot write ") + path);
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_read_field_bin(mom6b_model* m, int f, const char* path)
+{
+    if (!m || !path) return fail(MOM6B_ERR_ARG, "null argument");
+    std::vector<double> full;
+    int ni, nj, nk;
+    if (int rc = comp_domain(m, f, full, &ni, &nj, &nk)) return rc;
+    const int nl = nk > 0 ? nk : 1;
+    std::vector<double> comp((size_t)ni * nj * nl);
+    const int r = diag_read_bin(path, comp.data(), ni, nj, nk);
+    if (r == -2) return fail(MOM6B_ERR_ARG, std::string("dimensions in ") + path + " do not match");
+    if (r != 0) return fail(MOM6B_ERR_ARG, std::string("cannot read ") + path);
+    if (int rc = mom6b_get_field(m, f, full.data(), full.size())) return rc;
+    const HostGrid& g = *m->grid;
+    for (int k = 0; k < nl; ++k)
+        for (int j = 0; j < nj; ++j)
+            for (int i = 0; i < ni; ++i)
+                full[(size_t)k * g.plane + (size_t)(g.js - 1 + j) * g.n1 + (g.is - 1 + i)] =
+                    comp[((size_t)k * nj + j) * ni + i];
+    return mom6b_set_field(m, f, full.data(), full.size());
+}
+
 struct mom6b_ensemble {
     std::vector<mom6b_model*> doms;
     std::vector<EnsDomain> host;

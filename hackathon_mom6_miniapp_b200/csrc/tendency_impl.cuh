@@ -59,12 +59,15 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // double-buffered: layer k+1 is copied into shared memory (cp.async) while
 // layer k is evaluated, so the loads' latency leaves the layer loop and each
 // layer takes two barriers.
-template <int TX, int TY, bool UNI, typename R>
+// DIAG: also store the horizontal-viscosity accelerations diffu, diffv of the
+// updated points in dfu, dfv (the driver's diffu_sum / diffv_sum diagnostics).
+template <int TX, int TY, bool UNI, typename R, bool DIAG = false>
 __device__ __forceinline__ void
 tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __restrict__ uin,
               const R* __restrict__ vin, const R* __restrict__ h,
               const R* ubase, const R* vbase, R* uout, R* vout,
-              R coef, R h_neglect, int k0, int KC, int bx, int by, int bz)
+              R coef, R h_neglect, int k0, int KC, int bx, int by, int bz,
+              R* dfu = nullptr, R* dfv = nullptr)
 {
     constexpr int SX = TX + 2, SY = TY + 2;  // staged inputs: [i0-1, i0+TX] x [j0-1, j0+TY]
     constexpr int CX = TX + 1, CY = TY + 1;  // intermediates
@@ -242,6 +245,7 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
                             G2(IareaCu, I, j),
                         h_u + h_neglect);
         uout[oo] = ub + coef * (CAu + diffu);
+        if (DIAG) dfu[oo] = diffu;
     }
     // ---- v point (i, J) = (I, j) -------------------------------------------
     if (I <= D.ie && j <= D.je - 1) {
@@ -261,6 +265,7 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
                             G2(IareaCv, i, J),
                         h_v + h_neglect);
         vout[oo] = vb + coef * (CAv + diffv);
+        if (DIAG) dfv[oo] = diffv;
     }
   }  // layer loop
 #undef SU
@@ -276,33 +281,47 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
 #undef VH
 }
 
-template <int TX, int TY, bool UNI, typename R, int MINB = 1>
+template <int TX, int TY, bool UNI, typename R, int MINB = 1, bool DIAG = false>
 __global__ void __launch_bounds__(TX * TY, MINB)
 k_tendency(Dims D, Metrics M, UniMetrics U, const R* __restrict__ uin,
            const R* __restrict__ vin, const R* __restrict__ h,
            const R* ubase, const R* vbase, R* uout, R* vout,
-           R coef, R h_neglect, int k0, int KC)
+           R coef, R h_neglect, int k0, int KC, R* dfu = nullptr, R* dfv = nullptr)
 {
-    tendency_tile<TX, TY, UNI, R>(D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef,
-                                  h_neglect, k0, KC, (int)blockIdx.x, (int)blockIdx.y,
-                                  (int)blockIdx.z);
+    tendency_tile<TX, TY, UNI, R, DIAG>(D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef,
+                                        h_neglect, k0, KC, (int)blockIdx.x, (int)blockIdx.y,
+                                        (int)blockIdx.z, dfu, dfv);
 }
 
 constexpr int kTendTX = 32, kTendTY = 8, kTendKC = 5;
 
 // Host launcher: one CTA per (TX x TY) tile of the compute domain and chunk of
 // kTendKC layers.
+// dfu, dfv (both or neither): also store diffu, diffv (the diagnostic form of
+// the kernel; the step's own launches pass neither).
 template <typename R>
 cudaError_t launch_tendency_t(const Dims& D, const Metrics& M, const UniMetrics& U,
                               const R* uin, const R* vin, const R* h, const R* ubase,
                               const R* vbase, R* uout, R* vout, R coef, R h_neglect,
-                              cudaStream_t s)
+                              cudaStream_t s, R* dfu = nullptr, R* dfv = nullptr)
 {
     constexpr int TY = kTendTY;
     int nx = D.ie - D.is + 1, ny = D.je - D.js + 1;
     dim3 block(kTendTX, TY, 1);
     int nchunks = (D.nk + kTendKC - 1) / kTendKC;
     dim3 grid((nx + kTendTX - 1) / kTendTX, (ny + TY - 1) / TY, nchunks);
+    if (dfu || dfv) {
+        if (!dfu || !dfv) return cudaErrorInvalidValue;
+        if (U.valid)
+            k_tendency<kTendTX, TY, true, R, 3, true><<<grid, block, 0, s>>>(
+                D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, kTendKC,
+                dfu, dfv);
+        else
+            k_tendency<kTendTX, TY, false, R, 3, true><<<grid, block, 0, s>>>(
+                D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, kTendKC,
+                dfu, dfv);
+        return cudaGetLastError();
+    }
     // CTAs per SM the registers are held to: 4 (64 registers) is the fastest
     // uniform-metric form on B200 (FP64 tendency 2.01 ms per step against 2.13
     // at 3 and 2.62 uncapped); the 2-D metric form keeps 3 (80 registers).

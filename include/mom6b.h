@@ -44,9 +44,10 @@ enum {
 /* arithmetic forms */
 enum {
     MOM6B_FP64 = 0,  /* every field and every operation in double precision */
-    MOM6B_MIXED = 1  /* fields and stencils in single precision, the thickness
-                        update, barotropic accumulators and the vertical
-                        tridiagonal elimination in double */
+    MOM6B_MIXED = 1  /* fields, stencils and the vertical tridiagonal
+                        elimination in single precision; the continuity column
+                        sums, the thickness update and the barotropic loop in
+                        double */
 };
 
 /* field ids (get/set) */
@@ -125,6 +126,51 @@ void mom6b_reset_launch_count(mom6b_model *m);
 int mom6b_kernel_timing(mom6b_model *m, int enable);
 int mom6b_kernel_time_ms(mom6b_model *m, const char *kernel, double *avg_ms,
                          int64_t *launches);
+
+/* ---- diagnostics (mom6_diag.F90) ----------------------------------------
+ * The mini-app's diagnostic module for fields resident on the device, one
+ * per model.  mom6b_diag_init replaces diag_init (:77-112; output_freq >= 1);
+ * mom6b_diag_register replaces register_diag_field (:130-166) and gives the
+ * id (-1 for MOM6B_DIAG_NONE or when 100 fields are registered).  A post
+ * (post_data_2d / post_data_3d, :169-272; the product sums of
+ * post_product_sum_u / _v, :274-334, on the GPU) counts a call, prints
+ * "  Diag: <name> min/max/mean/rms: " and the four values of the
+ * computational domain in Fortran ES14.6 when the mode has STATS, and when
+ * it has FILE writes every output_freq-th call to
+ * <output_dir>/<name><6-digit call count>.bin: ni, nj[, nk] as int32, then
+ * the computational domain as float64, column-major (:362-431).  Posts are
+ * synchronous; fields are device arrays of the model's shape.  The product
+ * sums share one work array, which keeps the points a sum does not cover. */
+enum { MOM6B_DIAG_NONE = 0, MOM6B_DIAG_STATS = 1, MOM6B_DIAG_FILE = 2, MOM6B_DIAG_BOTH = 3 };
+int mom6b_diag_init(mom6b_model *m, const char *output_dir, int output_freq);
+int mom6b_diag_end(mom6b_model *m);
+int mom6b_diag_register(mom6b_model *m, const char *name, const char *long_name,
+                        const char *units, int ndims, const char *position,
+                        int output_mode, int *id);
+int mom6b_diag_post_2d(mom6b_model *m, int id, const double *field);
+int mom6b_diag_post_3d(mom6b_model *m, int id, const double *field);
+int mom6b_diag_post_product_sum_u(mom6b_model *m, int id, const double *u_a,
+                                  const double *u_b);
+int mom6b_diag_post_product_sum_v(mom6b_model *m, int id, const double *v_a,
+                                  const double *v_b);
+/* out4 = {min, max, mean, rms} of the last post of id. */
+int mom6b_diag_stats(const mom6b_model *m, int id, double *out4);
+/* out3 = {registered fields, post calls, call count}; prints the summary of
+ * diag_report_timing (:336-346). */
+int mom6b_diag_report(mom6b_model *m, int *out3);
+/* The diagnostics of rk2_serial_driver with diag_mode = 1 (:152-170):
+ * registers KE, diffu_sum, diffv_sum and mass with output_mode; from then on
+ * every mom6b_step iteration posts diffu_sum and diffv_sum (the predictor's
+ * horizontal viscosity summed with the predicted thickness, :299-304) and
+ * every mom6b_step call ends with KE and mass of the final state (:385-391).
+ * FP64 form only; steps then run without the CUDA graph. */
+int mom6b_diag_driver(mom6b_model *m, int output_mode);
+
+/* Dump one field's computational domain in the diagnostics' binary format
+ * (a checkpoint; mixed-form fields are written as their values in double), or
+ * restore it from such a file (the halo is left as is).  Synchronous. */
+int mom6b_write_field_bin(mom6b_model *m, int field, const char *path);
+int mom6b_read_field_bin(mom6b_model *m, int field, const char *path);
 
 /* ---- allocation-free barotropic loop ------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device

@@ -52,6 +52,12 @@ struct oracle_model {
         *CoriolisBu, *IareaCu, *IareaCv, *dxBu, *dyBu, *IdxBu, *IdyBu, *bathyT,
         *mask2dT, *mask2dBu, *mask2dCu, *mask2dCv;
 
+    /* driver diagnostics (diag_mode = 1, rk2_serial_driver.F90:149-170):
+     * diag_work is mom6_diag's persistent work_2d (mom6_diag.F90:61, zero at
+     * diag_init); the posted fields are kept for the tests */
+    int diag_on;
+    double *diag_work, *diag_usum, *diag_vsum, *diag_KE, *diag_mass;
+
     /* driver state, rk2_serial_driver.F90:59-76 (zero-initialised) */
     double *u, *v, *h, *h0, *htmp, *uh, *vh, *CAu, *CAv, *up, *vp, *diffu,
         *diffv;
@@ -466,6 +472,8 @@ void oracle_destroy(oracle_model *m) {
         &m->bt_gtot_W, &m->bt_gtot_N, &m->bt_gtot_S, &m->bt_f_4_u, &m->bt_f_4_v,
         &m->bt_rem_u, &m->bt_rem_v, &m->bt_ubt_av, &m->bt_vbt_av};
     for (size_t a = 0; a < sizeof(p) / sizeof(p[0]); ++a) free(*p[a]);
+    free(m->diag_work); free(m->diag_usum); free(m->diag_vsum);
+    free(m->diag_KE); free(m->diag_mass);
     free(m);
 }
 
@@ -1462,6 +1470,59 @@ static void vel_update(oracle_model *m, const double *ubase, const double *vbase
     }
 }
 
+/* ------------------------------------------------------------------------ */
+/* driver diagnostics: post_product_sum_u/v (mom6_diag.F90:274-334) after the */
+/* predictor continuity (rk2_serial_driver.F90:299-304), compute_and_post_KE  */
+/* and compute_and_post_mass (:664-728) after the last iteration (:385-391).  */
+/* ------------------------------------------------------------------------ */
+void oracle_diag_enable(oracle_model *m, int on) {
+    size_t n2d = (size_t)N1 * N2, n3d = n2d * m->nk;
+    m->diag_on = on;
+    if (on && !m->diag_work) {
+        m->diag_work = zalloc(n2d); m->diag_usum = zalloc(n2d); m->diag_vsum = zalloc(n2d);
+        m->diag_KE = zalloc(n3d); m->diag_mass = zalloc(n2d);
+    }
+}
+
+/* work_2d(i, j) = sum_k a(i, j, k) * b(i, j, k) over [is, ie - iu] x [js, je - jv] */
+static void diag_product_sum(oracle_model *m, const double *a, const double *b, int iu, int jv) {
+    for (int j = m->js; j <= m->je - jv; ++j)
+        for (int i = m->is; i <= m->ie - iu; ++i) A2(m->diag_work, i, j) = 0.0;
+    for (int k = 1; k <= m->nk; ++k)
+        for (int j = m->js; j <= m->je - jv; ++j)
+            for (int i = m->is; i <= m->ie - iu; ++i)
+                A2(m->diag_work, i, j) = A2(m->diag_work, i, j) + A3(a, i, j, k) * A3(b, i, j, k);
+}
+
+static void diag_end_of_call(oracle_model *m) {
+    for (int k = 1; k <= m->nk; ++k)
+        for (int j = m->js; j <= m->je; ++j)
+            for (int i = m->is; i <= m->ie; ++i) {
+                double u0 = A3(m->u, i, j, k), u1 = A3(m->u, i - 1, j, k);
+                double v0 = A3(m->v, i, j, k), v1 = A3(m->v, i, j - 1, k);
+                A3(m->diag_KE, i, j, k) = 0.5 * (0.5 * (u0 * u0 + u1 * u1) + 0.5 * (v0 * v0 + v1 * v1));
+            }
+    memset(m->diag_mass, 0, (size_t)N1 * N2 * sizeof(double));
+    for (int k = 1; k <= m->nk; ++k)
+        for (int j = m->js; j <= m->je; ++j)
+            for (int i = m->is; i <= m->ie; ++i)
+                A2(m->diag_mass, i, j) = A2(m->diag_mass, i, j) + A3(m->h, i, j, k);
+}
+
+/* which: 0 the field posted by the last diffu_sum post, 1 diffv_sum, 2 KE (3-D),
+ * 3 mass; the computational domain of each is what the GPU posts */
+int oracle_diag_get(const oracle_model *m, int which, double *out) {
+    size_t n2d = (size_t)N1 * N2;
+    if (!m->diag_on) return -1;
+    switch (which) {
+    case 0: memcpy(out, m->diag_usum, n2d * sizeof(double)); return 0;
+    case 1: memcpy(out, m->diag_vsum, n2d * sizeof(double)); return 0;
+    case 2: memcpy(out, m->diag_KE, n2d * m->nk * sizeof(double)); return 0;
+    case 3: memcpy(out, m->diag_mass, n2d * sizeof(double)); return 0;
+    default: return -1;
+    }
+}
+
 static void one_step(oracle_model *m) {
     size_t n3d = (size_t)N1 * N2 * m->nk;
     double dt = m->dt;
@@ -1474,6 +1535,13 @@ static void one_step(oracle_model *m) {
     oracle_vert_visc(m, m->up, m->vp, m->h, dt);
     oracle_btstep(m, m->eta, m->ubt, m->vbt, m->ubt_av, m->vbt_av, m->eta_av);
     oracle_continuity(m, m->up, m->h0, m->h, m->uh, dt);
+    if (m->diag_on) {
+        size_t n2d = (size_t)N1 * N2;
+        diag_product_sum(m, m->diffu, m->h, 1, 0);
+        memcpy(m->diag_usum, m->diag_work, n2d * sizeof(double));
+        diag_product_sum(m, m->diffv, m->h, 0, 1);
+        memcpy(m->diag_vsum, m->diag_work, n2d * sizeof(double));
+    }
     if (m->cfg.bc_fill) {
         oracle_halo_fill(m, m->h, m->nk, 0);
         oracle_halo_fill(m, m->up, m->nk, 1);
@@ -1504,6 +1572,7 @@ static void one_step(oracle_model *m) {
 
 void oracle_step(oracle_model *m, int nsteps) {
     for (int s = 0; s < nsteps; ++s) one_step(m);
+    if (m->diag_on && nsteps > 0) diag_end_of_call(m);
 }
 
 /* ------------------------------------------------------------------------ */

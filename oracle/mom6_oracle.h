@@ -73,6 +73,14 @@ void oracle_destroy(oracle_model *m);
 /* One split RK2 iteration of rk2_serial_driver.F90:218-399 per call. */
 void oracle_step(oracle_model *m, int nsteps);
 
+/* Driver diagnostics (rk2_serial_driver.F90 with diag_mode = 1): when on,
+ * every step records the fields its diffu_sum and diffv_sum posts carry
+ * (mom6_diag's persistent work_2d after each product sum) and each
+ * oracle_step call ends with KE and mass of the final state.  which: 0
+ * diffu_sum, 1 diffv_sum, 2 KE (n1*n2*nk), 3 mass (n1*n2). */
+void oracle_diag_enable(oracle_model *m, int on);
+int oracle_diag_get(const oracle_model *m, int which, double *out);
+
 /* Field access: element count = n1*n2 (2-D) or n1*n2*nk (3-D). */
 size_t oracle_field_size(const oracle_model *m, int field);
 int oracle_get(const oracle_model *m, int field, double *out);

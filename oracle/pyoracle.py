@@ -78,6 +78,9 @@ def lib(parallel=False):
         L.oracle_array.restype = ctypes.c_int
         L.oracle_set_threads.argtypes = [ctypes.c_int]
         L.oracle_set_threads.restype = ctypes.c_int
+        L.oracle_diag_enable.argtypes = [vp, ctypes.c_int]
+        L.oracle_diag_get.argtypes = [vp, ctypes.c_int, P(d)]
+        L.oracle_diag_get.restype = ctypes.c_int
         _LIBS[parallel] = L
     return _LIBS[parallel]
 
@@ -145,6 +148,21 @@ class Oracle:
 
     def step(self, n=1):
         self._L.oracle_step(self._m, int(n))
+
+    DIAG_FIELDS = {"diffu_sum": 0, "diffv_sum": 1, "KE": 2, "mass": 3}
+
+    def diag_enable(self, on=True):
+        """Record the driver's diagnostics (rk2_serial_driver.F90 with
+        diag_mode = 1) from the next step on."""
+        self._L.oracle_diag_enable(self._m, int(bool(on)))
+
+    def diag_get(self, name):
+        """The field the last post of diagnostic `name` carried (full array;
+        the posts use its computational domain)."""
+        a = self.empty("h" if name == "KE" else "eta")
+        if self._L.oracle_diag_get(self._m, self.DIAG_FIELDS[name], _ptr(a)) != 0:
+            raise RuntimeError("diagnostics are not enabled")
+        return a
 
     def verify(self):
         out = (ctypes.c_double * 7)()
