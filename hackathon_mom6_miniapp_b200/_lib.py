@@ -13,9 +13,14 @@ FP64, MIXED = 0, 1
 FIELDS = ["u", "v", "h", "h0", "uh", "vh", "up", "vp", "eta", "ubt", "vbt",
           "ubt_av", "vbt_av", "eta_av", "hu_bt", "FA_u_W0", "FA_u_WW",
           "FA_u_E0", "FA_u_EE", "uBT_WW", "uBT_EE", "du_cor", "taux_bot",
-          "tauy_bot", "taux", "tauy", "Ray_u", "Ray_v"]
+          "tauy_bot", "taux", "tauy", "Ray_u", "Ray_v",
+          # ids 28..31: the oracle's Coriolis and viscosity fields (no model buffer)
+          "CAu", "CAv", "diffu", "diffv",
+          # the meridional continuity's outputs (Model.set_continuity_merid)
+          "hv_bt", "FA_v_S0", "FA_v_SS", "FA_v_N0", "FA_v_NN", "vBT_SS", "vBT_NN", "dv_cor"]
 FID = {n: i for i, n in enumerate(FIELDS)}
-FIELDS_3D = {"u", "v", "h", "h0", "uh", "vh", "up", "vp", "hu_bt", "Ray_u", "Ray_v"}
+FIELDS_3D = {"u", "v", "h", "h0", "uh", "vh", "up", "vp", "hu_bt", "Ray_u", "Ray_v", "CAu",
+             "CAv", "diffu", "diffv", "hv_bt"}
 
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of memory",
           4: "grid barrier timeout", 5: "invalid state"}
@@ -129,6 +134,8 @@ def library():
     L.mom6b_diag_report.argtypes = [vp, ip]
     L.mom6b_diag_driver.argtypes = [vp, ctypes.c_int]
     L.mom6b_write_field_bin.argtypes = [vp, ctypes.c_int, cp]
+    L.mom6b_set_continuity_merid.argtypes = [vp, ctypes.c_int]
+    L.mom6b_continuity_pass.argtypes = [vp, ctypes.c_int, ctypes.c_double]
     L.mom6b_read_field_bin.argtypes = [vp, ctypes.c_int, cp]
     L.mom6b_last_error.restype = ctypes.c_char_p
     L.mom6b_version.restype = ctypes.c_char_p
@@ -249,6 +256,15 @@ class Model:
         _check(library().mom6b_kernel_time_ms(self._m, name.encode(), ctypes.byref(ms),
                                               ctypes.byref(n)))
         return ms.value, n.value
+
+    def set_continuity_merid(self, on=True):
+        """Zonal then meridional continuity in every step (FP64 form)."""
+        _check(library().mom6b_set_continuity_merid(self._m, int(bool(on))))
+
+    def continuity_pass(self, direction, dt):
+        """One continuity pass ("x" or "y") from (u or v, h0) into h."""
+        _check(library().mom6b_continuity_pass(self._m, {"x": 0, "y": 1}[direction],
+                                               float(dt)))
 
     # ---- diagnostics (mom6_diag.F90) and binary dumps ----
     def diag_init(self, output_dir="./", output_freq=1):

@@ -27,6 +27,8 @@ struct Metrics {
     // forcing (rk2_serial_driver.F90:508-542)
     const double *taux, *tauy, *Ray_u, *Ray_v;
     const unsigned char *ray_layer_u, *ray_layer_v; // 1 where the layer is nonzero
+    // meridional continuity
+    const double *dyT, *IdyT;
 };
 
 struct Dims {

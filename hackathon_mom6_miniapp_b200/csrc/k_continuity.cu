@@ -228,6 +228,10 @@ struct FaceCol {
     EI estride;          // layer stride of hWc/hEc (plane, or the smem row length)
     double dy;           // dy_Cu(I, j) (times por_face_areaU = 1)
     double IdxT_i, IdxT_ip1;
+    // meridional faces (Y): offsets of the next cell (J + 1) in the h and
+    // edge arrays; zonal faces use the next element
+    size_t nbh = 1;
+    EI nbe = 1;
 };
 
 // The inputs of one layer of one face: u(I) and the cell values of the two
@@ -250,34 +254,38 @@ constexpr bool kContHints = MOM6B_CONT_HINTS != 0;
 // LAST: the face's last pass over its column; u and the global edge arrays
 // are then read with the evict-first hint (nothing reads them again), which
 // leaves L2 to the columns whose Newton passes are still to come.
-template <bool LAST = false, typename EI>
+// Y: a meridional face (i, J) whose cells are (i, J) and (i, J + 1); the
+// "W"/"E" edges are then the south/north edges.
+template <bool LAST = false, bool Y = false, typename EI>
 __device__ __forceinline__ LayerVals load_layer(const FaceCol<EI>& F, int k)
 {
     const size_t o = (size_t)(k - 1) * F.plane;
     const EI oe = (EI)(k - 1) * F.estride;
+    const size_t nh = Y ? F.nbh : (size_t)1;
+    const EI ne = Y ? F.nbe : (EI)1;
     LayerVals L;
     if constexpr (LAST && sizeof(EI) == sizeof(size_t)) {
         L.u = __ldcs(F.u + o);
         L.hWi = __ldcs(F.hWc + oe); L.hEi = __ldcs(F.hEc + oe);
-        L.hWp = __ldcs(F.hWc + oe + 1); L.hEp = __ldcs(F.hEc + oe + 1);
+        L.hWp = __ldcs(F.hWc + oe + ne); L.hEp = __ldcs(F.hEc + oe + ne);
     } else {
         L.u = F.u[o];
         L.hWi = F.hWc[oe]; L.hEi = F.hEc[oe];
-        L.hWp = F.hWc[oe + 1]; L.hEp = F.hEc[oe + 1];
+        L.hWp = F.hWc[oe + ne]; L.hEp = F.hEc[oe + ne];
     }
-    L.hi = F.hc[o]; L.hp = F.hc[o + 1];
+    L.hi = F.hc[o]; L.hp = F.hc[o + nh];
     return L;
 }
 
 // Visit layers 1..nz in order, fn(k, LayerVals).
-template <int CH, bool LAST = false, typename EI, typename Fn>
+template <int CH, bool LAST = false, bool Y = false, typename EI, typename Fn>
 __device__ __forceinline__ void for_layers(const FaceCol<EI>& F, int nz, Fn&& fn)
 {
     for (int kt = 1; kt <= nz; kt += CH) {
         LayerVals L[CH];
 #pragma unroll
         for (int c = 0; c < CH; ++c)
-            if (kt + c <= nz) L[c] = load_layer<LAST>(F, kt + c);
+            if (kt + c <= nz) L[c] = load_layer<LAST, Y>(F, kt + c);
 #pragma unroll
         for (int c = 0; c < CH; ++c)
             if (kt + c <= nz) fn(kt + c, L[c]);
@@ -382,7 +390,7 @@ __device__ __forceinline__ bool newton_iter(Newton& S, int itt, double tol_eta_d
 // zero-transport solve (:1002), live only when it is needed.  The two are
 // independent iterations, each with its own operation sequence; sharing the
 // column passes only halves how often the column is read.
-template <int CH, typename EI>
+template <int CH, typename EI, bool Y = false>
 __device__ void flux_adjust_pair(const FaceCol<EI>& F, int nz, double dt, double uhbt,
                                  double tol_eta_dt_fac, Newton& A, Newton& B,
                                  double* uh_out, size_t uh_stride)
@@ -397,7 +405,7 @@ __device__ void flux_adjust_pair(const FaceCol<EI>& F, int nz, double dt, double
         if (!pa && !pb) break;
         const double duA = A.du, duB = B.du;
         double eA = -uhbt, sA = 0.0, eB = -0.0, sB = 0.0;
-        for_layers<CH>(F, nz, [&](int k, const LayerVals& L) {
+        for_layers<CH, false, Y>(F, nz, [&](int k, const LayerVals& L) {
             if (pa) {
                 double hm;
                 double uhk = flux_eval(F, L, L.u + duA, dt, hm);
@@ -428,7 +436,7 @@ __device__ void flux_adjust_pair(const FaceCol<EI>& F, int nz, double dt, double
 // One zonal_flux_adjust solve on its own (:813-903): the transports of every
 // evaluated iterate go to uh_out when it is given (then the last iterate is
 // evaluated even at max_itts), otherwise passes run only to update.
-template <int CH, typename EI>
+template <int CH, typename EI, bool Y = false>
 __device__ void flux_adjust_one(const FaceCol<EI>& F, int nz, double dt, double target,
                                 double tol_eta_dt_fac, Newton& S, double* uh_out,
                                 size_t uh_stride)
@@ -440,7 +448,7 @@ __device__ void flux_adjust_one(const FaceCol<EI>& F, int nz, double dt, double 
         if (!update && !uh_out) break;
         const double du = S.du;
         double e = -target, sm = 0.0;
-        for_layers<CH>(F, nz, [&](int k, const LayerVals& L) {
+        for_layers<CH, false, Y>(F, nz, [&](int k, const LayerVals& L) {
             double hm;
             double uhk = flux_eval(F, L, L.u + du, dt, hm);
             if (uh_out) uh_out[(size_t)(k - 1) * uh_stride] = uhk;
@@ -461,22 +469,29 @@ __device__ void flux_adjust_one(const FaceCol<EI>& F, int nz, double dt, double 
 // transports (the output array, or the CTA's overlap column).
 // LOCK: the two solves in lockstep (one column pass serves both) or one
 // after the other (fewer live registers; the second runs only for uhbt /= 0).
-template <int CH, typename EI, bool LOCK = true>
+// Y: the face is the meridional face (I, j) = (i, J) and every metric is
+// its meridional counterpart (dyT, mask2dCv, dyCv; the cell beyond is
+// (i, J + 1)); the operations are the zonal ones.
+template <int CH, typename EI, bool LOCK = true, bool Y = false>
 __device__ __forceinline__ void face_work(const Dims& D, const Metrics& M, FaceCol<EI>& F,
                                           int I, int j, size_t f0, double* uh, size_t ust,
                                           bool owner, const double* uhbt2d, const ContOut& O,
                                           double dt)
 {
     const int nz = D.nk;
+    auto at = [&](const double* a) { return MOM6B_A2(a, I, j, D); };
+    auto beyond = [&](const double* a) {
+        return Y ? MOM6B_A2(a, I, j + 1, D) : MOM6B_A2(a, I + 1, j, D);
+    };
     // initial fluxes and their column sums (:305-355), and the CFL limits
     // (:335-433, vol_CFL = aggress_adjust = .false.) from the same u values
     const double CFL_dt = 0.5 / dt;
-    const double dx_W = MOM6B_A2(M.dxT, I, j, D), dx_E = MOM6B_A2(M.dxT, I + 1, j, D);
-    const double mCu = MOM6B_A2(M.mask2dCu, I, j, D);
+    const double dx_W = at(Y ? M.dyT : M.dxT), dx_E = beyond(Y ? M.dyT : M.dxT);
+    const double mCu = at(Y ? M.mask2dCv : M.mask2dCu);
     double du_max_CFL = 2.0 * (CFL_dt * dx_W);
     double du_min_CFL = -(2.0 * (CFL_dt * dx_E));
     double uh_tot_0 = 0.0, duhdu_tot_0 = 0.0;
-    for_layers<CH>(F, nz, [&](int k, const LayerVals& L) {
+    for_layers<CH, false, Y>(F, nz, [&](int k, const LayerVals& L) {
         double hm;
         double uhk = flux_eval(F, L, L.u, dt, hm);
         uh[(size_t)(k - 1) * ust] = uhk;
@@ -489,8 +504,8 @@ __device__ __forceinline__ void face_work(const Dims& D, const Metrics& M, FaceC
     du_max_CFL = dmax(du_max_CFL, 0.0);
     du_min_CFL = dmin(du_min_CFL, 0.0);
 
-    const double fac = dt * dmin(MOM6B_A2(M.IareaT, I, j, D), MOM6B_A2(M.IareaT, I + 1, j, D));
-    const double uhbt = MOM6B_A2(uhbt2d, I, j, D);
+    const double fac = dt * dmin(at(M.IareaT), beyond(M.IareaT));
+    const double uhbt = at(uhbt2d);
     // zonal_flux_adjust (A) and, for the owner with uhbt /= 0, the
     // zero-transport solve of set_zonal_BT_cont (B, :991-1002); with uhbt = 0
     // B would repeat A exactly, so du0 = du.
@@ -499,17 +514,17 @@ __device__ __forceinline__ void face_work(const Dims& D, const Metrics& M, FaceC
     if (LOCK) {
         Newton A = newton_start(uh_tot_0 - uhbt, duhdu_tot_0, du_max_CFL, du_min_CFL, true);
         Newton B = newton_start(uh_tot_0 - 0.0, duhdu_tot_0, du_max_CFL, du_min_CFL, solve0);
-        flux_adjust_pair<CH>(F, nz, dt, uhbt, fac, A, B, uh, ust);
+        flux_adjust_pair<CH, EI, Y>(F, nz, dt, uhbt, fac, A, B, uh, ust);
         du = A.du;
         du0 = solve0 ? B.du : du;
     } else {
         Newton A = newton_start(uh_tot_0 - uhbt, duhdu_tot_0, du_max_CFL, du_min_CFL, true);
-        flux_adjust_one<CH>(F, nz, dt, uhbt, fac, A, uh, ust);
+        flux_adjust_one<CH, EI, Y>(F, nz, dt, uhbt, fac, A, uh, ust);
         du = A.du;
         du0 = du;
         if (solve0) {
             Newton B = newton_start(uh_tot_0 - 0.0, duhdu_tot_0, du_max_CFL, du_min_CFL, true);
-            flux_adjust_one<CH>(F, nz, dt, 0.0, fac, B, (double*)nullptr, 0);
+            flux_adjust_one<CH, EI, Y>(F, nz, dt, 0.0, fac, B, (double*)nullptr, 0);
             du0 = B.du;
         }
     }
@@ -518,7 +533,7 @@ __device__ __forceinline__ void face_work(const Dims& D, const Metrics& M, FaceC
 
     // set_zonal_BT_cont (:991-1121)
     const double Idt = 1.0 / dt;
-    const double du_CFL = (F32(1e-6) * Idt) * MOM6B_A2(M.dxCu, I, j, D);
+    const double du_CFL = (F32(1e-6) * Idt) * at(Y ? M.dyCv : M.dxCu);
     double duR = dmin(0.0, du0 - du_CFL);
     double duL = dmax(0.0, du0 + du_CFL);
     // visc_rem_lim = max(1, 0.1 * 1) = 1 > 0 on every layer
@@ -529,7 +544,7 @@ __device__ __forceinline__ void face_work(const Dims& D, const Metrics& M, FaceC
     double FAmt_0 = 0.0, FAmt_L = 0.0, FAmt_R = 0.0, uhtot_L = 0.0, uhtot_R = 0.0;
     double* h_u = O.h_u + f0;
     const bool same = (du0 == du);
-    for_layers<CH, kContHints>(F, nz, [&](int k, const LayerVals& L) {
+    for_layers<CH, kContHints, Y>(F, nz, [&](int k, const LayerVals& L) {
         const double uk = L.u;
         double hm0, hmL, hmR;
         flux_eval(F, L, uk + du0, dt, hm0);
@@ -628,6 +643,108 @@ k_cont_faces(Dims D, Metrics M, const double* __restrict__ u,
     }
     __syncthreads();  // the CTA's transport columns are complete and visible
     cell_convergence(D, M, I, j, hin, ovl, O, dt);
+}
+
+// ---------------------------------------------------------------------------
+// Meridional continuity: the zonal algorithm on the v faces (i, J), J in
+// [js-1, je], i in [is, ie] -- the same operations with y in place of x
+// (continuity_PPM of MOM6 runs this pass after the zonal one; the reference
+// mini-app is zonal only, mom6_continuity_serial.F90:143).
+// ---------------------------------------------------------------------------
+// PPM edges along y of cell (i, j), j in [js-1, je+1]: ppm_stencil over
+// h(i, j-2 .. j+2); hS / hN take the places of h_W / h_E.
+__global__ void __launch_bounds__(128)
+k_ppm_edges_y(Dims D, Metrics M, const double* __restrict__ hin, double* __restrict__ hS,
+              double* __restrict__ hN, double h_min)
+{
+    const int i = D.is + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int j = D.js - 1 + (int)blockIdx.y;
+    const int k = 1 + (int)blockIdx.z;
+    if (i > D.ie) return;
+    const ptrdiff_t cm = (ptrdiff_t)(j - 1) * D.n1 + (i - 1);
+    const ptrdiff_t c = (ptrdiff_t)(k - 1) * D.plane + cm;
+    double h[5], m[5];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+        h[q] = hin[c + (ptrdiff_t)(q - 2) * D.n1];
+        m[q] = M.mask2dT[cm + (ptrdiff_t)(q - 2) * D.n1];
+    }
+    double hL, hR;
+    ppm_stencil(h, m, h_min, hL, hR);
+    hS[c] = hL;
+    hN[c] = hR;
+}
+
+// kYTX columns x kYTY face rows per CTA; consecutive CTAs in y overlap by one
+// face row, whose transports the upper CTA keeps in its overlap columns
+// ([CTA][column][nk]) -- the zonal kernel's scheme along y.
+constexpr int kYTX = 32, kYTY = 8;
+
+size_t continuity_overlap_doubles_y(const Dims& D)
+{
+    const int nfaces = D.je - (D.js - 1) + 1;
+    const size_t nbx = (size_t)(D.ie - D.is + 1 + kYTX - 1) / kYTX;
+    const size_t nby = (size_t)(nfaces - 1 + kYTY - 2) / (kYTY - 1);
+    return nbx * nby * kYTX * (size_t)D.nk;
+}
+
+template <int CH, int MINB>
+__global__ void __launch_bounds__(kYTX * kYTY, MINB)
+k_cont_faces_y(Dims D, Metrics M, const double* __restrict__ v, const double* __restrict__ hin,
+               const double* __restrict__ hS, const double* __restrict__ hN,
+               const double* __restrict__ vhbt2d, ContOut O, double* vh_ovl, double dt)
+{
+    const int nz = D.nk;
+    const int tx = (int)threadIdx.x, ty = (int)threadIdx.y;
+    const int i = D.is + (int)blockIdx.x * kYTX + tx;
+    const int J = D.js - 1 + (int)blockIdx.y * (kYTY - 1) + ty;
+    const bool owner = ty >= 1 || blockIdx.y == 0;
+    double* ovl = vh_ovl + (((size_t)blockIdx.y * gridDim.x + blockIdx.x) * kYTX + tx) * (size_t)nz;
+    if (i <= D.ie && J <= D.je) {
+        const size_t f0 = (size_t)(J - 1) * D.n1 + (i - 1);
+        FaceCol<size_t> F;
+        F.u = v + f0; F.hc = hin + f0; F.hWc = hS + f0; F.hEc = hN + f0;
+        F.plane = (size_t)D.plane;
+        F.estride = (size_t)D.plane;
+        F.nbh = (size_t)D.n1;
+        F.nbe = (size_t)D.n1;
+        F.dy = MOM6B_A2(M.dxCv, i, J, D);          // width of the v face
+        F.IdxT_i = MOM6B_A2(M.IdyT, i, J, D);
+        F.IdxT_ip1 = MOM6B_A2(M.IdyT, i, J + 1, D);
+        double* vh = owner ? O.uh + f0 : ovl;
+        const size_t vst = owner ? F.plane : 1;
+        face_work<CH, size_t, false, true>(D, M, F, i, J, f0, vh, vst, owner, vhbt2d, O, dt);
+    }
+    __syncthreads();  // the CTA's transport columns are complete and visible
+    // continuity_merid_convergence of cell (i, j = J): faces J-1 (row ty-1) and J
+    if (ty >= 1 && i <= D.ie && J >= D.js && J <= D.je) {
+        const size_t c0 = (size_t)(J - 1) * D.n1 + (i - 1);
+        const double fac = dt * MOM6B_A2(M.IareaT, i, J, D);
+        const bool from_ovl = ty == 1 && blockIdx.y > 0;
+        for (int k = 1; k <= nz; ++k) {
+            const size_t o = (size_t)(k - 1) * D.plane + c0;
+            const double vh_s = from_ovl ? ovl[k - 1] : O.uh[o - D.n1];
+            const double hn = dmax(hin[o] - fac * (O.uh[o] - vh_s), 0.0);
+            if (kContHints) __stcs(O.h + o, hn);
+            else O.h[o] = hn;
+        }
+    }
+}
+
+cudaError_t launch_continuity_y(const Dims& D, const Metrics& M, const double* v,
+                                const double* hin, double* hS, double* hN,
+                                const double* vhbt, const ContOut& O, double* vh_ovl,
+                                double dt, double h_min, cudaStream_t s)
+{
+    {
+        dim3 grid((D.ie - D.is + 1 + 127) / 128, D.je - D.js + 3, D.nk);
+        k_ppm_edges_y<<<grid, 128, 0, s>>>(D, M, hin, hS, hN, h_min);
+    }
+    const int nfaces = D.je - (D.js - 1) + 1;
+    dim3 grid((D.ie - D.is + 1 + kYTX - 1) / kYTX, (nfaces - 1 + kYTY - 2) / (kYTY - 1), 1);
+    k_cont_faces_y<4, 2><<<grid, dim3(kYTX, kYTY, 1), 0, s>>>(D, M, v, hin, hS, hN, vhbt, O,
+                                                              vh_ovl, dt);
+    return cudaGetLastError();
 }
 
 // Fused variant: the PPM edges of the CTA's cells are computed straight into

@@ -69,6 +69,14 @@ cudaError_t launch_vertvisc(const Dims& D, const Metrics& M, double* u, double* 
 // uh_ovl: scratch of continuity_overlap_doubles(D) doubles holding the
 // recomputed overlap face column of every CTA.
 size_t continuity_overlap_doubles(const Dims& D);
+// Meridional continuity (v faces; O.uh receives vh, O.h_u h_v and the BT_cont
+// fields their meridional counterparts); vh_ovl holds
+// continuity_overlap_doubles_y(D) doubles; hS, hN are scratch like hW, hE.
+size_t continuity_overlap_doubles_y(const Dims& D);
+cudaError_t launch_continuity_y(const Dims& D, const Metrics& M, const double* v,
+                                const double* hin, double* hS, double* hN,
+                                const double* vhbt, const ContOut& O, double* vh_ovl,
+                                double dt, double h_min, cudaStream_t s);
 cudaError_t launch_continuity(const Dims& D, const Metrics& M, const double* u,
                               const double* hin, double* hW, double* hE,
                               const double* uhbt, const ContOut& O, double* uh_ovl,

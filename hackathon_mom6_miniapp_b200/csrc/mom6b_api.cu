@@ -109,6 +109,11 @@ struct mom6b_model {
     bool diag_driver = false;
     int id_KE = -1, id_diffu_sum = -1, id_diffv_sum = -1, id_mass = -1;
     double *dg_du = nullptr, *dg_dv = nullptr, *dg_ke = nullptr, *dg_mass = nullptr;
+    // meridional continuity: intermediate thickness, vh, h_v, BT_cont's v fields
+    bool merid = false;
+    double *hZ = nullptr, *vh = nullptr, *h_v = nullptr, *vh_ovl = nullptr;
+    double *FA_v_S0 = nullptr, *FA_v_SS = nullptr, *FA_v_N0 = nullptr, *FA_v_NN = nullptr;
+    double *vBT_SS = nullptr, *vBT_NN = nullptr, *dv_cor = nullptr;
 };
 
 static double* dalloc(mom6b_model* m, size_t n, cudaError_t* err)
@@ -324,7 +329,8 @@ extern "C" int mom6b_create(const mom6b_config* cfg, mom6b_model** out)
         {&m->M.Kh_xx, &g.Kh_xx}, {&m->M.Kh_xy, &g.Kh_xy}, {&m->M.Datu, &g.Datu},
         {&m->M.Datv, &g.Datv}, {&m->M.gtot_E, &g.gtot_E}, {&m->M.gtot_W, &g.gtot_W},
         {&m->M.gtot_N, &g.gtot_N}, {&m->M.gtot_S, &g.gtot_S},
-        {&m->M.bt_rem_u, &g.bt_rem_u}, {&m->M.bt_rem_v, &g.bt_rem_v}};
+        {&m->M.bt_rem_u, &g.bt_rem_u}, {&m->M.bt_rem_v, &g.bt_rem_v},
+        {&m->M.dyT, &g.dyT}, {&m->M.IdyT, &g.IdyT}};
     for (auto& up : ups) {
         double* p = A2();
         if (!p) return fail(MOM6B_ERR_NOMEM, "device allocation failed");
@@ -583,6 +589,39 @@ static int enqueue_shadow_chain(mom6b_model* m, cudaStream_t s)
     return MOM6B_OK;
 }
 
+// The FP64 continuity of one half step: zonal from hin into O.h or, with the
+// meridional pass, zonal into hZ (a copy of hin, halo filled when bc_fill)
+// and meridional from hZ into O.h.
+static cudaError_t continuity_pass(mom6b_model* m, cudaStream_t s, const double* u,
+                                   const double* v, const double* hin, const ContOut& O,
+                                   double dt)
+{
+    const Dims& D = m->D;
+    const double h_min = step_h_min();
+    if (!m->merid)
+        return timed(m, s, "continuity", [&] {
+            return launch_continuity(D, m->M, u, hin, m->hW, m->hE, m->uhbt0, O, m->uh_ovl,
+                                     dt, h_min, s); });
+    ContOut OZ = O;
+    OZ.h = m->hZ;
+    cudaError_t e = cudaMemcpyAsync(m->hZ, hin, (size_t)D.plane * D.nk * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, s);
+    if (e != cudaSuccess) return e;
+    e = timed(m, s, "continuity", [&] {
+        return launch_continuity(D, m->M, u, hin, m->hW, m->hE, m->uhbt0, OZ, m->uh_ovl, dt,
+                                 h_min, s); });
+    if (e != cudaSuccess) return e;
+    if (m->cfg.bc_fill) {
+        e = timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->hZ, D.nk, 0, s); });
+        if (e != cudaSuccess) return e;
+    }
+    ContOut OV{O.h, m->vh, m->h_v, m->FA_v_S0, m->FA_v_SS, m->FA_v_N0, m->FA_v_NN,
+               m->vBT_SS, m->vBT_NN, m->dv_cor};
+    return timed(m, s, "continuity", [&] {
+        return launch_continuity_y(D, m->M, v, m->hZ, m->hW, m->hE, m->uhbt0, OV, m->vh_ovl, dt,
+                                   h_min, s); });
+}
+
 static int enqueue_step(mom6b_model* m)
 {
     const Dims& D = m->D;
@@ -652,9 +691,7 @@ static int enqueue_step(mom6b_model* m)
     CK(timed(m, s, "vertvisc", [&] {
         return launch_vertvisc(D, M, m->up, m->vp, m->h0, dt, VV, m->taux_bot,
                                m->tauy_bot, s); }));
-    CK(timed(m, s, "continuity", [&] {
-        return launch_continuity(D, M, m->up, m->h0, m->hW, m->hE, m->uhbt0, OB,
-                                 m->uh_ovl, dt, h_min, s); }));
+    CK(continuity_pass(m, s, m->up, m->vp, m->h0, OB, dt));
     if (c.bc_fill) {
         CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->hB, g.nk, 0, s); }));
         CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->up, g.nk, 1, s); }));
@@ -667,9 +704,7 @@ static int enqueue_step(mom6b_model* m)
     CK(timed(m, s, "vertvisc", [&] {
         return launch_vertvisc(D, M, m->u, m->v, m->hB, 0.5 * dt, VV, m->taux_bot,
                                m->tauy_bot, s); }));
-    CK(timed(m, s, "continuity", [&] {
-        return launch_continuity(D, M, m->u, m->hB, m->hW, m->hE, m->uhbt0, OA,
-                                 m->uh_ovl, 0.5 * dt, h_min, s); }));
+    CK(continuity_pass(m, s, m->u, m->v, m->hB, OA, 0.5 * dt));
     if (c.bc_fill) {
         CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->hA, g.nk, 0, s); }));
         CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->u, g.nk, 1, s); }));
@@ -878,6 +913,8 @@ static double* field_ptr(mom6b_model* m, int f, bool* is3d, bool* writable)
     case MOM6B_F_HU_BT: return m->h_u;
     case MOM6B_F_RAY_U: return m->Ray_u;
     case MOM6B_F_RAY_V: return m->Ray_v;
+    case MOM6B_F_VH: return m->vh;
+    case MOM6B_F_HV_BT: return m->h_v;
     default: break;
     }
     *is3d = false;
@@ -899,6 +936,13 @@ static double* field_ptr(mom6b_model* m, int f, bool* is3d, bool* writable)
     case MOM6B_F_TAUY_BOT: return m->tauy_bot;
     case MOM6B_F_TAUX: return m->taux;
     case MOM6B_F_TAUY: return m->tauy;
+    case MOM6B_F_FA_V_S0: return m->FA_v_S0;
+    case MOM6B_F_FA_V_SS: return m->FA_v_SS;
+    case MOM6B_F_FA_V_N0: return m->FA_v_N0;
+    case MOM6B_F_FA_V_NN: return m->FA_v_NN;
+    case MOM6B_F_VBT_SS: return m->vBT_SS;
+    case MOM6B_F_VBT_NN: return m->vBT_NN;
+    case MOM6B_F_DV_COR: return m->dv_cor;
     default: return nullptr;
     }
 }
@@ -1268,6 +1312,55 @@ extern "C" int mom6b_diag_driver(mom6b_model* m, int output_mode)
     }
     m->diag_driver = true;
     invalidate_graph(m);   // the predictor's tendency launch changes
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_set_continuity_merid(mom6b_model* m, int on)
+{
+    if (!m) return fail(MOM6B_ERR_ARG, "null model");
+    if (on && m->cfg.precision != MOM6B_FP64)
+        return fail(MOM6B_ERR_STATE, "the meridional pass is built for the FP64 form");
+    CK(cudaSetDevice(m->cfg.device));
+    CK(cudaStreamSynchronize(m->s3d));
+    if (on && !m->hZ) {
+        cudaError_t e = cudaSuccess;
+        const size_t n3 = (size_t)m->D.plane * m->D.nk, n2 = (size_t)m->D.plane;
+        m->hZ = dalloc(m, n3, &e);
+        m->vh = dalloc(m, n3, &e);
+        m->h_v = dalloc(m, n3, &e);
+        m->vh_ovl = dalloc(m, continuity_overlap_doubles_y(m->D), &e);
+        double** two[] = {&m->FA_v_S0, &m->FA_v_SS, &m->FA_v_N0, &m->FA_v_NN,
+                          &m->vBT_SS, &m->vBT_NN, &m->dv_cor};
+        for (double** p : two) *p = dalloc(m, n2, &e);
+        if (e != cudaSuccess) return fail(MOM6B_ERR_NOMEM, "meridional continuity buffers");
+    }
+    m->merid = on != 0;
+    invalidate_graph(m);
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_continuity_pass(mom6b_model* m, int dir, double dt)
+{
+    if (!m || (dir != 0 && dir != 1)) return fail(MOM6B_ERR_ARG, "bad argument");
+    if (m->cfg.precision != MOM6B_FP64) return fail(MOM6B_ERR_STATE, "FP64 form only");
+    if (dir == 1 && !m->hZ) return fail(MOM6B_ERR_STATE, "enable the meridional pass first");
+    CK(cudaSetDevice(m->cfg.device));
+    cudaStream_t s = m->s3d;
+    const double h_min = step_h_min();
+    if (dir == 0) {
+        ContOut O{m->hA, m->uh, m->h_u, m->FA_u_W0, m->FA_u_WW, m->FA_u_E0,
+                  m->FA_u_EE, m->uBT_WW, m->uBT_EE, m->du_cor};
+        CK(timed(m, s, "continuity", [&] {
+            return launch_continuity(m->D, m->M, m->u, m->h0, m->hW, m->hE, m->uhbt0, O,
+                                     m->uh_ovl, dt, h_min, s); }));
+    } else {
+        ContOut O{m->hA, m->vh, m->h_v, m->FA_v_S0, m->FA_v_SS, m->FA_v_N0, m->FA_v_NN,
+                  m->vBT_SS, m->vBT_NN, m->dv_cor};
+        CK(timed(m, s, "continuity", [&] {
+            return launch_continuity_y(m->D, m->M, m->v, m->h0, m->hW, m->hE, m->uhbt0, O,
+                                       m->vh_ovl, dt, h_min, s); }));
+    }
+    CK(cudaStreamSynchronize(s));
     return MOM6B_OK;
 }
 

@@ -58,7 +58,11 @@ enum {
     MOM6B_F_FA_U_W0, MOM6B_F_FA_U_WW, MOM6B_F_FA_U_E0, MOM6B_F_FA_U_EE,
     MOM6B_F_UBT_WW, MOM6B_F_UBT_EE, MOM6B_F_DU_COR, MOM6B_F_TAUX_BOT,
     MOM6B_F_TAUY_BOT, MOM6B_F_TAUX, MOM6B_F_TAUY, MOM6B_F_RAY_U, MOM6B_F_RAY_V,
-    MOM6B_F_COUNT
+    MOM6B_F_COUNT,
+    /* the meridional continuity's outputs (mom6b_set_continuity_merid); ids
+       28..31 are the oracle's Coriolis and viscosity fields */
+    MOM6B_F_HV_BT = 32, MOM6B_F_FA_V_S0, MOM6B_F_FA_V_SS, MOM6B_F_FA_V_N0,
+    MOM6B_F_FA_V_NN, MOM6B_F_VBT_SS, MOM6B_F_VBT_NN, MOM6B_F_DV_COR
 };
 
 typedef struct mom6b_config {
@@ -165,6 +169,22 @@ int mom6b_diag_report(mom6b_model *m, int *out3);
  * every mom6b_step call ends with KE and mass of the final state (:385-391).
  * FP64 form only; steps then run without the CUDA graph. */
 int mom6b_diag_driver(mom6b_model *m, int output_mode);
+
+/* Meridional continuity (MOM6's continuity_PPM follows the zonal pass with
+ * it; the reference mini-app is zonal only, mom6_continuity_serial.F90:143).
+ * on = 1: every continuity of the step runs the zonal pass into an
+ * intermediate thickness (a copy of the input whose computational domain the
+ * pass updates; its halo filled when bc_fill), then the meridional pass --
+ * the zonal algorithm on the v faces with the y metrics -- into h, writing vh
+ * (MOM6B_F_VH), h_v and the v fields of BT_cont (MOM6B_F_HV_BT ..
+ * MOM6B_F_DV_COR).  FP64 form only. */
+int mom6b_set_continuity_merid(mom6b_model *m, int on);
+/* One continuity pass of one direction on the model's fields, as one call of
+ * continuity_PPM: dir 0 zonal, from u and h0 into h, uh, h_u and BT_cont's u
+ * fields; dir 1 meridional, from v and h0 into h, vh, h_v and the v fields
+ * (after mom6b_set_continuity_merid(m, 1)).  Only the computational domain
+ * of h is written.  FP64 form; synchronous. */
+int mom6b_continuity_pass(mom6b_model *m, int dir, double dt);
 
 /* Dump one field's computational domain in the diagnostics' binary format
  * (a checkpoint; mixed-form fields are written as their values in double), or

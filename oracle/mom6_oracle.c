@@ -52,6 +52,12 @@ struct oracle_model {
         *CoriolisBu, *IareaCu, *IareaCv, *dxBu, *dyBu, *IdxBu, *IdyBu, *bathyT,
         *mask2dT, *mask2dBu, *mask2dCu, *mask2dCv;
 
+    /* meridional continuity (oracle_set_merid): its outputs, the
+     * intermediate thickness and the transposed problem's arrays */
+    int merid;
+    double *hz, *BT_h_v, *FA_v_S0, *FA_v_SS, *FA_v_N0, *FA_v_NN, *vBT_SS, *vBT_NN, *dv_cor;
+    double *mt[22];
+
     /* driver diagnostics (diag_mode = 1, rk2_serial_driver.F90:149-170):
      * diag_work is mom6_diag's persistent work_2d (mom6_diag.F90:61, zero at
      * diag_init); the posted fields are kept for the tests */
@@ -474,6 +480,9 @@ void oracle_destroy(oracle_model *m) {
     for (size_t a = 0; a < sizeof(p) / sizeof(p[0]); ++a) free(*p[a]);
     free(m->diag_work); free(m->diag_usum); free(m->diag_vsum);
     free(m->diag_KE); free(m->diag_mass);
+    free(m->hz); free(m->BT_h_v); free(m->FA_v_S0); free(m->FA_v_SS); free(m->FA_v_N0);
+    free(m->FA_v_NN); free(m->vBT_SS); free(m->vBT_NN); free(m->dv_cor);
+    for (int q = 0; q < 22; ++q) free(m->mt[q]);
     free(m);
 }
 
@@ -1452,6 +1461,105 @@ void oracle_continuity(oracle_model *m, const double *u, const double *hin,
 }
 
 /* ------------------------------------------------------------------------ */
+/* meridional continuity: MOM6's continuity_PPM follows the zonal pass with   */
+/* the meridional one; the mini-app's module is zonal only                    */
+/* (mom6_continuity_serial.F90:143).  The pass is the zonal restatement above */
+/* applied to the transposed problem and transposed back.                     */
+/* ------------------------------------------------------------------------ */
+enum { MT_IAREAT, MT_IDXT, MT_DXCU, MT_DXT, MT_DYCU, MT_MASKCU, MT_MASKT, MT_HW, MT_HE,
+       MT_UHBT, MT_DUCOR, MT_UCOR, MT_POR, MT_VISC, MT_FAW0, MT_FAWW, MT_FAE0, MT_FAEE,
+       MT_UBTWW, MT_UBTEE, MT_BTHU, MT_COUNT };
+
+static void transpose_plane(const double *a, double *at, int n1, int n2) {
+    for (int j = 1; j <= n2; ++j)
+        for (int i = 1; i <= n1; ++i)
+            at[(size_t)(i - 1) * n2 + (j - 1)] = a[(size_t)(j - 1) * n1 + (i - 1)];
+}
+
+static void transpose_field(const double *a, double *at, int n1, int n2, int nk) {
+    for (int k = 0; k < nk; ++k)
+        transpose_plane(a + (size_t)k * n1 * n2, at + (size_t)k * n1 * n2, n1, n2);
+}
+
+void oracle_set_merid(oracle_model *m, int on) {
+    size_t n2d = (size_t)N1 * N2, n3d = n2d * m->nk;
+    m->merid = on;
+    if (!on || m->hz) return;
+    m->hz = zalloc(n3d); m->BT_h_v = zalloc(n3d);
+    m->FA_v_S0 = zalloc(n2d); m->FA_v_SS = zalloc(n2d); m->FA_v_N0 = zalloc(n2d);
+    m->FA_v_NN = zalloc(n2d); m->vBT_SS = zalloc(n2d); m->vBT_NN = zalloc(n2d);
+    m->dv_cor = zalloc(n2d);
+    const int is3[MT_COUNT] = {0, 0, 0, 0, 0, 0, 0, 1, 1, 0, 0, 1, 1, 1, 0, 0, 0, 0, 0, 0, 1};
+    for (int q = 0; q < MT_COUNT; ++q) m->mt[q] = zalloc(is3[q] ? n3d : n2d);
+    for (size_t q = 0; q < n3d; ++q) { m->mt[MT_POR][q] = 1.0; m->mt[MT_VISC][q] = 1.0; }
+    /* the y metrics in the places of the x metrics, transposed */
+    transpose_plane(m->IareaT, m->mt[MT_IAREAT], N1, N2);
+    transpose_plane(m->IdyT, m->mt[MT_IDXT], N1, N2);
+    transpose_plane(m->dyCv, m->mt[MT_DXCU], N1, N2);
+    transpose_plane(m->dyT, m->mt[MT_DXT], N1, N2);
+    transpose_plane(m->dxCv, m->mt[MT_DYCU], N1, N2);
+    transpose_plane(m->mask2dCv, m->mt[MT_MASKCU], N1, N2);
+    transpose_plane(m->mask2dT, m->mt[MT_MASKT], N1, N2);
+}
+
+void oracle_continuity_merid(oracle_model *m, const double *v, const double *hin,
+                             double *h, double *vh, double dt) {
+    oracle_set_merid(m, 1);
+    const int n1 = N1, n2 = N2, nk = m->nk;
+    const size_t n3d = (size_t)n1 * n2 * nk;
+    oracle_model T = *m;   /* the transposed problem */
+    T.n1 = n2; T.n2 = n1; T.ni = m->nj; T.nj = m->ni;
+    T.is = m->js; T.ie = m->je; T.js = m->is; T.je = m->ie;
+    T.isd = m->jsd; T.ied = m->jed; T.jsd = m->isd; T.jed = m->ied;
+    T.IareaT = m->mt[MT_IAREAT]; T.IdxT = m->mt[MT_IDXT]; T.dxCu = m->mt[MT_DXCU];
+    T.dxT = m->mt[MT_DXT]; T.dy_Cu = m->mt[MT_DYCU]; T.mask2dCu = m->mt[MT_MASKCU];
+    T.mask2dT = m->mt[MT_MASKT]; T.hW = m->mt[MT_HW]; T.hE = m->mt[MT_HE];
+    T.c_uhbt = m->mt[MT_UHBT]; T.du_cor = m->mt[MT_DUCOR]; T.u_cor = m->mt[MT_UCOR];
+    T.por_face_areaU = m->mt[MT_POR]; T.visc_rem_u = m->mt[MT_VISC];
+    T.FA_u_W0 = m->mt[MT_FAW0]; T.FA_u_WW = m->mt[MT_FAWW]; T.FA_u_E0 = m->mt[MT_FAE0];
+    T.FA_u_EE = m->mt[MT_FAEE]; T.uBT_WW = m->mt[MT_UBTWW]; T.uBT_EE = m->mt[MT_UBTEE];
+    T.BT_h_u = m->mt[MT_BTHU];
+    double *vT = (double *)malloc(n3d * sizeof(double)), *hinT = (double *)malloc(n3d * sizeof(double));
+    double *hT = (double *)malloc(n3d * sizeof(double)), *vhT = (double *)calloc(n3d, sizeof(double));
+    transpose_field(v, vT, n1, n2, nk);
+    transpose_field(hin, hinT, n1, n2, nk);
+    transpose_field(h, hT, n1, n2, nk);
+    oracle_continuity(&T, vT, hinT, hT, vhT, dt);
+    /* back: cells [is, ie] x [js, je], faces [is, ie] x [js-1, je] */
+    for (int k = 1; k <= nk; ++k)
+        for (int j = m->js - 1; j <= m->je; ++j)
+            for (int i = m->is; i <= m->ie; ++i) {
+                size_t o = (size_t)(k - 1) * n1 * n2 + (size_t)(j - 1) * n1 + (i - 1);
+                size_t t = (size_t)(k - 1) * n1 * n2 + (size_t)(i - 1) * n2 + (j - 1);
+                if (j >= m->js) h[o] = hT[t];
+                vh[o] = vhT[t];
+                m->BT_h_v[o] = m->mt[MT_BTHU][t];
+            }
+    for (int j = m->js - 1; j <= m->je; ++j)
+        for (int i = m->is; i <= m->ie; ++i) {
+            size_t o = (size_t)(j - 1) * n1 + (i - 1), t = (size_t)(i - 1) * n2 + (j - 1);
+            m->FA_v_S0[o] = m->mt[MT_FAW0][t]; m->FA_v_SS[o] = m->mt[MT_FAWW][t];
+            m->FA_v_N0[o] = m->mt[MT_FAE0][t]; m->FA_v_NN[o] = m->mt[MT_FAEE][t];
+            m->vBT_SS[o] = m->mt[MT_UBTWW][t]; m->vBT_NN[o] = m->mt[MT_UBTEE][t];
+            m->dv_cor[o] = m->mt[MT_DUCOR][t];
+        }
+    free(vT); free(hinT); free(hT); free(vhT);
+}
+
+/* continuity of the step: zonal, or zonal then meridional through hz */
+static void step_continuity(oracle_model *m, const double *u, const double *v,
+                            const double *hin, double *h, double dt) {
+    if (!m->merid) {
+        oracle_continuity(m, u, hin, h, m->uh, dt);
+        return;
+    }
+    memcpy(m->hz, hin, (size_t)N1 * N2 * m->nk * sizeof(double));
+    oracle_continuity(m, u, hin, m->hz, m->uh, dt);
+    if (m->cfg.bc_fill) oracle_halo_fill(m, m->hz, m->nk, 0);
+    oracle_continuity_merid(m, v, m->hz, h, m->vh, dt);
+}
+
+/* ------------------------------------------------------------------------ */
 /* the split RK2 iteration, rk2_serial_driver.F90:218-399                   */
 /* ------------------------------------------------------------------------ */
 static void vel_update(oracle_model *m, const double *ubase, const double *vbase,
@@ -1534,7 +1642,7 @@ static void one_step(oracle_model *m) {
     vel_update(m, m->u, m->v, m->up, m->vp, dt);
     oracle_vert_visc(m, m->up, m->vp, m->h, dt);
     oracle_btstep(m, m->eta, m->ubt, m->vbt, m->ubt_av, m->vbt_av, m->eta_av);
-    oracle_continuity(m, m->up, m->h0, m->h, m->uh, dt);
+    step_continuity(m, m->up, m->vp, m->h0, m->h, dt);
     if (m->diag_on) {
         size_t n2d = (size_t)N1 * N2;
         diag_product_sum(m, m->diffu, m->h, 1, 0);
@@ -1561,7 +1669,7 @@ static void one_step(oracle_model *m) {
      * (rk2_serial_driver.F90:375), bounded here by ied as the CUDA C driver
      * does (rk2_cuda_c_driver.F90:471). */
     memcpy(m->htmp, m->h, n3d * sizeof(double));
-    oracle_continuity(m, m->u, m->htmp, m->h, m->uh, 0.5 * dt);
+    step_continuity(m, m->u, m->v, m->htmp, m->h, 0.5 * dt);
     if (m->cfg.bc_fill) {
         oracle_halo_fill(m, m->h, m->nk, 0);
         oracle_halo_fill(m, m->u, m->nk, 1);
@@ -1596,6 +1704,7 @@ static double *field_ptr(const oracle_model *m, int f, int *is3d) {
     case OR_F_CAV: return m->CAv;
     case OR_F_DIFFU: return m->diffu;
     case OR_F_DIFFV: return m->diffv;
+    case OR_F_HV_BT: return m->BT_h_v;
     default: break;
     }
     *is3d = 0;
@@ -1613,6 +1722,13 @@ static double *field_ptr(const oracle_model *m, int f, int *is3d) {
     case OR_F_UBT_WW: return m->uBT_WW;
     case OR_F_UBT_EE: return m->uBT_EE;
     case OR_F_DU_COR: return m->du_cor;
+    case OR_F_FA_V_S0: return m->FA_v_S0;
+    case OR_F_FA_V_SS: return m->FA_v_SS;
+    case OR_F_FA_V_N0: return m->FA_v_N0;
+    case OR_F_FA_V_NN: return m->FA_v_NN;
+    case OR_F_VBT_SS: return m->vBT_SS;
+    case OR_F_VBT_NN: return m->vBT_NN;
+    case OR_F_DV_COR: return m->dv_cor;
     case OR_F_TAUX_BOT: return m->vv_taux_bot;
     case OR_F_TAUY_BOT: return m->vv_tauy_bot;
     case OR_F_TAUX: return m->taux;

@@ -47,7 +47,10 @@ enum {
     OR_F_HU_BT, OR_F_FA_U_W0, OR_F_FA_U_WW, OR_F_FA_U_E0, OR_F_FA_U_EE,
     OR_F_UBT_WW, OR_F_UBT_EE, OR_F_DU_COR, OR_F_TAUX_BOT, OR_F_TAUY_BOT,
     OR_F_TAUX, OR_F_TAUY, OR_F_RAY_U, OR_F_RAY_V, OR_F_CAU, OR_F_CAV,
-    OR_F_DIFFU, OR_F_DIFFV, OR_F_COUNT
+    OR_F_DIFFU, OR_F_DIFFV,
+    /* meridional continuity (oracle_set_merid): h_v and BT_cont's v fields */
+    OR_F_HV_BT, OR_F_FA_V_S0, OR_F_FA_V_SS, OR_F_FA_V_N0, OR_F_FA_V_NN,
+    OR_F_VBT_SS, OR_F_VBT_NN, OR_F_DV_COR, OR_F_COUNT
 };
 
 typedef struct oracle_model oracle_model;
@@ -80,6 +83,17 @@ void oracle_step(oracle_model *m, int nsteps);
  * diffu_sum, 1 diffv_sum, 2 KE (n1*n2*nk), 3 mass (n1*n2). */
 void oracle_diag_enable(oracle_model *m, int on);
 int oracle_diag_get(const oracle_model *m, int which, double *out);
+
+/* Meridional continuity.  on = 1: every continuity of the step runs the
+ * zonal pass into an intermediate thickness (the full input array, whose
+ * computational domain the pass updates; with bc_fill its halo filled), then
+ * the meridional pass from it into h, with vh and the v fields of BT_cont.
+ * The meridional pass is the zonal restatement applied to the transposed
+ * problem ((i, j) -> (j, i); dyT, IdyT, dxCv, mask2dCv, dyCv in the places of
+ * dxT, IdxT, dy_Cu, mask2dCu, dxCu) and transposed back. */
+void oracle_set_merid(oracle_model *m, int on);
+void oracle_continuity_merid(oracle_model *m, const double *v, const double *hin,
+                             double *h, double *vh, double dt);
 
 /* Field access: element count = n1*n2 (2-D) or n1*n2*nk (3-D). */
 size_t oracle_field_size(const oracle_model *m, int field);

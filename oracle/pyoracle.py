@@ -19,10 +19,11 @@ FIELDS = ["u", "v", "h", "h0", "uh", "vh", "up", "vp", "eta", "ubt", "vbt",
           "ubt_av", "vbt_av", "eta_av", "hu_bt", "FA_u_W0", "FA_u_WW",
           "FA_u_E0", "FA_u_EE", "uBT_WW", "uBT_EE", "du_cor", "taux_bot",
           "tauy_bot", "taux", "tauy", "Ray_u", "Ray_v", "CAu", "CAv",
-          "diffu", "diffv"]
+          "diffu", "diffv", "hv_bt", "FA_v_S0", "FA_v_SS", "FA_v_N0", "FA_v_NN",
+          "vBT_SS", "vBT_NN", "dv_cor"]
 FID = {n: i for i, n in enumerate(FIELDS)}
 FIELDS_3D = {"u", "v", "h", "h0", "uh", "vh", "up", "vp", "hu_bt", "Ray_u",
-             "Ray_v", "CAu", "CAv", "diffu", "diffv"}
+             "Ray_v", "CAu", "CAv", "diffu", "diffv", "hv_bt"}
 
 
 class Config(ctypes.Structure):
@@ -70,6 +71,8 @@ def lib(parallel=False):
         L.oracle_vert_visc.argtypes = [vp, P(d), P(d), P(d), d]
         L.oracle_btstep.argtypes = [vp] + [P(d)] * 6
         L.oracle_continuity.argtypes = [vp, P(d), P(d), P(d), P(d), d]
+        L.oracle_continuity_merid.argtypes = [vp, P(d), P(d), P(d), P(d), d]
+        L.oracle_set_merid.argtypes = [vp, ctypes.c_int]
         L.oracle_halo_fill.argtypes = [vp, P(d), ctypes.c_int, ctypes.c_int]
         L.oracle_normal.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64]
         L.oracle_normal.restype = d
@@ -177,6 +180,18 @@ class Oracle:
         uh = self.get("uh")
         self._L.oracle_continuity(self._m, _ptr(u), _ptr(hin), _ptr(h), _ptr(uh), dt)
         return h, uh
+
+    def continuity_merid(self, v, hin, dt):
+        """The meridional pass alone: (h, vh) from v and hin (h starts as
+        the model's h; only the computational domain is written)."""
+        h = self.get("h")
+        vh = self.empty("vh")
+        self._L.oracle_continuity_merid(self._m, _ptr(v), _ptr(hin), _ptr(h), _ptr(vh), dt)
+        return h, vh
+
+    def set_merid(self, on=True):
+        """Zonal then meridional continuity in every step from now on."""
+        self._L.oracle_set_merid(self._m, int(bool(on)))
 
     def vert_visc(self, u, v, h, dt):
         u = u.copy(order="F")
