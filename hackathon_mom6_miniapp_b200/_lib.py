@@ -136,6 +136,7 @@ def library():
     L.mom6b_write_field_bin.argtypes = [vp, ctypes.c_int, cp]
     L.mom6b_set_continuity_merid.argtypes = [vp, ctypes.c_int]
     L.mom6b_continuity_pass.argtypes = [vp, ctypes.c_int, ctypes.c_double]
+    L.mom6b_set_coriolis_scheme.argtypes = [vp, ctypes.c_int]
     L.mom6b_read_field_bin.argtypes = [vp, ctypes.c_int, cp]
     L.mom6b_last_error.restype = ctypes.c_char_p
     L.mom6b_version.restype = ctypes.c_char_p
@@ -256,6 +257,10 @@ class Model:
         _check(library().mom6b_kernel_time_ms(self._m, name.encode(), ctypes.byref(ms),
                                               ctypes.byref(n)))
         return ms.value, n.value
+
+    def set_coriolis_scheme(self, scheme):
+        """1 SADOURNY75_ENERGY (default), 2 ARAKAWA_HSU90, 3 ARAKAWA_LAMB81."""
+        _check(library().mom6b_set_coriolis_scheme(self._m, int(scheme)))
 
     def set_continuity_merid(self, on=True):
         """Zonal then meridional continuity in every step (FP64 form)."""

@@ -57,12 +57,13 @@ struct BTParams {
 };
 
 // diffu, diffv (both or neither): also store the horizontal-viscosity
-// accelerations of the updated points (diagnostics).
+// accelerations of the updated points (diagnostics).  scheme: the Coriolis
+// scheme (1 SADOURNY75_ENERGY, 2 ARAKAWA_HSU90, 3 ARAKAWA_LAMB81).
 cudaError_t launch_tendency(const Dims& D, const Metrics& M, const UniMetrics& U,
                             const double* uin, const double* vin, const double* h,
                             const double* ubase, const double* vbase, double* uout,
                             double* vout, double coef, double h_neglect, cudaStream_t s,
-                            double* diffu = nullptr, double* diffv = nullptr);
+                            double* diffu = nullptr, double* diffv = nullptr, int scheme = 1);
 cudaError_t launch_vertvisc(const Dims& D, const Metrics& M, double* u, double* v,
                             const double* h, double dt, const VVParams& P,
                             double* taux_bot, double* tauy_bot, cudaStream_t s);

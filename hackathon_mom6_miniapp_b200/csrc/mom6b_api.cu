@@ -109,6 +109,8 @@ struct mom6b_model {
     bool diag_driver = false;
     int id_KE = -1, id_diffu_sum = -1, id_diffv_sum = -1, id_mass = -1;
     double *dg_du = nullptr, *dg_dv = nullptr, *dg_ke = nullptr, *dg_mass = nullptr;
+    // Coriolis scheme of the tendency (1 SADOURNY75_ENERGY, 2 ARAKAWA_HSU90, 3 ARAKAWA_LAMB81)
+    int cor_scheme = 1;
     // meridional continuity: intermediate thickness, vh, h_v, BT_cont's v fields
     bool merid = false;
     double *hZ = nullptr, *vh = nullptr, *h_v = nullptr, *vh_ovl = nullptr;
@@ -687,7 +689,7 @@ static int enqueue_step(mom6b_model* m)
     CK(timed(m, s, "tendency", [&] {
         return launch_tendency(D, M, m->U, m->u, m->v, m->h0, m->u, m->v, m->up, m->vp, dt,
                                hv_neglect, s, m->diag_driver ? m->dg_du : nullptr,
-                               m->diag_driver ? m->dg_dv : nullptr); }));
+                               m->diag_driver ? m->dg_dv : nullptr, m->cor_scheme); }));
     CK(timed(m, s, "vertvisc", [&] {
         return launch_vertvisc(D, M, m->up, m->vp, m->h0, dt, VV, m->taux_bot,
                                m->tauy_bot, s); }));
@@ -700,7 +702,7 @@ static int enqueue_step(mom6b_model* m)
     // ---- corrector ----
     CK(timed(m, s, "tendency", [&] {
         return launch_tendency(D, M, m->U, m->up, m->vp, m->hB, m->u, m->v, m->u, m->v,
-                               0.5 * dt, hv_neglect, s); }));
+                               0.5 * dt, hv_neglect, s, nullptr, nullptr, m->cor_scheme); }));
     CK(timed(m, s, "vertvisc", [&] {
         return launch_vertvisc(D, M, m->u, m->v, m->hB, 0.5 * dt, VV, m->taux_bot,
                                m->tauy_bot, s); }));
@@ -1312,6 +1314,18 @@ extern "C" int mom6b_diag_driver(mom6b_model* m, int output_mode)
     }
     m->diag_driver = true;
     invalidate_graph(m);   // the predictor's tendency launch changes
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_set_coriolis_scheme(mom6b_model* m, int scheme)
+{
+    if (!m || scheme < 1 || scheme > 3) return fail(MOM6B_ERR_ARG, "scheme must be 1, 2 or 3");
+    if (scheme != 1 && m->cfg.precision != MOM6B_FP64)
+        return fail(MOM6B_ERR_STATE, "the Arakawa schemes are built for the FP64 form");
+    CK(cudaSetDevice(m->cfg.device));
+    CK(cudaStreamSynchronize(m->s3d));
+    m->cor_scheme = scheme;
+    invalidate_graph(m);
     return MOM6B_OK;
 }
 

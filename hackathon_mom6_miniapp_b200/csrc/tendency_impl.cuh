@@ -61,7 +61,45 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // layer takes two barriers.
 // DIAG: also store the horizontal-viscosity accelerations diffu, diffv of the
 // updated points in dfu, dfv (the driver's diffu_sum / diffv_sum diagnostics).
-template <int TX, int TY, bool UNI, typename R, bool DIAG = false>
+// The Arakawa coefficients of the u point (I, j) (mom6_coriolis_serial.F90
+// :171-193) from q at its corners: a and d from the east pair of columns,
+// q00 = q(I, j), qp0 = q(I+1, j), q0m = q(I, j-1), qpm = q(I+1, j-1); b and
+// c from the west pair, qm0 = q(I-1, j), qmm = q(I-1, j-1).  LAMB81 writes a
+// and d at I = i - 1 of its loop; the values are the same expressions.
+template <int COR, typename R>
+__device__ __forceinline__ void arakawa_ad(R q00, R qp0, R q0m, R qpm, R& a, R& d)
+{
+    if constexpr (COR == 2) {
+        const R c12 = R(1.0) / R(12.0);
+        a = (q00 + (qp0 + q0m)) * c12;
+        d = ((q00 + qpm) + q0m) * c12;
+    } else {
+        const R c24 = R(1.0) / R(24.0);
+        a = (R(2.0) * (qp0 + q0m) + (q00 + qpm)) * c24;
+        d = ((qp0 + q0m) + R(2.0) * (q00 + qpm)) * c24;
+    }
+}
+
+template <int COR, typename R>
+__device__ __forceinline__ void arakawa_bc(R q00, R qm0, R q0m, R qmm, R& b, R& c)
+{
+    if constexpr (COR == 2) {
+        const R c12 = R(1.0) / R(12.0);
+        b = (q00 + (qm0 + q0m)) * c12;
+        c = ((q00 + qmm) + q0m) * c12;
+    } else {
+        const R c24 = R(1.0) / R(24.0);
+        b = ((q00 + qmm) + R(2.0) * (qm0 + q0m)) * c24;
+        c = (R(2.0) * (q00 + qmm) + (qm0 + q0m)) * c24;
+    }
+}
+
+// COR: the Coriolis scheme of CorAdCalc (mom6_coriolis_serial.F90:19-21):
+// 1 SADOURNY75_ENERGY (the driver's), 2 ARAKAWA_HSU90, 3 ARAKAWA_LAMB81.  The
+// Arakawa schemes' coefficients a, b, c, d (:171-193) reach q one corner
+// further east and north, so their tiles stage and evaluate one more column
+// and row; the coefficients are formed where CAu / CAv need them (:228-248).
+template <int TX, int TY, bool UNI, typename R, bool DIAG = false, int COR = 1>
 __device__ __forceinline__ void
 tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __restrict__ uin,
               const R* __restrict__ vin, const R* __restrict__ h,
@@ -69,8 +107,9 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
               R coef, R h_neglect, int k0, int KC, int bx, int by, int bz,
               R* dfu = nullptr, R* dfv = nullptr)
 {
-    constexpr int SX = TX + 2, SY = TY + 2;  // staged inputs: [i0-1, i0+TX] x [j0-1, j0+TY]
-    constexpr int CX = TX + 1, CY = TY + 1;  // intermediates
+    constexpr int W = COR >= 2 ? 1 : 0;      // the Arakawa schemes' extra column and row
+    constexpr int SX = TX + 2 + W, SY = TY + 2 + W;  // staged: [i0-1, i0+TX+W] x [j0-1, j0+TY+W]
+    constexpr int CX = TX + 1 + W, CY = TY + 1 + W;  // intermediates
     constexpr int NT = TX * TY;
     constexpr int NS = (SX * SY + NT - 1) / NT;  // staged elements per thread
     __shared__ R s_u[2][SY][SX], s_v[2][SY][SX], s_h[2][SY][SX];
@@ -232,11 +271,22 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
     if (I <= D.ie - 1 && j <= D.je) {
         R IdxCu = G2(IdxCu, I, j);
         R KEx = (KE(I + 1, j) - KE(I, j)) * IdxCu;
-        R CAu = R(0.25) *
-                         ((Q(I, j) * (VH(I + 1, j) + VH(I, j))) +
-                          (Q(I, j - 1) * (VH(I, j - 1) + VH(I + 1, j - 1)))) *
-                         IdxCu -
-                     KEx;
+        R CAu;
+        if constexpr (COR <= 1) {
+            CAu = R(0.25) *
+                      ((Q(I, j) * (VH(I + 1, j) + VH(I, j))) +
+                       (Q(I, j - 1) * (VH(I, j - 1) + VH(I + 1, j - 1)))) *
+                      IdxCu -
+                  KEx;
+        } else {
+            R a, b, c, d;
+            arakawa_ad<COR>(Q(I, j), Q(I + 1, j), Q(I, j - 1), Q(I + 1, j - 1), a, d);
+            arakawa_bc<COR>(Q(I, j), Q(I - 1, j), Q(I, j - 1), Q(I - 1, j - 1), b, c);
+            CAu = (((a * VH(I + 1, j)) + (c * VH(I, j - 1))) +
+                   ((b * VH(I, j)) + (d * VH(I + 1, j - 1)))) *
+                      IdxCu -
+                  KEx;
+        }
         R h_u = R(0.5) * (G2(mask2dT, I, j) * SH(I, j) + G2(mask2dT, I + 1, j) * SH(I + 1, j));
         R diffu = div_r((IdxCu * ((G2(dx2q, I, j - 1) * SXY(I, j - 1)) -
                                   (G2(dx2q, I, j) * SXY(I, j))) +
@@ -252,11 +302,25 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
         const int i = I, J = j;
         R IdyCv = G2(IdyCv, i, J);
         R KEy = (KE(i, J + 1) - KE(i, J)) * IdyCv;
-        R CAv = R(-0.25) *
-                         ((Q(i - 1, J) * (UH(i - 1, J) + UH(i - 1, J + 1))) +
-                          (Q(i, J) * (UH(i, J) + UH(i, J + 1)))) *
-                         IdyCv -
-                     KEy;
+        R CAv;
+        if constexpr (COR <= 1) {
+            CAv = R(-0.25) *
+                      ((Q(i - 1, J) * (UH(i - 1, J) + UH(i - 1, J + 1))) +
+                       (Q(i, J) * (UH(i, J) + UH(i, J + 1)))) *
+                      IdyCv -
+                  KEy;
+        } else {
+            // a(i-1, J), d(i-1, J+1) of the u points west of i; b(i, J), c(i, J+1)
+            R a, b, c, d, t;
+            arakawa_ad<COR>(Q(i - 1, J), Q(i, J), Q(i - 1, J - 1), Q(i, J - 1), a, t);
+            arakawa_ad<COR>(Q(i - 1, J + 1), Q(i, J + 1), Q(i - 1, J), Q(i, J), t, d);
+            arakawa_bc<COR>(Q(i, J), Q(i - 1, J), Q(i, J - 1), Q(i - 1, J - 1), b, t);
+            arakawa_bc<COR>(Q(i, J + 1), Q(i - 1, J + 1), Q(i, J), Q(i - 1, J), t, c);
+            CAv = -(((a * UH(i - 1, J)) + (c * UH(i, J + 1))) +
+                    ((b * UH(i, J)) + (d * UH(i - 1, J + 1)))) *
+                      IdyCv -
+                  KEy;
+        }
         R h_v = R(0.5) * (G2(mask2dT, i, J) * SH(i, J) + G2(mask2dT, i, J + 1) * SH(i, J + 1));
         R diffv = div_r((IdyCv * ((G2(dy2q, i - 1, J) * SXY(i - 1, J)) -
                                   (G2(dy2q, i, J) * SXY(i, J))) -
@@ -281,16 +345,44 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
 #undef VH
 }
 
-template <int TX, int TY, bool UNI, typename R, int MINB = 1, bool DIAG = false>
+template <int TX, int TY, bool UNI, typename R, int MINB = 1, bool DIAG = false, int COR = 1>
 __global__ void __launch_bounds__(TX * TY, MINB)
 k_tendency(Dims D, Metrics M, UniMetrics U, const R* __restrict__ uin,
            const R* __restrict__ vin, const R* __restrict__ h,
            const R* ubase, const R* vbase, R* uout, R* vout,
            R coef, R h_neglect, int k0, int KC, R* dfu = nullptr, R* dfv = nullptr)
 {
-    tendency_tile<TX, TY, UNI, R, DIAG>(D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef,
-                                        h_neglect, k0, KC, (int)blockIdx.x, (int)blockIdx.y,
-                                        (int)blockIdx.z, dfu, dfv);
+    tendency_tile<TX, TY, UNI, R, DIAG, COR>(D, M, U, uin, vin, h, ubase, vbase, uout, vout,
+                                             coef, h_neglect, k0, KC, (int)blockIdx.x,
+                                             (int)blockIdx.y, (int)blockIdx.z, dfu, dfv);
+}
+
+// The Arakawa schemes (COR = 2, 3): both metric forms, with or without the
+// diagnostic outputs, registers held to 3 CTAs/SM.
+template <typename R, int COR>
+cudaError_t launch_tendency_arakawa(const Dims& D, const Metrics& M, const UniMetrics& U,
+                                    dim3 grid, dim3 block, const R* uin, const R* vin,
+                                    const R* h, const R* ubase, const R* vbase, R* uout,
+                                    R* vout, R coef, R h_neglect, int KC, cudaStream_t s, R* dfu,
+                                    R* dfv)
+{
+    constexpr int TX = 32, TY = 8;
+    if (dfu) {
+        if (U.valid)
+            k_tendency<TX, TY, true, R, 3, true, COR><<<grid, block, 0, s>>>(
+                D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, KC, dfu, dfv);
+        else
+            k_tendency<TX, TY, false, R, 3, true, COR><<<grid, block, 0, s>>>(
+                D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, KC, dfu, dfv);
+    } else {
+        if (U.valid)
+            k_tendency<TX, TY, true, R, 3, false, COR><<<grid, block, 0, s>>>(
+                D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, KC);
+        else
+            k_tendency<TX, TY, false, R, 3, false, COR><<<grid, block, 0, s>>>(
+                D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, KC);
+    }
+    return cudaGetLastError();
 }
 
 constexpr int kTendTX = 32, kTendTY = 8, kTendKC = 5;
@@ -298,20 +390,29 @@ constexpr int kTendTX = 32, kTendTY = 8, kTendKC = 5;
 // Host launcher: one CTA per (TX x TY) tile of the compute domain and chunk of
 // kTendKC layers.
 // dfu, dfv (both or neither): also store diffu, diffv (the diagnostic form of
-// the kernel; the step's own launches pass neither).
+// the kernel; the step's own launches pass neither).  scheme: the Coriolis
+// scheme (1 SADOURNY75_ENERGY, 2 ARAKAWA_HSU90, 3 ARAKAWA_LAMB81).
 template <typename R>
 cudaError_t launch_tendency_t(const Dims& D, const Metrics& M, const UniMetrics& U,
                               const R* uin, const R* vin, const R* h, const R* ubase,
                               const R* vbase, R* uout, R* vout, R coef, R h_neglect,
-                              cudaStream_t s, R* dfu = nullptr, R* dfv = nullptr)
+                              cudaStream_t s, R* dfu = nullptr, R* dfv = nullptr,
+                              int scheme = 1)
 {
     constexpr int TY = kTendTY;
     int nx = D.ie - D.is + 1, ny = D.je - D.js + 1;
     dim3 block(kTendTX, TY, 1);
     int nchunks = (D.nk + kTendKC - 1) / kTendKC;
     dim3 grid((nx + kTendTX - 1) / kTendTX, (ny + TY - 1) / TY, nchunks);
+    if ((dfu == nullptr) != (dfv == nullptr)) return cudaErrorInvalidValue;
+    if (scheme == 2)
+        return launch_tendency_arakawa<R, 2>(D, M, U, grid, block, uin, vin, h, ubase, vbase,
+                                             uout, vout, coef, h_neglect, kTendKC, s, dfu, dfv);
+    if (scheme == 3)
+        return launch_tendency_arakawa<R, 3>(D, M, U, grid, block, uin, vin, h, ubase, vbase,
+                                             uout, vout, coef, h_neglect, kTendKC, s, dfu, dfv);
+    if (scheme != 1) return cudaErrorInvalidValue;
     if (dfu || dfv) {
-        if (!dfu || !dfv) return cudaErrorInvalidValue;
         if (U.valid)
             k_tendency<kTendTX, TY, true, R, 3, true><<<grid, block, 0, s>>>(
                 D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, kTendKC,

@@ -170,6 +170,13 @@ int mom6b_diag_report(mom6b_model *m, int *out3);
  * FP64 form only; steps then run without the CUDA graph. */
 int mom6b_diag_driver(mom6b_model *m, int output_mode);
 
+/* Coriolis scheme of CorAdCalc in the step (coriolis_init's scheme argument,
+ * mom6_coriolis_serial.F90:19-21): 1 SADOURNY75_ENERGY (the default, the
+ * driver's), 2 ARAKAWA_HSU90, 3 ARAKAWA_LAMB81 (:171-193, :228-248).  The
+ * Arakawa schemes are built for the FP64 form. */
+enum { MOM6B_SADOURNY75_ENERGY = 1, MOM6B_ARAKAWA_HSU90 = 2, MOM6B_ARAKAWA_LAMB81 = 3 };
+int mom6b_set_coriolis_scheme(mom6b_model *m, int scheme);
+
 /* Meridional continuity (MOM6's continuity_PPM follows the zonal pass with
  * it; the reference mini-app is zonal only, mom6_continuity_serial.F90:143).
  * on = 1: every continuity of the step runs the zonal pass into an

@@ -52,6 +52,12 @@ struct oracle_model {
         *CoriolisBu, *IareaCu, *IareaCv, *dxBu, *dyBu, *IdxBu, *IdyBu, *bathyT,
         *mask2dT, *mask2dBu, *mask2dCu, *mask2dCv;
 
+    /* Coriolis scheme (coriolis_init's scheme argument, mom6_coriolis_serial.F90:47-56):
+     * 1 SADOURNY75_ENERGY (the driver's), 2 ARAKAWA_HSU90, 3 ARAKAWA_LAMB81, and the
+     * scheme's coefficient arrays a, b, c, d (:29-39) */
+    int cor_scheme;
+    double *co_a, *co_b, *co_c, *co_d;
+
     /* meridional continuity (oracle_set_merid): its outputs, the
      * intermediate thickness and the transposed problem's arrays */
     int merid;
@@ -284,6 +290,8 @@ static void alloc_all(oracle_model *m) {
     m->co_q = zalloc(n2d); m->co_Ih_q = zalloc(n2d);
     m->co_hArea_u = zalloc(n2d); m->co_hArea_v = zalloc(n2d);
     m->co_Area_q = zalloc(n2d); m->co_KE = zalloc(n2d);
+    m->co_a = zalloc(n2d); m->co_b = zalloc(n2d); m->co_c = zalloc(n2d); m->co_d = zalloc(n2d);
+    m->cor_scheme = 1;
     for (int j = m->jsd; j <= m->jed - 1; ++j)
         for (int i = m->isd; i <= m->ied - 1; ++i)
             A2(m->co_Area_q, i, j) = (A2(m->areaT, i, j) + A2(m->areaT, i + 1, j + 1)) +
@@ -480,6 +488,7 @@ void oracle_destroy(oracle_model *m) {
     for (size_t a = 0; a < sizeof(p) / sizeof(p[0]); ++a) free(*p[a]);
     free(m->diag_work); free(m->diag_usum); free(m->diag_vsum);
     free(m->diag_KE); free(m->diag_mass);
+    free(m->co_a); free(m->co_b); free(m->co_c); free(m->co_d);
     free(m->hz); free(m->BT_h_v); free(m->FA_v_S0); free(m->FA_v_SS); free(m->FA_v_N0);
     free(m->FA_v_NN); free(m->vBT_SS); free(m->vBT_NN); free(m->dv_cor);
     for (int q = 0; q < 22; ++q) free(m->mt[q]);
@@ -706,6 +715,33 @@ void oracle_coriolis(oracle_model *m, const double *u, const double *v,
                 A2(Ihq, i, j) = A2(m->co_Area_q, i, j) / (hArea_q + vol_neglect);
                 A2(q, i, j) = A2(absv, i, j) * A2(Ihq, i, j);
             }
+        /* the Arakawa schemes' coefficients, :171-193 */
+        double *ca = m->co_a, *cb = m->co_b, *cc = m->co_c, *cd = m->co_d;
+        const double C1_12 = 1.0 / 12.0, C1_24 = 1.0 / 24.0;
+        if (m->cor_scheme == 2) {
+            for (int j = js; j <= je; ++j)
+                for (int i = is - 1; i <= ie; ++i) {
+                    A2(ca, i, j) = (A2(q, i, j) + (A2(q, i + 1, j) + A2(q, i, j - 1))) * C1_12;
+                    A2(cd, i, j) = ((A2(q, i, j) + A2(q, i + 1, j - 1)) + A2(q, i, j - 1)) * C1_12;
+                }
+            for (int j = js; j <= je; ++j)
+                for (int i = is; i <= ie; ++i) {
+                    A2(cb, i, j) = (A2(q, i, j) + (A2(q, i - 1, j) + A2(q, i, j - 1))) * C1_12;
+                    A2(cc, i, j) = ((A2(q, i, j) + A2(q, i - 1, j - 1)) + A2(q, i, j - 1)) * C1_12;
+                }
+        } else if (m->cor_scheme == 3) {
+            for (int j = js; j <= je; ++j)
+                for (int i = is; i <= ie; ++i) {
+                    A2(ca, i - 1, j) = (2.0 * (A2(q, i, j) + A2(q, i - 1, j - 1)) +
+                                        (A2(q, i - 1, j) + A2(q, i, j - 1))) * C1_24;
+                    A2(cd, i - 1, j) = ((A2(q, i, j) + A2(q, i - 1, j - 1)) +
+                                        2.0 * (A2(q, i - 1, j) + A2(q, i, j - 1))) * C1_24;
+                    A2(cb, i, j) = ((A2(q, i, j) + A2(q, i - 1, j - 1)) +
+                                    2.0 * (A2(q, i - 1, j) + A2(q, i, j - 1))) * C1_24;
+                    A2(cc, i, j) = (2.0 * (A2(q, i, j) + A2(q, i - 1, j - 1)) +
+                                    (A2(q, i - 1, j) + A2(q, i, j - 1))) * C1_24;
+                }
+        }
         OMP_FOR
         for (int j = js; j <= je; ++j)
             for (int i = is; i <= ie; ++i) {
@@ -720,23 +756,40 @@ void oracle_coriolis(oracle_model *m, const double *u, const double *v,
         for (int j = js; j <= je; ++j)
             for (int i = is; i <= ie - 1; ++i) {
                 double KEx = (A2(KE, i + 1, j) - A2(KE, i, j)) * A2(m->IdxCu, i, j);
-                A3(CAu, i, j, k) =
-                    0.25 *
-                        ((A2(q, i, j) * (A3(vh, i + 1, j, k) + A3(vh, i, j, k))) +
-                         (A2(q, i, j - 1) * (A3(vh, i, j - 1, k) + A3(vh, i + 1, j - 1, k)))) *
-                        A2(m->IdxCu, i, j) -
-                    KEx;
+                if (m->cor_scheme <= 1)
+                    A3(CAu, i, j, k) =
+                        0.25 *
+                            ((A2(q, i, j) * (A3(vh, i + 1, j, k) + A3(vh, i, j, k))) +
+                             (A2(q, i, j - 1) * (A3(vh, i, j - 1, k) + A3(vh, i + 1, j - 1, k)))) *
+                            A2(m->IdxCu, i, j) -
+                        KEx;
+                else   /* :230-236 */
+                    A3(CAu, i, j, k) =
+                        (((A2(ca, i, j) * A3(vh, i + 1, j, k)) + (A2(cc, i, j) * A3(vh, i, j - 1, k))) +
+                         ((A2(cb, i, j) * A3(vh, i, j, k)) +
+                          (A2(cd, i, j) * A3(vh, i + 1, j - 1, k)))) *
+                            A2(m->IdxCu, i, j) -
+                        KEx;
             }
         OMP_FOR
         for (int j = js; j <= je - 1; ++j)
             for (int i = is; i <= ie; ++i) {
                 double KEy = (A2(KE, i, j + 1) - A2(KE, i, j)) * A2(m->IdyCv, i, j);
-                A3(CAv, i, j, k) =
-                    -0.25 *
-                        ((A2(q, i - 1, j) * (A3(uh, i - 1, j, k) + A3(uh, i - 1, j + 1, k))) +
-                         (A2(q, i, j) * (A3(uh, i, j, k) + A3(uh, i, j + 1, k)))) *
-                        A2(m->IdyCv, i, j) -
-                    KEy;
+                if (m->cor_scheme <= 1)
+                    A3(CAv, i, j, k) =
+                        -0.25 *
+                            ((A2(q, i - 1, j) * (A3(uh, i - 1, j, k) + A3(uh, i - 1, j + 1, k))) +
+                             (A2(q, i, j) * (A3(uh, i, j, k) + A3(uh, i, j + 1, k)))) *
+                            A2(m->IdyCv, i, j) -
+                        KEy;
+                else   /* :238-245 */
+                    A3(CAv, i, j, k) =
+                        -(((A2(ca, i - 1, j) * A3(uh, i - 1, j, k)) +
+                           (A2(cc, i, j + 1) * A3(uh, i, j + 1, k))) +
+                          ((A2(cb, i, j) * A3(uh, i, j, k)) +
+                           (A2(cd, i - 1, j + 1) * A3(uh, i - 1, j + 1, k)))) *
+                            A2(m->IdyCv, i, j) -
+                        KEy;
             }
     }
 }
@@ -1479,6 +1532,12 @@ static void transpose_plane(const double *a, double *at, int n1, int n2) {
 static void transpose_field(const double *a, double *at, int n1, int n2, int nk) {
     for (int k = 0; k < nk; ++k)
         transpose_plane(a + (size_t)k * n1 * n2, at + (size_t)k * n1 * n2, n1, n2);
+}
+
+int oracle_set_coriolis_scheme(oracle_model *m, int scheme) {
+    if (scheme < 1 || scheme > 3) return -1;
+    m->cor_scheme = scheme;
+    return 0;
 }
 
 void oracle_set_merid(oracle_model *m, int on) {

@@ -92,6 +92,11 @@ int oracle_diag_get(const oracle_model *m, int which, double *out);
  * problem ((i, j) -> (j, i); dyT, IdyT, dxCv, mask2dCv, dyCv in the places of
  * dxT, IdxT, dy_Cu, mask2dCu, dxCu) and transposed back. */
 void oracle_set_merid(oracle_model *m, int on);
+
+/* Coriolis scheme of CorAdCalc (mom6_coriolis_serial.F90:19-21, :171-193,
+ * :211-248): 1 SADOURNY75_ENERGY (default, the driver's), 2 ARAKAWA_HSU90,
+ * 3 ARAKAWA_LAMB81.  0 on success. */
+int oracle_set_coriolis_scheme(oracle_model *m, int scheme);
 void oracle_continuity_merid(oracle_model *m, const double *v, const double *hin,
                              double *h, double *vh, double dt);
 

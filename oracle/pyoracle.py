@@ -73,6 +73,8 @@ def lib(parallel=False):
         L.oracle_continuity.argtypes = [vp, P(d), P(d), P(d), P(d), d]
         L.oracle_continuity_merid.argtypes = [vp, P(d), P(d), P(d), P(d), d]
         L.oracle_set_merid.argtypes = [vp, ctypes.c_int]
+        L.oracle_set_coriolis_scheme.argtypes = [vp, ctypes.c_int]
+        L.oracle_set_coriolis_scheme.restype = ctypes.c_int
         L.oracle_halo_fill.argtypes = [vp, P(d), ctypes.c_int, ctypes.c_int]
         L.oracle_normal.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64]
         L.oracle_normal.restype = d
@@ -188,6 +190,11 @@ class Oracle:
         vh = self.empty("vh")
         self._L.oracle_continuity_merid(self._m, _ptr(v), _ptr(hin), _ptr(h), _ptr(vh), dt)
         return h, vh
+
+    def set_coriolis_scheme(self, scheme):
+        """1 SADOURNY75_ENERGY, 2 ARAKAWA_HSU90, 3 ARAKAWA_LAMB81."""
+        if self._L.oracle_set_coriolis_scheme(self._m, int(scheme)) != 0:
+            raise ValueError(scheme)
 
     def set_merid(self, on=True):
         """Zonal then meridional continuity in every step from now on."""

@@ -156,6 +156,40 @@ def test_oracle_coriolis_matches_reference_kernels():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("scheme,coef", [(2, "launch_arakawa_hsu90_coef_kernel"),
+                                         (3, "launch_arakawa_lamb81_coef_kernel")])
+def test_oracle_arakawa_coriolis_matches_reference_kernels(scheme, coef):
+    """The Arakawa HSU90 / LAMB81 branches of CorAdCalc (serial :171-193,
+    :228-248), which the driver does not exercise, against the reference's
+    coefficient and Arakawa kernels."""
+    o, st = _setup()
+    o.set_coriolis_scheme(scheme)
+    R = RefKernels()
+    g = _geom(o)
+    n1, n2, nk = g["n1"], g["n2"], g["n3"]
+    for f in ("u", "v", "h", "uh", "vh"):
+        R.put(f, st[f])
+    for m in ("dyCv", "dxCu", "dyCu", "dxCv", "areaT", "IareaBu", "CoriolisBu", "mask2dBu",
+              "IdxCu", "IdyCv"):
+        R.put(m, o.array(m))
+    R.put("Area_q", np.repeat(o.array("Area_q")[:, :, None], nk, axis=2))
+    for s in ("dvdx", "dudy", "hArea_u", "hArea_v", "KE", "rel_vort", "abs_vort", "q", "Ih_q",
+              "a", "b", "c", "d", "CAu", "CAv"):
+        R.zeros(s, (n1, n2, nk))
+    R.call("launch_phase1_kernel", **g)
+    R.call("launch_vorticity_pv_kernel", **g)
+    R.call(coef, **g)
+    R.call("launch_coriolis_arakawa_kernel", **g)
+    cu, cv = o.coriolis(st["u"], st["v"], st["h"], st["uh"], st["vh"])
+    ru, rv = R.get("CAu", (n1, n2, nk)), R.get("CAv", (n1, n2, nk))
+    iu = (slice(o.is_ - 1, o.ie - 1), slice(o.js - 1, o.je))
+    iv = (slice(o.is_ - 1, o.ie), slice(o.js - 1, o.je - 1))
+    assert np.any(cu[iu] != 0)
+    assert np.array_equal(cu[iu], ru[iu]), _relmax(cu[iu], ru[iu])
+    assert np.array_equal(cv[iv], rv[iv]), _relmax(cv[iv], rv[iv])
+
+
+@pytest.mark.gpu
 def test_oracle_btstep_extended_matches_reference_kernels():
     o, st = _setup()
     o.set_bt_extended(True)
