@@ -576,9 +576,10 @@ def run_ours(args, world, rank, local, dist):
 def run_profile_case(args):
     """A small case of the same kernels for ncu: ni = nj = args.profile_case,
     nk = 75, bt 50, args.warmup + args.steps steps, nothing else."""
-    from hackathon_mom6_miniapp_b200 import INIT_CFG, Model
+    from hackathon_mom6_miniapp_b200 import FP64, INIT_CFG, MIXED, Model
     n = args.profile_case
-    m = Model(n, n, NK, BT, INIT_CFG, seed=0, dt=600.0)
+    m = Model(n, n, NK, BT, INIT_CFG, seed=0, dt=600.0,
+              precision=MIXED if args.profile_mixed else FP64)
     m.step(args.warmup + args.steps)
     m.synchronize()
     print(json.dumps({"profile_case": n, "steps": args.warmup + args.steps,
@@ -604,6 +605,8 @@ def main():
     ap.add_argument("--no-cfg2", action="store_true",
                     help="skip the mixed form's error at 1440x1080x75 after 100 steps")
     ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--profile-mixed", action="store_true",
+                    help="with --profile-case: the mixed-precision form's kernels")
     ap.add_argument("--profile-case", type=int, default=0,
                     help="run N steps of a ni=nj=N domain only (for ncu captures)")
     args = ap.parse_args()
