@@ -17,10 +17,12 @@ FIELDS = ["u", "v", "h", "h0", "uh", "vh", "up", "vp", "eta", "ubt", "vbt",
           # ids 28..31: the oracle's Coriolis and viscosity fields (no model buffer)
           "CAu", "CAv", "diffu", "diffv",
           # the meridional continuity's outputs (Model.set_continuity_merid)
-          "hv_bt", "FA_v_S0", "FA_v_SS", "FA_v_N0", "FA_v_NN", "vBT_SS", "vBT_NN", "dv_cor"]
+          "hv_bt", "FA_v_S0", "FA_v_SS", "FA_v_N0", "FA_v_NN", "vBT_SS", "vBT_NN", "dv_cor",
+          # the vertical-viscosity remnant (Model.set_visc_remnant)
+          "visc_rem_u", "visc_rem_v"]
 FID = {n: i for i, n in enumerate(FIELDS)}
 FIELDS_3D = {"u", "v", "h", "h0", "uh", "vh", "up", "vp", "hu_bt", "Ray_u", "Ray_v", "CAu",
-             "CAv", "diffu", "diffv", "hv_bt"}
+             "CAv", "diffu", "diffv", "hv_bt", "visc_rem_u", "visc_rem_v"}
 
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of memory",
           4: "grid barrier timeout", 5: "invalid state"}
@@ -135,6 +137,7 @@ def library():
     L.mom6b_diag_driver.argtypes = [vp, ctypes.c_int]
     L.mom6b_write_field_bin.argtypes = [vp, ctypes.c_int, cp]
     L.mom6b_set_continuity_merid.argtypes = [vp, ctypes.c_int]
+    L.mom6b_set_visc_remnant.argtypes = [vp, ctypes.c_int]
     L.mom6b_continuity_pass.argtypes = [vp, ctypes.c_int, ctypes.c_double]
     L.mom6b_set_coriolis_scheme.argtypes = [vp, ctypes.c_int]
     L.mom6b_read_field_bin.argtypes = [vp, ctypes.c_int, cp]
@@ -265,6 +268,11 @@ class Model:
     def set_continuity_merid(self, on=True):
         """Zonal then meridional continuity in every step (FP64 form)."""
         _check(library().mom6b_set_continuity_merid(self._m, int(bool(on))))
+
+    def set_visc_remnant(self, on=True):
+        """Every vertvisc also writes visc_rem_u / visc_rem_v and the continuity
+        after it runs with them (zonal_mass_flux's use_visc_rem form; FP64)."""
+        _check(library().mom6b_set_visc_remnant(self._m, int(bool(on))))
 
     def continuity_pass(self, direction, dt):
         """One continuity pass ("x" or "y") from (u or v, h0) into h."""

@@ -232,12 +232,15 @@ struct FaceCol {
     // edge arrays; zonal faces use the next element
     size_t nbh = 1;
     EI nbe = 1;
+    // the vertical-viscosity remnant of the face column (VREM), stride plane
+    const double* vr = nullptr;
 };
 
 // The inputs of one layer of one face: u(I) and the cell values of the two
 // cells either side (h_W, h_E, h of i = I and of i + 1).
 struct LayerVals {
     double u, hWi, hEi, hi, hWp, hEp, hp;
+    double vr;   // visc_rem of the layer (the remnant form only)
 };
 
 // Layers whose inputs one prefetch brings into registers (CH).  Each pass
@@ -256,7 +259,7 @@ constexpr bool kContHints = MOM6B_CONT_HINTS != 0;
 // leaves L2 to the columns whose Newton passes are still to come.
 // Y: a meridional face (i, J) whose cells are (i, J) and (i, J + 1); the
 // "W"/"E" edges are then the south/north edges.
-template <bool LAST = false, bool Y = false, typename EI>
+template <bool LAST = false, bool Y = false, bool VREM = false, typename EI>
 __device__ __forceinline__ LayerVals load_layer(const FaceCol<EI>& F, int k)
 {
     const size_t o = (size_t)(k - 1) * F.plane;
@@ -274,18 +277,37 @@ __device__ __forceinline__ LayerVals load_layer(const FaceCol<EI>& F, int k)
         L.hWp = F.hWc[oe + ne]; L.hEp = F.hEc[oe + ne];
     }
     L.hi = F.hc[o]; L.hp = F.hc[o + nh];
+    if constexpr (VREM) L.vr = LAST ? __ldcs(F.vr + o) : F.vr[o];
     return L;
 }
 
+// VREM: the velocity a face evaluates at is u + du visc_rem, and its
+// marginal areas (duhdu) carry the factor visc_rem (zonal_flux_layer :581,
+// zonal_flux_adjust :880); without it visc_rem = 1 and both factors are
+// exact, so they are omitted.
+template <bool VREM>
+__device__ __forceinline__ double u_at(const LayerVals& L, double du)
+{
+    if constexpr (VREM) return L.u + du * L.vr;
+    else return L.u + du;
+}
+template <bool VREM, typename EI>
+__device__ __forceinline__ double darea(const FaceCol<EI>& F, const LayerVals& L, double hm)
+{
+    if constexpr (VREM) return (F.dy * hm) * L.vr;
+    else return F.dy * hm;
+}
+
 // Visit layers 1..nz in order, fn(k, LayerVals).
-template <int CH, bool LAST = false, bool Y = false, typename EI, typename Fn>
+template <int CH, bool LAST = false, bool Y = false, bool VREM = false, typename EI,
+          typename Fn>
 __device__ __forceinline__ void for_layers(const FaceCol<EI>& F, int nz, Fn&& fn)
 {
     for (int kt = 1; kt <= nz; kt += CH) {
         LayerVals L[CH];
 #pragma unroll
         for (int c = 0; c < CH; ++c)
-            if (kt + c <= nz) L[c] = load_layer<LAST, Y>(F, kt + c);
+            if (kt + c <= nz) L[c] = load_layer<LAST, Y, VREM>(F, kt + c);
 #pragma unroll
         for (int c = 0; c < CH; ++c)
             if (kt + c <= nz) fn(kt + c, L[c]);
@@ -390,7 +412,7 @@ __device__ __forceinline__ bool newton_iter(Newton& S, int itt, double tol_eta_d
 // zero-transport solve (:1002), live only when it is needed.  The two are
 // independent iterations, each with its own operation sequence; sharing the
 // column passes only halves how often the column is read.
-template <int CH, typename EI, bool Y = false>
+template <int CH, typename EI, bool Y = false, bool VREM = false>
 __device__ void flux_adjust_pair(const FaceCol<EI>& F, int nz, double dt, double uhbt,
                                  double tol_eta_dt_fac, Newton& A, Newton& B,
                                  double* uh_out, size_t uh_stride)
@@ -405,19 +427,19 @@ __device__ void flux_adjust_pair(const FaceCol<EI>& F, int nz, double dt, double
         if (!pa && !pb) break;
         const double duA = A.du, duB = B.du;
         double eA = -uhbt, sA = 0.0, eB = -0.0, sB = 0.0;
-        for_layers<CH, false, Y>(F, nz, [&](int k, const LayerVals& L) {
+        for_layers<CH, false, Y, VREM>(F, nz, [&](int k, const LayerVals& L) {
             if (pa) {
                 double hm;
-                double uhk = flux_eval(F, L, L.u + duA, dt, hm);
+                double uhk = flux_eval(F, L, u_at<VREM>(L, duA), dt, hm);
                 uh_out[(size_t)(k - 1) * uh_stride] = uhk;
                 eA = eA + uhk;
-                sA = sA + F.dy * hm;
+                sA = sA + darea<VREM>(F, L, hm);
             }
             if (pb) {
                 double hm;
-                double uhk = flux_eval(F, L, L.u + duB, dt, hm);
+                double uhk = flux_eval(F, L, u_at<VREM>(L, duB), dt, hm);
                 eB = eB + uhk;
-                sB = sB + F.dy * hm;
+                sB = sB + darea<VREM>(F, L, hm);
             }
         });
         if (pa && update) {
@@ -436,7 +458,7 @@ __device__ void flux_adjust_pair(const FaceCol<EI>& F, int nz, double dt, double
 // One zonal_flux_adjust solve on its own (:813-903): the transports of every
 // evaluated iterate go to uh_out when it is given (then the last iterate is
 // evaluated even at max_itts), otherwise passes run only to update.
-template <int CH, typename EI, bool Y = false>
+template <int CH, typename EI, bool Y = false, bool VREM = false>
 __device__ void flux_adjust_one(const FaceCol<EI>& F, int nz, double dt, double target,
                                 double tol_eta_dt_fac, Newton& S, double* uh_out,
                                 size_t uh_stride)
@@ -448,12 +470,12 @@ __device__ void flux_adjust_one(const FaceCol<EI>& F, int nz, double dt, double 
         if (!update && !uh_out) break;
         const double du = S.du;
         double e = -target, sm = 0.0;
-        for_layers<CH, false, Y>(F, nz, [&](int k, const LayerVals& L) {
+        for_layers<CH, false, Y, VREM>(F, nz, [&](int k, const LayerVals& L) {
             double hm;
-            double uhk = flux_eval(F, L, L.u + du, dt, hm);
+            double uhk = flux_eval(F, L, u_at<VREM>(L, du), dt, hm);
             if (uh_out) uh_out[(size_t)(k - 1) * uh_stride] = uhk;
             e = e + uhk;
-            sm = sm + F.dy * hm;
+            sm = sm + darea<VREM>(F, L, hm);
         });
         if (update) {
             S.uh_err = e;
@@ -472,7 +494,14 @@ __device__ void flux_adjust_one(const FaceCol<EI>& F, int nz, double dt, double 
 // Y: the face is the meridional face (I, j) = (i, J) and every metric is
 // its meridional counterpart (dyT, mask2dCv, dyCv; the cell beyond is
 // (i, J + 1)); the operations are the zonal ones.
-template <int CH, typename EI, bool LOCK = true, bool Y = false>
+// VREM: the face's layers carry the vertical-viscosity remnant (F.vr).  The
+// CFL limits are scaled by 1/max_k visc_rem and bound u + du visc_rem
+// (zonal_mass_flux :335-433 with use_visc_rem_max), the bounding velocities
+// of set_zonal_BT_cont use visc_rem_lim = max(visc_rem, 0.1 max_k visc_rem)
+// (:1001-1018) and the face thickness is h_marg(u + du visc_rem) visc_rem
+// (zonal_flux_thickness :730).  Without it every visc_rem is 1 and these
+// reduce exactly to the forms below.
+template <int CH, typename EI, bool LOCK = true, bool Y = false, bool VREM = false>
 __device__ __forceinline__ void face_work(const Dims& D, const Metrics& M, FaceCol<EI>& F,
                                           int I, int j, size_t f0, double* uh, size_t ust,
                                           bool owner, const double* uhbt2d, const ContOut& O,
@@ -488,18 +517,36 @@ __device__ __forceinline__ void face_work(const Dims& D, const Metrics& M, FaceC
     const double CFL_dt = 0.5 / dt;
     const double dx_W = at(Y ? M.dyT : M.dxT), dx_E = beyond(Y ? M.dyT : M.dxT);
     const double mCu = at(Y ? M.mask2dCv : M.mask2dCu);
-    double du_max_CFL = 2.0 * (CFL_dt * dx_W);
-    double du_min_CFL = -(2.0 * (CFL_dt * dx_E));
+    double du_max_CFL, du_min_CFL;
+    double vr_max = 1.0;
+    if constexpr (VREM) {
+        vr_max = 0.0;
+        for (int k = 1; k <= nz; ++k) vr_max = dmax(vr_max, F.vr[(size_t)(k - 1) * F.plane]);
+        const double I_vrm = vr_max > 0.0 ? 1.0 / vr_max : 0.0;
+        du_max_CFL = 2.0 * (CFL_dt * dx_W) * I_vrm;
+        du_min_CFL = -(2.0 * (CFL_dt * dx_E) * I_vrm);
+    } else {
+        du_max_CFL = 2.0 * (CFL_dt * dx_W);
+        du_min_CFL = -(2.0 * (CFL_dt * dx_E));
+    }
     double uh_tot_0 = 0.0, duhdu_tot_0 = 0.0;
-    for_layers<CH, false, Y>(F, nz, [&](int k, const LayerVals& L) {
+    for_layers<CH, false, Y, VREM>(F, nz, [&](int k, const LayerVals& L) {
         double hm;
         double uhk = flux_eval(F, L, L.u, dt, hm);
         uh[(size_t)(k - 1) * ust] = uhk;
-        duhdu_tot_0 = duhdu_tot_0 + F.dy * hm;
+        duhdu_tot_0 = duhdu_tot_0 + darea<VREM>(F, L, hm);
         uh_tot_0 = uh_tot_0 + uhk;
         const double uk = L.u;
-        if (du_max_CFL > dx_W * CFL_dt - uk * mCu) du_max_CFL = dx_W * CFL_dt - uk;
-        if (du_min_CFL < -(dx_E * CFL_dt) - uk * mCu) du_min_CFL = -(dx_E * CFL_dt + uk);
+        if constexpr (VREM) {
+            const double vrk = L.vr;
+            if (du_max_CFL * vrk > dx_W * CFL_dt - uk * mCu)
+                du_max_CFL = (dx_W * CFL_dt - uk) / vrk;
+            if (du_min_CFL * vrk < -(dx_E * CFL_dt) - uk * mCu)
+                du_min_CFL = -(dx_E * CFL_dt + uk) / vrk;
+        } else {
+            if (du_max_CFL > dx_W * CFL_dt - uk * mCu) du_max_CFL = dx_W * CFL_dt - uk;
+            if (du_min_CFL < -(dx_E * CFL_dt) - uk * mCu) du_min_CFL = -(dx_E * CFL_dt + uk);
+        }
     });
     du_max_CFL = dmax(du_max_CFL, 0.0);
     du_min_CFL = dmin(du_min_CFL, 0.0);
@@ -514,17 +561,17 @@ __device__ __forceinline__ void face_work(const Dims& D, const Metrics& M, FaceC
     if (LOCK) {
         Newton A = newton_start(uh_tot_0 - uhbt, duhdu_tot_0, du_max_CFL, du_min_CFL, true);
         Newton B = newton_start(uh_tot_0 - 0.0, duhdu_tot_0, du_max_CFL, du_min_CFL, solve0);
-        flux_adjust_pair<CH, EI, Y>(F, nz, dt, uhbt, fac, A, B, uh, ust);
+        flux_adjust_pair<CH, EI, Y, VREM>(F, nz, dt, uhbt, fac, A, B, uh, ust);
         du = A.du;
         du0 = solve0 ? B.du : du;
     } else {
         Newton A = newton_start(uh_tot_0 - uhbt, duhdu_tot_0, du_max_CFL, du_min_CFL, true);
-        flux_adjust_one<CH, EI, Y>(F, nz, dt, uhbt, fac, A, uh, ust);
+        flux_adjust_one<CH, EI, Y, VREM>(F, nz, dt, uhbt, fac, A, uh, ust);
         du = A.du;
         du0 = du;
         if (solve0) {
             Newton B = newton_start(uh_tot_0 - 0.0, duhdu_tot_0, du_max_CFL, du_min_CFL, true);
-            flux_adjust_one<CH, EI, Y>(F, nz, dt, 0.0, fac, B, (double*)nullptr, 0);
+            flux_adjust_one<CH, EI, Y, VREM>(F, nz, dt, 0.0, fac, B, (double*)nullptr, 0);
             du0 = B.du;
         }
     }
@@ -536,28 +583,41 @@ __device__ __forceinline__ void face_work(const Dims& D, const Metrics& M, FaceC
     const double du_CFL = (F32(1e-6) * Idt) * at(Y ? M.dyCv : M.dxCu);
     double duR = dmin(0.0, du0 - du_CFL);
     double duL = dmax(0.0, du0 + du_CFL);
-    // visc_rem_lim = max(1, 0.1 * 1) = 1 > 0 on every layer
-    for_u<CH>(F, nz, [&](int, double uk) {
-        if (uk + duR > -du_CFL) duR = -(uk + du_CFL);
-        if (uk + duL < du_CFL) duL = -(uk - du_CFL);
-    });
+    if constexpr (VREM) {
+        const double lim_min = F32(0.1) * vr_max;
+        for (int k = 1; k <= nz; ++k) {
+            const size_t o = (size_t)(k - 1) * F.plane;
+            const double uk = F.u[o], vrk = F.vr[o];
+            const double lim = dmax(vrk, lim_min);
+            if (lim > 0.0) {
+                if (uk + duR * lim > -(du_CFL * vrk)) duR = -(uk + du_CFL * vrk) / lim;
+                if (uk + duL * lim < du_CFL * vrk) duL = -(uk - du_CFL * vrk) / lim;
+            }
+        }
+    } else {
+        // visc_rem_lim = max(1, 0.1 * 1) = 1 > 0 on every layer
+        for_u<CH>(F, nz, [&](int, double uk) {
+            if (uk + duR > -du_CFL) duR = -(uk + du_CFL);
+            if (uk + duL < du_CFL) duL = -(uk - du_CFL);
+        });
+    }
     double FAmt_0 = 0.0, FAmt_L = 0.0, FAmt_R = 0.0, uhtot_L = 0.0, uhtot_R = 0.0;
     double* h_u = O.h_u + f0;
     const bool same = (du0 == du);
-    for_layers<CH, kContHints, Y>(F, nz, [&](int k, const LayerVals& L) {
-        const double uk = L.u;
+    for_layers<CH, kContHints, Y, VREM>(F, nz, [&](int k, const LayerVals& L) {
         double hm0, hmL, hmR;
-        flux_eval(F, L, uk + du0, dt, hm0);
-        double uhL = flux_eval(F, L, uk + duL, dt, hmL);
-        double uhR = flux_eval(F, L, uk + duR, dt, hmR);
-        FAmt_0 = FAmt_0 + F.dy * hm0;
-        FAmt_L = FAmt_L + F.dy * hmL;
-        FAmt_R = FAmt_R + F.dy * hmR;
+        flux_eval(F, L, u_at<VREM>(L, du0), dt, hm0);
+        double uhL = flux_eval(F, L, u_at<VREM>(L, duL), dt, hmL);
+        double uhR = flux_eval(F, L, u_at<VREM>(L, duR), dt, hmR);
+        FAmt_0 = FAmt_0 + darea<VREM>(F, L, hm0);
+        FAmt_L = FAmt_L + darea<VREM>(F, L, hmL);
+        FAmt_R = FAmt_R + darea<VREM>(F, L, hmR);
         uhtot_L = uhtot_L + uhL;
         uhtot_R = uhtot_R + uhR;
-        // zonal_flux_thickness with u_cor = u + du (marginal faces)
+        // zonal_flux_thickness with u_cor = u + du visc_rem (marginal faces)
         double hmc = hm0;
-        if (!same) flux_eval(F, L, uk + du, dt, hmc);
+        if (!same) flux_eval(F, L, u_at<VREM>(L, du), dt, hmc);
+        if constexpr (VREM) hmc = hmc * L.vr;
         if (kContHints) __stcs(h_u + (size_t)(k - 1) * F.plane, hmc);
         else h_u[(size_t)(k - 1) * F.plane] = hmc;
     });
@@ -613,12 +673,12 @@ __device__ __forceinline__ void cell_convergence(const Dims& D, const Metrics& M
 }
 
 // MINB: the CTAs per SM the register allocation is held to (launch bounds).
-template <int CH, int MINB = 1, bool LOCK = true>
+template <int CH, int MINB = 1, bool LOCK = true, bool VREM = false>
 __global__ void __launch_bounds__(128, MINB)
 k_cont_faces(Dims D, Metrics M, const double* __restrict__ u,
              const double* __restrict__ hin, const double* __restrict__ hW,
              const double* __restrict__ hE, const double* __restrict__ uhbt2d,
-             ContOut O, double* uh_ovl, double dt)
+             ContOut O, double* uh_ovl, double dt, const double* __restrict__ visc_rem = nullptr)
 {
     const int nz = D.nk;
     const int step = (int)blockDim.x - 1;
@@ -636,10 +696,11 @@ k_cont_faces(Dims D, Metrics M, const double* __restrict__ u,
         F.dy = MOM6B_A2(M.dy_Cu, I, j, D);
         F.IdxT_i = MOM6B_A2(M.IdxT, I, j, D);
         F.IdxT_ip1 = MOM6B_A2(M.IdxT, I + 1, j, D);
+        if constexpr (VREM) F.vr = visc_rem + f0;
         const bool to_ovl = !owner;
         double* uh = to_ovl ? ovl : O.uh + f0;
         const size_t ust = to_ovl ? 1 : F.plane;
-        face_work<CH, size_t, LOCK>(D, M, F, I, j, f0, uh, ust, owner, uhbt2d, O, dt);
+        face_work<CH, size_t, LOCK, false, VREM>(D, M, F, I, j, f0, uh, ust, owner, uhbt2d, O, dt);
     }
     __syncthreads();  // the CTA's transport columns are complete and visible
     cell_convergence(D, M, I, j, hin, ovl, O, dt);
@@ -688,11 +749,12 @@ size_t continuity_overlap_doubles_y(const Dims& D)
     return nbx * nby * kYTX * (size_t)D.nk;
 }
 
-template <int CH, int MINB>
+template <int CH, int MINB, bool VREM = false>
 __global__ void __launch_bounds__(kYTX * kYTY, MINB)
 k_cont_faces_y(Dims D, Metrics M, const double* __restrict__ v, const double* __restrict__ hin,
                const double* __restrict__ hS, const double* __restrict__ hN,
-               const double* __restrict__ vhbt2d, ContOut O, double* vh_ovl, double dt)
+               const double* __restrict__ vhbt2d, ContOut O, double* vh_ovl, double dt,
+               const double* __restrict__ visc_rem = nullptr)
 {
     const int nz = D.nk;
     const int tx = (int)threadIdx.x, ty = (int)threadIdx.y;
@@ -711,9 +773,11 @@ k_cont_faces_y(Dims D, Metrics M, const double* __restrict__ v, const double* __
         F.dy = MOM6B_A2(M.dxCv, i, J, D);          // width of the v face
         F.IdxT_i = MOM6B_A2(M.IdyT, i, J, D);
         F.IdxT_ip1 = MOM6B_A2(M.IdyT, i, J + 1, D);
+        if constexpr (VREM) F.vr = visc_rem + f0;
         double* vh = owner ? O.uh + f0 : ovl;
         const size_t vst = owner ? F.plane : 1;
-        face_work<CH, size_t, false, true>(D, M, F, i, J, f0, vh, vst, owner, vhbt2d, O, dt);
+        face_work<CH, size_t, false, true, VREM>(D, M, F, i, J, f0, vh, vst, owner, vhbt2d, O,
+                                                 dt);
     }
     __syncthreads();  // the CTA's transport columns are complete and visible
     // continuity_merid_convergence of cell (i, j = J): faces J-1 (row ty-1) and J
@@ -734,7 +798,8 @@ k_cont_faces_y(Dims D, Metrics M, const double* __restrict__ v, const double* __
 cudaError_t launch_continuity_y(const Dims& D, const Metrics& M, const double* v,
                                 const double* hin, double* hS, double* hN,
                                 const double* vhbt, const ContOut& O, double* vh_ovl,
-                                double dt, double h_min, cudaStream_t s)
+                                double dt, double h_min, cudaStream_t s,
+                                const double* visc_rem)
 {
     {
         dim3 grid((D.ie - D.is + 1 + 127) / 128, D.je - D.js + 3, D.nk);
@@ -742,8 +807,12 @@ cudaError_t launch_continuity_y(const Dims& D, const Metrics& M, const double* v
     }
     const int nfaces = D.je - (D.js - 1) + 1;
     dim3 grid((D.ie - D.is + 1 + kYTX - 1) / kYTX, (nfaces - 1 + kYTY - 2) / (kYTY - 1), 1);
-    k_cont_faces_y<4, 2><<<grid, dim3(kYTX, kYTY, 1), 0, s>>>(D, M, v, hin, hS, hN, vhbt, O,
-                                                              vh_ovl, dt);
+    if (visc_rem)
+        k_cont_faces_y<4, 2, true><<<grid, dim3(kYTX, kYTY, 1), 0, s>>>(
+            D, M, v, hin, hS, hN, vhbt, O, vh_ovl, dt, visc_rem);
+    else
+        k_cont_faces_y<4, 2><<<grid, dim3(kYTX, kYTY, 1), 0, s>>>(D, M, v, hin, hS, hN, vhbt, O,
+                                                                  vh_ovl, dt);
     return cudaGetLastError();
 }
 
@@ -1172,12 +1241,13 @@ size_t continuity_overlap_doubles(const Dims& D)
 cudaError_t launch_continuity(const Dims& D, const Metrics& M, const double* u,
                               const double* hin, double* hW, double* hE,
                               const double* uhbt, const ContOut& O, double* uh_ovl,
-                              double dt, double h_min, cudaStream_t s)
+                              double dt, double h_min, cudaStream_t s,
+                              const double* visc_rem)
 {
     // The tile kernel keeps every column on chip (a quarter of the face
     // kernel's DRAM traffic) but is bounded by its serial column sums; the
     // face kernel below is faster on B200 and stays the default.
-    if (D.nk <= 16 * kTileWarps && getenv("MOM6B_CONT_TILE")) {
+    if (!visc_rem && D.nk <= 16 * kTileWarps && getenv("MOM6B_CONT_TILE")) {
         const size_t smem = ((size_t)D.nk * (kTileHalo + 4 * kTileCells) + kTileHalo + 6 * 32) *
                             sizeof(double);
         const int nfaces = D.ie - (D.is - 1) + 1;
@@ -1200,7 +1270,7 @@ cudaError_t launch_continuity(const Dims& D, const Metrics& M, const double* u,
     {
         const int nb = 32 * kFusedWarps, step = nb - 1;
         size_t smem = (size_t)kFusedWarps * 2 * D.nk * kFusedCells * sizeof(double);
-        if (smem <= 227 * 1024 && getenv("MOM6B_CONT_FUSED")) {
+        if (!visc_rem && smem <= 227 * 1024 && getenv("MOM6B_CONT_FUSED")) {
             cudaError_t e = cudaFuncSetAttribute(
                 k_cont_fused<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
@@ -1263,10 +1333,12 @@ cudaError_t launch_continuity(const Dims& D, const Metrics& M, const double* u,
                                             : minb == 5 ? k_cont_faces<4, 5, false>
                                                         : k_cont_faces<4, 3, false>))
                                  : (minb == 4 ? k_cont_faces<2, 4> : k_cont_faces<2>);
+        // the remnant form runs the default shape only
+        if (visc_rem) kern = k_cont_faces<4, 4, false, true>;
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e != cudaSuccess) return e;
-        kern<<<grid, nb, smem, s>>>(D, M, u, hin, hW, hE, uhbt, O, uh_ovl, dt);
+        kern<<<grid, nb, smem, s>>>(D, M, u, hin, hW, hE, uhbt, O, uh_ovl, dt, visc_rem);
     }
     return cudaGetLastError();
 }

@@ -189,10 +189,12 @@ static cudaError_t launch_vv(const Dims& D, const Metrics& M, double* u, double*
 
 cudaError_t launch_vertvisc(const Dims& D, const Metrics& M, double* u, double* v,
                             const double* h, double dt, const VVParams& P,
-                            double* taux_bot, double* tauy_bot, cudaStream_t s)
+                            double* taux_bot, double* tauy_bot, cudaStream_t s,
+                            double* rem_u, double* rem_v)
 {
-    if (!getenv("MOM6B_VV_LOCAL"))
-        return launch_vertvisc_pf_t<double>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s);
+    if (rem_u || !getenv("MOM6B_VV_LOCAL"))
+        return launch_vertvisc_pf_t<double>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s, rem_u,
+                                            rem_v);
     if (D.nk <= 80) return launch_vv<80>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s);
     if (D.nk <= 128) return launch_vv<128>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s);
     if (D.nk <= 256) return launch_vv<256>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s);

@@ -64,9 +64,12 @@ cudaError_t launch_tendency(const Dims& D, const Metrics& M, const UniMetrics& U
                             const double* ubase, const double* vbase, double* uout,
                             double* vout, double coef, double h_neglect, cudaStream_t s,
                             double* diffu = nullptr, double* diffv = nullptr, int scheme = 1);
+// rem_u, rem_v (both or neither): also the vertical-viscosity remnant of
+// every u / v column (vert_visc_remnant).
 cudaError_t launch_vertvisc(const Dims& D, const Metrics& M, double* u, double* v,
                             const double* h, double dt, const VVParams& P,
-                            double* taux_bot, double* tauy_bot, cudaStream_t s);
+                            double* taux_bot, double* tauy_bot, cudaStream_t s,
+                            double* rem_u = nullptr, double* rem_v = nullptr);
 // uh_ovl: scratch of continuity_overlap_doubles(D) doubles holding the
 // recomputed overlap face column of every CTA.
 size_t continuity_overlap_doubles(const Dims& D);
@@ -77,11 +80,15 @@ size_t continuity_overlap_doubles_y(const Dims& D);
 cudaError_t launch_continuity_y(const Dims& D, const Metrics& M, const double* v,
                                 const double* hin, double* hS, double* hN,
                                 const double* vhbt, const ContOut& O, double* vh_ovl,
-                                double dt, double h_min, cudaStream_t s);
+                                double dt, double h_min, cudaStream_t s,
+                                const double* visc_rem = nullptr);
+// visc_rem (optional, (n1, n2, nk)): the vertical-viscosity remnant of the
+// faces; the fluxes then follow zonal_mass_flux's use_visc_rem form.
 cudaError_t launch_continuity(const Dims& D, const Metrics& M, const double* u,
                               const double* hin, double* hW, double* hE,
                               const double* uhbt, const ContOut& O, double* uh_ovl,
-                              double dt, double h_min, cudaStream_t s);
+                              double dt, double h_min, cudaStream_t s,
+                              const double* visc_rem = nullptr);
 cudaError_t launch_btstep(const Dims& D, const Metrics& M, const UniMetrics& U,
                           const BTWork& W,
                           const BTParams& P, const double* eta_in,

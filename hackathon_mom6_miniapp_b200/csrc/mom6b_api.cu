@@ -116,6 +116,10 @@ struct mom6b_model {
     double *hZ = nullptr, *vh = nullptr, *h_v = nullptr, *vh_ovl = nullptr;
     double *FA_v_S0 = nullptr, *FA_v_SS = nullptr, *FA_v_N0 = nullptr, *FA_v_NN = nullptr;
     double *vBT_SS = nullptr, *vBT_NN = nullptr, *dv_cor = nullptr;
+    // vertical-viscosity remnant (vert_visc_remnant) written by every
+    // vertvisc and read by the continuity that follows it
+    bool remnant = false;
+    double *visc_rem_u = nullptr, *visc_rem_v = nullptr;
 };
 
 static double* dalloc(mom6b_model* m, size_t n, cudaError_t* err)
@@ -600,10 +604,12 @@ static cudaError_t continuity_pass(mom6b_model* m, cudaStream_t s, const double*
 {
     const Dims& D = m->D;
     const double h_min = step_h_min();
+    const double* vr_u = m->remnant ? m->visc_rem_u : nullptr;
+    const double* vr_v = m->remnant ? m->visc_rem_v : nullptr;
     if (!m->merid)
         return timed(m, s, "continuity", [&] {
             return launch_continuity(D, m->M, u, hin, m->hW, m->hE, m->uhbt0, O, m->uh_ovl,
-                                     dt, h_min, s); });
+                                     dt, h_min, s, vr_u); });
     ContOut OZ = O;
     OZ.h = m->hZ;
     cudaError_t e = cudaMemcpyAsync(m->hZ, hin, (size_t)D.plane * D.nk * sizeof(double),
@@ -611,7 +617,7 @@ static cudaError_t continuity_pass(mom6b_model* m, cudaStream_t s, const double*
     if (e != cudaSuccess) return e;
     e = timed(m, s, "continuity", [&] {
         return launch_continuity(D, m->M, u, hin, m->hW, m->hE, m->uhbt0, OZ, m->uh_ovl, dt,
-                                 h_min, s); });
+                                 h_min, s, vr_u); });
     if (e != cudaSuccess) return e;
     if (m->cfg.bc_fill) {
         e = timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->hZ, D.nk, 0, s); });
@@ -621,7 +627,7 @@ static cudaError_t continuity_pass(mom6b_model* m, cudaStream_t s, const double*
                m->vBT_SS, m->vBT_NN, m->dv_cor};
     return timed(m, s, "continuity", [&] {
         return launch_continuity_y(D, m->M, v, m->hZ, m->hW, m->hE, m->uhbt0, OV, m->vh_ovl, dt,
-                                   h_min, s); });
+                                   h_min, s, vr_v); });
 }
 
 static int enqueue_step(mom6b_model* m)
@@ -692,7 +698,8 @@ static int enqueue_step(mom6b_model* m)
                                m->diag_driver ? m->dg_dv : nullptr, m->cor_scheme); }));
     CK(timed(m, s, "vertvisc", [&] {
         return launch_vertvisc(D, M, m->up, m->vp, m->h0, dt, VV, m->taux_bot,
-                               m->tauy_bot, s); }));
+                               m->tauy_bot, s, m->remnant ? m->visc_rem_u : nullptr,
+                               m->remnant ? m->visc_rem_v : nullptr); }));
     CK(continuity_pass(m, s, m->up, m->vp, m->h0, OB, dt));
     if (c.bc_fill) {
         CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->hB, g.nk, 0, s); }));
@@ -705,7 +712,8 @@ static int enqueue_step(mom6b_model* m)
                                0.5 * dt, hv_neglect, s, nullptr, nullptr, m->cor_scheme); }));
     CK(timed(m, s, "vertvisc", [&] {
         return launch_vertvisc(D, M, m->u, m->v, m->hB, 0.5 * dt, VV, m->taux_bot,
-                               m->tauy_bot, s); }));
+                               m->tauy_bot, s, m->remnant ? m->visc_rem_u : nullptr,
+                               m->remnant ? m->visc_rem_v : nullptr); }));
     CK(continuity_pass(m, s, m->u, m->v, m->hB, OA, 0.5 * dt));
     if (c.bc_fill) {
         CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->hA, g.nk, 0, s); }));
@@ -917,6 +925,8 @@ static double* field_ptr(mom6b_model* m, int f, bool* is3d, bool* writable)
     case MOM6B_F_RAY_V: return m->Ray_v;
     case MOM6B_F_VH: return m->vh;
     case MOM6B_F_HV_BT: return m->h_v;
+    case MOM6B_F_VISC_REM_U: return m->visc_rem_u;
+    case MOM6B_F_VISC_REM_V: return m->visc_rem_v;
     default: break;
     }
     *is3d = false;
@@ -1353,6 +1363,29 @@ extern "C" int mom6b_set_continuity_merid(mom6b_model* m, int on)
     return MOM6B_OK;
 }
 
+extern "C" int mom6b_set_visc_remnant(mom6b_model* m, int on)
+{
+    if (!m) return fail(MOM6B_ERR_ARG, "null model");
+    if (on && m->cfg.precision != MOM6B_FP64)
+        return fail(MOM6B_ERR_STATE, "the viscous remnant is built for the FP64 form");
+    CK(cudaSetDevice(m->cfg.device));
+    CK(cudaStreamSynchronize(m->s3d));
+    if (on && !m->visc_rem_u) {
+        cudaError_t e = cudaSuccess;
+        const size_t n3 = (size_t)m->D.plane * m->D.nk;
+        m->visc_rem_u = dalloc(m, n3, &e);
+        m->visc_rem_v = dalloc(m, n3, &e);
+        if (e != cudaSuccess) return fail(MOM6B_ERR_NOMEM, "viscous remnant buffers");
+        // points outside every vertvisc column keep visc_rem = 1
+        std::vector<double> one(n3, 1.0);
+        CK(cudaMemcpy(m->visc_rem_u, one.data(), n3 * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(m->visc_rem_v, one.data(), n3 * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    m->remnant = on != 0;
+    invalidate_graph(m);
+    return MOM6B_OK;
+}
+
 extern "C" int mom6b_continuity_pass(mom6b_model* m, int dir, double dt)
 {
     if (!m || (dir != 0 && dir != 1)) return fail(MOM6B_ERR_ARG, "bad argument");
@@ -1366,13 +1399,15 @@ extern "C" int mom6b_continuity_pass(mom6b_model* m, int dir, double dt)
                   m->FA_u_EE, m->uBT_WW, m->uBT_EE, m->du_cor};
         CK(timed(m, s, "continuity", [&] {
             return launch_continuity(m->D, m->M, m->u, m->h0, m->hW, m->hE, m->uhbt0, O,
-                                     m->uh_ovl, dt, h_min, s); }));
+                                     m->uh_ovl, dt, h_min, s,
+                                     m->remnant ? m->visc_rem_u : nullptr); }));
     } else {
         ContOut O{m->hA, m->vh, m->h_v, m->FA_v_S0, m->FA_v_SS, m->FA_v_N0, m->FA_v_NN,
                   m->vBT_SS, m->vBT_NN, m->dv_cor};
         CK(timed(m, s, "continuity", [&] {
             return launch_continuity_y(m->D, m->M, m->v, m->h0, m->hW, m->hE, m->uhbt0, O,
-                                       m->vh_ovl, dt, h_min, s); }));
+                                       m->vh_ovl, dt, h_min, s,
+                                       m->remnant ? m->visc_rem_v : nullptr); }));
     }
     CK(cudaStreamSynchronize(s));
     return MOM6B_OK;

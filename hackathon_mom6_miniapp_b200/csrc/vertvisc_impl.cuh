@@ -38,11 +38,16 @@ constexpr int vv_min_blocks() { return sizeof(R) == 4 ? 10 : 6; }
 
 // The column of thread tx of the CTA with block coordinates (bx, by): row
 // by of the interleaved u/v row list, column bx * blockDim.x + tx.
-template <int KMAX, int CH, typename R>
+// REM (FP64): also the remnant of vert_visc_remnant (mom6_vert_visc_serial.F90
+// :295-387) of every column into rem_u / rem_v -- the same elimination with
+// h_u as the right-hand side, sharing b1, d1 and c1 with the velocity's;
+// 1 in masked columns.
+template <int KMAX, int CH, typename R, bool REM = false>
 __device__ __forceinline__ void
 vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restrict__ v,
                 const R* __restrict__ h, double dt, const VVParams& P,
-                double* __restrict__ taux_bot, double* __restrict__ tauy_bot, int bx, int by)
+                double* __restrict__ taux_bot, double* __restrict__ tauy_bot, int bx, int by,
+                double* __restrict__ rem_u = nullptr, double* __restrict__ rem_v = nullptr)
 {
     // Coefficients (h_harm, z_i, botfn, hvel, a(K)) and the tridiagonal
     // elimination (b1, d1, c1, the eliminated velocity and the back
@@ -79,9 +84,15 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
         ray_on = M.ray_layer_v; tbot = tauy_bot;
     }
     const double msk = MOM6B_A2(mask, i, j, D);
-    if (!(msk > 0.0)) return;  // vert_visc_apply leaves masked columns alone
-
     const size_t plane = (size_t)D.plane;
+    double* rcol = nullptr;
+    if constexpr (REM) rcol = (is_u ? rem_u : rem_v) + (size_t)(j - 1) * D.n1 + (i - 1);
+    if (!(msk > 0.0)) {  // vert_visc_apply leaves masked columns alone
+        if constexpr (REM)
+            for (int k = 1; k <= D.nk; ++k) rcol[(size_t)(k - 1) * plane] = 1.0;
+        return;
+    }
+
     const R* hc = h + (size_t)(j - 1) * D.n1 + (i - 1);               // h(i, j, 1)
     const R* hn_ = h + (size_t)(j - 1 + dj) * D.n1 + (i - 1 + di);     // neighbour
     R* vc = vel + (size_t)(j - 1) * D.n1 + (i - 1);
@@ -165,6 +176,11 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
     E d1 = b_denom_1 * b1;
     E u_prev = b1 * (h_u * v1 + sfc_stress);
     vc[0] = (R)u_prev;
+    E r_prev = E(0.0);   // the remnant's eliminated value (REM)
+    if constexpr (REM) {
+        r_prev = b1 * h_u;
+        rcol[0] = r_prev;
+    }
     for (int kt = 2; kt <= nz; kt += CH) {
         // layers kt .. kt+CH-1 are eliminated; they need h and vel of the
         // layer below each (k + 1) and Ray of k
@@ -209,6 +225,10 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
                 d1 = b_denom_1 * b1;
                 u_prev = (h_u * vk + dtE * a_k * u_prev) * b1;
                 vc[(size_t)(k - 1) * plane] = (R)u_prev;
+                if constexpr (REM) {
+                    r_prev = (h_u + dtE * a_k * r_prev) * b1;
+                    rcol[(size_t)(k - 1) * plane] = r_prev;
+                }
             }
         }
     }
@@ -216,14 +236,16 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
 
     // ---- sweep 3: back substitution (:447-449) ----------------------------
     E u_below = u_prev;
+    E r_below = r_prev;
     for (int kt = nz - 1; kt >= 1; kt -= CH) {
-        E pv[CH], pc[CH];
+        E pv[CH], pc[CH], pr2[CH];
 #pragma unroll
         for (int c = 0; c < CH; ++c) {
             int k = kt - c;
             if (k >= 1) {
                 pv[c] = vc[(size_t)(k - 1) * plane];
                 pc[c] = slot[k + 1];
+                if constexpr (REM) pr2[c] = rcol[(size_t)(k - 1) * plane];
             }
         }
 #pragma unroll
@@ -233,6 +255,11 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
                 E uk = pv[c] + pc[c] * u_below;
                 vc[(size_t)(k - 1) * plane] = (R)uk;
                 u_below = uk;
+                if constexpr (REM) {
+                    const E rk = pr2[c] + pc[c] * r_below;
+                    rcol[(size_t)(k - 1) * plane] = rk;
+                    r_below = rk;
+                }
             }
         }
     }
@@ -247,20 +274,22 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
 }
 
 // MINB: the CTAs per SM the register allocation is held to.
-template <int KMAX, int CH, typename R, int MINB = 1>
+template <int KMAX, int CH, typename R, int MINB = 1, bool REM = false>
 __global__ void __launch_bounds__(128, MINB)
 k_vertvisc_pf(Dims D, Metrics M, R* __restrict__ u, R* __restrict__ v,
               const R* __restrict__ h, double dt, VVParams P,
-              double* __restrict__ taux_bot, double* __restrict__ tauy_bot)
+              double* __restrict__ taux_bot, double* __restrict__ tauy_bot,
+              double* __restrict__ rem_u = nullptr, double* __restrict__ rem_v = nullptr)
 {
-    vertvisc_column<KMAX, CH, R>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, (int)blockIdx.x,
-                                 (int)blockIdx.y);
+    vertvisc_column<KMAX, CH, R, REM>(D, M, u, v, h, dt, P, taux_bot, tauy_bot,
+                                      (int)blockIdx.x, (int)blockIdx.y, rem_u, rem_v);
 }
 
 template <int KMAX, typename R>
 static cudaError_t launch_vv_pf(const Dims& D, const Metrics& M, R* u, R* v, const R* h,
                                 double dt, const VVParams& P, double* taux_bot,
-                                double* tauy_bot, cudaStream_t s)
+                                double* tauy_bot, cudaStream_t s, double* rem_u = nullptr,
+                                double* rem_v = nullptr)
 {
     const int nb = 128;
     int ncol = D.ie - D.is + 2;
@@ -272,6 +301,13 @@ static cudaError_t launch_vv_pf(const Dims& D, const Metrics& M, R* u, R* v, con
         chunk = e ? atoi(e) : kVvChunk;
         const char* b = getenv("MOM6B_VV_MINB");
         minb = b ? atoi(b) : vv_min_blocks<R>();
+    }
+    if constexpr (sizeof(R) == 8) {
+        if (rem_u) {   // with the remnant (the FP64 form's register cap)
+            k_vertvisc_pf<KMAX, 4, R, 6, true><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P, taux_bot,
+                                                                   tauy_bot, rem_u, rem_v);
+            return cudaGetLastError();
+        }
     }
     if (chunk == 2)
         k_vertvisc_pf<KMAX, 2, R><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P, taux_bot, tauy_bot);
@@ -290,15 +326,18 @@ static cudaError_t launch_vv_pf(const Dims& D, const Metrics& M, R* u, R* v, con
     return cudaGetLastError();
 }
 
+// rem_u, rem_v (FP64, both or neither): also the vertical-viscosity remnant.
 template <typename R>
 cudaError_t launch_vertvisc_pf_t(const Dims& D, const Metrics& M, R* u, R* v, const R* h,
                                  double dt, const VVParams& P, double* taux_bot,
-                                 double* tauy_bot, cudaStream_t s)
+                                 double* tauy_bot, cudaStream_t s, double* rem_u = nullptr,
+                                 double* rem_v = nullptr)
 {
-    if (D.nk <= 80) return launch_vv_pf<80>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s);
-    if (D.nk <= 128) return launch_vv_pf<128>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s);
-    if (D.nk <= 256) return launch_vv_pf<256>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s);
-    return launch_vv_pf<1024>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s);
+    if ((rem_u == nullptr) != (rem_v == nullptr)) return cudaErrorInvalidValue;
+    if (D.nk <= 80) return launch_vv_pf<80>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s, rem_u, rem_v);
+    if (D.nk <= 128) return launch_vv_pf<128>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s, rem_u, rem_v);
+    if (D.nk <= 256) return launch_vv_pf<256>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s, rem_u, rem_v);
+    return launch_vv_pf<1024>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s, rem_u, rem_v);
 }
 
 } // namespace mom6b

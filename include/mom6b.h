@@ -62,7 +62,10 @@ enum {
     /* the meridional continuity's outputs (mom6b_set_continuity_merid); ids
        28..31 are the oracle's Coriolis and viscosity fields */
     MOM6B_F_HV_BT = 32, MOM6B_F_FA_V_S0, MOM6B_F_FA_V_SS, MOM6B_F_FA_V_N0,
-    MOM6B_F_FA_V_NN, MOM6B_F_VBT_SS, MOM6B_F_VBT_NN, MOM6B_F_DV_COR
+    MOM6B_F_FA_V_NN, MOM6B_F_VBT_SS, MOM6B_F_VBT_NN, MOM6B_F_DV_COR,
+    /* the vertical-viscosity remnant at u and v points
+       (mom6b_set_visc_remnant) */
+    MOM6B_F_VISC_REM_U = 40, MOM6B_F_VISC_REM_V
 };
 
 typedef struct mom6b_config {
@@ -190,8 +193,21 @@ int mom6b_set_continuity_merid(mom6b_model *m, int on);
  * continuity_PPM: dir 0 zonal, from u and h0 into h, uh, h_u and BT_cont's u
  * fields; dir 1 meridional, from v and h0 into h, vh, h_v and the v fields
  * (after mom6b_set_continuity_merid(m, 1)).  Only the computational domain
- * of h is written.  FP64 form; synchronous. */
+ * of h is written.  With mom6b_set_visc_remnant(m, 1) the pass reads the
+ * model's visc_rem_u / visc_rem_v.  FP64 form; synchronous. */
 int mom6b_continuity_pass(mom6b_model *m, int dir, double dt);
+
+/* The vertical-viscosity remnant (vert_visc_remnant,
+ * mom6_vert_visc_serial.F90:295-387; the reference's step does not call it,
+ * MOM6's continuity_PPM takes it as visc_rem_u / visc_rem_v).  on = 1: every
+ * vertvisc of the step also writes visc_rem_u / visc_rem_v (MOM6B_F_VISC_REM_U
+ * / _V; 1 in masked columns and outside the vertvisc ranges), the fraction of
+ * a barotropic acceleration each layer keeps after the implicit viscosity,
+ * and the continuity after it runs with use_visc_rem: the CFL limits, the
+ * Newton velocities, the marginal areas, BT_cont's bounding velocities and
+ * the face thicknesses carry visc_rem (mom6_continuity_serial.F90:335-433,
+ * :581, :880, :1001-1018, :730).  FP64 form only. */
+int mom6b_set_visc_remnant(mom6b_model *m, int on);
 
 /* Dump one field's computational domain in the diagnostics' binary format
  * (a checkpoint; mixed-form fields are written as their values in double), or

@@ -58,6 +58,11 @@ struct oracle_model {
     int cor_scheme;
     double *co_a, *co_b, *co_c, *co_d;
 
+    /* the vertical-viscosity remnant fed to continuity (oracle_set_remnant):
+     * visc_rem_v beside the driver's visc_rem_u */
+    int remnant;
+    double *visc_rem_v;
+
     /* meridional continuity (oracle_set_merid): its outputs, the
      * intermediate thickness and the transposed problem's arrays */
     int merid;
@@ -488,7 +493,7 @@ void oracle_destroy(oracle_model *m) {
     for (size_t a = 0; a < sizeof(p) / sizeof(p[0]); ++a) free(*p[a]);
     free(m->diag_work); free(m->diag_usum); free(m->diag_vsum);
     free(m->diag_KE); free(m->diag_mass);
-    free(m->co_a); free(m->co_b); free(m->co_c); free(m->co_d);
+    free(m->co_a); free(m->co_b); free(m->co_c); free(m->co_d); free(m->visc_rem_v);
     free(m->hz); free(m->BT_h_v); free(m->FA_v_S0); free(m->FA_v_SS); free(m->FA_v_N0);
     free(m->FA_v_NN); free(m->vBT_SS); free(m->vBT_NN); free(m->dv_cor);
     for (int q = 0; q < 22; ++q) free(m->mt[q]);
@@ -930,6 +935,59 @@ void oracle_vert_visc(oracle_model *m, double *u, double *v, const double *h,
         }
     free(a); free(hc); free(hvel); free(z_i); free(c1);
     }
+}
+
+/* vert_visc_remnant, mom6_vert_visc_serial.F90:295-387: the fraction of a
+ * barotropic acceleration left in each layer after the implicit viscosity of
+ * the last oracle_vert_visc call (its a and h_u), with the driver's Rayleigh
+ * drag; 1 in masked columns. */
+static void alloc_visc_rem_v(oracle_model *m) {
+    if (m->visc_rem_v) return;
+    size_t n3d = (size_t)N1 * N2 * m->nk;
+    m->visc_rem_v = zalloc(n3d);
+    for (size_t q = 0; q < n3d; ++q) m->visc_rem_v[q] = 1.0;
+}
+
+void oracle_vert_visc_remnant(oracle_model *m, double dt) {
+    int is = m->is, ie = m->ie, js = m->js, je = m->je, nz = m->nk;
+    alloc_visc_rem_v(m);
+    double *c1 = (double *)malloc(sizeof(double) * (nz + 2));
+    for (int pass = 0; pass < 2; ++pass) {
+        const int u_pts = pass == 0;
+        const double *mask = u_pts ? m->mask2dCu : m->mask2dCv;
+        const double *a3 = u_pts ? m->vv_a_u : m->vv_a_v, *h3 = u_pts ? m->vv_h_u : m->vv_h_v;
+        const double *Ray3 = u_pts ? m->Ray_u : m->Ray_v;
+        double *rem = u_pts ? m->visc_rem_u : m->visc_rem_v;
+        const int j0 = u_pts ? js : js - 1, i0 = u_pts ? is - 1 : is;
+        for (int j = j0; j <= je; ++j)
+            for (int i = i0; i <= ie; ++i) {
+                if (!(A2(mask, i, j) > 0.0)) {
+                    for (int k = 1; k <= nz; ++k) A3(rem, i, j, k) = 1.0;
+                    continue;
+                }
+                double Ray = A3(Ray3, i, j, 1);
+                double b_denom_1 = A3(h3, i, j, 1) + dt * (Ray + A3(a3, i, j, 1));
+                double b1 = 1.0 / (b_denom_1 + dt * A3(a3, i, j, 2));
+                double d1 = b_denom_1 * b1;
+                A3(rem, i, j, 1) = b1 * A3(h3, i, j, 1);
+                for (int k = 2; k <= nz; ++k) {
+                    Ray = A3(Ray3, i, j, k);
+                    c1[k] = dt * A3(a3, i, j, k) * b1;
+                    b_denom_1 = A3(h3, i, j, k) + dt * (Ray + A3(a3, i, j, k) * d1);
+                    b1 = 1.0 / (b_denom_1 + dt * A3(a3, i, j, k + 1));
+                    d1 = b_denom_1 * b1;
+                    A3(rem, i, j, k) = (A3(h3, i, j, k) + dt * A3(a3, i, j, k) * A3(rem, i, j, k - 1)) * b1;
+                }
+                for (int k = nz - 1; k >= 1; --k)
+                    A3(rem, i, j, k) = A3(rem, i, j, k) + c1[k + 1] * A3(rem, i, j, k + 1);
+            }
+    }
+    free(c1);
+}
+
+void oracle_set_remnant(oracle_model *m, int on) {
+    m->remnant = on;
+    alloc_visc_rem_v(m);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -1578,6 +1636,7 @@ void oracle_continuity_merid(oracle_model *m, const double *v, const double *hin
     T.FA_u_W0 = m->mt[MT_FAW0]; T.FA_u_WW = m->mt[MT_FAWW]; T.FA_u_E0 = m->mt[MT_FAE0];
     T.FA_u_EE = m->mt[MT_FAEE]; T.uBT_WW = m->mt[MT_UBTWW]; T.uBT_EE = m->mt[MT_UBTEE];
     T.BT_h_u = m->mt[MT_BTHU];
+    if (m->visc_rem_v) transpose_field(m->visc_rem_v, m->mt[MT_VISC], n1, n2, nk);
     double *vT = (double *)malloc(n3d * sizeof(double)), *hinT = (double *)malloc(n3d * sizeof(double));
     double *hT = (double *)malloc(n3d * sizeof(double)), *vhT = (double *)calloc(n3d, sizeof(double));
     transpose_field(v, vT, n1, n2, nk);
@@ -1700,6 +1759,7 @@ static void one_step(oracle_model *m) {
     oracle_coriolis(m, m->u, m->v, m->h, m->uh, m->vh, m->CAu, m->CAv);
     vel_update(m, m->u, m->v, m->up, m->vp, dt);
     oracle_vert_visc(m, m->up, m->vp, m->h, dt);
+    if (m->remnant) oracle_vert_visc_remnant(m, dt);
     oracle_btstep(m, m->eta, m->ubt, m->vbt, m->ubt_av, m->vbt_av, m->eta_av);
     step_continuity(m, m->up, m->vp, m->h0, m->h, dt);
     if (m->diag_on) {
@@ -1723,6 +1783,7 @@ static void one_step(oracle_model *m) {
     oracle_coriolis(m, m->up, m->vp, m->h, m->uh, m->vh, m->CAu, m->CAv);
     vel_update(m, m->u, m->v, m->u, m->v, 0.5 * dt);
     oracle_vert_visc(m, m->u, m->v, m->h, 0.5 * dt);
+    if (m->remnant) oracle_vert_visc_remnant(m, 0.5 * dt);
     oracle_btstep(m, m->eta_av, m->ubt_av, m->vbt_av, m->ubt_av, m->vbt_av, m->eta);
     /* htmp <- h over the data domain; the reference loops i=isd,jed
      * (rk2_serial_driver.F90:375), bounded here by ied as the CUDA C driver
@@ -1764,6 +1825,8 @@ static double *field_ptr(const oracle_model *m, int f, int *is3d) {
     case OR_F_DIFFU: return m->diffu;
     case OR_F_DIFFV: return m->diffv;
     case OR_F_HV_BT: return m->BT_h_v;
+    case OR_F_VISC_REM_U: return m->visc_rem_u;
+    case OR_F_VISC_REM_V: return m->visc_rem_v;
     default: break;
     }
     *is3d = 0;

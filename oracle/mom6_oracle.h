@@ -3,12 +3,13 @@
  *
  * TEST INFRASTRUCTURE ONLY.  This is the parity oracle for the B200 library:
  * it restates, in plain C, the serial Fortran path of the reference
- * (app/rk2_serial_driver.F90 + src/serial/*.F90 + src/common/mom6_types.F90).
+ * (app/rk2_serial_driver.F90, the Fortran files of src/serial and
+ * src/common/mom6_types.F90).
  * Only tests/, the smoke check and the cpu_baseline leg of bench.py may link
  * or call it; the product library never does.
  *
  * Pinning: the reference has no golden vectors and its Fortran does not
- * compile here, but its CUDA C kernels (src/cuda_c/*.cu) build from their
+ * compile here, but its CUDA C kernels (the .cu files of src/cuda_c) build from their
  * sources into oracle/_ref.  Where the serial semantics and those kernels
  * coincide -- horizontal viscosity, the Sadourny Coriolis term, vertical
  * viscosity without Rayleigh drag, and btstep with extended ranges -- the
@@ -50,7 +51,9 @@ enum {
     OR_F_DIFFU, OR_F_DIFFV,
     /* meridional continuity (oracle_set_merid): h_v and BT_cont's v fields */
     OR_F_HV_BT, OR_F_FA_V_S0, OR_F_FA_V_SS, OR_F_FA_V_N0, OR_F_FA_V_NN,
-    OR_F_VBT_SS, OR_F_VBT_NN, OR_F_DV_COR, OR_F_COUNT
+    OR_F_VBT_SS, OR_F_VBT_NN, OR_F_DV_COR,
+    /* the vertical-viscosity remnant (oracle_set_remnant) */
+    OR_F_VISC_REM_U, OR_F_VISC_REM_V, OR_F_COUNT
 };
 
 typedef struct oracle_model oracle_model;
@@ -92,6 +95,14 @@ int oracle_diag_get(const oracle_model *m, int which, double *out);
  * problem ((i, j) -> (j, i); dyT, IdyT, dxCv, mask2dCv, dyCv in the places of
  * dxT, IdxT, dy_Cu, mask2dCu, dxCu) and transposed back. */
 void oracle_set_merid(oracle_model *m, int on);
+
+/* The vertical-viscosity remnant fed to continuity.  on = 1: every vertical
+ * viscosity of the step is followed by vert_visc_remnant
+ * (mom6_vert_visc_serial.F90:295-387) with the same dt, and the next
+ * continuity uses visc_rem_u (and the meridional pass visc_rem_v) in place of
+ * the driver's 1. */
+void oracle_set_remnant(oracle_model *m, int on);
+void oracle_vert_visc_remnant(oracle_model *m, double dt);
 
 /* Coriolis scheme of CorAdCalc (mom6_coriolis_serial.F90:19-21, :171-193,
  * :211-248): 1 SADOURNY75_ENERGY (default, the driver's), 2 ARAKAWA_HSU90,

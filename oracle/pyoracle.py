@@ -20,10 +20,10 @@ FIELDS = ["u", "v", "h", "h0", "uh", "vh", "up", "vp", "eta", "ubt", "vbt",
           "FA_u_E0", "FA_u_EE", "uBT_WW", "uBT_EE", "du_cor", "taux_bot",
           "tauy_bot", "taux", "tauy", "Ray_u", "Ray_v", "CAu", "CAv",
           "diffu", "diffv", "hv_bt", "FA_v_S0", "FA_v_SS", "FA_v_N0", "FA_v_NN",
-          "vBT_SS", "vBT_NN", "dv_cor"]
+          "vBT_SS", "vBT_NN", "dv_cor", "visc_rem_u", "visc_rem_v"]
 FID = {n: i for i, n in enumerate(FIELDS)}
 FIELDS_3D = {"u", "v", "h", "h0", "uh", "vh", "up", "vp", "hu_bt", "Ray_u",
-             "Ray_v", "CAu", "CAv", "diffu", "diffv", "hv_bt"}
+             "Ray_v", "CAu", "CAv", "diffu", "diffv", "hv_bt", "visc_rem_u", "visc_rem_v"}
 
 
 class Config(ctypes.Structure):
@@ -74,6 +74,8 @@ def lib(parallel=False):
         L.oracle_continuity_merid.argtypes = [vp, P(d), P(d), P(d), P(d), d]
         L.oracle_set_merid.argtypes = [vp, ctypes.c_int]
         L.oracle_set_coriolis_scheme.argtypes = [vp, ctypes.c_int]
+        L.oracle_set_remnant.argtypes = [vp, ctypes.c_int]
+        L.oracle_vert_visc_remnant.argtypes = [vp, d]
         L.oracle_set_coriolis_scheme.restype = ctypes.c_int
         L.oracle_halo_fill.argtypes = [vp, P(d), ctypes.c_int, ctypes.c_int]
         L.oracle_normal.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64]
@@ -195,6 +197,15 @@ class Oracle:
         """1 SADOURNY75_ENERGY, 2 ARAKAWA_HSU90, 3 ARAKAWA_LAMB81."""
         if self._L.oracle_set_coriolis_scheme(self._m, int(scheme)) != 0:
             raise ValueError(scheme)
+
+    def set_remnant(self, on=True):
+        """Feed the vertical-viscosity remnant to continuity from now on."""
+        self._L.oracle_set_remnant(self._m, int(bool(on)))
+
+    def vert_visc_remnant(self, dt):
+        """vert_visc_remnant after the last vert_visc; (visc_rem_u, visc_rem_v)."""
+        self._L.oracle_vert_visc_remnant(self._m, float(dt))
+        return self.get("visc_rem_u"), self.get("visc_rem_v")
 
     def set_merid(self, on=True):
         """Zonal then meridional continuity in every step from now on."""

@@ -294,3 +294,115 @@ def test_oracle_continuity_matches_reference_kernels():
     iu = (slice(o.is_ - 2, o.ie), slice(o.js - 1, o.je))
     assert _relmax(ho[ih], rh[ih]) < 1e-13
     assert _relmax(uho[iu], ruh[iu]) < 1e-13
+
+
+@pytest.mark.gpu
+def test_oracle_remnant_matches_reference_kernels_without_rayleigh():
+    """vert_visc_remnant (mom6_vert_visc_serial.F90:295-387) against the
+    remnant half of the fused cra kernels (mom6_vert_visc_kernels.cu:69-157).
+    Both start from the same coefficients, which differ by the z**6
+    association of botfn (1e-13 relative); 1 - visc_rem carries that error
+    and the cancellation of its subtraction (an ulp of 1 over 1 - visc_rem)."""
+    o, st = _setup()
+    n1, n2, nk = o.shape("u")
+    o.set("Ray_u", np.zeros((n1, n2, nk), order="F"))
+    o.set("Ray_v", np.zeros((n1, n2, nk), order="F"))
+    R = RefKernels()
+    g = _geom(o, "2d")
+    dt, hn = 300.0, 1.0e-10
+    for f in ("u", "v", "h"):
+        R.put(f, st[f])
+    R.put("taux", o.get("taux"))
+    R.put("tauy", o.get("tauy"))
+    for m in ("mask2dCu", "mask2dCv"):
+        R.put(m, o.array(m))
+    for s in ("vr_u", "vr_v", "hvel"):
+        R.zeros(s, (n1, n2, nk))
+    R.zeros("z_i", (n1, n2, nk + 1))
+    R.zeros("tau_bot", (n1, n2))
+    c = dict(Kv=1.0e-4, Kv_ml=1.0e-2, Kv_extra_bbl=1.0e-2, Hmix=50.0, Hbbl=10.0, dt=dt,
+             dt_Rho0=dt / 1035.0, h_neglect=hn, I_Hbbl=1.0 / (10.0 + hn), **g)
+    R.call("launch_vert_visc_cra_u_kernel", visc_rem_u="vr_u", taux_bot="tau_bot", **c)
+    R.call("launch_vert_visc_cra_v_kernel", visc_rem_v="vr_v", tauy_bot="tau_bot", **c)
+    o.vert_visc(st["u"], st["v"], st["h"], dt)
+    ou, ov = o.vert_visc_remnant(dt)
+    ru, rv = R.get("vr_u", (n1, n2, nk)), R.get("vr_v", (n1, n2, nk))
+    iu = (slice(o.is_ - 2, o.ie), slice(o.js - 1, o.je))
+    iv = (slice(o.is_ - 1, o.ie), slice(o.js - 2, o.je))
+    for a, b in ((ou[iu], ru[iu]), (ov[iv], rv[iv])):
+        assert (b < 1.0).any() and (b > 0.0).all()
+        assert _relmax(a, b) < 1e-14
+        assert _relmax(1.0 - a, 1.0 - b) < 1e-9
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("low", [False, True])
+def test_oracle_continuity_with_remnant_matches_reference_kernels(low):
+    """zonal_mass_flux with visc_rem_u present and use_visc_rem_max (the CFL
+    limits, the Newton velocities u + du visc_rem, the marginal areas),
+    set_zonal_BT_cont with visc_rem_lim, u_cor and zonal_flux_thickness
+    scaled by visc_rem, against the reference's CUDA C chain with
+    use_visc_rem_flag = use_vrm_max_flag = 1.  visc_rem is random in
+    [0.3, 1]; with low, one layer in ten is 0.02, below 0.1 of the column
+    maximum, so visc_rem_lim = min_visc_rem * visc_rem_max there.  The serial
+    code assigns min_visc_rem the default-real literal 0.1
+    (mom6_continuity_serial.F90:993), the CUDA C code the double 0.1
+    (mom6_continuity_kernels.cu:693): 1.5e-8 relative in visc_rem_lim, which
+    duL and duR take at such faces, so BT_cont's fields then agree to 1e-7
+    only.  uBT_WW and uBT_EE divide by FAmt - FA_0, a difference of two
+    nearly equal column areas, which magnifies the chains' 1e-13 rounding
+    differences in the areas; they are held to 1e-8.  Everything else agrees
+    as the plain chain does."""
+    o, st = _setup()
+    R = RefKernels()
+    g = _geom(o)
+    n1, n2, nk = g["n1"], g["n2"], g["n3"]
+    dt = 300.0
+    hin = np.asfortranarray(np.maximum(st["h"], 1.0))
+    rng = np.random.default_rng(17)
+    vr = rng.uniform(0.3, 1.0, (n1, n2, nk))
+    if low:
+        vr[rng.random((n1, n2, nk)) < 0.1] = 0.02
+    vr = np.asfortranarray(vr)
+    o.set("visc_rem_u", vr)
+    R.put("u", st["u"])
+    R.put("h_in", hin)
+    R.put("vr", vr)
+    for m in ("mask2dT", "dy_Cu", "IdxT", "IareaT", "dxT", "areaT", "mask2dCu", "dxCu"):
+        R.put(m, o.array(m))
+    for s in ("h_W", "h_E", "uh", "duhdu", "h", "h_u", "u_cor"):
+        R.zeros(s, (n1, n2, nk))
+    bt = ("FA_u_W0", "FA_u_WW", "uBT_WW", "FA_u_E0", "FA_u_EE", "uBT_EE")
+    for s in ("vrm", "uh_tot_0", "duhdu_tot_0", "du_max", "du_min", "du", "uhbt") + bt:
+        R.zeros(s, (n1, n2))
+    fl = dict(monotonic=0, upwind_1st_flag=0, simple_2nd_flag=0, vol_CFL_flag=0,
+              use_visc_rem_flag=1, use_por_face_flag=0, aggress_flag=0, better_iter_flag=1,
+              use_vrm_max_flag=1)
+    c = dict(h_min=2.0e-10, dt=dt, CFL_dt=0.5 / dt, I_dt=1.0 / dt, tol_eta_base=1.0e-12,
+             tol_vel_val=3.0e8, **fl, **g)
+    R.call("launch_ppm_reconstruction_3d_kernel", **c)
+    R.call("launch_zonal_flux_layer_3d_kernel", por_face_areaU="h_W", visc_rem_u="vr", **c)
+    R.call("launch_visc_rem_max_kernel", visc_rem_max_out="vrm", visc_rem_u="vr", **c)
+    R.call("launch_uh_duhdu_tot_kernel", **c)
+    R.call("launch_zonal_CFL_limits_kernel", du_max_CFL_out="du_max", du_min_CFL_out="du_min",
+           visc_rem_u="vr", visc_rem_max_in="vrm", **c)
+    R.call("launch_set_zonal_BT_cont_kernel", u="u", h_in="h_in", visc_rem_u="vr",
+           por_face_areaU="h_W", visc_rem_max_in="vrm", du_max_CFL_in="du_max",
+           du_min_CFL_in="du_min", uh_tot_0_in="uh_tot_0", duhdu_tot_0_in="duhdu_tot_0", **c)
+    R.call("launch_zonal_flux_adjust_kernel", du_out="du", visc_rem_u="vr",
+           por_face_areaU="h_W", du_max_CFL_in="du_max", du_min_CFL_in="du_min",
+           uh_tot_0_in="uh_tot_0", duhdu_tot_0_in="duhdu_tot_0", **c)
+    R.call("launch_u_cor_kernel", u_cor="u_cor", u="u", du="du", visc_rem_u="vr", **c)
+    R.call("launch_zonal_flux_thickness_kernel", h_u="h_u", u="u_cor", h="h_in",
+           por_face_areaU="h_W", visc_rem_u="vr", marginal_flag=1, has_visc_rem_flag=1, **c)
+    R.call("launch_zonal_convergence_kernel", hin="h_in", **c)
+    ho, uho = o.continuity(st["u"], hin, dt)
+    ih = (slice(o.is_ - 1, o.ie), slice(o.js - 1, o.je))
+    iu = (slice(o.is_ - 2, o.ie), slice(o.js - 1, o.je))
+    assert _relmax(ho[ih], R.get("h", (n1, n2, nk))[ih]) < 1e-13
+    assert _relmax(uho[iu], R.get("uh", (n1, n2, nk))[iu]) < 1e-13
+    assert _relmax(o.get("hu_bt")[iu], R.get("h_u", (n1, n2, nk))[iu]) < 1e-13
+    assert _relmax(o.get("du_cor")[iu], R.get("du", (n1, n2))[iu]) < 1e-12
+    for f in bt:
+        tol = 1e-7 if low else (1e-8 if f.startswith("uBT") else 1e-12)
+        assert _relmax(o.get(f)[iu], R.get(f, (n1, n2))[iu]) < tol, f
