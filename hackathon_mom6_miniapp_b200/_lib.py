@@ -28,6 +28,14 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of memory",
           4: "grid barrier timeout", 5: "invalid state"}
 
 
+class HorVisc(ctypes.Structure):
+    """mom6b_hor_visc: hor_visc_init's scheme options."""
+    _fields_ = [("laplacian", ctypes.c_int), ("biharmonic", ctypes.c_int),
+                ("smagorinsky", ctypes.c_int), ("leith", ctypes.c_int),
+                ("no_slip", ctypes.c_int), ("better_bound", ctypes.c_int),
+                ("modified_leith", ctypes.c_int), ("Ah", ctypes.c_double)]
+
+
 class Mom6bError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"mom6b error {code} ({STATUS.get(code, '?')}): {msg}")
@@ -138,6 +146,7 @@ def library():
     L.mom6b_write_field_bin.argtypes = [vp, ctypes.c_int, cp]
     L.mom6b_set_continuity_merid.argtypes = [vp, ctypes.c_int]
     L.mom6b_set_visc_remnant.argtypes = [vp, ctypes.c_int]
+    L.mom6b_set_hor_visc.argtypes = [vp, ctypes.POINTER(HorVisc)]
     L.mom6b_continuity_pass.argtypes = [vp, ctypes.c_int, ctypes.c_double]
     L.mom6b_set_coriolis_scheme.argtypes = [vp, ctypes.c_int]
     L.mom6b_read_field_bin.argtypes = [vp, ctypes.c_int, cp]
@@ -163,7 +172,7 @@ class Model:
 
     def __init__(self, ni=180, nj=180, nk=75, bt_nsteps=30, init_mode=INIT_CFG,
                  seed=0, dt=None, Kh=None, bc_fill=None, precision=FP64,
-                 device=0, use_graph=False):
+                 device=0, use_graph=False, dx_km=None):
         L = library()
         c = Config()
         _check(L.mom6b_config_default(ctypes.byref(c), init_mode))
@@ -174,6 +183,8 @@ class Model:
             c.Kh = Kh
         if bc_fill is not None:
             c.bc_fill = int(bc_fill)
+        if dx_km is not None:
+            c.dx_km = dx_km
         c.precision, c.device, c.use_graph = precision, device, int(use_graph)
         self.cfg = c
         h = ctypes.c_void_p()
@@ -268,6 +279,14 @@ class Model:
     def set_continuity_merid(self, on=True):
         """Zonal then meridional continuity in every step (FP64 form)."""
         _check(library().mom6b_set_continuity_merid(self._m, int(bool(on))))
+
+    def set_hor_visc(self, laplacian=True, biharmonic=False, smagorinsky=False, leith=False,
+                     no_slip=False, better_bound=False, modified_leith=False, Ah=1.0e10):
+        """hor_visc_init's scheme options (FP64 form for any but the default)."""
+        o = HorVisc(int(bool(laplacian)), int(bool(biharmonic)), int(bool(smagorinsky)),
+                    int(bool(leith)), int(bool(no_slip)), int(bool(better_bound)),
+                    int(bool(modified_leith)), float(Ah))
+        _check(library().mom6b_set_hor_visc(self._m, ctypes.byref(o)))
 
     def set_visc_remnant(self, on=True):
         """Every vertvisc also writes visc_rem_u / visc_rem_v and the continuity

@@ -23,7 +23,7 @@ CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", "-Wall"]
 CU_SOURCES = ["k_tendency.cu", "k_vertvisc.cu", "k_continuity.cu", "k_btstep.cu",
               "mom6b_api.cu", "abi_helpers.cu", "abi_barotropic.cu", "abi_hor_visc.cu",
               "abi_vert_visc.cu", "abi_coriolis.cu", "abi_continuity.cu",
-              "cudac_driver.cu", "k_mixed.cu", "k_ensemble.cu", "k_mlp.cu", "diag.cu"]
+              "cudac_driver.cu", "k_mixed.cu", "k_ensemble.cu", "k_mlp.cu", "diag.cu", "k_hor_visc.cu"]
 # the mixed-precision form contracts FMAs; the FP64 files must not
 FMA_SOURCES = {"k_mixed.cu", "k_ensemble.cu", "k_mlp.cu"}
 CXX_SOURCES = ["host_init.cpp"]

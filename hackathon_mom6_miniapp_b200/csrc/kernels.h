@@ -57,13 +57,16 @@ struct BTParams {
 };
 
 // diffu, diffv (both or neither): also store the horizontal-viscosity
-// accelerations of the updated points (diagnostics).  scheme: the Coriolis
-// scheme (1 SADOURNY75_ENERGY, 2 ARAKAWA_HSU90, 3 ARAKAWA_LAMB81).
+// accelerations of the updated points (diagnostics); with ext_visc they are
+// inputs instead (launch_hor_visc_gen's) and the kernel does not evaluate
+// the Laplacian.  scheme: the Coriolis scheme (1 SADOURNY75_ENERGY,
+// 2 ARAKAWA_HSU90, 3 ARAKAWA_LAMB81).
 cudaError_t launch_tendency(const Dims& D, const Metrics& M, const UniMetrics& U,
                             const double* uin, const double* vin, const double* h,
                             const double* ubase, const double* vbase, double* uout,
                             double* vout, double coef, double h_neglect, cudaStream_t s,
-                            double* diffu = nullptr, double* diffv = nullptr, int scheme = 1);
+                            double* diffu = nullptr, double* diffv = nullptr, int scheme = 1,
+                            bool ext_visc = false);
 // rem_u, rem_v (both or neither): also the vertical-viscosity remnant of
 // every u / v column (vert_visc_remnant).
 cudaError_t launch_vertvisc(const Dims& D, const Metrics& M, double* u, double* v,

@@ -35,6 +35,7 @@
 #include "../../include/mom6b.h"
 #include "diag.h"
 #include "host_init.h"
+#include "hor_visc.h"
 #include "kernels.h"
 #include "mlp.h"
 
@@ -120,6 +121,11 @@ struct mom6b_model {
     // vertvisc and read by the continuity that follows it
     bool remnant = false;
     double *visc_rem_u = nullptr, *visc_rem_v = nullptr;
+    // hor_visc scheme branches (mom6b_set_hor_visc): the general kernel's
+    // parameters and arrays, and the accelerations it hands to the tendency
+    bool hvgen = false;
+    HorViscGen hvp{};
+    double *hv_du = nullptr, *hv_dv = nullptr;
 };
 
 static double* dalloc(mom6b_model* m, size_t n, cudaError_t* err)
@@ -692,10 +698,22 @@ static int enqueue_step(mom6b_model* m)
         }
     } else {
     // ---- predictor ----  (with the driver's diagnostics, diffu and diffv are kept)
+    if (m->hvgen) {
+        // the general hor_visc, then the tendency on its accelerations (the
+        // predictor's are the driver diagnostics' diffu, diffv)
+        double* du = m->diag_driver ? m->dg_du : m->hv_du;
+        double* dv = m->diag_driver ? m->dg_dv : m->hv_dv;
+        CK(timed(m, s, "hor_visc", [&] {
+            return launch_hor_visc_gen(D, M, m->hvp, m->u, m->v, m->h0, du, dv, s); }));
+        CK(timed(m, s, "tendency", [&] {
+            return launch_tendency(D, M, m->U, m->u, m->v, m->h0, m->u, m->v, m->up, m->vp, dt,
+                                   hv_neglect, s, du, dv, m->cor_scheme, true); }));
+    } else {
     CK(timed(m, s, "tendency", [&] {
         return launch_tendency(D, M, m->U, m->u, m->v, m->h0, m->u, m->v, m->up, m->vp, dt,
                                hv_neglect, s, m->diag_driver ? m->dg_du : nullptr,
                                m->diag_driver ? m->dg_dv : nullptr, m->cor_scheme); }));
+    }
     CK(timed(m, s, "vertvisc", [&] {
         return launch_vertvisc(D, M, m->up, m->vp, m->h0, dt, VV, m->taux_bot,
                                m->tauy_bot, s, m->remnant ? m->visc_rem_u : nullptr,
@@ -707,9 +725,19 @@ static int enqueue_step(mom6b_model* m)
         CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->vp, g.nk, 2, s); }));
     }
     // ---- corrector ----
+    if (m->hvgen) {
+        CK(timed(m, s, "hor_visc", [&] {
+            return launch_hor_visc_gen(D, M, m->hvp, m->up, m->vp, m->hB, m->hv_du, m->hv_dv,
+                                       s); }));
+        CK(timed(m, s, "tendency", [&] {
+            return launch_tendency(D, M, m->U, m->up, m->vp, m->hB, m->u, m->v, m->u, m->v,
+                                   0.5 * dt, hv_neglect, s, m->hv_du, m->hv_dv, m->cor_scheme,
+                                   true); }));
+    } else {
     CK(timed(m, s, "tendency", [&] {
         return launch_tendency(D, M, m->U, m->up, m->vp, m->hB, m->u, m->v, m->u, m->v,
                                0.5 * dt, hv_neglect, s, nullptr, nullptr, m->cor_scheme); }));
+    }
     CK(timed(m, s, "vertvisc", [&] {
         return launch_vertvisc(D, M, m->u, m->v, m->hB, 0.5 * dt, VV, m->taux_bot,
                                m->tauy_bot, s, m->remnant ? m->visc_rem_u : nullptr,
@@ -1359,6 +1387,67 @@ extern "C" int mom6b_set_continuity_merid(mom6b_model* m, int on)
         if (e != cudaSuccess) return fail(MOM6B_ERR_NOMEM, "meridional continuity buffers");
     }
     m->merid = on != 0;
+    invalidate_graph(m);
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_set_hor_visc(mom6b_model* m, const mom6b_hor_visc* o)
+{
+    if (!m || !o) return fail(MOM6B_ERR_ARG, "null argument");
+    const bool plain = o->laplacian && !o->biharmonic && !o->smagorinsky && !o->leith &&
+                       !o->no_slip && !o->better_bound && !o->modified_leith;
+    if (!plain && m->cfg.precision != MOM6B_FP64)
+        return fail(MOM6B_ERR_STATE, "the hor_visc schemes are built for the FP64 form");
+    CK(cudaSetDevice(m->cfg.device));
+    CK(cudaStreamSynchronize(m->s3d));
+    HorViscGen& P = m->hvp;
+    P.lap = o->laplacian != 0;
+    P.bih = o->biharmonic != 0;
+    P.smag_kh = o->smagorinsky && P.lap;
+    P.smag_ah = o->smagorinsky && P.bih;
+    P.leith_kh = o->leith != 0;
+    P.leith_ah = o->leith && P.bih;
+    P.no_slip = o->no_slip != 0;
+    P.bb = o->better_bound != 0;
+    P.mod_leith = o->modified_leith != 0;
+    P.Kh_bg = m->cfg.Kh;
+    P.Ah_bg = o->Ah;
+    P.Kh_bg_min = 0.0;
+    P.h_neglect = step_hv_neglect();
+    if (!plain && !m->hv_du) {
+        cudaError_t e = cudaSuccess;
+        const HostGrid& g = *m->grid;
+        const size_t n2 = (size_t)m->D.plane, n3 = n2 * m->D.nk;
+        m->hv_du = dalloc(m, n3, &e);
+        m->hv_dv = dalloc(m, n3, &e);
+        // hor_visc_init (mom6_hor_visc_serial.F90:207-268)
+        std::vector<double> a[10];
+        for (auto& x : a) x.resize(n2);
+        const double Smag_Lap_const = 0.15, Smag_bi_const = 0.06, Leith_const = 1.0;
+        for (size_t p = 0; p < n2; ++p) {
+            const double h2 = g.areaT[p], h3 = std::sqrt(h2) * h2, h4 = h2 * h2;
+            a[0][p] = 0.25 * h2 / 1.0;
+            a[1][p] = 0.0625 * h4 / 1.0;
+            a[2][p] = Smag_Lap_const * Smag_Lap_const * h2;
+            a[3][p] = Smag_bi_const * Smag_bi_const * h4;
+            a[4][p] = Leith_const * h3;
+            a[5][p] = Leith_const * h3 * h3;
+            a[6][p] = g.IdxCu[p] * g.IdxCu[p] * g.IdyCu[p];
+            a[7][p] = g.IdxCu[p] * g.IdyCu[p] * g.IdyCu[p];
+            a[8][p] = g.IdxCv[p] * g.IdxCv[p] * g.IdyCv[p];
+            a[9][p] = g.IdxCv[p] * g.IdyCv[p] * g.IdyCv[p];
+        }
+        const double** dst[10] = {&P.Kh_Max, &P.Ah_Max, &P.L2c, &P.Bc, &P.L3c, &P.B6c,
+                                  &P.Idx2dyCu, &P.Idxdy2u, &P.Idx2dyCv, &P.Idxdy2v};
+        for (int q = 0; q < 10; ++q) {
+            double* d = dalloc(m, n2, &e);
+            if (e != cudaSuccess) break;
+            e = cudaMemcpy(d, a[q].data(), n2 * sizeof(double), cudaMemcpyHostToDevice);
+            *dst[q] = d;
+        }
+        if (e != cudaSuccess) return fail(MOM6B_ERR_NOMEM, "hor_visc scheme buffers");
+    }
+    m->hvgen = !plain;
     invalidate_graph(m);
     return MOM6B_OK;
 }

@@ -94,12 +94,15 @@ __device__ __forceinline__ void arakawa_bc(R q00, R qm0, R q0m, R qmm, R& b, R& 
     }
 }
 
+// EXTV: diffu, diffv come from dfu, dfv (the general hor_visc kernel's
+// outputs) and the stresses are not evaluated.
 // COR: the Coriolis scheme of CorAdCalc (mom6_coriolis_serial.F90:19-21):
 // 1 SADOURNY75_ENERGY (the driver's), 2 ARAKAWA_HSU90, 3 ARAKAWA_LAMB81.  The
 // Arakawa schemes' coefficients a, b, c, d (:171-193) reach q one corner
 // further east and north, so their tiles stage and evaluate one more column
 // and row; the coefficients are formed where CAu / CAv need them (:228-248).
-template <int TX, int TY, bool UNI, typename R, bool DIAG = false, int COR = 1>
+template <int TX, int TY, bool UNI, typename R, bool DIAG = false, int COR = 1,
+          bool EXTV = false>
 __device__ __forceinline__ void
 tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __restrict__ uin,
               const R* __restrict__ vin, const R* __restrict__ h,
@@ -201,6 +204,7 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
                 R hArea_q = (hAu0 + hAu1) + (hAv0 + hAv1);
                 R Ih_q = div_r(G2(Area_q, I, J), hArea_q + R(1.0e-20));
                 qv = absv * Ih_q;
+                if constexpr (!EXTV) {
                 // hor_visc: shearing strain and stress at q-points (:513-520, :544, :579, :964, :1050)
                 R dvdx_v = G2(DY_dxBu, I, J) *
                                 ((v1 * G2(IdyCv, I + 1, J)) - (v0 * G2(IdyCv, I, J)));
@@ -211,6 +215,7 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
                 R hq = R(0.25) * ((h00 + h11) + (h10 + h01));
                 sxy = -(G2(Kh_xy, I, J) * sh_xy);
                 sxy = sxy * (hq * mBu * G2(red_xy, I, J));
+                }
             }
             s_q[r][c] = qv;
             s_sxy[r][c] = sxy;
@@ -225,6 +230,7 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
                                ((G2(dyCu, i, j) * (uc * uc) + G2(dyCu, i - 1, j) * (um * um)) +
                                 (G2(dxCv, i, j) * (vc * vc) + G2(dxCv, i, j - 1) * (vm * vm))),
                            G2(areaT, i, j));
+                if constexpr (!EXTV) {
                 R dudx = G2(DY_dxT, i, j) *
                               ((G2(IdyCu, i, j) * uc) - (G2(IdyCu, i - 1, j) * um));
                 R dvdy = G2(DX_dyT, i, j) *
@@ -232,6 +238,7 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
                 R sh_xx = dudx - dvdy;
                 sxx = -(G2(Kh_xx, i, j) * sh_xx);
                 sxx = sxx * (SH(i, j) * G2(red_xx, i, j));
+                }
             }
             s_ke[r][c] = ke;
             s_sxx[r][c] = sxx;
@@ -287,15 +294,20 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
                       IdxCu -
                   KEx;
         }
-        R h_u = R(0.5) * (G2(mask2dT, I, j) * SH(I, j) + G2(mask2dT, I + 1, j) * SH(I + 1, j));
-        R diffu = div_r((IdxCu * ((G2(dx2q, I, j - 1) * SXY(I, j - 1)) -
-                                  (G2(dx2q, I, j) * SXY(I, j))) +
-                         G2(IdyCu, I, j) * ((G2(dy2h, I, j) * SXX(I, j)) -
-                                            (G2(dy2h, I + 1, j) * SXX(I + 1, j)))) *
-                            G2(IareaCu, I, j),
-                        h_u + h_neglect);
+        R diffu;
+        if constexpr (EXTV) {
+            diffu = dfu[oo];
+        } else {
+            R h_u = R(0.5) * (G2(mask2dT, I, j) * SH(I, j) + G2(mask2dT, I + 1, j) * SH(I + 1, j));
+            diffu = div_r((IdxCu * ((G2(dx2q, I, j - 1) * SXY(I, j - 1)) -
+                                    (G2(dx2q, I, j) * SXY(I, j))) +
+                           G2(IdyCu, I, j) * ((G2(dy2h, I, j) * SXX(I, j)) -
+                                              (G2(dy2h, I + 1, j) * SXX(I + 1, j)))) *
+                              G2(IareaCu, I, j),
+                          h_u + h_neglect);
+        }
         uout[oo] = ub + coef * (CAu + diffu);
-        if (DIAG) dfu[oo] = diffu;
+        if (DIAG && !EXTV) dfu[oo] = diffu;
     }
     // ---- v point (i, J) = (I, j) -------------------------------------------
     if (I <= D.ie && j <= D.je - 1) {
@@ -321,15 +333,20 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
                       IdyCv -
                   KEy;
         }
-        R h_v = R(0.5) * (G2(mask2dT, i, J) * SH(i, J) + G2(mask2dT, i, J + 1) * SH(i, J + 1));
-        R diffv = div_r((IdyCv * ((G2(dy2q, i - 1, J) * SXY(i - 1, J)) -
-                                  (G2(dy2q, i, J) * SXY(i, J))) -
-                         G2(IdxCv, i, J) * ((G2(dx2h, i, J) * SXX(i, J)) -
-                                            (G2(dx2h, i, J + 1) * SXX(i, J + 1)))) *
-                            G2(IareaCv, i, J),
-                        h_v + h_neglect);
+        R diffv;
+        if constexpr (EXTV) {
+            diffv = dfv[oo];
+        } else {
+            R h_v = R(0.5) * (G2(mask2dT, i, J) * SH(i, J) + G2(mask2dT, i, J + 1) * SH(i, J + 1));
+            diffv = div_r((IdyCv * ((G2(dy2q, i - 1, J) * SXY(i - 1, J)) -
+                                    (G2(dy2q, i, J) * SXY(i, J))) -
+                           G2(IdxCv, i, J) * ((G2(dx2h, i, J) * SXX(i, J)) -
+                                              (G2(dx2h, i, J + 1) * SXX(i, J + 1)))) *
+                              G2(IareaCv, i, J),
+                          h_v + h_neglect);
+        }
         vout[oo] = vb + coef * (CAv + diffv);
-        if (DIAG) dfv[oo] = diffv;
+        if (DIAG && !EXTV) dfv[oo] = diffv;
     }
   }  // layer loop
 #undef SU
@@ -345,16 +362,34 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
 #undef VH
 }
 
-template <int TX, int TY, bool UNI, typename R, int MINB = 1, bool DIAG = false, int COR = 1>
+template <int TX, int TY, bool UNI, typename R, int MINB = 1, bool DIAG = false, int COR = 1,
+          bool EXTV = false>
 __global__ void __launch_bounds__(TX * TY, MINB)
 k_tendency(Dims D, Metrics M, UniMetrics U, const R* __restrict__ uin,
            const R* __restrict__ vin, const R* __restrict__ h,
            const R* ubase, const R* vbase, R* uout, R* vout,
            R coef, R h_neglect, int k0, int KC, R* dfu = nullptr, R* dfv = nullptr)
 {
-    tendency_tile<TX, TY, UNI, R, DIAG, COR>(D, M, U, uin, vin, h, ubase, vbase, uout, vout,
-                                             coef, h_neglect, k0, KC, (int)blockIdx.x,
-                                             (int)blockIdx.y, (int)blockIdx.z, dfu, dfv);
+    tendency_tile<TX, TY, UNI, R, DIAG, COR, EXTV>(D, M, U, uin, vin, h, ubase, vbase, uout,
+                                                   vout, coef, h_neglect, k0, KC,
+                                                   (int)blockIdx.x, (int)blockIdx.y,
+                                                   (int)blockIdx.z, dfu, dfv);
+}
+
+// diffu, diffv from the general hor_visc kernel (EXTV), every Coriolis scheme.
+template <typename R, int COR>
+void launch_tendency_extv(const Dims& D, const Metrics& M, const UniMetrics& U, dim3 grid,
+                          dim3 block, const R* uin, const R* vin, const R* h, const R* ubase,
+                          const R* vbase, R* uout, R* vout, R coef, R h_neglect, int KC,
+                          cudaStream_t s, R* dfu, R* dfv)
+{
+    constexpr int TX = 32, TY = 8;
+    if (U.valid)
+        k_tendency<TX, TY, true, R, 3, false, COR, true><<<grid, block, 0, s>>>(
+            D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, KC, dfu, dfv);
+    else
+        k_tendency<TX, TY, false, R, 3, false, COR, true><<<grid, block, 0, s>>>(
+            D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, KC, dfu, dfv);
 }
 
 // The Arakawa schemes (COR = 2, 3): both metric forms, with or without the
@@ -397,7 +432,7 @@ cudaError_t launch_tendency_t(const Dims& D, const Metrics& M, const UniMetrics&
                               const R* uin, const R* vin, const R* h, const R* ubase,
                               const R* vbase, R* uout, R* vout, R coef, R h_neglect,
                               cudaStream_t s, R* dfu = nullptr, R* dfv = nullptr,
-                              int scheme = 1)
+                              int scheme = 1, bool ext_visc = false)
 {
     constexpr int TY = kTendTY;
     int nx = D.ie - D.is + 1, ny = D.je - D.js + 1;
@@ -405,6 +440,19 @@ cudaError_t launch_tendency_t(const Dims& D, const Metrics& M, const UniMetrics&
     int nchunks = (D.nk + kTendKC - 1) / kTendKC;
     dim3 grid((nx + kTendTX - 1) / kTendTX, (ny + TY - 1) / TY, nchunks);
     if ((dfu == nullptr) != (dfv == nullptr)) return cudaErrorInvalidValue;
+    if (ext_visc) {
+        if (!dfu || scheme < 1 || scheme > 3) return cudaErrorInvalidValue;
+        if (scheme == 1)
+            launch_tendency_extv<R, 1>(D, M, U, grid, block, uin, vin, h, ubase, vbase, uout,
+                                       vout, coef, h_neglect, kTendKC, s, dfu, dfv);
+        else if (scheme == 2)
+            launch_tendency_extv<R, 2>(D, M, U, grid, block, uin, vin, h, ubase, vbase, uout,
+                                       vout, coef, h_neglect, kTendKC, s, dfu, dfv);
+        else
+            launch_tendency_extv<R, 3>(D, M, U, grid, block, uin, vin, h, ubase, vbase, uout,
+                                       vout, coef, h_neglect, kTendKC, s, dfu, dfv);
+        return cudaGetLastError();
+    }
     if (scheme == 2)
         return launch_tendency_arakawa<R, 2>(D, M, U, grid, block, uin, vin, h, ubase, vbase,
                                              uout, vout, coef, h_neglect, kTendKC, s, dfu, dfv);

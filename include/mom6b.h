@@ -197,6 +197,22 @@ int mom6b_set_continuity_merid(mom6b_model *m, int on);
  * model's visc_rem_u / visc_rem_v.  FP64 form; synchronous. */
 int mom6b_continuity_pass(mom6b_model *m, int dir, double dt);
 
+/* hor_visc_init's scheme options (mom6_hor_visc_serial.F90:160-193); the
+ * model starts with the driver's: Laplacian only, free slip, no bounds.
+ * Smagorinsky applies to whichever of the Laplacian and biharmonic
+ * viscosities is on, Leith to the Laplacian and (with biharmonic) the
+ * biharmonic one; better_bound sets the thickness-aware bounds of both;
+ * modified_leith (CS%modified_Leith, no hor_visc_init argument) adds the
+ * divergence gradient to Leith's.  Kh is the config's; Ah the background
+ * biharmonic viscosity (hor_visc_init's default 1e10 m4 s-1).  Any option
+ * other than the driver's runs a separate hor_visc kernel before each
+ * tendency (FP64 form). */
+typedef struct mom6b_hor_visc {
+    int laplacian, biharmonic, smagorinsky, leith, no_slip, better_bound, modified_leith;
+    double Ah;
+} mom6b_hor_visc;
+int mom6b_set_hor_visc(mom6b_model *m, const mom6b_hor_visc *opts);
+
 /* The vertical-viscosity remnant (vert_visc_remnant,
  * mom6_vert_visc_serial.F90:295-387; the reference's step does not call it,
  * MOM6's continuity_PPM takes it as visc_rem_u / visc_rem_v).  on = 1: every

@@ -96,6 +96,18 @@ struct oracle_model {
         *hv_red_xy, *hv_dudx, *hv_dvdy, *hv_dvdx, *hv_dudy, *hv_sh_xx,
         *hv_sh_xy, *hv_str_xx, *hv_str_xy, *hv_h_u, *hv_h_v, *hv_hq, *hv_Kh;
     double hv_Kh_bg_min, hv_h_neglect;
+    /* the scheme branches (:37-57, :71-152): flags, background / maximum
+     * viscosities and the Smagorinsky / Leith constants (xx at h-points, xy
+     * at q-points), biharmonic metrics and the persistent work arrays */
+    int hv_lap, hv_bih, hv_smag_kh, hv_smag_ah, hv_leith_kh, hv_leith_ah, hv_no_slip,
+        hv_bound_kh, hv_bound_ah, hv_bb_kh, hv_bb_ah, hv_mod_leith;
+    double *hv_Ah_bg_xx, *hv_Ah_bg_xy, *hv_Kh_Max_xx, *hv_Kh_Max_xy, *hv_Ah_Max_xx,
+        *hv_Ah_Max_xy, *hv_L2c_xx, *hv_L2c_xy, *hv_Bc_xx, *hv_Bc_xy, *hv_L3c_xx,
+        *hv_L3c_xy, *hv_B6c_xx, *hv_B6c_xy, *hv_Idx2dyCu, *hv_Idxdy2u, *hv_Idx2dyCv,
+        *hv_Idxdy2v, *hv_Ah, *hv_Shear_mag, *hv_Del2u, *hv_Del2v, *hv_hrat_min,
+        *hv_vbr, *hv_vort, *hv_vort_dx, *hv_vort_dy, *hv_gvm_h, *hv_gvm_q, *hv_vvm,
+        *hv_Del2vort_q, *hv_div, *hv_div_dx, *hv_div_dy, *hv_gdm_h, *hv_bhstr_xx,
+        *hv_bhstr_xy;
 
     /* vert_visc CS, mom6_vert_visc_serial.F90:27-55 */
     double *vv_a_u, *vv_a_v, *vv_h_u, *vv_h_v, *vv_taux_bot, *vv_tauy_bot;
@@ -308,7 +320,16 @@ static void alloc_all(oracle_model *m) {
                      &m->hv_DX_dyBu, &m->hv_DY_dxBu, &m->hv_red_xx,
                      &m->hv_red_xy, &m->hv_dudx, &m->hv_dvdy, &m->hv_dvdx,
                      &m->hv_dudy, &m->hv_sh_xx, &m->hv_sh_xy, &m->hv_str_xx,
-                     &m->hv_str_xy, &m->hv_h_u, &m->hv_h_v, &m->hv_hq, &m->hv_Kh};
+                     &m->hv_str_xy, &m->hv_h_u, &m->hv_h_v, &m->hv_hq, &m->hv_Kh,
+                     &m->hv_Ah_bg_xx, &m->hv_Ah_bg_xy, &m->hv_Kh_Max_xx, &m->hv_Kh_Max_xy,
+                     &m->hv_Ah_Max_xx, &m->hv_Ah_Max_xy, &m->hv_L2c_xx, &m->hv_L2c_xy,
+                     &m->hv_Bc_xx, &m->hv_Bc_xy, &m->hv_L3c_xx, &m->hv_L3c_xy,
+                     &m->hv_B6c_xx, &m->hv_B6c_xy, &m->hv_Idx2dyCu, &m->hv_Idxdy2u,
+                     &m->hv_Idx2dyCv, &m->hv_Idxdy2v, &m->hv_Ah, &m->hv_Shear_mag,
+                     &m->hv_Del2u, &m->hv_Del2v, &m->hv_hrat_min, &m->hv_vbr, &m->hv_vort,
+                     &m->hv_vort_dx, &m->hv_vort_dy, &m->hv_gvm_h, &m->hv_gvm_q, &m->hv_vvm,
+                     &m->hv_Del2vort_q, &m->hv_div, &m->hv_div_dx, &m->hv_div_dy,
+                     &m->hv_gdm_h, &m->hv_bhstr_xx, &m->hv_bhstr_xy};
     for (size_t a = 0; a < sizeof(hv) / sizeof(hv[0]); ++a) *hv[a] = zalloc(n2d);
     m->hv_Kh_bg_min = 0.0;
     m->Angstrom_H = 1.0e-10; /* init_verticalGrid, mom6_types.F90:318-331 */
@@ -328,6 +349,10 @@ static void alloc_all(oracle_model *m) {
             A2(m->hv_Kh_bg_xx, i, j) = m->cfg.Kh;
             A2(m->hv_Kh_bg_xy, i, j) = m->cfg.Kh;
         }
+    {
+        oracle_hor_visc_opts o = {1, 0, 0, 0, 0, 0, 0, 1.0e10};
+        oracle_set_hor_visc(m, &o);
+    }
 
     /* vert_visc_init, mom6_vert_visc_serial.F90:60-112 */
     m->vv_a_u = zalloc(n3p); m->vv_a_v = zalloc(n3p);
@@ -489,7 +514,15 @@ void oracle_destroy(oracle_model *m) {
         &m->bt_vbt_prev, &m->bt_uhbt, &m->bt_vhbt, &m->bt_PFu, &m->bt_PFv,
         &m->bt_Cor_u, &m->bt_Cor_v, &m->bt_Datu, &m->bt_Datv, &m->bt_gtot_E,
         &m->bt_gtot_W, &m->bt_gtot_N, &m->bt_gtot_S, &m->bt_f_4_u, &m->bt_f_4_v,
-        &m->bt_rem_u, &m->bt_rem_v, &m->bt_ubt_av, &m->bt_vbt_av};
+        &m->bt_rem_u, &m->bt_rem_v, &m->bt_ubt_av, &m->bt_vbt_av,
+        &m->hv_Ah_bg_xx, &m->hv_Ah_bg_xy, &m->hv_Kh_Max_xx, &m->hv_Kh_Max_xy,
+        &m->hv_Ah_Max_xx, &m->hv_Ah_Max_xy, &m->hv_L2c_xx, &m->hv_L2c_xy, &m->hv_Bc_xx,
+        &m->hv_Bc_xy, &m->hv_L3c_xx, &m->hv_L3c_xy, &m->hv_B6c_xx, &m->hv_B6c_xy,
+        &m->hv_Idx2dyCu, &m->hv_Idxdy2u, &m->hv_Idx2dyCv, &m->hv_Idxdy2v, &m->hv_Ah,
+        &m->hv_Shear_mag, &m->hv_Del2u, &m->hv_Del2v, &m->hv_hrat_min, &m->hv_vbr,
+        &m->hv_vort, &m->hv_vort_dx, &m->hv_vort_dy, &m->hv_gvm_h, &m->hv_gvm_q,
+        &m->hv_vvm, &m->hv_Del2vort_q, &m->hv_div, &m->hv_div_dx, &m->hv_div_dy,
+        &m->hv_gdm_h, &m->hv_bhstr_xx, &m->hv_bhstr_xy};
     for (size_t a = 0; a < sizeof(p) / sizeof(p[0]); ++a) free(*p[a]);
     free(m->diag_work); free(m->diag_usum); free(m->diag_vsum);
     free(m->diag_KE); free(m->diag_mass);
@@ -550,10 +583,77 @@ void oracle_compute_transports(oracle_model *m, const double *u, const double *v
 }
 
 /* ------------------------------------------------------------------------ */
-/* hor_visc, mom6_hor_visc_serial.F90:464-1109.  Active configuration of the */
-/* driver: Laplacian, free slip, land-mask interpolation, no bounds; the    */
-/* biharmonic / Smagorinsky / Leith branches are never entered.  CS%Kh is a */
-/* persistent array shared by h- and q-points, as in the reference.         */
+/* hor_visc_init's scheme options, mom6_hor_visc_serial.F90:160-286: the     */
+/* flags as the optional arguments set them (:177-193), the background and   */
+/* maximum viscosities, the Smagorinsky / Leith constants and biharmonic     */
+/* metrics (:207-268), and the work arrays reset to their initial values     */
+/* (:271-282).  modified_Leith (:49) has no hor_visc_init argument; it is    */
+/* the extra flag here.                                                      */
+/* ------------------------------------------------------------------------ */
+int oracle_set_hor_visc(oracle_model *m, const oracle_hor_visc_opts *o) {
+    m->hv_lap = o->laplacian != 0;
+    m->hv_bih = o->biharmonic != 0;
+    m->hv_smag_kh = o->smagorinsky && m->hv_lap;
+    m->hv_smag_ah = o->smagorinsky && m->hv_bih;
+    m->hv_leith_kh = o->leith != 0;
+    m->hv_leith_ah = o->leith && m->hv_bih;
+    m->hv_no_slip = o->no_slip != 0;
+    m->hv_bb_kh = m->hv_bb_ah = m->hv_bound_kh = m->hv_bound_ah = o->better_bound != 0;
+    m->hv_mod_leith = o->modified_leith != 0;
+    const double Smag_Lap_const = 0.15, Smag_bi_const = 0.06, Leith_const = 1.0;
+    for (int j = m->jsd; j <= m->jed; ++j)
+        for (int i = m->isd; i <= m->ied; ++i) {
+            A2(m->hv_Idx2dyCu, i, j) = A2(m->IdxCu, i, j) * A2(m->IdxCu, i, j) * A2(m->IdyCu, i, j);
+            A2(m->hv_Idxdy2u, i, j) = A2(m->IdxCu, i, j) * A2(m->IdyCu, i, j) * A2(m->IdyCu, i, j);
+            A2(m->hv_Idx2dyCv, i, j) = A2(m->IdxCv, i, j) * A2(m->IdxCv, i, j) * A2(m->IdyCv, i, j);
+            A2(m->hv_Idxdy2v, i, j) = A2(m->IdxCv, i, j) * A2(m->IdyCv, i, j) * A2(m->IdyCv, i, j);
+            double h2 = A2(m->areaT, i, j);
+            double h3 = sqrt(h2) * h2;
+            double h4 = h2 * h2;
+            A2(m->hv_Ah_bg_xx, i, j) = o->Ah;
+            A2(m->hv_Ah_bg_xy, i, j) = o->Ah;
+            A2(m->hv_Kh_Max_xx, i, j) = 0.25 * h2 / 1.0;
+            A2(m->hv_Kh_Max_xy, i, j) = 0.25 * h2 / 1.0;
+            A2(m->hv_Ah_Max_xx, i, j) = 0.0625 * h4 / 1.0;
+            A2(m->hv_Ah_Max_xy, i, j) = 0.0625 * h4 / 1.0;
+            A2(m->hv_L2c_xx, i, j) = Smag_Lap_const * Smag_Lap_const * h2;
+            A2(m->hv_L2c_xy, i, j) = Smag_Lap_const * Smag_Lap_const * h2;
+            A2(m->hv_Bc_xx, i, j) = Smag_bi_const * Smag_bi_const * h4;
+            A2(m->hv_Bc_xy, i, j) = Smag_bi_const * Smag_bi_const * h4;
+            A2(m->hv_L3c_xx, i, j) = Leith_const * h3;
+            A2(m->hv_L3c_xy, i, j) = Leith_const * h3;
+            A2(m->hv_B6c_xx, i, j) = Leith_const * h3 * h3;
+            A2(m->hv_B6c_xy, i, j) = Leith_const * h3 * h3;
+        }
+    size_t n2d = (size_t)N1 * N2;
+    double *zero[] = {m->hv_dudx, m->hv_dvdy, m->hv_dvdx, m->hv_dudy, m->hv_sh_xx,
+                      m->hv_sh_xy, m->hv_str_xx, m->hv_str_xy, m->hv_h_u, m->hv_h_v,
+                      m->hv_hq, m->hv_Kh, m->hv_Ah, m->hv_Shear_mag, m->hv_Del2u,
+                      m->hv_Del2v, m->hv_vort, m->hv_vort_dx, m->hv_vort_dy, m->hv_gvm_h,
+                      m->hv_gvm_q, m->hv_vvm, m->hv_div, m->hv_div_dx, m->hv_div_dy,
+                      m->hv_gdm_h, m->hv_bhstr_xx, m->hv_bhstr_xy, m->hv_Del2vort_q};
+    for (size_t a = 0; a < sizeof(zero) / sizeof(zero[0]); ++a)
+        memset(zero[a], 0, n2d * sizeof(double));
+    for (size_t q = 0; q < n2d; ++q) {
+        m->hv_hrat_min[q] = 1.0;
+        m->hv_vbr[q] = 1.0;
+    }
+    return 0;
+}
+
+/* inv_PI3 = 1/3.14159265358979**3 and inv_PI6 = 1/3.14159265358979**6
+ * (mom6_hor_visc_serial.F90:154-155): the powers and quotients correctly
+ * rounded (a compile-time constant folded exactly; the run-time products
+ * x*x*x and (x*x*x)*(x*x*x) round to the same doubles). */
+static const double kInvPI3 = 0x1.08345eb45d78dp-5;
+static const double kInvPI6 = 0x1.10ac0e0a9d181p-10;
+#define SQ(x) ((x) * (x))
+
+/* ------------------------------------------------------------------------ */
+/* hor_visc, mom6_hor_visc_serial.F90:464-1109, every branch but FrictWork   */
+/* (compute_FrictWork has no setter).  CS%Kh and CS%Ah are persistent arrays */
+/* shared by h- and q-points, as in the reference; the other work arrays     */
+/* keep their values outside the ranges each step writes.                    */
 /* ------------------------------------------------------------------------ */
 static void hor_visc_rows(oracle_model *m, const double *u, const double *v,
                           const double *h, double *diffu, double *diffv, int k) {
@@ -563,7 +663,11 @@ static void hor_visc_rows(oracle_model *m, const double *u, const double *v,
     double *dudx = m->hv_dudx, *dvdy = m->hv_dvdy, *dvdx = m->hv_dvdx,
            *dudy = m->hv_dudy, *sh_xx = m->hv_sh_xx, *sh_xy = m->hv_sh_xy,
            *str_xx = m->hv_str_xx, *str_xy = m->hv_str_xy, *h_u = m->hv_h_u,
-           *h_v = m->hv_h_v, *hq = m->hv_hq, *Kh = m->hv_Kh;
+           *h_v = m->hv_h_v, *hq = m->hv_hq, *Kh = m->hv_Kh, *Ah = m->hv_Ah,
+           *Del2u = m->hv_Del2u, *Del2v = m->hv_Del2v, *vort = m->hv_vort,
+           *vdx = m->hv_vort_dx, *vdy = m->hv_vort_dy, *D2vq = m->hv_Del2vort_q,
+           *div = m->hv_div, *ddx = m->hv_div_dx, *ddy = m->hv_div_dy,
+           *hrat = m->hv_hrat_min, *vbr = m->hv_vbr;
     /* STEP 1 */
     OMP_FOR
     for (int j = Jsq; j <= Jeq + 1; ++j)
@@ -593,7 +697,9 @@ static void hor_visc_rows(oracle_model *m, const double *u, const double *v,
     OMP_FOR
     for (int J = Jsq; J <= Jeq; ++J)
         for (int I = Isq; I <= Ieq; ++I)
-            A2(sh_xy, I, J) = A2(m->mask2dBu, I, J) * (A2(dvdx, I, J) + A2(dudy, I, J));
+            A2(sh_xy, I, J) = (m->hv_no_slip ? (2.0 - A2(m->mask2dBu, I, J))
+                                             : A2(m->mask2dBu, I, J)) *
+                              (A2(dvdx, I, J) + A2(dudy, I, J));
     /* STEP 3 (use_land_mask) */
     OMP_FOR
     for (int j = js - 1; j <= je + 1; ++j)
@@ -610,39 +716,259 @@ static void hor_visc_rows(oracle_model *m, const double *u, const double *v,
         for (int I = Isq; I <= Ieq; ++I)
             A2(hq, I, J) = 0.25 * ((A3(h, I, J, k) + A3(h, I + 1, J + 1, k)) +
                                    (A3(h, I + 1, J, k) + A3(h, I, J + 1, k)));
-    /* STEP 8: Kh at h-points (interior only), floor, str_xx */
-    OMP_FOR
-    for (int j = js; j <= je; ++j)
-        for (int i = is; i <= ie; ++i) A2(Kh, i, j) = A2(m->hv_Kh_bg_xx, i, j);
-    OMP_FOR
-    for (int j = js; j <= je; ++j)
-        for (int i = is; i <= ie; ++i) A2(Kh, i, j) = MAX(A2(Kh, i, j), m->hv_Kh_bg_min);
-    OMP_FOR
-    for (int j = Jsq; j <= Jeq + 1; ++j)
-        for (int i = Isq; i <= Ieq + 1; ++i)
-            A2(str_xx, i, j) = -(A2(Kh, i, j) * A2(sh_xx, i, j));
+    /* STEP 4: Del2u, Del2v (:587-608) */
+    if (m->hv_bih) {
+        OMP_FOR
+        for (int j = js; j <= je; ++j)
+            for (int I = Isq; I <= Ieq; ++I)
+                A2(Del2u, I, j) =
+                    A2(m->hv_Idx2dyCu, I, j) * ((A2(m->hv_dx2q, I, j) * A2(sh_xy, I, j)) -
+                                                (A2(m->hv_dx2q, I, j - 1) * A2(sh_xy, I, j - 1))) +
+                    A2(m->hv_Idxdy2u, I, j) * ((A2(m->hv_dy2h, I + 1, j) * A2(sh_xx, I + 1, j)) -
+                                               (A2(m->hv_dy2h, I, j) * A2(sh_xx, I, j)));
+        OMP_FOR
+        for (int J = Jsq; J <= Jeq; ++J)
+            for (int i = is; i <= ie; ++i)
+                A2(Del2v, i, J) =
+                    A2(m->hv_Idxdy2v, i, J) * ((A2(m->hv_dy2q, i, J) * A2(sh_xy, i, J)) -
+                                               (A2(m->hv_dy2q, i - 1, J) * A2(sh_xy, i - 1, J))) -
+                    A2(m->hv_Idx2dyCv, i, J) * ((A2(m->hv_dx2h, i, J + 1) * A2(sh_xx, i, J + 1)) -
+                                                (A2(m->hv_dx2h, i, J) * A2(sh_xx, i, J)));
+    }
+    /* STEP 5: Leith vorticity (:612-714) */
+    if (m->hv_leith_kh) {
+        OMP_FOR
+        for (int J = Jsq; J <= Jeq; ++J)
+            for (int I = Isq; I <= Ieq; ++I)
+                A2(vort, I, J) = (m->hv_no_slip ? (2.0 - A2(m->mask2dBu, I, J))
+                                                : A2(m->mask2dBu, I, J)) *
+                                 (A2(dvdx, I, J) - A2(dudy, I, J));
+        OMP_FOR
+        for (int j = js; j <= je; ++j)
+            for (int i = is; i <= ie; ++i) {
+                double DY_dxBu_loc = A2(m->dyBu, i, j) * A2(m->IdxBu, i, j);
+                A2(vdx, i, j) = DY_dxBu_loc * ((A2(vort, i, j) * A2(m->IdyCu, i, j)) -
+                                               (A2(vort, i - 1, j) * A2(m->IdyCu, i - 1, j)));
+            }
+        OMP_FOR
+        for (int j = js; j <= je; ++j)
+            for (int I = Isq; I <= Ieq; ++I) {
+                double DX_dyBu_loc = A2(m->dxBu, I, j) * A2(m->IdyBu, I, j);
+                A2(vdy, I, j) = DX_dyBu_loc * ((A2(vort, I, j) * A2(m->IdxCv, I, j)) -
+                                               (A2(vort, I, j - 1) * A2(m->IdxCv, I, j - 1)));
+            }
+        if (m->hv_leith_ah) {
+            OMP_FOR
+            for (int J = Jsq; J <= Jeq; ++J)
+                for (int I = Isq; I <= Ieq; ++I)
+                    A2(D2vq, I, J) =
+                        A2(m->hv_DY_dxBu, I, J) * ((A2(vdx, I + 1, J) * A2(m->IdyCv, I + 1, J)) -
+                                                   (A2(vdx, I, J) * A2(m->IdyCv, I, J))) +
+                        A2(m->hv_DX_dyBu, I, J) * ((A2(vdy, I, J + 1) * A2(m->IdxCu, I, J + 1)) -
+                                                   (A2(vdy, I, J) * A2(m->IdxCu, I, J)));
+        }
+        if (m->hv_mod_leith) {
+            OMP_FOR
+            for (int j = js; j <= je; ++j)
+                for (int i = is; i <= ie; ++i) A2(div, i, j) = A2(dudx, i, j) + A2(dvdy, i, j);
+            OMP_FOR
+            for (int j = js; j <= je; ++j)
+                for (int I = Isq; I <= Ieq; ++I)
+                    A2(ddx, I, j) = A2(m->IdxCu, I, j) * (A2(div, I + 1, j) - A2(div, I, j));
+            OMP_FOR
+            for (int J = Jsq; J <= Jeq; ++J)
+                for (int i = is; i <= ie; ++i)
+                    A2(ddy, i, J) = A2(m->IdyCv, i, J) * (A2(div, i, J + 1) - A2(div, i, J));
+            OMP_FOR
+            for (int j = js; j <= je; ++j)
+                for (int i = is; i <= ie; ++i)
+                    A2(m->hv_gdm_h, i, j) =
+                        sqrt(SQ(0.5 * (A2(ddx, i, j) + A2(ddx, i - 1, j))) +
+                             SQ(0.5 * (A2(ddy, i, j) + A2(ddy, i, j - 1))));
+        } else {
+            OMP_FOR
+            for (int j = js; j <= je; ++j)
+                for (int i = is; i <= ie; ++i) A2(m->hv_gdm_h, i, j) = 0.0;
+        }
+        OMP_FOR
+        for (int j = js; j <= je; ++j)
+            for (int i = is; i <= ie; ++i) {
+                A2(m->hv_gvm_h, i, j) = sqrt(SQ(0.5 * (A2(vdx, i, j) + A2(vdx, i, j - 1))) +
+                                             SQ(0.5 * (A2(vdy, i, j) + A2(vdy, i - 1, j))));
+                A2(m->hv_vvm, i, j) = A2(m->hv_gvm_h, i, j) + A2(m->hv_gdm_h, i, j);
+            }
+        OMP_FOR
+        for (int J = Jsq; J <= Jeq; ++J)
+            for (int I = Isq; I <= Ieq; ++I)
+                A2(m->hv_gvm_q, I, J) = sqrt(SQ(0.5 * (A2(vdx, I, J) + A2(vdx, I + 1, J))) +
+                                             SQ(0.5 * (A2(vdy, I, J) + A2(vdy, I, J + 1))));
+    }
+    /* STEP 6: Smagorinsky shear magnitude (:718-727) */
+    if (m->hv_smag_kh || m->hv_smag_ah) {
+        OMP_FOR
+        for (int j = js; j <= je; ++j)
+            for (int i = is; i <= ie; ++i) {
+                double sh_xx_sq = SQ(A2(sh_xx, i, j));
+                double sh_xy_sq = 0.25 * ((SQ(A2(sh_xy, i - 1, j - 1)) + SQ(A2(sh_xy, i, j))) +
+                                          (SQ(A2(sh_xy, i - 1, j)) + SQ(A2(sh_xy, i, j - 1))));
+                A2(m->hv_Shear_mag, i, j) = sqrt(sh_xx_sq + sh_xy_sq);
+            }
+    }
+    /* STEP 7: thickness ratio (:732-739) */
+    if (m->hv_bb_kh || m->hv_bb_ah) {
+        OMP_FOR
+        for (int j = js; j <= je; ++j)
+            for (int i = is; i <= ie; ++i) {
+                double h_min = MIN(MIN(MIN(A2(h_u, i, j), A2(h_u, i - 1, j)), A2(h_v, i, j)),
+                                   A2(h_v, i, j - 1));
+                A2(hrat, i, j) = MIN(1.0, h_min / (A3(h, i, j, k) + h_neglect));
+            }
+    }
+    /* STEP 8: Kh at h-points, str_xx (:744-816) */
+    if (m->hv_lap) {
+        OMP_FOR
+        for (int j = js; j <= je; ++j)
+            for (int i = is; i <= ie; ++i) {
+                double K = A2(m->hv_Kh_bg_xx, i, j);
+                if (m->hv_smag_kh) K = MAX(K, A2(m->hv_L2c_xx, i, j) * A2(m->hv_Shear_mag, i, j));
+                if (m->hv_leith_kh)
+                    K = MAX(K, A2(m->hv_L3c_xx, i, j) * A2(m->hv_vvm, i, j) * kInvPI3);
+                K = MAX(K, m->hv_Kh_bg_min);
+                if (m->hv_bb_kh && m->hv_bb_ah) {
+                    A2(vbr, i, j) = 1.0;
+                    double Kh_max_here = A2(hrat, i, j) * A2(m->hv_Kh_Max_xx, i, j);
+                    if (K >= Kh_max_here) {
+                        A2(vbr, i, j) = 0.0;
+                        K = Kh_max_here;
+                    } else if (K > 0.0) {
+                        A2(vbr, i, j) = 1.0 - K / Kh_max_here;
+                    }
+                } else if (m->hv_bb_kh) {
+                    K = MIN(K, A2(hrat, i, j) * A2(m->hv_Kh_Max_xx, i, j));
+                } else if (m->hv_bound_kh) {
+                    K = MIN(K, A2(m->hv_Kh_Max_xx, i, j));
+                }
+                A2(Kh, i, j) = K;
+            }
+        OMP_FOR
+        for (int j = Jsq; j <= Jeq + 1; ++j)
+            for (int i = Isq; i <= Ieq + 1; ++i)
+                A2(str_xx, i, j) = -(A2(Kh, i, j) * A2(sh_xx, i, j));
+    } else {
+        OMP_FOR
+        for (int j = Jsq; j <= Jeq + 1; ++j)
+            for (int i = Isq; i <= Ieq + 1; ++i) A2(str_xx, i, j) = 0.0;
+    }
+    /* STEP 9: Ah at h-points, biharmonic str_xx (:824-896) */
+    if (m->hv_bih) {
+        OMP_FOR
+        for (int j = js; j <= je; ++j)
+            for (int i = is; i <= ie; ++i) {
+                double A = A2(m->hv_Ah_bg_xx, i, j);
+                if (m->hv_smag_ah) A = MAX(A, A2(m->hv_Bc_xx, i, j) * A2(m->hv_Shear_mag, i, j));
+                if (m->hv_leith_ah) {
+                    double Del2vort_h = 0.25 * ((A2(D2vq, i, j) + A2(D2vq, i - 1, j - 1)) +
+                                                (A2(D2vq, i - 1, j) + A2(D2vq, i, j - 1)));
+                    A = MAX(A, A2(m->hv_B6c_xx, i, j) * fabs(Del2vort_h) * kInvPI6);
+                }
+                if (m->hv_bb_ah) {
+                    if (m->hv_bb_kh)
+                        A = MIN(A, A2(vbr, i, j) * A2(hrat, i, j) * A2(m->hv_Ah_Max_xx, i, j));
+                    else
+                        A = MIN(A, A2(hrat, i, j) * A2(m->hv_Ah_Max_xx, i, j));
+                } else if (m->hv_bound_ah) {
+                    A = MIN(A, A2(m->hv_Ah_Max_xx, i, j));
+                }
+                A2(Ah, i, j) = A;
+            }
+        OMP_FOR
+        for (int j = Jsq; j <= Jeq + 1; ++j)
+            for (int i = Isq; i <= Ieq + 1; ++i) {
+                double d_del2u = (A2(m->IdyCu, i, j) * A2(Del2u, i, j)) -
+                                 (A2(m->IdyCu, i - 1, j) * A2(Del2u, i - 1, j));
+                double d_del2v = (A2(m->IdxCv, i, j) * A2(Del2v, i, j)) -
+                                 (A2(m->IdxCv, i, j - 1) * A2(Del2v, i, j - 1));
+                double d_str = A2(Ah, i, j) * ((A2(m->hv_DY_dxT, i, j) * d_del2u) -
+                                               (A2(m->hv_DX_dyT, i, j) * d_del2v));
+                A2(m->hv_bhstr_xx, i, j) = d_str * (A3(h, i, j, k) * A2(m->hv_red_xx, i, j));
+                A2(str_xx, i, j) = A2(str_xx, i, j) + d_str;
+            }
+    }
     /* STEP 10 */
     OMP_FOR
     for (int j = Jsq; j <= Jeq + 1; ++j)
         for (int i = Isq; i <= Ieq + 1; ++i)
             A2(str_xx, i, j) = A2(str_xx, i, j) * (A3(h, i, j, k) * A2(m->hv_red_xx, i, j));
-    /* STEP 11: Kh at q-points (overwrites the shared CS%Kh), str_xy */
-    OMP_FOR
-    for (int J = Jsq; J <= Jeq; ++J)
-        for (int I = Isq; I <= Ieq; ++I) A2(Kh, I, J) = A2(m->hv_Kh_bg_xy, I, J);
-    OMP_FOR
-    for (int J = Jsq; J <= Jeq; ++J)
-        for (int I = Isq; I <= Ieq; ++I) A2(Kh, I, J) = MAX(A2(Kh, I, J), m->hv_Kh_bg_min);
+    /* STEP 11: Kh at q-points (overwrites the shared CS%Kh), str_xy (:900-974) */
+    if (m->hv_lap) {
+        OMP_FOR
+        for (int J = Jsq; J <= Jeq; ++J)
+            for (int I = Isq; I <= Ieq; ++I) {
+                double K = A2(m->hv_Kh_bg_xy, I, J);
+                if (m->hv_smag_kh) {
+                    double sh_xx_sq = 0.25 * ((SQ(A2(sh_xx, I, J)) + SQ(A2(sh_xx, I + 1, J + 1))) +
+                                              (SQ(A2(sh_xx, I + 1, J)) + SQ(A2(sh_xx, I, J + 1))));
+                    double sh_xy_sq = SQ(A2(sh_xy, I, J));
+                    K = MAX(K, A2(m->hv_L2c_xy, I, J) * sqrt(sh_xx_sq + sh_xy_sq));
+                }
+                if (m->hv_leith_kh)
+                    K = MAX(K, A2(m->hv_L3c_xy, I, J) * A2(m->hv_gvm_q, I, J) * kInvPI3);
+                K = MAX(K, m->hv_Kh_bg_min);
+                if (m->hv_bb_kh) {
+                    double h_min = 0.25 * ((A2(hrat, I, J) + A2(hrat, I + 1, J + 1)) +
+                                           (A2(hrat, I + 1, J) + A2(hrat, I, J + 1)));
+                    K = MIN(K, h_min * A2(m->hv_Kh_Max_xy, I, J));
+                } else if (m->hv_bound_kh) {
+                    K = MIN(K, A2(m->hv_Kh_Max_xy, I, J));
+                }
+                A2(Kh, I, J) = K;
+                A2(str_xy, I, J) = -(K * A2(sh_xy, I, J));
+            }
+    } else {
+        OMP_FOR
+        for (int J = Jsq; J <= Jeq; ++J)
+            for (int I = Isq; I <= Ieq; ++I) A2(str_xy, I, J) = 0.0;
+    }
+    /* STEP 12: Ah at q-points, biharmonic str_xy (:979-1035) */
+    if (m->hv_bih) {
+        OMP_FOR
+        for (int J = Jsq; J <= Jeq; ++J)
+            for (int I = Isq; I <= Ieq; ++I) {
+                double A = A2(m->hv_Ah_bg_xy, I, J);
+                if (m->hv_smag_ah) {
+                    double sh_xx_sq = 0.25 * ((SQ(A2(sh_xx, I, J)) + SQ(A2(sh_xx, I + 1, J + 1))) +
+                                              (SQ(A2(sh_xx, I + 1, J)) + SQ(A2(sh_xx, I, J + 1))));
+                    double sh_xy_sq = SQ(A2(sh_xy, I, J));
+                    A = MAX(A, A2(m->hv_Bc_xy, I, J) * sqrt(sh_xx_sq + sh_xy_sq));
+                }
+                if (m->hv_leith_ah)
+                    A = MAX(A, A2(m->hv_B6c_xy, I, J) * fabs(A2(D2vq, I, J)) * kInvPI6);
+                if (m->hv_bb_ah) {
+                    double h_min = 0.25 * ((A2(hrat, I, J) + A2(hrat, I + 1, J + 1)) +
+                                           (A2(hrat, I + 1, J) + A2(hrat, I, J + 1)));
+                    A = MIN(A, h_min * A2(m->hv_Ah_Max_xy, I, J));
+                } else if (m->hv_bound_ah) {
+                    A = MIN(A, A2(m->hv_Ah_Max_xy, I, J));
+                }
+                A2(Ah, I, J) = A;
+                double d_str =
+                    A * ((A2(m->hv_DY_dxBu, I, J) * ((A2(Del2v, I + 1, J) * A2(m->IdyCv, I + 1, J)) -
+                                                     (A2(Del2v, I, J) * A2(m->IdyCv, I, J)))) +
+                         (A2(m->hv_DX_dyBu, I, J) * ((A2(Del2u, I, J + 1) * A2(m->IdxCu, I, J + 1)) -
+                                                     (A2(Del2u, I, J) * A2(m->IdxCu, I, J)))));
+                A2(m->hv_bhstr_xy, I, J) = d_str * (A2(hq, I, J) * A2(m->hv_red_xy, I, J));
+                A2(str_xy, I, J) = A2(str_xy, I, J) + d_str;
+            }
+    }
+    /* STEP 13 */
     OMP_FOR
     for (int J = Jsq; J <= Jeq; ++J)
         for (int I = Isq; I <= Ieq; ++I)
-            A2(str_xy, I, J) = -(A2(Kh, I, J) * A2(sh_xy, I, J));
-    /* STEP 13 (free slip) */
-    OMP_FOR
-    for (int J = Jsq; J <= Jeq; ++J)
-        for (int I = Isq; I <= Ieq; ++I)
-            A2(str_xy, I, J) = A2(str_xy, I, J) *
-                               (A2(hq, I, J) * A2(m->mask2dBu, I, J) * A2(m->hv_red_xy, I, J));
+            A2(str_xy, I, J) =
+                m->hv_no_slip
+                    ? A2(str_xy, I, J) * (A2(hq, I, J) * A2(m->hv_red_xy, I, J))
+                    : A2(str_xy, I, J) *
+                          (A2(hq, I, J) * A2(m->mask2dBu, I, J) * A2(m->hv_red_xy, I, J));
     /* STEP 14 */
     OMP_FOR
     for (int j = js; j <= je; ++j)
@@ -665,6 +991,7 @@ static void hor_visc_rows(oracle_model *m, const double *u, const double *v,
                  A2(m->IareaCv, i, J)) /
                 (A2(h_v, i, J) + h_neglect);
 }
+#undef SQ
 
 void oracle_hor_visc(oracle_model *m, const double *u, const double *v,
                      const double *h, double *diffu, double *diffv) {

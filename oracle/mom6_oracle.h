@@ -108,6 +108,16 @@ void oracle_vert_visc_remnant(oracle_model *m, double dt);
  * :211-248): 1 SADOURNY75_ENERGY (default, the driver's), 2 ARAKAWA_HSU90,
  * 3 ARAKAWA_LAMB81.  0 on success. */
 int oracle_set_coriolis_scheme(oracle_model *m, int scheme);
+
+/* hor_visc_init's scheme options (mom6_hor_visc_serial.F90:160-193): the
+ * model is created with Laplacian only (the driver's).  modified_leith sets
+ * CS%modified_Leith, which hor_visc_init has no argument for.  Resets the
+ * module's work arrays as hor_visc_init does.  0 on success. */
+typedef struct {
+    int laplacian, biharmonic, smagorinsky, leith, no_slip, better_bound, modified_leith;
+    double Ah;   /* background biharmonic viscosity [m4 s-1] (default 1e10) */
+} oracle_hor_visc_opts;
+int oracle_set_hor_visc(oracle_model *m, const oracle_hor_visc_opts *o);
 void oracle_continuity_merid(oracle_model *m, const double *v, const double *hin,
                              double *h, double *vh, double dt);
 

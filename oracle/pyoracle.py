@@ -26,6 +26,21 @@ FIELDS_3D = {"u", "v", "h", "h0", "uh", "vh", "up", "vp", "hu_bt", "Ray_u",
              "Ray_v", "CAu", "CAv", "diffu", "diffv", "hv_bt", "visc_rem_u", "visc_rem_v"}
 
 
+class HorViscOpts(ctypes.Structure):
+    """hor_visc_init's scheme options (mom6_hor_visc_serial.F90:160-193)."""
+    _fields_ = [("laplacian", ctypes.c_int), ("biharmonic", ctypes.c_int),
+                ("smagorinsky", ctypes.c_int), ("leith", ctypes.c_int),
+                ("no_slip", ctypes.c_int), ("better_bound", ctypes.c_int),
+                ("modified_leith", ctypes.c_int), ("Ah", ctypes.c_double)]
+
+
+def hor_visc_opts(laplacian=True, biharmonic=False, smagorinsky=False, leith=False,
+                  no_slip=False, better_bound=False, modified_leith=False, Ah=1.0e10):
+    return HorViscOpts(int(bool(laplacian)), int(bool(biharmonic)), int(bool(smagorinsky)),
+                       int(bool(leith)), int(bool(no_slip)), int(bool(better_bound)),
+                       int(bool(modified_leith)), float(Ah))
+
+
 class Config(ctypes.Structure):
     _fields_ = [("ni", ctypes.c_int), ("nj", ctypes.c_int), ("nk", ctypes.c_int),
                 ("bt_nsteps", ctypes.c_int), ("init_mode", ctypes.c_int),
@@ -77,6 +92,8 @@ def lib(parallel=False):
         L.oracle_set_remnant.argtypes = [vp, ctypes.c_int]
         L.oracle_vert_visc_remnant.argtypes = [vp, d]
         L.oracle_set_coriolis_scheme.restype = ctypes.c_int
+        L.oracle_set_hor_visc.argtypes = [vp, ctypes.POINTER(HorViscOpts)]
+        L.oracle_set_hor_visc.restype = ctypes.c_int
         L.oracle_halo_fill.argtypes = [vp, P(d), ctypes.c_int, ctypes.c_int]
         L.oracle_normal.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64]
         L.oracle_normal.restype = d
@@ -101,7 +118,7 @@ class Oracle:
     """One oracle model (grid + state + persistent module work arrays)."""
 
     def __init__(self, ni, nj, nk, bt_nsteps, init_mode=INIT_CFG, seed=0,
-                 dt=None, Kh=None, bc_fill=None, threads=None):
+                 dt=None, Kh=None, bc_fill=None, threads=None, dx_km=None):
         """threads: None for the single-threaded build, else the OpenMP build
         on that many threads (0: all the runtime offers)."""
         L = lib(parallel=threads is not None)
@@ -116,6 +133,8 @@ class Oracle:
             c.Kh = Kh
         if bc_fill is not None:
             c.bc_fill = int(bc_fill)
+        if dx_km is not None:
+            c.dx_km = dx_km
         self.cfg = c
         self._m = L.oracle_create(ctypes.byref(c))
         if not self._m:
@@ -197,6 +216,13 @@ class Oracle:
         """1 SADOURNY75_ENERGY, 2 ARAKAWA_HSU90, 3 ARAKAWA_LAMB81."""
         if self._L.oracle_set_coriolis_scheme(self._m, int(scheme)) != 0:
             raise ValueError(scheme)
+
+    def set_hor_visc(self, **opts):
+        """hor_visc_init's options: laplacian, biharmonic, smagorinsky, leith,
+        no_slip, better_bound, modified_leith (bools) and Ah."""
+        o = hor_visc_opts(**opts)
+        if self._L.oracle_set_hor_visc(self._m, ctypes.byref(o)) != 0:
+            raise ValueError(opts)
 
     def set_remnant(self, on=True):
         """Feed the vertical-viscosity remnant to continuity from now on."""
