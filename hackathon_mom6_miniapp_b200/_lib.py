@@ -147,6 +147,7 @@ def library():
     L.mom6b_set_continuity_merid.argtypes = [vp, ctypes.c_int]
     L.mom6b_set_visc_remnant.argtypes = [vp, ctypes.c_int]
     L.mom6b_set_hor_visc.argtypes = [vp, ctypes.POINTER(HorVisc)]
+    L.mom6b_set_bt_overlap.argtypes = [vp, ctypes.c_int]
     L.mom6b_continuity_pass.argtypes = [vp, ctypes.c_int, ctypes.c_double]
     L.mom6b_set_coriolis_scheme.argtypes = [vp, ctypes.c_int]
     L.mom6b_read_field_bin.argtypes = [vp, ctypes.c_int, cp]
@@ -287,6 +288,10 @@ class Model:
                     int(bool(leith)), int(bool(no_slip)), int(bool(better_bound)),
                     int(bool(modified_leith)), float(Ah))
         _check(library().mom6b_set_hor_visc(self._m, ctypes.byref(o)))
+
+    def set_bt_overlap(self, on=True):
+        """Run the barotropic chain on a second stream beside the 3-D chain."""
+        _check(library().mom6b_set_bt_overlap(self._m, int(bool(on))))
 
     def set_visc_remnant(self, on=True):
         """Every vertvisc also writes visc_rem_u / visc_rem_v and the continuity

@@ -1391,6 +1391,17 @@ extern "C" int mom6b_set_continuity_merid(mom6b_model* m, int on)
     return MOM6B_OK;
 }
 
+extern "C" int mom6b_set_bt_overlap(mom6b_model* m, int on)
+{
+    if (!m) return fail(MOM6B_ERR_ARG, "null model");
+    CK(cudaSetDevice(m->cfg.device));
+    CK(cudaStreamSynchronize(m->s3d));
+    CK(cudaStreamSynchronize(m->s2d));
+    m->overlap_bt = on != 0;
+    invalidate_graph(m);
+    return MOM6B_OK;
+}
+
 extern "C" int mom6b_set_hor_visc(mom6b_model* m, const mom6b_hor_visc* o)
 {
     if (!m || !o) return fail(MOM6B_ERR_ARG, "null argument");

@@ -197,6 +197,14 @@ int mom6b_set_continuity_merid(mom6b_model *m, int on);
  * model's visc_rem_u / visc_rem_v.  FP64 form; synchronous. */
 int mom6b_continuity_pass(mom6b_model *m, int dir, double dt);
 
+/* on = 1: the barotropic chain of each step (both btstep calls and their
+ * halo fills) runs on a second stream concurrently with the 3-D chain; its
+ * inputs (eta, ubt, vbt) and outputs are disjoint from the 3-D chain's, so
+ * the results are unchanged.  The btstep is a cooperative launch whose
+ * blocks wait at grid barriers; blocks that become resident while the 3-D
+ * kernels hold SMs wait (bounded) for the rest. */
+int mom6b_set_bt_overlap(mom6b_model *m, int on);
+
 /* hor_visc_init's scheme options (mom6_hor_visc_serial.F90:160-193); the
  * model starts with the driver's: Laplacian only, free slip, no bounds.
  * Smagorinsky applies to whichever of the Laplacian and biharmonic
