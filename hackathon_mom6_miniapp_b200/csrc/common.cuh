@@ -52,6 +52,26 @@ constexpr double kRho0 = 1035.0;
 // Status flags written by kernels that can give up (grid barrier timeouts).
 enum : int { kDevOk = 0, kDevTimeout = 1 };
 
+// One element global -> shared with cp.async (bypasses registers); ok = false
+// writes zero (src-size 0) and reads nothing.
+template <typename R>
+__device__ __forceinline__ void cp_async_elem(R* sdst, const R* gsrc, bool ok)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    if constexpr (sizeof(R) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gsrc),
+                     "r"(ok ? 8 : 0)
+                     : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(gsrc),
+                     "r"(ok ? 4 : 0)
+                     : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+// the calling thread's copies except the most recent group are complete
+__device__ __forceinline__ void cp_async_wait_prior() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
 __device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }
 __device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }
 

@@ -34,24 +34,6 @@ namespace mom6b {
 // per row); otherwise every metric is read from its 2-D array.  The CTA with
 // block coordinates (bx, by, bz) owns the tile i0 = is + bx TX, j0 = js + by TY
 // and walks the KC consecutive layers from k0 + bz KC.
-// One element global -> shared with cp.async (bypasses registers); ok = false
-// writes zero (src-size 0) and reads nothing.
-template <typename R>
-__device__ __forceinline__ void cp_async_elem(R* sdst, const R* gsrc, bool ok)
-{
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
-    if constexpr (sizeof(R) == 8)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gsrc),
-                     "r"(ok ? 8 : 0)
-                     : "memory");
-    else
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(gsrc),
-                     "r"(ok ? 4 : 0)
-                     : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
 // UNI selects the uniform-metric instantiation (metrics as scalars, Coriolis
 // per row); otherwise every metric is read from its 2-D array.  The CTA with
 // block coordinates (bx, by, bz) owns the tile i0 = is + bx TX, j0 = js + by TY

@@ -42,12 +42,17 @@ constexpr int vv_min_blocks() { return sizeof(R) == 4 ? 10 : 6; }
 // :295-387) of every column into rem_u / rem_v -- the same elimination with
 // h_u as the right-hand side, sharing b1, d1 and c1 with the velocity's;
 // 1 in masked columns.
-template <int KMAX, int CH, typename R, bool REM = false>
+// ASYNC: sweeps 1 and 2 stage the next chunk's h, h(neighbour) and velocity
+// in shared memory with cp.async (per-thread slots of stage, [2][CH][3][128])
+// while the current chunk is computed, instead of loading each chunk into
+// registers before computing it.  The arithmetic is unchanged.
+template <int KMAX, int CH, typename R, bool REM = false, bool ASYNC = false>
 __device__ __forceinline__ void
 vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restrict__ v,
                 const R* __restrict__ h, double dt, const VVParams& P,
                 double* __restrict__ taux_bot, double* __restrict__ tauy_bot, int bx, int by,
-                double* __restrict__ rem_u = nullptr, double* __restrict__ rem_v = nullptr)
+                double* __restrict__ rem_u = nullptr, double* __restrict__ rem_v = nullptr,
+                R* stage = nullptr)
 {
     // Coefficients (h_harm, z_i, botfn, hvel, a(K)) and the tridiagonal
     // elimination (b1, d1, c1, the eliminated velocity and the back
@@ -101,10 +106,41 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
     const C Kv_extra_bbl = (C)P.Kv_extra_bbl, Hmix = (C)P.Hmix;
 
     // ---- sweep 1: h_harm and z_i bottom-up (vert_visc_coef :160-179) -----
+    // stage slot (b, c, f) of this thread
+    const int tid = (int)threadIdx.x;
+    auto ST = [&](int b, int c, int f) -> R& { return stage[((b * CH + c) * 3 + f) * 128 + tid]; };
     C z = C(0.0);
     slot[nz + 1] = vv_botfn(C(0.0));
-    for (int kt = nz; kt >= 2; kt -= CH) {
+    auto stage1 = [&](int kt, int b) {
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            const int k = kt - c;
+            const bool ok = k >= 2;
+            const size_t o = ok ? (size_t)(k - 1) * plane : 0;
+            cp_async_elem(&ST(b, c, 0), hc + o, ok);
+            cp_async_elem(&ST(b, c, 1), hn_ + o, ok);
+        }
+        cp_async_commit();
+    };
+    if constexpr (ASYNC) {
+        if (nz >= 2) stage1(nz, 0);
+    }
+    for (int kt = nz, it = 0; kt >= 2; kt -= CH, ++it) {
         C a0[CH], a1[CH];
+        if constexpr (ASYNC) {
+            const int b = it & 1;
+            if (kt - CH >= 2) {
+                stage1(kt - CH, b ^ 1);
+                cp_async_wait_prior();
+            } else {
+                cp_async_wait_all();
+            }
+#pragma unroll
+            for (int c = 0; c < CH; ++c) {
+                a0[c] = ST(b, c, 0);
+                a1[c] = ST(b, c, 1);
+            }
+        } else {
 #pragma unroll
         for (int c = 0; c < CH; ++c) {
             int k = kt - c;
@@ -112,6 +148,7 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
                 a0[c] = hc[(size_t)(k - 1) * plane];
                 a1[c] = hn_[(size_t)(k - 1) * plane];
             }
+        }
         }
 #pragma unroll
         for (int c = 0; c < CH; ++c) {
@@ -181,13 +218,47 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
         r_prev = b1 * h_u;
         rcol[0] = r_prev;
     }
-    for (int kt = 2; kt <= nz; kt += CH) {
+    // sweep 2 stages h, h(neighbour) and vel of layer k + 1 for k in the
+    // chunk; every staged layer is read before this thread overwrites it
+    auto stage2 = [&](int kt, int b) {
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            const int k = kt + c;
+            const bool ok = k < nz;
+            const size_t o = ok ? (size_t)k * plane : 0;
+            cp_async_elem(&ST(b, c, 0), hc + o, ok);
+            cp_async_elem(&ST(b, c, 1), hn_ + o, ok);
+            cp_async_elem(&ST(b, c, 2), (const R*)vc + o, ok);
+        }
+        cp_async_commit();
+    };
+    if constexpr (ASYNC) {
+        if (nz >= 2) stage2(2, 0);
+    }
+    for (int kt = 2, it = 0; kt <= nz; kt += CH, ++it) {
         // layers kt .. kt+CH-1 are eliminated; they need h and vel of the
         // layer below each (k + 1) and Ray of k
         // and botfn of interfaces k+1, k+2 (slots kt+1 .. kt+CH+1, read
         // before this chunk overwrites slots kt .. kt+CH-1 with c1)
         C p0[CH], p1[CH], pb[CH + 1];
         E pv[CH], pr[CH];
+        if constexpr (ASYNC) {
+            const int b = it & 1;
+            if (kt + CH <= nz) {
+                stage2(kt + CH, b ^ 1);
+                cp_async_wait_prior();
+            } else {
+                cp_async_wait_all();
+            }
+#pragma unroll
+            for (int c = 0; c < CH; ++c) {
+                const int k = kt + c;
+                p0[c] = ST(b, c, 0);
+                p1[c] = ST(b, c, 1);
+                pv[c] = (E)ST(b, c, 2);
+                if (k <= nz) pr[c] = ray_on[k - 1] ? (E)rc[(size_t)(k - 1) * plane] : E(0.0);
+            }
+        } else {
 #pragma unroll
         for (int c = 0; c < CH; ++c) {
             int k = kt + c;
@@ -197,6 +268,7 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
                 pv[c] = vc[(size_t)k * plane];
             }
             if (k <= nz) pr[c] = ray_on[k - 1] ? (E)rc[(size_t)(k - 1) * plane] : E(0.0);
+        }
         }
 #pragma unroll
         for (int c = 0; c <= CH; ++c)
@@ -274,15 +346,17 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
 }
 
 // MINB: the CTAs per SM the register allocation is held to.
-template <int KMAX, int CH, typename R, int MINB = 1, bool REM = false>
+template <int KMAX, int CH, typename R, int MINB = 1, bool REM = false, bool ASYNC = false>
 __global__ void __launch_bounds__(128, MINB)
 k_vertvisc_pf(Dims D, Metrics M, R* __restrict__ u, R* __restrict__ v,
               const R* __restrict__ h, double dt, VVParams P,
               double* __restrict__ taux_bot, double* __restrict__ tauy_bot,
               double* __restrict__ rem_u = nullptr, double* __restrict__ rem_v = nullptr)
 {
-    vertvisc_column<KMAX, CH, R, REM>(D, M, u, v, h, dt, P, taux_bot, tauy_bot,
-                                      (int)blockIdx.x, (int)blockIdx.y, rem_u, rem_v);
+    __shared__ R stage[ASYNC ? 2 * CH * 3 * 128 : 1];
+    vertvisc_column<KMAX, CH, R, REM, ASYNC>(D, M, u, v, h, dt, P, taux_bot, tauy_bot,
+                                             (int)blockIdx.x, (int)blockIdx.y, rem_u, rem_v,
+                                             stage);
 }
 
 template <int KMAX, typename R>
@@ -295,12 +369,33 @@ static cudaError_t launch_vv_pf(const Dims& D, const Metrics& M, R* u, R* v, con
     int ncol = D.ie - D.is + 2;
     int nrows = (D.je - D.js + 1) + (D.je - D.js + 2);
     dim3 grid((ncol + nb - 1) / nb, nrows, 1);
-    static int chunk = -1, minb = -1;
+    static int chunk = -1, minb = -1, async = -1;
     if (chunk < 0) {
         const char* e = getenv("MOM6B_VV_CHUNK");
         chunk = e ? atoi(e) : kVvChunk;
         const char* b = getenv("MOM6B_VV_MINB");
         minb = b ? atoi(b) : vv_min_blocks<R>();
+        // staged sweeps: FP64 2.215 ms per step against 2.285 loaded into
+        // registers; the FP32 form is faster loading into registers (1.02
+        // against 1.10-1.14 ms)
+        const char* a = getenv("MOM6B_VV_ASYNC");
+        async = a ? atoi(a) : (sizeof(R) == 8 ? 6 : 0);
+    }
+    if (async && !rem_u) {
+        // staged sweeps, the register cap by the async minb
+        if (async == 8)
+            k_vertvisc_pf<KMAX, 4, R, 8, false, true><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P,
+                                                                        taux_bot, tauy_bot);
+        else if (async == 4)
+            k_vertvisc_pf<KMAX, 4, R, 4, false, true><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P,
+                                                                        taux_bot, tauy_bot);
+        else if (async == 10 && sizeof(R) == 4)
+            k_vertvisc_pf<KMAX, 4, R, 10, false, true><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P,
+                                                                         taux_bot, tauy_bot);
+        else
+            k_vertvisc_pf<KMAX, 4, R, 6, false, true><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P,
+                                                                        taux_bot, tauy_bot);
+        return cudaGetLastError();
     }
     if constexpr (sizeof(R) == 8) {
         if (rem_u) {   // with the remnant (the FP64 form's register cap)
