@@ -580,6 +580,10 @@ def run_profile_case(args):
     n = args.profile_case
     m = Model(n, n, NK, BT, INIT_CFG, seed=0, dt=600.0,
               precision=MIXED if args.profile_mixed else FP64)
+    if args.profile_options:
+        # the optional physics: hor_visc's scheme branches and the remnant
+        m.set_hor_visc(biharmonic=True, smagorinsky=True, leith=True, better_bound=True)
+        m.set_visc_remnant(True)
     m.step(args.warmup + args.steps)
     m.synchronize()
     print(json.dumps({"profile_case": n, "steps": args.warmup + args.steps,
@@ -607,6 +611,8 @@ def main():
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--profile-mixed", action="store_true",
                     help="with --profile-case: the mixed-precision form's kernels")
+    ap.add_argument("--profile-options", action="store_true",
+                    help="with --profile-case: hor_visc schemes and the viscous remnant on")
     ap.add_argument("--profile-case", type=int, default=0,
                     help="run N steps of a ni=nj=N domain only (for ncu captures)")
     args = ap.parse_args()

@@ -18,12 +18,16 @@ struct HorViscGen {
     double Kh_bg, Ah_bg, Kh_bg_min, h_neglect;
     const double *Kh_Max, *Ah_Max, *L2c, *Bc, *L3c, *B6c;
     const double *Idx2dyCu, *Idxdy2u, *Idx2dyCv, *Idxdy2v;
+    // the same arrays as scalars, when uni = 1 (every one of them and every
+    // grid metric uniform over the points the kernel reads)
+    int uni;
+    double sKh_Max, sAh_Max, sL2c, sBc, sL3c, sB6c, sIdx2dyCu, sIdxdy2u, sIdx2dyCv, sIdxdy2v;
 };
 
 // diffu on [is, ie-1] x [js, je] and diffv on [is, ie] x [js, je-1], every
 // layer, from u, v, h: the points the velocity update reads.
-cudaError_t launch_hor_visc_gen(const Dims& D, const Metrics& M, const HorViscGen& P,
-                                const double* u, const double* v, const double* h,
-                                double* diffu, double* diffv, cudaStream_t s);
+cudaError_t launch_hor_visc_gen(const Dims& D, const Metrics& M, const UniMetrics& U,
+                                const HorViscGen& P, const double* u, const double* v,
+                                const double* h, double* diffu, double* diffv, cudaStream_t s);
 
 } // namespace mom6b

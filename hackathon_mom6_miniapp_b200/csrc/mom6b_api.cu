@@ -704,7 +704,7 @@ static int enqueue_step(mom6b_model* m)
         double* du = m->diag_driver ? m->dg_du : m->hv_du;
         double* dv = m->diag_driver ? m->dg_dv : m->hv_dv;
         CK(timed(m, s, "hor_visc", [&] {
-            return launch_hor_visc_gen(D, M, m->hvp, m->u, m->v, m->h0, du, dv, s); }));
+            return launch_hor_visc_gen(D, M, m->U, m->hvp, m->u, m->v, m->h0, du, dv, s); }));
         CK(timed(m, s, "tendency", [&] {
             return launch_tendency(D, M, m->U, m->u, m->v, m->h0, m->u, m->v, m->up, m->vp, dt,
                                    hv_neglect, s, du, dv, m->cor_scheme, true); }));
@@ -727,8 +727,8 @@ static int enqueue_step(mom6b_model* m)
     // ---- corrector ----
     if (m->hvgen) {
         CK(timed(m, s, "hor_visc", [&] {
-            return launch_hor_visc_gen(D, M, m->hvp, m->up, m->vp, m->hB, m->hv_du, m->hv_dv,
-                                       s); }));
+            return launch_hor_visc_gen(D, M, m->U, m->hvp, m->up, m->vp, m->hB, m->hv_du,
+                                       m->hv_dv, s); }));
         CK(timed(m, s, "tendency", [&] {
             return launch_tendency(D, M, m->U, m->up, m->vp, m->hB, m->u, m->v, m->u, m->v,
                                    0.5 * dt, hv_neglect, s, m->hv_du, m->hv_dv, m->cor_scheme,
@@ -1450,6 +1450,16 @@ extern "C" int mom6b_set_hor_visc(mom6b_model* m, const mom6b_hor_visc* o)
         }
         const double** dst[10] = {&P.Kh_Max, &P.Ah_Max, &P.L2c, &P.Bc, &P.L3c, &P.B6c,
                                   &P.Idx2dyCu, &P.Idxdy2u, &P.Idx2dyCv, &P.Idxdy2v};
+        double* sdst[10] = {&P.sKh_Max, &P.sAh_Max, &P.sL2c, &P.sBc, &P.sL3c, &P.sB6c,
+                            &P.sIdx2dyCu, &P.sIdxdy2u, &P.sIdx2dyCv, &P.sIdxdy2v};
+        // uniform over the points the kernel reads ([1, n1-1] x [1, n2-1])
+        P.uni = 1;
+        for (int q = 0; q < 10; ++q) {
+            *sdst[q] = a[q][g.at(1, 1)];
+            for (int j = 1; j <= g.n2 - 1 && P.uni; ++j)
+                for (int i = 1; i <= g.n1 - 1; ++i)
+                    if (a[q][g.at(i, j)] != *sdst[q]) { P.uni = 0; break; }
+        }
         for (int q = 0; q < 10; ++q) {
             double* d = dalloc(m, n2, &e);
             if (e != cudaSuccess) break;

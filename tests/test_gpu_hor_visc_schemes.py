@@ -60,6 +60,18 @@ def test_scheme_steps_match_the_oracle(case):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("case", ["modified_leith_no_slip", "better_bound"])
+def test_scheme_steps_with_metric_arrays(case, monkeypatch):
+    """The kernel's 2-D metric form (the uniform grid read through its arrays)
+    gives the same steps."""
+    monkeypatch.setenv("MOM6B_GENERAL_METRICS", "1")
+    opts, cfg = CASES[case]
+    m, o = _pair(opts, cfg)
+    for f in FIELDS:
+        assert np.array_equal(m.get(f), o.get(f)), f
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("case", ["biharmonic", "leith_biharmonic", "better_bound"])
 def test_the_branch_changes_the_step(case):
     """The branch under test moves the solution away from the driver's
