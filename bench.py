@@ -76,22 +76,34 @@ class ClockSampler:
     def __init__(self, device):
         self.device = device
         self.proc = None
-        self.lines = []
+        self.lines = []          # (host time the line arrived, line)
+        self.t_begin = self.t_end = None
 
     def start(self):
+        """Start sampling every 50 ms and wait (at most 5 s) for the first
+        sample, so that the sampler runs before the timed region begins."""
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 5.0 and self.proc.poll() is None:
+                time.sleep(0.02)
         except Exception:
             self.proc = None
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
+
+    def begin(self):
+        self.t_begin = time.time()
+
+    def end(self):
+        self.t_end = time.time()
 
     def stop(self):
         if not self.proc:
@@ -103,7 +115,14 @@ class ClockSampler:
             self.proc.kill()
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        lines = [ln for t, ln in self.lines]
+        if self.t_begin is not None and self.t_end is not None:
+            # the samples that arrived while the timed region ran (a sample
+            # reaches the reader a little after it is taken)
+            inside = [ln for t, ln in self.lines if self.t_begin <= t <= self.t_end + 0.06]
+            if inside:
+                lines = inside
+        for ln in lines:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -460,11 +479,13 @@ def run_ours(args, world, rank, local, dist):
     m.reset_launch_count()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    clocks.begin()
     e0.record(stream)
     m.step(args.steps)
     e1.record(stream)
     m.synchronize()
     torch.cuda.synchronize()
+    clocks.end()
     launches = m.launch_count()
     ck = clocks.stop()
     ms_local = e0.elapsed_time(e1)
