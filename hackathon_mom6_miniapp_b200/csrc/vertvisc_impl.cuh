@@ -399,8 +399,12 @@ static cudaError_t launch_vv_pf(const Dims& D, const Metrics& M, R* u, R* v, con
     }
     if constexpr (sizeof(R) == 8) {
         if (rem_u) {   // with the remnant (the FP64 form's register cap)
-            k_vertvisc_pf<KMAX, 4, R, 6, true><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P, taux_bot,
-                                                                   tauy_bot, rem_u, rem_v);
+            if (async)
+                k_vertvisc_pf<KMAX, 4, R, 6, true, true><<<grid, nb, 0, s>>>(
+                    D, M, u, v, h, dt, P, taux_bot, tauy_bot, rem_u, rem_v);
+            else
+                k_vertvisc_pf<KMAX, 4, R, 6, true><<<grid, nb, 0, s>>>(
+                    D, M, u, v, h, dt, P, taux_bot, tauy_bot, rem_u, rem_v);
             return cudaGetLastError();
         }
     }
