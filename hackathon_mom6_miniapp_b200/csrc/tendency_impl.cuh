@@ -419,37 +419,47 @@ cudaError_t launch_tendency_t(const Dims& D, const Metrics& M, const UniMetrics&
     constexpr int TY = kTendTY;
     int nx = D.ie - D.is + 1, ny = D.je - D.js + 1;
     dim3 block(kTendTX, TY, 1);
-    int nchunks = (D.nk + kTendKC - 1) / kTendKC;
+    // layers per CTA: 5, 8, 15 and 25 measure the same on B200 (FP64 2.00-2.01 ms
+    // per step, mixed 1.49) -- the staging of the first layer of a chunk is
+    // hidden by the other resident CTAs
+    static int kc = -1;
+    if (kc < 0) {
+        const char* e = getenv("MOM6B_TEND_KC");
+        kc = e ? atoi(e) : kTendKC;
+        if (kc < 1) kc = kTendKC;
+    }
+    const int KCh = kc;
+    int nchunks = (D.nk + KCh - 1) / KCh;
     dim3 grid((nx + kTendTX - 1) / kTendTX, (ny + TY - 1) / TY, nchunks);
     if ((dfu == nullptr) != (dfv == nullptr)) return cudaErrorInvalidValue;
     if (ext_visc) {
         if (!dfu || scheme < 1 || scheme > 3) return cudaErrorInvalidValue;
         if (scheme == 1)
             launch_tendency_extv<R, 1>(D, M, U, grid, block, uin, vin, h, ubase, vbase, uout,
-                                       vout, coef, h_neglect, kTendKC, s, dfu, dfv);
+                                       vout, coef, h_neglect, KCh, s, dfu, dfv);
         else if (scheme == 2)
             launch_tendency_extv<R, 2>(D, M, U, grid, block, uin, vin, h, ubase, vbase, uout,
-                                       vout, coef, h_neglect, kTendKC, s, dfu, dfv);
+                                       vout, coef, h_neglect, KCh, s, dfu, dfv);
         else
             launch_tendency_extv<R, 3>(D, M, U, grid, block, uin, vin, h, ubase, vbase, uout,
-                                       vout, coef, h_neglect, kTendKC, s, dfu, dfv);
+                                       vout, coef, h_neglect, KCh, s, dfu, dfv);
         return cudaGetLastError();
     }
     if (scheme == 2)
         return launch_tendency_arakawa<R, 2>(D, M, U, grid, block, uin, vin, h, ubase, vbase,
-                                             uout, vout, coef, h_neglect, kTendKC, s, dfu, dfv);
+                                             uout, vout, coef, h_neglect, KCh, s, dfu, dfv);
     if (scheme == 3)
         return launch_tendency_arakawa<R, 3>(D, M, U, grid, block, uin, vin, h, ubase, vbase,
-                                             uout, vout, coef, h_neglect, kTendKC, s, dfu, dfv);
+                                             uout, vout, coef, h_neglect, KCh, s, dfu, dfv);
     if (scheme != 1) return cudaErrorInvalidValue;
     if (dfu || dfv) {
         if (U.valid)
             k_tendency<kTendTX, TY, true, R, 3, true><<<grid, block, 0, s>>>(
-                D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, kTendKC,
+                D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, KCh,
                 dfu, dfv);
         else
             k_tendency<kTendTX, TY, false, R, 3, true><<<grid, block, 0, s>>>(
-                D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, kTendKC,
+                D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, KCh,
                 dfu, dfv);
         return cudaGetLastError();
     }
@@ -464,16 +474,16 @@ cudaError_t launch_tendency_t(const Dims& D, const Metrics& M, const UniMetrics&
     if (U.valid) {
         if (minb == 4)
             k_tendency<kTendTX, TY, true, R, 4><<<grid, block, 0, s>>>(
-                D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, kTendKC);
+                D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, KCh);
         else if (minb == 3)
             k_tendency<kTendTX, TY, true, R, 3><<<grid, block, 0, s>>>(
-                D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, kTendKC);
+                D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, KCh);
         else
             k_tendency<kTendTX, TY, true, R><<<grid, block, 0, s>>>(
-                D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, kTendKC);
+                D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, KCh);
     } else {
         k_tendency<kTendTX, TY, false, R, 3><<<grid, block, 0, s>>>(
-            D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, kTendKC);
+            D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, KCh);
     }
     return cudaGetLastError();
 }
