@@ -142,3 +142,19 @@ def test_schemes_are_refused_in_the_mixed_form():
     m.set_hor_visc()                       # the driver's options stay available
     with pytest.raises(Mom6bError):
         m.set_hor_visc(biharmonic=True)
+
+
+@pytest.mark.gpu
+def test_all_schemes_at_180x180x75():
+    """Every branch at once at the configs' small size, bit for bit."""
+    from hackathon_mom6_miniapp_b200 import Model
+    opts = dict(biharmonic=True, smagorinsky=True, leith=True, modified_leith=True,
+                better_bound=True, Ah=1.0e9)
+    m = Model(180, 180, 75, 30, INIT_CFG, seed=11, Kh=0.0)
+    o = Oracle(180, 180, 75, 30, INIT_CFG, seed=11, Kh=0.0, threads=0)
+    m.set_hor_visc(**opts)
+    o.set_hor_visc(**opts)
+    m.step(2)
+    o.step(2)
+    for f in FIELDS:
+        assert np.array_equal(m.get(f), o.get(f)), f

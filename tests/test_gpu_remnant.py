@@ -82,3 +82,17 @@ def test_remnant_is_refused_in_the_mixed_form():
     m = Model(*SHAPE, 30, INIT_CFG, seed=1, precision=MIXED)
     with pytest.raises(Mom6bError):
         m.set_visc_remnant(True)
+
+
+@pytest.mark.gpu
+def test_remnant_steps_at_180x180x75():
+    """The remnant path at the configs' small size, bit for bit."""
+    from hackathon_mom6_miniapp_b200 import Model
+    m = Model(180, 180, 75, 30, INIT_CFG, seed=12)
+    o = Oracle(180, 180, 75, 30, INIT_CFG, seed=12, threads=0)
+    m.set_visc_remnant(True)
+    o.set_remnant(True)
+    m.step(2)
+    o.step(2)
+    for f in ["h", "u", "v", "eta", "hu_bt", "visc_rem_u", "visc_rem_v"] + BT_U:
+        assert np.array_equal(m.get(f), o.get(f)), f
