@@ -234,6 +234,10 @@ struct FaceCol {
     EI nbe = 1;
     // the vertical-viscosity remnant of the face column (VREM), stride plane
     const double* vr = nullptr;
+    // AS: this thread's staging slots in shared memory, slot (b, c, f) at
+    // st[((b * CH + c) * 7 + f) * sts]
+    double* st = nullptr;
+    int sts = 0;
 };
 
 // The inputs of one layer of one face: u(I) and the cell values of the two
@@ -299,10 +303,56 @@ __device__ __forceinline__ double darea(const FaceCol<EI>& F, const LayerVals& L
 }
 
 // Visit layers 1..nz in order, fn(k, LayerVals).
-template <int CH, bool LAST = false, bool Y = false, bool VREM = false, typename EI,
-          typename Fn>
+// AS: the next chunk's seven values per layer are copied into shared memory
+// with cp.async while the current chunk is evaluated (zonal, without the
+// remnant); otherwise each chunk is loaded into registers before it is
+// evaluated.
+template <int CH, bool LAST = false, bool Y = false, bool VREM = false, bool AS = false,
+          typename EI, typename Fn>
 __device__ __forceinline__ void for_layers(const FaceCol<EI>& F, int nz, Fn&& fn)
 {
+    if constexpr (AS && !Y && !VREM) {
+        auto slot = [&](int b, int c, int f) -> double& {
+            return F.st[(size_t)((b * CH + c) * 7 + f) * F.sts];
+        };
+        auto stage = [&](int kt, int b) {
+#pragma unroll
+            for (int c = 0; c < CH; ++c) {
+                const int k = kt + c;
+                const bool ok = k <= nz;
+                const size_t o = ok ? (size_t)(k - 1) * F.plane : 0;
+                const EI oe = ok ? (EI)(k - 1) * F.estride : (EI)0;
+                cp_async_elem(&slot(b, c, 0), F.u + o, ok);
+                cp_async_elem(&slot(b, c, 1), F.hWc + oe, ok);
+                cp_async_elem(&slot(b, c, 2), F.hEc + oe, ok);
+                cp_async_elem(&slot(b, c, 3), F.hc + o, ok);
+                cp_async_elem(&slot(b, c, 4), F.hWc + oe + 1, ok);
+                cp_async_elem(&slot(b, c, 5), F.hEc + oe + 1, ok);
+                cp_async_elem(&slot(b, c, 6), F.hc + o + 1, ok);
+            }
+            cp_async_commit();
+        };
+        stage(1, 0);
+        for (int kt = 1, it = 0; kt <= nz; kt += CH, ++it) {
+            const int b = it & 1;
+            if (kt + CH <= nz) {
+                stage(kt + CH, b ^ 1);
+                cp_async_wait_prior();
+            } else {
+                cp_async_wait_all();
+            }
+            LayerVals L[CH];
+#pragma unroll
+            for (int c = 0; c < CH; ++c) {
+                L[c].u = slot(b, c, 0);
+                L[c].hWi = slot(b, c, 1); L[c].hEi = slot(b, c, 2); L[c].hi = slot(b, c, 3);
+                L[c].hWp = slot(b, c, 4); L[c].hEp = slot(b, c, 5); L[c].hp = slot(b, c, 6);
+            }
+#pragma unroll
+            for (int c = 0; c < CH; ++c)
+                if (kt + c <= nz) fn(kt + c, L[c]);
+        }
+    } else {
     for (int kt = 1; kt <= nz; kt += CH) {
         LayerVals L[CH];
 #pragma unroll
@@ -311,6 +361,7 @@ __device__ __forceinline__ void for_layers(const FaceCol<EI>& F, int nz, Fn&& fn
 #pragma unroll
         for (int c = 0; c < CH; ++c)
             if (kt + c <= nz) fn(kt + c, L[c]);
+    }
     }
 }
 
@@ -412,7 +463,7 @@ __device__ __forceinline__ bool newton_iter(Newton& S, int itt, double tol_eta_d
 // zero-transport solve (:1002), live only when it is needed.  The two are
 // independent iterations, each with its own operation sequence; sharing the
 // column passes only halves how often the column is read.
-template <int CH, typename EI, bool Y = false, bool VREM = false>
+template <int CH, typename EI, bool Y = false, bool VREM = false, bool AS = false>
 __device__ void flux_adjust_pair(const FaceCol<EI>& F, int nz, double dt, double uhbt,
                                  double tol_eta_dt_fac, Newton& A, Newton& B,
                                  double* uh_out, size_t uh_stride)
@@ -427,7 +478,7 @@ __device__ void flux_adjust_pair(const FaceCol<EI>& F, int nz, double dt, double
         if (!pa && !pb) break;
         const double duA = A.du, duB = B.du;
         double eA = -uhbt, sA = 0.0, eB = -0.0, sB = 0.0;
-        for_layers<CH, false, Y, VREM>(F, nz, [&](int k, const LayerVals& L) {
+        for_layers<CH, false, Y, VREM, AS>(F, nz, [&](int k, const LayerVals& L) {
             if (pa) {
                 double hm;
                 double uhk = flux_eval(F, L, u_at<VREM>(L, duA), dt, hm);
@@ -458,7 +509,7 @@ __device__ void flux_adjust_pair(const FaceCol<EI>& F, int nz, double dt, double
 // One zonal_flux_adjust solve on its own (:813-903): the transports of every
 // evaluated iterate go to uh_out when it is given (then the last iterate is
 // evaluated even at max_itts), otherwise passes run only to update.
-template <int CH, typename EI, bool Y = false, bool VREM = false>
+template <int CH, typename EI, bool Y = false, bool VREM = false, bool AS = false>
 __device__ void flux_adjust_one(const FaceCol<EI>& F, int nz, double dt, double target,
                                 double tol_eta_dt_fac, Newton& S, double* uh_out,
                                 size_t uh_stride)
@@ -470,7 +521,7 @@ __device__ void flux_adjust_one(const FaceCol<EI>& F, int nz, double dt, double 
         if (!update && !uh_out) break;
         const double du = S.du;
         double e = -target, sm = 0.0;
-        for_layers<CH, false, Y, VREM>(F, nz, [&](int k, const LayerVals& L) {
+        for_layers<CH, false, Y, VREM, AS>(F, nz, [&](int k, const LayerVals& L) {
             double hm;
             double uhk = flux_eval(F, L, u_at<VREM>(L, du), dt, hm);
             if (uh_out) uh_out[(size_t)(k - 1) * uh_stride] = uhk;
@@ -501,7 +552,8 @@ __device__ void flux_adjust_one(const FaceCol<EI>& F, int nz, double dt, double 
 // (:1001-1018) and the face thickness is h_marg(u + du visc_rem) visc_rem
 // (zonal_flux_thickness :730).  Without it every visc_rem is 1 and these
 // reduce exactly to the forms below.
-template <int CH, typename EI, bool LOCK = true, bool Y = false, bool VREM = false>
+template <int CH, typename EI, bool LOCK = true, bool Y = false, bool VREM = false,
+          bool AS = false>
 __device__ __forceinline__ void face_work(const Dims& D, const Metrics& M, FaceCol<EI>& F,
                                           int I, int j, size_t f0, double* uh, size_t ust,
                                           bool owner, const double* uhbt2d, const ContOut& O,
@@ -530,7 +582,7 @@ __device__ __forceinline__ void face_work(const Dims& D, const Metrics& M, FaceC
         du_min_CFL = -(2.0 * (CFL_dt * dx_E));
     }
     double uh_tot_0 = 0.0, duhdu_tot_0 = 0.0;
-    for_layers<CH, false, Y, VREM>(F, nz, [&](int k, const LayerVals& L) {
+    for_layers<CH, false, Y, VREM, AS>(F, nz, [&](int k, const LayerVals& L) {
         double hm;
         double uhk = flux_eval(F, L, L.u, dt, hm);
         uh[(size_t)(k - 1) * ust] = uhk;
@@ -561,17 +613,17 @@ __device__ __forceinline__ void face_work(const Dims& D, const Metrics& M, FaceC
     if (LOCK) {
         Newton A = newton_start(uh_tot_0 - uhbt, duhdu_tot_0, du_max_CFL, du_min_CFL, true);
         Newton B = newton_start(uh_tot_0 - 0.0, duhdu_tot_0, du_max_CFL, du_min_CFL, solve0);
-        flux_adjust_pair<CH, EI, Y, VREM>(F, nz, dt, uhbt, fac, A, B, uh, ust);
+        flux_adjust_pair<CH, EI, Y, VREM, AS>(F, nz, dt, uhbt, fac, A, B, uh, ust);
         du = A.du;
         du0 = solve0 ? B.du : du;
     } else {
         Newton A = newton_start(uh_tot_0 - uhbt, duhdu_tot_0, du_max_CFL, du_min_CFL, true);
-        flux_adjust_one<CH, EI, Y, VREM>(F, nz, dt, uhbt, fac, A, uh, ust);
+        flux_adjust_one<CH, EI, Y, VREM, AS>(F, nz, dt, uhbt, fac, A, uh, ust);
         du = A.du;
         du0 = du;
         if (solve0) {
             Newton B = newton_start(uh_tot_0 - 0.0, duhdu_tot_0, du_max_CFL, du_min_CFL, true);
-            flux_adjust_one<CH, EI, Y, VREM>(F, nz, dt, 0.0, fac, B, (double*)nullptr, 0);
+            flux_adjust_one<CH, EI, Y, VREM, AS>(F, nz, dt, 0.0, fac, B, (double*)nullptr, 0);
             du0 = B.du;
         }
     }
@@ -604,7 +656,7 @@ __device__ __forceinline__ void face_work(const Dims& D, const Metrics& M, FaceC
     double FAmt_0 = 0.0, FAmt_L = 0.0, FAmt_R = 0.0, uhtot_L = 0.0, uhtot_R = 0.0;
     double* h_u = O.h_u + f0;
     const bool same = (du0 == du);
-    for_layers<CH, kContHints, Y, VREM>(F, nz, [&](int k, const LayerVals& L) {
+    for_layers<CH, kContHints, Y, VREM, AS>(F, nz, [&](int k, const LayerVals& L) {
         double hm0, hmL, hmR;
         flux_eval(F, L, u_at<VREM>(L, du0), dt, hm0);
         double uhL = flux_eval(F, L, u_at<VREM>(L, duL), dt, hmL);
@@ -673,7 +725,7 @@ __device__ __forceinline__ void cell_convergence(const Dims& D, const Metrics& M
 }
 
 // MINB: the CTAs per SM the register allocation is held to (launch bounds).
-template <int CH, int MINB = 1, bool LOCK = true, bool VREM = false>
+template <int CH, int MINB = 1, bool LOCK = true, bool VREM = false, bool AS = false>
 __global__ void __launch_bounds__(128, MINB)
 k_cont_faces(Dims D, Metrics M, const double* __restrict__ u,
              const double* __restrict__ hin, const double* __restrict__ hW,
@@ -697,10 +749,16 @@ k_cont_faces(Dims D, Metrics M, const double* __restrict__ u,
         F.IdxT_i = MOM6B_A2(M.IdxT, I, j, D);
         F.IdxT_ip1 = MOM6B_A2(M.IdxT, I + 1, j, D);
         if constexpr (VREM) F.vr = visc_rem + f0;
+        if constexpr (AS) {
+            extern __shared__ double cont_stage[];
+            F.st = cont_stage + threadIdx.x;
+            F.sts = (int)blockDim.x;
+        }
         const bool to_ovl = !owner;
         double* uh = to_ovl ? ovl : O.uh + f0;
         const size_t ust = to_ovl ? 1 : F.plane;
-        face_work<CH, size_t, LOCK, false, VREM>(D, M, F, I, j, f0, uh, ust, owner, uhbt2d, O, dt);
+        face_work<CH, size_t, LOCK, false, VREM, AS>(D, M, F, I, j, f0, uh, ust, owner, uhbt2d,
+                                                     O, dt);
     }
     __syncthreads();  // the CTA's transport columns are complete and visible
     cell_convergence(D, M, I, j, hin, ovl, O, dt);
@@ -1335,6 +1393,24 @@ cudaError_t launch_continuity(const Dims& D, const Metrics& M, const double* u,
                                  : (minb == 4 ? k_cont_faces<2, 4> : k_cont_faces<2>);
         // the remnant form runs the default shape only
         if (visc_rem) kern = k_cont_faces<4, 4, false, true>;
+        // staged sweeps (chunks of 3 layers copied with cp.async while the
+        // previous 3 are evaluated): 3.50 ms per step against 3.60 loading
+        // chunks of 4 into registers (2: 3.68, 4 at 3 CTAs/SM: 3.62)
+        static int cas = -1;
+        if (cas < 0) {
+            const char* e = getenv("MOM6B_CONT_ASYNC");
+            cas = e ? atoi(e) : 3;
+        }
+        if (!visc_rem && cas == 2) {
+            kern = k_cont_faces<2, 4, false, false, true>;
+            smem = (size_t)2 * 2 * 7 * nb * sizeof(double);
+        } else if (!visc_rem && cas == 3) {
+            kern = k_cont_faces<3, 4, false, false, true>;
+            smem = (size_t)2 * 3 * 7 * nb * sizeof(double);
+        } else if (!visc_rem && cas == 4) {
+            kern = k_cont_faces<4, 3, false, false, true>;
+            smem = (size_t)2 * 4 * 7 * nb * sizeof(double);
+        }
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e != cudaSuccess) return e;
