@@ -52,14 +52,16 @@ k_ppm_edges_warp_f(Dims D, Metrics M, const float* __restrict__ hin, float* __re
                      D.js + (int)blockIdx.y, 1 + (int)blockIdx.z * kEdgeLayersF);
 }
 
-template <int MINB>
+// AS: the column sweeps stage the next chunk in shared memory with cp.async.
+template <int MINB, bool AS = false>
 __global__ void __launch_bounds__(128, MINB)
 k_cont_faces_f(Dims D, Metrics M, const float* __restrict__ u, const float* __restrict__ hin,
                const float* __restrict__ hW, const float* __restrict__ hE,
                const double* __restrict__ uhbt2d, ContOutF O, float* ovl_all, double dt)
 {
+    __shared__ float stage[AS ? 2 * kMixCH * 7 * 128 : 1];
     cont_faces_f(D, M, u, hin, hW, hE, uhbt2d, O, ovl_all, dt, (int)blockIdx.x,
-                 (int)blockIdx.y, (int)gridDim.x);
+                 (int)blockIdx.y, (int)gridDim.x, AS ? stage : nullptr);
 }
 
 cudaError_t launch_continuity_f(const Dims& D, const Metrics& M, const float* u,
@@ -93,7 +95,20 @@ cudaError_t launch_continuity_f(const Dims& D, const Metrics& M, const float* u,
         const char* e = getenv("MOM6B_CONTF_MINB");
         minb = e ? atoi(e) : 6;   // 6 CTAs per SM: 2.19 ms per step (5: 2.23, 4: 2.38)
     }
-    if (minb == 4)
+    // staged sweeps (5 or 6 CTAs per SM): slower in FP32 on B200 (2.30 and 2.38 ms per
+    // step against 2.19 loading chunks into registers), so off by default
+    static int as = -1;
+    if (as < 0) {
+        const char* e = getenv("MOM6B_CONTF_ASYNC");
+        as = e ? atoi(e) : 0;
+    }
+    if (as == 6)
+        k_cont_faces_f<6, true><<<grid, nb, 0, s>>>(D, M, u, hin, hW, hE, uhbt, O,
+                                                    (float*)uh_ovl, dt);
+    else if (as == 5)
+        k_cont_faces_f<5, true><<<grid, nb, 0, s>>>(D, M, u, hin, hW, hE, uhbt, O,
+                                                    (float*)uh_ovl, dt);
+    else if (minb == 4)
         k_cont_faces_f<4><<<grid, nb, 0, s>>>(D, M, u, hin, hW, hE, uhbt, O, (float*)uh_ovl, dt);
     else if (minb == 5)
         k_cont_faces_f<5><<<grid, nb, 0, s>>>(D, M, u, hin, hW, hE, uhbt, O, (float*)uh_ovl, dt);

@@ -147,6 +147,10 @@ struct FaceF {
     const float *u, *hc, *hW, *hE;
     size_t plane;
     float dy, Idx_i, Idx_p, dt;
+    // this thread's staging slots (nullptr: chunks are loaded into registers);
+    // slot (b, c, f) at st[((b * kMixCH + c) * 7 + f) * sts]
+    float* st = nullptr;
+    int sts = 0;
     __device__ LayerF load(int k) const
     {
         const size_t o = (size_t)(k - 1) * plane;
@@ -180,6 +184,48 @@ constexpr int kMixCH = 4;
 template <bool LAST = false, typename Fn>
 __device__ __forceinline__ void mix_layers(const FaceF& F, int nz, Fn&& fn)
 {
+    if (F.st) {
+        // the next chunk's seven values copied with cp.async while the
+        // current chunk is evaluated
+        auto slot = [&](int b, int c, int f) -> float& {
+            return F.st[(size_t)((b * kMixCH + c) * 7 + f) * F.sts];
+        };
+        auto stage = [&](int kt, int b) {
+#pragma unroll
+            for (int c = 0; c < kMixCH; ++c) {
+                const int k = kt + c;
+                const bool ok = k <= nz;
+                const size_t o = ok ? (size_t)(k - 1) * F.plane : 0;
+                cp_async_elem(&slot(b, c, 0), F.u + o, ok);
+                cp_async_elem(&slot(b, c, 1), F.hW + o, ok);
+                cp_async_elem(&slot(b, c, 2), F.hE + o, ok);
+                cp_async_elem(&slot(b, c, 3), F.hc + o, ok);
+                cp_async_elem(&slot(b, c, 4), F.hW + o + 1, ok);
+                cp_async_elem(&slot(b, c, 5), F.hE + o + 1, ok);
+                cp_async_elem(&slot(b, c, 6), F.hc + o + 1, ok);
+            }
+            cp_async_commit();
+        };
+        stage(1, 0);
+        for (int kt = 1, it = 0; kt <= nz; kt += kMixCH, ++it) {
+            const int b = it & 1;
+            if (kt + kMixCH <= nz) {
+                stage(kt + kMixCH, b ^ 1);
+                cp_async_wait_prior();
+            } else {
+                cp_async_wait_all();
+            }
+            LayerF L[kMixCH];
+#pragma unroll
+            for (int c = 0; c < kMixCH; ++c)
+                L[c] = LayerF{slot(b, c, 0), slot(b, c, 1), slot(b, c, 2), slot(b, c, 3),
+                              slot(b, c, 4), slot(b, c, 5), slot(b, c, 6)};
+#pragma unroll
+            for (int c = 0; c < kMixCH; ++c)
+                if (kt + c <= nz) fn(kt + c, L[c]);
+        }
+        return;
+    }
     for (int kt = 1; kt <= nz; kt += kMixCH) {
         LayerF L[kMixCH];
 #pragma unroll
@@ -279,7 +325,7 @@ __device__ __forceinline__ void cont_faces_f(const Dims& D, const Metrics& M,
                                              const float* __restrict__ hE,
                                              const double* __restrict__ uhbt2d,
                                              const ContOutF& O, float* ovl_all, double dt,
-                                             int bx, int by, int gx)
+                                             int bx, int by, int gx, float* stage = nullptr)
 {
     const int nz = D.nk;
     const int I = D.is - 1 + bx * ((int)blockDim.x - 1) + (int)threadIdx.x;
@@ -293,6 +339,10 @@ __device__ __forceinline__ void cont_faces_f(const Dims& D, const Metrics& M,
         FaceF F{u + f0, hin + f0, hW + f0, hE + f0, plane,
                 (float)MOM6B_A2(M.dy_Cu, I, j, D), (float)MOM6B_A2(M.IdxT, I, j, D),
                 (float)MOM6B_A2(M.IdxT, I + 1, j, D), (float)dt};
+        if (stage) {
+            F.st = stage + threadIdx.x;
+            F.sts = (int)blockDim.x;
+        }
         float* uh = owner ? O.uh + f0 : ovl;
         const size_t ust = owner ? plane : 1;
         // initial fluxes, column sums, CFL limits
