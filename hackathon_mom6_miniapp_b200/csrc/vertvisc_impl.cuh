@@ -376,8 +376,8 @@ static cudaError_t launch_vv_pf(const Dims& D, const Metrics& M, R* u, R* v, con
         const char* b = getenv("MOM6B_VV_MINB");
         minb = b ? atoi(b) : vv_min_blocks<R>();
         // staged sweeps: FP64 2.215 ms per step against 2.285 loaded into
-        // registers; the FP32 form is faster loading into registers (1.02
-        // against 1.10-1.14 ms)
+        // registers (chunks of 6 layers: 3.11, spilling); the FP32 form is
+        // faster loading into registers (1.02 against 1.10-1.14 ms)
         const char* a = getenv("MOM6B_VV_ASYNC");
         async = a ? atoi(a) : (sizeof(R) == 8 ? 6 : 0);
     }
