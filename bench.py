@@ -2,7 +2,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Workload: the seeded beta-plane state (CFG init,
+Workload: the seeded beta-plane state at 720x720x75 (CFG init,
 Philox4x32-10 normals, dt = 600 s, Kh = 1e3, halo fill on), ni = nj = 720,
 nk = 75, bt_nsteps = 50, plain FP64.  One "step" is one split RK2 iteration
 of rk2_serial_driver.F90:218-399 on the whole domain.  The state (~6 GB)
@@ -27,7 +27,7 @@ autotuner, and reports aggregate cell-layer updates/s over 50 steps.
 The "surrogate" object trains the learned barotropic surrogate on the GPU
 (8 seeded states x 2000 steps of the plain btstep, batch 65536), reports its
 transport error on a held-out state, and times the step with the network in
-place of btstep: with the plain btstep as shadow judge every 10 steps
+place of btstep: with the plain btstep as shadow check every 10 steps
 (threshold 1e-3 relative eta error, falling back when exceeded) and alone,
 with the network-alone eta error after 100 steps against the FP64 form.
 
@@ -404,7 +404,7 @@ def run_surrogate(args, world, rank, local, dist, fp64_ms_per_step):
     """The learned barotropic surrogate at 720x720x75 bt50: the network is
     trained on the GPU (8 seeded barotropic states x args.sur_steps RK2 steps
     of the plain btstep, batch 65536, Adam lr 1e-3), checked on a held-out
-    state, then run in place of btstep with the plain btstep as shadow judge
+    state, then run in place of btstep with the plain btstep as shadow check
     (every 10 steps, relative eta error threshold 1e-3), and on its own."""
     from hackathon_mom6_miniapp_b200 import FP64, INIT_CFG, Model
     t = Model(NI, NJ, 2, BT, INIT_CFG, seed=rank, dt=600.0, device=local)
@@ -416,7 +416,7 @@ def run_surrogate(args, world, rank, local, dist, fp64_ms_per_step):
                             lr=1e-3),
            "heldout_transport_rel_l2": held["rel_error"],
            "heldout_zero_transport_rel_l2": held["zero_prediction_error"]}
-    # with the shadow judge
+    # with the shadow check
     m = Model(NI, NJ, NK, BT, INIT_CFG, seed=rank, dt=600.0, device=local, use_graph=True)
     m.set_surrogate_params(params)
     m.surrogate_enable(True, shadow_every=10, threshold=1e-3)

@@ -355,7 +355,7 @@ int mom6b_ensemble_set_tuning(mom6b_ensemble *e, const int *in7);
  *
  * mom6b_surrogate_enable(on = 1) makes mom6b_step use the network instead of
  * btstep; every shadow_every steps (0: never) the plain btstep runs from the
- * same state and judges: when the relative L2 difference of the two etas over
+ * same state as the check: when the relative L2 difference of the two etas over
  * the compute domain exceeds threshold, the plain results are kept and the
  * model uses the plain btstep from then on (mom6b_surrogate_enable again
  * re-arms it).  status10: enabled, fallen back, steps, shadow checks,
