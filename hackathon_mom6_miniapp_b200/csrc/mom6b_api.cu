@@ -91,7 +91,7 @@ struct mom6b_model {
     std::map<std::string, std::pair<double, int64_t>> timed;  // ms total, launches
     // learned barotropic surrogate (k_mlp.cu): the network, whether it
     // replaces btstep, the shadow check (every sur_every steps the plain loop
-    // runs from the same state and judges the surrogate's eta) and its record
+    // runs from the same state and checks the surrogate's eta) and its record
     std::unique_ptr<Mlp> sur;
     bool sur_on = false, sur_fallen = false;
     int sur_every = 10;
@@ -583,7 +583,7 @@ static int enqueue_surrogate_chain(mom6b_model* m, cudaStream_t s)
 }
 
 // The plain barotropic chain from the model's (eta, ubt, vbt) into the
-// shadow buffers (the judge of the surrogate).
+// shadow buffers (the check of the surrogate).
 static int enqueue_shadow_chain(mom6b_model* m, cudaStream_t s)
 {
     const Dims& D = m->D;

@@ -152,7 +152,7 @@ def test_trained_network_gains_over_the_method_without_it(trained_params):
     update left out).  Its eta after a few steps is printed beside
     the same two, for the record: a 5 x 5 stencil sees +-2 cells while gravity
     waves cross about 12 cells in one barotropic call here, which is why the
-    shadow run is the judge of the multi-step error."""
+    shadow run is the check of the multi-step error."""
     p, _, _ = trained_params
     errs, eta_errs = {}, {}
     nsteps = 4

@@ -1,5 +1,5 @@
 """The CPU restatement of the surrogate network checks itself before it
-judges the GPU: its bf16 rounding equals torch's bfloat16 conversion, and its
+checks the GPU: its bf16 rounding equals torch's bfloat16 conversion, and its
 backward pass equals finite differences of its forward pass (with the bf16
 rounding switched off, in float64)."""
 import numpy as np
