@@ -12,17 +12,29 @@ domain (the path does not shard across GPUs: replicas only, weak scaling);
 the timed region is bracketed by a barrier and device synchronisation and
 the time is the maximum over ranks.
 
-The line's "mixed" object measures the mixed-precision form (FP32 state,
-fluxes, stencils and vertical elimination; FP64 column sums, thickness update
-and barotropic loop) on the same workload and protocol, with its speed-up
-over the FP64 form and its per-field relative L2 error against the FP64 form
-of the same seed after 10 steps at 720x720x75 and after 100 steps at
-1440x1080x75 (the mixed-form configuration).
+The line's "reference_cuda_c" object times the reference's own CUDA C
+backend on the same GPU and workload: its src/cuda_c kernels built from their
+sources with the reference's -O3 for sm_100a (oracle/_ref), driven by a C++
+mirror of rk2_cuda_c_driver and the src/cuda_c Fortran wrappers (same launch
+sequence, arguments and per-phase device synchronisation).  "abi_dropin"
+times this library's launch_* entry points through the same mirror: the path
+an unchanged Fortran build of rk2_cuda_c_driver takes when it links this
+library.  Both report the median per-step time over K steps after W warm-up
+steps (CUDA events).
+
+The "mixed" object measures the mixed-precision form (FP32 state, fluxes,
+stencils and vertical-viscosity coefficients; FP64 column sums, thickness
+update, vertical tridiagonal elimination and barotropic loop) on the same
+workload and protocol, with its speed-up over the FP64 form, the same pair
+at the mixed-form configuration 1440x1080x75 bt50, and its per-field
+relative L2 error against the exact FP64 form of the same seed after 10 steps
+at 720x720x75 and after 100 steps at 1440x1080x75.
 
 The "ensemble" object advances 64 independent domains of uneven size
-(ni = nj in {90, ..., 360}, nk in {25, 50, 75}, bt_nsteps = 30, mixed form)
+(ni = nj in {90, ..., 360}, nk in {25, 50, 75}, bt_nsteps = 31, mixed form)
 together, one launch per phase for all of them with launch shapes from the
-autotuner, and reports aggregate cell-layer updates/s over 50 steps.
+autotuner, reports aggregate cell-layer updates/s over 50 steps and checks
+every domain for finite fields and conserved volume afterwards.
 
 The "surrogate" object trains the learned barotropic surrogate on the GPU
 (8 seeded states x 2000 steps of the plain btstep, batch 65536), reports its
@@ -34,7 +46,8 @@ with the network-alone eta error after 100 steps against the FP64 form.
 --impl reference times the reference's CPU implementation of the path on the
 host cores: the C restatement of the serial Fortran driver (the Fortran
 itself cannot be compiled here), built with OpenMP over rows and run on all
-host threads (its single-thread rate beside it), on rank 0 only.
+host threads, on W untimed and K timed whole steps of the workload, on rank
+0 only.
 """
 import argparse
 import json
@@ -189,59 +202,91 @@ def barrier(dist):
         dist.barrier()
 
 
-def cpu_reference_rate(threads=None):
-    """Time the oracle restatement of the serial driver on a bounded sample of
-    the workload: a strip of the 720x720x75 bt50 domain (all 720 points in i,
-    40 rows in j), one RK2 step, scaled by compute cells.  threads=None is the
-    single-threaded build (the reference serial backend has no threading);
-    threads=0 the OpenMP build of the same source on all host threads (rows in
-    parallel, results identical)."""
+def cpu_whole_steps(ni, nj, bt, nsteps, threads, warmup=1):
+    """Time the oracle restatement of the serial driver on whole RK2 steps of
+    the seeded ni x nj x 75 domain (dt 600 s): `warmup` untimed steps, then
+    nsteps timed ones.  threads=None is the single-threaded build (the
+    reference serial backend has no threading); threads=0 the OpenMP build of
+    the same source on all host threads (rows in parallel, results
+    identical)."""
     from oracle.pyoracle import INIT_CFG, Oracle
-    nj_s = 40
-    o = Oracle(NI, nj_s, NK, BT, INIT_CFG, seed=0, dt=600.0, threads=threads)
+    o = Oracle(ni, nj, NK, bt, INIT_CFG, seed=0, dt=600.0, threads=threads)
     cores = o.threads
+    if warmup:
+        o.step(warmup)
     t0 = time.perf_counter()
-    o.step(1)
+    o.step(nsteps)
     dt = time.perf_counter() - t0
     o.close()
-    scale = ((NI - 4) * (NJ - 4)) / ((NI - 4) * (nj_s - 4))
-    per_full_step = dt * scale
     what = "OpenMP over rows" if threads is not None else "single thread"
-    return 1.0 / per_full_step, f"1 RK2 step of a 720x{nj_s}x75 bt50 strip ({dt:.2f} s, " \
-        f"{what}, {cores} thread(s)), scaled by compute cells to 720x720", cores
+    return nsteps / dt, (f"{nsteps} whole RK2 steps of {ni}x{nj}x{NK} bt{bt} after {warmup} "
+                         f"untimed ({dt:.1f} s, {what}, {cores} thread(s))"), cores
 
 
 def cpu_baseline_line():
-    """cpu_baseline: the oracle on all host threads, with its single-thread rate."""
-    r1, s1, _ = cpu_reference_rate(None)
-    rn, sn, cores = cpu_reference_rate(0)
+    """cpu_baseline: the oracle on all host threads on whole steps of the
+    bench workload, and the single-thread build on whole steps of the
+    180x180x75 case (a whole 720x720 step single-threaded takes about a
+    minute)."""
+    rn, sn, cores = cpu_whole_steps(NI, NJ, BT, 2, 0)
+    r1, s1, _ = cpu_whole_steps(180, 180, 31, 2, None)
     return {"value": rn, "unit": "steps/s", "cores": cores, "kind": "port", "sample": sn,
-            "single_thread": {"value": r1, "unit": "steps/s", "cores": 1, "sample": s1}}
+            "single_thread_180x180x75": {"value": r1, "unit": "steps/s", "cores": 1,
+                                         "sample": s1}}
 
 
 def run_reference(args, world, rank, local, dist):
+    """The reference's CPU implementation of the path (the oracle's C
+    restatement of rk2_serial_driver, OpenMP over rows on all host threads)
+    on the bench workload: args.warmup untimed whole steps, then args.steps
+    timed whole steps.  Rank 0 only."""
     if rank != 0:
         return
-    rates = []
-    sample, cores = "", 1
-    for _ in range(max(1, min(args.steps, 3))):
-        r, sample, cores = cpu_reference_rate(0)
-        rates.append(r)
-    value = sorted(rates)[len(rates) // 2]
-    r1, s1, _ = cpu_reference_rate(None)
+    value, sample, cores = cpu_whole_steps(NI, NJ, BT, args.steps, 0, warmup=args.warmup)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "split RK2 step 720x720x75 bt50 (seeded beta plane)",
-                       "ni": NI, "nj": NJ, "nk": NK, "bt_nsteps": BT},
+                       "ni": NI, "nj": NJ, "nk": NK, "bt_nsteps": BT, "dt": 600.0},
             "cpu_baseline": {"value": value, "unit": "steps/s", "cores": cores,
-                             "kind": "port", "sample": sample,
-                             "single_thread": {"value": r1, "unit": "steps/s", "cores": 1,
-                                               "sample": s1}},
+                             "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def run_cudac(kernel_lib, steps, warmup, local):
+    """steps/s of the reference's CUDA C host side (the C++ mirror of
+    rk2_cuda_c_driver and the src/cuda_c wrappers, per-phase device
+    synchronisation included) on the bench workload (CFG state, dt 600 s,
+    720x720x75, bt 50): kernel_lib None drives this library's launch_* entry
+    points (the drop-in path), a path drives that library's (the reference's
+    own kernels).  Median of per-step CUDA-event times after warm-up."""
+    import numpy as np
+    import torch
+    from hackathon_mom6_miniapp_b200 import INIT_CFG, CudaCDriver
+    d = CudaCDriver(NI, NJ, NK, BT, dt=600.0, kernel_lib=kernel_lib, init_mode=INIT_CFG,
+                    seed=0)
+    d.step(warmup)
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        d.step(1)
+        e1.record()
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    finite = bool(np.isfinite(d.get("h")).all() and np.isfinite(d.get("eta")).all())
+    d.close()
+    times.sort()
+    med = times[len(times) // 2]
+    return {"value": 1000.0 / med, "unit": "steps/s", "ms_per_step_median": med,
+            "ms_per_step_min": times[0], "steps": steps, "warmup": warmup, "finite": finite,
+            "config": {"ni": NI, "nj": NJ, "nk": NK, "bt_nsteps": BT, "dt": 600.0,
+                       "init": "seeded beta plane (CFG), no halo fill"}}
 
 
 def measured_traffic():
@@ -297,27 +342,25 @@ def _finite(x):
     return x
 
 
-def run_mixed(args, world, rank, local, dist, fp64_ms_per_step):
-    """The mixed form (FP32 state, fluxes, stencils and vertical elimination;
-    FP64 column sums, thickness update and barotropic loop) on the same
-    workload and timing protocol, with its per-field error."""
-    import torch
-    from hackathon_mom6_miniapp_b200 import INIT_CFG, MIXED, Model
-    m = Model(NI, NJ, NK, BT, INIT_CFG, seed=rank, dt=600.0, device=local,
-              precision=MIXED, use_graph=not args.no_graph)
-    stream = torch.cuda.ExternalStream(m.stream(), device=f"cuda:{local}")
+def _time_model(m, args, local, dist):
+    """Device time of args.steps steps of a model after args.warmup, max over
+    ranks (ms)."""
     m.step(args.warmup)
     m.synchronize()
     barrier(dist)
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    m.step(args.steps)
-    e1.record(stream)
-    m.synchronize()
-    torch.cuda.synchronize()
-    ms = max_over_ranks(e0.elapsed_time(e1), dist, local)
+    return max_over_ranks(_timed_steps(m, args.steps, local), dist, local)
+
+
+def run_mixed(args, world, rank, local, dist, fp64_ms_per_step):
+    """The mixed form (FP32 state, fluxes, stencils and vertical-viscosity
+    coefficients; FP64 column sums, thickness update, vertical elimination and
+    barotropic loop) on the headline workload and timing protocol, and at the
+    mixed-form configuration (1440x1080x75 bt50) beside the FP64 form of the
+    same size, with its per-field errors."""
+    from hackathon_mom6_miniapp_b200 import FP64, INIT_CFG, MIXED, Model
+    m = Model(NI, NJ, NK, BT, INIT_CFG, seed=rank, dt=600.0, device=local,
+              precision=MIXED, use_graph=not args.no_graph)
+    ms = _time_model(m, args, local, dist)
     m.kernel_timing(True)
     m.step(2)
     m.synchronize()
@@ -328,32 +371,69 @@ def run_mixed(args, world, rank, local, dist, fp64_ms_per_step):
            "ms_per_step": ms / args.steps,
            "speedup_vs_fp64": fp64_ms_per_step / (ms / args.steps),
            "kernel_ms_per_step": {k: v[0] * v[1] / 2 for k, v in kt.items()},
-           "dtype": "f32 state/stencils/vertical elimination, f64 column sums/thickness update/btstep"}
+           "dtype": "f32 state/stencils/vertvisc coefficients, f64 column sums/thickness "
+                    "update/vertical elimination/btstep"}
+    if not args.no_cfg2:
+        c2 = {}
+        for name, prec in (("mixed", MIXED), ("fp64", FP64)):
+            mm = Model(1440, 1080, NK, BT, INIT_CFG, seed=rank, dt=600.0, device=local,
+                       precision=prec, use_graph=not args.no_graph)
+            t = _time_model(mm, args, local, dist)
+            mm.close()
+            c2[name + "_steps_per_s"] = world * args.steps / (t / 1000.0)
+            c2[name + "_ms_per_step"] = t / args.steps
+        c2["speedup_vs_fp64"] = c2["fp64_ms_per_step"] / c2["mixed_ms_per_step"]
+        c2["config"] = {"ni": 1440, "nj": 1080, "nk": NK, "bt_nsteps": BT, "dt": 600.0}
+        out["config2_1440x1080x75"] = c2
     if rank == 0:
         out["rel_l2_720x720x75_10_steps"] = mixed_errors(NI, NJ, 10, 0, local)
         if not args.no_cfg2:
             out["rel_l2_1440x1080x75_100_steps"] = mixed_errors(1440, 1080, 100, 0, local)
-        out["error_reference"] = "FP64 form of the same seed (bit-identical to the oracle)"
+        out["error_reference"] = ("exact FP64 form of the same seed (bit-identical to the "
+                                  "oracle); eta, ubt_av, vbt_av come from the FP64 "
+                                  "barotropic loop in both forms")
     return out
+
+
+ENS_BT = 31
 
 
 def ensemble_domains(n=64, seed=0):
     """The batched-ensemble configuration: n domains, square ni = nj drawn
     uniformly from {90, 120, ..., 360} and nk from {25, 50, 75}, each built
-    like the 180x180 case (seeded beta plane, bt_nsteps = 30) with its own
-    seed."""
+    like the 180x180 case (seeded beta plane, dt 600 s) with its own seed, at
+    31 barotropic substeps: 30, the configured count, is unstable at dt
+    600 s in the serial scheme itself (eta grows past 1e170 m in 50 steps),
+    and 31 is the fewest that stay bounded."""
     import numpy as np
     rng = np.random.default_rng(seed)
     sizes = rng.choice(np.arange(90, 361, 30), size=n)
     depths = rng.choice(np.array([25, 50, 75]), size=n)
-    return [dict(ni=int(a), nj=int(a), nk=int(k), bt_nsteps=30, seed=q)
+    return [dict(ni=int(a), nj=int(a), nk=int(k), bt_nsteps=ENS_BT, seed=q)
             for q, (a, k) in enumerate(zip(sizes, depths))]
+
+
+def _ensemble_health(e):
+    """Every domain finite after the run, and the largest relative change of
+    its total volume (sum of h over the compute domain against h0's: the
+    step conserves it with the periodic / wall halo fill)."""
+    import numpy as np
+    finite, worst = True, 0.0
+    for d in range(len(e)):
+        h, h0 = e.get(d, "h"), e.get(d, "h0")
+        for n in ("u", "v", "eta"):
+            finite = finite and bool(np.isfinite(e.get(d, n)).all())
+        finite = finite and bool(np.isfinite(h).all())
+        sl = (slice(3, -3), slice(3, -3))
+        m0, m1 = float(h0[sl].sum()), float(h[sl].sum())
+        worst = max(worst, abs(m1 - m0) / m0)
+    return finite, worst
 
 
 def run_ensemble(args, world, rank, local, dist):
     """64 uneven domains advanced together (one launch per phase for all of
     them, launch shapes from the autotuner): aggregate cell-layer updates/s
-    over 50 steps."""
+    over 50 steps, with every domain checked for finiteness and volume."""
     import torch
     from hackathon_mom6_miniapp_b200 import Ensemble
     doms = ensemble_domains(64, seed=rank)
@@ -376,13 +456,16 @@ def run_ensemble(args, world, rank, local, dist):
     ms = max_over_ranks(e0.elapsed_time(e1), dist, local)
     launches = e.launch_count() - n0
     cells = e.cell_layers()
+    finite, mass_err = _ensemble_health(e)
     out = {"value": world * cells * steps / (ms / 1000.0), "unit": "cell-layer updates/s",
-           "domains": len(doms), "steps": steps, "bt_nsteps": 30, "ms_per_step": ms / steps,
+           "domains": len(doms), "steps": steps, "bt_nsteps": ENS_BT, "ms_per_step": ms / steps,
            "cell_layers": cells, "launches_per_step": launches / steps,
+           "finite": finite, "max_rel_volume_change": mass_err,
            "tuning": e.tuning(), "autotune_best_ms": best, "autotune_s": t_tune,
            "sizes": "ni=nj from {90..360 step 30}, nk from {25,50,75}, numpy "
                     "default_rng(rank) draws, seeds 0..63",
-           "dtype": "mixed form (f32 state/stencils/vertical elimination, f64 column sums/thickness update/btstep)"}
+           "dtype": "mixed form (f32 state/stencils, f64 column sums/thickness "
+                    "update/vertical elimination/btstep)"}
     e.close()
     return out
 
@@ -546,6 +629,24 @@ def run_ours(args, world, rank, local, dist):
     t1 = time.perf_counter()
     e2e_res = world * args.steps / max_over_ranks(t1 - t0, dist, local)
 
+    # the reference CUDA C backend on this GPU (its kernels built from their
+    # sources with the reference's -O3) and this library's drop-in launch_*
+    # path, both driven by the mirror of the reference host side
+    ref_cudac = abi_dropin = None
+    if not args.no_cudac:
+        ref_so = os.path.join(ROOT, "oracle", "_ref", "libref_cuda_c.so")
+        if os.path.exists(ref_so):
+            ref_cudac = run_cudac(ref_so, args.steps, args.warmup, local)
+            ref_cudac["kernels"] = "reference src/cuda_c/*.cu, nvcc -O3 sm_100a (oracle/_ref)"
+        else:
+            ref_cudac = {"unavailable": "oracle/_ref/libref_cuda_c.so not built "
+                                        "(make -C oracle ref needs the reference sources)"}
+        abi_dropin = run_cudac(None, args.steps, args.warmup, local)
+        abi_dropin["kernels"] = "this library's launch_* entry points"
+        if "value" in ref_cudac:
+            abi_dropin["speedup_vs_reference_cuda_c"] = abi_dropin["value"] / ref_cudac["value"]
+            ref_cudac["fused_speedup"] = value / world / ref_cudac["value"]
+
     mixed = None if args.no_mixed else run_mixed(args, world, rank, local, dist,
                                                    ms / args.steps)
     ensemble = None if args.no_ensemble else run_ensemble(args, world, rank, local, dist)
@@ -585,6 +686,8 @@ def run_ours(args, world, rank, local, dist):
                 "e2e_resident": {"value": e2e_res, "unit": "steps/s",
                                  "h2d_bytes_per_step": bytes_h2d / args.steps,
                                  "d2h_bytes_per_step": bytes_d2h / args.steps},
+                "reference_cuda_c": ref_cudac,
+                "abi_dropin": abi_dropin,
                 "mixed": mixed,
                 "ensemble": ensemble,
                 "surrogate": surrogate,
@@ -630,6 +733,8 @@ def main():
     ap.add_argument("--no-cfg2", action="store_true",
                     help="skip the mixed form's error at 1440x1080x75 after 100 steps")
     ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--no-cudac", action="store_true",
+                    help="skip the reference CUDA C backend and drop-in ABI timings")
     ap.add_argument("--profile-mixed", action="store_true",
                     help="with --profile-case: the mixed-precision form's kernels")
     ap.add_argument("--profile-options", action="store_true",

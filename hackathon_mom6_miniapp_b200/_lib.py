@@ -55,7 +55,10 @@ class Config(ctypes.Structure):
                 ("Kv_ml", ctypes.c_double), ("Kv_extra_bbl", ctypes.c_double),
                 ("Hmix", ctypes.c_double), ("Hbbl", ctypes.c_double),
                 ("bc_fill", ctypes.c_int), ("precision", ctypes.c_int),
-                ("device", ctypes.c_int), ("use_graph", ctypes.c_int)]
+                ("device", ctypes.c_int), ("use_graph", ctypes.c_int),
+                ("exact", ctypes.c_int), ("bt_untiled", ctypes.c_int),
+                ("general_metrics", ctypes.c_int), ("wait_cycles", ctypes.c_longlong),
+                ("mixed_f32_vertvisc", ctypes.c_int)]
 
 
 def library_path():
@@ -94,6 +97,7 @@ def library():
     L.mom6b_kernel_time_ms.argtypes = [vp, ctypes.c_char_p, P(d), P(i64)]
     L.mom6b_cudac_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                      ctypes.c_double, ctypes.c_char_p, P(vp)]
+    L.mom6b_cudac_create_cfg.argtypes = [P(Config), ctypes.c_char_p, P(vp)]
     L.mom6b_cudac_step.argtypes = [vp, ctypes.c_int]
     L.mom6b_cudac_field_size.argtypes = [vp, ctypes.c_int]
     L.mom6b_cudac_field_size.restype = ctypes.c_size_t
@@ -148,6 +152,9 @@ def library():
     L.mom6b_set_visc_remnant.argtypes = [vp, ctypes.c_int]
     L.mom6b_set_hor_visc.argtypes = [vp, ctypes.POINTER(HorVisc)]
     L.mom6b_set_bt_overlap.argtypes = [vp, ctypes.c_int]
+    L.mom6b_set_wait_limit.argtypes = [vp, ctypes.c_longlong, ctypes.c_int]
+    L.mom6b_btstep_noalloc_status.argtypes = [vp]
+    L.mom6b_btstep_noalloc_set_wait.argtypes = [ctypes.c_longlong, ctypes.c_int]
     L.mom6b_continuity_pass.argtypes = [vp, ctypes.c_int, ctypes.c_double]
     L.mom6b_set_coriolis_scheme.argtypes = [vp, ctypes.c_int]
     L.mom6b_read_field_bin.argtypes = [vp, ctypes.c_int, cp]
@@ -173,7 +180,10 @@ class Model:
 
     def __init__(self, ni=180, nj=180, nk=75, bt_nsteps=30, init_mode=INIT_CFG,
                  seed=0, dt=None, Kh=None, bc_fill=None, precision=FP64,
-                 device=0, use_graph=False, dx_km=None):
+                 device=0, use_graph=False, dx_km=None, exact=False, bt_untiled=False,
+                 general_metrics=False, wait_cycles=0, mixed_f32_vertvisc=False):
+        """exact=True: the bit-identical FP64 kernels (the serial driver's
+        roundings); False: the fast FP64 kernels (within 1e-12 relative L2)."""
         L = library()
         c = Config()
         _check(L.mom6b_config_default(ctypes.byref(c), init_mode))
@@ -187,6 +197,9 @@ class Model:
         if dx_km is not None:
             c.dx_km = dx_km
         c.precision, c.device, c.use_graph = precision, device, int(use_graph)
+        c.exact, c.bt_untiled = int(bool(exact)), int(bool(bt_untiled))
+        c.general_metrics, c.wait_cycles = int(bool(general_metrics)), int(wait_cycles)
+        c.mixed_f32_vertvisc = int(bool(mixed_f32_vertvisc))
         self.cfg = c
         h = ctypes.c_void_p()
         rc = L.mom6b_create(ctypes.byref(c), ctypes.byref(h))
@@ -292,6 +305,12 @@ class Model:
     def set_bt_overlap(self, on=True):
         """Run the barotropic chain on a second stream beside the 3-D chain."""
         _check(library().mom6b_set_bt_overlap(self._m, int(bool(on))))
+
+    def set_wait_limit(self, cycles=0, stall_test=False):
+        """Bound of the barotropic barrier waits (clock64 cycles, 0: default);
+        stall_test=True makes the next steps' first barrier wait for an
+        arrival that never comes (a testing aid for the timeout path)."""
+        _check(library().mom6b_set_wait_limit(self._m, int(cycles), int(bool(stall_test))))
 
     def set_visc_remnant(self, on=True):
         """Every vertvisc also writes visc_rem_u / visc_rem_v and the continuity
@@ -580,11 +599,16 @@ class CudaCDriver:
     kernel_lib=None runs this library's own entry points; a path runs the
     entry points of another shared object with the same symbols."""
 
-    def __init__(self, ni=180, nj=180, nk=75, bt_nsteps=30, dt=300.0, kernel_lib=None):
+    def __init__(self, ni=180, nj=180, nk=75, bt_nsteps=30, dt=300.0, kernel_lib=None,
+                 init_mode=INIT_REF, seed=0):
+        """init_mode INIT_REF: the driver's analytic state (dt as given);
+        INIT_CFG: the seeded beta-plane state a Model of the same arguments
+        builds (its Kh and viscosity defaults)."""
         L = library()
         h = ctypes.c_void_p()
         lib = kernel_lib.encode() if kernel_lib else None
-        _check(L.mom6b_cudac_create(ni, nj, nk, bt_nsteps, dt, lib, ctypes.byref(h)))
+        c = make_config(ni, nj, nk, bt_nsteps, init_mode, seed, dt=dt)
+        _check(L.mom6b_cudac_create_cfg(ctypes.byref(c), lib, ctypes.byref(h)))
         self._h = h
         self.n1, self.n2, self.nk = ni + 2, nj + 2, nk
 

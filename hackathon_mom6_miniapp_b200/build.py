@@ -2,9 +2,11 @@
 
 Every CUDA source is compiled with
     -gencode arch=compute_100a,code=sm_100a -O3 -lineinfo --fmad=false
-(no FMA contraction: the FP64 kernels reproduce the serial reference's
-roundings exactly) and linked into hackathon_mom6_miniapp_b200/libmom6b.so.
-Host C++ is compiled with -ffp-contract=off for the same reason.
+(no FMA contraction: the exact FP64 kernels reproduce the serial reference's
+roundings) except FMA_SOURCES -- the mixed form, the ensemble, the network
+and the fast FP64 kernels -- which contract multiply-adds; all are linked
+into hackathon_mom6_miniapp_b200/libmom6b.so.  Host C++ is compiled with
+-ffp-contract=off.
 """
 import os
 import subprocess
@@ -23,13 +25,16 @@ CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", "-Wall"]
 CU_SOURCES = ["k_tendency.cu", "k_vertvisc.cu", "k_continuity.cu", "k_btstep.cu",
               "mom6b_api.cu", "abi_helpers.cu", "abi_barotropic.cu", "abi_hor_visc.cu",
               "abi_vert_visc.cu", "abi_coriolis.cu", "abi_continuity.cu",
-              "cudac_driver.cu", "k_mixed.cu", "k_ensemble.cu", "k_mlp.cu", "diag.cu", "k_hor_visc.cu"]
-# the mixed-precision form contracts FMAs; the FP64 files must not
-FMA_SOURCES = {"k_mixed.cu", "k_ensemble.cu", "k_mlp.cu"}
+              "cudac_driver.cu", "k_mixed.cu", "k_ensemble.cu", "k_mlp.cu", "diag.cu", "k_hor_visc.cu",
+              "k_cont_fast.cu", "k_vv_fast.cu", "k_tendency_fast.cu"]
+# the mixed-precision form and the fast FP64 kernels contract FMAs; the exact
+# FP64 files must not
+FMA_SOURCES = {"k_mixed.cu", "k_ensemble.cu", "k_mlp.cu", "k_cont_fast.cu", "k_vv_fast.cu",
+               "k_tendency_fast.cu"}
 CXX_SOURCES = ["host_init.cpp"]
 HEADERS = ["common.cuh", "kernels.h", "host_init.h", "abi_common.cuh", "tendency_impl.cuh",
            "vertvisc_impl.cuh", "mixed_impl.cuh", "halo_impl.cuh", "mlp.h", "mlp_gemm.cuh",
-           "diag.h"]
+           "diag.h", "cont_impl.cuh", "tma.cuh"]
 
 
 def _newer(target, deps):

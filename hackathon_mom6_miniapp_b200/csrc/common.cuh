@@ -81,4 +81,22 @@ __device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : 
 __device__ __forceinline__ double div_r(double a, double b) { return a / b; }
 __device__ __forceinline__ float div_r(float a, float b) { return __fdividef(a, b); }
 
+// a / b for the fast forms: the hardware's approximate reciprocal of b refined
+// by two Newton-Raphson steps r <- r + r (1 - b r) (each doubles the correct
+// bits), then the quotient corrected once by its residual, q <- q + r (a - b q)
+// (Markstein's scheme).  Within about an ulp of the IEEE quotient; b must be
+// a normal nonzero number (every use here divides by a positive thickness,
+// viscosity or pivot).
+__device__ __forceinline__ double div_nr(double a, double b)
+{
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(b));
+    double e = fma(-b, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-b, r, 1.0);
+    r = fma(r, e, r);
+    const double q = a * r;
+    return fma(r, fma(-b, q, a), q);
+}
+
 } // namespace mom6b

@@ -454,7 +454,20 @@ double* field_ptr(mom6b_cudac* m, int f, bool* three_d)
 extern "C" int mom6b_cudac_create(int ni, int nj, int nk, int bt_nsteps, double dt,
                                   const char* kernel_lib, mom6b_cudac** out)
 {
-    if (!out || ni < 8 || nj < 8 || nk < 1 || bt_nsteps < 1 || !(dt > 0.0))
+    mom6b_config c;
+    mom6b_config_default(&c, MOM6B_INIT_REF);
+    c.ni = ni; c.nj = nj; c.nk = nk; c.bt_nsteps = bt_nsteps; c.dt = dt;
+    return mom6b_cudac_create_cfg(&c, kernel_lib, out);
+}
+
+extern "C" int mom6b_cudac_create_cfg(const mom6b_config* cfg, const char* kernel_lib,
+                                      mom6b_cudac** out)
+{
+    if (!out || !cfg) return mom6b_internal_fail(MOM6B_ERR_ARG, "bad argument");
+    const int ni = cfg->ni, nj = cfg->nj, nk = cfg->nk, bt_nsteps = cfg->bt_nsteps;
+    const double dt = cfg->dt;
+    if (ni < 8 || nj < 8 || nk < 1 || bt_nsteps < 1 || !(dt > 0.0) ||
+        (cfg->init_mode != MOM6B_INIT_REF && cfg->init_mode != MOM6B_INIT_CFG))
         return mom6b_internal_fail(MOM6B_ERR_ARG, "bad argument");
     *out = nullptr;
     std::unique_ptr<mom6b_cudac> m(new mom6b_cudac());
@@ -466,12 +479,11 @@ extern "C" int mom6b_cudac_create(int ni, int nj, int nk, int bt_nsteps, double 
     } else {
         m->T = own_table();
     }
-    mom6b_config c;
-    mom6b_config_default(&c, MOM6B_INIT_REF);
-    c.ni = ni; c.nj = nj; c.nk = nk; c.bt_nsteps = bt_nsteps; c.dt = dt;
+    mom6b_config c = *cfg;
     m->grid = std::make_unique<HostGrid>(c);
     HostGrid& g = *m->grid;
-    g.pi_init = 3.14159265358979323846;   // PI, rk2_cuda_c_driver.F90:477-542
+    if (c.init_mode == MOM6B_INIT_REF)
+        g.pi_init = 3.14159265358979323846;   // PI, rk2_cuda_c_driver.F90:477-542
     g.build();
     m->n1 = g.n1; m->n2 = g.n2; m->nk = nk; m->nstep = bt_nsteps; m->dt = dt;
     // local 1-based bounds: is - isd + 1 with isd = 1

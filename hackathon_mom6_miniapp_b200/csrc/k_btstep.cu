@@ -150,7 +150,7 @@ k_btstep(Dims D, Metrics M, BTWork W, BTParams P, const double* eta_in,
         W.vbt[p] = vbt_in[p];
         if (!FAST) { W.ubt_av[p] = 0.0; W.vbt_av[p] = 0.0; }
     }
-    if (!grid_barrier(W, nblocks, P.spin_budget)) return;
+    if (!grid_barrier(W, nblocks + (unsigned)P.stall_test, P.spin_budget)) return;
 
     auto phase_A = [&]() {
         for_points([&](int r, int i, int j, int p) {
@@ -366,7 +366,7 @@ k_btstep_tiled(Dims D, Metrics M, UniMetrics U, BTWork W, BTParams P, BTTiles T,
         if (TAVG) { W.uhbt[p] = 0.0; W.vhbt[p] = 0.0; }
     }
     if (tid == 0) W.tile_flag[blockIdx.x] = 0u;
-    if (!grid_barrier(W, nblocks, P.spin_budget)) return;
+    if (!grid_barrier(W, nblocks + (unsigned)P.stall_test, P.spin_budget)) return;
 
     // the (up to 8) tiles whose points lie in this tile's width-2 halo
     int nbr[8];
@@ -664,7 +664,7 @@ k_btstep_slots(Dims D, Metrics M, UniMetrics U, BTWork W, BTParams P, BTTiles T,
         if (TAVG) { W.uhbt[p] = 0.0; W.vhbt[p] = 0.0; }
     }
     if (tid == 0) W.tile_flag[blockIdx.x] = 0u;
-    if (!grid_barrier(W, nblocks, P.spin_budget)) return;
+    if (!grid_barrier(W, nblocks + (unsigned)P.stall_test, P.spin_budget)) return;
 
     int nbr[8];
     int nnb = 0;
@@ -1081,48 +1081,44 @@ k_btstep_ens(const EnsDomain* __restrict__ doms, const EnsBtGeo* __restrict__ ge
     }
 }
 
-static int g_bt_blocks = 0;
+// SM count of each device, looked up the first time a barotropic kernel is
+// launched with that device current (one persistent CTA per SM).
+static int g_bt_sms[64];
 
-static cudaError_t init_bt_blocks()
+static cudaError_t bt_blocks(int* out)
 {
-    if (g_bt_blocks != 0) return cudaSuccess;
-    int dev = 0, nsm = 0;
+    int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (e != cudaSuccess) return e;
-    g_bt_blocks = nsm;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (g_bt_sms[dev] == 0) {
+        int nsm = 0;
+        e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return e;
+        g_bt_sms[dev] = nsm;
+    }
+    *out = g_bt_sms[dev];
     return cudaSuccess;
 }
 
-static bool tiles_for(const Dims& D, BTTiles& T)
+// Tiles of the tiled kernel: nbx x nby tiles (at most one per SM) of at most
+// 64 x 64 points covering the updated box [is-1, ie] x [js-1, je]; false when
+// the box needs more (either side above 64 tiles' worth for the SM count).
+static bool tiles_for(const Dims& D, int nsm, BTTiles& T)
 {
-    static int nt = -1;
-    if (nt < 0) {
-        const char* e = getenv("MOM6B_BT_NT");
-        nt = (e && atoi(e) == 512) ? 512 : 1024;
-    }
-    int bw = D.ie - D.is + 2, bh = D.je - D.js + 2;
-    T.nt = nt;
-    if (nt == 512) {
-        // two CTAs per SM, each thread of the 32 x 16 layout owns 2 x 2 points
-        const int maxt = 2 * g_bt_blocks;
-        int nbx = (bw + 63) / 64, nby = (bh + 31) / 32;
-        if ((long long)nbx * nby > maxt) return false;
-        while ((long long)nbx * (nby + 1) <= maxt && (long long)(nbx + 1) * nby > maxt &&
-               (bh + nby) / (nby + 1) >= 8)
-            ++nby;
-        T.nbx = nbx; T.nby = nby;
-        T.tw = (bw + nbx - 1) / nbx; T.th = (bh + nby - 1) / nby;
-        const size_t smem = (size_t)6 * (T.tw + 3) * (T.th + 3) * sizeof(double);
-        return T.tw <= 64 && T.th <= 32 && smem <= 113 * 1024 && nbx * nby <= kBtMaxTiles;
-    }
-    int nbx = 1, nby = 1;
-    while ((long long)(nbx + 1) * (nby + 1) <= g_bt_blocks) { ++nbx; ++nby; }
-    while ((long long)(nbx + 1) * nby <= g_bt_blocks && (bw + nbx) / (nbx + 1) >= 8) ++nbx;
+    const int bw = D.ie - D.is + 2, bh = D.je - D.js + 2;
+    T.nt = 1024;
+    // the fewest tiles of at most 64 points per side, then as many as the SMs
+    // allow while a tile keeps at least 8 points per side
+    int nbx = (bw + 63) / 64, nby = (bh + 63) / 64;
+    if ((long long)nbx * nby > nsm) return false;
+    while ((long long)(nbx + 1) * (nby + 1) <= nsm && (bw + nbx) / (nbx + 1) >= 8 &&
+           (bh + nby) / (nby + 1) >= 8) { ++nbx; ++nby; }
+    while ((long long)(nbx + 1) * nby <= nsm && (bw + nbx) / (nbx + 1) >= 8) ++nbx;
+    while ((long long)nbx * (nby + 1) <= nsm && (bh + nby) / (nby + 1) >= 8) ++nby;
     T.nbx = nbx; T.nby = nby;
     T.tw = (bw + nbx - 1) / nbx; T.th = (bh + nby - 1) / nby;
-    size_t smem = (size_t)6 * (T.tw + 3) * (T.th + 3) * sizeof(double);
+    const size_t smem = (size_t)6 * (T.tw + 3) * (T.th + 3) * sizeof(double);
     // each of the 32 x 32 threads owns the points (txl + 32a, tyl + 32b), a, b in {0, 1}
     return T.tw <= 64 && T.th <= 64 && smem <= 227 * 1024 && nbx * nby <= kBtMaxTiles;
 }
@@ -1136,22 +1132,14 @@ static cudaError_t launch_btstep_tiled(const Dims& D, const Metrics& M, const Un
 {
     const int NT = T.nt;
     size_t smem = (size_t)6 * (T.tw + 3) * (T.th + 3) * sizeof(double);
+    // the slot kernel (four fixed points per thread) up to 62 x 62 tiles,
+    // the general tiled kernel for 63 and 64
     const void* fn;
-    static int slots = -1;
-    if (slots < 0) {
-        const char* e = getenv("MOM6B_BT_SLOTS");
-        slots = e ? atoi(e) : 1;
-    }
-    if (slots && NT == 1024 && T.tw <= 62 && T.th <= 62)
+    if (T.tw <= 62 && T.th <= 62)
         fn = tavg ? (U.valid_bt ? (const void*)k_btstep_slots<true, true>
                                 : (const void*)k_btstep_slots<false, true>)
                   : (U.valid_bt ? (const void*)k_btstep_slots<true, false>
                                 : (const void*)k_btstep_slots<false, false>);
-    else if (NT == 512)
-        fn = tavg ? (U.valid_bt ? (const void*)k_btstep_tiled<512, true, true>
-                                : (const void*)k_btstep_tiled<512, false, true>)
-                  : (U.valid_bt ? (const void*)k_btstep_tiled<512, true, false>
-                                : (const void*)k_btstep_tiled<512, false, false>);
     else
         fn = tavg ? (U.valid_bt ? (const void*)k_btstep_tiled<1024, true, true>
                                 : (const void*)k_btstep_tiled<1024, false, true>)
@@ -1184,25 +1172,22 @@ cudaError_t launch_btstep(const Dims& D, const Metrics& M, const UniMetrics& U,
                           cudaStream_t s)
 {
     const size_t smem_fast = (size_t)PV_N * kBtMaxR * kBtThreads * sizeof(double);
-    cudaError_t e0 = init_bt_blocks();
+    int nsm = 0;
+    cudaError_t e0 = bt_blocks(&nsm);
     if (e0 != cudaSuccess) return e0;
-    {
-        static bool fast_attr = false;
-        if (!fast_attr) {
-            cudaError_t e = cudaFuncSetAttribute(k_btstep<true>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)smem_fast);
-            if (e != cudaSuccess) return e;
-            fast_attr = true;
-        }
-    }
     // tiled variant: the updated box split into at most one tile per SM
     BTTiles T;
-    if (tiles_for(D, T) && !getenv("MOM6B_BT_UNTILED"))
+    if (!P.untiled && tiles_for(D, nsm, T))
         return launch_btstep_tiled(D, M, U, W, P, T, eta_in, ubt_in, vbt_in, u_av, v_av,
                                    eta_av, s);
+    {
+        cudaError_t e = cudaFuncSetAttribute(k_btstep<true>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem_fast);
+        if (e != cudaSuccess) return e;
+    }
     const long long nbox = (long long)(D.ie - D.is + 3) * (D.je - D.js + 3);
-    int blocks = g_bt_blocks;
+    int blocks = nsm;
     int need = (int)((nbox + kBtThreads - 1) / kBtThreads);
     if (blocks > need) blocks = need;
     const bool fast = (long long)blocks * kBtThreads * kBtMaxR >= nbox;
@@ -1241,7 +1226,8 @@ cudaError_t launch_ens_btstep(const EnsDomain* doms, const EnsBtGeo* geo, const 
 {
     if (ntiles <= 0) return cudaSuccess;
     if (max_tw > 64 || max_th > 64) return cudaErrorInvalidValue;
-    cudaError_t e0 = init_bt_blocks();
+    int nsm = 0;
+    cudaError_t e0 = bt_blocks(&nsm);
     if (e0 != cudaSuccess) return e0;
     const int NT = 1024;
     const size_t smem = (size_t)6 * (max_tw + 3) * (max_th + 3) * sizeof(double);
@@ -1253,7 +1239,7 @@ cudaError_t launch_ens_btstep(const EnsDomain* doms, const EnsBtGeo* geo, const 
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, NT, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
-    int blocks = per_sm * g_bt_blocks;
+    int blocks = per_sm * nsm;
     if (blocks > ntiles) blocks = ntiles;
     BTWork C = ctl;
     void* args[] = {(void*)&doms, (void*)&geo, (void*)&tstart, (void*)&n, (void*)&ntiles,
@@ -1276,10 +1262,11 @@ cudaError_t launch_btstep_tavg(const Dims& D, const Metrics& M, const UniMetrics
                                const double* ubt_in, const double* vbt_in, double* u_av,
                                double* v_av, double* eta_av, cudaStream_t s)
 {
-    cudaError_t e0 = init_bt_blocks();
+    int nsm = 0;
+    cudaError_t e0 = bt_blocks(&nsm);
     if (e0 != cudaSuccess) return e0;
     BTTiles T;
-    if (!tiles_for(D, T)) return cudaErrorNotSupported;
+    if (!tiles_for(D, nsm, T)) return cudaErrorNotSupported;
     return launch_btstep_tiled(D, M, U, W, P, T, eta_in, ubt_in, vbt_in, u_av, v_av, eta_av, s,
                                true);
 }
@@ -1304,6 +1291,10 @@ static __device__ __align__(256) double g_noalloc_scratch[kNoAllocHeader +
 // device current.  In host code the symbol is only a host-side stand-in;
 // kernels must be given the address returned by cudaGetSymbolAddress.
 static double* g_noalloc_ptr[64];
+// Wait limit of the loop's barriers (0: kBtDefaultWait) and the stall test
+// aid (BTParams::stall_test), set by mom6b_btstep_noalloc_set_wait.
+static long long g_noalloc_wait = 0;
+static int g_noalloc_stall = 0;
 
 static cudaError_t noalloc_scratch(double** out)
 {
@@ -1380,6 +1371,15 @@ extern "C" int mom6b_btstep_noalloc(
         return MOM6B_NOALLOC_ERR_ARG;
     if ((long long)n1 * (long long)n2 > kNoAllocMaxPoints)
         return MOM6B_NOALLOC_ERR_TOO_LARGE;
+    Dims D{};
+    D.n1 = n1; D.n2 = n2; D.nk = 1;
+    D.is = is; D.ie = ie; D.js = js; D.je = je;
+    D.isd = 1; D.ied = n1; D.jsd = 1; D.jed = n2;
+    D.plane = (long long)n1 * (long long)n2;
+    int nsm = 0;
+    if (bt_blocks(&nsm) != cudaSuccess) return MOM6B_NOALLOC_ERR_CUDA;
+    BTTiles T;
+    if (!tiles_for(D, nsm, T)) return MOM6B_NOALLOC_ERR_TOO_LARGE;
     double* base = nullptr;
     if (noalloc_scratch(&base) != cudaSuccess) return MOM6B_NOALLOC_ERR_CUDA;
     cudaStream_t s = (cudaStream_t)stream;
@@ -1399,11 +1399,6 @@ extern "C" int mom6b_btstep_noalloc(
     W.status = (int*)base + 8;
     W.tile_flag = (unsigned int*)base + 16;   // kBtMaxTiles words, inside the header
     static_assert(64 + kBtMaxTiles * 4 <= kNoAllocHeader * 8, "noalloc header too small");
-    Dims D{};
-    D.n1 = n1; D.n2 = n2; D.nk = 1;
-    D.is = is; D.ie = ie; D.js = js; D.je = je;
-    D.isd = 1; D.ied = n1; D.jsd = 1; D.jed = n2;
-    D.plane = (long long)np;
     Metrics M{};
     M.Datu = Datu; M.Datv = Datv; M.gtot_E = gtot_E; M.gtot_W = gtot_W;
     M.gtot_N = gtot_N; M.gtot_S = gtot_S; M.f_4_u = f_4_u; M.f_4_v = f_4_v;
@@ -1416,12 +1411,35 @@ extern "C" int mom6b_btstep_noalloc(
     P.inv_nstep = 1.0 / (double)nstep;
     P.nstep = nstep; P.first_direction = first_direction;
     P.extended = extended_ranges ? 1 : 0;
-    P.spin_budget = 4000000000LL;
-    if (init_bt_blocks() != cudaSuccess) return MOM6B_NOALLOC_ERR_CUDA;
-    BTTiles T;
-    if (!tiles_for(D, T)) return MOM6B_NOALLOC_ERR_TOO_LARGE;
+    P.spin_budget = g_noalloc_wait > 0 ? g_noalloc_wait : kBtDefaultWait;
+    P.stall_test = g_noalloc_stall;
     if (launch_btstep_tiled(D, M, U, W, P, T, eta_in, ubt_in, vbt_in, u_av, v_av, eta_av,
                             s) != cudaSuccess)
         return MOM6B_NOALLOC_ERR_CUDA;
+    return MOM6B_NOALLOC_OK;
+}
+
+// See mom6b.h: the status word of the last call on the current device.
+extern "C" int mom6b_btstep_noalloc_status(void* stream)
+{
+    using namespace mom6b;
+    double* base = nullptr;
+    if (noalloc_scratch(&base) != cudaSuccess) return MOM6B_NOALLOC_ERR_CUDA;
+    if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess) return MOM6B_NOALLOC_ERR_CUDA;
+    int* status = (int*)base + 8;
+    int st = 0;
+    if (cudaMemcpy(&st, status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return MOM6B_NOALLOC_ERR_CUDA;
+    if (st == kDevOk) return MOM6B_NOALLOC_OK;
+    // clear the word and the barrier count the timed-out blocks left behind
+    if (cudaMemset(base, 0, 16 * sizeof(double)) != cudaSuccess) return MOM6B_NOALLOC_ERR_CUDA;
+    return MOM6B_NOALLOC_ERR_TIMEOUT;
+}
+
+extern "C" int mom6b_btstep_noalloc_set_wait(long long cycles, int stall_test)
+{
+    if (cycles < 0) return MOM6B_NOALLOC_ERR_ARG;
+    mom6b::g_noalloc_wait = cycles;
+    mom6b::g_noalloc_stall = stall_test ? 1 : 0;
     return MOM6B_NOALLOC_OK;
 }

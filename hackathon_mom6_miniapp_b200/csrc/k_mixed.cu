@@ -7,8 +7,10 @@
 //   continuity  the per-face column sums (uh_tot, duhdu_tot, the BT_cont face
 //               areas), the Newton scalars and the thickness update
 //               h = max(hin - dt IareaT (uh(I) - uh(I-1)), 0);
-//   vertvisc    the bottom stress (the coefficients and the elimination are
-//               FP32: the system is diagonally dominant);
+//   vertvisc    the tridiagonal elimination (b1, d1, c1, the eliminated
+//               velocity, the back substitution) and the bottom stress; the
+//               coefficients are FP32.  An opt-in variant eliminates in FP32
+//               too (the system is diagonally dominant);
 //   btstep      runs in FP64 (its 2-D state is a few MB and its cost is the
 //               latency of the substep loop, not bytes).
 // This file is built with FMA contraction (the FP64 files are not), and the
@@ -30,17 +32,11 @@ cudaError_t launch_tendency_f(const Dims& D, const Metrics& M, const UniMetrics&
 
 cudaError_t launch_vertvisc_f(const Dims& D, const Metrics& M, float* u, float* v,
                               const float* h, double dt, const VVParams& P, double* taux_bot,
-                              double* tauy_bot, cudaStream_t s)
+                              double* tauy_bot, cudaStream_t s, bool f32_elim)
 {
-    return launch_vertvisc_pf_t<float>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s);
-}
-
-// PPM edges of every cell of the face rows, then the faces.
-__global__ void __launch_bounds__(128)
-k_ppm_edges_f(Dims D, Metrics M, const float* __restrict__ hin, float* __restrict__ hW,
-              float* __restrict__ hE, float h_min)
-{
-    ppm_cell_f(D, M, hin, hW, hE, h_min, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z);
+    if (f32_elim)
+        return launch_vertvisc_pf_t<float, float>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s);
+    return launch_vertvisc_pf_t<float, double>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s);
 }
 
 __global__ void __launch_bounds__(128)
@@ -70,52 +66,20 @@ cudaError_t launch_continuity_f(const Dims& D, const Metrics& M, const float* u,
                                 double* uh_ovl, double dt, double h_min, cudaStream_t s)
 {
     {
-        static int edges_warp = -1;
-        if (edges_warp < 0) {
-            const char* e = getenv("MOM6B_PPM_WARP");
-            edges_warp = e ? atoi(e) : 1;
-        }
-        int n = (D.ie + 1) - (D.is - 1) + 1;
-        if (edges_warp) {
-            const int warps = (n + kEdgeCellsPerWarpF - 1) / kEdgeCellsPerWarpF;
-            dim3 grid((warps + 3) / 4, D.je - D.js + 1, (D.nk + kEdgeLayersF - 1) / kEdgeLayersF);
-            k_ppm_edges_warp_f<<<grid, 128, 0, s>>>(D, M, hin, hW, hE, (float)h_min);
-        } else {
-            dim3 grid((n + 127) / 128, D.je - D.js + 1, D.nk);
-            k_ppm_edges_f<<<grid, 128, 0, s>>>(D, M, hin, hW, hE, (float)h_min);
-        }
+        const int n = (D.ie + 1) - (D.is - 1) + 1;
+        const int warps = (n + kEdgeCellsPerWarpF - 1) / kEdgeCellsPerWarpF;
+        dim3 grid((warps + 3) / 4, D.je - D.js + 1, (D.nk + kEdgeLayersF - 1) / kEdgeLayersF);
+        k_ppm_edges_warp_f<<<grid, 128, 0, s>>>(D, M, hin, hW, hE, (float)h_min);
     }
     ContOutF O{h, uh, h_u, O2.FA_u_W0, O2.FA_u_WW, O2.FA_u_E0, O2.FA_u_EE, O2.uBT_WW,
                O2.uBT_EE, O2.du_cor};
     const int nb = 128, step = nb - 1;
     const int nfaces = D.ie - (D.is - 1) + 1;
     dim3 grid((nfaces - 1 + step - 1) / step, D.je - D.js + 1, 1);
-    static int minb = -1;
-    if (minb < 0) {
-        const char* e = getenv("MOM6B_CONTF_MINB");
-        minb = e ? atoi(e) : 6;   // 6 CTAs per SM: 2.19 ms per step (5: 2.23, 4: 2.38)
-    }
-    // staged sweeps (5 or 6 CTAs per SM): slower in FP32 on B200 (2.30 and 2.38 ms per
-    // step against 2.19 loading chunks into registers), so off by default
-    static int as = -1;
-    if (as < 0) {
-        const char* e = getenv("MOM6B_CONTF_ASYNC");
-        as = e ? atoi(e) : 0;
-    }
-    if (as == 6)
-        k_cont_faces_f<6, true><<<grid, nb, 0, s>>>(D, M, u, hin, hW, hE, uhbt, O,
-                                                    (float*)uh_ovl, dt);
-    else if (as == 5)
-        k_cont_faces_f<5, true><<<grid, nb, 0, s>>>(D, M, u, hin, hW, hE, uhbt, O,
-                                                    (float*)uh_ovl, dt);
-    else if (minb == 4)
-        k_cont_faces_f<4><<<grid, nb, 0, s>>>(D, M, u, hin, hW, hE, uhbt, O, (float*)uh_ovl, dt);
-    else if (minb == 5)
-        k_cont_faces_f<5><<<grid, nb, 0, s>>>(D, M, u, hin, hW, hE, uhbt, O, (float*)uh_ovl, dt);
-    else if (minb == 6)
-        k_cont_faces_f<6><<<grid, nb, 0, s>>>(D, M, u, hin, hW, hE, uhbt, O, (float*)uh_ovl, dt);
-    else
-        k_cont_faces_f<1><<<grid, nb, 0, s>>>(D, M, u, hin, hW, hE, uhbt, O, (float*)uh_ovl, dt);
+    // 6 CTAs per SM, chunks loaded into registers: 2.19 ms per step at
+    // 720x720x75 (5 CTAs: 2.23, 4: 2.38; staging the sweeps in shared memory
+    // with cp.async: 2.30 and 2.38)
+    k_cont_faces_f<6><<<grid, nb, 0, s>>>(D, M, u, hin, hW, hE, uhbt, O, (float*)uh_ovl, dt);
     return cudaGetLastError();
 }
 

@@ -54,7 +54,18 @@ struct BTParams {
     double dtbt, dgeo_de, trans_wt1, trans_wt2, inv_nstep;
     int nstep, first_direction, extended;
     long long spin_budget;     // clock64 cycles a block may wait at one barrier
+    // Testing aid for the timeout path: 1 makes the loop's first grid barrier
+    // wait for one more block than the launch holds, an arrival that never
+    // comes, so every block's wait runs into spin_budget, records kDevTimeout
+    // and returns.  0 in normal use.
+    int stall_test = 0;
+    // 1: the point-parallel persistent kernel even where the tiled one fits
+    int untiled = 0;
 };
+
+// The default wait limit of the barotropic barriers: 2^31 clock64 cycles,
+// about 1.1 s at the B200's 1965 MHz.
+constexpr long long kBtDefaultWait = 2147483648LL;
 
 // diffu, diffv (both or neither): also store the horizontal-viscosity
 // accelerations of the updated points (diagnostics); with ext_visc they are
@@ -67,6 +78,11 @@ cudaError_t launch_tendency(const Dims& D, const Metrics& M, const UniMetrics& U
                             double* vout, double coef, double h_neglect, cudaStream_t s,
                             double* diffu = nullptr, double* diffv = nullptr, int scheme = 1,
                             bool ext_visc = false);
+// The fast FP64 form (k_tendency_fast.cu): Sadourny scheme, no diagnostics.
+cudaError_t launch_tendency_fast(const Dims& D, const Metrics& M, const UniMetrics& U,
+                                 const double* uin, const double* vin, const double* h,
+                                 const double* ubase, const double* vbase, double* uout,
+                                 double* vout, double coef, double h_neglect, cudaStream_t s);
 // rem_u, rem_v (both or neither): also the vertical-viscosity remnant of
 // every u / v column (vert_visc_remnant).
 cudaError_t launch_vertvisc(const Dims& D, const Metrics& M, double* u, double* v,
@@ -92,6 +108,22 @@ cudaError_t launch_continuity(const Dims& D, const Metrics& M, const double* u,
                               const double* uhbt, const ContOut& O, double* uh_ovl,
                               double dt, double h_min, cudaStream_t s,
                               const double* visc_rem = nullptr);
+// The fast forms of the vertical viscosity (k_vv_fast.cu): FP64 and the
+// mixed form's FP32 storage with the elimination in double.
+bool vertvisc_fast_fits(const Dims& D);
+cudaError_t launch_vertvisc_fast(const Dims& D, const Metrics& M, double* u, double* v,
+                                 const double* h, double dt, const VVParams& P,
+                                 double* taux_bot, double* tauy_bot, cudaStream_t s);
+cudaError_t launch_vertvisc_fast_f(const Dims& D, const Metrics& M, float* u, float* v,
+                                   const float* h, double dt, const VVParams& P,
+                                   double* taux_bot, double* tauy_bot, cudaStream_t s);
+// The fast FP64 form of the zonal continuity (k_cont_fast.cu): no scratch
+// arrays; status receives kDevTimeout if a tile load never lands.  Only for
+// grids with continuity_fast_fits(D) (nk <= 128).
+bool continuity_fast_fits(const Dims& D);
+cudaError_t launch_continuity_fast(const Dims& D, const Metrics& M, const double* u,
+                                   const double* hin, const double* uhbt, const ContOut& O,
+                                   double dt, double h_min, int* status, cudaStream_t s);
 cudaError_t launch_btstep(const Dims& D, const Metrics& M, const UniMetrics& U,
                           const BTWork& W,
                           const BTParams& P, const double* eta_in,
@@ -112,9 +144,11 @@ cudaError_t launch_tendency_f(const Dims& D, const Metrics& M, const UniMetrics&
                               const float* uin, const float* vin, const float* h,
                               const float* ubase, const float* vbase, float* uout,
                               float* vout, float coef, float h_neglect, cudaStream_t s);
+// f32_elim: the tridiagonal elimination in FP32 too (opt-in; the mixed form
+// eliminates in FP64)
 cudaError_t launch_vertvisc_f(const Dims& D, const Metrics& M, float* u, float* v,
                               const float* h, double dt, const VVParams& P, double* taux_bot,
-                              double* tauy_bot, cudaStream_t s);
+                              double* tauy_bot, cudaStream_t s, bool f32_elim = false);
 // O2 supplies the FP64 2-D outputs (BT_cont face areas, du_cor); h, uh, h_u
 // are the FP32 3-D outputs.
 cudaError_t launch_continuity_f(const Dims& D, const Metrics& M, const float* u,

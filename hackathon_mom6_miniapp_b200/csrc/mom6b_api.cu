@@ -17,8 +17,8 @@
 // reading h0 directly in the predictor; the thickness ping-pongs between hB
 // (after the predictor, the reference's htmp) and hA (the state h), whose
 // halo ring is h0 unless the halo fill is enabled.  The barotropic chain
-// reads nothing the 3-D chain writes (SURVEY of the driver: btstep only sees
-// eta/ubt/vbt), so it runs on a second stream joined by events.
+// reads nothing the 3-D chain writes (in rk2_serial_driver.F90:218-399 btstep
+// only sees eta/ubt/vbt), so it can run on a second stream joined by events.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -87,6 +87,7 @@ struct mom6b_model {
     cudaGraphExec_t graph_exec = nullptr;
     bool overlap_bt = false;
     bool timing = false;
+    int stall_test = 0;   // BTParams::stall_test of the step's barotropic loops
     std::vector<TimedLaunch> pending;
     std::map<std::string, std::pair<double, int64_t>> timed;  // ms total, launches
     // learned barotropic surrogate (k_mlp.cu): the network, whether it
@@ -221,7 +222,7 @@ static int detect_uniform(mom6b_model* m)
     UniMetrics& U = m->U;
     U.valid = 0;
     U.valid_bt = 0;
-    if (getenv("MOM6B_GENERAL_METRICS")) return MOM6B_OK;
+    if (m->cfg.general_metrics) return MOM6B_OK;
     bool ok = true;
     auto uni = [&](const std::vector<double>& a, double* out) {
         double v0 = a[g.at(1, 1)];
@@ -520,7 +521,8 @@ static BTParams step_bt_params(const mom6b_config& c)
     P.nstep = c.bt_nsteps;
     P.first_direction = 0;
     P.extended = 0;
-    P.spin_budget = 4000000000LL;
+    P.spin_budget = c.wait_cycles > 0 ? c.wait_cycles : kBtDefaultWait;
+    P.untiled = c.bt_untiled ? 1 : 0;
     return P;
 }
 
@@ -612,6 +614,10 @@ static cudaError_t continuity_pass(mom6b_model* m, cudaStream_t s, const double*
     const double h_min = step_h_min();
     const double* vr_u = m->remnant ? m->visc_rem_u : nullptr;
     const double* vr_v = m->remnant ? m->visc_rem_v : nullptr;
+    if (!m->merid && !m->remnant && !m->cfg.exact && continuity_fast_fits(D))
+        return timed(m, s, "continuity", [&] {
+            return launch_continuity_fast(D, m->M, u, hin, m->uhbt0, O, dt, h_min,
+                                          m->bt.status, s); });
     if (!m->merid)
         return timed(m, s, "continuity", [&] {
             return launch_continuity(D, m->M, u, hin, m->hW, m->hE, m->uhbt0, O, m->uh_ovl,
@@ -669,8 +675,11 @@ static int enqueue_step(mom6b_model* m)
             return launch_tendency_f(D, M, m->U, F(m->u), F(m->v), F(m->h0), F(m->u), F(m->v),
                                      F(m->up), F(m->vp), (float)dt, hvn, s); }));
         CK(timed(m, s, "vertvisc", [&] {
-            return launch_vertvisc_f(D, M, F(m->up), F(m->vp), F(m->h0), dt, VV, m->taux_bot,
-                                     m->tauy_bot, s); }));
+            if (c.mixed_f32_vertvisc || !vertvisc_fast_fits(D))
+                return launch_vertvisc_f(D, M, F(m->up), F(m->vp), F(m->h0), dt, VV, m->taux_bot,
+                                         m->tauy_bot, s, c.mixed_f32_vertvisc != 0);
+            return launch_vertvisc_fast_f(D, M, F(m->up), F(m->vp), F(m->h0), dt, VV,
+                                          m->taux_bot, m->tauy_bot, s); }));
         CK(timed(m, s, "continuity", [&] {
             return launch_continuity_f(D, M, F(m->up), F(m->h0), F(m->hW), F(m->hE), m->uhbt0,
                                        F(m->hB), F(m->uh), F(m->h_u), OB, m->uh_ovl, dt, h_min,
@@ -685,8 +694,12 @@ static int enqueue_step(mom6b_model* m)
             return launch_tendency_f(D, M, m->U, F(m->up), F(m->vp), F(m->hB), F(m->u), F(m->v),
                                      F(m->u), F(m->v), (float)(0.5 * dt), hvn, s); }));
         CK(timed(m, s, "vertvisc", [&] {
-            return launch_vertvisc_f(D, M, F(m->u), F(m->v), F(m->hB), 0.5 * dt, VV,
-                                     m->taux_bot, m->tauy_bot, s); }));
+            if (c.mixed_f32_vertvisc || !vertvisc_fast_fits(D))
+                return launch_vertvisc_f(D, M, F(m->u), F(m->v), F(m->hB), 0.5 * dt, VV,
+                                         m->taux_bot, m->tauy_bot, s,
+                                         c.mixed_f32_vertvisc != 0);
+            return launch_vertvisc_fast_f(D, M, F(m->u), F(m->v), F(m->hB), 0.5 * dt, VV,
+                                          m->taux_bot, m->tauy_bot, s); }));
         CK(timed(m, s, "continuity", [&] {
             return launch_continuity_f(D, M, F(m->u), F(m->hB), F(m->hW), F(m->hE), m->uhbt0,
                                        F(m->hA), F(m->uh), F(m->h_u), OA, m->uh_ovl, 0.5 * dt,
@@ -709,12 +722,20 @@ static int enqueue_step(mom6b_model* m)
             return launch_tendency(D, M, m->U, m->u, m->v, m->h0, m->u, m->v, m->up, m->vp, dt,
                                    hv_neglect, s, du, dv, m->cor_scheme, true); }));
     } else {
+    const bool td_fast = !c.exact && !m->diag_driver && m->cor_scheme == 1;
     CK(timed(m, s, "tendency", [&] {
+        if (td_fast)
+            return launch_tendency_fast(D, M, m->U, m->u, m->v, m->h0, m->u, m->v, m->up, m->vp,
+                                        dt, hv_neglect, s);
         return launch_tendency(D, M, m->U, m->u, m->v, m->h0, m->u, m->v, m->up, m->vp, dt,
                                hv_neglect, s, m->diag_driver ? m->dg_du : nullptr,
                                m->diag_driver ? m->dg_dv : nullptr, m->cor_scheme); }));
     }
+    const bool vv_fast = !c.exact && !m->remnant && vertvisc_fast_fits(D);
     CK(timed(m, s, "vertvisc", [&] {
+        if (vv_fast)
+            return launch_vertvisc_fast(D, M, m->up, m->vp, m->h0, dt, VV, m->taux_bot,
+                                        m->tauy_bot, s);
         return launch_vertvisc(D, M, m->up, m->vp, m->h0, dt, VV, m->taux_bot,
                                m->tauy_bot, s, m->remnant ? m->visc_rem_u : nullptr,
                                m->remnant ? m->visc_rem_v : nullptr); }));
@@ -734,11 +755,18 @@ static int enqueue_step(mom6b_model* m)
                                    0.5 * dt, hv_neglect, s, m->hv_du, m->hv_dv, m->cor_scheme,
                                    true); }));
     } else {
+    const bool td_fast = !c.exact && m->cor_scheme == 1;
     CK(timed(m, s, "tendency", [&] {
+        if (td_fast)
+            return launch_tendency_fast(D, M, m->U, m->up, m->vp, m->hB, m->u, m->v, m->u, m->v,
+                                        0.5 * dt, hv_neglect, s);
         return launch_tendency(D, M, m->U, m->up, m->vp, m->hB, m->u, m->v, m->u, m->v,
                                0.5 * dt, hv_neglect, s, nullptr, nullptr, m->cor_scheme); }));
     }
     CK(timed(m, s, "vertvisc", [&] {
+        if (vv_fast)
+            return launch_vertvisc_fast(D, M, m->u, m->v, m->hB, 0.5 * dt, VV, m->taux_bot,
+                                        m->tauy_bot, s);
         return launch_vertvisc(D, M, m->u, m->v, m->hB, 0.5 * dt, VV, m->taux_bot,
                                m->tauy_bot, s, m->remnant ? m->visc_rem_u : nullptr,
                                m->remnant ? m->visc_rem_v : nullptr); }));
@@ -762,6 +790,7 @@ static int enqueue_step(mom6b_model* m)
         return MOM6B_OK;
     }
     BTParams P = step_bt_params(c);
+    P.stall_test = m->stall_test;
     CK(timed(m, s2, "btstep", [&] {
         return launch_btstep(D, M, m->U, m->bt, P, m->eta, m->ubt, m->vbt, m->ubt_av,
                              m->vbt_av, m->eta_av, s2); }));
@@ -1398,6 +1427,18 @@ extern "C" int mom6b_set_bt_overlap(mom6b_model* m, int on)
     CK(cudaStreamSynchronize(m->s3d));
     CK(cudaStreamSynchronize(m->s2d));
     m->overlap_bt = on != 0;
+    invalidate_graph(m);
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_set_wait_limit(mom6b_model* m, long long cycles, int stall_test)
+{
+    if (!m || cycles < 0) return fail(MOM6B_ERR_ARG, "bad argument");
+    CK(cudaSetDevice(m->cfg.device));
+    CK(cudaStreamSynchronize(m->s3d));
+    CK(cudaStreamSynchronize(m->s2d));
+    m->cfg.wait_cycles = cycles;
+    m->stall_test = stall_test ? 1 : 0;
     invalidate_graph(m);
     return MOM6B_OK;
 }

@@ -24,8 +24,6 @@
 // vs :162-168).
 #pragma once
 
-#include <cstdlib>
-
 #include "kernels.h"
 
 namespace mom6b {
@@ -83,8 +81,19 @@ __device__ __forceinline__ void arakawa_bc(R q00, R qm0, R q0m, R qmm, R& b, R& 
 // Arakawa schemes' coefficients a, b, c, d (:171-193) reach q one corner
 // further east and north, so their tiles stage and evaluate one more column
 // and row; the coefficients are formed where CAu / CAv need them (:228-248).
+// FAST: the fast FP64 form's arithmetic (built with FMA contraction in
+// k_tendency_fast.cu): quotients by div_nr.
+template <bool FAST>
+__device__ __forceinline__ double td_div(double a, double b)
+{
+    if constexpr (FAST) return div_nr(a, b);
+    else return a / b;
+}
+template <bool FAST>
+__device__ __forceinline__ float td_div(float a, float b) { return div_r(a, b); }
+
 template <int TX, int TY, bool UNI, typename R, bool DIAG = false, int COR = 1,
-          bool EXTV = false>
+          bool EXTV = false, bool FAST = false>
 __device__ __forceinline__ void
 tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __restrict__ uin,
               const R* __restrict__ vin, const R* __restrict__ h,
@@ -184,7 +193,7 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
                 R hAv0 = (I >= D.is) ? R(0.5) * ((aT00 * h00) + (aT01 * h01)) : R(0.0);
                 R hAv1 = R(0.5) * ((aT10 * h10) + (aT11 * h11));
                 R hArea_q = (hAu0 + hAu1) + (hAv0 + hAv1);
-                R Ih_q = div_r(G2(Area_q, I, J), hArea_q + R(1.0e-20));
+                R Ih_q = td_div<FAST>(G2(Area_q, I, J), hArea_q + R(1.0e-20));
                 qv = absv * Ih_q;
                 if constexpr (!EXTV) {
                 // hor_visc: shearing strain and stress at q-points (:513-520, :544, :579, :964, :1050)
@@ -208,7 +217,7 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
             R ke = R(0.0), sxx = R(0.0);
             if (i <= D.n1 && j <= D.n2) {
                 R uc = SU(i, j), um = SU(i - 1, j), vc = SV(i, j), vm = SV(i, j - 1);
-                ke = div_r(R(0.25) *
+                ke = td_div<FAST>(R(0.25) *
                                ((G2(dyCu, i, j) * (uc * uc) + G2(dyCu, i - 1, j) * (um * um)) +
                                 (G2(dxCv, i, j) * (vc * vc) + G2(dxCv, i, j - 1) * (vm * vm))),
                            G2(areaT, i, j));
@@ -281,7 +290,7 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
             diffu = dfu[oo];
         } else {
             R h_u = R(0.5) * (G2(mask2dT, I, j) * SH(I, j) + G2(mask2dT, I + 1, j) * SH(I + 1, j));
-            diffu = div_r((IdxCu * ((G2(dx2q, I, j - 1) * SXY(I, j - 1)) -
+            diffu = td_div<FAST>((IdxCu * ((G2(dx2q, I, j - 1) * SXY(I, j - 1)) -
                                     (G2(dx2q, I, j) * SXY(I, j))) +
                            G2(IdyCu, I, j) * ((G2(dy2h, I, j) * SXX(I, j)) -
                                               (G2(dy2h, I + 1, j) * SXX(I + 1, j)))) *
@@ -320,7 +329,7 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
             diffv = dfv[oo];
         } else {
             R h_v = R(0.5) * (G2(mask2dT, i, J) * SH(i, J) + G2(mask2dT, i, J + 1) * SH(i, J + 1));
-            diffv = div_r((IdyCv * ((G2(dy2q, i - 1, J) * SXY(i - 1, J)) -
+            diffv = td_div<FAST>((IdyCv * ((G2(dy2q, i - 1, J) * SXY(i - 1, J)) -
                                     (G2(dy2q, i, J) * SXY(i, J))) -
                            G2(IdxCv, i, J) * ((G2(dx2h, i, J) * SXX(i, J)) -
                                               (G2(dx2h, i, J + 1) * SXX(i, J + 1)))) *
@@ -345,17 +354,17 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
 }
 
 template <int TX, int TY, bool UNI, typename R, int MINB = 1, bool DIAG = false, int COR = 1,
-          bool EXTV = false>
+          bool EXTV = false, bool FAST = false>
 __global__ void __launch_bounds__(TX * TY, MINB)
 k_tendency(Dims D, Metrics M, UniMetrics U, const R* __restrict__ uin,
            const R* __restrict__ vin, const R* __restrict__ h,
            const R* ubase, const R* vbase, R* uout, R* vout,
            R coef, R h_neglect, int k0, int KC, R* dfu = nullptr, R* dfv = nullptr)
 {
-    tendency_tile<TX, TY, UNI, R, DIAG, COR, EXTV>(D, M, U, uin, vin, h, ubase, vbase, uout,
-                                                   vout, coef, h_neglect, k0, KC,
-                                                   (int)blockIdx.x, (int)blockIdx.y,
-                                                   (int)blockIdx.z, dfu, dfv);
+    tendency_tile<TX, TY, UNI, R, DIAG, COR, EXTV, FAST>(D, M, U, uin, vin, h, ubase, vbase,
+                                                         uout, vout, coef, h_neglect, k0, KC,
+                                                         (int)blockIdx.x, (int)blockIdx.y,
+                                                         (int)blockIdx.z, dfu, dfv);
 }
 
 // diffu, diffv from the general hor_visc kernel (EXTV), every Coriolis scheme.
@@ -405,11 +414,14 @@ cudaError_t launch_tendency_arakawa(const Dims& D, const Metrics& M, const UniMe
 constexpr int kTendTX = 32, kTendTY = 8, kTendKC = 5;
 
 // Host launcher: one CTA per (TX x TY) tile of the compute domain and chunk of
-// kTendKC layers.
+// kTendKC layers (5, 8, 15 and 25 layers per CTA measure the same on B200:
+// FP64 2.00-2.01 ms per step, mixed 1.49 -- the staging of the first layer of
+// a chunk is hidden by the other resident CTAs).
 // dfu, dfv (both or neither): also store diffu, diffv (the diagnostic form of
 // the kernel; the step's own launches pass neither).  scheme: the Coriolis
-// scheme (1 SADOURNY75_ENERGY, 2 ARAKAWA_HSU90, 3 ARAKAWA_LAMB81).
-template <typename R>
+// scheme (1 SADOURNY75_ENERGY, 2 ARAKAWA_HSU90, 3 ARAKAWA_LAMB81).  FAST: the
+// fast FP64 arithmetic, Sadourny scheme without the diagnostic outputs only.
+template <typename R, bool FAST = false>
 cudaError_t launch_tendency_t(const Dims& D, const Metrics& M, const UniMetrics& U,
                               const R* uin, const R* vin, const R* h, const R* ubase,
                               const R* vbase, R* uout, R* vout, R coef, R h_neglect,
@@ -419,19 +431,13 @@ cudaError_t launch_tendency_t(const Dims& D, const Metrics& M, const UniMetrics&
     constexpr int TY = kTendTY;
     int nx = D.ie - D.is + 1, ny = D.je - D.js + 1;
     dim3 block(kTendTX, TY, 1);
-    // layers per CTA: 5, 8, 15 and 25 measure the same on B200 (FP64 2.00-2.01 ms
-    // per step, mixed 1.49) -- the staging of the first layer of a chunk is
-    // hidden by the other resident CTAs
-    static int kc = -1;
-    if (kc < 0) {
-        const char* e = getenv("MOM6B_TEND_KC");
-        kc = e ? atoi(e) : kTendKC;
-        if (kc < 1) kc = kTendKC;
-    }
-    const int KCh = kc;
+    const int KCh = kTendKC;
     int nchunks = (D.nk + KCh - 1) / KCh;
     dim3 grid((nx + kTendTX - 1) / kTendTX, (ny + TY - 1) / TY, nchunks);
     if ((dfu == nullptr) != (dfv == nullptr)) return cudaErrorInvalidValue;
+    if constexpr (FAST) {
+        if (ext_visc || dfu || scheme != 1) return cudaErrorInvalidValue;
+    }
     if (ext_visc) {
         if (!dfu || scheme < 1 || scheme > 3) return cudaErrorInvalidValue;
         if (scheme == 1)
@@ -466,25 +472,12 @@ cudaError_t launch_tendency_t(const Dims& D, const Metrics& M, const UniMetrics&
     // CTAs per SM the registers are held to: 4 (64 registers) is the fastest
     // uniform-metric form on B200 (FP64 tendency 2.01 ms per step against 2.13
     // at 3 and 2.62 uncapped); the 2-D metric form keeps 3 (80 registers).
-    static int minb = -1;
-    if (minb < 0) {
-        const char* e = getenv("MOM6B_TEND_MINB");
-        minb = e ? atoi(e) : 4;
-    }
-    if (U.valid) {
-        if (minb == 4)
-            k_tendency<kTendTX, TY, true, R, 4><<<grid, block, 0, s>>>(
-                D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, KCh);
-        else if (minb == 3)
-            k_tendency<kTendTX, TY, true, R, 3><<<grid, block, 0, s>>>(
-                D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, KCh);
-        else
-            k_tendency<kTendTX, TY, true, R><<<grid, block, 0, s>>>(
-                D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, KCh);
-    } else {
-        k_tendency<kTendTX, TY, false, R, 3><<<grid, block, 0, s>>>(
+    if (U.valid)
+        k_tendency<kTendTX, TY, true, R, 4, false, 1, false, FAST><<<grid, block, 0, s>>>(
             D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, KCh);
-    }
+    else
+        k_tendency<kTendTX, TY, false, R, 3, false, 1, false, FAST><<<grid, block, 0, s>>>(
+            D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, KCh);
     return cudaGetLastError();
 }
 

@@ -1,9 +1,11 @@
 // vertvisc_impl.cuh -- the prefetching vertical viscosity kernel, templated
-// on the storage type R of u, v and h, in which the coefficients and the
-// tridiagonal elimination are computed: R = double is the bit-exact FP64
-// form (k_vertvisc.cu); R = float is the mixed form (k_mixed.cu).  The
-// system is diagonally dominant (every pivot is h + dt (Ray + a d1 + a_next)
-// with nonnegative terms), so the FP32 elimination loses only a few units in
+// on the storage type R of u, v and h, in which the coefficients are
+// computed, and on the type E of the tridiagonal elimination: R = E = double
+// is the bit-exact FP64 form (k_vertvisc.cu); R = float, E = double is the
+// mixed form (k_mixed.cu: FP32 state and coefficients, FP64 elimination);
+// R = E = float is the mixed form's opt-in all-FP32 variant.  The system is
+// diagonally dominant (every pivot is h + dt (Ray + a d1 + a_next) with
+// nonnegative terms), so even an FP32 elimination loses only a few units in
 // the last place per layer; the bottom stress accumulates in double.
 //
 // Restates vert_visc_coef + vert_visc_apply of the serial module
@@ -17,9 +19,22 @@
 
 namespace mom6b {
 
-template <typename C>
+template <bool FAST = false>
+__device__ __forceinline__ double vv_div(double a, double b) {
+    if constexpr (FAST) return div_nr(a, b);
+    else return a / b;
+}
+template <bool FAST = false>
+__device__ __forceinline__ float vv_div(float a, float b) { return div_r(a, b); }
+
+template <bool FAST = false, typename C>
 __device__ __forceinline__ C vv_botfn(C z2) {
-    return div_r(C(1.0), C(1.0) + C(0.09) * z2 * z2 * z2 * z2 * z2 * z2);
+    if constexpr (FAST) {
+        const C zz = z2 * z2;
+        return vv_div<true>(C(1.0), C(1.0) + C(0.09) * (zz * zz * zz));
+    } else {
+        return div_r(C(1.0), C(1.0) + C(0.09) * z2 * z2 * z2 * z2 * z2 * z2);
+    }
 }
 
 // Prefetching variant (the default): one per-column local array (botfn(z_i(m)),
@@ -33,8 +48,8 @@ constexpr int kVvChunk = 4;
 // CTAs per SM the registers are held to, by storage type: measured fastest on
 // B200 (FP64 6: 2.28 ms per step, no cap 2.50; FP32 10: 1.13 ms, 8: 1.23,
 // 12: 1.36).
-template <typename R>
-constexpr int vv_min_blocks() { return sizeof(R) == 4 ? 10 : 6; }
+template <typename R, typename E>
+constexpr int vv_min_blocks() { return sizeof(R) == 8 ? 6 : (sizeof(E) == 8 ? 8 : 10); }
 
 // The column of thread tx of the CTA with block coordinates (bx, by): row
 // by of the interleaved u/v row list, column bx * blockDim.x + tx.
@@ -46,7 +61,12 @@ constexpr int vv_min_blocks() { return sizeof(R) == 4 ? 10 : 6; }
 // in shared memory with cp.async (per-thread slots of stage, [2][CH][3][128])
 // while the current chunk is computed, instead of loading each chunk into
 // registers before computing it.  The arithmetic is unchanged.
-template <int KMAX, int CH, typename R, bool REM = false, bool ASYNC = false>
+// FAST: the fast forms' arithmetic (built with FMA contraction): quotients
+// by div_nr, and botfn(z_i) formed top-down from the column total Z = z_i(2)
+// (z_i(K) = Z - the harmonic thickness above K; z_i(nz+1) = 0) instead of
+// being stored by sweep 1, so the per-column local array holds c1 only.
+template <int KMAX, int CH, typename R, typename E, bool REM = false, bool ASYNC = false,
+          bool FAST = false>
 __device__ __forceinline__ void
 vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restrict__ v,
                 const R* __restrict__ h, double dt, const VVParams& P,
@@ -54,12 +74,11 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
                 double* __restrict__ rem_u = nullptr, double* __restrict__ rem_v = nullptr,
                 R* stage = nullptr)
 {
-    // Coefficients (h_harm, z_i, botfn, hvel, a(K)) and the tridiagonal
-    // elimination (b1, d1, c1, the eliminated velocity and the back
-    // substitution) are computed in the storage type R; the bottom stress
+    // Coefficients (h_harm, z_i, botfn, hvel, a(K)) are computed in the
+    // storage type R, the tridiagonal elimination (b1, d1, c1, the
+    // eliminated velocity and the back substitution) in E; the bottom stress
     // accumulates in double.
     using C = R;
-    using E = R;
     E slot[KMAX + 2];   // botfn(z_i(m)), then c1(m)
     const int nz = D.nk;
     // Rows are interleaved so that the u row j and the v rows j-1, j, which
@@ -110,7 +129,7 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
     const int tid = (int)threadIdx.x;
     auto ST = [&](int b, int c, int f) -> R& { return stage[((b * CH + c) * 3 + f) * 128 + tid]; };
     C z = C(0.0);
-    slot[nz + 1] = vv_botfn(C(0.0));
+    if constexpr (!FAST) slot[nz + 1] = vv_botfn(C(0.0));
     auto stage1 = [&](int kt, int b) {
 #pragma unroll
         for (int c = 0; c < CH; ++c) {
@@ -154,9 +173,9 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
         for (int c = 0; c < CH; ++c) {
             int k = kt - c;
             if (k >= 2) {
-                C h_harm = div_r(C(2.0) * a0[c] * a1[c], a0[c] + a1[c] + hn);
+                C h_harm = vv_div<FAST>(C(2.0) * a0[c] * a1[c], a0[c] + a1[c] + hn);
                 z = z + h_harm * I_Hbbl;
-                slot[k] = vv_botfn(z);
+                if constexpr (!FAST) slot[k] = vv_botfn(z);
             }
         }
     }
@@ -164,8 +183,8 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
     // hvel(k): harmonic mean, blended toward the arithmetic mean where the
     // flow opposes the thickness gradient (:162-177)
     // bf_up = botfn(z_i(k+1)) (slot k+1 of sweep 1)
-    auto hvel = [&](C bf_up, C h0, C h1, C vk) -> C {
-        C h_harm = div_r(C(2.0) * h0 * h1, h0 + h1 + hn);
+    auto harm = [&](C h0, C h1) -> C { return vv_div<FAST>(C(2.0) * h0 * h1, h0 + h1 + hn); };
+    auto hvel_h = [&](C bf_up, C h_harm, C h0, C h1, C vk) -> C {
         C hv = h_harm;
         if (vk * (h1 - h0) < C(0.0)) {
             C bf = bf_up;
@@ -174,17 +193,20 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
         }
         return hv;
     };
+    auto hvel = [&](C bf_up, C h0, C h1, C vk) -> C {
+        return hvel_h(bf_up, harm(h0, h1), h0, h1, vk);
+    };
     // a(K2) for K2 in [2, nz] given the running z_top (:185-202)
     // bf_K2 = botfn(z_i(K2)) (slot K2 of sweep 1)
     auto a_of = [&](C bf_K2, C z_top, C hv_lo, C hv_up) -> C {
         C Kv_tot = Kv;
         if (z_top < Hmix) {
-            C topfn = C(1.0) - div_r(z_top, Hmix);
+            C topfn = C(1.0) - vv_div<FAST>(z_top, Hmix);
             Kv_tot = Kv_tot + (Kv_ml - Kv) * topfn;
         }
         Kv_tot = Kv_tot + Kv_extra_bbl * bf_K2;
         C h_shear = C(0.5) * (hv_lo + hv_up + hn);
-        return div_r(Kv_tot, h_shear);
+        return vv_div<FAST>(Kv_tot, h_shear);
     };
     const C a_bot_num = Kv + Kv_extra_bbl;
 
@@ -192,24 +214,41 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
     const E dtE = (E)dt;
     const E sfc_stress = (E)(dt / kRho0 * MOM6B_A2(tau, i, j, D) * msk);
     const E v1 = vc[0];
-    C hv_k = hvel((C)slot[2], hc[0], hn_[0], (C)v1);
+    // FAST: zi is z_i(m) of the deepest interface m whose botfn is formed,
+    // bf_cur = botfn(z_i(k + 1)) for the layer k about to be eliminated
+    C zi = z, bf_cur = C(0.0);
+    const C bf2 = FAST ? vv_botfn<FAST>(zi) : C(0.0);
+    C bf_first;
+    if constexpr (FAST) bf_first = bf2;
+    else bf_first = (C)slot[2];
+    C hv_k = hvel(bf_first, hc[0], hn_[0], (C)v1);
     C z_top = C(0.0);
     C hv_next, a_next;
     E vnext = E(0.0);                        // vel(k + 1) before elimination
     if (nz >= 2) {
         vnext = vc[plane];
-        hv_next = hvel((C)slot[3], hc[plane], hn_[plane], (C)vnext);
-        z_top = z_top + hv_k;
-        a_next = a_of((C)slot[2], z_top, hv_next, hv_k);
+        if constexpr (FAST) {
+            const C h0 = hc[plane], h1 = hn_[plane];
+            const C hh = harm(h0, h1);
+            zi = nz >= 3 ? zi - hh * I_Hbbl : C(0.0);          // z_i(3)
+            bf_cur = vv_botfn<FAST>(zi);
+            hv_next = hvel_h(bf_cur, hh, h0, h1, (C)vnext);
+            z_top = z_top + hv_k;
+            a_next = a_of(bf2, z_top, hv_next, hv_k);
+        } else {
+            hv_next = hvel((C)slot[3], hc[plane], hn_[plane], (C)vnext);
+            z_top = z_top + hv_k;
+            a_next = a_of((C)slot[2], z_top, hv_next, hv_k);
+        }
     } else {
         hv_next = C(0.0);
-        a_next = div_r(a_bot_num, C(0.5) * hv_k + hn);
+        a_next = vv_div<FAST>(a_bot_num, C(0.5) * hv_k + hn);
     }
     E a_k = E(0.0);  // a(1) = 0, surface
     E Rayk = ray_on[0] ? (E)rc[0] : E(0.0);
     E h_u = (E)(hv_k + hn);
     E b_denom_1 = h_u + dtE * (Rayk + a_k);
-    E b1 = div_r(E(1.0), b_denom_1 + dtE * (E)a_next);
+    E b1 = vv_div<FAST>(E(1.0), b_denom_1 + dtE * (E)a_next);
     E d1 = b_denom_1 * b1;
     E u_prev = b1 * (h_u * v1 + sfc_stress);
     vc[0] = (R)u_prev;
@@ -270,9 +309,11 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
             if (k <= nz) pr[c] = ray_on[k - 1] ? (E)rc[(size_t)(k - 1) * plane] : E(0.0);
         }
         }
+        if constexpr (!FAST) {
 #pragma unroll
-        for (int c = 0; c <= CH; ++c)
-            if (kt + 1 + c <= nz + 1) pb[c] = (C)slot[kt + 1 + c];
+            for (int c = 0; c <= CH; ++c)
+                if (kt + 1 + c <= nz + 1) pb[c] = (C)slot[kt + 1 + c];
+        }
 #pragma unroll
         for (int c = 0; c < CH; ++c) {
             int k = kt + c;
@@ -282,18 +323,29 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
                 hv_k = hv_next;
                 if (k < nz) {
                     vnext = pv[c];
-                    hv_next = hvel(pb[c + 1], p0[c], p1[c], (C)vnext);
-                    z_top = z_top + hv_k;
-                    a_next = a_of(pb[c], z_top, hv_next, hv_k);
+                    if constexpr (FAST) {
+                        // botfn(z_i(k + 1)) is bf_cur; z_i(k + 2) drops layer k + 1
+                        const C hh = harm(p0[c], p1[c]);
+                        const C bf_k1 = bf_cur;
+                        zi = k + 2 <= nz ? zi - hh * I_Hbbl : C(0.0);
+                        bf_cur = vv_botfn<FAST>(zi);
+                        hv_next = hvel_h(bf_cur, hh, p0[c], p1[c], (C)vnext);
+                        z_top = z_top + hv_k;
+                        a_next = a_of(bf_k1, z_top, hv_next, hv_k);
+                    } else {
+                        hv_next = hvel(pb[c + 1], p0[c], p1[c], (C)vnext);
+                        z_top = z_top + hv_k;
+                        a_next = a_of(pb[c], z_top, hv_next, hv_k);
+                    }
                 } else {
-                    a_next = div_r(a_bot_num, C(0.5) * hv_k + hn);
+                    a_next = vv_div<FAST>(a_bot_num, C(0.5) * hv_k + hn);
                 }
                 Rayk = pr[c];
                 E c1 = dtE * a_k * b1;
                 slot[k] = c1;
                 h_u = (E)(hv_k + hn);
                 b_denom_1 = h_u + dtE * (Rayk + a_k * d1);
-                b1 = div_r(E(1.0), b_denom_1 + dtE * (E)a_next);
+                b1 = vv_div<FAST>(E(1.0), b_denom_1 + dtE * (E)a_next);
                 d1 = b_denom_1 * b1;
                 u_prev = (h_u * vk + dtE * a_k * u_prev) * b1;
                 vc[(size_t)(k - 1) * plane] = (R)u_prev;
@@ -346,7 +398,8 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
 }
 
 // MINB: the CTAs per SM the register allocation is held to.
-template <int KMAX, int CH, typename R, int MINB = 1, bool REM = false, bool ASYNC = false>
+template <int KMAX, int CH, typename R, typename E, int MINB = 1, bool REM = false,
+          bool ASYNC = false, bool FAST = false>
 __global__ void __launch_bounds__(128, MINB)
 k_vertvisc_pf(Dims D, Metrics M, R* __restrict__ u, R* __restrict__ v,
               const R* __restrict__ h, double dt, VVParams P,
@@ -354,12 +407,17 @@ k_vertvisc_pf(Dims D, Metrics M, R* __restrict__ u, R* __restrict__ v,
               double* __restrict__ rem_u = nullptr, double* __restrict__ rem_v = nullptr)
 {
     __shared__ R stage[ASYNC ? 2 * CH * 3 * 128 : 1];
-    vertvisc_column<KMAX, CH, R, REM, ASYNC>(D, M, u, v, h, dt, P, taux_bot, tauy_bot,
-                                             (int)blockIdx.x, (int)blockIdx.y, rem_u, rem_v,
-                                             stage);
+    vertvisc_column<KMAX, CH, R, E, REM, ASYNC, FAST>(D, M, u, v, h, dt, P, taux_bot,
+                                                      tauy_bot, (int)blockIdx.x,
+                                                      (int)blockIdx.y, rem_u, rem_v, stage);
 }
 
-template <int KMAX, typename R>
+// Launch shapes measured fastest on B200 at 720x720x75: the FP64 form stages
+// sweeps 1 and 2 with cp.async and holds registers to 6 CTAs per SM (2.215 ms
+// per step against 2.285 loaded into registers); the FP32-storage forms load
+// 4-layer chunks into registers (staging measured slower there), held to
+// vv_min_blocks CTAs per SM.
+template <int KMAX, typename R, typename E, bool FAST>
 static cudaError_t launch_vv_pf(const Dims& D, const Metrics& M, R* u, R* v, const R* h,
                                 double dt, const VVParams& P, double* taux_bot,
                                 double* tauy_bot, cudaStream_t s, double* rem_u = nullptr,
@@ -369,74 +427,40 @@ static cudaError_t launch_vv_pf(const Dims& D, const Metrics& M, R* u, R* v, con
     int ncol = D.ie - D.is + 2;
     int nrows = (D.je - D.js + 1) + (D.je - D.js + 2);
     dim3 grid((ncol + nb - 1) / nb, nrows, 1);
-    static int chunk = -1, minb = -1, async = -1;
-    if (chunk < 0) {
-        const char* e = getenv("MOM6B_VV_CHUNK");
-        chunk = e ? atoi(e) : kVvChunk;
-        const char* b = getenv("MOM6B_VV_MINB");
-        minb = b ? atoi(b) : vv_min_blocks<R>();
-        // staged sweeps: FP64 2.215 ms per step against 2.285 loaded into
-        // registers (chunks of 6 layers: 3.11, spilling); the FP32 form is
-        // faster loading into registers (1.02 against 1.10-1.14 ms)
-        const char* a = getenv("MOM6B_VV_ASYNC");
-        async = a ? atoi(a) : (sizeof(R) == 8 ? 6 : 0);
-    }
-    if (async && !rem_u) {
-        // staged sweeps, the register cap by the async minb
-        if (async == 8)
-            k_vertvisc_pf<KMAX, 4, R, 8, false, true><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P,
-                                                                        taux_bot, tauy_bot);
-        else if (async == 4)
-            k_vertvisc_pf<KMAX, 4, R, 4, false, true><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P,
-                                                                        taux_bot, tauy_bot);
-        else if (async == 10 && sizeof(R) == 4)
-            k_vertvisc_pf<KMAX, 4, R, 10, false, true><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P,
-                                                                         taux_bot, tauy_bot);
-        else
-            k_vertvisc_pf<KMAX, 4, R, 6, false, true><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P,
-                                                                        taux_bot, tauy_bot);
-        return cudaGetLastError();
-    }
+    constexpr int MB = vv_min_blocks<R, E>();
     if constexpr (sizeof(R) == 8) {
-        if (rem_u) {   // with the remnant (the FP64 form's register cap)
-            if (async)
-                k_vertvisc_pf<KMAX, 4, R, 6, true, true><<<grid, nb, 0, s>>>(
-                    D, M, u, v, h, dt, P, taux_bot, tauy_bot, rem_u, rem_v);
-            else
-                k_vertvisc_pf<KMAX, 4, R, 6, true><<<grid, nb, 0, s>>>(
-                    D, M, u, v, h, dt, P, taux_bot, tauy_bot, rem_u, rem_v);
-            return cudaGetLastError();
-        }
+        if (rem_u)
+            k_vertvisc_pf<KMAX, kVvChunk, R, E, MB, true, true, FAST><<<grid, nb, 0, s>>>(
+                D, M, u, v, h, dt, P, taux_bot, tauy_bot, rem_u, rem_v);
+        else
+            k_vertvisc_pf<KMAX, kVvChunk, R, E, MB, false, true, FAST><<<grid, nb, 0, s>>>(
+                D, M, u, v, h, dt, P, taux_bot, tauy_bot);
+    } else {
+        k_vertvisc_pf<KMAX, kVvChunk, R, E, MB, false, false, FAST><<<grid, nb, 0, s>>>(
+            D, M, u, v, h, dt, P, taux_bot, tauy_bot);
     }
-    if (chunk == 2)
-        k_vertvisc_pf<KMAX, 2, R><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P, taux_bot, tauy_bot);
-    else if (chunk == 8)
-        k_vertvisc_pf<KMAX, 8, R><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P, taux_bot, tauy_bot);
-    else if (minb == 6)
-        k_vertvisc_pf<KMAX, 4, R, 6><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P, taux_bot, tauy_bot);
-    else if (minb == 8)
-        k_vertvisc_pf<KMAX, 4, R, 8><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P, taux_bot, tauy_bot);
-    else if (minb == 10 && sizeof(R) == 4)
-        k_vertvisc_pf<KMAX, 4, R, 10><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P, taux_bot, tauy_bot);
-    else if (minb == 12 && sizeof(R) == 4)
-        k_vertvisc_pf<KMAX, 4, R, 12><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P, taux_bot, tauy_bot);
-    else
-        k_vertvisc_pf<KMAX, 4, R><<<grid, nb, 0, s>>>(D, M, u, v, h, dt, P, taux_bot, tauy_bot);
     return cudaGetLastError();
 }
 
 // rem_u, rem_v (FP64, both or neither): also the vertical-viscosity remnant.
-template <typename R>
+template <typename R, typename E = R, bool FAST = false>
 cudaError_t launch_vertvisc_pf_t(const Dims& D, const Metrics& M, R* u, R* v, const R* h,
                                  double dt, const VVParams& P, double* taux_bot,
                                  double* tauy_bot, cudaStream_t s, double* rem_u = nullptr,
                                  double* rem_v = nullptr)
 {
     if ((rem_u == nullptr) != (rem_v == nullptr)) return cudaErrorInvalidValue;
-    if (D.nk <= 80) return launch_vv_pf<80>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s, rem_u, rem_v);
-    if (D.nk <= 128) return launch_vv_pf<128>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s, rem_u, rem_v);
-    if (D.nk <= 256) return launch_vv_pf<256>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s, rem_u, rem_v);
-    return launch_vv_pf<1024>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s, rem_u, rem_v);
+    if (D.nk <= 80)
+        return launch_vv_pf<80, R, E, FAST>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s, rem_u,
+                                            rem_v);
+    if (D.nk <= 128)
+        return launch_vv_pf<128, R, E, FAST>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s, rem_u,
+                                             rem_v);
+    if (D.nk <= 256)
+        return launch_vv_pf<256, R, E, FAST>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s, rem_u,
+                                             rem_v);
+    return launch_vv_pf<1024, R, E, FAST>(D, M, u, v, h, dt, P, taux_bot, tauy_bot, s, rem_u,
+                                          rem_v);
 }
 
 } // namespace mom6b

@@ -44,10 +44,10 @@ enum {
 /* arithmetic forms */
 enum {
     MOM6B_FP64 = 0,  /* every field and every operation in double precision */
-    MOM6B_MIXED = 1  /* fields, stencils and the vertical tridiagonal
-                        elimination in single precision; the continuity column
-                        sums, the thickness update and the barotropic loop in
-                        double */
+    MOM6B_MIXED = 1  /* fields, stencils and the vertical-viscosity
+                        coefficients in single precision; the continuity column
+                        sums, the thickness update, the vertical tridiagonal
+                        elimination and the barotropic loop in double */
 };
 
 /* field ids (get/set) */
@@ -82,6 +82,23 @@ typedef struct mom6b_config {
     int precision;         /* MOM6B_FP64 / MOM6B_MIXED */
     int device;            /* CUDA device ordinal */
     int use_graph;         /* 1: replay each step from a captured CUDA graph */
+    int exact;             /* 1: every FP64 kernel keeps the serial driver's
+                              roundings (no FMA contraction, column sums in
+                              layer order): the step is bit-identical to
+                              rk2_serial_driver.  0 (default): the FP64
+                              kernels may contract multiply-adds and sum
+                              columns in another order; every prognostic
+                              field stays within a relative L2 of 1e-12 of
+                              the exact form after 10 steps */
+    int bt_untiled;        /* 1: the point-parallel barotropic kernel even where
+                              the tiled one fits (both give the same answers) */
+    int general_metrics;   /* 1: read every metric from its 2-D array even when
+                              the grid is uniform (same answers) */
+    long long wait_cycles; /* limit of each barotropic barrier wait in clock64
+                              cycles; 0: the default (2^31, about 1.1 s) */
+    int mixed_f32_vertvisc;/* MOM6B_MIXED only, opt-in: the vertical tridiagonal
+                              elimination in FP32 as well (outside the mixed
+                              form's definition, which eliminates in FP64) */
 } mom6b_config;
 
 typedef struct mom6b_model mom6b_model;
@@ -122,6 +139,14 @@ int mom6b_step_host(mom6b_model *m, int nsteps, double *u, double *v, double *h,
 /* verify_state of rk2_serial_driver.F90:563-623 computed on the device:
  * out = {mass_init, mass_final, rel_error, max_u, max_v, max_eta, ke_total}. */
 int mom6b_verify(mom6b_model *m, double *out7);
+
+/* Bound of every barotropic barrier wait of later steps (clock64 cycles; 0:
+ * the default) and, with stall_test = 1, a testing aid that makes the first
+ * barrier of each barotropic loop wait for an arrival that never comes: its
+ * wait runs into the limit, every block returns, and mom6b_synchronize
+ * reports MOM6B_ERR_TIMEOUT (the step's barotropic outputs are then
+ * incomplete).  The model stays usable: set stall_test = 0 and step again. */
+int mom6b_set_wait_limit(mom6b_model *m, long long cycles, int stall_test);
 
 /* Per-kernel launch accounting: number of kernels of this library launched
  * on the model's stream since the last reset. */
@@ -251,16 +276,34 @@ int mom6b_read_field_bin(mom6b_model *m, int field, const char *path);
  * f_4_v are (4, n1, n2)); the outputs may alias the inputs.  The loop's work
  * arrays live in one static device array of the library sized for
  * n1 * n2 <= 589,824 points (768 x 768, about 28.3 MB per GPU, held until the
- * process exits); larger grids return MOM6B_NOALLOC_ERR_TOO_LARGE.  All calls
- * share that array, so calls that overlap on the GPU race.  The first call on
- * each device looks up the array's device address: make it before any stream
- * capture.  The work is enqueued on `stream` (a cudaStream_t); the call does
- * not synchronize. */
+ * process exits); larger grids return MOM6B_NOALLOC_ERR_TOO_LARGE.  The loop
+ * also splits its updated box of bw x bh = (ie - is + 2) x (je - js + 2)
+ * points into tiles of at most 64 x 64, at most one per SM, so it needs
+ * ceil(bw / 64) * ceil(bh / 64) <= the SM count (148 on a B200: every square
+ * box of the capacity, 1024 x 576 and the like qualify; a 4096 x 144 box does
+ * not); a box that does not qualify also returns MOM6B_NOALLOC_ERR_TOO_LARGE.
+ * All calls share that array, so calls that overlap on the GPU race.  The
+ * first call on each device looks up the array's device address: make it
+ * before any stream capture.  The work is enqueued on `stream` (a
+ * cudaStream_t); the call does not synchronize.
+ *
+ * The loop's grid barriers wait a bounded time (about 1.1 s by default); a
+ * barrier that gives up makes every block return and leaves a timeout status
+ * in the static array.  mom6b_btstep_noalloc_status synchronizes `stream`,
+ * reads that status for the current device and clears it: it returns
+ * MOM6B_NOALLOC_ERR_TIMEOUT when the last call's loop gave up (its outputs
+ * are then incomplete), MOM6B_NOALLOC_OK otherwise.  Query it before the next
+ * call on that device, which resets the status.
+ * mom6b_btstep_noalloc_set_wait sets the wait limit of later calls in clock64
+ * cycles (0: the default); stall_test = 1 is a testing aid that makes the
+ * loop's first barrier wait for an arrival that never comes, so that the
+ * timeout path can be exercised without a fault. */
 enum {
     MOM6B_NOALLOC_OK = 0,
     MOM6B_NOALLOC_ERR_ARG = 1,       /* null pointer or inconsistent bounds */
-    MOM6B_NOALLOC_ERR_TOO_LARGE = 2, /* n1 * n2 above the static capacity */
-    MOM6B_NOALLOC_ERR_CUDA = 3       /* a CUDA runtime call failed */
+    MOM6B_NOALLOC_ERR_TOO_LARGE = 2, /* grid above the static capacity */
+    MOM6B_NOALLOC_ERR_CUDA = 3,      /* a CUDA runtime call failed */
+    MOM6B_NOALLOC_ERR_TIMEOUT = 4    /* a barrier of the last call gave up */
 };
 int mom6b_btstep_noalloc(const double *eta_in, const double *ubt_in,
                          const double *vbt_in, double *u_av, double *v_av,
@@ -274,6 +317,8 @@ int mom6b_btstep_noalloc(const double *eta_in, const double *ubt_in,
                          int js, int je, int nstep, double dtbt, double bebt,
                          double dgeo_de, int first_direction,
                          int extended_ranges, void *stream);
+int mom6b_btstep_noalloc_status(void *stream);
+int mom6b_btstep_noalloc_set_wait(long long cycles, int stall_test);
 
 /* Device address of one of the model's 2-D metric arrays by name ("IareaT",
  * "IdxCu", "IdyCv", "Datu", "Datv", "gtot_E", "gtot_W", "gtot_N", "gtot_S",
@@ -297,6 +342,12 @@ int mom6b_metric_device_ptr(mom6b_model *m, const char *name, void **dptr);
 typedef struct mom6b_cudac mom6b_cudac;
 int mom6b_cudac_create(int ni, int nj, int nk, int bt_nsteps, double dt,
                        const char *kernel_lib, mom6b_cudac **out);
+/* The same mirror on the grid, forcing and initial state a model of *cfg
+ * would build (cfg->init_mode REF or CFG, seed, dt, Kh, vertical viscosity);
+ * the reference's host side has no halo fill, so cfg->bc_fill, precision and
+ * the model-only options are ignored. */
+int mom6b_cudac_create_cfg(const mom6b_config *cfg, const char *kernel_lib,
+                           mom6b_cudac **out);
 int mom6b_cudac_step(mom6b_cudac *m, int nsteps);
 size_t mom6b_cudac_field_size(const mom6b_cudac *m, int field);
 int mom6b_cudac_get_field(mom6b_cudac *m, int field, double *host, size_t count);

@@ -2209,6 +2209,9 @@ int oracle_set(oracle_model *m, int field, const double *in) {
 }
 
 void oracle_set_bt_extended(oracle_model *m, int on) { m->bt_extended = on ? 1 : 0; }
+/* btstep's G%first_direction (mom6_barotropic_serial.F90:250): which velocity
+ * component the odd substeps update first */
+void oracle_set_bt_first_direction(oracle_model *m, int d) { m->first_direction = d; }
 
 /* Copy one of the oracle's grid or control-structure arrays by name (count
  * doubles: n1*n2, or 4*n1*n2 for f_4_u/f_4_v).  Returns 0, or -1 for an

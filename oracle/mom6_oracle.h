@@ -128,6 +128,7 @@ int oracle_set(oracle_model *m, int field, const double *in);
 void oracle_dims(const oracle_model *m, int *out8);
 /* btstep transport ranges: 0 serial (default), 1 extended (CUDA C kernels). */
 void oracle_set_bt_extended(oracle_model *m, int on);
+void oracle_set_bt_first_direction(oracle_model *m, int d);
 /* Copy a named grid / control-structure array (see mom6_oracle.c). */
 int oracle_array(const oracle_model *m, const char *name, double *out, size_t count); /* n1 n2 nk is ie js je ... */
 

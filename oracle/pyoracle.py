@@ -98,6 +98,7 @@ def lib(parallel=False):
         L.oracle_normal.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64]
         L.oracle_normal.restype = d
         L.oracle_set_bt_extended.argtypes = [vp, ctypes.c_int]
+        L.oracle_set_bt_first_direction.argtypes = [vp, ctypes.c_int]
         L.oracle_array.argtypes = [vp, ctypes.c_char_p, P(d), ctypes.c_size_t]
         L.oracle_array.restype = ctypes.c_int
         L.oracle_set_threads.argtypes = [ctypes.c_int]
@@ -278,6 +279,9 @@ class Oracle:
 
     def set_bt_extended(self, on):
         self._L.oracle_set_bt_extended(self._m, 1 if on else 0)
+
+    def set_bt_first_direction(self, d):
+        self._L.oracle_set_bt_first_direction(self._m, int(d))
 
     def halo_fill(self, f, kind):
         f = np.asfortranarray(f.copy())

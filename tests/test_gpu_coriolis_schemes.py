@@ -14,7 +14,7 @@ FIELDS = ["u", "v", "h", "up", "vp", "eta", "ubt_av"]
 def _pair(scheme, mode, shape=(40, 30, 6), seed=2):
     from hackathon_mom6_miniapp_b200 import Model
     dt = 300.0 if mode == INIT_REF else None
-    m = Model(*shape, 30, mode, seed=seed, dt=dt)
+    m = Model(*shape, 30, mode, seed=seed, dt=dt, exact=True)
     o = Oracle(*shape, 30, mode, seed=seed, dt=dt)
     m.set_coriolis_scheme(scheme)
     o.set_coriolis_scheme(scheme)
@@ -35,9 +35,9 @@ def test_arakawa_steps_match_the_oracle(scheme, mode):
 @pytest.mark.gpu
 def test_schemes_differ_and_switch_back():
     from hackathon_mom6_miniapp_b200 import Model
-    a = Model(40, 30, 6, 30, INIT_CFG, seed=2)
-    b = Model(40, 30, 6, 30, INIT_CFG, seed=2)
-    c = Model(40, 30, 6, 30, INIT_CFG, seed=2)
+    a = Model(40, 30, 6, 30, INIT_CFG, seed=2, exact=True)
+    b = Model(40, 30, 6, 30, INIT_CFG, seed=2, exact=True)
+    c = Model(40, 30, 6, 30, INIT_CFG, seed=2, exact=True)
     b.set_coriolis_scheme(2)
     c.set_coriolis_scheme(3)
     c.set_coriolis_scheme(1)

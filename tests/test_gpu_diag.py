@@ -20,7 +20,7 @@ ARGS = (40, 30, 6, 30)
 
 def _model(**kw):
     from hackathon_mom6_miniapp_b200 import INIT_CFG, Model
-    return Model(*ARGS, INIT_CFG, seed=kw.pop("seed", 2), **kw)
+    return Model(*ARGS, INIT_CFG, seed=kw.pop("seed", 2), **kw, exact=True)
 
 
 def _comp(m, a):

@@ -28,7 +28,7 @@ def _singles(domains, nsteps):
     out = []
     for kw in domains:
         m = Model(kw["ni"], kw["nj"], kw["nk"], kw["bt_nsteps"], INIT_CFG, seed=kw["seed"],
-                  precision=MIXED)
+                  precision=MIXED, exact=True)
         m.step(nsteps)
         out.append({f: m.get(f) for f in FIELDS})
         m.close()

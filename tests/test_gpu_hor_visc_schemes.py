@@ -39,7 +39,7 @@ FIELDS = ["u", "v", "h", "eta", "ubt_av", "vbt_av", "up", "vp"]
 
 def _pair(opts, cfg, seed=4, bc_fill=None, nsteps=3):
     from hackathon_mom6_miniapp_b200 import Model
-    m = Model(*SHAPE, 30, INIT_CFG, seed=seed, bc_fill=bc_fill, **cfg)
+    m = Model(*SHAPE, 30, INIT_CFG, seed=seed, bc_fill=bc_fill, **cfg, exact=True)
     o = Oracle(*SHAPE, 30, INIT_CFG, seed=seed, bc_fill=bc_fill, **cfg)
     m.set_hor_visc(**opts)
     o.set_hor_visc(**opts)
@@ -89,8 +89,8 @@ def test_background_dominated_smagorinsky_is_the_fused_laplacian():
     the general kernel plus the external-viscosity tendency reproduce the
     fused Laplacian tendency bit for bit."""
     from hackathon_mom6_miniapp_b200 import Model
-    a = Model(*SHAPE, 30, INIT_CFG, seed=9)
-    b = Model(*SHAPE, 30, INIT_CFG, seed=9)
+    a = Model(*SHAPE, 30, INIT_CFG, seed=9, exact=True)
+    b = Model(*SHAPE, 30, INIT_CFG, seed=9, exact=True)
     b.set_hor_visc(smagorinsky=True)
     a.step(3)
     b.step(3)
@@ -103,7 +103,7 @@ def test_background_dominated_smagorinsky_is_the_fused_laplacian():
 def test_schemes_with_the_arakawa_coriolis(scheme):
     from hackathon_mom6_miniapp_b200 import Model
     opts = dict(biharmonic=True, smagorinsky=True, Ah=0.0)
-    m = Model(*SHAPE, 30, INIT_CFG, seed=5, Kh=0.0)
+    m = Model(*SHAPE, 30, INIT_CFG, seed=5, Kh=0.0, exact=True)
     o = Oracle(*SHAPE, 30, INIT_CFG, seed=5, Kh=0.0)
     for x in (m, o):
         x.set_hor_visc(**opts)
@@ -120,7 +120,7 @@ def test_driver_diagnostics_with_a_scheme(tmp_path):
     from hackathon_mom6_miniapp_b200 import Model
     from hackathon_mom6_miniapp_b200.diag_format import dump_name, read_bin
     opts = dict(biharmonic=True, leith=True, Ah=0.0)
-    m = Model(*SHAPE, 30, INIT_CFG, seed=2, Kh=0.0)
+    m = Model(*SHAPE, 30, INIT_CFG, seed=2, Kh=0.0, exact=True)
     o = Oracle(*SHAPE, 30, INIT_CFG, seed=2, Kh=0.0)
     m.set_hor_visc(**opts)
     o.set_hor_visc(**opts)
@@ -138,7 +138,7 @@ def test_driver_diagnostics_with_a_scheme(tmp_path):
 @pytest.mark.gpu
 def test_schemes_are_refused_in_the_mixed_form():
     from hackathon_mom6_miniapp_b200 import MIXED, Model, Mom6bError
-    m = Model(*SHAPE, 30, INIT_CFG, seed=1, precision=MIXED)
+    m = Model(*SHAPE, 30, INIT_CFG, seed=1, precision=MIXED, exact=True)
     m.set_hor_visc()                       # the driver's options stay available
     with pytest.raises(Mom6bError):
         m.set_hor_visc(biharmonic=True)
@@ -150,7 +150,7 @@ def test_all_schemes_at_180x180x75():
     from hackathon_mom6_miniapp_b200 import Model
     opts = dict(biharmonic=True, smagorinsky=True, leith=True, modified_leith=True,
                 better_bound=True, Ah=1.0e9)
-    m = Model(180, 180, 75, 30, INIT_CFG, seed=11, Kh=0.0)
+    m = Model(180, 180, 75, 30, INIT_CFG, seed=11, Kh=0.0, exact=True)
     o = Oracle(180, 180, 75, 30, INIT_CFG, seed=11, Kh=0.0, threads=0)
     m.set_hor_visc(**opts)
     o.set_hor_visc(**opts)

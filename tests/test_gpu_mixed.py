@@ -14,7 +14,7 @@ BOUND = 1e-5
 
 def _mixed(ni, nj, nk, bt, mode, seed=0, dt=None):
     from hackathon_mom6_miniapp_b200 import MIXED, Model
-    return Model(ni, nj, nk, bt, mode, seed=seed, dt=dt, precision=MIXED)
+    return Model(ni, nj, nk, bt, mode, seed=seed, dt=dt, precision=MIXED, exact=True)
 
 
 @pytest.mark.gpu

@@ -19,7 +19,7 @@ SHAPE = (40, 28, 6)
 
 def _pair(merid, bc_fill=0, seed=5):
     from hackathon_mom6_miniapp_b200 import Model
-    m = Model(*SHAPE, 30, INIT_CFG, seed=seed, bc_fill=bc_fill)
+    m = Model(*SHAPE, 30, INIT_CFG, seed=seed, bc_fill=bc_fill, exact=True)
     o = Oracle(*SHAPE, 30, INIT_CFG, seed=seed, bc_fill=bc_fill)
     m.set_visc_remnant(True)
     o.set_remnant(True)
@@ -61,7 +61,7 @@ def test_unit_remnant_is_the_plain_continuity(direction):
     from hackathon_mom6_miniapp_b200 import Model
     out = []
     for rem in (False, True):
-        m = Model(*SHAPE, 30, INIT_CFG, seed=8)
+        m = Model(*SHAPE, 30, INIT_CFG, seed=8, exact=True)
         m.set_continuity_merid(True)
         if rem:
             m.set_visc_remnant(True)   # buffers start at 1; no vertvisc runs
@@ -79,7 +79,7 @@ def test_unit_remnant_is_the_plain_continuity(direction):
 @pytest.mark.gpu
 def test_remnant_is_refused_in_the_mixed_form():
     from hackathon_mom6_miniapp_b200 import MIXED, Model, Mom6bError
-    m = Model(*SHAPE, 30, INIT_CFG, seed=1, precision=MIXED)
+    m = Model(*SHAPE, 30, INIT_CFG, seed=1, precision=MIXED, exact=True)
     with pytest.raises(Mom6bError):
         m.set_visc_remnant(True)
 
@@ -88,7 +88,7 @@ def test_remnant_is_refused_in_the_mixed_form():
 def test_remnant_steps_at_180x180x75():
     """The remnant path at the configs' small size, bit for bit."""
     from hackathon_mom6_miniapp_b200 import Model
-    m = Model(180, 180, 75, 30, INIT_CFG, seed=12)
+    m = Model(180, 180, 75, 30, INIT_CFG, seed=12, exact=True)
     o = Oracle(180, 180, 75, 30, INIT_CFG, seed=12, threads=0)
     m.set_visc_remnant(True)
     o.set_remnant(True)

@@ -19,7 +19,7 @@ EXTRA = ["ubt_av", "vbt_av", "eta_av", "up", "vp"]
 def _pair(ni, nj, nk, bt, mode, seed=0, dt=None):
     from hackathon_mom6_miniapp_b200 import Model
     o = Oracle(ni, nj, nk, bt, mode, seed=seed, dt=dt)
-    g = Model(ni, nj, nk, bt, mode, seed=seed, dt=dt)
+    g = Model(ni, nj, nk, bt, mode, seed=seed, dt=dt, exact=True)
     return o, g
 
 
@@ -92,7 +92,7 @@ def test_continuity_outputs_bitwise():
 @pytest.mark.gpu
 def test_mass_conservation_device():
     from hackathon_mom6_miniapp_b200 import Model
-    g = Model(64, 48, 10, 40, INIT_CFG, seed=1)
+    g = Model(64, 48, 10, 40, INIT_CFG, seed=1, exact=True)
     g.step(5)
     v = g.verify()
     assert v["rel_error"] < 1e-10
@@ -125,8 +125,8 @@ def test_step_host_roundtrip():
 @pytest.mark.gpu
 def test_graph_replay_matches_eager():
     from hackathon_mom6_miniapp_b200 import Model
-    a = Model(36, 30, 8, 40, INIT_CFG, seed=3, use_graph=False)
-    b = Model(36, 30, 8, 40, INIT_CFG, seed=3, use_graph=True)
+    a = Model(36, 30, 8, 40, INIT_CFG, seed=3, use_graph=False, exact=True)
+    b = Model(36, 30, 8, 40, INIT_CFG, seed=3, use_graph=True, exact=True)
     a.step(4)
     b.step(4)
     for n in STATE + EXTRA:
@@ -136,12 +136,12 @@ def test_graph_replay_matches_eager():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("untiled", [False, True])
-def test_barotropic_variants_bitwise(untiled, monkeypatch):
+def test_barotropic_variants_bitwise(untiled):
     # the tiled (one barrier per substep) and the point-parallel persistent
     # kernels give the oracle's btstep bit for bit
-    if untiled:
-        monkeypatch.setenv("MOM6B_BT_UNTILED", "1")
-    o, g = _pair(70, 50, 6, 40, INIT_CFG, seed=6)
+    from hackathon_mom6_miniapp_b200 import Model
+    o = Oracle(70, 50, 6, 40, INIT_CFG, seed=6)
+    g = Model(70, 50, 6, 40, INIT_CFG, seed=6, exact=True, bt_untiled=untiled)
     o.step(2)
     g.step(2)
     for n in ["eta", "eta_av", "ubt_av", "vbt_av"]:
@@ -150,12 +150,73 @@ def test_barotropic_variants_bitwise(untiled, monkeypatch):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("shape", [(36, 30, 8), (70, 50, 12), (13, 11, 5)])
-def test_continuity_tile_kernel_bitwise(shape, monkeypatch):
-    # the shared-memory tile variant of continuity gives the same step
-    monkeypatch.setenv("MOM6B_CONT_TILE", "1")
-    ni, nj, nk = shape
-    o, g = _pair(ni, nj, nk, 40, INIT_CFG, seed=9)
-    o.step(3)
-    g.step(3)
-    _cmp(o, g, STATE + EXTRA, 0.0, bitwise=True)
+@pytest.mark.parametrize("exact", [True, False])
+def test_config0_as_written(exact):
+    """Configuration 0 as the benchmark defines it -- CFG init, dt = 600 s,
+    180x180x75, 10 steps -- at bt_nsteps = 31, the fewest substeps at which
+    the serial scheme is stable at this time step (30 diverges in the oracle
+    itself, tests/test_config0.py).  Every prognostic field within the
+    north-star 1e-12 relative L2 of the oracle (OpenMP build, identical to
+    the serial one); the exact form bit for bit."""
+    from hackathon_mom6_miniapp_b200 import Model
+    o = Oracle(180, 180, 75, 31, INIT_CFG, seed=0, dt=600.0, threads=0)
+    g = Model(180, 180, 75, 31, INIT_CFG, seed=0, dt=600.0, exact=exact)
+    o.step(10)
+    g.step(10)
+    _cmp(o, g, STATE + ["ubt_av", "vbt_av", "eta_av"], TOL)
+    if exact:
+        _cmp(o, g, STATE, 0.0, bitwise=True)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("exact", [True, False])
+def test_verify_state_matches_oracle(exact):
+    """mom6b_verify's seven statistics (verify_state of
+    rk2_serial_driver.F90:563-623: initial and final mass, their relative
+    difference, max |u|, max |v|, max |eta|, kinetic energy) against the
+    oracle's after 5 steps: equal in the exact form, within 1e-12 relative
+    in the fast form (the mass difference, a difference of two nearly equal
+    sums, within 1e-12 of the mass)."""
+    from hackathon_mom6_miniapp_b200 import Model
+    o = Oracle(64, 48, 10, 40, INIT_CFG, seed=3)
+    g = Model(64, 48, 10, 40, INIT_CFG, seed=3, exact=exact)
+    o.step(5)
+    g.step(5)
+    a, b = g.verify(), o.verify()
+    assert set(a) == set(b)
+    for k in b:
+        if exact:
+            assert a[k] == b[k], (k, a[k], b[k])
+        elif k == "rel_error":
+            assert abs(a[k] - b[k]) <= 1e-12, (k, a[k], b[k])
+        else:
+            assert abs(a[k] - b[k]) <= 1e-12 * abs(b[k]), (k, a[k], b[k])
+    assert b["rel_error"] < 1e-10
+
+
+@pytest.mark.gpu
+def test_barrier_timeout_is_reported_and_recovers():
+    """The barotropic loop's bounded waits: with the stall testing aid its
+    first grid barrier waits for an arrival that never comes, every block
+    gives up after the wait limit (2e6 cycles, about 1 ms) and returns, and
+    mom6b_synchronize reports MOM6B_ERR_TIMEOUT; with the aid off the model
+    steps again and matches a model that never timed out."""
+    from hackathon_mom6_miniapp_b200 import Model, Mom6bError
+    g = Model(36, 30, 8, 40, INIT_CFG, seed=5, exact=True)
+    ref = Model(36, 30, 8, 40, INIT_CFG, seed=5, exact=True)
+    g.set_wait_limit(2_000_000, stall_test=True)
+    g.step(1)
+    with pytest.raises(Mom6bError) as err:
+        g.synchronize()
+    assert err.value.code == 4
+    # restart both from the same state with normal waits (up and vp too: the
+    # velocity update never writes their points at ie / je, which carry over)
+    g.set_wait_limit(0, stall_test=False)
+    for n in ("u", "v", "h", "up", "vp", "eta", "ubt", "vbt", "ubt_av", "vbt_av", "eta_av"):
+        g.set(n, ref.get(n))
+    g.step(2)
+    g.synchronize()
+    ref.step(2)
+    ref.synchronize()
+    for n in STATE:
+        assert np.array_equal(g.get(n), ref.get(n)), n

@@ -83,7 +83,7 @@ def _model(**kw):
     args = dict(ni=96, nj=80, nk=4, bt_nsteps=50, init_mode=INIT_CFG, seed=0, dt=600.0)
     args.update(kw)
     return Model(args.pop("ni"), args.pop("nj"), args.pop("nk"), args.pop("bt_nsteps"),
-                 args.pop("init_mode"), **args)
+                 args.pop("init_mode"), **args, exact=True)
 
 
 def _volume(m):
