@@ -703,7 +703,7 @@ def run_profile_case(args):
     from hackathon_mom6_miniapp_b200 import FP64, INIT_CFG, MIXED, Model
     n = args.profile_case
     m = Model(n, n, NK, BT, INIT_CFG, seed=0, dt=600.0,
-              precision=MIXED if args.profile_mixed else FP64)
+              precision=MIXED if args.profile_mixed else FP64, exact=args.profile_exact)
     if args.profile_options:
         # the optional physics: hor_visc's scheme branches and the remnant
         m.set_hor_visc(biharmonic=True, smagorinsky=True, leith=True, better_bound=True)
@@ -713,6 +713,40 @@ def run_profile_case(args):
     print(json.dumps({"profile_case": n, "steps": args.warmup + args.steps,
                       "launches": m.launch_count()}))
     m.close()
+
+
+def run_profile_abi(args):
+    """A small case of the drop-in path for ncu: the mirror of the reference
+    host side driving this library's launch_* entry points (kernel_lib None)
+    or the reference's kernels (--profile-abi-ref), ni = nj =
+    args.profile_abi, nk = 75, bt 50, CFG state, args.warmup + args.steps
+    steps."""
+    from hackathon_mom6_miniapp_b200 import INIT_CFG, CudaCDriver
+    n = args.profile_abi
+    lib = os.path.join(ROOT, "oracle", "_ref", "libref_cuda_c.so") if args.profile_abi_ref else None
+    d = CudaCDriver(n, n, NK, BT, dt=600.0, kernel_lib=lib, init_mode=INIT_CFG, seed=0)
+    d.step(args.warmup + args.steps)
+    print(json.dumps({"profile_abi": n, "steps": args.warmup + args.steps,
+                      "kernels": "reference" if lib else "libmom6b launch_*"}))
+    d.close()
+
+
+def run_profile_mlp(args):
+    """The surrogate network's tensor-core kernels for ncu: forward and
+    backward of a 65536-row batch (args.warmup + args.steps gradient calls)
+    and one 716 x 716-column inference."""
+    import numpy as np
+    from hackathon_mom6_miniapp_b200 import Mlp
+    B = 65536
+    net = Mlp(batch=B, seed=1)
+    rng = np.random.default_rng(0)
+    X = rng.normal(size=(B, 175)).astype(np.float32)
+    Y = rng.normal(size=(B, 2)).astype(np.float32)
+    for _ in range(args.warmup + args.steps):
+        net.gradients(X, Y)
+    net.predict(X)
+    print(json.dumps({"profile_mlp": B, "gradient_calls": args.warmup + args.steps}))
+    net.close()
 
 
 def main():
@@ -741,11 +775,23 @@ def main():
                     help="with --profile-case: hor_visc schemes and the viscous remnant on")
     ap.add_argument("--profile-case", type=int, default=0,
                     help="run N steps of a ni=nj=N domain only (for ncu captures)")
+    ap.add_argument("--profile-exact", action="store_true",
+                    help="with --profile-case: the exact FP64 kernels")
+    ap.add_argument("--profile-abi", type=int, default=0,
+                    help="run the drop-in launch_* path on a ni=nj=N domain (for ncu)")
+    ap.add_argument("--profile-abi-ref", action="store_true",
+                    help="with --profile-abi: drive the reference's kernels instead")
+    ap.add_argument("--profile-mlp", action="store_true",
+                    help="run the surrogate network's GEMM kernels only (for ncu)")
     args = ap.parse_args()
     world, rank, local, dist = dist_setup(args)
     try:
         if args.profile_case:
             run_profile_case(args)
+        elif args.profile_abi:
+            run_profile_abi(args)
+        elif args.profile_mlp:
+            run_profile_mlp(args)
         elif args.impl == "reference":
             run_reference(args, world, rank, local, dist)
         else:

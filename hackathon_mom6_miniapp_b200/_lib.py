@@ -153,6 +153,7 @@ def library():
     L.mom6b_set_hor_visc.argtypes = [vp, ctypes.POINTER(HorVisc)]
     L.mom6b_set_bt_overlap.argtypes = [vp, ctypes.c_int]
     L.mom6b_set_wait_limit.argtypes = [vp, ctypes.c_longlong, ctypes.c_int]
+    L.mom6b_abi_set_deferral.argtypes = [ctypes.c_int]
     L.mom6b_btstep_noalloc_status.argtypes = [vp]
     L.mom6b_btstep_noalloc_set_wait.argtypes = [ctypes.c_longlong, ctypes.c_int]
     L.mom6b_continuity_pass.argtypes = [vp, ctypes.c_int, ctypes.c_double]
@@ -423,6 +424,12 @@ class Model:
         a = np.ascontiguousarray(a, dtype=np.float32)
         _check(library().mom6b_surrogate_set_params(
             self._m, a.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), a.size))
+
+
+def abi_set_deferral(on=True):
+    """Defer the launch_bt_* substep calls of one btstep_cuda_c into one
+    persistent loop (mom6b_abi_set_deferral; on by default)."""
+    _check(library().mom6b_abi_set_deferral(int(bool(on))))
 
 
 def make_config(ni=180, nj=180, nk=75, bt_nsteps=30, init_mode=INIT_CFG, seed=0, dt=None,

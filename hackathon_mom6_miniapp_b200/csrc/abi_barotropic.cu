@@ -4,15 +4,35 @@
 // backend (mom6_barotropic_kernels.cu:12-334, launchers :347-523).  Each
 // covers the index ranges of the reference kernel and evaluates the same
 // arithmetic in the same order, so results are bit-identical to that kernel
-// built without FMA contraction.  The fused persistent barotropic loop of the
-// high-level API (k_btstep.cu) is the fast path; these entry points exist so
-// the reference's Fortran btstep_cuda_c runs unchanged on this library.
+// built without FMA contraction (the eager_* functions below).
+//
+// Deferral.  btstep_cuda_c (mom6_barotropic_cuda_c.F90:342-431) issues
+// launch_bt_init_kernel, then per substep the nine substep kernels in a fixed
+// order on fixed arrays, then launch_bt_copy_output_kernel, and reads nothing
+// in between.  launch_bt_init_kernel therefore runs and opens a record; each
+// substep call that continues the wrapper's sequence (same arrays, bounds,
+// scalars and stream; the Coriolis updates alternating as first_direction
+// dictates) is recorded instead of launched; launch_bt_copy_output_kernel
+// then runs the whole loop as one persistent launch (k_btstep.cu, extended
+// transport ranges, bit-identical to the substep kernels) into the copy's
+// outputs, on the library's static scratch (the ABI's callee allocates
+// nothing).  A call that breaks the sequence, any other entry point and any
+// cuda_*_c helper replay the record call by call first.  What the deferred
+// loop does not produce are the substep kernels' own arrays (eta, ubt, vbt,
+// their averages and the substep scratch of the control structure, which the
+// next launch_bt_init_kernel re-initialises); the wrapper reads none of them.
+// mom6b_abi_set_deferral(0) turns the deferral off.
+#include <functional>
+#include <vector>
+
 #include "../../include/mom6_cuda_c.h"
+#include "../../include/mom6b.h"
 #include "abi_common.cuh"
+#include "kernels.h"
 
 using namespace mom6b::abi;
 
-extern "C" void launch_bt_init_kernel(double* eta, double* ubt, double* vbt, double* ubt_av,
+static void eager_bt_init_kernel(double* eta, double* ubt, double* vbt, double* ubt_av,
                                       double* vbt_av, double* uhbt_av, double* vhbt_av,
                                       double* eta_in, double* ubt_in, double* vbt_in, int n1,
                                       int n2, int, int, int, int, void* stream)
@@ -29,7 +49,7 @@ extern "C" void launch_bt_init_kernel(double* eta, double* ubt, double* vbt, dou
     });
 }
 
-extern "C" void launch_bt_store_prev_u_kernel(double* ubt_prev, double* ubt, int n1, int n2,
+static void eager_bt_store_prev_u_kernel(double* ubt_prev, double* ubt, int n1, int n2,
                                               int is_l, int ie_l, int js_l, int je_l, int, int,
                                               int, int, void* stream)
 {
@@ -37,7 +57,7 @@ extern "C" void launch_bt_store_prev_u_kernel(double* ubt_prev, double* ubt, int
             [=] __device__(int i, int j, int) { ubt_prev[at2(i, j, n1)] = ubt[at2(i, j, n1)]; });
 }
 
-extern "C" void launch_bt_store_prev_v_kernel(double* vbt_prev, double* vbt, int n1, int n2,
+static void eager_bt_store_prev_v_kernel(double* vbt_prev, double* vbt, int n1, int n2,
                                               int is_l, int ie_l, int js_l, int je_l, int, int,
                                               int, int, void* stream)
 {
@@ -46,7 +66,7 @@ extern "C" void launch_bt_store_prev_v_kernel(double* vbt_prev, double* vbt, int
 }
 
 // eta_pred = eta + (dtbt IareaT) (div of Datu ubt, Datv vbt)   (:86-106)
-extern "C" void launch_bt_eta_pred_kernel(double* eta_pred, double* eta, double* ubt,
+static void eager_bt_eta_pred_kernel(double* eta_pred, double* eta, double* ubt,
                                           double* vbt, double* Datu, double* Datv,
                                           double* IareaT, int n1, int n2, int is_l, int ie_l,
                                           int js_l, int je_l, double dtbt, int, int, int, int,
@@ -62,7 +82,7 @@ extern "C" void launch_bt_eta_pred_kernel(double* eta_pred, double* eta, double*
 }
 
 // PFu = (eta_pred gtot_E - eta_pred(i+1) gtot_W(i+1)) dgeo_de IdxCu   (:112-131)
-extern "C" void launch_bt_pressure_force_u_kernel(double* PFu, double* eta_pred, double* gtot_E,
+static void eager_bt_pressure_force_u_kernel(double* PFu, double* eta_pred, double* gtot_E,
                                                   double* gtot_W, double* IdxCu, int n1, int n2,
                                                   int is_l, int ie_l, int js_l, int je_l,
                                                   double dgeo_de, int, int, int, int,
@@ -76,7 +96,7 @@ extern "C" void launch_bt_pressure_force_u_kernel(double* PFu, double* eta_pred,
             });
 }
 
-extern "C" void launch_bt_pressure_force_v_kernel(double* PFv, double* eta_pred, double* gtot_N,
+static void eager_bt_pressure_force_v_kernel(double* PFv, double* eta_pred, double* gtot_N,
                                                   double* gtot_S, double* IdyCv, int n1, int n2,
                                                   int is_l, int ie_l, int js_l, int je_l,
                                                   double dgeo_de, int, int, int, int,
@@ -92,7 +112,7 @@ extern "C" void launch_bt_pressure_force_v_kernel(double* PFv, double* eta_pred,
 
 // Four-point Coriolis on the other component, then the damped update
 // (:164-189): the pairing of the four products is part of the result.
-extern "C" void launch_bt_coriolis_update_u_kernel(double* ubt, double* Cor_u, double* vbt,
+static void eager_bt_coriolis_update_u_kernel(double* ubt, double* Cor_u, double* vbt,
                                                    double* PFu, double* f_4_u, double* bt_rem_u,
                                                    int n1, int n2, int is_l, int ie_l, int js_l,
                                                    int je_l, double dtbt, int, int, int, int,
@@ -111,7 +131,7 @@ extern "C" void launch_bt_coriolis_update_u_kernel(double* ubt, double* Cor_u, d
             });
 }
 
-extern "C" void launch_bt_coriolis_update_v_kernel(double* vbt, double* Cor_v, double* ubt,
+static void eager_bt_coriolis_update_v_kernel(double* vbt, double* Cor_v, double* ubt,
                                                    double* PFv, double* f_4_v, double* bt_rem_v,
                                                    int n1, int n2, int is_l, int ie_l, int js_l,
                                                    int je_l, double dtbt, int, int, int, int,
@@ -131,7 +151,7 @@ extern "C" void launch_bt_coriolis_update_v_kernel(double* vbt, double* Cor_v, d
 }
 
 // uhbt/vhbt on the extended ranges and the running averages (:228-271).
-extern "C" void launch_bt_transport_eta_accum_kernel(
+static void eager_bt_transport_eta_accum_kernel(
     double* uhbt, double* vhbt, double*, double* ubt_av, double* vbt_av, double* uhbt_av,
     double* vhbt_av, double* ubt, double* vbt, double* ubt_prev, double* vbt_prev, double* Datu,
     double* Datv, double*, int n1, int n2, int is_l, int ie_l, int js_l, int je_l, double,
@@ -156,7 +176,7 @@ extern "C" void launch_bt_transport_eta_accum_kernel(
 }
 
 // eta -= dtbt IareaT div(uhbt, vhbt)   (:279-297)
-extern "C" void launch_bt_eta_update_kernel(double* eta, double* uhbt, double* vhbt,
+static void eager_bt_eta_update_kernel(double* eta, double* uhbt, double* vhbt,
                                             double* IareaT, int n1, int n2, int is_l, int ie_l,
                                             int js_l, int je_l, double dtbt, int, int, int, int,
                                             void* stream)
@@ -170,7 +190,7 @@ extern "C" void launch_bt_eta_update_kernel(double* eta, double* uhbt, double* v
             });
 }
 
-extern "C" void launch_bt_copy_output_kernel(double* u_av_out, double* v_av_out, double* eta_out,
+static void eager_bt_copy_output_kernel(double* u_av_out, double* v_av_out, double* eta_out,
                                              double* ubt_av, double* vbt_av, double* eta, int n1,
                                              int n2, int, int, int, int, void* stream)
 {
@@ -180,4 +200,351 @@ extern "C" void launch_bt_copy_output_kernel(double* u_av_out, double* v_av_out,
         v_av_out[p] = vbt_av[p];
         eta_out[p] = eta[p];
     });
+}
+
+// ---------------------------------------------------------------------------
+// the deferral
+// ---------------------------------------------------------------------------
+namespace {
+
+struct BtRecord {
+    bool open = false;
+    void* stream = nullptr;
+    int n1 = 0, n2 = 0, is = 0, ie = 0, js = 0, je = 0;
+    // launch_bt_init_kernel's arrays (the control structure's state)
+    double *eta = nullptr, *ubt = nullptr, *vbt = nullptr, *ubt_av = nullptr,
+           *vbt_av = nullptr, *uhbt_av = nullptr, *vhbt_av = nullptr;
+    double *eta_in = nullptr, *ubt_in = nullptr, *vbt_in = nullptr;
+    // fixed by the first substep
+    double *ubt_prev = nullptr, *vbt_prev = nullptr, *eta_pred = nullptr, *Datu = nullptr,
+           *Datv = nullptr, *IareaT = nullptr, *PFu = nullptr, *PFv = nullptr,
+           *gtot_E = nullptr, *gtot_W = nullptr, *gtot_N = nullptr, *gtot_S = nullptr,
+           *IdxCu = nullptr, *IdyCv = nullptr, *Cor_u = nullptr, *Cor_v = nullptr,
+           *f_4_u = nullptr, *f_4_v = nullptr, *bt_rem_u = nullptr, *bt_rem_v = nullptr,
+           *uhbt = nullptr, *vhbt = nullptr;
+    double dtbt = 0.0, dgeo_de = 0.0, wt1 = 0.0, wt2 = 0.0, inv_nstep = 0.0;
+    int first_direction = -1;
+    int nsub = 0;       // completed substeps
+    int phase = 0;      // next call within the substep: 0 .. 8
+    std::vector<std::function<void()>> calls;
+};
+
+thread_local BtRecord g_rec;
+bool g_defer = true;
+
+enum { kPrevU = 0, kPrevV, kEtaPred, kPfU, kPfV, kCor1, kCor2, kAccum, kEtaUpd };
+
+bool bounds_ok(int n1, int n2, int is, int ie, int js, int je, void* stream)
+{
+    const BtRecord& R = g_rec;
+    return R.open && n1 == R.n1 && n2 == R.n2 && is == R.is && ie == R.ie && js == R.js &&
+           je == R.je && stream == R.stream;
+}
+
+// Set a fixed array on the first substep, compare it afterwards.
+bool fix(double*& slot, double* p)
+{
+    if (g_rec.nsub == 0 && slot == nullptr) {
+        slot = p;
+        return true;
+    }
+    return slot == p;
+}
+bool fixv(double& slot, double v)
+{
+    if (g_rec.nsub == 0 && g_rec.phase <= kCor1 && slot == 0.0) {
+        slot = v;
+        return true;
+    }
+    return slot == v;
+}
+
+// Which Coriolis update comes first in substep n (1-based): v first when
+// (n + first_direction) is odd (mom6_barotropic_cuda_c.F90, the order of
+// btstep_cuda_c).
+bool v_first(int n) { return ((n + g_rec.first_direction) % 2) == 1; }
+
+void record(std::function<void()> f)
+{
+    g_rec.calls.push_back(std::move(f));
+    if (++g_rec.phase > kEtaUpd) {
+        g_rec.phase = 0;
+        ++g_rec.nsub;
+    }
+}
+
+void close_record() { g_rec = BtRecord(); }
+
+} // namespace
+
+namespace mom6b {
+namespace abi {
+
+void flush_deferred()
+{
+    if (!g_rec.open) return;
+    std::vector<std::function<void()>> calls;
+    calls.swap(g_rec.calls);
+    close_record();
+    for (auto& f : calls) f();
+}
+
+} // namespace abi
+} // namespace mom6b
+
+extern "C" int mom6b_abi_set_deferral(int on)
+{
+    flush_deferred();
+    g_defer = on != 0;
+    return MOM6B_OK;
+}
+
+extern "C" void launch_bt_init_kernel(double* eta, double* ubt, double* vbt, double* ubt_av,
+                                      double* vbt_av, double* uhbt_av, double* vhbt_av,
+                                      double* eta_in, double* ubt_in, double* vbt_in, int n1,
+                                      int n2, int a, int b, int c, int d, void* stream)
+{
+    flush_deferred();
+    eager_bt_init_kernel(eta, ubt, vbt, ubt_av, vbt_av, uhbt_av, vhbt_av, eta_in, ubt_in, vbt_in,
+                         n1, n2, a, b, c, d, stream);
+    if (!g_defer) return;
+    BtRecord& R = g_rec;
+    R.open = true;
+    R.stream = stream;
+    R.n1 = n1; R.n2 = n2;
+    R.eta = eta; R.ubt = ubt; R.vbt = vbt; R.ubt_av = ubt_av; R.vbt_av = vbt_av;
+    R.uhbt_av = uhbt_av; R.vhbt_av = vhbt_av;
+    R.eta_in = eta_in; R.ubt_in = ubt_in; R.vbt_in = vbt_in;
+}
+
+extern "C" void launch_bt_store_prev_u_kernel(double* ubt_prev, double* ubt, int n1, int n2,
+                                              int is_l, int ie_l, int js_l, int je_l, int a,
+                                              int b, int c, int d, void* stream)
+{
+    BtRecord& R = g_rec;
+    if (R.open && R.phase == kPrevU && R.nsub == 0 && R.is == 0 && n1 == R.n1 && n2 == R.n2 &&
+        stream == R.stream) {
+        R.is = is_l; R.ie = ie_l; R.js = js_l; R.je = je_l;   // the loop's bounds
+    }
+    if (R.open && R.phase == kPrevU && bounds_ok(n1, n2, is_l, ie_l, js_l, je_l, stream) &&
+        ubt == R.ubt && fix(R.ubt_prev, ubt_prev)) {
+        record([=] { eager_bt_store_prev_u_kernel(ubt_prev, ubt, n1, n2, is_l, ie_l, js_l, je_l,
+                                                  a, b, c, d, stream); });
+        return;
+    }
+    flush_deferred();
+    eager_bt_store_prev_u_kernel(ubt_prev, ubt, n1, n2, is_l, ie_l, js_l, je_l, a, b, c, d,
+                                 stream);
+}
+
+extern "C" void launch_bt_store_prev_v_kernel(double* vbt_prev, double* vbt, int n1, int n2,
+                                              int is_l, int ie_l, int js_l, int je_l, int a,
+                                              int b, int c, int d, void* stream)
+{
+    BtRecord& R = g_rec;
+    if (R.phase == kPrevV && bounds_ok(n1, n2, is_l, ie_l, js_l, je_l, stream) &&
+        vbt == R.vbt && fix(R.vbt_prev, vbt_prev)) {
+        record([=] { eager_bt_store_prev_v_kernel(vbt_prev, vbt, n1, n2, is_l, ie_l, js_l, je_l,
+                                                  a, b, c, d, stream); });
+        return;
+    }
+    flush_deferred();
+    eager_bt_store_prev_v_kernel(vbt_prev, vbt, n1, n2, is_l, ie_l, js_l, je_l, a, b, c, d,
+                                 stream);
+}
+
+extern "C" void launch_bt_eta_pred_kernel(double* eta_pred, double* eta, double* ubt,
+                                          double* vbt, double* Datu, double* Datv,
+                                          double* IareaT, int n1, int n2, int is_l, int ie_l,
+                                          int js_l, int je_l, double dtbt, int a, int b, int c,
+                                          int d, void* stream)
+{
+    BtRecord& R = g_rec;
+    if (R.phase == kEtaPred && bounds_ok(n1, n2, is_l, ie_l, js_l, je_l, stream) &&
+        eta == R.eta && ubt == R.ubt && vbt == R.vbt && fix(R.eta_pred, eta_pred) &&
+        fix(R.Datu, Datu) && fix(R.Datv, Datv) && fix(R.IareaT, IareaT) && fixv(R.dtbt, dtbt)) {
+        record([=] { eager_bt_eta_pred_kernel(eta_pred, eta, ubt, vbt, Datu, Datv, IareaT, n1, n2,
+                                              is_l, ie_l, js_l, je_l, dtbt, a, b, c, d,
+                                              stream); });
+        return;
+    }
+    flush_deferred();
+    eager_bt_eta_pred_kernel(eta_pred, eta, ubt, vbt, Datu, Datv, IareaT, n1, n2, is_l, ie_l,
+                             js_l, je_l, dtbt, a, b, c, d, stream);
+}
+
+extern "C" void launch_bt_pressure_force_u_kernel(double* PFu, double* eta_pred, double* gtot_E,
+                                                  double* gtot_W, double* IdxCu, int n1, int n2,
+                                                  int is_l, int ie_l, int js_l, int je_l,
+                                                  double dgeo_de, int a, int b, int c, int d,
+                                                  void* stream)
+{
+    BtRecord& R = g_rec;
+    if (R.phase == kPfU && bounds_ok(n1, n2, is_l, ie_l, js_l, je_l, stream) &&
+        eta_pred == R.eta_pred && fix(R.PFu, PFu) && fix(R.gtot_E, gtot_E) &&
+        fix(R.gtot_W, gtot_W) && fix(R.IdxCu, IdxCu) && fixv(R.dgeo_de, dgeo_de)) {
+        record([=] { eager_bt_pressure_force_u_kernel(PFu, eta_pred, gtot_E, gtot_W, IdxCu, n1,
+                                                      n2, is_l, ie_l, js_l, je_l, dgeo_de, a, b,
+                                                      c, d, stream); });
+        return;
+    }
+    flush_deferred();
+    eager_bt_pressure_force_u_kernel(PFu, eta_pred, gtot_E, gtot_W, IdxCu, n1, n2, is_l, ie_l,
+                                     js_l, je_l, dgeo_de, a, b, c, d, stream);
+}
+
+extern "C" void launch_bt_pressure_force_v_kernel(double* PFv, double* eta_pred, double* gtot_N,
+                                                  double* gtot_S, double* IdyCv, int n1, int n2,
+                                                  int is_l, int ie_l, int js_l, int je_l,
+                                                  double dgeo_de, int a, int b, int c, int d,
+                                                  void* stream)
+{
+    BtRecord& R = g_rec;
+    if (R.phase == kPfV && bounds_ok(n1, n2, is_l, ie_l, js_l, je_l, stream) &&
+        eta_pred == R.eta_pred && fix(R.PFv, PFv) && fix(R.gtot_N, gtot_N) &&
+        fix(R.gtot_S, gtot_S) && fix(R.IdyCv, IdyCv) && dgeo_de == R.dgeo_de) {
+        record([=] { eager_bt_pressure_force_v_kernel(PFv, eta_pred, gtot_N, gtot_S, IdyCv, n1,
+                                                      n2, is_l, ie_l, js_l, je_l, dgeo_de, a, b,
+                                                      c, d, stream); });
+        return;
+    }
+    flush_deferred();
+    eager_bt_pressure_force_v_kernel(PFv, eta_pred, gtot_N, gtot_S, IdyCv, n1, n2, is_l, ie_l,
+                                     js_l, je_l, dgeo_de, a, b, c, d, stream);
+}
+
+// The Coriolis updates: the first of substep 1 fixes first_direction, every
+// later pair must alternate as it dictates.
+static bool cor_in_order(bool is_v)
+{
+    BtRecord& R = g_rec;
+    if (R.phase != kCor1 && R.phase != kCor2) return false;
+    const int n = R.nsub + 1;
+    if (R.phase == kCor1 && R.nsub == 0 && R.first_direction < 0)
+        R.first_direction = is_v ? 0 : 1;   // v first at n = 1 iff first_direction is even
+    if (R.first_direction < 0) return false;
+    const bool first_is_v = v_first(n);
+    return (R.phase == kCor1) == (is_v == first_is_v);
+}
+
+extern "C" void launch_bt_coriolis_update_u_kernel(double* ubt, double* Cor_u, double* vbt,
+                                                   double* PFu, double* f_4_u, double* bt_rem_u,
+                                                   int n1, int n2, int is_l, int ie_l, int js_l,
+                                                   int je_l, double dtbt, int a, int b, int c,
+                                                   int d, void* stream)
+{
+    BtRecord& R = g_rec;
+    if (bounds_ok(n1, n2, is_l, ie_l, js_l, je_l, stream) && cor_in_order(false) &&
+        ubt == R.ubt && vbt == R.vbt && PFu == R.PFu && fix(R.Cor_u, Cor_u) &&
+        fix(R.f_4_u, f_4_u) && fix(R.bt_rem_u, bt_rem_u) && dtbt == R.dtbt) {
+        record([=] { eager_bt_coriolis_update_u_kernel(ubt, Cor_u, vbt, PFu, f_4_u, bt_rem_u, n1,
+                                                       n2, is_l, ie_l, js_l, je_l, dtbt, a, b, c,
+                                                       d, stream); });
+        return;
+    }
+    flush_deferred();
+    eager_bt_coriolis_update_u_kernel(ubt, Cor_u, vbt, PFu, f_4_u, bt_rem_u, n1, n2, is_l, ie_l,
+                                      js_l, je_l, dtbt, a, b, c, d, stream);
+}
+
+extern "C" void launch_bt_coriolis_update_v_kernel(double* vbt, double* Cor_v, double* ubt,
+                                                   double* PFv, double* f_4_v, double* bt_rem_v,
+                                                   int n1, int n2, int is_l, int ie_l, int js_l,
+                                                   int je_l, double dtbt, int a, int b, int c,
+                                                   int d, void* stream)
+{
+    BtRecord& R = g_rec;
+    if (bounds_ok(n1, n2, is_l, ie_l, js_l, je_l, stream) && cor_in_order(true) &&
+        vbt == R.vbt && ubt == R.ubt && PFv == R.PFv && fix(R.Cor_v, Cor_v) &&
+        fix(R.f_4_v, f_4_v) && fix(R.bt_rem_v, bt_rem_v) && dtbt == R.dtbt) {
+        record([=] { eager_bt_coriolis_update_v_kernel(vbt, Cor_v, ubt, PFv, f_4_v, bt_rem_v, n1,
+                                                       n2, is_l, ie_l, js_l, je_l, dtbt, a, b, c,
+                                                       d, stream); });
+        return;
+    }
+    flush_deferred();
+    eager_bt_coriolis_update_v_kernel(vbt, Cor_v, ubt, PFv, f_4_v, bt_rem_v, n1, n2, is_l, ie_l,
+                                      js_l, je_l, dtbt, a, b, c, d, stream);
+}
+
+extern "C" void launch_bt_transport_eta_accum_kernel(
+    double* uhbt, double* vhbt, double* eta, double* ubt_av, double* vbt_av, double* uhbt_av,
+    double* vhbt_av, double* ubt, double* vbt, double* ubt_prev, double* vbt_prev, double* Datu,
+    double* Datv, double* IareaT, int n1, int n2, int is_l, int ie_l, int js_l, int je_l,
+    double dtbt, double trans_wt1, double trans_wt2, double inv_nstep, int a, int b, int c,
+    int d, void* stream)
+{
+    BtRecord& R = g_rec;
+    const bool first = R.nsub == 0;
+    if (R.phase == kAccum && bounds_ok(n1, n2, is_l, ie_l, js_l, je_l, stream) &&
+        ubt_av == R.ubt_av && vbt_av == R.vbt_av && uhbt_av == R.uhbt_av &&
+        vhbt_av == R.vhbt_av && ubt == R.ubt && vbt == R.vbt && ubt_prev == R.ubt_prev &&
+        vbt_prev == R.vbt_prev && Datu == R.Datu && Datv == R.Datv && fix(R.uhbt, uhbt) &&
+        fix(R.vhbt, vhbt) && dtbt == R.dtbt &&
+        (first ? (R.wt1 = trans_wt1, R.wt2 = trans_wt2, R.inv_nstep = inv_nstep, true)
+               : (trans_wt1 == R.wt1 && trans_wt2 == R.wt2 && inv_nstep == R.inv_nstep))) {
+        record([=] { eager_bt_transport_eta_accum_kernel(
+                         uhbt, vhbt, eta, ubt_av, vbt_av, uhbt_av, vhbt_av, ubt, vbt, ubt_prev,
+                         vbt_prev, Datu, Datv, IareaT, n1, n2, is_l, ie_l, js_l, je_l, dtbt,
+                         trans_wt1, trans_wt2, inv_nstep, a, b, c, d, stream); });
+        return;
+    }
+    flush_deferred();
+    eager_bt_transport_eta_accum_kernel(uhbt, vhbt, eta, ubt_av, vbt_av, uhbt_av, vhbt_av, ubt,
+                                        vbt, ubt_prev, vbt_prev, Datu, Datv, IareaT, n1, n2,
+                                        is_l, ie_l, js_l, je_l, dtbt, trans_wt1, trans_wt2,
+                                        inv_nstep, a, b, c, d, stream);
+}
+
+extern "C" void launch_bt_eta_update_kernel(double* eta, double* uhbt, double* vhbt,
+                                            double* IareaT, int n1, int n2, int is_l, int ie_l,
+                                            int js_l, int je_l, double dtbt, int a, int b, int c,
+                                            int d, void* stream)
+{
+    BtRecord& R = g_rec;
+    if (R.phase == kEtaUpd && bounds_ok(n1, n2, is_l, ie_l, js_l, je_l, stream) &&
+        eta == R.eta && uhbt == R.uhbt && vhbt == R.vhbt && IareaT == R.IareaT &&
+        dtbt == R.dtbt) {
+        record([=] { eager_bt_eta_update_kernel(eta, uhbt, vhbt, IareaT, n1, n2, is_l, ie_l,
+                                                js_l, je_l, dtbt, a, b, c, d, stream); });
+        return;
+    }
+    flush_deferred();
+    eager_bt_eta_update_kernel(eta, uhbt, vhbt, IareaT, n1, n2, is_l, ie_l, js_l, je_l, dtbt, a,
+                               b, c, d, stream);
+}
+
+extern "C" void launch_bt_copy_output_kernel(double* u_av_out, double* v_av_out, double* eta_out,
+                                             double* ubt_av, double* vbt_av, double* eta, int n1,
+                                             int n2, int a, int b, int c, int d, void* stream)
+{
+    BtRecord& R = g_rec;
+    if (R.open && R.phase == 0 && R.nsub >= 1 && n1 == R.n1 && n2 == R.n2 &&
+        stream == R.stream && ubt_av == R.ubt_av && vbt_av == R.vbt_av && eta == R.eta) {
+        // one persistent loop from the inputs of launch_bt_init_kernel
+        mom6b::Dims D{};
+        D.n1 = n1; D.n2 = n2; D.nk = 1;
+        D.is = R.is; D.ie = R.ie; D.js = R.js; D.je = R.je;
+        D.isd = 1; D.ied = n1; D.jsd = 1; D.jed = n2;
+        D.plane = (long long)n1 * (long long)n2;
+        mom6b::Metrics M{};
+        M.Datu = R.Datu; M.Datv = R.Datv; M.gtot_E = R.gtot_E; M.gtot_W = R.gtot_W;
+        M.gtot_N = R.gtot_N; M.gtot_S = R.gtot_S; M.f_4_u = R.f_4_u; M.f_4_v = R.f_4_v;
+        M.bt_rem_u = R.bt_rem_u; M.bt_rem_v = R.bt_rem_v; M.IareaT = R.IareaT;
+        M.IdxCu = R.IdxCu; M.IdyCv = R.IdyCv;
+        mom6b::BTParams P{};
+        P.dtbt = R.dtbt; P.dgeo_de = R.dgeo_de;
+        P.trans_wt1 = R.wt1; P.trans_wt2 = R.wt2; P.inv_nstep = R.inv_nstep;
+        P.nstep = R.nsub; P.first_direction = R.first_direction; P.extended = 1;
+        // (the loop copies its inputs first, so they may alias its outputs, and
+        // launch_bt_init_kernel left them unchanged)
+        if (mom6b::btstep_static(R.eta_in, R.ubt_in, R.vbt_in, u_av_out, v_av_out, eta_out, M, D,
+                                 P, (cudaStream_t)stream) == MOM6B_NOALLOC_OK) {
+            close_record();
+            return;
+        }
+    }
+    flush_deferred();
+    eager_bt_copy_output_kernel(u_av_out, v_av_out, eta_out, ubt_av, vbt_av, eta, n1, n2, a, b, c,
+                                d, stream);
 }

@@ -67,5 +67,12 @@ inline void run_box(Box b, int nk, void* stream, F f)
     k_box<<<grid, 256, 0, (cudaStream_t)stream>>>(b, f);
 }
 
+// The barotropic deferral (abi_barotropic.cu): the launch_bt_* calls of one
+// btstep_cuda_c are recorded from launch_bt_init_kernel on and run as one
+// persistent loop at launch_bt_copy_output_kernel.  Every other entry point
+// and every runtime helper first replays an open record call by call, so the
+// device state any of them can observe is the reference sequence's.
+void flush_deferred();
+
 } // namespace abi
 } // namespace mom6b

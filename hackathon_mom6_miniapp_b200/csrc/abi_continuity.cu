@@ -168,6 +168,7 @@ extern "C" void launch_ppm_reconstruction_3d_kernel(double* h_W, double* h_E, do
                                                     int upwind_1st_flag, int simple_2nd_flag,
                                                     int, int, int, int, int, int, void* stream)
 {
+    flush_deferred();
     run_box(clip(Box{is_l - 1, ie_l + 1, js_l, je_l}, n1, n2), n3, stream,
             [=] __device__(int i, int j, int k) {
                 const size_t p = at3(i, j, k, n1, n2);
@@ -240,6 +241,7 @@ extern "C" void launch_zonal_flux_layer_3d_kernel(
     int n3, int is_l, int ie_l, int js_l, int je_l, double dt, int vol_CFL_flag,
     int use_visc_rem_flag, int use_por_face_flag, int, int, int, int, int, int, void* stream)
 {
+    flush_deferred();
     const FaceFlags fl{vol_CFL_flag == 1, use_visc_rem_flag == 1, use_por_face_flag == 1};
     run_box(clip(Box{is_l - 1, ie_l, js_l, je_l}, n1, n2), n3, stream,
             [=] __device__(int i, int j, int k) {
@@ -260,6 +262,7 @@ extern "C" void launch_zonal_convergence_kernel(double* h, double* hin, double* 
                                                 double dt, int, int, int, int, int, int,
                                                 void* stream)
 {
+    flush_deferred();
     run_box(clip(Box{is_l, ie_l, js_l, je_l}, n1, n2), n3, stream,
             [=] __device__(int i, int j, int k) {
                 const size_t p = at3(i, j, k, n1, n2);
@@ -272,6 +275,7 @@ extern "C" void launch_visc_rem_max_kernel(double* visc_rem_max_out, double* vis
                                            int je_l, int use_vrm_max_flag, int, int, int, int,
                                            int, int, void* stream)
 {
+    flush_deferred();
     const size_t plane = (size_t)n1 * (size_t)n2;
     run_box(clip(Box{is_l - 1, ie_l, js_l, je_l}, n1, n2), 1, stream,
             [=] __device__(int i, int j, int) {
@@ -291,6 +295,7 @@ extern "C" void launch_uh_duhdu_tot_kernel(double* uh_tot_0, double* duhdu_tot_0
                                            int ie_l, int js_l, int je_l, int, int, int, int,
                                            int, int, void* stream)
 {
+    flush_deferred();
     const size_t plane = (size_t)n1 * (size_t)n2;
     run_box(clip(Box{is_l - 1, ie_l, js_l, je_l}, n1, n2), 1, stream,
             [=] __device__(int i, int j, int) {
@@ -313,6 +318,7 @@ extern "C" void launch_zonal_CFL_limits_kernel(
     int vol_CFL_flag, int use_visc_rem_flag, int aggress_flag, int, int, int, int, int, int,
     void* stream)
 {
+    flush_deferred();
     const size_t plane = (size_t)n1 * (size_t)n2;
     run_box(clip(Box{is_l - 1, ie_l, js_l, je_l}, n1, n2), 1, stream,
             [=] __device__(int i, int j, int) {
@@ -371,6 +377,7 @@ extern "C" void launch_zonal_flux_adjust_kernel(
     double tol_eta_base, double tol_vel_val, int vol_CFL_flag, int use_visc_rem_flag,
     int better_iter_flag, int use_por_face_flag, int, int, int, int, int, int, void* stream)
 {
+    flush_deferred();
     const FaceFlags fl{vol_CFL_flag == 1, use_visc_rem_flag == 1, use_por_face_flag == 1};
     run_box(clip(Box{is_l - 1, ie_l, js_l, je_l}, n1, n2), 1, stream,
             [=] __device__(int i, int j, int) {
@@ -403,6 +410,7 @@ extern "C" void launch_set_zonal_BT_cont_kernel(
     double dt, double tol_eta_base, double tol_vel_val, int vol_CFL_flag, int use_visc_rem_flag,
     int better_iter_flag, int use_por_face_flag, int, int, int, int, int, int, void* stream)
 {
+    flush_deferred();
     const FaceFlags fl{vol_CFL_flag == 1, use_visc_rem_flag == 1, use_por_face_flag == 1};
     run_box(clip(Box{is_l - 1, ie_l, js_l, je_l}, n1, n2), 1, stream,
             [=] __device__(int i, int j, int) {
@@ -471,6 +479,7 @@ extern "C" void launch_zonal_flux_thickness_kernel(
     int is_l, int ie_l, int js_l, int je_l, double dt, int vol_CFL_flag, int marginal_flag,
     int has_visc_rem_flag, int use_por_face_flag, int, int, int, int, int, int, void* stream)
 {
+    flush_deferred();
     const FaceFlags fl{vol_CFL_flag == 1, has_visc_rem_flag == 1, use_por_face_flag == 1};
     run_box(clip(Box{is_l - 1, ie_l, js_l, je_l}, n1, n2), n3, stream,
             [=] __device__(int i, int j, int k) {
@@ -492,6 +501,7 @@ extern "C" void launch_u_cor_kernel(double* u_cor, double* u, double* du, double
                                     int je_l, int use_visc_rem_flag, int, int, int, int, int,
                                     int, void* stream)
 {
+    flush_deferred();
     run_box(clip(Box{is_l - 1, ie_l, js_l, je_l}, n1, n2), n3, stream,
             [=] __device__(int i, int j, int k) {
                 const size_t p = at3(i, j, k, n1, n2);

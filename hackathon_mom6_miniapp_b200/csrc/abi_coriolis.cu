@@ -100,6 +100,7 @@ extern "C" void launch_phase1_kernel(double* dvdx, double* dudy, double* hArea_u
                                      int is_l, int ie_l, int js_l, int je_l, int, int, int, int,
                                      int, int, void* stream)
 {
+    flush_deferred();
     run_phase1(Phase1{dvdx, dudy, hArea_u, hArea_v, KE, u, v, h, dyCv, dxCu, dyCu, dxCv, areaT,
                       n1, n2, is_l, ie_l, js_l, je_l, true, true},
                n3, stream);
@@ -112,6 +113,7 @@ extern "C" void launch_phase1_kernel_smem(double* dvdx, double* dudy, double* hA
                                           int is_l, int ie_l, int js_l, int je_l, int, int, int,
                                           int, int, int, void* stream)
 {
+    flush_deferred();
     run_phase1(Phase1{dvdx, dudy, hArea_u, hArea_v, KE, u, v, h, dyCv, dxCu, dyCu, dxCv, areaT,
                       n1, n2, is_l, ie_l, js_l, je_l, true, true},
                n3, stream);
@@ -123,6 +125,7 @@ extern "C" void launch_phase1a_circ_kernel(double* dvdx, double* dudy, double* h
                                            int n2, int n3, int is_l, int ie_l, int js_l,
                                            int je_l, int, int, int, int, int, int, void* stream)
 {
+    flush_deferred();
     run_phase1(Phase1{dvdx, dudy, hArea_u, hArea_v, nullptr, u, v, h, dyCv, dxCu, nullptr,
                       nullptr, areaT, n1, n2, is_l, ie_l, js_l, je_l, true, false},
                n3, stream);
@@ -133,6 +136,7 @@ extern "C" void launch_phase1b_ke_kernel(double* KE, double* u, double* v, doubl
                                          int is_l, int ie_l, int js_l, int je_l, int, int, int,
                                          int, int, int, void* stream)
 {
+    flush_deferred();
     run_phase1(Phase1{nullptr, nullptr, nullptr, nullptr, KE, u, v, nullptr, nullptr, nullptr,
                       dyCu, dxCv, areaT, n1, n2, is_l, ie_l, js_l, je_l, false, true},
                n3, stream);
@@ -147,6 +151,7 @@ extern "C" void launch_vorticity_pv_kernel(double* rel_vort, double* abs_vort, d
                                            int ie_l, int js_l, int je_l, int, int, int, int,
                                            int, int, void* stream)
 {
+    flush_deferred();
     run_box(clip(Box{is_l - 1, ie_l, js_l - 1, je_l}, n1, n2), n3, stream,
             [=] __device__(int i, int j, int k) {
                 const size_t p = at3(i, j, k, n1, n2), p2 = at2(i, j, n1);
@@ -168,6 +173,7 @@ extern "C" void launch_arakawa_hsu90_coef_kernel(double* a, double* b, double* c
                                                  int ie_l, int js_l, int je_l, int, int, int,
                                                  int, int, int, void* stream)
 {
+    flush_deferred();
     run_box(clip(Box{is_l - 1, ie_l, js_l, je_l}, n1, n2), n3, stream,
             [=] __device__(int i, int j, int k) {
                 const size_t p = at3(i, j, k, n1, n2);
@@ -189,6 +195,7 @@ extern "C" void launch_arakawa_lamb81_coef_kernel(double* a, double* b, double* 
                                                   int ie_l, int js_l, int je_l, int, int, int,
                                                   int, int, int, void* stream)
 {
+    flush_deferred();
     run_box(clip(Box{is_l, ie_l, js_l, je_l}, n1, n2), n3, stream,
             [=] __device__(int i, int j, int k) {
                 const double q00 = q[at3(i, j, k, n1, n2)];
@@ -210,6 +217,7 @@ extern "C" void launch_coriolis_sadourny_kernel(double* CAu, double* CAv, double
                                                 int ie_l, int js_l, int je_l, int, int, int, int,
                                                 int, int, void* stream)
 {
+    flush_deferred();
     run_box(Box{is_l, ie_l, js_l, je_l}, n3, stream, [=] __device__(int i, int j, int k) {
         const size_t p = at3(i, j, k, n1, n2), p2 = at2(i, j, n1);
         if (i <= ie_l - 1) {
@@ -236,6 +244,7 @@ extern "C" void launch_coriolis_arakawa_kernel(double* CAu, double* CAv, double*
                                                int je_l, int, int, int, int, int, int,
                                                void* stream)
 {
+    flush_deferred();
     run_box(Box{is_l, ie_l, js_l, je_l}, n3, stream, [=] __device__(int i, int j, int k) {
         const size_t p = at3(i, j, k, n1, n2), p2 = at2(i, j, n1);
         if (i <= ie_l - 1) {
@@ -263,6 +272,7 @@ extern "C" void launch_coriolis_fused_sadourny_kernel(
     double* CoriolisBu, double* mask2dBu, double* IdxCu, double* IdyCv, int n1, int n2, int n3,
     int is_l, int ie_l, int js_l, int je_l, int, int, int, int, int, int, void* stream)
 {
+    flush_deferred();
     run_box(Box{is_l, ie_l, js_l, je_l}, n3, stream, [=] __device__(int i, int j, int k) {
         const bool do_u = i <= ie_l - 1, do_v = j <= je_l - 1;
         if (!do_u && !do_v) return;

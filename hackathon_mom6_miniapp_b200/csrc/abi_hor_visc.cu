@@ -17,6 +17,7 @@ extern "C" void launch_stress_kernel(double* str_xx, double* str_xy, double* u, 
                                      int n1, int n2, int n3, int is_l, int ie_l, int js_l,
                                      int je_l, int, int, int, int, int, int, void* stream)
 {
+    flush_deferred();
     // str_xx on [is-1, ie+1] x [js-1, je+1], str_xy on [is-1, ie] x [js-1, je]
     const int Isq = is_l - 1, Ieq = ie_l, Jsq = js_l - 1, Jeq = je_l;
     run_box(clip(Box{Isq, Ieq + 1, Jsq, Jeq + 1}, n1, n2), n3, stream,
@@ -53,6 +54,7 @@ extern "C" void launch_divergence_kernel(double* diffu, double* diffv, double* s
                                          int ie_l, int js_l, int je_l, int, int, int, int, int,
                                          int, void* stream)
 {
+    flush_deferred();
     // diffu on [is-1, ie] x [js, je], diffv on [is, ie] x [js-1, je]
     run_box(clip(Box{is_l - 1, ie_l, js_l - 1, je_l}, n1, n2), n3, stream,
             [=] __device__(int i, int j, int k) {

@@ -196,6 +196,7 @@ extern "C" void launch_vert_visc_cra_u_kernel(double* u, double* h, double* mask
                                               int ie_l, int js_l, int je_l, double*, double*,
                                               int, int, int, int, void* stream)
 {
+    flush_deferred();
     if (nz > 1024) return;
     VvArgs A{u, visc_rem_u, taux_bot, h, mask2dCu, taux, Kv, Kv_ml, Kv_extra_bbl, Hmix,
              dt, dt_Rho0, h_neglect, I_Hbbl, n1, n2, nz,
@@ -213,6 +214,7 @@ extern "C" void launch_vert_visc_cra_v_kernel(double* v, double* h, double* mask
                                               int ie_l, int js_l, int je_l, double*, double*,
                                               int, int, int, int, void* stream)
 {
+    flush_deferred();
     if (nz > 1024) return;
     VvArgs A{v, visc_rem_v, tauy_bot, h, mask2dCv, tauy, Kv, Kv_ml, Kv_extra_bbl, Hmix,
              dt, dt_Rho0, h_neglect, I_Hbbl, n1, n2, nz,

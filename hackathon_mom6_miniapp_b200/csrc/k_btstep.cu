@@ -1345,6 +1345,47 @@ cudaError_t launch_halo_fill_f(const Dims& D, float* f, int nz, int kind, cudaSt
     return launch_halo_fill_t<float>(D, f, nz, kind, s);
 }
 
+// The barotropic loop on the static scratch (no allocation) with the
+// caller's metric arrays and parameters: the allocation-free entry point and
+// the deferred barotropic calls of the reference ABI.  P's wait limit and
+// stall aid come from mom6b_btstep_noalloc_set_wait.  MOM6B_NOALLOC_* codes.
+int btstep_static(const double* eta_in, const double* ubt_in, const double* vbt_in,
+                  double* u_av, double* v_av, double* eta_av, const Metrics& M, const Dims& D,
+                  BTParams P, cudaStream_t s)
+{
+    if ((long long)D.n1 * (long long)D.n2 > kNoAllocMaxPoints)
+        return MOM6B_NOALLOC_ERR_TOO_LARGE;
+    int nsm = 0;
+    if (bt_blocks(&nsm) != cudaSuccess) return MOM6B_NOALLOC_ERR_CUDA;
+    BTTiles T;
+    if (!tiles_for(D, nsm, T)) return MOM6B_NOALLOC_ERR_TOO_LARGE;
+    double* base = nullptr;
+    if (noalloc_scratch(&base) != cudaSuccess) return MOM6B_NOALLOC_ERR_CUDA;
+    // barrier words and status must start at zero; the field buffers are
+    // fully written by the kernel's initial copy
+    if (cudaMemsetAsync(base, 0, kNoAllocHeader * sizeof(double), s) != cudaSuccess)
+        return MOM6B_NOALLOC_ERR_CUDA;
+    const size_t np = (size_t)D.n1 * (size_t)D.n2;
+    double* f = base + kNoAllocHeader;
+    BTWork W{};
+    W.eta = f; W.ubt = f + np; W.vbt = f + 2 * np;
+    W.eta_pred = f + 3 * np; W.ubt_prev = f + 4 * np; W.vbt_prev = f + 5 * np;
+    W.uhbt = nullptr; W.vhbt = nullptr; W.PFu = nullptr; W.PFv = nullptr;
+    W.ubt_av = nullptr; W.vbt_av = nullptr;
+    W.bar_count = (unsigned int*)base;
+    W.bar_gen = (unsigned int*)base + 4;
+    W.status = (int*)base + 8;
+    W.tile_flag = (unsigned int*)base + 16;   // kBtMaxTiles words, inside the header
+    static_assert(64 + kBtMaxTiles * 4 <= kNoAllocHeader * 8, "noalloc header too small");
+    P.spin_budget = g_noalloc_wait > 0 ? g_noalloc_wait : kBtDefaultWait;
+    P.stall_test = g_noalloc_stall;
+    UniMetrics U{};
+    if (launch_btstep_tiled(D, M, U, W, P, T, eta_in, ubt_in, vbt_in, u_av, v_av, eta_av, s) !=
+        cudaSuccess)
+        return MOM6B_NOALLOC_ERR_CUDA;
+    return MOM6B_NOALLOC_OK;
+}
+
 } // namespace mom6b
 
 // See mom6b.h.  Every call shares g_noalloc_scratch: calls that overlap on
@@ -1369,57 +1410,26 @@ extern "C" int mom6b_btstep_noalloc(
     if (n1 < 4 || n2 < 4 || nstep < 1 || is < 2 || js < 2 || ie > n1 - 1 || je > n2 - 1 ||
         ie - is < 2 || je - js < 2)
         return MOM6B_NOALLOC_ERR_ARG;
-    if ((long long)n1 * (long long)n2 > kNoAllocMaxPoints)
-        return MOM6B_NOALLOC_ERR_TOO_LARGE;
     Dims D{};
     D.n1 = n1; D.n2 = n2; D.nk = 1;
     D.is = is; D.ie = ie; D.js = js; D.je = je;
     D.isd = 1; D.ied = n1; D.jsd = 1; D.jed = n2;
     D.plane = (long long)n1 * (long long)n2;
-    int nsm = 0;
-    if (bt_blocks(&nsm) != cudaSuccess) return MOM6B_NOALLOC_ERR_CUDA;
-    BTTiles T;
-    if (!tiles_for(D, nsm, T)) return MOM6B_NOALLOC_ERR_TOO_LARGE;
-    double* base = nullptr;
-    if (noalloc_scratch(&base) != cudaSuccess) return MOM6B_NOALLOC_ERR_CUDA;
-    cudaStream_t s = (cudaStream_t)stream;
-    // barrier words and status must start at zero; the field buffers are
-    // fully written by the kernel's initial copy
-    if (cudaMemsetAsync(base, 0, kNoAllocHeader * sizeof(double), s) != cudaSuccess)
-        return MOM6B_NOALLOC_ERR_CUDA;
-    const size_t np = (size_t)n1 * (size_t)n2;
-    double* f = base + kNoAllocHeader;
-    BTWork W{};
-    W.eta = f; W.ubt = f + np; W.vbt = f + 2 * np;
-    W.eta_pred = f + 3 * np; W.ubt_prev = f + 4 * np; W.vbt_prev = f + 5 * np;
-    W.uhbt = nullptr; W.vhbt = nullptr; W.PFu = nullptr; W.PFv = nullptr;
-    W.ubt_av = nullptr; W.vbt_av = nullptr;
-    W.bar_count = (unsigned int*)base;
-    W.bar_gen = (unsigned int*)base + 4;
-    W.status = (int*)base + 8;
-    W.tile_flag = (unsigned int*)base + 16;   // kBtMaxTiles words, inside the header
-    static_assert(64 + kBtMaxTiles * 4 <= kNoAllocHeader * 8, "noalloc header too small");
     Metrics M{};
     M.Datu = Datu; M.Datv = Datv; M.gtot_E = gtot_E; M.gtot_W = gtot_W;
     M.gtot_N = gtot_N; M.gtot_S = gtot_S; M.f_4_u = f_4_u; M.f_4_v = f_4_v;
     M.bt_rem_u = bt_rem_u; M.bt_rem_v = bt_rem_v; M.IareaT = IareaT;
     M.IdxCu = IdxCu; M.IdyCv = IdyCv;
-    UniMetrics U{};
     BTParams P{};
     P.dtbt = dtbt; P.dgeo_de = dgeo_de;
     P.trans_wt1 = 1.0 + bebt; P.trans_wt2 = -bebt;
     P.inv_nstep = 1.0 / (double)nstep;
     P.nstep = nstep; P.first_direction = first_direction;
     P.extended = extended_ranges ? 1 : 0;
-    P.spin_budget = g_noalloc_wait > 0 ? g_noalloc_wait : kBtDefaultWait;
-    P.stall_test = g_noalloc_stall;
-    if (launch_btstep_tiled(D, M, U, W, P, T, eta_in, ubt_in, vbt_in, u_av, v_av, eta_av,
-                            s) != cudaSuccess)
-        return MOM6B_NOALLOC_ERR_CUDA;
-    return MOM6B_NOALLOC_OK;
+    return btstep_static(eta_in, ubt_in, vbt_in, u_av, v_av, eta_av, M, D, P,
+                         (cudaStream_t)stream);
 }
 
-// See mom6b.h: the status word of the last call on the current device.
 extern "C" int mom6b_btstep_noalloc_status(void* stream)
 {
     using namespace mom6b;

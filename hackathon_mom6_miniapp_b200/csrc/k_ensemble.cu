@@ -160,7 +160,7 @@ k_ens_vertvisc(const EnsDomain* __restrict__ doms, const int* __restrict__ start
     const int local = b - __ldg(start + d);
     const int gx = (E.D.ie - E.D.is + 2 + NB - 1) / NB;
     const bool corr = half != 0;
-    vertvisc_column<KMAX, CH, float, double>(E.D, E.M, corr ? E.u : E.up, corr ? E.v : E.vp,
+    vertvisc_column<KMAX, CH, float, double, false, false, true>(E.D, E.M, corr ? E.u : E.up, corr ? E.v : E.vp,
                                              corr ? E.hB : E.h0, corr ? 0.5 * E.dt : E.dt,
                                              E.VV, E.taux_bot, E.tauy_bot, local % gx,
                                              local / gx);

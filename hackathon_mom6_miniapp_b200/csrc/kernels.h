@@ -136,6 +136,11 @@ cudaError_t launch_btstep_tavg(const Dims& D, const Metrics& M, const UniMetrics
                                const double* ubt_in, const double* vbt_in, double* u_av,
                                double* v_av, double* eta_av, cudaStream_t s);
 cudaError_t launch_halo_fill(const Dims& D, double* f, int nz, int kind, cudaStream_t s);
+// The barotropic loop on the library's static scratch (no allocation), with
+// the caller's metric arrays in M and parameters in P; MOM6B_NOALLOC_* codes.
+int btstep_static(const double* eta_in, const double* ubt_in, const double* vbt_in,
+                  double* u_av, double* v_av, double* eta_av, const Metrics& M, const Dims& D,
+                  BTParams P, cudaStream_t s);
 
 // Mixed-precision form (k_mixed.cu): FP32 state and stencils, FP64 column
 // sums, Newton scalars, thickness update and tridiagonal elimination.

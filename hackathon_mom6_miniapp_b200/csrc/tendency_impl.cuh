@@ -436,8 +436,18 @@ cudaError_t launch_tendency_t(const Dims& D, const Metrics& M, const UniMetrics&
     dim3 grid((nx + kTendTX - 1) / kTendTX, (ny + TY - 1) / TY, nchunks);
     if ((dfu == nullptr) != (dfv == nullptr)) return cudaErrorInvalidValue;
     if constexpr (FAST) {
+        // only the plain Sadourny kernel exists in the fast form; the other
+        // kernels are not instantiated here, so the exact translation unit's
+        // instances (same template arguments) are the only ones linked
         if (ext_visc || dfu || scheme != 1) return cudaErrorInvalidValue;
-    }
+        if (U.valid)
+            k_tendency<kTendTX, TY, true, R, 4, false, 1, false, true><<<grid, block, 0, s>>>(
+                D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, KCh);
+        else
+            k_tendency<kTendTX, TY, false, R, 3, false, 1, false, true><<<grid, block, 0, s>>>(
+                D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, KCh);
+        return cudaGetLastError();
+    } else {
     if (ext_visc) {
         if (!dfu || scheme < 1 || scheme > 3) return cudaErrorInvalidValue;
         if (scheme == 1)
@@ -473,12 +483,13 @@ cudaError_t launch_tendency_t(const Dims& D, const Metrics& M, const UniMetrics&
     // uniform-metric form on B200 (FP64 tendency 2.01 ms per step against 2.13
     // at 3 and 2.62 uncapped); the 2-D metric form keeps 3 (80 registers).
     if (U.valid)
-        k_tendency<kTendTX, TY, true, R, 4, false, 1, false, FAST><<<grid, block, 0, s>>>(
+        k_tendency<kTendTX, TY, true, R, 4><<<grid, block, 0, s>>>(
             D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, KCh);
     else
-        k_tendency<kTendTX, TY, false, R, 3, false, 1, false, FAST><<<grid, block, 0, s>>>(
+        k_tendency<kTendTX, TY, false, R, 3><<<grid, block, 0, s>>>(
             D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, KCh);
     return cudaGetLastError();
+    }
 }
 
 } // namespace mom6b

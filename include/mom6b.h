@@ -320,6 +320,21 @@ int mom6b_btstep_noalloc(const double *eta_in, const double *ubt_in,
 int mom6b_btstep_noalloc_status(void *stream);
 int mom6b_btstep_noalloc_set_wait(long long cycles, int stall_test);
 
+/* ---- barotropic deferral of the reference ABI -----------------------------
+ * No counterpart in the reference.  The launch_bt_* entry points of
+ * mom6_cuda_c.h defer the substep kernels of one btstep_cuda_c call
+ * (launch_bt_init_kernel runs and opens a record; the substep calls that
+ * continue the wrapper's fixed sequence are recorded; launch_bt_copy_output_kernel
+ * runs the whole loop as one persistent launch on the library's static
+ * scratch, bit-identical to the substep kernels).  Any call that breaks the
+ * sequence, any other launch_* entry point and any cuda_*_c helper first
+ * replay the record call by call.  The substep kernels' own arrays of the
+ * control structure are not written by a deferred loop (the wrapper reads
+ * only the copy's outputs).  on = 0 runs every launch_bt_* call as it comes
+ * (on by default).  The setting is process-wide; a record belongs to the
+ * host thread that opened it. */
+int mom6b_abi_set_deferral(int on);
+
 /* Device address of one of the model's 2-D metric arrays by name ("IareaT",
  * "IdxCu", "IdyCv", "Datu", "Datv", "gtot_E", "gtot_W", "gtot_N", "gtot_S",
  * "f_4_u", "f_4_v", "bt_rem_u", "bt_rem_v"). */

@@ -26,7 +26,10 @@ GRIDS = [Grid(38, 32, 8), Grid(71, 45, 5)]
 def _libs():
     if not os.path.exists(REF):
         pytest.skip("oracle/_ref not built (make -C oracle ref)")
-    from hackathon_mom6_miniapp_b200._lib import library_path
+    from hackathon_mom6_miniapp_b200._lib import abi_set_deferral, library_path
+    # one kernel at a time: the barotropic deferral off, so every launch_bt_*
+    # call runs as it comes
+    abi_set_deferral(False)
     ours = ctypes.CDLL(library_path())
     ref = ctypes.CDLL(REF)
     return ours, ref

@@ -28,10 +28,15 @@ def _need(path):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("defer", [True, False])
 @pytest.mark.parametrize("shape", [(36, 30, 8, 20), (70, 50, 12, 30)])
-def test_abi_step_matches_reference_kernels(shape):
+def test_abi_step_matches_reference_kernels(shape, defer):
+    """Whole steps through the mirror, bit for bit against the reference's
+    kernels: with the barotropic deferral (each btstep_cuda_c as one
+    persistent loop) and with every launch_bt_* call run as it comes."""
     _need(REF_NOFMA)
-    from hackathon_mom6_miniapp_b200 import CudaCDriver
+    from hackathon_mom6_miniapp_b200 import CudaCDriver, abi_set_deferral
+    abi_set_deferral(defer)
     ni, nj, nk, bt = shape
     ours = CudaCDriver(ni, nj, nk, bt, dt=300.0)
     ref = CudaCDriver(ni, nj, nk, bt, dt=300.0, kernel_lib=REF_NOFMA)
@@ -40,6 +45,7 @@ def test_abi_step_matches_reference_kernels(shape):
         ref.step(1)
         bad = [f for f in FIELDS if not np.array_equal(ours.get(f), ref.get(f))]
         assert not bad, f"step {step + 1}: fields differ: {bad}"
+    abi_set_deferral(True)
 
 
 @pytest.mark.gpu

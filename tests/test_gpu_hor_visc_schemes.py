@@ -37,9 +37,10 @@ CASES = {
 FIELDS = ["u", "v", "h", "eta", "ubt_av", "vbt_av", "up", "vp"]
 
 
-def _pair(opts, cfg, seed=4, bc_fill=None, nsteps=3):
+def _pair(opts, cfg, seed=4, bc_fill=None, nsteps=3, general_metrics=False):
     from hackathon_mom6_miniapp_b200 import Model
-    m = Model(*SHAPE, 30, INIT_CFG, seed=seed, bc_fill=bc_fill, **cfg, exact=True)
+    m = Model(*SHAPE, 30, INIT_CFG, seed=seed, bc_fill=bc_fill, **cfg, exact=True,
+              general_metrics=general_metrics)
     o = Oracle(*SHAPE, 30, INIT_CFG, seed=seed, bc_fill=bc_fill, **cfg)
     m.set_hor_visc(**opts)
     o.set_hor_visc(**opts)
@@ -61,12 +62,11 @@ def test_scheme_steps_match_the_oracle(case):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("case", ["modified_leith_no_slip", "better_bound"])
-def test_scheme_steps_with_metric_arrays(case, monkeypatch):
+def test_scheme_steps_with_metric_arrays(case):
     """The kernel's 2-D metric form (the uniform grid read through its arrays)
     gives the same steps."""
-    monkeypatch.setenv("MOM6B_GENERAL_METRICS", "1")
     opts, cfg = CASES[case]
-    m, o = _pair(opts, cfg)
+    m, o = _pair(opts, cfg, general_metrics=True)
     for f in FIELDS:
         assert np.array_equal(m.get(f), o.get(f)), f
 
