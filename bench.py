@@ -4,7 +4,10 @@
 
 Workload: the seeded beta-plane state at 720x720x75 (CFG init,
 Philox4x32-10 normals, dt = 600 s, Kh = 1e3, halo fill on), ni = nj = 720,
-nk = 75, bt_nsteps = 50, plain FP64.  One "step" is one split RK2 iteration
+nk = 75, bt_nsteps = 50, plain FP64 in its fast form (FMA contraction,
+column sums in another order; within 1e-12 relative L2 of the serial driver,
+tested).  The "exact_fp64" object times the exact form (bit-identical to the
+serial driver) on the same protocol.  One "step" is one split RK2 iteration
 of rk2_serial_driver.F90:218-399 on the whole domain.  The state (~6 GB)
 stays resident in HBM and is far larger than L2, so no L2 flush is needed
 between steps.  Under torchrun each rank advances its own replica of the
@@ -647,6 +650,18 @@ def run_ours(args, world, rank, local, dist):
             abi_dropin["speedup_vs_reference_cuda_c"] = abi_dropin["value"] / ref_cudac["value"]
             ref_cudac["fused_speedup"] = value / world / ref_cudac["value"]
 
+    # the exact form (bit-identical to the serial driver) on the same protocol
+    exact_line = None
+    if not args.no_exact:
+        mx = Model(NI, NJ, NK, BT, INIT_CFG, seed=rank, dt=600.0, device=local,
+                   use_graph=not args.no_graph, exact=True)
+        t_ex = _time_model(mx, args, local, dist)
+        mx.close()
+        exact_line = {"value": world * args.steps / (t_ex / 1000.0), "unit": "steps/s",
+                      "ms_per_step": t_ex / args.steps,
+                      "what": "exact FP64 kernels (no FMA, serial column sums): bit-identical "
+                              "to the serial driver"}
+
     mixed = None if args.no_mixed else run_mixed(args, world, rank, local, dist,
                                                    ms / args.steps)
     ensemble = None if args.no_ensemble else run_ensemble(args, world, rank, local, dist)
@@ -686,6 +701,7 @@ def run_ours(args, world, rank, local, dist):
                 "e2e_resident": {"value": e2e_res, "unit": "steps/s",
                                  "h2d_bytes_per_step": bytes_h2d / args.steps,
                                  "d2h_bytes_per_step": bytes_d2h / args.steps},
+                "exact_fp64": exact_line,
                 "reference_cuda_c": ref_cudac,
                 "abi_dropin": abi_dropin,
                 "mixed": mixed,
@@ -767,6 +783,8 @@ def main():
     ap.add_argument("--no-cfg2", action="store_true",
                     help="skip the mixed form's error at 1440x1080x75 after 100 steps")
     ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--no-exact", action="store_true",
+                    help="skip the exact FP64 form's timing")
     ap.add_argument("--no-cudac", action="store_true",
                     help="skip the reference CUDA C backend and drop-in ABI timings")
     ap.add_argument("--profile-mixed", action="store_true",
