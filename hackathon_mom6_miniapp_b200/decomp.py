@@ -14,8 +14,12 @@ halo], mom6_mpi_domain.F90:157-172).
 
 `HaloExchange.exchange` restates halo_exchange_3d / halo_exchange_2d
 (mom6_mpi_halo.F90:107-431): every send strip is packed before any receive
-is unpacked; east/west strips span the rows [jsd + hw, jed - hw], north/south
-strips the full data width (so they carry the sender's east/west halo columns
+is unpacked; east/west strips span the rows [jsd + hw, jed - hw] (and the
+halo rows on a side without a north / south neighbour: there the reference's
+strips stop at the compute rows, which leaves the corner between a cut and a
+wall holding its initial values; the strips here carry the neighbour's
+wall-face values there, so that the decomposed step is the single-domain
+one), north/south strips the full data width (so they carry the sender's east/west halo columns
 as they were before the exchange); received strips are unpacked in the order
 E, W, N, S, NE, NW, SE, SW, the corner blocks overwriting the corners of the
 north/south strips where a diagonal neighbour exists; nothing is written on a
@@ -98,7 +102,12 @@ class HaloExchange:
 
     def _regions(self, n1, n2):
         hw = self.d.halo
-        rows_in = slice(hw, n2 - hw)
+        # east/west strips: the compute rows, and the halo rows of a wall side
+        # (no south / north neighbour), whose wall-face values the neighbour
+        # computes as the single domain does (vert_visc updates v on the
+        # south wall face J = js-1, mom6_vert_visc_serial.F90:394-506)
+        rows_in = slice(0 if self.nbr["S"] is None else hw,
+                        n2 if self.nbr["N"] is None else n2 - hw)
         e_s, w_s = slice(n1 - 2 * hw, n1 - hw), slice(hw, 2 * hw)
         n_s, s_s = slice(n2 - 2 * hw, n2 - hw), slice(hw, 2 * hw)
         e_r, w_r = slice(n1 - hw, n1), slice(0, hw)

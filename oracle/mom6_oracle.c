@@ -121,6 +121,11 @@ struct oracle_model {
         *bt_f_4_v, *bt_rem_u, *bt_rem_v, *bt_ubt_av, *bt_vbt_av;
     int first_direction;
     int bt_extended; /* 1: uhbt/vhbt and averages on the extended ranges */
+    /* decomposed runs: global sizes, offsets, the cut sides (0 / 1) and the
+     * halo exchange */
+    int gni, gnj, ioff, joff, cw, ce, cs, cn;
+    oracle_exchange_fn xfn;
+    void *xctx;
 };
 
 /* ------------------------------------------------------------------------ */
@@ -230,7 +235,9 @@ static void init_grid(oracle_model *m) {
     m->dx = dx_m;
     double f0 = 2.0 * OMEGA * sin(c->lat_deg * PI_REF / 180.0);
     double beta = 2.0 * OMEGA * cos(c->lat_deg * PI_REF / 180.0) / EARTH_RADIUS;
-    double Ly = (double)(m->je - m->js + 1) * dx_m;
+    const int gie = m->gni - 1, gje = m->gnj - 1;   /* the global ie, je */
+    double Ly = (double)(gje - m->js + 1) * dx_m;
+    (void)gie;
     for (int j = m->jsd; j <= m->jed; ++j)
         for (int i = m->isd; i <= m->ied; ++i) {
             A2(m->areaT, i, j) = dx_m * dx_m;
@@ -263,9 +270,9 @@ static void init_grid(oracle_model *m) {
             A2(m->bathyT, i, j) = 4000.0;
             if (c->init_mode == OR_INIT_REF) {
                 A2(m->CoriolisBu, i, j) =
-                    f0 + beta * ((double)(j - 1 - m->nj / 2) - 0.5) * dx_m;
+                    f0 + beta * ((double)(j + m->joff - 1 - m->gnj / 2) - 0.5) * dx_m;
             } else {
-                double yq = (double)(j - m->js + 1) * dx_m;
+                double yq = (double)(j + m->joff - m->js + 1) * dx_m;
                 A2(m->CoriolisBu, i, j) = 1.0e-4 + 2.0e-11 * (yq - 0.5 * Ly);
             }
         }
@@ -396,9 +403,12 @@ static void alloc_all(oracle_model *m) {
 static void init_state(oracle_model *m) {
     const oracle_config *c = &m->cfg;
     int nk = m->nk;
+    /* the global point of each local one (init_ocean_grid_mpi,
+     * mom6_mpi_domain.F90:144-258: positions by global index) */
+    const int io = m->ioff, jo = m->joff, gni = m->gni, gnj = m->gnj;
     for (int j = m->jsd; j <= m->jed; ++j)
         for (int i = m->isd; i <= m->ied; ++i) {
-            A2(m->taux, i, j) = 0.1 * sin((double)(j - 1) / (double)m->nj * 3.14159);
+            A2(m->taux, i, j) = 0.1 * sin((double)(j + jo - 1) / (double)gnj * 3.14159);
             A2(m->tauy, i, j) = 0.0;
         }
     for (int j = m->jsd; j <= m->jed; ++j)
@@ -413,32 +423,33 @@ static void init_state(oracle_model *m) {
                 for (int i = m->isd; i <= m->ied; ++i) {
                     A3(m->h0, i, j, k) =
                         total_depth / (double)nk +
-                        10.0 * sin((double)(i - 1) / (double)m->ni * 3.14159) *
-                            cos((double)(j - 1) / (double)m->nj * 3.14159) *
+                        10.0 * sin((double)(i + io - 1) / (double)gni * 3.14159) *
+                            cos((double)(j + jo - 1) / (double)gnj * 3.14159) *
                             exp(-(double)k / 20.0);
                     A3(m->h, i, j, k) = A3(m->h0, i, j, k);
                     A3(m->u, i, j, k) =
-                        0.1 * sin((double)(j - 1) / (double)m->nj * 3.14159 * 2.0) *
+                        0.1 * sin((double)(j + jo - 1) / (double)gnj * 3.14159 * 2.0) *
                         exp(-(double)k / 30.0);
                     A3(m->v, i, j, k) =
-                        0.1 * cos((double)(i - 1) / (double)m->ni * 3.14159 * 2.0) *
+                        0.1 * cos((double)(i + io - 1) / (double)gni * 3.14159 * 2.0) *
                         exp(-(double)k / 30.0);
                 }
         for (int j = m->jsd; j <= m->jed; ++j)
             for (int i = m->isd; i <= m->ied; ++i) {
                 A2(m->eta, i, j) =
-                    0.5 * sin((double)(i - 1) / (double)m->ni * 3.14159 * 2.0) *
-                    cos((double)(j - 1) / (double)m->nj * 3.14159 * 2.0);
-                A2(m->ubt, i, j) = 0.05 * sin((double)(j - 1) / (double)m->nj * 3.14159);
-                A2(m->vbt, i, j) = 0.05 * cos((double)(i - 1) / (double)m->ni * 3.14159);
+                    0.5 * sin((double)(i + io - 1) / (double)gni * 3.14159 * 2.0) *
+                    cos((double)(j + jo - 1) / (double)gnj * 3.14159 * 2.0);
+                A2(m->ubt, i, j) = 0.05 * sin((double)(j + jo - 1) / (double)gnj * 3.14159);
+                A2(m->vbt, i, j) = 0.05 * cos((double)(i + io - 1) / (double)gni * 3.14159);
             }
     } else {
         double hbar = 4000.0 / (double)nk;
         for (int k = 1; k <= nk; ++k)
             for (int j = m->jsd; j <= m->jed; ++j)
                 for (int i = m->isd; i <= m->ied; ++i) {
-                    uint64_t idx = ((uint64_t)(k - 1) * (uint64_t)N2 + (uint64_t)(j - 1)) *
-                                       (uint64_t)N1 + (uint64_t)(i - 1);
+                    uint64_t idx = ((uint64_t)(k - 1) * (uint64_t)(gnj + 2) +
+                                    (uint64_t)(j + jo - 1)) * (uint64_t)(gni + 2) +
+                                   (uint64_t)(i + io - 1);
                     double hv = hbar * (1.0 + 0.01 * oracle_normal(c->seed, 1u, idx));
                     if (hv < 0.01 * hbar) hv = 0.01 * hbar;
                     A3(m->h0, i, j, k) = hv;
@@ -447,13 +458,13 @@ static void init_state(oracle_model *m) {
                     A3(m->v, i, j, k) = 0.05 * oracle_normal(c->seed, 3u, idx);
                 }
         double dx = m->dx;
-        double Lx = (double)(m->ie - m->is + 1) * dx;
-        double Ly = (double)(m->je - m->js + 1) * dx;
+        double Lx = (double)((gni - 1) - m->is + 1) * dx;
+        double Ly = (double)((gnj - 1) - m->js + 1) * dx;
         double R = 200.0e3;
         for (int j = m->jsd; j <= m->jed; ++j)
             for (int i = m->isd; i <= m->ied; ++i) {
-                double x = ((double)(i - m->is) + 0.5) * dx - 0.5 * Lx;
-                double y = ((double)(j - m->js) + 0.5) * dx - 0.5 * Ly;
+                double x = ((double)(i + io - m->is) + 0.5) * dx - 0.5 * Lx;
+                double y = ((double)(j + jo - m->js) + 0.5) * dx - 0.5 * Ly;
                 A2(m->eta, i, j) = 0.1 * exp(-(x * x + y * y) / (R * R));
                 A2(m->ubt, i, j) = 0.0;
                 A2(m->vbt, i, j) = 0.0;
@@ -463,9 +474,17 @@ static void init_state(oracle_model *m) {
 
 oracle_model *oracle_create(const oracle_config *c) {
     if (c->ni < 8 || c->nj < 8 || c->nk < 2 || c->bt_nsteps < 1) return NULL;
+    const int gni = c->ni_global > 0 ? c->ni_global : c->ni;
+    const int gnj = c->nj_global > 0 ? c->nj_global : c->nj;
+    if (c->i_offset < 0 || c->j_offset < 0 || c->i_offset + (c->ni - 4) > gni - 4 ||
+        c->j_offset + (c->nj - 4) > gnj - 4 || (c->cuts & ~15) || (c->cuts && c->bc_fill))
+        return NULL;
     oracle_model *m = (oracle_model *)calloc(1, sizeof(oracle_model));
     m->cfg = *c;
     m->ni = c->ni; m->nj = c->nj; m->nk = c->nk;
+    m->gni = gni; m->gnj = gnj; m->ioff = c->i_offset; m->joff = c->j_offset;
+    m->cw = (c->cuts & OR_CUT_W) != 0; m->ce = (c->cuts & OR_CUT_E) != 0;
+    m->cs = (c->cuts & OR_CUT_S) != 0; m->cn = (c->cuts & OR_CUT_N) != 0;
     /* mom6_types.F90:145-148 */
     m->isd = 1; m->ied = c->ni + 2; m->jsd = 1; m->jed = c->nj + 2;
     m->is = m->isd + 3; m->ie = m->ied - 3; m->js = m->jsd + 3; m->je = m->jed - 3;
@@ -824,11 +843,13 @@ static void hor_visc_rows(oracle_model *m, const double *u, const double *v,
                 A2(hrat, i, j) = MIN(1.0, h_min / (A3(h, i, j, k) + h_neglect));
             }
     }
-    /* STEP 8: Kh at h-points, str_xx (:744-816) */
+    /* STEP 8: Kh at h-points, str_xx (:744-816).  str_xx(ie+1, :) and
+     * str_xx(:, je+1) read the shared Kh where this step does not write it;
+     * at an east / north cut those cells are interior and get their Kh. */
     if (m->hv_lap) {
         OMP_FOR
-        for (int j = js; j <= je; ++j)
-            for (int i = is; i <= ie; ++i) {
+        for (int j = js; j <= je + m->cn; ++j)
+            for (int i = is; i <= ie + m->ce; ++i) {
                 double K = A2(m->hv_Kh_bg_xx, i, j);
                 if (m->hv_smag_kh) K = MAX(K, A2(m->hv_L2c_xx, i, j) * A2(m->hv_Shear_mag, i, j));
                 if (m->hv_leith_kh)
@@ -1022,13 +1043,15 @@ void oracle_coriolis(oracle_model *m, const double *u, const double *v,
                 A2(dudy, i, j) = (A3(u, i, j + 1, k) * A2(m->dxCu, i, j + 1)) -
                                  (A3(u, i, j, k) * A2(m->dxCu, i, j));
             }
+        /* at a west / south cut the q-points on the cut are interior: their
+         * hArea_v(is-1, :) / hArea_u(:, js-1) exist */
         OMP_FOR
         for (int j = js - 1; j <= je; ++j)
-            for (int i = is; i <= ie + 1; ++i)
+            for (int i = is - m->cw; i <= ie + 1; ++i)
                 A2(hAv, i, j) = 0.5 * ((A2(m->areaT, i, j) * A3(h, i, j, k)) +
                                        (A2(m->areaT, i, j + 1) * A3(h, i, j + 1, k)));
         OMP_FOR
-        for (int j = js; j <= je + 1; ++j)
+        for (int j = js - m->cs; j <= je + 1; ++j)
             for (int i = is - 1; i <= ie; ++i)
                 A2(hAu, i, j) = 0.5 * ((A2(m->areaT, i, j) * A3(h, i, j, k)) +
                                        (A2(m->areaT, i + 1, j) * A3(h, i + 1, j, k)));
@@ -1074,9 +1097,10 @@ void oracle_coriolis(oracle_model *m, const double *u, const double *v,
                                     (A2(q, i - 1, j) + A2(q, i, j - 1))) * C1_24;
                 }
         }
+        /* at a cut the face on it is interior: KE one cell further */
         OMP_FOR
-        for (int j = js; j <= je; ++j)
-            for (int i = is; i <= ie; ++i) {
+        for (int j = js; j <= je + m->cn; ++j)
+            for (int i = is; i <= ie + m->ce; ++i) {
                 double u0 = A3(u, i, j, k), um = A3(u, i - 1, j, k);
                 double v0 = A3(v, i, j, k), vm = A3(v, i, j - 1, k);
                 A2(KE, i, j) = 0.25 *
@@ -1086,7 +1110,7 @@ void oracle_coriolis(oracle_model *m, const double *u, const double *v,
             }
         OMP_FOR
         for (int j = js; j <= je; ++j)
-            for (int i = is; i <= ie - 1; ++i) {
+            for (int i = is; i <= ie - 1 + m->ce; ++i) {
                 double KEx = (A2(KE, i + 1, j) - A2(KE, i, j)) * A2(m->IdxCu, i, j);
                 if (m->cor_scheme <= 1)
                     A3(CAu, i, j, k) =
@@ -1104,7 +1128,7 @@ void oracle_coriolis(oracle_model *m, const double *u, const double *v,
                         KEx;
             }
         OMP_FOR
-        for (int j = js; j <= je - 1; ++j)
+        for (int j = js; j <= je - 1 + m->cn; ++j)
             for (int i = is; i <= ie; ++i) {
                 double KEy = (A2(KE, i, j + 1) - A2(KE, i, j)) * A2(m->IdyCv, i, j);
                 if (m->cor_scheme <= 1)
@@ -1363,6 +1387,14 @@ void oracle_btstep(oracle_model *m, const double *eta_in, const double *ubt_in,
     double trans_wt2 = -m->bt_bebt;
     double inv_nstep = 1.0 / (double)m->nstep;
     double dtbt = m->bt_dtbt;
+    /* A subdomain of a decomposed run reaches two points into the halo at a
+     * cut: then the substep's values at the owned points need only the halo
+     * exchanged before the substep (a point's new eta reads ubt, vbt and eta
+     * of the old substep up to two points away).  Without cuts these are the
+     * serial ranges. */
+    const int xw = 2 * m->cw, xe = 2 * m->ce, xs = 2 * m->cs, xn = 2 * m->cn;
+    const int ci0 = is - xw, ci1 = ie + xe, cj0 = js - xs, cj1 = je + xn;
+    const int ui1 = ie - 1 + xe, vj1 = je - 1 + xn;
     OMP_FOR
     for (int j = m->jsd; j <= m->jed; ++j)
         for (int i = m->isd; i <= m->ied; ++i) {
@@ -1373,17 +1405,22 @@ void oracle_btstep(oracle_model *m, const double *eta_in, const double *ubt_in,
             A2(m->bt_vbt_av, i, j) = 0.0;
         }
     for (int n = 1; n <= m->nstep; ++n) {
+        if (m->xfn) {
+            m->xfn(m->xctx, m->bt_ubt, 1, 1);
+            m->xfn(m->xctx, m->bt_vbt, 1, 2);
+            m->xfn(m->xctx, m->bt_eta, 1, 0);
+        }
         OMP_FOR
-        for (int j = js; j <= je; ++j)
-            for (int i = is - 1; i <= ie + 1; ++i)
+        for (int j = cj0; j <= cj1; ++j)
+            for (int i = is - 1 - xw; i <= ie + 1 + xe; ++i)
                 A2(m->bt_ubt_prev, i, j) = A2(m->bt_ubt, i, j);
         OMP_FOR
-        for (int j = js - 1; j <= je + 1; ++j)
-            for (int i = is; i <= ie; ++i)
+        for (int j = js - 1 - xs; j <= je + 1 + xn; ++j)
+            for (int i = ci0; i <= ci1; ++i)
                 A2(m->bt_vbt_prev, i, j) = A2(m->bt_vbt, i, j);
         OMP_FOR
-        for (int j = js; j <= je; ++j)
-            for (int i = is; i <= ie; ++i)
+        for (int j = cj0; j <= cj1; ++j)
+            for (int i = ci0; i <= ci1; ++i)
                 A2(m->bt_eta_pred, i, j) =
                     A2(m->bt_eta, i, j) +
                     (dtbt * A2(m->IareaT, i, j)) *
@@ -1392,46 +1429,48 @@ void oracle_btstep(oracle_model *m, const double *eta_in, const double *ubt_in,
                          ((A2(m->bt_Datv, i, j - 1) * A2(m->bt_vbt, i, j - 1)) -
                           (A2(m->bt_Datv, i, j) * A2(m->bt_vbt, i, j))));
         OMP_FOR
-        for (int j = js; j <= je; ++j)
-            for (int i = is; i <= ie - 1; ++i)
+        for (int j = cj0; j <= cj1; ++j)
+            for (int i = ci0; i <= ui1; ++i)
                 A2(m->bt_PFu, i, j) =
                     ((A2(m->bt_eta_pred, i, j) * A2(m->bt_gtot_E, i, j)) -
                      (A2(m->bt_eta_pred, i + 1, j) * A2(m->bt_gtot_W, i + 1, j))) *
                     m->bt_dgeo_de * A2(m->IdxCu, i, j);
         OMP_FOR
-        for (int j = js; j <= je - 1; ++j)
-            for (int i = is; i <= ie; ++i)
+        for (int j = cj0; j <= vj1; ++j)
+            for (int i = ci0; i <= ci1; ++i)
                 A2(m->bt_PFv, i, j) =
                     ((A2(m->bt_eta_pred, i, j) * A2(m->bt_gtot_N, i, j)) -
                      (A2(m->bt_eta_pred, i, j + 1) * A2(m->bt_gtot_S, i, j + 1))) *
                     m->bt_dgeo_de * A2(m->IdyCv, i, j);
         int v_first = ((n + m->first_direction) % 2) == 1;
         if (v_first) {
-            bt_update_v(m, is, ie, js, je - 1);
-            bt_update_u(m, is, ie - 1, js, je);
+            bt_update_v(m, ci0, ci1, cj0, vj1);
+            bt_update_u(m, ci0, ui1, cj0, cj1);
         } else {
-            bt_update_u(m, is, ie - 1, js, je);
-            bt_update_v(m, is, ie, js, je - 1);
+            bt_update_u(m, ci0, ui1, cj0, cj1);
+            bt_update_v(m, ci0, ci1, cj0, vj1);
         }
         /* transport ranges: serial (:263-291) or, with bt_extended, those
          * of btstep_do_step and the CUDA C kernels (:443-452) */
-        const int iu0 = m->bt_extended ? is - 1 : is, iu1 = m->bt_extended ? ie : ie - 1;
-        const int jv0 = m->bt_extended ? js - 1 : js, jv1 = m->bt_extended ? je : je - 1;
+        const int iu0 = xw ? ci0 : (m->bt_extended ? is - 1 : is);
+        const int iu1 = xe ? ui1 : (m->bt_extended ? ie : ie - 1);
+        const int jv0 = xs ? cj0 : (m->bt_extended ? js - 1 : js);
+        const int jv1 = xn ? vj1 : (m->bt_extended ? je : je - 1);
         OMP_FOR
-        for (int j = js; j <= je; ++j)
+        for (int j = cj0; j <= cj1; ++j)
             for (int i = iu0; i <= iu1; ++i)
                 A2(m->bt_uhbt, i, j) =
                     A2(m->bt_Datu, i, j) *
                     (trans_wt1 * A2(m->bt_ubt, i, j) + trans_wt2 * A2(m->bt_ubt_prev, i, j));
         OMP_FOR
         for (int j = jv0; j <= jv1; ++j)
-            for (int i = is; i <= ie; ++i)
+            for (int i = ci0; i <= ci1; ++i)
                 A2(m->bt_vhbt, i, j) =
                     A2(m->bt_Datv, i, j) *
                     (trans_wt1 * A2(m->bt_vbt, i, j) + trans_wt2 * A2(m->bt_vbt_prev, i, j));
         OMP_FOR
-        for (int j = js; j <= je; ++j)
-            for (int i = is; i <= ie; ++i)
+        for (int j = cj0; j <= cj1; ++j)
+            for (int i = ci0; i <= ci1; ++i)
                 A2(m->bt_eta, i, j) =
                     A2(m->bt_eta, i, j) -
                     dtbt * A2(m->IareaT, i, j) *
@@ -2012,11 +2051,11 @@ static void vel_update(oracle_model *m, const double *ubase, const double *vbase
     for (int k = 1; k <= m->nk; ++k) {
         OMP_FOR
         for (int j = m->js; j <= m->je; ++j)
-            for (int i = m->is; i <= m->ie - 1; ++i)
+            for (int i = m->is; i <= m->ie - 1 + m->ce; ++i)
                 A3(uout, i, j, k) = A3(ubase, i, j, k) +
                                     coef * (A3(m->CAu, i, j, k) + A3(m->diffu, i, j, k));
         OMP_FOR
-        for (int j = m->js; j <= m->je - 1; ++j)
+        for (int j = m->js; j <= m->je - 1 + m->cn; ++j)
             for (int i = m->is; i <= m->ie; ++i)
                 A3(vout, i, j, k) = A3(vbase, i, j, k) +
                                     coef * (A3(m->CAv, i, j, k) + A3(m->diffv, i, j, k));
@@ -2088,7 +2127,12 @@ static void one_step(oracle_model *m) {
     oracle_vert_visc(m, m->up, m->vp, m->h, dt);
     if (m->remnant) oracle_vert_visc_remnant(m, dt);
     oracle_btstep(m, m->eta, m->ubt, m->vbt, m->ubt_av, m->vbt_av, m->eta_av);
+    if (m->xfn) {   /* rk2_mpi_cuda_c_driver.F90:409-412 */
+        m->xfn(m->xctx, m->up, m->nk, 1);
+        m->xfn(m->xctx, m->vp, m->nk, 2);
+    }
     step_continuity(m, m->up, m->vp, m->h0, m->h, dt);
+    if (m->xfn) m->xfn(m->xctx, m->h, m->nk, 0);
     if (m->diag_on) {
         size_t n2d = (size_t)N1 * N2;
         diag_product_sum(m, m->diffu, m->h, 1, 0);
@@ -2112,6 +2156,10 @@ static void one_step(oracle_model *m) {
     oracle_vert_visc(m, m->u, m->v, m->h, 0.5 * dt);
     if (m->remnant) oracle_vert_visc_remnant(m, 0.5 * dt);
     oracle_btstep(m, m->eta_av, m->ubt_av, m->vbt_av, m->ubt_av, m->vbt_av, m->eta);
+    if (m->xfn) {
+        m->xfn(m->xctx, m->u, m->nk, 1);
+        m->xfn(m->xctx, m->v, m->nk, 2);
+    }
     /* htmp <- h over the data domain; the reference loops i=isd,jed
      * (rk2_serial_driver.F90:375), bounded here by ied as the CUDA C driver
      * does (rk2_cuda_c_driver.F90:471). */
@@ -2212,6 +2260,10 @@ void oracle_set_bt_extended(oracle_model *m, int on) { m->bt_extended = on ? 1 :
 /* btstep's G%first_direction (mom6_barotropic_serial.F90:250): which velocity
  * component the odd substeps update first */
 void oracle_set_bt_first_direction(oracle_model *m, int d) { m->first_direction = d; }
+void oracle_set_exchange(oracle_model *m, oracle_exchange_fn fn, void *ctx) {
+    m->xfn = fn;
+    m->xctx = ctx;
+}
 
 /* Copy one of the oracle's grid or control-structure arrays by name (count
  * doubles: n1*n2, or 4*n1*n2 for f_4_u/f_4_v).  Returns 0, or -1 for an

@@ -69,7 +69,21 @@ typedef struct {
     double Kh;          /* Laplacian viscosity [m2 s-1] */
     double Kv, Kv_ml, Kv_extra_bbl, Hmix, Hbbl;
     int bc_fill;        /* 1: apply the periodic-x / wall-y halo fill */
+    /* one subdomain of a decomposed run (mpi_domain_init, mom6_mpi_domain.F90:
+     * 57-137): the global ni, nj (0: this model is the whole domain) and the
+     * offsets of this model's compute domain in the global one; the initial
+     * state and the grid are those of the global points.  cuts: OR_CUT_* bits,
+     * the sides where a neighbouring subdomain lies (no wall). */
+    int ni_global, nj_global, i_offset, j_offset;
+    int cuts;
 } oracle_config;
+
+enum { OR_CUT_W = 1, OR_CUT_E = 2, OR_CUT_S = 4, OR_CUT_N = 8 };
+
+/* The halo exchange of a decomposed run: called on a field (n1 x n2 x nz,
+ * Fortran order) whose halo must be refreshed from the neighbours before the
+ * next phase reads it.  kind: 0 h points, 1 u faces, 2 v faces. */
+typedef void (*oracle_exchange_fn)(void *ctx, double *field, int nz, int kind);
 
 void oracle_config_default(oracle_config *c, int init_mode);
 
@@ -129,6 +143,11 @@ void oracle_dims(const oracle_model *m, int *out8);
 /* btstep transport ranges: 0 serial (default), 1 extended (CUDA C kernels). */
 void oracle_set_bt_extended(oracle_model *m, int on);
 void oracle_set_bt_first_direction(oracle_model *m, int d);
+/* Install the halo exchange of a decomposed run (NULL: none).  The step then
+ * exchanges up, vp before the predictor continuity, h after it, u, v before
+ * the corrector continuity, and the barotropic eta, ubt, vbt before every
+ * substep; the ranges that stop short of a wall reach the cut instead. */
+void oracle_set_exchange(oracle_model *m, oracle_exchange_fn fn, void *ctx);
 /* Copy a named grid / control-structure array (see mom6_oracle.c). */
 int oracle_array(const oracle_model *m, const char *name, double *out, size_t count); /* n1 n2 nk is ie js je ... */
 

@@ -49,7 +49,14 @@ class Config(ctypes.Structure):
                 ("Kh", ctypes.c_double), ("Kv", ctypes.c_double),
                 ("Kv_ml", ctypes.c_double), ("Kv_extra_bbl", ctypes.c_double),
                 ("Hmix", ctypes.c_double), ("Hbbl", ctypes.c_double),
-                ("bc_fill", ctypes.c_int)]
+                ("bc_fill", ctypes.c_int),
+                ("ni_global", ctypes.c_int), ("nj_global", ctypes.c_int),
+                ("i_offset", ctypes.c_int), ("j_offset", ctypes.c_int), ("cuts", ctypes.c_int)]
+
+CUT_W, CUT_E, CUT_S, CUT_N = 1, 2, 4, 8
+# void (*)(void *ctx, double *field, int nz, int kind)
+ExchangeFn = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                              ctypes.c_int, ctypes.c_int)
 
 
 def build():
@@ -99,6 +106,7 @@ def lib(parallel=False):
         L.oracle_normal.restype = d
         L.oracle_set_bt_extended.argtypes = [vp, ctypes.c_int]
         L.oracle_set_bt_first_direction.argtypes = [vp, ctypes.c_int]
+        L.oracle_set_exchange.argtypes = [vp, ExchangeFn, vp]
         L.oracle_array.argtypes = [vp, ctypes.c_char_p, P(d), ctypes.c_size_t]
         L.oracle_array.restype = ctypes.c_int
         L.oracle_set_threads.argtypes = [ctypes.c_int]
@@ -119,9 +127,12 @@ class Oracle:
     """One oracle model (grid + state + persistent module work arrays)."""
 
     def __init__(self, ni, nj, nk, bt_nsteps, init_mode=INIT_CFG, seed=0,
-                 dt=None, Kh=None, bc_fill=None, threads=None, dx_km=None):
+                 dt=None, Kh=None, bc_fill=None, threads=None, dx_km=None,
+                 subdomain=None):
         """threads: None for the single-threaded build, else the OpenMP build
-        on that many threads (0: all the runtime offers)."""
+        on that many threads (0: all the runtime offers).  subdomain: (ni_global,
+        nj_global, i_offset, j_offset, cuts) for one subdomain of a decomposed
+        run, ni and nj then being the local sizes (compute width + 4)."""
         L = lib(parallel=threads is not None)
         self._L = L
         self.threads = 1 if threads is None else L.oracle_set_threads(int(threads))
@@ -136,7 +147,10 @@ class Oracle:
             c.bc_fill = int(bc_fill)
         if dx_km is not None:
             c.dx_km = dx_km
+        if subdomain is not None:
+            c.ni_global, c.nj_global, c.i_offset, c.j_offset, c.cuts = map(int, subdomain)
         self.cfg = c
+        self._xfn = None
         self._m = L.oracle_create(ctypes.byref(c))
         if not self._m:
             raise ValueError("oracle_create rejected the configuration")
@@ -282,6 +296,23 @@ class Oracle:
 
     def set_bt_first_direction(self, d):
         self._L.oracle_set_bt_first_direction(self._m, int(d))
+
+    def set_exchange(self, fn):
+        """fn(a, kind) refreshes the halo of a, a Fortran-ordered (n1, n2, nz)
+        view of the model's field, in place; None removes the exchange."""
+        if fn is None:
+            self._xfn = None
+            self._L.oracle_set_exchange(self._m, ExchangeFn(), None)
+            return
+        n1, n2 = self.n1, self.n2
+
+        def cb(_ctx, ptr, nz, kind):
+            a = np.ctypeslib.as_array(ptr, shape=(n1 * n2 * nz,)).reshape((n1, n2, nz),
+                                                                           order="F")
+            fn(a, kind)
+
+        self._xfn = ExchangeFn(cb)
+        self._L.oracle_set_exchange(self._m, self._xfn, None)
 
     def halo_fill(self, f, kind):
         f = np.asfortranarray(f.copy())
