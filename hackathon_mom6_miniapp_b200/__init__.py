@@ -8,8 +8,8 @@ fallback: every entry point raises if the CUDA library cannot be loaded.
 """
 from ._lib import (Model, Ensemble, Mlp, CudaCDriver, MixedNotBuilt, Mom6bError, FIELDS,
                    FIELDS_3D, INIT_CFG, INIT_REF, FP64, MIXED, TUNING_KEYS, library,
-                   library_path, make_config, abi_set_deferral)
+                   library_path, make_config, abi_set_deferral, HaloGroup, subdomain_config)
 
 __all__ = ["Model", "Ensemble", "Mlp", "CudaCDriver", "Mom6bError", "MixedNotBuilt", "FIELDS",
            "FIELDS_3D", "INIT_CFG", "INIT_REF", "FP64", "MIXED", "TUNING_KEYS", "library",
-           "library_path", "make_config", "abi_set_deferral"]
+           "library_path", "make_config", "abi_set_deferral", "HaloGroup", "subdomain_config"]

@@ -58,7 +58,14 @@ class Config(ctypes.Structure):
                 ("device", ctypes.c_int), ("use_graph", ctypes.c_int),
                 ("exact", ctypes.c_int), ("bt_untiled", ctypes.c_int),
                 ("general_metrics", ctypes.c_int), ("wait_cycles", ctypes.c_longlong),
-                ("mixed_f32_vertvisc", ctypes.c_int)]
+                ("mixed_f32_vertvisc", ctypes.c_int),
+                ("ni_global", ctypes.c_int), ("nj_global", ctypes.c_int),
+                ("i_offset", ctypes.c_int), ("j_offset", ctypes.c_int), ("cuts", ctypes.c_int)]
+
+CUT_W, CUT_E, CUT_S, CUT_N = 1, 2, 4, 8
+# int (*)(void *ctx, double *field, int nz, int kind, void *stream)
+_ExchangeFn = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                               ctypes.c_int, ctypes.c_void_p)
 
 
 def library_path():
@@ -153,6 +160,12 @@ def library():
     L.mom6b_set_hor_visc.argtypes = [vp, ctypes.POINTER(HorVisc)]
     L.mom6b_set_bt_overlap.argtypes = [vp, ctypes.c_int]
     L.mom6b_set_wait_limit.argtypes = [vp, ctypes.c_longlong, ctypes.c_int]
+    L.mom6b_set_exchange.argtypes = [vp, vp, vp]
+    L.mom6b_halo_group_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                          ctypes.POINTER(vp)]
+    L.mom6b_halo_group_join.argtypes = [vp, vp, ctypes.c_int]
+    L.mom6b_halo_group_destroy.argtypes = [vp]
+    L.mom6b_halo_group_destroy.restype = None
     L.mom6b_abi_set_deferral.argtypes = [ctypes.c_int]
     L.mom6b_btstep_noalloc_status.argtypes = [vp]
     L.mom6b_btstep_noalloc_set_wait.argtypes = [ctypes.c_longlong, ctypes.c_int]
@@ -182,9 +195,13 @@ class Model:
     def __init__(self, ni=180, nj=180, nk=75, bt_nsteps=30, init_mode=INIT_CFG,
                  seed=0, dt=None, Kh=None, bc_fill=None, precision=FP64,
                  device=0, use_graph=False, dx_km=None, exact=False, bt_untiled=False,
-                 general_metrics=False, wait_cycles=0, mixed_f32_vertvisc=False):
+                 general_metrics=False, wait_cycles=0, mixed_f32_vertvisc=False,
+                 subdomain=None):
         """exact=True: the bit-identical FP64 kernels (the serial driver's
-        roundings); False: the fast FP64 kernels (within 1e-12 relative L2)."""
+        roundings); False: the fast FP64 kernels (within 1e-12 relative L2).
+        subdomain: (ni_global, nj_global, i_offset, j_offset, cuts) for one
+        subdomain of a decomposed run (ni, nj then its own sizes; see
+        HaloGroup)."""
         L = library()
         c = Config()
         _check(L.mom6b_config_default(ctypes.byref(c), init_mode))
@@ -201,6 +218,8 @@ class Model:
         c.exact, c.bt_untiled = int(bool(exact)), int(bool(bt_untiled))
         c.general_metrics, c.wait_cycles = int(bool(general_metrics)), int(wait_cycles)
         c.mixed_f32_vertvisc = int(bool(mixed_f32_vertvisc))
+        if subdomain is not None:
+            c.ni_global, c.nj_global, c.i_offset, c.j_offset, c.cuts = map(int, subdomain)
         self.cfg = c
         h = ctypes.c_void_p()
         rc = L.mom6b_create(ctypes.byref(c), ctypes.byref(h))
@@ -244,6 +263,41 @@ class Model:
 
     def synchronize(self):
         _check(library().mom6b_synchronize(self._m))
+
+    def set_exchange(self, fn):
+        """The halo exchange of a decomposed run, from Python (mom6b_set_exchange):
+        fn(t, kind) refreshes in place the halo of t, a torch CUDA tensor viewing
+        the model's device field as (nz, n2, n1) (the Fortran array's memory),
+        with the model's stream current, so work fn enqueues there is ordered
+        with the step; kind 0 h points, 1 u faces, 2 v faces.  With one process
+        per GPU, fn = decomp.HaloExchange(d).exchange over torch.distributed
+        (NCCL); within one process, decomp.LocalHaloExchange.  None removes it."""
+        L = library()
+        if fn is None:
+            self._xfn = None
+            _check(L.mom6b_set_exchange(self._m, None, None))
+            return
+        import torch
+        dev = torch.device("cuda", int(self.cfg.device))
+        n1, n2 = self.n1, self.n2
+
+        class _View:
+            def __init__(self, ptr, nz):
+                self.__cuda_array_interface__ = {"shape": (nz, n2, n1), "typestr": "<f8",
+                                                 "data": (ptr, False), "version": 2}
+
+        def cb(_ctx, ptr, nz, kind, stream):
+            try:
+                t = torch.as_tensor(_View(ptr, nz), device=dev)
+                with torch.cuda.stream(torch.cuda.ExternalStream(stream, device=dev)):
+                    fn(t, kind)
+                return 0
+            except Exception as e:   # the step reports the failure
+                self.exchange_error = e
+                return 1
+
+        self._xfn = _ExchangeFn(cb)
+        _check(L.mom6b_set_exchange(self._m, ctypes.cast(self._xfn, ctypes.c_void_p), None))
 
     def step_host(self, n, u=None, v=None, h=None, eta=None):
         """End-to-end: upload the given host arrays, run n steps, download them."""
@@ -430,6 +484,45 @@ def abi_set_deferral(on=True):
     """Defer the launch_bt_* substep calls of one btstep_cuda_c into one
     persistent loop (mom6b_abi_set_deferral; on by default)."""
     _check(library().mom6b_abi_set_deferral(int(bool(on))))
+
+
+class HaloGroup:
+    """The library's in-process halo exchange among npes_x * npes_y subdomain
+    models (mom6b_halo_group_*): join each model at its rank (pos_x * npes_y
+    + pos_y), then step every model from its own host thread."""
+
+    def __init__(self, npes_x, npes_y, timeout_s=60.0):
+        h = ctypes.c_void_p()
+        _check(library().mom6b_halo_group_create(int(npes_x), int(npes_y), float(timeout_s),
+                                                 ctypes.byref(h)))
+        self._g = h
+        self.members = {}
+
+    def join(self, model, rank):
+        _check(library().mom6b_halo_group_join(self._g, model._m, int(rank)))
+        self.members[int(rank)] = model
+
+    def close(self):
+        if getattr(self, "_g", None):
+            library().mom6b_halo_group_destroy(self._g)
+            self._g = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def subdomain_config(ni_global, nj_global, npes_x, npes_y, rank):
+    """(ni, nj, subdomain) of one rank's model: the global compute domain
+    (ni_global - 4 by nj_global - 4 points) split as mpi_domain_init splits
+    it (mom6_mpi_domain.F90:57-137, remainder to the first positions)."""
+    from .decomp import Decomposition
+    d = Decomposition(ni_global - 4, nj_global - 4, npes_x, npes_y, rank)
+    cuts = sum(bit for side, bit in (("W", CUT_W), ("E", CUT_E), ("S", CUT_S), ("N", CUT_N))
+               if d.neighbour(side) is not None)
+    return d.ni_local + 4, d.nj_local + 4, (ni_global, nj_global, d.i_offset, d.j_offset, cuts)
 
 
 def make_config(ni=180, nj=180, nk=75, bt_nsteps=30, init_mode=INIT_CFG, seed=0, dt=None,

@@ -36,6 +36,9 @@ struct Dims {
     int is, ie, js, je;   // compute domain, 1-based
     int isd, ied, jsd, jed;
     long long plane;      // n1 * n2
+    // sides (west, east, south, north) where a decomposed run's neighbouring
+    // subdomain lies: 1 at a cut, 0 at a wall or for the whole domain
+    int cw = 0, ce = 0, cs = 0, cn = 0;
 };
 
 #define MOM6B_A2(a, i, j, D) (a)[(size_t)((j)-1) * (size_t)(D).n1 + (size_t)((i)-1)]

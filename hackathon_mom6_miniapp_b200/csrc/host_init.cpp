@@ -52,6 +52,9 @@ double philox_normal(uint64_t seed, uint32_t stream, uint64_t index)
 HostGrid::HostGrid(const mom6b_config& c) : cfg(c)
 {
     ni = c.ni; nj = c.nj; nk = c.nk;
+    gni = c.ni_global > 0 ? c.ni_global : c.ni;
+    gnj = c.nj_global > 0 ? c.nj_global : c.nj;
+    ioff = c.i_offset; joff = c.j_offset;
     isd = 1; ied = ni + 2; jsd = 1; jed = nj + 2;
     is = isd + 3; ie = ied - 3; js = jsd + 3; je = jed - 3;
     n1 = ied; n2 = jed;
@@ -77,7 +80,7 @@ void HostGrid::build()
     dx = dx_m;
     const double f0 = 2.0 * kOmega * std::sin(cfg.lat_deg * kPiRef / 180.0);
     const double beta = 2.0 * kOmega * std::cos(cfg.lat_deg * kPiRef / 180.0) / kEarthRadius;
-    const double Ly = (double)(je - js + 1) * dx_m;
+    const double Ly = (double)((gnj - 1) - js + 1) * dx_m;
     for (int j = jsd; j <= jed; ++j)
         for (int i = isd; i <= ied; ++i) {
             size_t p = at(i, j);
@@ -97,9 +100,9 @@ void HostGrid::build()
             IdxBu[p] = 1.0 / dx_m; IdyBu[p] = 1.0 / dx_m;
             mask2dT[p] = 1.0; mask2dBu[p] = 1.0; mask2dCu[p] = 1.0; mask2dCv[p] = 1.0;
             if (cfg.init_mode == MOM6B_INIT_REF) {
-                CoriolisBu[p] = f0 + beta * ((double)(j - 1 - nj / 2) - 0.5) * dx_m;
+                CoriolisBu[p] = f0 + beta * ((double)(j + joff - 1 - gnj / 2) - 0.5) * dx_m;
             } else {
-                double yq = (double)(j - js + 1) * dx_m;
+                double yq = (double)(j + joff - js + 1) * dx_m;
                 CoriolisBu[p] = 1.0e-4 + 2.0e-11 * (yq - 0.5 * Ly);
             }
         }
@@ -143,7 +146,7 @@ void HostGrid::build()
     // forcing: wind stress and bottom-layer Rayleigh drag
     for (int j = jsd; j <= jed; ++j)
         for (int i = isd; i <= ied; ++i) {
-            taux[at(i, j)] = 0.1 * std::sin((double)(j - 1) / (double)nj * pi_init);
+            taux[at(i, j)] = 0.1 * std::sin((double)(j + joff - 1) / (double)gnj * pi_init);
             tauy[at(i, j)] = 0.0;
         }
 }
@@ -162,21 +165,21 @@ void HostGrid::initial_state(std::vector<double>& u, std::vector<double>& v,
                 for (int i = isd; i <= ied; ++i) {
                     size_t p = at(i, j, k);
                     h0[p] = total_depth / (double)nk +
-                            10.0 * std::sin((double)(i - 1) / (double)ni * pi_init) *
-                                std::cos((double)(j - 1) / (double)nj * pi_init) *
+                            10.0 * std::sin((double)(i + ioff - 1) / (double)gni * pi_init) *
+                                std::cos((double)(j + joff - 1) / (double)gnj * pi_init) *
                                 std::exp(-(double)k / 20.0);
-                    u[p] = 0.1 * std::sin((double)(j - 1) / (double)nj * pi_init * 2.0) *
+                    u[p] = 0.1 * std::sin((double)(j + joff - 1) / (double)gnj * pi_init * 2.0) *
                            std::exp(-(double)k / 30.0);
-                    v[p] = 0.1 * std::cos((double)(i - 1) / (double)ni * pi_init * 2.0) *
+                    v[p] = 0.1 * std::cos((double)(i + ioff - 1) / (double)gni * pi_init * 2.0) *
                            std::exp(-(double)k / 30.0);
                 }
         for (int j = jsd; j <= jed; ++j)
             for (int i = isd; i <= ied; ++i) {
                 size_t p = at(i, j);
-                eta[p] = 0.5 * std::sin((double)(i - 1) / (double)ni * pi_init * 2.0) *
-                         std::cos((double)(j - 1) / (double)nj * pi_init * 2.0);
-                ubt[p] = 0.05 * std::sin((double)(j - 1) / (double)nj * pi_init);
-                vbt[p] = 0.05 * std::cos((double)(i - 1) / (double)ni * pi_init);
+                eta[p] = 0.5 * std::sin((double)(i + ioff - 1) / (double)gni * pi_init * 2.0) *
+                         std::cos((double)(j + joff - 1) / (double)gnj * pi_init * 2.0);
+                ubt[p] = 0.05 * std::sin((double)(j + joff - 1) / (double)gnj * pi_init);
+                vbt[p] = 0.05 * std::cos((double)(i + ioff - 1) / (double)gni * pi_init);
             }
     } else {
         const double hbar = 4000.0 / (double)nk;
@@ -184,20 +187,23 @@ void HostGrid::initial_state(std::vector<double>& u, std::vector<double>& v,
             for (int j = jsd; j <= jed; ++j)
                 for (int i = isd; i <= ied; ++i) {
                     size_t p = at(i, j, k);
-                    uint64_t idx = (uint64_t)p;
+                    // the global point's Philox counter
+                    uint64_t idx = ((uint64_t)(k - 1) * (uint64_t)(gnj + 2) +
+                                    (uint64_t)(j + joff - 1)) * (uint64_t)(gni + 2) +
+                                   (uint64_t)(i + ioff - 1);
                     double hv = hbar * (1.0 + 0.01 * philox_normal(cfg.seed, 1u, idx));
                     if (hv < 0.01 * hbar) hv = 0.01 * hbar;
                     h0[p] = hv;
                     u[p] = 0.05 * philox_normal(cfg.seed, 2u, idx);
                     v[p] = 0.05 * philox_normal(cfg.seed, 3u, idx);
                 }
-        const double Lx = (double)(ie - is + 1) * dx;
-        const double Ly = (double)(je - js + 1) * dx;
+        const double Lx = (double)((gni - 1) - is + 1) * dx;
+        const double Ly = (double)((gnj - 1) - js + 1) * dx;
         const double R = 200.0e3;
         for (int j = jsd; j <= jed; ++j)
             for (int i = isd; i <= ied; ++i) {
-                double x = ((double)(i - is) + 0.5) * dx - 0.5 * Lx;
-                double y = ((double)(j - js) + 0.5) * dx - 0.5 * Ly;
+                double x = ((double)(i + ioff - is) + 0.5) * dx - 0.5 * Lx;
+                double y = ((double)(j + joff - js) + 0.5) * dx - 0.5 * Ly;
                 eta[at(i, j)] = 0.1 * std::exp(-(x * x + y * y) / (R * R));
             }
     }

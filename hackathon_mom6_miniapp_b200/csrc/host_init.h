@@ -16,6 +16,9 @@ double philox_normal(uint64_t seed, uint32_t stream, uint64_t index);
 struct HostGrid {
     mom6b_config cfg;
     int ni, nj, nk, n1, n2;
+    // a subdomain's global ni, nj and compute-domain offsets (the whole
+    // domain: ni, nj, 0, 0); positions are evaluated at the global indices
+    int gni, gnj, ioff, joff;
     int isd, ied, jsd, jed, is, ie, js, je;
     size_t plane;
     double dx = 0.0;

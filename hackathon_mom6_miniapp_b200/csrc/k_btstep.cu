@@ -104,11 +104,22 @@ k_btstep(Dims D, Metrics M, BTWork W, BTParams P, const double* eta_in,
     const int gtid = (int)(blockIdx.x * blockDim.x + threadIdx.x);
     const int gsz = (int)(gridDim.x * blockDim.x);
     const int is = D.is, ie = D.ie, js = D.js, je = D.je;
+    // A subdomain of a decomposed run reaches two points into the halo at a
+    // cut, so that a substep's values at the owned points need only the halo
+    // exchanged before it (a new eta reads the old ubt, vbt, eta up to two
+    // points away).  Without cuts these are the serial ranges: cells
+    // [ci0, ci1] x [cj0, cj1], u faces to ui1, v faces to vj1.
+    const int xw = 2 * D.cw, xe = 2 * D.ce, xs = 2 * D.cs, xn = 2 * D.cn;
+    const int ci0 = is - xw, ci1 = ie + xe, cj0 = js - xs, cj1 = je + xn;
+    const int ui1 = ie - 1 + xe, vj1 = je - 1 + xn;
     // serial ranges vs. extended ranges for uhbt/vhbt and the averages
-    const int iu0 = P.extended ? is - 1 : is, iu1 = P.extended ? ie : ie - 1;
-    const int jv0 = P.extended ? js - 1 : js, jv1 = P.extended ? je : je - 1;
-    const int bw = ie - is + 3;                 // active box width
-    const int nbox = bw * (je - js + 3);
+    const int iu0 = xw ? ci0 : (P.extended ? is - 1 : is);
+    const int iu1 = xe ? ui1 : (P.extended ? ie : ie - 1);
+    const int jv0 = xs ? cj0 : (P.extended ? js - 1 : js);
+    const int jv1 = xn ? vj1 : (P.extended ? je : je - 1);
+    const int bx0 = is - 1 - xw, by0 = js - 1 - xs;   // active box origin
+    const int bw = ie - is + 3 + xw + xe;             // active box width
+    const int nbox = bw * (je - js + 3 + xs + xn);
     const int nr = FAST ? (nbox - gtid + gsz - 1) / gsz : 0;
 #define A(a, ii, jj) MOM6B_A2(a, ii, jj, D)
 #define PV(q, r, p) (*(FAST ? &s_priv[((q) * kBtMaxR + (r)) * blockDim.x + threadIdx.x] \
@@ -119,8 +130,8 @@ k_btstep(Dims D, Metrics M, BTWork W, BTParams P, const double* eta_in,
 #pragma unroll
         for (int r = 0; r < kBtMaxR; ++r) {
             int q = gtid + r * gsz;
-            pi[r] = is - 1 + q % bw;
-            pj[r] = js - 1 + q / bw;
+            pi[r] = bx0 + q % bw;
+            pj[r] = by0 + q / bw;
             pp[r] = (pj[r] - 1) * D.n1 + (pi[r] - 1);
 #pragma unroll
             for (int v = 0; v < PV_N; ++v)
@@ -137,26 +148,29 @@ k_btstep(Dims D, Metrics M, BTWork W, BTParams P, const double* eta_in,
             }
         } else {
             for (int q = gtid; q < nbox; q += gsz) {
-                int i = is - 1 + q % bw, j = js - 1 + q / bw;
+                int i = bx0 + q % bw, j = by0 + q / bw;
                 f(0, i, j, (j - 1) * D.n1 + (i - 1));
             }
         }
     };
 
     // init (:199-207): state copies over the whole data domain
-    for (int p = gtid; p < npts; p += gsz) {
-        W.eta[p] = eta_in[p];
-        W.ubt[p] = ubt_in[p];
-        W.vbt[p] = vbt_in[p];
-        if (!FAST) { W.ubt_av[p] = 0.0; W.vbt_av[p] = 0.0; }
+    if (P.substep == 0 || P.substep == kBtInit) {
+        for (int p = gtid; p < npts; p += gsz) {
+            W.eta[p] = eta_in[p];
+            W.ubt[p] = ubt_in[p];
+            W.vbt[p] = vbt_in[p];
+            if (!FAST) { W.ubt_av[p] = 0.0; W.vbt_av[p] = 0.0; }
+        }
+        if (!grid_barrier(W, nblocks + (unsigned)P.stall_test, P.spin_budget)) return;
+        if (P.substep == kBtInit) return;
     }
-    if (!grid_barrier(W, nblocks + (unsigned)P.stall_test, P.spin_budget)) return;
 
     auto phase_A = [&]() {
         for_points([&](int r, int i, int j, int p) {
-            if (j >= js && j <= je) PV(PV_PREVU, r, p) = W.ubt[p];  // i in [is-1, ie+1]
-            if (i >= is && i <= ie) PV(PV_PREVV, r, p) = W.vbt[p];  // j in [js-1, je+1]
-            if (i >= is && i <= ie && j >= js && j <= je)
+            if (j >= cj0 && j <= cj1) PV(PV_PREVU, r, p) = W.ubt[p];  // i: the box's
+            if (i >= ci0 && i <= ci1) PV(PV_PREVV, r, p) = W.vbt[p];  // j: the box's
+            if (i >= ci0 && i <= ci1 && j >= cj0 && j <= cj1)
                 W.eta_pred[p] =
                     W.eta[p] + (P.dtbt * A(M.IareaT, i, j)) *
                                    (((A(M.Datu, i - 1, j) * A(W.ubt, i - 1, j)) -
@@ -180,26 +194,28 @@ k_btstep(Dims D, Metrics M, BTWork W, BTParams P, const double* eta_in,
         W.vbt[p] = A(M.bt_rem_v, i, j) * (W.vbt[p] + P.dtbt * (Cor_v + PFv));
     };
 
+    const int n0 = P.substep > 0 ? P.substep : 1, n1 = P.substep > 0 ? P.substep : P.nstep;
+    if (P.substep != kBtFinish) {
     phase_A();
     if (!grid_barrier(W, nblocks, P.spin_budget)) return;
 
-    for (int n = 1; n <= P.nstep; ++n) {
+    for (int n = n0; n <= n1; ++n) {
         const bool v_first = ((n + P.first_direction) % 2) == 1;
         // phase B: pressure force (:234-247) and the first update
         for_points([&](int r, int i, int j, int p) {
-            if (j >= js && j <= je && i >= is && i <= ie - 1)
+            if (j >= cj0 && j <= cj1 && i >= ci0 && i <= ui1)
                 PV(PV_PFU, r, p) = ((W.eta_pred[p] * A(M.gtot_E, i, j)) -
                                     (A(W.eta_pred, i + 1, j) * A(M.gtot_W, i + 1, j))) *
                                    P.dgeo_de * A(M.IdxCu, i, j);
-            if (j >= js && j <= je - 1 && i >= is && i <= ie)
+            if (j >= cj0 && j <= vj1 && i >= ci0 && i <= ci1)
                 PV(PV_PFV, r, p) = ((W.eta_pred[p] * A(M.gtot_N, i, j)) -
                                     (A(W.eta_pred, i, j + 1) * A(M.gtot_S, i, j + 1))) *
                                    P.dgeo_de * A(M.IdyCv, i, j);
             if (v_first) {
-                if (i >= is && i <= ie && j >= js && j <= je - 1)
+                if (i >= ci0 && i <= ci1 && j >= cj0 && j <= vj1)
                     update_v(p, i, j, PV(PV_PFV, r, p));
             } else {
-                if (i >= is && i <= ie - 1 && j >= js && j <= je)
+                if (i >= ci0 && i <= ui1 && j >= cj0 && j <= cj1)
                     update_u(p, i, j, PV(PV_PFU, r, p));
             }
         });
@@ -207,18 +223,18 @@ k_btstep(Dims D, Metrics M, BTWork W, BTParams P, const double* eta_in,
         // phase C: second update, transports (:263-272), averages (:282-291)
         for_points([&](int r, int i, int j, int p) {
             if (v_first) {
-                if (i >= is && i <= ie - 1 && j >= js && j <= je)
+                if (i >= ci0 && i <= ui1 && j >= cj0 && j <= cj1)
                     update_u(p, i, j, PV(PV_PFU, r, p));
             } else {
-                if (i >= is && i <= ie && j >= js && j <= je - 1)
+                if (i >= ci0 && i <= ci1 && j >= cj0 && j <= vj1)
                     update_v(p, i, j, PV(PV_PFV, r, p));
             }
-            if (j >= js && j <= je && i >= iu0 && i <= iu1) {
+            if (j >= cj0 && j <= cj1 && i >= iu0 && i <= iu1) {
                 double ub = W.ubt[p];
                 W.uhbt[p] = A(M.Datu, i, j) * (P.trans_wt1 * ub + P.trans_wt2 * PV(PV_PREVU, r, p));
                 PV(PV_AVU, r, p) = PV(PV_AVU, r, p) + ub * P.inv_nstep;
             }
-            if (j >= jv0 && j <= jv1 && i >= is && i <= ie) {
+            if (j >= jv0 && j <= jv1 && i >= ci0 && i <= ci1) {
                 double vb = W.vbt[p];
                 W.vhbt[p] = A(M.Datv, i, j) * (P.trans_wt1 * vb + P.trans_wt2 * PV(PV_PREVV, r, p));
                 PV(PV_AVV, r, p) = PV(PV_AVV, r, p) + vb * P.inv_nstep;
@@ -227,16 +243,18 @@ k_btstep(Dims D, Metrics M, BTWork W, BTParams P, const double* eta_in,
         if (!grid_barrier(W, nblocks, P.spin_budget)) return;
         // phase D: eta update (:274-279), then phase A of the next substep
         for_points([&](int r, int i, int j, int p) {
-            if (i >= is && i <= ie && j >= js && j <= je)
+            if (i >= ci0 && i <= ci1 && j >= cj0 && j <= cj1)
                 W.eta[p] = W.eta[p] - P.dtbt * A(M.IareaT, i, j) *
                                           ((W.uhbt[p] - A(W.uhbt, i - 1, j)) +
                                            (W.vhbt[p] - A(W.vhbt, i, j - 1)));
         });
         // eta_pred(i,j) needs only this thread's new eta(i,j); the velocity
         // neighbours were final before the last barrier
-        if (n < P.nstep) phase_A();
+        if (n < n1) phase_A();
         if (!grid_barrier(W, nblocks, P.spin_budget)) return;
     }
+    }
+    if (P.substep > 0) return;
     // copy output (:296-302); outputs may alias the inputs.  The averages are
     // zero outside their ranges (the init of :204-205).
     if (FAST) {
@@ -1177,7 +1195,9 @@ cudaError_t launch_btstep(const Dims& D, const Metrics& M, const UniMetrics& U,
     if (e0 != cudaSuccess) return e0;
     // tiled variant: the updated box split into at most one tile per SM
     BTTiles T;
-    if (!P.untiled && tiles_for(D, nsm, T))
+    const bool cut = D.cw || D.ce || D.cs || D.cn;
+    if (cut && P.substep == 0) return cudaErrorInvalidValue;   // one launch per substep
+    if (!P.untiled && !cut && P.substep == 0 && tiles_for(D, nsm, T))
         return launch_btstep_tiled(D, M, U, W, P, T, eta_in, ubt_in, vbt_in, u_av, v_av,
                                    eta_av, s);
     {
@@ -1186,11 +1206,14 @@ cudaError_t launch_btstep(const Dims& D, const Metrics& M, const UniMetrics& U,
                                              (int)smem_fast);
         if (e != cudaSuccess) return e;
     }
-    const long long nbox = (long long)(D.ie - D.is + 3) * (D.je - D.js + 3);
+    const long long nbox = (long long)(D.ie - D.is + 3 + 2 * (D.cw + D.ce)) *
+                           (D.je - D.js + 3 + 2 * (D.cs + D.cn));
     int blocks = nsm;
     int need = (int)((nbox + kBtThreads - 1) / kBtThreads);
     if (blocks > need) blocks = need;
-    const bool fast = (long long)blocks * kBtThreads * kBtMaxR >= nbox;
+    // the shared-memory privates last one launch: a loop split over launches
+    // keeps them in the global work arrays
+    const bool fast = P.substep == 0 && (long long)blocks * kBtThreads * kBtMaxR >= nbox;
     Dims Dc = D; Metrics Mc = M; BTWork Wc = W; BTParams Pc = P;
     void* args[] = {&Dc, &Mc, &Wc, &Pc, (void*)&eta_in, (void*)&ubt_in, (void*)&vbt_in,
                     (void*)&u_av, (void*)&v_av, (void*)&eta_av};

@@ -61,7 +61,13 @@ struct BTParams {
     int stall_test = 0;
     // 1: the point-parallel persistent kernel even where the tiled one fits
     int untiled = 0;
+    // Part of the loop one launch runs (the point-parallel kernel, privates in
+    // the global work arrays): 0 all of it; kBtInit the state copies and the
+    // zeroed averages only; n >= 1 substep n only; kBtFinish the output copy
+    // only.  A decomposed run exchanges halos between the launches.
+    int substep = 0;
 };
+constexpr int kBtInit = -1, kBtFinish = -2;
 
 // The default wait limit of the barotropic barriers: 2^31 clock64 cycles,
 // about 1.1 s at the B200's 1965 MHz.

@@ -24,11 +24,13 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -127,6 +129,9 @@ struct mom6b_model {
     bool hvgen = false;
     HorViscGen hvp{};
     double *hv_du = nullptr, *hv_dv = nullptr;
+    // the halo exchange of a decomposed run (mom6b_set_exchange)
+    mom6b_exchange_fn xfn = nullptr;
+    void* xctx = nullptr;
 };
 
 static double* dalloc(mom6b_model* m, size_t n, cudaError_t* err)
@@ -304,6 +309,15 @@ extern "C" int mom6b_create(const mom6b_config* cfg, mom6b_model** out)
         return fail(MOM6B_ERR_ARG, "horizontal grid too large");
     if (cfg->precision != MOM6B_FP64 && cfg->precision != MOM6B_MIXED)
         return fail(MOM6B_ERR_ARG, "unknown precision");
+    {
+        const int gni = cfg->ni_global > 0 ? cfg->ni_global : cfg->ni;
+        const int gnj = cfg->nj_global > 0 ? cfg->nj_global : cfg->nj;
+        if (cfg->i_offset < 0 || cfg->j_offset < 0 || cfg->i_offset + (cfg->ni - 4) > gni - 4 ||
+            cfg->j_offset + (cfg->nj - 4) > gnj - 4 || (cfg->cuts & ~15))
+            return fail(MOM6B_ERR_ARG, "subdomain outside the global domain");
+        if (cfg->cuts && (cfg->bc_fill || cfg->precision != MOM6B_FP64))
+            return fail(MOM6B_ERR_ARG, "a subdomain with cuts steps in FP64 without halo fill");
+    }
     CK(cudaSetDevice(cfg->device));
 
     auto m = std::make_unique<mom6b_model>();
@@ -316,6 +330,8 @@ extern "C" int mom6b_create(const mom6b_config* cfg, mom6b_model** out)
     D.is = g.is; D.ie = g.ie; D.js = g.js; D.je = g.je;
     D.isd = g.isd; D.ied = g.ied; D.jsd = g.jsd; D.jed = g.jed;
     D.plane = (long long)g.plane;
+    D.cw = (cfg->cuts & MOM6B_CUT_W) != 0; D.ce = (cfg->cuts & MOM6B_CUT_E) != 0;
+    D.cs = (cfg->cuts & MOM6B_CUT_S) != 0; D.cn = (cfg->cuts & MOM6B_CUT_N) != 0;
 
     const size_t n2 = g.plane, n3 = g.plane * (size_t)g.nk;
     cudaError_t err = cudaSuccess;
@@ -651,8 +667,16 @@ static int enqueue_step(mom6b_model* m)
     cudaStream_t s = m->s3d;
     // The barotropic chain only needs co-residency of its own blocks; it is
     // overlapped with the 3-D chain only when enabled.
-    cudaStream_t s2 = m->overlap_bt ? m->s2d : m->s3d;
+    cudaStream_t s2 = (m->overlap_bt && !m->xfn) ? m->s2d : m->s3d;
     const double dt = c.dt;
+    // the halo exchange of a decomposed run (none for a whole domain)
+    auto xch = [&](double* f, int nz, int kind, cudaStream_t st) -> int {
+        if (!m->xfn) return MOM6B_OK;
+        if (m->xfn(m->xctx, f, nz, kind, (void*)st) != 0)
+            return fail(MOM6B_ERR_STATE, "halo exchange failed");
+        return MOM6B_OK;
+    };
+#define XCH(f, nz, kind, st) do { if (int rc_ = xch(f, nz, kind, st)) return rc_; } while (0)
     const double hv_neglect = step_hv_neglect();
     const double h_min = step_h_min();
     VVParams VV = step_vv_params(c);
@@ -739,7 +763,10 @@ static int enqueue_step(mom6b_model* m)
         return launch_vertvisc(D, M, m->up, m->vp, m->h0, dt, VV, m->taux_bot,
                                m->tauy_bot, s, m->remnant ? m->visc_rem_u : nullptr,
                                m->remnant ? m->visc_rem_v : nullptr); }));
+    XCH(m->up, g.nk, 1, s);   // rk2_mpi_cuda_c_driver.F90:409-412
+    XCH(m->vp, g.nk, 2, s);
     CK(continuity_pass(m, s, m->up, m->vp, m->h0, OB, dt));
+    XCH(m->hB, g.nk, 0, s);
     if (c.bc_fill) {
         CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->hB, g.nk, 0, s); }));
         CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->up, g.nk, 1, s); }));
@@ -770,6 +797,8 @@ static int enqueue_step(mom6b_model* m)
         return launch_vertvisc(D, M, m->u, m->v, m->hB, 0.5 * dt, VV, m->taux_bot,
                                m->tauy_bot, s, m->remnant ? m->visc_rem_u : nullptr,
                                m->remnant ? m->visc_rem_v : nullptr); }));
+    XCH(m->u, g.nk, 1, s);
+    XCH(m->v, g.nk, 2, s);
     CK(continuity_pass(m, s, m->u, m->v, m->hB, OA, 0.5 * dt));
     if (c.bc_fill) {
         CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->hA, g.nk, 0, s); }));
@@ -791,6 +820,32 @@ static int enqueue_step(mom6b_model* m)
     }
     BTParams P = step_bt_params(c);
     P.stall_test = m->stall_test;
+    if (m->xfn) {
+        // a subdomain: one launch per substep, the eta, ubt, vbt halos
+        // exchanged before each (rk2_mpi_cuda_c_driver.F90:376-401)
+        auto bt_sub = [&](const double* ei, const double* ui, const double* vi, double* ua,
+                          double* va, double* ea) -> int {
+            BTParams Q = P;
+            Q.substep = kBtInit;
+            CK(timed(m, s2, "btstep", [&] {
+                return launch_btstep(D, M, m->U, m->bt, Q, ei, ui, vi, ua, va, ea, s2); }));
+            for (int n = 1; n <= P.nstep; ++n) {
+                XCH(m->bt.ubt, 1, 1, s2);
+                XCH(m->bt.vbt, 1, 2, s2);
+                XCH(m->bt.eta, 1, 0, s2);
+                Q.substep = n;
+                CK(timed(m, s2, "btstep", [&] {
+                    return launch_btstep(D, M, m->U, m->bt, Q, ei, ui, vi, ua, va, ea, s2); }));
+            }
+            Q.substep = kBtFinish;
+            CK(timed(m, s2, "btstep", [&] {
+                return launch_btstep(D, M, m->U, m->bt, Q, ei, ui, vi, ua, va, ea, s2); }));
+            return MOM6B_OK;
+        };
+        if (int rc = bt_sub(m->eta, m->ubt, m->vbt, m->ubt_av, m->vbt_av, m->eta_av)) return rc;
+        return bt_sub(m->eta_av, m->ubt_av, m->vbt_av, m->ubt_av, m->vbt_av, m->eta);
+    }
+#undef XCH
     CK(timed(m, s2, "btstep", [&] {
         return launch_btstep(D, M, m->U, m->bt, P, m->eta, m->ubt, m->vbt, m->ubt_av,
                              m->vbt_av, m->eta_av, s2); }));
@@ -909,6 +964,11 @@ extern "C" int mom6b_step(mom6b_model* m, int nsteps)
 {
     if (!m || nsteps < 0) return fail(MOM6B_ERR_ARG, "bad argument");
     CK(cudaSetDevice(m->cfg.device));
+    if (m->cfg.cuts && !m->xfn)
+        return fail(MOM6B_ERR_STATE, "a subdomain with cuts needs a halo exchange");
+    if (m->xfn && (m->diag_driver || m->diag || m->merid || m->remnant || m->hvgen ||
+                   m->cor_scheme != 1 || (m->sur && m->sur_on)))
+        return fail(MOM6B_ERR_STATE, "the decomposed step supports the default FP64 step only");
     if (m->diag_driver) return diag_driver_steps(m, nsteps);
     if (m->sur && m->sur_on && !m->sur_fallen) {
         for (int n = 0; n < nsteps; ++n) {
@@ -928,7 +988,7 @@ extern "C" int mom6b_step(mom6b_model* m, int nsteps)
 
 static int step_plain_or_graph(mom6b_model* m, int nsteps)
 {
-    if (m->cfg.use_graph && !m->timing) {
+    if (m->cfg.use_graph && !m->timing && !m->xfn) {
         if (!m->graph_exec) {
             if (int rc = capture_step(m)) return rc;
         }
@@ -1442,6 +1502,178 @@ extern "C" int mom6b_set_wait_limit(mom6b_model* m, long long cycles, int stall_
     invalidate_graph(m);
     return MOM6B_OK;
 }
+
+extern "C" int mom6b_set_exchange(mom6b_model* m, mom6b_exchange_fn fn, void* ctx)
+{
+    if (!m) return fail(MOM6B_ERR_ARG, "null model");
+    CK(cudaSetDevice(m->cfg.device));
+    CK(cudaStreamSynchronize(m->s3d));
+    CK(cudaStreamSynchronize(m->s2d));
+    m->xfn = fn;
+    m->xctx = fn ? ctx : nullptr;
+    invalidate_graph(m);
+    return MOM6B_OK;
+}
+
+// ---- the in-process halo group --------------------------------------------
+// Members post their field, meet at a host barrier, pull their neighbours'
+// strips with 3-D copies on their own streams (peer copies across devices),
+// and meet again before any owner may change its strips.
+struct mom6b_halo_group {
+    int px = 0, py = 0;
+    double timeout_s = 60.0;
+    std::mutex mu;
+    std::condition_variable cv;
+    int arrived = 0;
+    unsigned long long gen = 0;
+    bool failed = false;
+    struct Member {
+        mom6b_model* m = nullptr;
+        double* ptr = nullptr;
+        int nz = 0;
+    };
+    std::vector<Member> mem;
+    struct Ctx {
+        mom6b_halo_group* g;
+        int rank;
+    };
+    std::vector<std::unique_ptr<Ctx>> ctx;
+    int rank_at(int x, int y) const { return (x >= 0 && x < px && y >= 0 && y < py) ? x * py + y : -1; }
+};
+
+static bool group_meet(mom6b_halo_group* g)
+{
+    std::unique_lock<std::mutex> lk(g->mu);
+    if (g->failed) return false;
+    const unsigned long long my = g->gen;
+    if (++g->arrived == (int)g->mem.size()) {
+        g->arrived = 0;
+        ++g->gen;
+        g->cv.notify_all();
+        return true;
+    }
+    const bool met = g->cv.wait_for(lk, std::chrono::duration<double>(g->timeout_s),
+                                    [&] { return g->gen != my || g->failed; });
+    if (!met || g->failed) {
+        g->failed = true;
+        g->cv.notify_all();
+        return false;
+    }
+    return true;
+}
+
+static int group_exchange(void* vctx, double* field, int nz, int kind, void* stream)
+{
+    (void)kind;
+    auto* c = (mom6b_halo_group::Ctx*)vctx;
+    mom6b_halo_group* g = c->g;
+    const int r = c->rank;
+    cudaStream_t s = (cudaStream_t)stream;
+    mom6b_halo_group::Member& me = g->mem[r];
+    me.ptr = field;
+    me.nz = nz;
+    if (cudaStreamSynchronize(s) != cudaSuccess || !group_meet(g)) {
+        std::lock_guard<std::mutex> lk(g->mu);
+        g->failed = true;
+        g->cv.notify_all();
+        return 1;
+    }
+    const int hw = 3;
+    const Dims& D = me.m->D;
+    const int x = r / g->py, y = r % g->py;
+    const bool hw_ = g->rank_at(x - 1, y) >= 0, he = g->rank_at(x + 1, y) >= 0;
+    const bool hs = g->rank_at(x, y - 1) >= 0, hn = g->rank_at(x, y + 1) >= 0;
+    const int r0 = hs ? hw : 0, r1 = hn ? D.n2 - hw : D.n2;   // east / west strip rows
+    const int c0 = hw_ ? hw : 0, c1 = he ? D.n1 - hw : D.n1;  // north / south strip columns
+    int bad = 0;
+    for (int dy = -1; dy <= 1 && !bad; ++dy)
+        for (int dx = -1; dx <= 1 && !bad; ++dx) {
+            if (!dx && !dy) continue;
+            const int nr = g->rank_at(x + dx, y + dy);
+            if (nr < 0) continue;
+            const mom6b_halo_group::Member& nb = g->mem[nr];
+            const Dims& N = nb.m->D;
+            if (nb.nz != nz) { bad = 1; break; }
+            // this member's receive box and the neighbour's send box (0-based)
+            const int mx0 = dx > 0 ? D.n1 - hw : (dx < 0 ? 0 : c0);
+            const int mx1 = dx > 0 ? D.n1 : (dx < 0 ? hw : c1);
+            const int my0 = dy > 0 ? D.n2 - hw : (dy < 0 ? 0 : r0);
+            const int my1 = dy > 0 ? D.n2 : (dy < 0 ? hw : r1);
+            const int sx0 = dx > 0 ? hw : (dx < 0 ? N.n1 - 2 * hw : c0);
+            const int sy0 = dy > 0 ? hw : (dy < 0 ? N.n2 - 2 * hw : r0);
+            const size_t w = (size_t)(mx1 - mx0), h = (size_t)(my1 - my0);
+            const int dd = me.m->cfg.device, sd = nb.m->cfg.device;
+            cudaError_t e;
+            if (dd == sd) {
+                cudaMemcpy3DParms p = {};
+                p.srcPtr = make_cudaPitchedPtr((void*)nb.ptr, (size_t)N.n1 * 8, N.n1, N.n2);
+                p.srcPos = make_cudaPos((size_t)sx0 * 8, sy0, 0);
+                p.dstPtr = make_cudaPitchedPtr((void*)field, (size_t)D.n1 * 8, D.n1, D.n2);
+                p.dstPos = make_cudaPos((size_t)mx0 * 8, my0, 0);
+                p.extent = make_cudaExtent(w * 8, h, (size_t)nz);
+                p.kind = cudaMemcpyDeviceToDevice;
+                e = cudaMemcpy3DAsync(&p, s);
+            } else {
+                cudaMemcpy3DPeerParms p = {};
+                p.srcPtr = make_cudaPitchedPtr((void*)nb.ptr, (size_t)N.n1 * 8, N.n1, N.n2);
+                p.srcPos = make_cudaPos((size_t)sx0 * 8, sy0, 0);
+                p.srcDevice = sd;
+                p.dstPtr = make_cudaPitchedPtr((void*)field, (size_t)D.n1 * 8, D.n1, D.n2);
+                p.dstPos = make_cudaPos((size_t)mx0 * 8, my0, 0);
+                p.dstDevice = dd;
+                p.extent = make_cudaExtent(w * 8, h, (size_t)nz);
+                e = cudaMemcpy3DPeerAsync(&p, s);
+            }
+            if (e != cudaSuccess) bad = 1;
+        }
+    if (bad || cudaStreamSynchronize(s) != cudaSuccess) {
+        std::lock_guard<std::mutex> lk(g->mu);
+        g->failed = true;
+        g->cv.notify_all();
+        return 1;
+    }
+    return group_meet(g) ? 0 : 1;
+}
+
+extern "C" int mom6b_halo_group_create(int npes_x, int npes_y, double timeout_s,
+                                       mom6b_halo_group** out)
+{
+    if (!out || npes_x < 1 || npes_y < 1 || npes_x * npes_y > 4096 || !(timeout_s > 0.0))
+        return fail(MOM6B_ERR_ARG, "bad halo group layout");
+    auto g = std::make_unique<mom6b_halo_group>();
+    g->px = npes_x;
+    g->py = npes_y;
+    g->timeout_s = timeout_s;
+    g->mem.resize((size_t)npes_x * npes_y);
+    *out = g.release();
+    return MOM6B_OK;
+}
+
+extern "C" int mom6b_halo_group_join(mom6b_halo_group* g, mom6b_model* m, int rank)
+{
+    if (!g || !m || rank < 0 || rank >= (int)g->mem.size())
+        return fail(MOM6B_ERR_ARG, "bad halo group member");
+    if (g->mem[rank].m) return fail(MOM6B_ERR_STATE, "rank already joined");
+    const int x = rank / g->py, y = rank % g->py;
+    const int want = (g->rank_at(x - 1, y) >= 0 ? MOM6B_CUT_W : 0) |
+                     (g->rank_at(x + 1, y) >= 0 ? MOM6B_CUT_E : 0) |
+                     (g->rank_at(x, y - 1) >= 0 ? MOM6B_CUT_S : 0) |
+                     (g->rank_at(x, y + 1) >= 0 ? MOM6B_CUT_N : 0);
+    if (m->cfg.cuts != want) return fail(MOM6B_ERR_ARG, "model cuts do not match its position");
+    // the neighbours along each axis share the other axis' size
+    for (int o = 0; o < (int)g->mem.size(); ++o) {
+        const mom6b_model* q = g->mem[o].m;
+        if (!q) continue;
+        const int ox = o / g->py, oy = o % g->py;
+        if ((ox == x && q->D.n1 != m->D.n1) || (oy == y && q->D.n2 != m->D.n2))
+            return fail(MOM6B_ERR_ARG, "subdomain sizes do not tile the layout");
+    }
+    g->mem[rank].m = m;
+    g->ctx.push_back(std::make_unique<mom6b_halo_group::Ctx>(mom6b_halo_group::Ctx{g, rank}));
+    return mom6b_set_exchange(m, group_exchange, g->ctx.back().get());
+}
+
+extern "C" void mom6b_halo_group_destroy(mom6b_halo_group* g) { delete g; }
 
 extern "C" int mom6b_set_hor_visc(mom6b_model* m, const mom6b_hor_visc* o)
 {

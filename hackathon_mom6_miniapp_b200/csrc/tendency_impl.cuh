@@ -21,7 +21,9 @@
 // the FP64 result equals the serial Fortran bit for bit.  Two reference
 // quirks are reproduced: hArea_u(:, js-1) and hArea_v(is-1, :) are never
 // written by CorAdCalc and enter q as zero (mom6_coriolis_serial.F90:142-152
-// vs :162-168).
+// vs :162-168).  In a subdomain of a decomposed run (Dims' cut flags) the
+// points on a cut are interior: there hArea exists, and the u (v) update
+// reaches ie (je) at an east (north) cut.
 #pragma once
 
 #include "kernels.h"
@@ -157,8 +159,9 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
     // this thread's bases, loaded before the intermediates are evaluated
     const int Io = i0 + (int)threadIdx.x;
     const int jo = j0 + (int)threadIdx.y;
-    const bool do_u = Io <= D.ie - 1 && jo <= D.je;
-    const bool do_v = Io <= D.ie && jo <= D.je - 1;
+    // at an east / north cut the face on it is interior and updated
+    const bool do_u = Io <= D.ie - 1 + D.ce && jo <= D.je;
+    const bool do_v = Io <= D.ie && jo <= D.je - 1 + D.cn;
     const size_t oo = koff + (size_t)(jo - 1) * D.n1 + (Io - 1);
     const R ub = do_u ? ubase[oo] : R(0.0);
     const R vb = do_v ? vbase[oo] : R(0.0);
@@ -188,9 +191,9 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
                 R absv = COR(I, J) + rel;
                 R aT00 = G2(areaT, I, J), aT10 = G2(areaT, I + 1, J),
                        aT01 = G2(areaT, I, J + 1), aT11 = G2(areaT, I + 1, J + 1);
-                R hAu0 = (J >= D.js) ? R(0.5) * ((aT00 * h00) + (aT10 * h10)) : R(0.0);
+                R hAu0 = (J >= D.js - D.cs) ? R(0.5) * ((aT00 * h00) + (aT10 * h10)) : R(0.0);
                 R hAu1 = R(0.5) * ((aT01 * h01) + (aT11 * h11));
-                R hAv0 = (I >= D.is) ? R(0.5) * ((aT00 * h00) + (aT01 * h01)) : R(0.0);
+                R hAv0 = (I >= D.is - D.cw) ? R(0.5) * ((aT00 * h00) + (aT01 * h01)) : R(0.0);
                 R hAv1 = R(0.5) * ((aT10 * h10) + (aT11 * h11));
                 R hArea_q = (hAu0 + hAu1) + (hAv0 + hAv1);
                 R Ih_q = td_div<FAST>(G2(Area_q, I, J), hArea_q + R(1.0e-20));
@@ -266,7 +269,7 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
     const int I = i0 + (int)threadIdx.x;
     const int j = j0 + (int)threadIdx.y;
     // ---- u point (I, j) ---------------------------------------------------
-    if (I <= D.ie - 1 && j <= D.je) {
+    if (I <= D.ie - 1 + D.ce && j <= D.je) {
         R IdxCu = G2(IdxCu, I, j);
         R KEx = (KE(I + 1, j) - KE(I, j)) * IdxCu;
         R CAu;
@@ -301,7 +304,7 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
         if (DIAG && !EXTV) dfu[oo] = diffu;
     }
     // ---- v point (i, J) = (I, j) -------------------------------------------
-    if (I <= D.ie && j <= D.je - 1) {
+    if (I <= D.ie && j <= D.je - 1 + D.cn) {
         const int i = I, J = j;
         R IdyCv = G2(IdyCv, i, J);
         R KEy = (KE(i, J + 1) - KE(i, J)) * IdyCv;

@@ -152,4 +152,55 @@ class HaloExchange:
         return a
 
 
-__all__ = ["Decomposition", "HaloExchange"]
+class LocalBoard:
+    """Where the subdomains held by the threads of one process meet: one slot
+    per rank and a barrier (timeout in seconds) for a LocalHaloExchange."""
+
+    def __init__(self, world, timeout=120.0):
+        import threading
+        self.barrier = threading.Barrier(world, timeout=timeout)
+        self.slots = [None] * world
+
+
+class LocalHaloExchange(HaloExchange):
+    """The same 8-direction exchange among subdomains held by threads of one
+    process (one model per thread, on one or several GPUs): every rank packs
+    its send strips, meets the others at the board's barrier, unpacks its
+    neighbours' strips in the order E, W, N, S, NE, NW, SE, SW, and meets them
+    again before the strips may change.  CUDA tensors are packed and unpacked
+    on the current stream, which is synchronised before each meeting."""
+
+    def __init__(self, decomp: Decomposition, board: LocalBoard):
+        super().__init__(decomp)
+        self.board = board
+
+    def exchange(self, a):
+        n2, n1 = a.shape[-2], a.shape[-1]
+        if (n1, n2) != (self.d.n1, self.d.n2):
+            raise ValueError(f"array {tuple(a.shape)} does not match the data domain "
+                             f"({self.d.n2}, {self.d.n1})")
+        send, recv = self._regions(n1, n2)
+        packed = {}
+        for k in _DIRS:
+            if self.nbr[k] is not None:
+                rs, cs = send[k]
+                packed[k] = a[..., rs, cs].clone()
+        self._sync(a)
+        self.board.slots[self.d.rank] = packed
+        self.board.barrier.wait()
+        for k in _DIRS:
+            if self.nbr[k] is not None:
+                rr, cr = recv[k]
+                a[..., rr, cr] = self.board.slots[self.nbr[k]][_OPPOSITE[k]].to(a.device)
+        self._sync(a)
+        self.board.barrier.wait()
+        return a
+
+    @staticmethod
+    def _sync(a):
+        if a.is_cuda:
+            import torch
+            torch.cuda.current_stream(a.device).synchronize()
+
+
+__all__ = ["Decomposition", "HaloExchange", "LocalBoard", "LocalHaloExchange"]

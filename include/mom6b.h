@@ -99,7 +99,20 @@ typedef struct mom6b_config {
     int mixed_f32_vertvisc;/* MOM6B_MIXED only, opt-in: the vertical tridiagonal
                               elimination in FP32 as well (outside the mixed
                               form's definition, which eliminates in FP64) */
+    /* One subdomain of a 2-D decomposition (mpi_domain_init,
+     * mom6_mpi_domain.F90:57-137, non-periodic).  ni_global, nj_global: the
+     * whole domain's ni, nj (0: this model is the whole domain); ni, nj
+     * above are then this subdomain's (its compute width + 4), and i_offset,
+     * j_offset the 0-based offsets of its compute domain in the global one.
+     * The grid and the initial state are those of the global points
+     * (init_ocean_grid_mpi, :144-258).  cuts: MOM6B_CUT_* bits, the sides
+     * with a neighbouring subdomain; a step with cuts needs a halo exchange
+     * (mom6b_set_exchange). */
+    int ni_global, nj_global, i_offset, j_offset;
+    int cuts;
 } mom6b_config;
+
+enum { MOM6B_CUT_W = 1, MOM6B_CUT_E = 2, MOM6B_CUT_S = 4, MOM6B_CUT_N = 8 };
 
 typedef struct mom6b_model mom6b_model;
 
@@ -147,6 +160,47 @@ int mom6b_verify(mom6b_model *m, double *out7);
  * reports MOM6B_ERR_TIMEOUT (the step's barotropic outputs are then
  * incomplete).  The model stays usable: set stall_test = 0 and step again. */
 int mom6b_set_wait_limit(mom6b_model *m, long long cycles, int stall_test);
+
+/* ---- domain decomposition (no reference counterpart in src/cuda_c: the
+ * reference decomposes in its MPI drivers, rk2_mpi_cuda_c_driver.F90:248-577,
+ * with halo_exchange_3d / _2d of mom6_mpi_halo_omp.F90:106-427) ----
+ *
+ * A halo exchange refreshes the halo of one of the model's device fields
+ * (n1 x n2 x nz, Fortran order; kind 0 h points, 1 u faces, 2 v faces) from
+ * the neighbouring subdomains.  The step calls it from the host thread that
+ * called mom6b_step, with the model's stream, at these points: up, vp before
+ * the predictor continuity, the predictor's h after it, u, v before the
+ * corrector continuity, and the barotropic eta, ubt, vbt before every
+ * substep.  It returns 0, or nonzero to abandon the step (mom6b_step then
+ * returns MOM6B_ERR_STATE).  Work it enqueues on the stream is ordered with
+ * the step's kernels.  With cuts, the ranges that stop short of a wall
+ * (velocity update, CorAdCalc's u and v points) reach the cut, CorAdCalc's
+ * and hor_visc's intermediates on the cut exist, and the barotropic loop
+ * runs one launch per substep on ranges two points into the halo, so that
+ * the decomposed step equals the single-domain one bit for bit (exact
+ * form).  Supported: MOM6B_FP64 without halo fill, the default Sadourny
+ * Coriolis and Laplacian hor_visc, zonal continuity, no remnant, no
+ * diagnostics, no surrogate; the step is not captured in a CUDA graph. */
+typedef int (*mom6b_exchange_fn)(void *ctx, double *field, int nz, int kind, void *stream);
+int mom6b_set_exchange(mom6b_model *m, mom6b_exchange_fn fn, void *ctx);
+
+/* An in-process exchange among npes_x * npes_y subdomain models (one host
+ * thread per model, on one or several devices; rank = pos_x * npes_y +
+ * pos_y as MPI_Cart_create orders a 2-D grid).  Each exchange posts the
+ * field, waits for every member, copies each neighbour's edge strips into
+ * this model's halo (peer copies between devices), and waits again before
+ * the owner may change them.  East/west strips span the compute rows plus
+ * the halo rows on a side without a north/south neighbour, north/south
+ * strips the compute columns plus the halo columns on a side without an
+ * east/west neighbour, the corner blocks come from the diagonal neighbours,
+ * so every halo point is written once.  A member that does not arrive
+ * within timeout_s seconds fails the exchange of the others. */
+typedef struct mom6b_halo_group mom6b_halo_group;
+int mom6b_halo_group_create(int npes_x, int npes_y, double timeout_s, mom6b_halo_group **out);
+/* Install the group's exchange on m as member `rank` (m's cuts must be its
+ * position's). */
+int mom6b_halo_group_join(mom6b_halo_group *g, mom6b_model *m, int rank);
+void mom6b_halo_group_destroy(mom6b_halo_group *g);
 
 /* Per-kernel launch accounting: number of kernels of this library launched
  * on the model's stream since the last reset. */

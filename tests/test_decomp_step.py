@@ -113,3 +113,48 @@ def test_decomposed_step_other_first_direction():
     for rank, res in out:
         bad = {k: v for k, v in res.items() if k != "finite" and v}
         assert not bad, (rank, bad)
+
+
+def test_decomposed_step_in_threads_with_the_local_exchange():
+    """The same decomposition with the subdomains held by threads of one
+    process, exchanging through decomp.LocalHaloExchange (the in-process form
+    of the exchange that Model.set_exchange takes): bit-identical as well."""
+    import threading
+
+    import torch
+    from hackathon_mom6_miniapp_b200.decomp import Decomposition, LocalBoard, LocalHaloExchange
+    from oracle.pyoracle import CUT_E, CUT_N, CUT_S, CUT_W, Oracle
+    px, py, NI, NJ, nk, nbt, nsteps = 2, 2, 27, 30, 4, 6, 2
+    board = LocalBoard(px * py, timeout=120.0)
+    locs, errs = [], []
+    for r in range(px * py):
+        d = Decomposition(NI - 4, NJ - 4, px, py, r)
+        cuts = sum(bit for side, bit in (("W", CUT_W), ("E", CUT_E), ("S", CUT_S),
+                                         ("N", CUT_N)) if d.neighbour(side) is not None)
+        o = Oracle(d.ni_local + 4, d.nj_local + 4, nk, nbt, init_mode=1, bc_fill=False,
+                   subdomain=(NI, NJ, d.i_offset, d.j_offset, cuts))
+        x = LocalHaloExchange(d, board)
+        o.set_exchange(lambda a, kind, x=x: x.exchange(torch.from_numpy(a.T)))
+        locs.append((d, o))
+
+    def run(o):
+        try:
+            o.step(nsteps)
+        except Exception as e:
+            errs.append(e)
+
+    ts = [threading.Thread(target=run, args=(o,)) for _, o in locs]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join(timeout=300)
+    assert not errs
+    glob = Oracle(NI, NJ, nk, nbt, init_mode=1, bc_fill=False)
+    glob.step(nsteps)
+    for d, o in locs:
+        i0, i1, j0, j1 = o.is_ - 1, o.ie, o.js - 1, o.je
+        for name in ("u", "v", "h", "eta", "ubt_av", "vbt_av"):
+            a = o.get(name)[i0:i1, j0:j1]
+            g = glob.get(name)[i0 + d.i_offset:i1 + d.i_offset, j0 + d.j_offset:j1 + d.j_offset]
+            assert np.array_equal(a, g), (d.rank, name)
+        o.set_exchange(None)
