@@ -220,3 +220,53 @@ def test_barrier_timeout_is_reported_and_recovers():
     ref.synchronize()
     for n in STATE:
         assert np.array_equal(g.get(n), ref.get(n)), n
+
+
+def _golden_module():
+    import importlib.util
+    import os
+    path = os.path.join(os.path.dirname(__file__), "golden", "make_golden.py")
+    spec = importlib.util.spec_from_file_location("make_golden", path)
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    return mg
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["ref_13x11x5", "cfg_13x11x5", "ref_36x30x8", "cfg_36x30x8",
+                                  "ref_20x16x5", "cfg_20x16x5"])
+@pytest.mark.parametrize("exact", [True, False])
+def test_golden_fixtures(case, exact):
+    """The committed oracle fixtures (tests/golden): the exact form equals them
+    bit for bit, the fast form within the north-star 1e-12 per field."""
+    import os
+    from hackathon_mom6_miniapp_b200 import Model
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", f"{case}.npz"))
+    mode = INIT_REF if case.startswith("ref") else INIT_CFG
+    m = Model(int(g["ni"]), int(g["nj"]), int(g["nk"]), int(g["bt_nsteps"]), mode,
+              seed=int(g["seed"]), dt=float(g["dt"]), exact=exact)
+    m.step(int(g["nsteps"]))
+    for n in ("h", "u", "v", "eta", "ubt_av", "vbt_av"):
+        a = m.get(n)
+        if exact:
+            assert np.array_equal(a, g[n]), n
+        else:
+            assert rel_l2(a, g[n]) <= TOL, (n, rel_l2(a, g[n]))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["ref_180x180x75", "cfg_180x180x75"])
+def test_golden_hashes_180(case):
+    """180x180x75 after 3 steps, exact form: the SHA-256 of every field equals
+    the committed oracle hash (tests/golden/hashes_180x180x75.json)."""
+    import json
+    import os
+    from hackathon_mom6_miniapp_b200 import Model
+    mg = _golden_module()
+    with open(os.path.join(os.path.dirname(__file__), "golden", "hashes_180x180x75.json")) as f:
+        c = json.load(f)[case]
+    m = Model(c["ni"], c["nj"], c["nk"], c["bt_nsteps"], c["mode"], seed=c["seed"], dt=c["dt"],
+              exact=True)
+    m.step(c["nsteps"])
+    for n, h in c["fields"].items():
+        assert mg.field_hash(m.get(n)) == h, n
