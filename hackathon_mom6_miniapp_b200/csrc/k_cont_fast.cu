@@ -505,8 +505,8 @@ typedef CUresult (*CfEncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, vo
                                const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
                                CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-cudaError_t tma_map_field3d(CUtensorMap* map, const double* base, int n1, int n2, int nk,
-                            int box_w)
+cudaError_t tma_map_box3d(CUtensorMap* map, const double* base, int n1, int n2, int nk,
+                          int box_w, int box_h, int box_d)
 {
     static CfEncodeFn fn = nullptr;
     if (!fn) {
@@ -518,12 +518,12 @@ cudaError_t tma_map_field3d(CUtensorMap* map, const double* base, int n1, int n2
             return cudaErrorNotSupported;
         fn = (CfEncodeFn)p;
     }
-    if (((uintptr_t)base & 15u) || (n1 & 1) || (box_w & 1) || box_w > 256 || nk > 256 ||
-        nk < 1)
+    if (((uintptr_t)base & 15u) || (n1 & 1) || (box_w & 1) || box_w > 256 || box_h > 256 ||
+        box_d > 256 || box_w < 2 || box_h < 1 || box_d < 1 || nk < 1)
         return cudaErrorNotSupported;
     cuuint64_t gdim[3] = {(cuuint64_t)n1, (cuuint64_t)n2, (cuuint64_t)nk};
     cuuint64_t gstride[2] = {(cuuint64_t)n1 * 8, (cuuint64_t)n1 * (cuuint64_t)n2 * 8};
-    cuuint32_t box[3] = {(cuuint32_t)box_w, 1, (cuuint32_t)nk};
+    cuuint32_t box[3] = {(cuuint32_t)box_w, (cuuint32_t)box_h, (cuuint32_t)box_d};
     cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double*>(base), gdim,
                     gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -531,21 +531,34 @@ cudaError_t tma_map_field3d(CUtensorMap* map, const double* base, int n1, int n2
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorNotSupported;
 }
 
+cudaError_t tma_map_field3d(CUtensorMap* map, const double* base, int n1, int n2, int nk,
+                            int box_w)
+{
+    return tma_map_box3d(map, base, n1, n2, nk, box_w, 1, nk);
+}
+
 // Tensor maps are encoded once per (field address, shape, box) and kept.
-static bool cf_map(const double* base, const Dims& D, int box_w, CUtensorMap* out)
+bool tma_map_cached(const double* base, int n1, int n2, int nk, int box_w, int box_h,
+                    int box_d, CUtensorMap* out)
 {
     static std::mutex mu;
-    static std::map<std::tuple<const void*, int, int, int, int>, CUtensorMap> maps;
-    const auto key = std::make_tuple((const void*)base, D.n1, D.n2, D.nk, box_w);
+    static std::map<std::tuple<const void*, int, int, int, int, int, int>, CUtensorMap> maps;
+    const auto key = std::make_tuple((const void*)base, n1, n2, nk, box_w, box_h, box_d);
     std::lock_guard<std::mutex> lock(mu);
     auto it = maps.find(key);
     if (it == maps.end()) {
         CUtensorMap m;
-        if (tma_map_field3d(&m, base, D.n1, D.n2, D.nk, box_w) != cudaSuccess) return false;
+        if (tma_map_box3d(&m, base, n1, n2, nk, box_w, box_h, box_d) != cudaSuccess)
+            return false;
         it = maps.emplace(key, m).first;
     }
     *out = it->second;
     return true;
+}
+
+static bool cf_map(const double* base, const Dims& D, int box_w, CUtensorMap* out)
+{
+    return tma_map_cached(base, D.n1, D.n2, D.nk, box_w, 1, D.nk, out);
 }
 
 bool continuity_fast_fits(const Dims& D) { return D.nk >= 1 && D.nk <= 128; }

@@ -10,10 +10,11 @@ namespace mom6b {
 cudaError_t launch_tendency_fast(const Dims& D, const Metrics& M, const UniMetrics& U,
                                  const double* uin, const double* vin, const double* h,
                                  const double* ubase, const double* vbase, double* uout,
-                                 double* vout, double coef, double h_neglect, cudaStream_t s)
+                                 double* vout, double coef, double h_neglect, cudaStream_t s,
+                                 int* status)
 {
     return launch_tendency_t<double, true>(D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef,
-                                           h_neglect, s);
+                                           h_neglect, s, nullptr, nullptr, 1, false, status);
 }
 
 } // namespace mom6b

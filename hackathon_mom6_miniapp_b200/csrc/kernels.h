@@ -83,12 +83,15 @@ cudaError_t launch_tendency(const Dims& D, const Metrics& M, const UniMetrics& U
                             const double* ubase, const double* vbase, double* uout,
                             double* vout, double coef, double h_neglect, cudaStream_t s,
                             double* diffu = nullptr, double* diffv = nullptr, int scheme = 1,
-                            bool ext_visc = false);
+                            bool ext_visc = false, int* status = nullptr);
 // The fast FP64 form (k_tendency_fast.cu): Sadourny scheme, no diagnostics.
+// status (optional): with it, the uniform-metric Sadourny tendency stages its
+// tiles with TMA and records kDevTimeout there if a tile never lands.
 cudaError_t launch_tendency_fast(const Dims& D, const Metrics& M, const UniMetrics& U,
                                  const double* uin, const double* vin, const double* h,
                                  const double* ubase, const double* vbase, double* uout,
-                                 double* vout, double coef, double h_neglect, cudaStream_t s);
+                                 double* vout, double coef, double h_neglect, cudaStream_t s,
+                                 int* status = nullptr);
 // rem_u, rem_v (both or neither): also the vertical-viscosity remnant of
 // every u / v column (vert_visc_remnant).
 cudaError_t launch_vertvisc(const Dims& D, const Metrics& M, double* u, double* v,

@@ -750,10 +750,11 @@ static int enqueue_step(mom6b_model* m)
     CK(timed(m, s, "tendency", [&] {
         if (td_fast)
             return launch_tendency_fast(D, M, m->U, m->u, m->v, m->h0, m->u, m->v, m->up, m->vp,
-                                        dt, hv_neglect, s);
+                                        dt, hv_neglect, s, m->bt.status);
         return launch_tendency(D, M, m->U, m->u, m->v, m->h0, m->u, m->v, m->up, m->vp, dt,
                                hv_neglect, s, m->diag_driver ? m->dg_du : nullptr,
-                               m->diag_driver ? m->dg_dv : nullptr, m->cor_scheme); }));
+                               m->diag_driver ? m->dg_dv : nullptr, m->cor_scheme, false,
+                               m->bt.status); }));
     }
     const bool vv_fast = !c.exact && !m->remnant && vertvisc_fast_fits(D);
     CK(timed(m, s, "vertvisc", [&] {
@@ -786,9 +787,10 @@ static int enqueue_step(mom6b_model* m)
     CK(timed(m, s, "tendency", [&] {
         if (td_fast)
             return launch_tendency_fast(D, M, m->U, m->up, m->vp, m->hB, m->u, m->v, m->u, m->v,
-                                        0.5 * dt, hv_neglect, s);
+                                        0.5 * dt, hv_neglect, s, m->bt.status);
         return launch_tendency(D, M, m->U, m->up, m->vp, m->hB, m->u, m->v, m->u, m->v,
-                               0.5 * dt, hv_neglect, s, nullptr, nullptr, m->cor_scheme); }));
+                               0.5 * dt, hv_neglect, s, nullptr, nullptr, m->cor_scheme, false,
+                               m->bt.status); }));
     }
     CK(timed(m, s, "vertvisc", [&] {
         if (vv_fast)

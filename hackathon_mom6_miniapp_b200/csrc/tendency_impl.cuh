@@ -27,6 +27,7 @@
 #pragma once
 
 #include "kernels.h"
+#include "tma.cuh"
 
 namespace mom6b {
 
@@ -94,21 +95,38 @@ __device__ __forceinline__ double td_div(double a, double b)
 template <bool FAST>
 __device__ __forceinline__ float td_div(float a, float b) { return div_r(a, b); }
 
+// TMA: the u, v, h tiles of a layer arrive as three TMA box loads
+// ({SX, SY, 1} of the fields' tensor maps tmaps[0..2]) issued by one thread
+// into 128-byte-aligned double buffers, completing on one mbarrier per
+// buffer; a load that does not land within the wait budget records
+// kDevTimeout in *status and the CTA returns.  FP64 Sadourny tiles only: the
+// box row (SX doubles) and its x origin i0 - 2 = is - 2 + TX bx (even) meet
+// the unit's 16-byte rules.  Otherwise every thread copies its share of the
+// tile element by element with cp.async.
 template <int TX, int TY, bool UNI, typename R, bool DIAG = false, int COR = 1,
-          bool EXTV = false, bool FAST = false>
+          bool EXTV = false, bool FAST = false, bool TMA = false>
 __device__ __forceinline__ void
 tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __restrict__ uin,
               const R* __restrict__ vin, const R* __restrict__ h,
               const R* ubase, const R* vbase, R* uout, R* vout,
               R coef, R h_neglect, int k0, int KC, int bx, int by, int bz,
-              R* dfu = nullptr, R* dfv = nullptr)
+              R* dfu = nullptr, R* dfv = nullptr, const CUtensorMap* tmaps = nullptr,
+              int* status = nullptr)
 {
     constexpr int W = COR >= 2 ? 1 : 0;      // the Arakawa schemes' extra column and row
     constexpr int SX = TX + 2 + W, SY = TY + 2 + W;  // staged: [i0-1, i0+TX+W] x [j0-1, j0+TY+W]
     constexpr int CX = TX + 1 + W, CY = TY + 1 + W;  // intermediates
     constexpr int NT = TX * TY;
     constexpr int NS = (SX * SY + NT - 1) / NT;  // staged elements per thread
-    __shared__ R s_u[2][SY][SX], s_v[2][SY][SX], s_h[2][SY][SX];
+    static_assert(!TMA || (sizeof(R) == 8 && COR <= 1 && (SX * sizeof(R)) % 16 == 0 && TX % 2 == 0),
+                  "TMA tiles need 16-byte rows and even x origins");
+    // the element-wise staging buffers, and the TMA buffers (each tile a
+    // multiple of 128 bytes so that every TMA destination is 128-byte aligned)
+    constexpr int AX = TMA ? 1 : SX, AY = TMA ? 1 : SY, AB = TMA ? 1 : 2;
+    constexpr int TPAD = ((SX * SY + 15) / 16) * 16;
+    __shared__ R s_u[AB][AY][AX], s_v[AB][AY][AX], s_h[AB][AY][AX];
+    __shared__ __align__(128) R s_t[TMA ? 2 * 3 * TPAD : 1];
+    __shared__ __align__(8) uint64_t s_tbar[2];
     __shared__ R s_q[CY][CX], s_sxy[CY][CX];   // corners  [i0-1, i0+TX-1] x [j0-1, j0+TY-1]
     __shared__ R s_ke[CY][CX], s_sxx[CY][CX];  // centres  [i0, i0+TX] x [j0, j0+TY]
     __shared__ R s_uh[CY][CX];                 // u-faces  [i0-1, i0+TX-1] x [j0, j0+TY]
@@ -134,27 +152,66 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
         go[q] = gok[q] ? (size_t)(j - 1) * D.n1 + (size_t)(i - 1) : 0;
     }
     auto stage = [&](int k, int b) {
-        const size_t koff = (size_t)(k - 1) * (size_t)D.plane;
+        if constexpr (TMA) {
+            if (tid == 0) {
+                tma_bar_expect(&s_tbar[b], (uint32_t)(3 * SX * SY * sizeof(R)));
 #pragma unroll
-        for (int q = 0; q < NS; ++q) {
-            if (sp[q] >= 0) {
-                const size_t o = gok[q] ? koff + go[q] : 0;
-                cp_async_elem(&s_u[b][0][0] + sp[q], uin + o, gok[q]);
-                cp_async_elem(&s_v[b][0][0] + sp[q], vin + o, gok[q]);
-                cp_async_elem(&s_h[b][0][0] + sp[q], h + o, gok[q]);
+                for (int f = 0; f < 3; ++f)
+                    tma_load_3d(&s_t[(b * 3 + f) * TPAD], &tmaps[f], i0 - 2, j0 - 2, k - 1,
+                                &s_tbar[b]);
             }
+        } else {
+            const size_t koff = (size_t)(k - 1) * (size_t)D.plane;
+#pragma unroll
+            for (int q = 0; q < NS; ++q) {
+                if (sp[q] >= 0) {
+                    const size_t o = gok[q] ? koff + go[q] : 0;
+                    cp_async_elem(&s_u[b][0][0] + sp[q], uin + o, gok[q]);
+                    cp_async_elem(&s_v[b][0][0] + sp[q], vin + o, gok[q]);
+                    cp_async_elem(&s_h[b][0][0] + sp[q], h + o, gok[q]);
+                }
+            }
+            cp_async_commit();
         }
-        cp_async_commit();
     };
+    if constexpr (TMA) {
+        if (tid == 0) {
+            tma_prefetch_map(&tmaps[0]);
+            tma_prefetch_map(&tmaps[1]);
+            tma_prefetch_map(&tmaps[2]);
+            tma_bar_init(&s_tbar[0], 1);
+            tma_bar_init(&s_tbar[1], 1);
+        }
+        __syncthreads();
+    }
     if (kb <= ke) stage(kb, 0);
   for (int k = kb; k <= ke; ++k) {
     const size_t koff = (size_t)(k - 1) * (size_t)D.plane;
     const int b = (k - kb) & 1;
-    cp_async_wait_all();
     // layer k's tiles are visible to all threads, and every thread is done
     // with layer k-1 (its outputs read buffer b^1 and the intermediates)
-    __syncthreads();
+    if constexpr (TMA) {
+        // buffer b's (k - kb) / 2-th use completes its phase of that parity
+        const bool late = !tma_bar_wait(&s_tbar[b], (uint32_t)(((k - kb) >> 1) & 1),
+                                        kBtDefaultWait);
+        if (__syncthreads_or(late)) {
+            if (tid == 0) {
+                if (status) atomicExch(status, kDevTimeout);
+                // the load still in flight lands in this CTA's shared memory:
+                // wait for it once more (bounded) before the CTA exits
+                tma_bar_wait(&s_tbar[b], (uint32_t)(((k - kb) >> 1) & 1), kBtDefaultWait);
+            }
+            __syncthreads();
+            return;
+        }
+    } else {
+        cp_async_wait_all();
+        __syncthreads();
+    }
     if (k < ke) stage(k + 1, b ^ 1);
+    const R* t_u = TMA ? &s_t[(b * 3 + 0) * TPAD] : &s_u[b][0][0];
+    const R* t_v = TMA ? &s_t[(b * 3 + 1) * TPAD] : &s_v[b][0][0];
+    const R* t_h = TMA ? &s_t[(b * 3 + 2) * TPAD] : &s_h[b][0][0];
 
     // this thread's bases, loaded before the intermediates are evaluated
     const int Io = i0 + (int)threadIdx.x;
@@ -166,9 +223,9 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
     const R ub = do_u ? ubase[oo] : R(0.0);
     const R vb = do_v ? vbase[oo] : R(0.0);
 
-#define SU(i, j) s_u[b][(j) - (j0 - 1)][(i) - (i0 - 1)]
-#define SV(i, j) s_v[b][(j) - (j0 - 1)][(i) - (i0 - 1)]
-#define SH(i, j) s_h[b][(j) - (j0 - 1)][(i) - (i0 - 1)]
+#define SU(i, j) t_u[((j) - (j0 - 1)) * SX + ((i) - (i0 - 1))]
+#define SV(i, j) t_v[((j) - (j0 - 1)) * SX + ((i) - (i0 - 1))]
+#define SH(i, j) t_h[((j) - (j0 - 1)) * SX + ((i) - (i0 - 1))]
 #define G2(a, i, j) ((R)(UNI ? U.a : MOM6B_A2(M.a, i, j, D)))
 #define COR(i, j) ((R)(UNI ? U.cor_row[(j) - 1] : MOM6B_A2(M.CoriolisBu, i, j, D)))
 
@@ -370,6 +427,36 @@ k_tendency(Dims D, Metrics M, UniMetrics U, const R* __restrict__ uin,
                                                          (int)blockIdx.z, dfu, dfv);
 }
 
+// The FP64 Sadourny tendency with TMA-staged tiles; the tensor maps of uin,
+// vin, h ride in the parameter bank.
+struct TendMaps {
+    CUtensorMap m[3];
+};
+
+template <int TX, int TY, bool UNI, int MINB, bool FAST>
+__global__ void __launch_bounds__(TX * TY, MINB)
+k_tendency_tma(Dims D, Metrics M, UniMetrics U, const __grid_constant__ TendMaps T,
+               const double* __restrict__ uin, const double* __restrict__ vin,
+               const double* __restrict__ h, const double* ubase, const double* vbase,
+               double* uout, double* vout, double coef, double h_neglect, int k0, int KC,
+               int* status)
+{
+    tendency_tile<TX, TY, UNI, double, false, 1, false, FAST, true>(
+        D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, k0, KC,
+        (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, nullptr, nullptr, T.m, status);
+}
+
+// The tensor maps of a tendency's uin, vin, h ({TX + 2, TY + 2, 1} boxes);
+// false when a field's layout does not qualify (odd n1, unaligned base).
+inline bool tendency_maps(const Dims& D, const double* uin, const double* vin,
+                          const double* h, int TX, int TY, TendMaps& T)
+{
+    return tma_map_cached(uin, D.n1, D.n2, D.nk, TX + 2, TY + 2, 1, &T.m[0]) &&
+           tma_map_cached(vin, D.n1, D.n2, D.nk, TX + 2, TY + 2, 1, &T.m[1]) &&
+           tma_map_cached(h, D.n1, D.n2, D.nk, TX + 2, TY + 2, 1, &T.m[2]) &&
+           (D.is - 2) % 2 == 0;
+}
+
 // diffu, diffv from the general hor_visc kernel (EXTV), every Coriolis scheme.
 template <typename R, int COR>
 void launch_tendency_extv(const Dims& D, const Metrics& M, const UniMetrics& U, dim3 grid,
@@ -429,7 +516,7 @@ cudaError_t launch_tendency_t(const Dims& D, const Metrics& M, const UniMetrics&
                               const R* uin, const R* vin, const R* h, const R* ubase,
                               const R* vbase, R* uout, R* vout, R coef, R h_neglect,
                               cudaStream_t s, R* dfu = nullptr, R* dfv = nullptr,
-                              int scheme = 1, bool ext_visc = false)
+                              int scheme = 1, bool ext_visc = false, int* status = nullptr)
 {
     constexpr int TY = kTendTY;
     int nx = D.ie - D.is + 1, ny = D.je - D.js + 1;
@@ -443,6 +530,15 @@ cudaError_t launch_tendency_t(const Dims& D, const Metrics& M, const UniMetrics&
         // kernels are not instantiated here, so the exact translation unit's
         // instances (same template arguments) are the only ones linked
         if (ext_visc || dfu || scheme != 1) return cudaErrorInvalidValue;
+        if constexpr (sizeof(R) == 8) {
+            TendMaps T;
+            if (U.valid && status && tendency_maps(D, uin, vin, h, kTendTX, TY, T)) {
+                k_tendency_tma<kTendTX, TY, true, 4, true><<<grid, block, 0, s>>>(
+                    D, M, U, T, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, KCh,
+                    status);
+                return cudaGetLastError();
+            }
+        }
         if (U.valid)
             k_tendency<kTendTX, TY, true, R, 4, false, 1, false, true><<<grid, block, 0, s>>>(
                 D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, KCh);
@@ -485,6 +581,15 @@ cudaError_t launch_tendency_t(const Dims& D, const Metrics& M, const UniMetrics&
     // CTAs per SM the registers are held to: 4 (64 registers) is the fastest
     // uniform-metric form on B200 (FP64 tendency 2.01 ms per step against 2.13
     // at 3 and 2.62 uncapped); the 2-D metric form keeps 3 (80 registers).
+    if constexpr (sizeof(R) == 8) {
+        TendMaps T;
+        if (U.valid && status && tendency_maps(D, uin, vin, h, kTendTX, TY, T)) {
+            k_tendency_tma<kTendTX, TY, true, 4, false><<<grid, block, 0, s>>>(
+                D, M, U, T, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, KCh,
+                status);
+            return cudaGetLastError();
+        }
+    }
     if (U.valid)
         k_tendency<kTendTX, TY, true, R, 4><<<grid, block, 0, s>>>(
             D, M, U, uin, vin, h, ubase, vbase, uout, vout, coef, h_neglect, 1, KCh);

@@ -85,5 +85,12 @@ __device__ __forceinline__ void tma_prefetch_map(const CUtensorMap* map)
 // unit's alignment rules (odd n1, misaligned base, box beyond 256).
 cudaError_t tma_map_field3d(CUtensorMap* map, const double* base, int n1, int n2, int nk,
                             int box_w);
+// The same field read in boxes of {box_w, box_h, box_d} (landing as
+// [box_d][box_h][box_w]); tma_map_cached keeps one map per (address, shape,
+// box) and returns false when the layout does not qualify.
+cudaError_t tma_map_box3d(CUtensorMap* map, const double* base, int n1, int n2, int nk,
+                          int box_w, int box_h, int box_d);
+bool tma_map_cached(const double* base, int n1, int n2, int nk, int box_w, int box_h,
+                    int box_d, CUtensorMap* out);
 
 } // namespace mom6b
