@@ -765,6 +765,64 @@ def run_profile_mlp(args):
     net.close()
 
 
+def run_decomp(args):
+    """The decomposed step on one GPU: the 720x720x75 bt50 domain (FP64, no
+    halo fill, seeded state) split PX x PY ways, one subdomain model per host
+    thread, halos exchanged through the library's in-process halo group (peer
+    copies, two host barriers per exchange, one launch per barotropic
+    substep), against the same domain undecomposed (graph replay off in both,
+    so the comparison is of the decomposition alone).  Wall time over
+    args.steps steps after args.warmup, each subdomain synchronised.  Prints
+    its own JSON line."""
+    import threading
+    import time
+    from hackathon_mom6_miniapp_b200 import HaloGroup, INIT_CFG, Model, subdomain_config
+    px, py = (int(x) for x in args.decomp.lower().split("x"))
+    NI = NJ = 720
+
+    def wall(models):
+        errs = []
+
+        def run(m, n):
+            try:
+                m.step(n)
+                m.synchronize()
+            except Exception as e:
+                errs.append(e)
+
+        for n in (args.warmup, args.steps):
+            ts = [threading.Thread(target=run, args=(m, n)) for m in models]
+            t0 = time.perf_counter()
+            for t in ts:
+                t.start()
+            for t in ts:
+                t.join()
+            dt = time.perf_counter() - t0
+        if errs:
+            raise errs[0]
+        return 1000.0 * dt / args.steps
+
+    glob = Model(NI, NJ, NK, BT, INIT_CFG, seed=0, bc_fill=False, dt=600.0)
+    single_ms = wall([glob])
+    glob.close()
+    group = HaloGroup(px, py, timeout_s=300.0)
+    models = []
+    for r in range(px * py):
+        ni, nj, sub = subdomain_config(NI, NJ, px, py, r)
+        m = Model(ni, nj, NK, BT, INIT_CFG, seed=0, bc_fill=False, dt=600.0, subdomain=sub)
+        group.join(m, r)
+        models.append(m)
+    dec_ms = wall(models)
+    print(json.dumps({"decomp": f"{px}x{py}", "workload": "720x720x75 bt50 FP64 fast form",
+                      "single_domain_ms_per_step": single_ms,
+                      "decomposed_ms_per_step": dec_ms,
+                      "exchanges_per_step": 6 + 3 * 2 * BT,
+                      "note": "one GPU; every subdomain on the same device"}))
+    for m in models:
+        m.close()
+    group.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -801,6 +859,9 @@ def main():
                     help="with --profile-abi: drive the reference's kernels instead")
     ap.add_argument("--profile-mlp", action="store_true",
                     help="run the surrogate network's GEMM kernels only (for ncu)")
+    ap.add_argument("--decomp", default="",
+                    help="PXxPY: time the decomposed step on one GPU against the single "
+                         "domain (its own JSON line)")
     args = ap.parse_args()
     world, rank, local, dist = dist_setup(args)
     try:
@@ -810,6 +871,8 @@ def main():
             run_profile_abi(args)
         elif args.profile_mlp:
             run_profile_mlp(args)
+        elif args.decomp:
+            run_decomp(args)
         elif args.impl == "reference":
             run_reference(args, world, rank, local, dist)
         else:

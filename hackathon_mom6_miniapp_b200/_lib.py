@@ -63,9 +63,9 @@ class Config(ctypes.Structure):
                 ("i_offset", ctypes.c_int), ("j_offset", ctypes.c_int), ("cuts", ctypes.c_int)]
 
 CUT_W, CUT_E, CUT_S, CUT_N = 1, 2, 4, 8
-# int (*)(void *ctx, double *field, int nz, int kind, void *stream)
+# int (*)(void *ctx, double *field, int nz, int kind, int more, void *stream)
 _ExchangeFn = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
-                               ctypes.c_int, ctypes.c_void_p)
+                               ctypes.c_int, ctypes.c_int, ctypes.c_void_p)
 
 
 def library_path():
@@ -264,14 +264,17 @@ class Model:
     def synchronize(self):
         _check(library().mom6b_synchronize(self._m))
 
-    def set_exchange(self, fn):
+    def set_exchange(self, fn, batch=False):
         """The halo exchange of a decomposed run, from Python (mom6b_set_exchange):
         fn(t, kind) refreshes in place the halo of t, a torch CUDA tensor viewing
         the model's device field as (nz, n2, n1) (the Fortran array's memory),
         with the model's stream current, so work fn enqueues there is ordered
-        with the step; kind 0 h points, 1 u faces, 2 v faces.  With one process
-        per GPU, fn = decomp.HaloExchange(d).exchange over torch.distributed
-        (NCCL); within one process, decomp.LocalHaloExchange.  None removes it."""
+        with the step; kind 0 h points, 1 u faces, 2 v faces.  batch=True: fn
+        receives the list of (t, kind) of one exchange point at once (e.g.
+        HaloExchange.exchange_many, one round of messages for all of them).
+        With one process per GPU, fn = decomp.HaloExchange(d).exchange over
+        torch.distributed (NCCL); within one process, decomp.LocalHaloExchange.
+        None removes it."""
         L = library()
         if fn is None:
             self._xfn = None
@@ -286,13 +289,24 @@ class Model:
                 self.__cuda_array_interface__ = {"shape": (nz, n2, n1), "typestr": "<f8",
                                                  "data": (ptr, False), "version": 2}
 
-        def cb(_ctx, ptr, nz, kind, stream):
+        held = []
+
+        def cb(_ctx, ptr, nz, kind, more, stream):
             try:
                 t = torch.as_tensor(_View(ptr, nz), device=dev)
+                if batch:
+                    held.append((t, kind))
+                    if more:
+                        return 0
                 with torch.cuda.stream(torch.cuda.ExternalStream(stream, device=dev)):
-                    fn(t, kind)
+                    if batch:
+                        fn(list(held))
+                    else:
+                        fn(t, kind)
+                held.clear()
                 return 0
             except Exception as e:   # the step reports the failure
+                held.clear()
                 self.exchange_error = e
                 return 1
 

@@ -670,13 +670,14 @@ static int enqueue_step(mom6b_model* m)
     cudaStream_t s2 = (m->overlap_bt && !m->xfn) ? m->s2d : m->s3d;
     const double dt = c.dt;
     // the halo exchange of a decomposed run (none for a whole domain)
-    auto xch = [&](double* f, int nz, int kind, cudaStream_t st) -> int {
+    auto xch = [&](double* f, int nz, int kind, int more, cudaStream_t st) -> int {
         if (!m->xfn) return MOM6B_OK;
-        if (m->xfn(m->xctx, f, nz, kind, (void*)st) != 0)
+        if (m->xfn(m->xctx, f, nz, kind, more, (void*)st) != 0)
             return fail(MOM6B_ERR_STATE, "halo exchange failed");
         return MOM6B_OK;
     };
-#define XCH(f, nz, kind, st) do { if (int rc_ = xch(f, nz, kind, st)) return rc_; } while (0)
+#define XCH(f, nz, kind, more, st) \
+    do { if (int rc_ = xch(f, nz, kind, more, st)) return rc_; } while (0)
     const double hv_neglect = step_hv_neglect();
     const double h_min = step_h_min();
     VVParams VV = step_vv_params(c);
@@ -764,10 +765,10 @@ static int enqueue_step(mom6b_model* m)
         return launch_vertvisc(D, M, m->up, m->vp, m->h0, dt, VV, m->taux_bot,
                                m->tauy_bot, s, m->remnant ? m->visc_rem_u : nullptr,
                                m->remnant ? m->visc_rem_v : nullptr); }));
-    XCH(m->up, g.nk, 1, s);   // rk2_mpi_cuda_c_driver.F90:409-412
-    XCH(m->vp, g.nk, 2, s);
+    XCH(m->up, g.nk, 1, 1, s);   // rk2_mpi_cuda_c_driver.F90:409-412
+    XCH(m->vp, g.nk, 2, 0, s);
     CK(continuity_pass(m, s, m->up, m->vp, m->h0, OB, dt));
-    XCH(m->hB, g.nk, 0, s);
+    XCH(m->hB, g.nk, 0, 0, s);
     if (c.bc_fill) {
         CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->hB, g.nk, 0, s); }));
         CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->up, g.nk, 1, s); }));
@@ -799,8 +800,8 @@ static int enqueue_step(mom6b_model* m)
         return launch_vertvisc(D, M, m->u, m->v, m->hB, 0.5 * dt, VV, m->taux_bot,
                                m->tauy_bot, s, m->remnant ? m->visc_rem_u : nullptr,
                                m->remnant ? m->visc_rem_v : nullptr); }));
-    XCH(m->u, g.nk, 1, s);
-    XCH(m->v, g.nk, 2, s);
+    XCH(m->u, g.nk, 1, 1, s);
+    XCH(m->v, g.nk, 2, 0, s);
     CK(continuity_pass(m, s, m->u, m->v, m->hB, OA, 0.5 * dt));
     if (c.bc_fill) {
         CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->hA, g.nk, 0, s); }));
@@ -832,9 +833,9 @@ static int enqueue_step(mom6b_model* m)
             CK(timed(m, s2, "btstep", [&] {
                 return launch_btstep(D, M, m->U, m->bt, Q, ei, ui, vi, ua, va, ea, s2); }));
             for (int n = 1; n <= P.nstep; ++n) {
-                XCH(m->bt.ubt, 1, 1, s2);
-                XCH(m->bt.vbt, 1, 2, s2);
-                XCH(m->bt.eta, 1, 0, s2);
+                XCH(m->bt.ubt, 1, 1, 1, s2);
+                XCH(m->bt.vbt, 1, 2, 1, s2);
+                XCH(m->bt.eta, 1, 0, 0, s2);
                 Q.substep = n;
                 CK(timed(m, s2, "btstep", [&] {
                     return launch_btstep(D, M, m->U, m->bt, Q, ei, ui, vi, ua, va, ea, s2); }));
@@ -1531,8 +1532,7 @@ struct mom6b_halo_group {
     bool failed = false;
     struct Member {
         mom6b_model* m = nullptr;
-        double* ptr = nullptr;
-        int nz = 0;
+        std::vector<std::pair<double*, int>> posted;   // the fields of the open point
     };
     std::vector<Member> mem;
     struct Ctx {
@@ -1564,7 +1564,7 @@ static bool group_meet(mom6b_halo_group* g)
     return true;
 }
 
-static int group_exchange(void* vctx, double* field, int nz, int kind, void* stream)
+static int group_exchange(void* vctx, double* field, int nz, int kind, int more, void* stream)
 {
     (void)kind;
     auto* c = (mom6b_halo_group::Ctx*)vctx;
@@ -1572,8 +1572,8 @@ static int group_exchange(void* vctx, double* field, int nz, int kind, void* str
     const int r = c->rank;
     cudaStream_t s = (cudaStream_t)stream;
     mom6b_halo_group::Member& me = g->mem[r];
-    me.ptr = field;
-    me.nz = nz;
+    me.posted.emplace_back(field, nz);
+    if (more) return 0;   // the point's other fields follow
     if (cudaStreamSynchronize(s) != cudaSuccess || !group_meet(g)) {
         std::lock_guard<std::mutex> lk(g->mu);
         g->failed = true;
@@ -1588,6 +1588,7 @@ static int group_exchange(void* vctx, double* field, int nz, int kind, void* str
     const int r0 = hs ? hw : 0, r1 = hn ? D.n2 - hw : D.n2;   // east / west strip rows
     const int c0 = hw_ ? hw : 0, c1 = he ? D.n1 - hw : D.n1;  // north / south strip columns
     int bad = 0;
+    for (size_t fi = 0; fi < me.posted.size() && !bad; ++fi)
     for (int dy = -1; dy <= 1 && !bad; ++dy)
         for (int dx = -1; dx <= 1 && !bad; ++dx) {
             if (!dx && !dy) continue;
@@ -1595,7 +1596,13 @@ static int group_exchange(void* vctx, double* field, int nz, int kind, void* str
             if (nr < 0) continue;
             const mom6b_halo_group::Member& nb = g->mem[nr];
             const Dims& N = nb.m->D;
-            if (nb.nz != nz) { bad = 1; break; }
+            if (nb.posted.size() != me.posted.size() || nb.posted[fi].second != me.posted[fi].second) {
+                bad = 1;
+                break;
+            }
+            double* field = me.posted[fi].first;
+            const int nz = me.posted[fi].second;
+            const double* src = nb.posted[fi].first;
             // this member's receive box and the neighbour's send box (0-based)
             const int mx0 = dx > 0 ? D.n1 - hw : (dx < 0 ? 0 : c0);
             const int mx1 = dx > 0 ? D.n1 : (dx < 0 ? hw : c1);
@@ -1608,7 +1615,7 @@ static int group_exchange(void* vctx, double* field, int nz, int kind, void* str
             cudaError_t e;
             if (dd == sd) {
                 cudaMemcpy3DParms p = {};
-                p.srcPtr = make_cudaPitchedPtr((void*)nb.ptr, (size_t)N.n1 * 8, N.n1, N.n2);
+                p.srcPtr = make_cudaPitchedPtr((void*)src, (size_t)N.n1 * 8, N.n1, N.n2);
                 p.srcPos = make_cudaPos((size_t)sx0 * 8, sy0, 0);
                 p.dstPtr = make_cudaPitchedPtr((void*)field, (size_t)D.n1 * 8, D.n1, D.n2);
                 p.dstPos = make_cudaPos((size_t)mx0 * 8, my0, 0);
@@ -1617,7 +1624,7 @@ static int group_exchange(void* vctx, double* field, int nz, int kind, void* str
                 e = cudaMemcpy3DAsync(&p, s);
             } else {
                 cudaMemcpy3DPeerParms p = {};
-                p.srcPtr = make_cudaPitchedPtr((void*)nb.ptr, (size_t)N.n1 * 8, N.n1, N.n2);
+                p.srcPtr = make_cudaPitchedPtr((void*)src, (size_t)N.n1 * 8, N.n1, N.n2);
                 p.srcPos = make_cudaPos((size_t)sx0 * 8, sy0, 0);
                 p.srcDevice = sd;
                 p.dstPtr = make_cudaPitchedPtr((void*)field, (size_t)D.n1 * 8, D.n1, D.n2);
@@ -1632,9 +1639,12 @@ static int group_exchange(void* vctx, double* field, int nz, int kind, void* str
         std::lock_guard<std::mutex> lk(g->mu);
         g->failed = true;
         g->cv.notify_all();
+        me.posted.clear();
         return 1;
     }
-    return group_meet(g) ? 0 : 1;
+    const bool ok = group_meet(g);   // no member reads the posts after this
+    me.posted.clear();
+    return ok ? 0 : 1;
 }
 
 extern "C" int mom6b_halo_group_create(int npes_x, int npes_y, double timeout_s,

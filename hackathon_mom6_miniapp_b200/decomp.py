@@ -121,35 +121,48 @@ class HaloExchange:
 
     def exchange(self, a):
         """Exchange the halo of `a` ((n2, n1) or (nk, n2, n1)) in place."""
+        self.exchange_many([a])
+        return a
+
+    def exchange_many(self, arrays):
+        """Exchange the halos of several arrays (or (array, kind) pairs, as
+        Model.set_exchange(batch=True) passes them) in one round of messages."""
         import torch
         import torch.distributed as dist
-        n2, n1 = a.shape[-2], a.shape[-1]
-        if (n1, n2) != (self.d.n1, self.d.n2):
-            raise ValueError(f"array {tuple(a.shape)} does not match the data domain "
-                             f"({self.d.n2}, {self.d.n1})")
-        send, recv = self._regions(n1, n2)
-        bufs_s, bufs_r, ops = {}, {}, []
-        for k in _DIRS:
-            if self.nbr[k] is None:
-                continue
-            rs, cs = send[k]
-            bufs_s[k] = a[..., rs, cs].contiguous()          # packed before any unpack
-            rr, cr = recv[k]
-            bufs_r[k] = torch.empty_like(a[..., rr, cr]).contiguous()
-        for k in _DIRS:
-            if self.nbr[k] is None:
-                continue
-            ops.append(dist.P2POp(dist.irecv, bufs_r[k], self.nbr[k], self.group))
-            ops.append(dist.P2POp(dist.isend, bufs_s[k], self.nbr[k], self.group))
+        arrays = [x[0] if isinstance(x, tuple) else x for x in arrays]
+        plan = []
+        for a in arrays:
+            n2, n1 = a.shape[-2], a.shape[-1]
+            if (n1, n2) != (self.d.n1, self.d.n2):
+                raise ValueError(f"array {tuple(a.shape)} does not match the data domain "
+                                 f"({self.d.n2}, {self.d.n1})")
+            send, recv = self._regions(n1, n2)
+            bufs_s, bufs_r = {}, {}
+            for k in _DIRS:
+                if self.nbr[k] is None:
+                    continue
+                rs, cs = send[k]
+                bufs_s[k] = a[..., rs, cs].contiguous()      # packed before any unpack
+                rr, cr = recv[k]
+                bufs_r[k] = torch.empty_like(a[..., rr, cr]).contiguous()
+            plan.append((a, recv, bufs_s, bufs_r))
+        ops = []
+        for _, _, bufs_s, bufs_r in plan:
+            for k in _DIRS:
+                if self.nbr[k] is None:
+                    continue
+                ops.append(dist.P2POp(dist.irecv, bufs_r[k], self.nbr[k], self.group))
+                ops.append(dist.P2POp(dist.isend, bufs_s[k], self.nbr[k], self.group))
         if ops:
             for req in dist.batch_isend_irecv(ops):
                 req.wait()
-        for k in _DIRS:                                        # E, W, N, S, NE, NW, SE, SW
-            if self.nbr[k] is None:
-                continue
-            rr, cr = recv[k]
-            a[..., rr, cr] = bufs_r[k]
-        return a
+        for a, recv, _, bufs_r in plan:
+            for k in _DIRS:                                    # E, W, N, S, NE, NW, SE, SW
+                if self.nbr[k] is None:
+                    continue
+                rr, cr = recv[k]
+                a[..., rr, cr] = bufs_r[k]
+        return arrays
 
 
 class LocalBoard:
@@ -174,27 +187,35 @@ class LocalHaloExchange(HaloExchange):
         super().__init__(decomp)
         self.board = board
 
-    def exchange(self, a):
-        n2, n1 = a.shape[-2], a.shape[-1]
-        if (n1, n2) != (self.d.n1, self.d.n2):
-            raise ValueError(f"array {tuple(a.shape)} does not match the data domain "
-                             f"({self.d.n2}, {self.d.n1})")
-        send, recv = self._regions(n1, n2)
-        packed = {}
-        for k in _DIRS:
-            if self.nbr[k] is not None:
-                rs, cs = send[k]
-                packed[k] = a[..., rs, cs].clone()
-        self._sync(a)
-        self.board.slots[self.d.rank] = packed
+    def exchange_many(self, arrays):
+        arrays = [x[0] if isinstance(x, tuple) else x for x in arrays]
+        packs, recvs = [], []
+        for a in arrays:
+            n2, n1 = a.shape[-2], a.shape[-1]
+            if (n1, n2) != (self.d.n1, self.d.n2):
+                raise ValueError(f"array {tuple(a.shape)} does not match the data domain "
+                                 f"({self.d.n2}, {self.d.n1})")
+            send, recv = self._regions(n1, n2)
+            packed = {}
+            for k in _DIRS:
+                if self.nbr[k] is not None:
+                    rs, cs = send[k]
+                    packed[k] = a[..., rs, cs].clone()
+            packs.append(packed)
+            recvs.append(recv)
+        for a in arrays:
+            self._sync(a)
+        self.board.slots[self.d.rank] = packs
         self.board.barrier.wait()
-        for k in _DIRS:
-            if self.nbr[k] is not None:
-                rr, cr = recv[k]
-                a[..., rr, cr] = self.board.slots[self.nbr[k]][_OPPOSITE[k]].to(a.device)
-        self._sync(a)
+        for f, a in enumerate(arrays):
+            for k in _DIRS:
+                if self.nbr[k] is not None:
+                    rr, cr = recvs[f][k]
+                    a[..., rr, cr] = self.board.slots[self.nbr[k]][f][_OPPOSITE[k]].to(a.device)
+        for a in arrays:
+            self._sync(a)
         self.board.barrier.wait()
-        return a
+        return arrays
 
     @staticmethod
     def _sync(a):

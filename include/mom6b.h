@@ -171,9 +171,12 @@ int mom6b_set_wait_limit(mom6b_model *m, long long cycles, int stall_test);
  * called mom6b_step, with the model's stream, at these points: up, vp before
  * the predictor continuity, the predictor's h after it, u, v before the
  * corrector continuity, and the barotropic eta, ubt, vbt before every
- * substep.  It returns 0, or nonzero to abandon the step (mom6b_step then
- * returns MOM6B_ERR_STATE).  Work it enqueues on the stream is ordered with
- * the step's kernels.  With cuts, the ranges that stop short of a wall
+ * substep.  The fields of one point come in consecutive calls, all but the
+ * last with more = 1: an exchange may hold them and move them together when
+ * the call with more = 0 comes, and every field of the point must be
+ * exchanged when that call returns.  It returns 0, or nonzero to abandon the
+ * step (mom6b_step then returns MOM6B_ERR_STATE).  Work it enqueues on the
+ * stream is ordered with the step's kernels.  With cuts, the ranges that stop short of a wall
  * (velocity update, CorAdCalc's u and v points) reach the cut, CorAdCalc's
  * and hor_visc's intermediates on the cut exist, and the barotropic loop
  * runs one launch per substep on ranges two points into the halo, so that
@@ -181,15 +184,16 @@ int mom6b_set_wait_limit(mom6b_model *m, long long cycles, int stall_test);
  * form).  Supported: MOM6B_FP64 without halo fill, the default Sadourny
  * Coriolis and Laplacian hor_visc, zonal continuity, no remnant, no
  * diagnostics, no surrogate; the step is not captured in a CUDA graph. */
-typedef int (*mom6b_exchange_fn)(void *ctx, double *field, int nz, int kind, void *stream);
+typedef int (*mom6b_exchange_fn)(void *ctx, double *field, int nz, int kind, int more,
+                                 void *stream);
 int mom6b_set_exchange(mom6b_model *m, mom6b_exchange_fn fn, void *ctx);
 
 /* An in-process exchange among npes_x * npes_y subdomain models (one host
  * thread per model, on one or several devices; rank = pos_x * npes_y +
- * pos_y as MPI_Cart_create orders a 2-D grid).  Each exchange posts the
- * field, waits for every member, copies each neighbour's edge strips into
- * this model's halo (peer copies between devices), and waits again before
- * the owner may change them.  East/west strips span the compute rows plus
+ * pos_y as MPI_Cart_create orders a 2-D grid).  Each exchange point posts
+ * its fields, waits for every member, copies each neighbour's edge strips
+ * into this model's halos (peer copies between devices), and waits again
+ * before the owners may change them.  East/west strips span the compute rows plus
  * the halo rows on a side without a north/south neighbour, north/south
  * strips the compute columns plus the halo columns on a side without an
  * east/west neighbour, the corner blocks come from the diagonal neighbours,

@@ -91,7 +91,8 @@ def test_cut_model_refuses_to_step_without_exchange():
 
 
 @pytest.mark.gpu
-def test_python_exchange_hook_is_bit_identical():
+@pytest.mark.parametrize("batch", [False, True])
+def test_python_exchange_hook_is_bit_identical(batch):
     """Model.set_exchange with decomp.LocalHaloExchange: the library calls back
     into Python with torch views of its device fields on the model's stream
     (the path a one-process-per-GPU run takes with decomp.HaloExchange over
@@ -106,7 +107,10 @@ def test_python_exchange_hook_is_bit_identical():
         ni, nj, sub = subdomain_config(NI, NJ, px, py, r)
         m = Model(ni, nj, nk, nbt, init_mode=1, bc_fill=False, exact=True, subdomain=sub)
         x = LocalHaloExchange(Decomposition(NI - 4, NJ - 4, px, py, r), board)
-        m.set_exchange(lambda t, kind, x=x: x.exchange(t))
+        if batch:   # one round per exchange point
+            m.set_exchange(x.exchange_many, batch=True)
+        else:       # one round per field
+            m.set_exchange(lambda t, kind, x=x: x.exchange(t))
         locs.append((m, sub))
 
     def run(m):
