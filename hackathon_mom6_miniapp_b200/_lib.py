@@ -95,6 +95,7 @@ def library():
     L.mom6b_dims.argtypes = [vp, P(ctypes.c_int)]
     L.mom6b_stream.argtypes = [vp, P(vp)]
     L.mom6b_step_host.argtypes = [vp, ctypes.c_int, P(d), P(d), P(d), P(d)]
+    L.mom6b_step_host_io.argtypes = [vp, ctypes.c_int] + [P(d)] * 7
     L.mom6b_verify.argtypes = [vp, P(d)]
     L.mom6b_launch_count.argtypes = [vp]
     L.mom6b_launch_count.restype = i64
@@ -321,6 +322,18 @@ class Model:
             assert a.dtype == np.float64 and a.flags["F_CONTIGUOUS"]
             return _dptr(a)
         _check(library().mom6b_step_host(self._m, int(n), p(u), p(v), p(h), p(eta)))
+
+    def step_host_io(self, n, u_in=None, v_in=None, eta_in=None, u_out=None, v_out=None,
+                     h_out=None, eta_out=None):
+        """End-to-end with the step's inputs (u, v, eta) and outputs (u, v, h, eta)
+        apart (mom6b_step_host_io); an input and an output may be the same array."""
+        def p(a):
+            if a is None:
+                return None
+            assert a.dtype == np.float64 and a.flags["F_CONTIGUOUS"]
+            return _dptr(a)
+        _check(library().mom6b_step_host_io(self._m, int(n), p(u_in), p(v_in), p(eta_in),
+                                            p(u_out), p(v_out), p(h_out), p(eta_out)))
 
     def verify(self):
         out = (ctypes.c_double * 7)()

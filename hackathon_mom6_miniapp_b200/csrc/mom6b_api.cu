@@ -1226,6 +1226,40 @@ extern "C" int mom6b_step_host(mom6b_model* m, int nsteps, double* u, double* v,
     return check_status(m);
 }
 
+extern "C" int mom6b_step_host_io(mom6b_model* m, int nsteps, const double* u_in,
+                                  const double* v_in, const double* eta_in, double* u_out,
+                                  double* v_out, double* h_out, double* eta_out)
+{
+    if (!m || nsteps < 0) return fail(MOM6B_ERR_ARG, "bad argument");
+    CK(cudaSetDevice(m->cfg.device));
+    const size_t n3 = m->grid->plane * (size_t)m->grid->nk, n2 = m->grid->plane;
+    cudaStream_t s = m->s3d;
+    if (m->cfg.precision == MOM6B_MIXED) {  // FP32 state: convert through set/get
+        if (u_in) if (int rc = mom6b_set_field(m, MOM6B_F_U, u_in, n3)) return rc;
+        if (v_in) if (int rc = mom6b_set_field(m, MOM6B_F_V, v_in, n3)) return rc;
+        if (eta_in) if (int rc = mom6b_set_field(m, MOM6B_F_ETA, eta_in, n2)) return rc;
+        if (int rc = mom6b_step(m, nsteps)) return rc;
+        if (u_out) if (int rc = mom6b_get_field(m, MOM6B_F_U, u_out, n3)) return rc;
+        if (v_out) if (int rc = mom6b_get_field(m, MOM6B_F_V, v_out, n3)) return rc;
+        if (h_out) if (int rc = mom6b_get_field(m, MOM6B_F_H, h_out, n3)) return rc;
+        if (eta_out) if (int rc = mom6b_get_field(m, MOM6B_F_ETA, eta_out, n2)) return rc;
+        return check_status(m);
+    }
+    CK(cudaStreamSynchronize(m->s2d));
+    if (u_in) CK(cudaMemcpyAsync(m->u, u_in, n3 * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (v_in) CK(cudaMemcpyAsync(m->v, v_in, n3 * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (eta_in)
+        CK(cudaMemcpyAsync(m->eta, eta_in, n2 * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (int rc = mom6b_step(m, nsteps)) return rc;
+    if (u_out) CK(cudaMemcpyAsync(u_out, m->u, n3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (v_out) CK(cudaMemcpyAsync(v_out, m->v, n3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (h_out) CK(cudaMemcpyAsync(h_out, m->hA, n3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (eta_out)
+        CK(cudaMemcpyAsync(eta_out, m->eta, n2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return check_status(m);
+}
+
 extern "C" int mom6b_verify(mom6b_model* m, double* out)
 {
     if (!m || !out) return fail(MOM6B_ERR_ARG, "null argument");
@@ -1578,6 +1612,7 @@ static int group_exchange(void* vctx, double* field, int nz, int kind, int more,
         std::lock_guard<std::mutex> lk(g->mu);
         g->failed = true;
         g->cv.notify_all();
+        me.posted.clear();
         return 1;
     }
     const int hw = 3;
@@ -1636,10 +1671,11 @@ static int group_exchange(void* vctx, double* field, int nz, int kind, int more,
             if (e != cudaSuccess) bad = 1;
         }
     if (bad || cudaStreamSynchronize(s) != cudaSuccess) {
+        // the neighbours may still be reading this member's posts: they stay
+        // (the group is failed, so no later round reads them)
         std::lock_guard<std::mutex> lk(g->mu);
         g->failed = true;
         g->cv.notify_all();
-        me.posted.clear();
         return 1;
     }
     const bool ok = group_meet(g);   // no member reads the posts after this

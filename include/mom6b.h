@@ -148,6 +148,14 @@ int mom6b_stream(mom6b_model *m, void **stream);
  * be NULL to skip that field. */
 int mom6b_step_host(mom6b_model *m, int nsteps, double *u, double *v, double *h,
                     double *eta);
+/* The same with the step's inputs and outputs apart: upload u_in, v_in,
+ * eta_in (the state a step reads; h restarts from h0 at every step,
+ * rk2_serial_driver.F90:225-232, so an uploaded h would be overwritten
+ * unread), run nsteps, download u_out, v_out, h_out, eta_out.  Any pointer
+ * may be NULL; an input and an output may be the same buffer. */
+int mom6b_step_host_io(mom6b_model *m, int nsteps, const double *u_in, const double *v_in,
+                       const double *eta_in, double *u_out, double *v_out, double *h_out,
+                       double *eta_out);
 
 /* verify_state of rk2_serial_driver.F90:563-623 computed on the device:
  * out = {mass_init, mass_final, rel_error, max_u, max_v, max_eta, ke_total}. */

@@ -135,3 +135,31 @@ def test_python_exchange_hook_is_bit_identical(batch):
             g = glob.get(name)[i0 + io:i1 + io, j0 + jo:j1 + jo]
             assert np.array_equal(a, g), (sub, name, int(np.count_nonzero(a != g)))
         m.set_exchange(None)
+
+
+@pytest.mark.gpu
+def test_halo_group_reports_a_member_that_never_arrives():
+    """Failure detection on the host: one member of a 2x1 group never steps.
+    The other's first exchange waits out the group's timeout, the step returns
+    an error instead of hanging, and the group stays failed (a later exchange
+    fails at once).  No kernel waits on another: the wait is a host barrier."""
+    import time
+    from hackathon_mom6_miniapp_b200 import HaloGroup, Model, Mom6bError, subdomain_config
+    group = HaloGroup(2, 1, timeout_s=2.0)
+    ms = []
+    for r in range(2):
+        ni, nj, sub = subdomain_config(40, 36, 2, 1, r)
+        m = Model(ni, nj, 4, 5, init_mode=1, bc_fill=False, exact=True, subdomain=sub)
+        group.join(m, r)
+        ms.append(m)
+    t0 = time.perf_counter()
+    with pytest.raises(Mom6bError):
+        ms[0].step(1)
+    waited = time.perf_counter() - t0
+    assert 1.5 < waited < 60.0, waited
+    t0 = time.perf_counter()
+    with pytest.raises(Mom6bError):
+        ms[0].step(1)
+    assert time.perf_counter() - t0 < 1.5
+    ms[0].synchronize()
+    group.close()

@@ -112,6 +112,19 @@ def test_set_state_then_step_matches():
 
 
 @pytest.mark.gpu
+def test_step_host_io_roundtrip():
+    """Inputs u, v, eta and outputs u, v, h, eta apart, sharing buffers."""
+    from hackathon_mom6_miniapp_b200 import Model
+    o, g = _pair(24, 20, 6, 40, INIT_CFG, seed=8)
+    u, v, eta = (np.asfortranarray(o.get(n)) for n in ("u", "v", "eta"))
+    h = np.zeros_like(u, order="F")
+    g.step_host_io(3, u, v, eta, u, v, h, eta)
+    o.step(3)
+    for n, a in zip(("u", "v", "h", "eta"), (u, v, h, eta)):
+        assert np.array_equal(a, o.get(n)), n
+
+
+@pytest.mark.gpu
 def test_step_host_roundtrip():
     from hackathon_mom6_miniapp_b200 import Model
     o, g = _pair(24, 20, 6, 40, INIT_CFG, seed=8)
