@@ -52,12 +52,12 @@ def _run(cmd):
     return r
 
 
-def build(verbose=False, force=False):
+def build(verbose=False, force=False, jobs=None):
     os.makedirs(BUILD, exist_ok=True)
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [
         os.path.join(HERE, "..", "include", "mom6b.h"),
         os.path.join(HERE, "..", "include", "mom6_cuda_c.h")]
-    objs = []
+    objs, cmds = [], []
     for src in CU_SOURCES + CXX_SOURCES:
         path = os.path.join(CSRC, src)
         obj = os.path.join(BUILD, src + ".o")
@@ -73,7 +73,14 @@ def build(verbose=False, force=False):
                                              "-c", "-o", obj, path]
             if verbose:
                 print(" ".join(cmd))
-            _run(cmd)
+            cmds.append(cmd)
+    # the translation units compile independently: one compiler per core
+    if cmds:
+        from concurrent.futures import ThreadPoolExecutor
+        n = jobs or max(1, min(len(cmds), os.cpu_count() or 1))
+        with ThreadPoolExecutor(max_workers=n) as ex:
+            for f in [ex.submit(_run, c) for c in cmds]:
+                f.result()
     if force or _newer(LIB, objs):
         cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-ldl"]
         if verbose:

@@ -1358,6 +1358,45 @@ static cudaError_t launch_halo_fill_t(const Dims& D, T* f, int nz, int kind, cud
     return cudaGetLastError();
 }
 
+// The fills of an h-point, a u-point and a v-point field (kinds 0, 1, 2) in one
+// launch: grid row y fills the field of kind y.  The three fields are
+// distinct arrays and each fill reads only its own field, so the result is
+// that of the three separate fills.
+template <typename T>
+__global__ void k_halo_fill3(Dims D, T* fh, T* fu, T* fv, int nz)
+{
+    const int kind = (int)blockIdx.y;
+    T* f = kind == 0 ? fh : (kind == 1 ? fu : fv);
+    halo_fill_point<T>(D, f, nz, kind, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+template <typename T>
+static cudaError_t launch_halo_fill3_t(const Dims& D, T* fh, T* fu, T* fv, int nz,
+                                       cudaStream_t s)
+{
+    long long most = 0;
+    for (int kind = 0; kind < 3; ++kind) {
+        const long long t = halo_points_per_layer(D, kind) * nz;
+        if (t > most) most = t;
+    }
+    const int nb = 256;
+    const long long blocks = (most + nb - 1) / nb;
+    k_halo_fill3<T><<<dim3((unsigned)blocks, 3, 1), nb, 0, s>>>(D, fh, fu, fv, nz);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_halo_fill3(const Dims& D, double* fh, double* fu, double* fv, int nz,
+                              cudaStream_t s)
+{
+    return launch_halo_fill3_t<double>(D, fh, fu, fv, nz, s);
+}
+
+cudaError_t launch_halo_fill3_f(const Dims& D, float* fh, float* fu, float* fv, int nz,
+                                cudaStream_t s)
+{
+    return launch_halo_fill3_t<float>(D, fh, fu, fv, nz, s);
+}
+
 cudaError_t launch_halo_fill(const Dims& D, double* f, int nz, int kind, cudaStream_t s)
 {
     return launch_halo_fill_t<double>(D, f, nz, kind, s);

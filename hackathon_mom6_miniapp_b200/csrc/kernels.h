@@ -5,11 +5,27 @@
 
 namespace mom6b {
 
+// Products of the uniform metrics that the fast FP64 tendency multiplies
+// by (formed on the host when the metrics are uniform; the serial
+// expressions with the metrics factored out): rel = kRv dv - kRu du,
+// q = absv kQn / (S + kQe) with S the four-cell thickness sum of hArea_q,
+// str_xy = (kSv dv + kSu du) (h00 + h10 + h01 + h11), KE = kKu (uc^2 + um^2)
+// + kKv (vc^2 + vm^2), str_xx = h (kXv dv - kXu du), uh = kTu u (h + h+),
+// vh = kTv v (h + h+), CAu = kCu (q0 s0 + q1 s1) - IdxCu dKE, CAv = -kCv
+// (...) - IdyCv dKE, h_u = kHm (h + h+), diffu = (kDq dstr_xy + kDh
+// dstr_xx) / (h_u + h_neglect), diffv = (kEq dstr_xy - kEh dstr_xx) / (h_v
+// + h_neglect).
+struct TendFold {
+    double kRv, kRu, kQn, kQe, kSv, kSu, kKu, kKv, kXu, kXv, kTu, kTv, kCu, kCv, kHm, kDq,
+        kDh, kEq, kEh;
+};
+
 // Spatially uniform metrics as scalars.  init_ocean_grid builds every metric
 // array uniform (mom6_types.F90:193-228) except CoriolisBu, which varies with
 // j only; when the model detects this it passes the values here and the
 // kernels read them from the parameter bank instead of 2-D arrays.  The
-// arithmetic is unchanged: the same values enter the same operations.
+// exact kernels' arithmetic is unchanged: the same values enter the same
+// operations (the fast tendency also multiplies by the products in tf).
 struct UniMetrics {
     double IareaT, areaT, dxT, IdxT, dxCu, dyCu, dy_Cu, IdxCu, IdyCu, dxCv, dyCv,
         IdxCv, IdyCv, IareaBu, IareaCu, IareaCv, mask2dT, mask2dBu, mask2dCu,
@@ -17,6 +33,7 @@ struct UniMetrics {
         red_xx, red_xy, Kh_xx, Kh_xy;
     const double* cor_row;  // CoriolisBu(:, J) for J = 1..n2 (constant in i)
     int valid;              // 1 when the grid qualifies
+    TendFold tf;            // the fast tendency's products (when valid)
     // barotropic metrics (barotropic_init): scalars, and f_4_u/f_4_v per row
     double Datu, Datv, gtot_E, gtot_W, gtot_N, gtot_S, bt_rem_u, bt_rem_v;
     const double* f4u_row;  // f_4_u(c, :, J) at [(J-1)*4 + c-1]
@@ -154,6 +171,11 @@ int btstep_static(const double* eta_in, const double* ubt_in, const double* vbt_
 // Mixed-precision form (k_mixed.cu): FP32 state and stencils, FP64 column
 // sums, Newton scalars, thickness update and tridiagonal elimination.
 cudaError_t launch_halo_fill_f(const Dims& D, float* f, int nz, int kind, cudaStream_t s);
+// The fills of an h-, a u- and a v-point field (kinds 0, 1, 2) in one launch.
+cudaError_t launch_halo_fill3(const Dims& D, double* fh, double* fu, double* fv, int nz,
+                              cudaStream_t s);
+cudaError_t launch_halo_fill3_f(const Dims& D, float* fh, float* fu, float* fv, int nz,
+                                cudaStream_t s);
 cudaError_t launch_tendency_f(const Dims& D, const Metrics& M, const UniMetrics& U,
                               const float* uin, const float* vin, const float* h,
                               const float* ubase, const float* vbase, float* uout,

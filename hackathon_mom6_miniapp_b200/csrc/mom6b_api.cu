@@ -281,6 +281,28 @@ static int detect_uniform(mom6b_model* m)
         CK(cudaMemcpy(d, cor.data(), g.n2 * sizeof(double), cudaMemcpyHostToDevice));
         U.cor_row = d;
         U.valid = 1;
+        // the fast tendency's products of the uniform metrics
+        TendFold& K = U.tf;
+        const double mB = U.mask2dBu;
+        K.kRv = mB * U.dyCv * U.IareaBu;
+        K.kRu = mB * U.dxCu * U.IareaBu;
+        K.kQn = 2.0 * U.Area_q / U.areaT;
+        K.kQe = 2.0e-20 / U.areaT;
+        K.kSv = -0.25 * U.Kh_xy * mB * mB * U.red_xy * U.DY_dxBu * U.IdyCv;
+        K.kSu = -0.25 * U.Kh_xy * mB * mB * U.red_xy * U.DX_dyBu * U.IdxCu;
+        K.kKu = 0.25 * U.dyCu / U.areaT;
+        K.kKv = 0.25 * U.dxCv / U.areaT;
+        K.kXu = U.Kh_xx * U.red_xx * U.DY_dxT * U.IdyCu;
+        K.kXv = U.Kh_xx * U.red_xx * U.DX_dyT * U.IdxCv;
+        K.kTu = 0.5 * U.dyCu;
+        K.kTv = 0.5 * U.dxCv;
+        K.kCu = 0.25 * U.IdxCu;
+        K.kCv = 0.25 * U.IdyCv;
+        K.kHm = 0.5 * U.mask2dT;
+        K.kDq = U.IdxCu * U.dx2q * U.IareaCu;
+        K.kDh = U.IdyCu * U.dy2h * U.IareaCu;
+        K.kEq = U.IdyCv * U.dy2q * U.IareaCv;
+        K.kEh = U.IdxCv * U.dx2h * U.IareaCv;
     }
     if (okb && IareaT_uniform(g)) {
         double* du = dalloc(m, 4 * (size_t)g.n2, &err);
@@ -588,9 +610,8 @@ static int enqueue_surrogate_chain(mom6b_model* m, cudaStream_t s)
     if (int rc = surrogate_call(m, m->eta, m->ubt, m->vbt, m->ubt_av, m->vbt_av, m->eta_av, s))
         return rc;
     if (fill) {
-        CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->eta_av, 1, 0, s); }));
-        CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->ubt_av, 1, 1, s); }));
-        CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->vbt_av, 1, 2, s); }));
+        CK(timed(m, s, "halo_fill", [&] {
+            return launch_halo_fill3(D, m->eta_av, m->ubt_av, m->vbt_av, 1, s); }));
     }
     if (int rc = surrogate_call(m, m->eta_av, m->ubt_av, m->vbt_av, m->ubt_av, m->vbt_av,
                                 m->eta, s))
@@ -710,9 +731,8 @@ static int enqueue_step(mom6b_model* m)
                                        F(m->hB), F(m->uh), F(m->h_u), OB, m->uh_ovl, dt, h_min,
                                        s); }));
         if (c.bc_fill) {
-            CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill_f(D, F(m->hB), g.nk, 0, s); }));
-            CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill_f(D, F(m->up), g.nk, 1, s); }));
-            CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill_f(D, F(m->vp), g.nk, 2, s); }));
+            CK(timed(m, s, "halo_fill", [&] {
+                return launch_halo_fill3_f(D, F(m->hB), F(m->up), F(m->vp), g.nk, s); }));
         }
         // ---- corrector ----
         CK(timed(m, s, "tendency", [&] {
@@ -730,9 +750,8 @@ static int enqueue_step(mom6b_model* m)
                                        F(m->hA), F(m->uh), F(m->h_u), OA, m->uh_ovl, 0.5 * dt,
                                        h_min, s); }));
         if (c.bc_fill) {
-            CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill_f(D, F(m->hA), g.nk, 0, s); }));
-            CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill_f(D, F(m->u), g.nk, 1, s); }));
-            CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill_f(D, F(m->v), g.nk, 2, s); }));
+            CK(timed(m, s, "halo_fill", [&] {
+                return launch_halo_fill3_f(D, F(m->hA), F(m->u), F(m->v), g.nk, s); }));
         }
     } else {
     // ---- predictor ----  (with the driver's diagnostics, diffu and diffv are kept)
@@ -770,9 +789,8 @@ static int enqueue_step(mom6b_model* m)
     CK(continuity_pass(m, s, m->up, m->vp, m->h0, OB, dt));
     XCH(m->hB, g.nk, 0, 0, s);
     if (c.bc_fill) {
-        CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->hB, g.nk, 0, s); }));
-        CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->up, g.nk, 1, s); }));
-        CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->vp, g.nk, 2, s); }));
+        CK(timed(m, s, "halo_fill", [&] {
+            return launch_halo_fill3(D, m->hB, m->up, m->vp, g.nk, s); }));
     }
     // ---- corrector ----
     if (m->hvgen) {
@@ -804,9 +822,8 @@ static int enqueue_step(mom6b_model* m)
     XCH(m->v, g.nk, 2, 0, s);
     CK(continuity_pass(m, s, m->u, m->v, m->hB, OA, 0.5 * dt));
     if (c.bc_fill) {
-        CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->hA, g.nk, 0, s); }));
-        CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->u, g.nk, 1, s); }));
-        CK(timed(m, s, "halo_fill", [&] { return launch_halo_fill(D, m->v, g.nk, 2, s); }));
+        CK(timed(m, s, "halo_fill", [&] {
+            return launch_halo_fill3(D, m->hA, m->u, m->v, g.nk, s); }));
     }
 
     }
@@ -853,9 +870,8 @@ static int enqueue_step(mom6b_model* m)
         return launch_btstep(D, M, m->U, m->bt, P, m->eta, m->ubt, m->vbt, m->ubt_av,
                              m->vbt_av, m->eta_av, s2); }));
     if (c.bc_fill) {
-        CK(timed(m, s2, "halo_fill", [&] { return launch_halo_fill(D, m->eta_av, 1, 0, s2); }));
-        CK(timed(m, s2, "halo_fill", [&] { return launch_halo_fill(D, m->ubt_av, 1, 1, s2); }));
-        CK(timed(m, s2, "halo_fill", [&] { return launch_halo_fill(D, m->vbt_av, 1, 2, s2); }));
+        CK(timed(m, s2, "halo_fill", [&] {
+            return launch_halo_fill3(D, m->eta_av, m->ubt_av, m->vbt_av, 1, s2); }));
     }
     CK(timed(m, s2, "btstep", [&] {
         return launch_btstep(D, M, m->U, m->bt, P, m->eta_av, m->ubt_av, m->vbt_av,

@@ -86,6 +86,11 @@ __device__ __forceinline__ void arakawa_bc(R q00, R qm0, R q0m, R qmm, R& b, R& 
 // and row; the coefficients are formed where CAu / CAv need them (:228-248).
 // FAST: the fast FP64 form's arithmetic (built with FMA contraction in
 // k_tendency_fast.cu): quotients by div_nr.
+// multiply-add in the stencil type (the folded stencils of the fast FP64 and
+// the mixed forms)
+__device__ __forceinline__ double td_fma(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float td_fma(float a, float b, float c) { return fmaf(a, b, c); }
+
 template <bool FAST>
 __device__ __forceinline__ double td_div(double a, double b)
 {
@@ -113,6 +118,10 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
               R* dfu = nullptr, R* dfv = nullptr, const CUtensorMap* tmaps = nullptr,
               int* status = nullptr)
 {
+    // FU: the fast FP64 form and the mixed form on uniform metrics, whose
+    // Sadourny stencils multiply by the folded products of U.tf (the exact
+    // form keeps the serial expressions)
+    constexpr bool FU = (FAST || sizeof(R) == 4) && UNI && COR == 1 && !EXTV && !DIAG;
     constexpr int W = COR >= 2 ? 1 : 0;      // the Arakawa schemes' extra column and row
     constexpr int SX = TX + 2 + W, SY = TY + 2 + W;  // staged: [i0-1, i0+TX+W] x [j0-1, j0+TY+W]
     constexpr int CX = TX + 1 + W, CY = TY + 1 + W;  // intermediates
@@ -236,7 +245,18 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
         {
             int I = i0 - 1 + c, J = j0 - 1 + r;
             R qv = R(0.0), sxy = R(0.0);
-            if (I + 1 <= D.n1 && J + 1 <= D.n2) {
+            if (FU && I + 1 <= D.n1 && J + 1 <= D.n2) {
+                // the same expressions with the uniform metrics factored out
+                const R dv = SV(I + 1, J) - SV(I, J), du = SU(I, J + 1) - SU(I, J);
+                const R h00 = SH(I, J), h10 = SH(I + 1, J), h01 = SH(I, J + 1),
+                        h11 = SH(I + 1, J + 1);
+                const R a = h00 + h10, b = h01 + h11;
+                const R absv = COR(I, J) + td_fma(R(U.tf.kRv), dv, -(R(U.tf.kRu) * du));
+                const R S = ((J >= D.js - D.cs ? a : R(0.0)) + b) +
+                            ((I >= D.is - D.cw ? h00 + h01 : R(0.0)) + (h10 + h11));
+                qv = td_div<FAST>(absv * R(U.tf.kQn), S + R(U.tf.kQe));
+                sxy = td_fma(R(U.tf.kSv), dv, R(U.tf.kSu) * du) * (a + b);
+            } else if (I + 1 <= D.n1 && J + 1 <= D.n2) {
                 R v0 = SV(I, J), v1 = SV(I + 1, J);
                 R u0 = SU(I, J), u1 = SU(I, J + 1);
                 R h00 = SH(I, J), h10 = SH(I + 1, J), h01 = SH(I, J + 1),
@@ -275,7 +295,12 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
         {
             int i = i0 + c, j = j0 + r;
             R ke = R(0.0), sxx = R(0.0);
-            if (i <= D.n1 && j <= D.n2) {
+            if (FU && i <= D.n1 && j <= D.n2) {
+                const R uc = SU(i, j), um = SU(i - 1, j), vc = SV(i, j), vm = SV(i, j - 1);
+                ke = td_fma(R(U.tf.kKu), td_fma(uc, uc, um * um),
+                            R(U.tf.kKv) * td_fma(vc, vc, vm * vm));
+                sxx = SH(i, j) * td_fma(R(U.tf.kXv), vc - vm, -(R(U.tf.kXu) * (uc - um)));
+            } else if (i <= D.n1 && j <= D.n2) {
                 R uc = SU(i, j), um = SU(i - 1, j), vc = SV(i, j), vm = SV(i, j - 1);
                 ke = td_div<FAST>(R(0.25) *
                                ((G2(dyCu, i, j) * (uc * uc) + G2(dyCu, i - 1, j) * (um * um)) +
@@ -301,7 +326,8 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
             if (I <= D.n1 && J <= D.n2) {
                 int Ip = I + 1 < D.ied ? I + 1 : D.ied;
                 R hp = (Ip - (i0 - 1) < SX) ? SH(Ip, J) : R(0.0);
-                uhv = SU(I, J) * R(0.5) * (SH(I, J) + hp) * G2(dyCu, I, J);
+                if constexpr (FU) uhv = (R(U.tf.kTu) * SU(I, J)) * (SH(I, J) + hp);
+                else uhv = SU(I, J) * R(0.5) * (SH(I, J) + hp) * G2(dyCu, I, J);
             }
             s_uh[r][c] = uhv;
             int i = i0 + c, j = j0 - 1 + r;
@@ -309,7 +335,8 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
             if (i <= D.n1 && j <= D.n2) {
                 int Jp = j + 1 < D.jed ? j + 1 : D.jed;
                 R hp = (Jp - (j0 - 1) < SY) ? SH(i, Jp) : R(0.0);
-                vhv = SV(i, j) * R(0.5) * (SH(i, j) + hp) * G2(dxCv, i, j);
+                if constexpr (FU) vhv = (R(U.tf.kTv) * SV(i, j)) * (SH(i, j) + hp);
+                else vhv = SV(i, j) * R(0.5) * (SH(i, j) + hp) * G2(dxCv, i, j);
             }
             s_vh[r][c] = vhv;
         }
@@ -326,7 +353,16 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
     const int I = i0 + (int)threadIdx.x;
     const int j = j0 + (int)threadIdx.y;
     // ---- u point (I, j) ---------------------------------------------------
-    if (I <= D.ie - 1 + D.ce && j <= D.je) {
+    if (FU && I <= D.ie - 1 + D.ce && j <= D.je) {
+        const R CAu = td_fma(R(U.tf.kCu), td_fma(Q(I, j), VH(I + 1, j) + VH(I, j),
+                                                 Q(I, j - 1) * (VH(I, j - 1) + VH(I + 1, j - 1))),
+                             -(R(U.IdxCu) * (KE(I + 1, j) - KE(I, j))));
+        const R diffu =
+            td_div<FAST>(td_fma(R(U.tf.kDq), SXY(I, j - 1) - SXY(I, j),
+                                R(U.tf.kDh) * (SXX(I, j) - SXX(I + 1, j))),
+                         td_fma(R(U.tf.kHm), SH(I, j) + SH(I + 1, j), h_neglect));
+        uout[oo] = td_fma(coef, CAu + diffu, ub);
+    } else if (I <= D.ie - 1 + D.ce && j <= D.je) {
         R IdxCu = G2(IdxCu, I, j);
         R KEx = (KE(I + 1, j) - KE(I, j)) * IdxCu;
         R CAu;
@@ -361,7 +397,17 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
         if (DIAG && !EXTV) dfu[oo] = diffu;
     }
     // ---- v point (i, J) = (I, j) -------------------------------------------
-    if (I <= D.ie && j <= D.je - 1 + D.cn) {
+    if (FU && I <= D.ie && j <= D.je - 1 + D.cn) {
+        const int i = I, J = j;
+        const R CAv = -td_fma(R(U.tf.kCv), td_fma(Q(i - 1, J), UH(i - 1, J) + UH(i - 1, J + 1),
+                                                  Q(i, J) * (UH(i, J) + UH(i, J + 1))),
+                              R(U.IdyCv) * (KE(i, J + 1) - KE(i, J)));
+        const R diffv =
+            td_div<FAST>(td_fma(R(U.tf.kEq), SXY(i - 1, J) - SXY(i, J),
+                                -(R(U.tf.kEh) * (SXX(i, J) - SXX(i, J + 1)))),
+                         td_fma(R(U.tf.kHm), SH(i, J) + SH(i, J + 1), h_neglect));
+        vout[oo] = td_fma(coef, CAv + diffv, vb);
+    } else if (I <= D.ie && j <= D.je - 1 + D.cn) {
         const int i = I, J = j;
         R IdyCv = G2(IdyCv, i, J);
         R KEy = (KE(i, J + 1) - KE(i, J)) * IdyCv;

@@ -80,3 +80,4 @@ def test_fast_graph_replay_matches_eager():
     b.step(4)
     for n in STATE + ["uh", "hu_bt"]:
         assert np.array_equal(a.get(n), b.get(n)), n
+
