@@ -397,6 +397,260 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
     tbot[(size_t)(j - 1) * D.n1 + (i - 1)] = tb;
 }
 
+// The fast forms' column in two sweeps: the tridiagonal system is eliminated
+// bottom-up and back-substituted top-down (the serial code's elimination
+// mirrored), so that z_i, the bottom-up sum of the harmonic thicknesses that
+// botfn(z_i) needs, is formed on the way up instead of by a sweep of its own.
+// The mixed-layer taper 1 - z_top / Hmix needs z_top, the sum of hvel from the
+// surface, which the upward sweep only has at the end; it applies only to the
+// interfaces with z_top < Hmix.  hvel >= h_harm, so when the harmonic
+// thicknesses of the top MTOP layers already sum to Hmix (checked first, with
+// a relative margin for rounding) every interface below layer MTOP is untapered:
+// the sweep runs up to layer MTOP + 1 without z_top, then forms z_i, hvel,
+// z_top and a(K) of the top MTOP layers and eliminates them.  Returns false,
+// having written nothing, for a column where the check fails (thin surface
+// layers, or nz <= MTOP + 1); the caller then runs vertvisc_column.
+// Per layer: h, h(neighbour) and the velocity are read once by the upward
+// sweep (staged in shared memory, CH layers ahead, with cp.async), the
+// eliminated velocity and the multiplier once by the downward one.
+// Within a few units in the last place of the top-down elimination (the
+// system is diagonally dominant); the serial arithmetic of each coefficient
+// is the fast form's (vv_div, top-down botfn replaced by the bottom-up z_i).
+constexpr int kVvTop = 4;
+
+template <int KMAX, int CH, typename R, typename E, int MTOP = kVvTop>
+__device__ __forceinline__ bool
+vertvisc_column_up(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restrict__ v,
+                   const R* __restrict__ h, double dt, const VVParams& P,
+                   double* __restrict__ taux_bot, double* __restrict__ tauy_bot, int bx, int by,
+                   R* stage)
+{
+    using C = R;
+    const int nz = D.nk;
+    const int yb = by;
+    const bool is_u = yb >= 1 && ((yb - 1) & 1) == 0;
+    const int q = yb >= 1 ? (yb - 1) >> 1 : -1;
+    int i, j, di, dj;
+    R* vel;
+    const double *mask, *tau, *Ray;
+    const unsigned char* ray_on;
+    double* tbot;
+    if (is_u) {  // u columns: I in [is-1, ie], j in [js, je]
+        j = D.js + q;
+        i = D.is - 1 + bx * (int)blockDim.x + (int)threadIdx.x;
+        if (i > D.ie) return true;
+        di = 1; dj = 0;
+        vel = u; mask = M.mask2dCu; tau = M.taux; Ray = M.Ray_u;
+        ray_on = M.ray_layer_u; tbot = taux_bot;
+    } else {     // v columns: i in [is, ie], J in [js-1, je]
+        j = D.js + q;
+        i = D.is + bx * (int)blockDim.x + (int)threadIdx.x;
+        if (i > D.ie) return true;
+        di = 0; dj = 1;
+        vel = v; mask = M.mask2dCv; tau = M.tauy; Ray = M.Ray_v;
+        ray_on = M.ray_layer_v; tbot = tauy_bot;
+    }
+    const double msk = MOM6B_A2(mask, i, j, D);
+    if (!(msk > 0.0)) return true;   // vert_visc_apply leaves masked columns alone
+    if (nz <= MTOP + 1) return false;
+    const size_t plane = (size_t)D.plane;
+    const R* hc = h + (size_t)(j - 1) * D.n1 + (i - 1);               // h(i, j, 1)
+    const R* hn_ = h + (size_t)(j - 1 + dj) * D.n1 + (i - 1 + di);     // neighbour
+    R* vc = vel + (size_t)(j - 1) * D.n1 + (i - 1);
+    const double* rc = Ray + (size_t)(j - 1) * D.n1 + (i - 1);
+    const C hn = (C)P.h_neglect, I_Hbbl = (C)P.I_Hbbl, Kv = (C)P.Kv, Kv_ml = (C)P.Kv_ml;
+    const C Kv_extra_bbl = (C)P.Kv_extra_bbl, Hmix = (C)P.Hmix;
+    auto harm = [&](C h0, C h1) -> C { return vv_div<true>(C(2.0) * h0 * h1, h0 + h1 + hn); };
+    // hvel(k) from botfn(z_i(k + 1)) (vert_visc_coef :162-177)
+    auto hvel_h = [&](C bf, C hh, C h0, C h1, C vk) -> C {
+        C hv = hh;
+        if (vk * (h1 - h0) < C(0.0)) hv = (C(1.0) - bf) * hh + bf * (C(0.5) * (h1 + h0));
+        return hv;
+    };
+
+    // the top MTOP layers' harmonic thicknesses must reach Hmix
+    {
+        C h0[MTOP], h1[MTOP];
+#pragma unroll
+        for (int k = 0; k < MTOP; ++k) {
+            h0[k] = hc[(size_t)k * plane];
+            h1[k] = hn_[(size_t)k * plane];
+        }
+        C top = C(0.0);
+#pragma unroll
+        for (int k = 0; k < MTOP; ++k) top = top + harm(h0[k], h1[k]);
+        const C margin = sizeof(C) == 8 ? C(1.0e-12) : C(1.0e-5);
+        if (!(top >= Hmix + Hmix * margin)) return false;
+    }
+
+    E slot[KMAX + 2];   // c1r(L) = dt a(L) b1(L), the downward sweep's multipliers
+    const E dtE = (E)dt;
+    const E sfc_stress = (E)(dt / kRho0 * MOM6B_A2(tau, i, j, D) * msk);
+    const int tid = (int)threadIdx.x;
+    auto ST = [&](int b, int c, int f) -> R& { return stage[((b * CH + c) * 3 + f) * 128 + tid]; };
+
+    // ---- upward sweep: layer nz ----------------------------------------------
+    C hhL, hvL;           // harm and hvel of the layer L being eliminated
+    E vL;                 // its velocity
+    {
+        const C h0 = hc[(size_t)(nz - 1) * plane], h1 = hn_[(size_t)(nz - 1) * plane];
+        vL = (E)vc[(size_t)(nz - 1) * plane];
+        hhL = harm(h0, h1);
+        hvL = hvel_h(vv_botfn<true>(C(0.0)), hhL, h0, h1, (C)vL);   // z_i(nz + 1) = 0
+    }
+    // a(nz + 1), the bottom interface (:205-206)
+    const C a_bot = vv_div<true>(Kv + Kv_extra_bbl, C(0.5) * hvL + hn);
+    E a_below = (E)a_bot;        // a(L + 1)
+    E d1 = E(1.0), up = E(0.0);  // d1 and the eliminated velocity of layer L + 1
+    C zL = C(0.0);               // z_i(L + 1)
+    // eliminate layer L with a(L) above it (u'(L) -> vel(L), c1r(L) -> slot)
+    auto eliminate = [&](int L, C hv, E aL, E vk, E Rayk, E rhs_extra) {
+        const E hu = (E)(hv + hn);
+        const E bd = hu + dtE * (Rayk + a_below * d1);
+        const E b1 = vv_div<true>(E(1.0), bd + dtE * aL);
+        d1 = bd * b1;
+        up = (hu * vk + rhs_extra + dtE * a_below * up) * b1;
+        vc[(size_t)(L - 1) * plane] = (R)up;
+        slot[L] = dtE * aL * b1;
+        a_below = aL;
+    };
+    // lookahead layers L - 1 of the chunk's layers L = Lt .. Lt - CH + 1 (those
+    // with L >= MTOP + 1) into buffer b; every staged velocity is read before
+    // this thread overwrites it
+    auto stage_up = [&](int Lt, int b) {
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            const int L = Lt - c;
+            const bool ok = L >= MTOP + 1;
+            const size_t o = ok ? (size_t)(L - 2) * plane : 0;
+            cp_async_elem(&ST(b, c, 0), hc + o, ok);
+            cp_async_elem(&ST(b, c, 1), hn_ + o, ok);
+            cp_async_elem(&ST(b, c, 2), (const R*)vc + o, ok);
+        }
+        cp_async_commit();
+    };
+    stage_up(nz, 0);
+    for (int Lt = nz, it = 0; Lt >= MTOP + 1; Lt -= CH, ++it) {
+        const int b = it & 1;
+        if (Lt - CH >= MTOP + 1) {
+            stage_up(Lt - CH, b ^ 1);
+            cp_async_wait_prior();
+        } else {
+            cp_async_wait_all();
+        }
+        C p0[CH], p1[CH];
+        E pv[CH], pr[CH];
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            const int L = Lt - c;
+            p0[c] = ST(b, c, 0);
+            p1[c] = ST(b, c, 1);
+            pv[c] = (E)ST(b, c, 2);
+            pr[c] = (L >= MTOP + 1 && ray_on[L - 1]) ? (E)rc[(size_t)(L - 1) * plane] : E(0.0);
+        }
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            const int L = Lt - c;
+            if (L >= MTOP + 1) {
+                const C z_L = zL + hhL * I_Hbbl;                 // z_i(L)
+                const C hhu = harm(p0[c], p1[c]);                // layer L - 1
+                const C bfL = vv_botfn<true>(z_L);
+                const C hvu = hvel_h(bfL, hhu, p0[c], p1[c], (C)pv[c]);
+                // a(L) below the untapered depth (:185-202)
+                const C aL = vv_div<true>(Kv + Kv_extra_bbl * bfL,
+                                          C(0.5) * (hvL + hvu + hn));
+                eliminate(L, hvL, (E)aL, vL, pr[c], E(0.0));
+                zL = z_L; hhL = hhu; hvL = hvu; vL = pv[c];
+            }
+        }
+    }
+
+    // ---- the top MTOP layers ------------------------------------------------
+    // hvel(MTOP) = hvL, harm(MTOP) = hhL, z_i(MTOP + 1) = zL
+    C hvT[MTOP + 1], zT[MTOP + 2];
+    E vT[MTOP + 1];
+    hvT[MTOP] = hvL;
+    vT[MTOP] = vL;
+    zT[MTOP + 1] = zL;
+    {
+        C hh = hhL;
+#pragma unroll
+        for (int k = MTOP; k >= 2; --k) {
+            zT[k] = zT[k + 1] + hh * I_Hbbl;                     // z_i(k)
+            const C h0 = hc[(size_t)(k - 2) * plane], h1 = hn_[(size_t)(k - 2) * plane];
+            const E vk = (E)vc[(size_t)(k - 2) * plane];
+            hh = harm(h0, h1);
+            hvT[k - 1] = hvel_h(vv_botfn<true>(zT[k]), hh, h0, h1, (C)vk);
+            vT[k - 1] = vk;
+        }
+    }
+    C ztop[MTOP + 1];   // z_top(K) = hvel(1) + ... + hvel(K - 1)
+    ztop[1] = C(0.0);
+#pragma unroll
+    for (int K = 2; K <= MTOP; ++K) ztop[K] = ztop[K - 1] + hvT[K - 1];
+#pragma unroll
+    for (int L = MTOP; L >= 1; --L) {
+        E aL = E(0.0);   // a(1) = 0, the surface
+        if (L >= 2) {
+            C Kv_tot = Kv;
+            if (ztop[L] < Hmix) Kv_tot = Kv_tot + (Kv_ml - Kv) * (C(1.0) - vv_div<true>(ztop[L], Hmix));
+            Kv_tot = Kv_tot + Kv_extra_bbl * vv_botfn<true>(zT[L]);
+            aL = (E)vv_div<true>(Kv_tot, C(0.5) * (hvT[L] + hvT[L - 1] + hn));
+        }
+        const E Rayk = ray_on[L - 1] ? (E)rc[(size_t)(L - 1) * plane] : E(0.0);
+        eliminate(L, hvT[L], aL, vT[L], Rayk, L == 1 ? sfc_stress : E(0.0));
+    }
+
+    // ---- downward sweep: back substitution u(L) = u'(L) + c1r(L) u(L - 1) ----
+    E u_above = up;   // u(1) = u'(1), already in place
+    for (int kt = 2; kt <= nz; kt += CH) {
+        E pv[CH], pc[CH];
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            const int L = kt + c;
+            if (L <= nz) {
+                pv[c] = (E)vc[(size_t)(L - 1) * plane];
+                pc[c] = slot[L];
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            const int L = kt + c;
+            if (L <= nz) {
+                const E uk = pv[c] + pc[c] * u_above;
+                vc[(size_t)(L - 1) * plane] = (R)uk;
+                u_above = uk;
+            }
+        }
+    }
+    // bottom stress (:452-458)
+    double tb = kRho0 * (double)u_above * (double)a_bot;
+    for (int k = 1; k <= nz; ++k)
+        if (ray_on[k - 1]) {
+            const size_t o = (size_t)(k - 1) * plane;
+            tb = tb + kRho0 * rc[o] * (double)vc[o];
+        }
+    tbot[(size_t)(j - 1) * D.n1 + (i - 1)] = tb;
+    return true;
+}
+
+// The fast forms' kernel: the two-sweep column where it applies, else the
+// three-sweep one.
+template <int KMAX, int CH, typename R, typename E, int MINB, bool ASYNC>
+__global__ void __launch_bounds__(128, MINB)
+k_vertvisc_up(Dims D, Metrics M, R* __restrict__ u, R* __restrict__ v, const R* __restrict__ h,
+              double dt, VVParams P, double* __restrict__ taux_bot,
+              double* __restrict__ tauy_bot)
+{
+    __shared__ R stage[2 * CH * 3 * 128];
+    if (!vertvisc_column_up<KMAX, CH, R, E>(D, M, u, v, h, dt, P, taux_bot, tauy_bot,
+                                             (int)blockIdx.x, (int)blockIdx.y, stage))
+        vertvisc_column<KMAX, CH, R, E, false, ASYNC, true>(D, M, u, v, h, dt, P, taux_bot,
+                                                            tauy_bot, (int)blockIdx.x,
+                                                            (int)blockIdx.y, nullptr, nullptr,
+                                                            stage);
+}
+
 // MINB: the CTAs per SM the register allocation is held to.
 template <int KMAX, int CH, typename R, typename E, int MINB = 1, bool REM = false,
           bool ASYNC = false, bool FAST = false>
@@ -428,7 +682,14 @@ static cudaError_t launch_vv_pf(const Dims& D, const Metrics& M, R* u, R* v, con
     int nrows = (D.je - D.js + 1) + (D.je - D.js + 2);
     dim3 grid((ncol + nb - 1) / nb, nrows, 1);
     constexpr int MB = vv_min_blocks<R, E>();
-    if constexpr (sizeof(R) == 8) {
+    if constexpr (FAST && sizeof(R) == 8) {
+        // the fast FP64 form: the two-sweep column (three sweeps where it does
+        // not apply); no remnant in the fast form.  (The mixed form keeps the
+        // three-sweep column, which its ensemble kernel shares.)
+        if (rem_u) return cudaErrorInvalidValue;
+        k_vertvisc_up<KMAX, kVvChunk, R, E, MB, true><<<grid, nb, 0, s>>>(
+            D, M, u, v, h, dt, P, taux_bot, tauy_bot);
+    } else if constexpr (sizeof(R) == 8) {
         if (rem_u)
             k_vertvisc_pf<KMAX, kVvChunk, R, E, MB, true, true, FAST><<<grid, nb, 0, s>>>(
                 D, M, u, v, h, dt, P, taux_bot, tauy_bot, rem_u, rem_v);

@@ -81,3 +81,28 @@ def test_fast_graph_replay_matches_eager():
     for n in STATE + ["uh", "hu_bt"]:
         assert np.array_equal(a.get(n), b.get(n)), n
 
+
+
+@pytest.mark.gpu
+def test_vertvisc_two_sweep_and_fallback_columns():
+    """The fast vertical viscosity eliminates bottom-up and back-substitutes
+    top-down where the top four layers' harmonic thicknesses reach Hmix (50 m),
+    and falls back to the three-sweep column elsewhere.  Half of this domain
+    gets 5 m surface layers (20 m in total: fallback), the rest keeps its
+    layers; the step's velocities, bottom stresses and thicknesses stay
+    within the bound of the exact form's in both halves."""
+    ni, nj, nk = 40, 30, 12
+    fast, exact = _models(ni, nj, nk, 40, INIT_CFG, 9)
+    h0 = exact.get("h0")
+    h0[:, : h0.shape[1] // 2, :4] = 5.0
+    for m in (fast, exact):
+        m.set("h0", h0)
+        m.set("h", h0)
+    fast.step(2)
+    exact.step(2)
+    for n in ("u", "v", "h", "up", "vp"):
+        a, b = fast.get(n), exact.get(n)
+        assert rel_l2(a, b) <= 1e-12, f"{n}: {describe(a, b)}"
+    for n in ("taux_bot", "tauy_bot"):
+        a, b = fast.get(n), exact.get(n)
+        assert rel_l2(a, b) <= 1e-11, f"{n}: {describe(a, b)}"
