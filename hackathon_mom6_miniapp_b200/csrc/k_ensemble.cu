@@ -160,10 +160,17 @@ k_ens_vertvisc(const EnsDomain* __restrict__ doms, const int* __restrict__ start
     const int local = b - __ldg(start + d);
     const int gx = (E.D.ie - E.D.is + 2 + NB - 1) / NB;
     const bool corr = half != 0;
-    vertvisc_column<KMAX, CH, float, double, false, false, true>(E.D, E.M, corr ? E.u : E.up, corr ? E.v : E.vp,
-                                             corr ? E.hB : E.h0, corr ? 0.5 * E.dt : E.dt,
-                                             E.VV, E.taux_bot, E.tauy_bot, local % gx,
-                                             local / gx);
+    // the single-domain mixed kernel's columns: two sweeps where they apply
+    __shared__ float stage[2 * CH * 3 * NB];
+    float* u = corr ? E.u : E.up;
+    float* v = corr ? E.v : E.vp;
+    const float* h = corr ? E.hB : E.h0;
+    const double dt = corr ? 0.5 * E.dt : E.dt;
+    if (!vertvisc_column_up<KMAX, CH, float, double, NB>(E.D, E.M, u, v, h, dt, E.VV, E.taux_bot,
+                                                         E.tauy_bot, local % gx, local / gx,
+                                                         stage))
+        vertvisc_column<KMAX, CH, float, double, false, false, true>(
+            E.D, E.M, u, v, h, dt, E.VV, E.taux_bot, E.tauy_bot, local % gx, local / gx);
 }
 
 template <int KMAX>

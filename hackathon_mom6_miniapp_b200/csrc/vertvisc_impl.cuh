@@ -418,7 +418,8 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
 // is the fast form's (vv_div, top-down botfn replaced by the bottom-up z_i).
 constexpr int kVvTop = 4;
 
-template <int KMAX, int CH, typename R, typename E, int MTOP = kVvTop>
+// NT: the threads of the CTA (the stride of stage, [2][CH][3][NT]).
+template <int KMAX, int CH, typename R, typename E, int NT = 128, int MTOP = kVvTop>
 __device__ __forceinline__ bool
 vertvisc_column_up(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restrict__ v,
                    const R* __restrict__ h, double dt, const VVParams& P,
@@ -487,7 +488,7 @@ vertvisc_column_up(const Dims& D, const Metrics& M, R* __restrict__ u, R* __rest
     const E dtE = (E)dt;
     const E sfc_stress = (E)(dt / kRho0 * MOM6B_A2(tau, i, j, D) * msk);
     const int tid = (int)threadIdx.x;
-    auto ST = [&](int b, int c, int f) -> R& { return stage[((b * CH + c) * 3 + f) * 128 + tid]; };
+    auto ST = [&](int b, int c, int f) -> R& { return stage[((b * CH + c) * 3 + f) * NT + tid]; };
 
     // ---- upward sweep: layer nz ----------------------------------------------
     C hhL, hvL;           // harm and hvel of the layer L being eliminated
@@ -682,12 +683,11 @@ static cudaError_t launch_vv_pf(const Dims& D, const Metrics& M, R* u, R* v, con
     int nrows = (D.je - D.js + 1) + (D.je - D.js + 2);
     dim3 grid((ncol + nb - 1) / nb, nrows, 1);
     constexpr int MB = vv_min_blocks<R, E>();
-    if constexpr (FAST && sizeof(R) == 8) {
-        // the fast FP64 form: the two-sweep column (three sweeps where it does
-        // not apply); no remnant in the fast form.  (The mixed form keeps the
-        // three-sweep column, which its ensemble kernel shares.)
+    if constexpr (FAST) {
+        // the fast FP64 and mixed forms: the two-sweep column (three sweeps
+        // where it does not apply); no remnant in these forms
         if (rem_u) return cudaErrorInvalidValue;
-        k_vertvisc_up<KMAX, kVvChunk, R, E, MB, true><<<grid, nb, 0, s>>>(
+        k_vertvisc_up<KMAX, kVvChunk, R, E, MB, (sizeof(R) == 8)><<<grid, nb, 0, s>>>(
             D, M, u, v, h, dt, P, taux_bot, tauy_bot);
     } else if constexpr (sizeof(R) == 8) {
         if (rem_u)
