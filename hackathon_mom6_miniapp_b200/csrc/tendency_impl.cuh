@@ -239,10 +239,16 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
 #define COR(i, j) ((R)(UNI ? U.cor_row[(j) - 1] : MOM6B_A2(M.CoriolisBu, i, j, D)))
 
     // ---- intermediates ----------------------------------------------------
-    for (int p = tid; p < CX * CY; p += TX * TY) {
+    // The items of intermediate point p = r CX + c: bit 0 the corner (q,
+    // str_xy), bit 1 the centre (KE, str_xx), bit 2 uh, bit 3 vh.  Every thread
+    // evaluates all items of its own point; with uniform metrics the CX CY -
+    // TX TY fringe points' items are then spread one per thread, so that no
+    // thread evaluates a second whole point while the rest of the CTA waits at
+    // the barrier.
+    auto interm = [&](int p, unsigned items) {
         int r = p / CX, c = p - r * CX;
         // corner point (I, J) = (i0-1+c, j0-1+r): q and str_xy
-        {
+        if (items & 1u) {
             int I = i0 - 1 + c, J = j0 - 1 + r;
             R qv = R(0.0), sxy = R(0.0);
             if (FU && I + 1 <= D.n1 && J + 1 <= D.n2) {
@@ -292,7 +298,7 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
             s_sxy[r][c] = sxy;
         }
         // centre point (i, j) = (i0+c, j0+r): KE and str_xx
-        {
+        if (items & 2u) {
             int i = i0 + c, j = j0 + r;
             R ke = R(0.0), sxx = R(0.0);
             if (FU && i <= D.n1 && j <= D.n2) {
@@ -320,7 +326,7 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
             s_sxx[r][c] = sxx;
         }
         // transports (compute_transports uses min(i+1, ied), min(j+1, jed))
-        {
+        if (items & 4u) {
             int I = i0 - 1 + c, J = j0 + r;
             R uhv = R(0.0);
             if (I <= D.n1 && J <= D.n2) {
@@ -330,6 +336,8 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
                 else uhv = SU(I, J) * R(0.5) * (SH(I, J) + hp) * G2(dyCu, I, J);
             }
             s_uh[r][c] = uhv;
+        }
+        if (items & 8u) {
             int i = i0 + c, j = j0 - 1 + r;
             R vhv = R(0.0);
             if (i <= D.n1 && j <= D.n2) {
@@ -340,6 +348,14 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
             }
             s_vh[r][c] = vhv;
         }
+    };
+    if constexpr (UNI) {
+        interm(tid, 15u);
+        constexpr int NF = CX * CY - NT;
+        for (int e = tid; e < 4 * NF; e += NT) interm(NT + e % NF, 1u << (e / NF));
+    } else {
+        // the 2-D metric form (more registers per point): whole points
+        for (int p = tid; p < CX * CY; p += NT) interm(p, 15u);
     }
     __syncthreads();
 

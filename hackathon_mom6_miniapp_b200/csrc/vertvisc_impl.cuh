@@ -603,11 +603,13 @@ vertvisc_column_up(const Dims& D, const Metrics& M, R* __restrict__ u, R* __rest
     }
 
     // ---- downward sweep: back substitution u(L) = u'(L) + c1r(L) u(L - 1) ----
+    // one multiply-add per layer: the loads of 2 CH layers are issued together
+    constexpr int CHD = 2 * CH;
     E u_above = up;   // u(1) = u'(1), already in place
-    for (int kt = 2; kt <= nz; kt += CH) {
-        E pv[CH], pc[CH];
+    for (int kt = 2; kt <= nz; kt += CHD) {
+        E pv[CHD], pc[CHD];
 #pragma unroll
-        for (int c = 0; c < CH; ++c) {
+        for (int c = 0; c < CHD; ++c) {
             const int L = kt + c;
             if (L <= nz) {
                 pv[c] = (E)vc[(size_t)(L - 1) * plane];
@@ -615,7 +617,7 @@ vertvisc_column_up(const Dims& D, const Metrics& M, R* __restrict__ u, R* __rest
             }
         }
 #pragma unroll
-        for (int c = 0; c < CH; ++c) {
+        for (int c = 0; c < CHD; ++c) {
             const int L = kt + c;
             if (L <= nz) {
                 const E uk = pv[c] + pc[c] * u_above;
