@@ -28,6 +28,8 @@ __device__ __forceinline__ double ppm_slope3(double hm, double hc, double hp, bo
 // Edge values of a cell from h of the cell and its neighbours, their masks
 // (ml, mr; oml = 1 - ml, omr = 1 - mr) and the slopes of cells i-1, i, i+1:
 // the rest of PPM_reconstruction_x and PPM_limit_pos (ppm_cell's operations).
+// FAST: the limiter's quotient (rounded to single precision) by div_nr.
+template <bool FAST = false>
 __device__ __forceinline__ void ppm_edges_limited(double hm1, double hc, double hp1, double ml,
                                                   double oml, double mr, double omr, double slm,
                                                   double slc, double slp, double h_min,
@@ -49,7 +51,9 @@ __device__ __forceinline__ void ppm_edges_limited(double hm1, double hc, double 
                 float den = __fadd_rn(__fmul_rn(curv, curv), __fmul_rn(3.0f, __fmul_rn(dh, dh)));
                 double lhs = (double)c12 * (hc - h_min);
                 if (lhs < (double)den) {
-                    float scale = (float)(lhs / (double)den);
+                    float scale;
+                    if constexpr (FAST) scale = (float)div_nr(lhs, (double)den);
+                    else scale = (float)(lhs / (double)den);
                     hL = hc + (double)scale * (hL - hc);
                     hR = hc + (double)scale * (hR - hc);
                 }
@@ -84,7 +88,9 @@ __device__ __forceinline__ Newton newton_start(double uh_err, double duhdu_tot,
 }
 
 // Iteration itt of zonal_flux_adjust up to its exit test (:829-883): bounds
-// the root, takes the Newton (or bisection) step; returns do_I.
+// the root, takes the Newton (or bisection) step; returns do_I.  FAST: the
+// Newton step's quotient by div_nr.
+template <bool FAST = false>
 __device__ __forceinline__ bool newton_iter(Newton& S, int itt, double tol_eta_dt_fac)
 {
     const double tol_eta_cs = 1.0e-12, tol_vel = 3.0e8;
@@ -101,7 +107,11 @@ __device__ __forceinline__ bool newton_iter(Newton& S, int itt, double tol_eta_d
         double ae = fabs(S.uh_err);
         if ((tol_eta_dt_fac * ae > tol_eta) ||
             ((ae > tol_vel * S.duhdu_tot) || (ae > S.uh_err_best))) {
-            double ddu = -(S.uh_err / S.duhdu_tot);
+            double ddu;
+            // (div_nr wants a normal divisor; a column without thickness keeps
+            // the IEEE quotient's infinity, which the bounds then catch)
+            if (FAST && fabs(S.duhdu_tot) > 1.0e-300) ddu = -div_nr(S.uh_err, S.duhdu_tot);
+            else ddu = -(S.uh_err / S.duhdu_tot);
             double du_prev = S.du;
             S.du = S.du + ddu;
             if (fabs(ddu) < F32(1.0e-15) * fabs(S.du)) {

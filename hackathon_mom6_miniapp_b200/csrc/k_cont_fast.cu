@@ -293,7 +293,8 @@ k_cont_fast(Dims D, Metrics M, const __grid_constant__ CUtensorMap map_u,
             const double slm = __shfl_up_sync(kFull, slc, 1);
             const double slp = __shfl_down_sync(kFull, slc, 1);
             double hL, hR;
-            ppm_edges_limited(hm, hc, hp, ml, oml, mr, omr, slm, slc, slp, h_min, hL, hR);
+            ppm_edges_limited<true>(hm, hc, hp, ml, oml, mr, omr, slm, slc, slp, h_min, hL,
+                                    hR);
             if (write) {
                 sh_ab[k * kCfAB + lane] = make_double2(0.5 * (hL + hR), 0.5 * (hL - hR));
                 sh_c3[k * kCfC3 + lane] = (hL + hR) - 2.0 * hc;
@@ -356,7 +357,7 @@ k_cont_fast(Dims D, Metrics M, const __grid_constant__ CUtensorMap map_u,
     Newton A = newton_start(uh_tot_0 - uhbt, duhdu_tot_0, du_max_CFL, du_min_CFL, face_ok);
     double du_eval = 0.0, sd_eval = duhdu_tot_0;
     for (int itt = 1; itt <= max_itts; ++itt) {
-        if (A.live) A.live = newton_iter(A, itt, fac);
+        if (A.live) A.live = newton_iter<true>(A, itt, fac);
         const bool pa = A.live;
         if (!__any_sync(kFull, pa)) break;
         double su = 0.0, sd = 0.0;
@@ -381,7 +382,7 @@ k_cont_fast(Dims D, Metrics M, const __grid_constant__ CUtensorMap map_u,
     if (__any_sync(kFull, solve0)) {
         Newton B = newton_start(uh_tot_0, duhdu_tot_0, du_max_CFL, du_min_CFL, solve0);
         for (int itt = 1; itt <= max_itts; ++itt) {
-            if (B.live) B.live = newton_iter(B, itt, fac);
+            if (B.live) B.live = newton_iter<true>(B, itt, fac);
             const bool pb = B.live && itt < max_itts;
             if (!__any_sync(kFull, pb)) break;
             double su = 0.0, sd = 0.0;
