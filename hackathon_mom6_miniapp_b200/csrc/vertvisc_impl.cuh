@@ -501,19 +501,41 @@ vertvisc_column_up(const Dims& D, const Metrics& M, R* __restrict__ u, R* __rest
     }
     // a(nz + 1), the bottom interface (:205-206)
     const C a_bot = vv_div<true>(Kv + Kv_extra_bbl, C(0.5) * hvL + hn);
-    E a_below = (E)a_bot;        // a(L + 1)
-    E d1 = E(1.0), up = E(0.0);  // d1 and the eliminated velocity of layer L + 1
+    // FP64 storage: with a(L) = Kv_tot / h_shear, the step's products of
+    // dt a(L + 1) are carried instead of a(L + 1): Pd = dt a(L + 1) d1(L + 1)
+    // and Pu = dt a(L + 1) u'(L + 1) (at the bottom d1 = 1 and u' = 0: the
+    // zero-velocity bottom).  With K = dt Kv_tot(L), S = h_shear(L) and r =
+    // 1 / (bd S + K), b1 = S r, dt a(L) b1 = K r, dt a(L) d1 = K bd r and
+    // dt a(L) u' = K rhs r, so a layer takes one quotient instead of two (a(L)
+    // and b1).  FP32 storage (the mixed form, whose kernels are held to 64
+    // registers) keeps a(L) and the two quotients.
+    E Pd = dtE * (E)a_bot, Pu = E(0.0);
+    E a_below = (E)a_bot, d1 = E(1.0);
+    E up = E(0.0);               // the eliminated velocity of the last layer
     C zL = C(0.0);               // z_i(L + 1)
-    // eliminate layer L with a(L) above it (u'(L) -> vel(L), c1r(L) -> slot)
-    auto eliminate = [&](int L, C hv, E aL, E vk, E Rayk, E rhs_extra) {
+    // eliminate layer L with a(L) = Kv_tot / h_shear above it (u'(L) ->
+    // vel(L), c1r(L) -> slot); Kv_tot = 0, h_shear = 1 at the surface (a(1) = 0)
+    auto eliminate = [&](int L, C hv, C Kv_tot, C h_shear, E vk, E Rayk, E rhs_extra) {
         const E hu = (E)(hv + hn);
-        const E bd = hu + dtE * (Rayk + a_below * d1);
-        const E b1 = vv_div<true>(E(1.0), bd + dtE * aL);
-        d1 = bd * b1;
-        up = (hu * vk + rhs_extra + dtE * a_below * up) * b1;
+        if constexpr (sizeof(R) == 8) {
+            const E K = dtE * (E)Kv_tot, S = (E)h_shear;
+            const E bd = hu + (dtE * Rayk + Pd);
+            const E r = vv_div<true>(E(1.0), bd * S + K);
+            const E rhs = hu * vk + rhs_extra + Pu;
+            up = rhs * (S * r);
+            slot[L] = K * r;
+            Pd = K * bd * r;
+            Pu = K * rhs * r;
+        } else {
+            const E aL = (E)vv_div<true>(Kv_tot, h_shear);
+            const E bd = hu + dtE * (Rayk + a_below * d1);
+            const E b1 = vv_div<true>(E(1.0), bd + dtE * aL);
+            d1 = bd * b1;
+            up = (hu * vk + rhs_extra + dtE * a_below * up) * b1;
+            slot[L] = dtE * aL * b1;
+            a_below = aL;
+        }
         vc[(size_t)(L - 1) * plane] = (R)up;
-        slot[L] = dtE * aL * b1;
-        a_below = aL;
     };
     // lookahead layers L - 1 of the chunk's layers L = Lt .. Lt - CH + 1 (those
     // with L >= MTOP + 1) into buffer b; every staged velocity is read before
@@ -557,10 +579,9 @@ vertvisc_column_up(const Dims& D, const Metrics& M, R* __restrict__ u, R* __rest
                 const C hhu = harm(p0[c], p1[c]);                // layer L - 1
                 const C bfL = vv_botfn<true>(z_L);
                 const C hvu = hvel_h(bfL, hhu, p0[c], p1[c], (C)pv[c]);
-                // a(L) below the untapered depth (:185-202)
-                const C aL = vv_div<true>(Kv + Kv_extra_bbl * bfL,
-                                          C(0.5) * (hvL + hvu + hn));
-                eliminate(L, hvL, (E)aL, vL, pr[c], E(0.0));
+                // a(L) below the untapered depth (:185-202), as Kv_tot / h_shear
+                eliminate(L, hvL, Kv + Kv_extra_bbl * bfL, C(0.5) * (hvL + hvu + hn), vL,
+                          pr[c], E(0.0));
                 zL = z_L; hhL = hhu; hvL = hvu; vL = pv[c];
             }
         }
@@ -591,29 +612,37 @@ vertvisc_column_up(const Dims& D, const Metrics& M, R* __restrict__ u, R* __rest
     for (int K = 2; K <= MTOP; ++K) ztop[K] = ztop[K - 1] + hvT[K - 1];
 #pragma unroll
     for (int L = MTOP; L >= 1; --L) {
-        E aL = E(0.0);   // a(1) = 0, the surface
+        C Kv_tot = C(0.0), h_shear = C(1.0);   // a(1) = 0, the surface
         if (L >= 2) {
-            C Kv_tot = Kv;
+            Kv_tot = Kv;
             if (ztop[L] < Hmix) Kv_tot = Kv_tot + (Kv_ml - Kv) * (C(1.0) - vv_div<true>(ztop[L], Hmix));
             Kv_tot = Kv_tot + Kv_extra_bbl * vv_botfn<true>(zT[L]);
-            aL = (E)vv_div<true>(Kv_tot, C(0.5) * (hvT[L] + hvT[L - 1] + hn));
+            h_shear = C(0.5) * (hvT[L] + hvT[L - 1] + hn);
         }
         const E Rayk = ray_on[L - 1] ? (E)rc[(size_t)(L - 1) * plane] : E(0.0);
-        eliminate(L, hvT[L], aL, vT[L], Rayk, L == 1 ? sfc_stress : E(0.0));
+        eliminate(L, hvT[L], Kv_tot, h_shear, vT[L], Rayk, L == 1 ? sfc_stress : E(0.0));
     }
 
     // ---- downward sweep: back substitution u(L) = u'(L) + c1r(L) u(L - 1) ----
     // one multiply-add per layer: the loads of 2 CH layers are issued together
+    // The Rayleigh part of the bottom stress (:452-458) is summed in the serial
+    // order of the layers from the stored velocities: on the way down for FP64
+    // storage, by a pass of its own for FP32 storage (64 registers).
+    constexpr bool RAY_DOWN = sizeof(R) == 8;
     constexpr int CHD = 2 * CH;
     E u_above = up;   // u(1) = u'(1), already in place
+    double tray = (RAY_DOWN && ray_on[0]) ? kRho0 * rc[0] * (double)(R)up : 0.0;
     for (int kt = 2; kt <= nz; kt += CHD) {
         E pv[CHD], pc[CHD];
+        double pr[RAY_DOWN ? CHD : 1];
 #pragma unroll
         for (int c = 0; c < CHD; ++c) {
             const int L = kt + c;
             if (L <= nz) {
                 pv[c] = (E)vc[(size_t)(L - 1) * plane];
                 pc[c] = slot[L];
+                if constexpr (RAY_DOWN)
+                    pr[c] = ray_on[L - 1] ? rc[(size_t)(L - 1) * plane] : 0.0;
             }
         }
 #pragma unroll
@@ -623,17 +652,19 @@ vertvisc_column_up(const Dims& D, const Metrics& M, R* __restrict__ u, R* __rest
                 const E uk = pv[c] + pc[c] * u_above;
                 vc[(size_t)(L - 1) * plane] = (R)uk;
                 u_above = uk;
+                if constexpr (RAY_DOWN)
+                    if (pr[c] != 0.0) tray = tray + kRho0 * pr[c] * (double)(R)uk;
             }
         }
     }
-    // bottom stress (:452-458)
-    double tb = kRho0 * (double)u_above * (double)a_bot;
-    for (int k = 1; k <= nz; ++k)
-        if (ray_on[k - 1]) {
-            const size_t o = (size_t)(k - 1) * plane;
-            tb = tb + kRho0 * rc[o] * (double)vc[o];
-        }
-    tbot[(size_t)(j - 1) * D.n1 + (i - 1)] = tb;
+    if constexpr (!RAY_DOWN) {
+        for (int k = 1; k <= nz; ++k)
+            if (ray_on[k - 1]) {
+                const size_t o = (size_t)(k - 1) * plane;
+                tray = tray + kRho0 * rc[o] * (double)vc[o];
+            }
+    }
+    tbot[(size_t)(j - 1) * D.n1 + (i - 1)] = kRho0 * (double)u_above * (double)a_bot + tray;
     return true;
 }
 
