@@ -136,10 +136,14 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
     __shared__ R s_u[AB][AY][AX], s_v[AB][AY][AX], s_h[AB][AY][AX];
     __shared__ __align__(128) R s_t[TMA ? 2 * 3 * TPAD : 1];
     __shared__ __align__(8) uint64_t s_tbar[2];
-    __shared__ R s_q[CY][CX], s_sxy[CY][CX];   // corners  [i0-1, i0+TX-1] x [j0-1, j0+TY-1]
-    __shared__ R s_ke[CY][CX], s_sxx[CY][CX];  // centres  [i0, i0+TX] x [j0, j0+TY]
-    __shared__ R s_uh[CY][CX];                 // u-faces  [i0-1, i0+TX-1] x [j0, j0+TY]
-    __shared__ R s_vh[CY][CX];                 // v-faces  [i0, i0+TX] x [j0-1, j0+TY-1]
+    // the intermediates; with TMA tiles two sets, layer k in set k & 1, so
+    // that layer k + 1's intermediates never overwrite what layer k's outputs
+    // still read and one barrier per layer suffices
+    constexpr int IB = TMA ? 2 : 1;
+    __shared__ R s_q[IB][CY][CX], s_sxy[IB][CY][CX];   // corners  [i0-1, i0+TX-1] x [j0-1, j0+TY-1]
+    __shared__ R s_ke[IB][CY][CX], s_sxx[IB][CY][CX];  // centres  [i0, i0+TX] x [j0, j0+TY]
+    __shared__ R s_uh[IB][CY][CX];                     // u-faces  [i0-1, i0+TX-1] x [j0, j0+TY]
+    __shared__ R s_vh[IB][CY][CX];                     // v-faces  [i0, i0+TX] x [j0-1, j0+TY-1]
 
     const int i0 = D.is + bx * TX;
     const int j0 = D.js + by * TY;
@@ -193,31 +197,30 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
         }
         __syncthreads();
     }
+    // TMA: layers kb and kb + 1 are requested up front and layer k + 2 as soon
+    // as every thread is done with layer k's tile (after its intermediates);
+    // the element-wise staging requests layer k + 1 at the top of layer k
     if (kb <= ke) stage(kb, 0);
+    if (TMA && kb + 1 <= ke) stage(kb + 1, 1);
+    // buffer b's n-th use (layer kb + 2 n + b) completes its phase of parity n & 1
+    auto parity = [&](int k) { return (uint32_t)(((k - kb) >> 1) & 1); };
   for (int k = kb; k <= ke; ++k) {
     const size_t koff = (size_t)(k - 1) * (size_t)D.plane;
     const int b = (k - kb) & 1;
-    // layer k's tiles are visible to all threads, and every thread is done
-    // with layer k-1 (its outputs read buffer b^1 and the intermediates)
+    const int ib = TMA ? b : 0;
+    bool late = false;
     if constexpr (TMA) {
-        // buffer b's (k - kb) / 2-th use completes its phase of that parity
-        const bool late = !tma_bar_wait(&s_tbar[b], (uint32_t)(((k - kb) >> 1) & 1),
-                                        kBtDefaultWait);
-        if (__syncthreads_or(late)) {
-            if (tid == 0) {
-                if (status) atomicExch(status, kDevTimeout);
-                // the load still in flight lands in this CTA's shared memory:
-                // wait for it once more (bounded) before the CTA exits
-                tma_bar_wait(&s_tbar[b], (uint32_t)(((k - kb) >> 1) & 1), kBtDefaultWait);
-            }
-            __syncthreads();
-            return;
-        }
+        // layer k's tiles; no barrier: the intermediates' set ib was last read
+        // by layer k - 2's outputs, which every thread finished before layer
+        // k - 1's barrier
+        late = !tma_bar_wait(&s_tbar[b], parity(k), kBtDefaultWait);
     } else {
+        // layer k's tiles are visible to all threads, and every thread is done
+        // with layer k-1 (its outputs read buffer b^1 and the intermediates)
         cp_async_wait_all();
         __syncthreads();
+        if (k < ke) stage(k + 1, b ^ 1);
     }
-    if (k < ke) stage(k + 1, b ^ 1);
     const R* t_u = TMA ? &s_t[(b * 3 + 0) * TPAD] : &s_u[b][0][0];
     const R* t_v = TMA ? &s_t[(b * 3 + 1) * TPAD] : &s_v[b][0][0];
     const R* t_h = TMA ? &s_t[(b * 3 + 2) * TPAD] : &s_h[b][0][0];
@@ -294,8 +297,8 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
                 sxy = sxy * (hq * mBu * G2(red_xy, I, J));
                 }
             }
-            s_q[r][c] = qv;
-            s_sxy[r][c] = sxy;
+            s_q[ib][r][c] = qv;
+            s_sxy[ib][r][c] = sxy;
         }
         // centre point (i, j) = (i0+c, j0+r): KE and str_xx
         if (items & 2u) {
@@ -322,8 +325,8 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
                 sxx = sxx * (SH(i, j) * G2(red_xx, i, j));
                 }
             }
-            s_ke[r][c] = ke;
-            s_sxx[r][c] = sxx;
+            s_ke[ib][r][c] = ke;
+            s_sxx[ib][r][c] = sxx;
         }
         // transports (compute_transports uses min(i+1, ied), min(j+1, jed))
         if (items & 4u) {
@@ -335,7 +338,7 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
                 if constexpr (FU) uhv = (R(U.tf.kTu) * SU(I, J)) * (SH(I, J) + hp);
                 else uhv = SU(I, J) * R(0.5) * (SH(I, J) + hp) * G2(dyCu, I, J);
             }
-            s_uh[r][c] = uhv;
+            s_uh[ib][r][c] = uhv;
         }
         if (items & 8u) {
             int i = i0 + c, j = j0 - 1 + r;
@@ -346,7 +349,7 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
                 if constexpr (FU) vhv = (R(U.tf.kTv) * SV(i, j)) * (SH(i, j) + hp);
                 else vhv = SV(i, j) * R(0.5) * (SH(i, j) + hp) * G2(dxCv, i, j);
             }
-            s_vh[r][c] = vhv;
+            s_vh[ib][r][c] = vhv;
         }
     };
     if constexpr (UNI) {
@@ -357,14 +360,31 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
         // the 2-D metric form (more registers per point): whole points
         for (int p = tid; p < CX * CY; p += NT) interm(p, 15u);
     }
-    __syncthreads();
+    // the thicknesses the outputs read, so that the tile is free after the barrier
+    const R hIj = SH(Io, jo), hIpj = SH(Io + 1, jo), hIjp = SH(Io, jo + 1);
+    if constexpr (TMA) {
+        if (__syncthreads_or(late)) {
+            if (tid == 0) {
+                if (status) atomicExch(status, kDevTimeout);
+                // the loads still in flight land in this CTA's shared memory:
+                // wait for them once more (bounded) before the CTA exits
+                tma_bar_wait(&s_tbar[b], parity(k), kBtDefaultWait);
+                if (k + 1 <= ke) tma_bar_wait(&s_tbar[b ^ 1], parity(k + 1), kBtDefaultWait);
+            }
+            __syncthreads();
+            return;
+        }
+        if (k + 2 <= ke) stage(k + 2, b);
+    } else {
+        __syncthreads();
+    }
 
-#define Q(I, J) s_q[(J) - (j0 - 1)][(I) - (i0 - 1)]
-#define SXY(I, J) s_sxy[(J) - (j0 - 1)][(I) - (i0 - 1)]
-#define KE(i, j) s_ke[(j) - j0][(i) - i0]
-#define SXX(i, j) s_sxx[(j) - j0][(i) - i0]
-#define UH(I, J) s_uh[(J) - j0][(I) - (i0 - 1)]
-#define VH(i, j) s_vh[(j) - (j0 - 1)][(i) - i0]
+#define Q(I, J) s_q[ib][(J) - (j0 - 1)][(I) - (i0 - 1)]
+#define SXY(I, J) s_sxy[ib][(J) - (j0 - 1)][(I) - (i0 - 1)]
+#define KE(i, j) s_ke[ib][(j) - j0][(i) - i0]
+#define SXX(i, j) s_sxx[ib][(j) - j0][(i) - i0]
+#define UH(I, J) s_uh[ib][(J) - j0][(I) - (i0 - 1)]
+#define VH(i, j) s_vh[ib][(j) - (j0 - 1)][(i) - i0]
 
     const int I = i0 + (int)threadIdx.x;
     const int j = j0 + (int)threadIdx.y;
@@ -376,7 +396,7 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
         const R diffu =
             td_div<FAST>(td_fma(R(U.tf.kDq), SXY(I, j - 1) - SXY(I, j),
                                 R(U.tf.kDh) * (SXX(I, j) - SXX(I + 1, j))),
-                         td_fma(R(U.tf.kHm), SH(I, j) + SH(I + 1, j), h_neglect));
+                         td_fma(R(U.tf.kHm), hIj + hIpj, h_neglect));
         uout[oo] = td_fma(coef, CAu + diffu, ub);
     } else if (I <= D.ie - 1 + D.ce && j <= D.je) {
         R IdxCu = G2(IdxCu, I, j);
@@ -401,7 +421,7 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
         if constexpr (EXTV) {
             diffu = dfu[oo];
         } else {
-            R h_u = R(0.5) * (G2(mask2dT, I, j) * SH(I, j) + G2(mask2dT, I + 1, j) * SH(I + 1, j));
+            R h_u = R(0.5) * (G2(mask2dT, I, j) * hIj + G2(mask2dT, I + 1, j) * hIpj);
             diffu = td_div<FAST>((IdxCu * ((G2(dx2q, I, j - 1) * SXY(I, j - 1)) -
                                     (G2(dx2q, I, j) * SXY(I, j))) +
                            G2(IdyCu, I, j) * ((G2(dy2h, I, j) * SXX(I, j)) -
@@ -421,7 +441,7 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
         const R diffv =
             td_div<FAST>(td_fma(R(U.tf.kEq), SXY(i - 1, J) - SXY(i, J),
                                 -(R(U.tf.kEh) * (SXX(i, J) - SXX(i, J + 1)))),
-                         td_fma(R(U.tf.kHm), SH(i, J) + SH(i, J + 1), h_neglect));
+                         td_fma(R(U.tf.kHm), hIj + hIjp, h_neglect));
         vout[oo] = td_fma(coef, CAv + diffv, vb);
     } else if (I <= D.ie && j <= D.je - 1 + D.cn) {
         const int i = I, J = j;
@@ -450,7 +470,7 @@ tendency_tile(const Dims& D, const Metrics& M, const UniMetrics& U, const R* __r
         if constexpr (EXTV) {
             diffv = dfv[oo];
         } else {
-            R h_v = R(0.5) * (G2(mask2dT, i, J) * SH(i, J) + G2(mask2dT, i, J + 1) * SH(i, J + 1));
+            R h_v = R(0.5) * (G2(mask2dT, i, J) * hIj + G2(mask2dT, i, J + 1) * hIjp);
             diffv = td_div<FAST>((IdyCv * ((G2(dy2q, i - 1, J) * SXY(i - 1, J)) -
                                     (G2(dy2q, i, J) * SXY(i, J))) -
                            G2(IdxCv, i, J) * ((G2(dx2h, i, J) * SXX(i, J)) -
