@@ -583,12 +583,13 @@ cudaError_t launch_tendency_arakawa(const Dims& D, const Metrics& M, const UniMe
     return cudaGetLastError();
 }
 
-constexpr int kTendTX = 32, kTendTY = 8, kTendKC = 5;
+constexpr int kTendTX = 32, kTendTY = 8, kTendKC = 15;
 
 // Host launcher: one CTA per (TX x TY) tile of the compute domain and chunk of
-// kTendKC layers (5, 8, 15 and 25 layers per CTA measure the same on B200:
-// FP64 2.00-2.01 ms per step, mixed 1.49 -- the staging of the first layer of
-// a chunk is hidden by the other resident CTAs).
+// kTendKC layers (with the one-barrier TMA loop, 15 layers per CTA: 1.394 ms
+// per step at 720x720x75 against 1.397 for 8 and 1.411 for 5 -- the first two
+// layers of a chunk, requested up front, are the only loads a CTA waits for
+// unhidden by its own work).
 // dfu, dfv (both or neither): also store diffu, diffv (the diagnostic form of
 // the kernel; the step's own launches pass neither).  scheme: the Coriolis
 // scheme (1 SADOURNY75_ENERGY, 2 ARAKAWA_HSU90, 3 ARAKAWA_LAMB81).  FAST: the
