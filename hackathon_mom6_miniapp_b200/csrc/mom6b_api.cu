@@ -88,6 +88,9 @@ struct mom6b_model {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     bool overlap_bt = false;
+    // set by mom6b_step_host_io for one eager step: the barotropic chain on
+    // s2d, which the caller has already forked from s3d
+    bool split_bt = false;
     bool timing = false;
     int stall_test = 0;   // BTParams::stall_test of the step's barotropic loops
     std::vector<TimedLaunch> pending;
@@ -688,7 +691,7 @@ static int enqueue_step(mom6b_model* m)
     cudaStream_t s = m->s3d;
     // The barotropic chain only needs co-residency of its own blocks; it is
     // overlapped with the 3-D chain only when enabled.
-    cudaStream_t s2 = (m->overlap_bt && !m->xfn) ? m->s2d : m->s3d;
+    cudaStream_t s2 = ((m->overlap_bt || m->split_bt) && !m->xfn) ? m->s2d : m->s3d;
     const double dt = c.dt;
     // the halo exchange of a decomposed run (none for a whole domain)
     auto xch = [&](double* f, int nz, int kind, int more, cudaStream_t st) -> int {
@@ -707,8 +710,8 @@ static int enqueue_step(mom6b_model* m)
     ContOut OA = OB;
     OA.h = m->hA;
 
-    // fork the barotropic chain onto its own stream
-    if (s2 != s) {
+    // fork the barotropic chain onto its own stream (split_bt: the caller did)
+    if (s2 != s && !m->split_bt) {
         CK(cudaEventRecord(m->ev_fork, s));
         CK(cudaStreamWaitEvent(s2, m->ev_fork, 0));
     }
@@ -1262,11 +1265,31 @@ extern "C" int mom6b_step_host_io(mom6b_model* m, int nsteps, const double* u_in
         return check_status(m);
     }
     CK(cudaStreamSynchronize(m->s2d));
+    // One plain step: the barotropic chain reads only eta, ubt and vbt, so it
+    // runs on its own stream as soon as eta has arrived, while u and v are
+    // still being uploaded for the 3-D chain (eager launches; the fields equal
+    // those of mom6b_step).
+    const bool split = nsteps == 1 && !m->cfg.cuts && !m->xfn && !m->diag_driver &&
+                       !(m->sur && m->sur_on) && !m->timing;
+    if (split) {
+        CK(cudaEventRecord(m->ev_fork, s));
+        CK(cudaStreamWaitEvent(m->s2d, m->ev_fork, 0));
+        if (eta_in)
+            CK(cudaMemcpyAsync(m->eta, eta_in, n2 * sizeof(double), cudaMemcpyHostToDevice,
+                               m->s2d));
+    }
     if (u_in) CK(cudaMemcpyAsync(m->u, u_in, n3 * sizeof(double), cudaMemcpyHostToDevice, s));
     if (v_in) CK(cudaMemcpyAsync(m->v, v_in, n3 * sizeof(double), cudaMemcpyHostToDevice, s));
-    if (eta_in)
-        CK(cudaMemcpyAsync(m->eta, eta_in, n2 * sizeof(double), cudaMemcpyHostToDevice, s));
-    if (int rc = mom6b_step(m, nsteps)) return rc;
+    if (split) {
+        m->split_bt = true;
+        const int rc = enqueue_step(m);
+        m->split_bt = false;
+        if (rc) return rc;
+    } else {
+        if (eta_in)
+            CK(cudaMemcpyAsync(m->eta, eta_in, n2 * sizeof(double), cudaMemcpyHostToDevice, s));
+        if (int rc = mom6b_step(m, nsteps)) return rc;
+    }
     if (u_out) CK(cudaMemcpyAsync(u_out, m->u, n3 * sizeof(double), cudaMemcpyDeviceToHost, s));
     if (v_out) CK(cudaMemcpyAsync(v_out, m->v, n3 * sizeof(double), cudaMemcpyDeviceToHost, s));
     if (h_out) CK(cudaMemcpyAsync(h_out, m->hA, n3 * sizeof(double), cudaMemcpyDeviceToHost, s));

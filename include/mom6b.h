@@ -152,7 +152,9 @@ int mom6b_step_host(mom6b_model *m, int nsteps, double *u, double *v, double *h,
  * eta_in (the state a step reads; h restarts from h0 at every step,
  * rk2_serial_driver.F90:225-232, so an uploaded h would be overwritten
  * unread), run nsteps, download u_out, v_out, h_out, eta_out.  Any pointer
- * may be NULL; an input and an output may be the same buffer. */
+ * may be NULL; an input and an output may be the same buffer.  With
+ * nsteps = 1 (FP64, a whole domain) the barotropic chain, which reads only
+ * eta, ubt and vbt, runs beside the upload of u and v. */
 int mom6b_step_host_io(mom6b_model *m, int nsteps, const double *u_in, const double *v_in,
                        const double *eta_in, double *u_out, double *v_out, double *h_out,
                        double *eta_out);

@@ -125,6 +125,25 @@ def test_step_host_io_roundtrip():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("exact", [True, False])
+def test_step_host_io_one_step_calls(exact):
+    """One-step calls run the barotropic chain on its own stream beside the
+    upload of u and v; the fields equal those of mom6b_step's steps."""
+    from hackathon_mom6_miniapp_b200 import Model
+    g = Model(36, 30, 8, 40, INIT_CFG, seed=8, exact=exact)
+    ref = Model(36, 30, 8, 40, INIT_CFG, seed=8, exact=exact)
+    u, v, eta = (np.asfortranarray(g.get(n)) for n in ("u", "v", "eta"))
+    h = np.zeros_like(u, order="F")
+    for _ in range(3):
+        g.step_host_io(1, u, v, eta, u, v, h, eta)
+    ref.step(3)
+    for n, a in zip(("u", "v", "h", "eta"), (u, v, h, eta)):
+        assert np.array_equal(a, ref.get(n)), n
+    for n in ("ubt_av", "vbt_av", "eta_av", "up", "vp"):
+        assert np.array_equal(g.get(n), ref.get(n)), n
+
+
+@pytest.mark.gpu
 def test_step_host_roundtrip():
     from hackathon_mom6_miniapp_b200 import Model
     o, g = _pair(24, 20, 6, 40, INIT_CFG, seed=8)
