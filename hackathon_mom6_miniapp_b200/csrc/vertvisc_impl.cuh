@@ -414,8 +414,9 @@ vertvisc_column(const Dims& D, const Metrics& M, R* __restrict__ u, R* __restric
 // sweep (staged in shared memory, CH layers ahead, with cp.async), the
 // eliminated velocity and the multiplier once by the downward one.
 // Within a few units in the last place of the top-down elimination (the
-// system is diagonally dominant); the serial arithmetic of each coefficient
-// is the fast form's (vv_div, top-down botfn replaced by the bottom-up z_i).
+// system is diagonally dominant); each coefficient follows the serial
+// expressions with vv_div quotients, and z_i is summed bottom-up as the serial
+// code sums it.
 constexpr int kVvTop = 4;
 
 // NT: the threads of the CTA (the stride of stage, [2][CH][3][NT]).
