@@ -77,20 +77,13 @@ __device__ __forceinline__ void arakawa_bc(R q00, R qm0, R q0m, R qmm, R& b, R& 
     }
 }
 
-// EXTV: diffu, diffv come from dfu, dfv (the general hor_visc kernel's
-// outputs) and the stresses are not evaluated.
-// COR: the Coriolis scheme of CorAdCalc (mom6_coriolis_serial.F90:19-21):
-// 1 SADOURNY75_ENERGY (the driver's), 2 ARAKAWA_HSU90, 3 ARAKAWA_LAMB81.  The
-// Arakawa schemes' coefficients a, b, c, d (:171-193) reach q one corner
-// further east and north, so their tiles stage and evaluate one more column
-// and row; the coefficients are formed where CAu / CAv need them (:228-248).
-// FAST: the fast FP64 form's arithmetic (built with FMA contraction in
-// k_tendency_fast.cu): quotients by div_nr.
-// multiply-add in the stencil type (the folded stencils of the fast FP64 and
-// the mixed forms)
+// Multiply-add in the stencil type (the folded stencils of the fast FP64 and
+// the mixed forms).
 __device__ __forceinline__ double td_fma(double a, double b, double c) { return fma(a, b, c); }
 __device__ __forceinline__ float td_fma(float a, float b, float c) { return fmaf(a, b, c); }
 
+// Quotients of the tendency: div_nr in the fast FP64 form, IEEE division in
+// the exact form, div_r in float.
 template <bool FAST>
 __device__ __forceinline__ double td_div(double a, double b)
 {
@@ -100,6 +93,15 @@ __device__ __forceinline__ double td_div(double a, double b)
 template <bool FAST>
 __device__ __forceinline__ float td_div(float a, float b) { return div_r(a, b); }
 
+// EXTV: diffu, diffv come from dfu, dfv (the general hor_visc kernel's
+// outputs) and the stresses are not evaluated.
+// COR: the Coriolis scheme of CorAdCalc (mom6_coriolis_serial.F90:19-21):
+// 1 SADOURNY75_ENERGY (the driver's), 2 ARAKAWA_HSU90, 3 ARAKAWA_LAMB81.  The
+// Arakawa schemes' coefficients a, b, c, d (:171-193) reach q one corner
+// further east and north, so their tiles stage and evaluate one more column
+// and row; the coefficients are formed where CAu / CAv need them (:228-248).
+// FAST: the fast FP64 form's arithmetic (built with FMA contraction in
+// k_tendency_fast.cu): quotients by div_nr.
 // TMA: the u, v, h tiles of a layer arrive as three TMA box loads
 // ({SX, SY, 1} of the fields' tensor maps tmaps[0..2]) issued by one thread
 // into 128-byte-aligned double buffers, completing on one mbarrier per
