@@ -701,9 +701,10 @@ k_vertvisc_pf(Dims D, Metrics M, R* __restrict__ u, R* __restrict__ v,
                                                       (int)blockIdx.y, rem_u, rem_v, stage);
 }
 
-// Launch shapes measured fastest on B200 at 720x720x75: the FP64 form stages
-// sweeps 1 and 2 with cp.async and holds registers to 6 CTAs per SM (2.215 ms
-// per step against 2.285 loaded into registers); the FP32-storage forms load
+// Launch shapes measured fastest on B200 at 720x720x75: the fast FP64 and
+// mixed forms run the two-sweep kernel; the exact FP64 form stages sweeps 1
+// and 2 with cp.async and holds registers to 6 CTAs per SM (2.215 ms per step
+// against 2.285 loaded into registers); the other FP32-storage forms load
 // 4-layer chunks into registers (staging measured slower there), held to
 // vv_min_blocks CTAs per SM.
 template <int KMAX, typename R, typename E, bool FAST>
