@@ -4,7 +4,7 @@ The fast kernels may contract multiply-adds, form quotients by refined
 reciprocals and sum columns in another order (the continuity kernel splits
 each face column over 8 lanes and combines their partial sums by shuffles;
 the vertical viscosity forms its bottom-boundary function top-down), so they
-are held to the north-star bound instead of bit equality: relative L2 <=
+are held to the step's parity bound instead of bit equality: relative L2 <=
 1e-12 per prognostic field after 10 steps, and the continuity and vertical
 viscosity outputs of a step (transports, face thicknesses, BT_cont face
 areas and velocities, bottom stresses) close to the exact form's.  Shapes

@@ -1,6 +1,6 @@
 """GPU parity of the fused FP64 split RK2 step against the oracle.
 
-The oracle restates rk2_serial_driver.F90 + src/serial/*.F90.  The north-star
+The oracle restates rk2_serial_driver.F90 + src/serial/*.F90.  The parity
 bound is a relative L2 error of at most 1e-12 per prognostic field after 10
 steps; the kernels are built without FMA contraction and are designed to
 match the oracle bit for bit, which test_bitwise_* checks separately.
@@ -11,7 +11,7 @@ import pytest
 from oracle.pyoracle import INIT_CFG, INIT_REF, Oracle
 from tests.util import describe, rel_l2
 
-TOL = 1e-12   # north-star tolerance, relative L2 per field
+TOL = 1e-12   # parity tolerance, relative L2 per field
 STATE = ["h", "u", "v", "eta", "ubt", "vbt"]
 EXTRA = ["ubt_av", "vbt_av", "eta_av", "up", "vp"]
 
@@ -188,7 +188,7 @@ def test_config0_as_written(exact):
     180x180x75, 10 steps -- at bt_nsteps = 31, the fewest substeps at which
     the serial scheme is stable at this time step (30 diverges in the oracle
     itself, tests/test_config0.py).  Every prognostic field within the
-    north-star 1e-12 relative L2 of the oracle (OpenMP build, identical to
+    1e-12 relative L2 parity bound of the oracle (OpenMP build, identical to
     the serial one); the exact form bit for bit."""
     from hackathon_mom6_miniapp_b200 import Model
     o = Oracle(180, 180, 75, 31, INIT_CFG, seed=0, dt=600.0, threads=0)
@@ -270,7 +270,7 @@ def _golden_module():
 @pytest.mark.parametrize("exact", [True, False])
 def test_golden_fixtures(case, exact):
     """The committed oracle fixtures (tests/golden): the exact form equals them
-    bit for bit, the fast form within the north-star 1e-12 per field."""
+    bit for bit, the fast form within the 1e-12 parity bound per field."""
     import os
     from hackathon_mom6_miniapp_b200 import Model
     g = np.load(os.path.join(os.path.dirname(__file__), "golden", f"{case}.npz"))
